@@ -1,0 +1,160 @@
+// Algorithm handles behind the C ABI: the kNN handle and the k-means handle,
+// both templated on the working precision (float / double) like the
+// reference's basic_handle<T> family (source/core/utilities/basic_handle.hpp).
+#pragma once
+#include "b200_kernels.hpp"
+#include "host_common.hpp"
+#include <random>
+#include <set>
+
+namespace b200 {
+
+struct AlgBase {
+    Registry opts;
+    ErrorRecord *err = nullptr;
+    CudaCtx *cuda = nullptr;
+    bool model_trained = false;
+    virtual ~AlgBase() = default;
+    virtual void refresh() {}
+    virtual da_status get_result(da_result q, da_int *dim, double *out) {
+        (void)q, (void)dim, (void)out;
+        return err->warn(da_status_unknown_query, "The requested result could not be found.");
+    }
+    virtual da_status get_result(da_result q, da_int *dim, float *out) {
+        (void)q, (void)dim, (void)out;
+        return err->warn(da_status_unknown_query, "The requested result could not be found.");
+    }
+    virtual da_status get_result_int(da_result q, da_int *dim, da_int *out) {
+        if (q == da_trained) {
+            if (*dim < 1) {
+                *dim = 1;
+                return err->warn(da_status_invalid_array_dimension,
+                                 "Size of the result array is too small, provide an array of "
+                                 "at least size: 1.");
+            }
+            out[0] = da_int(model_trained);
+            return da_status_success;
+        }
+        return err->warn(da_status_unknown_query, "The requested result could not be found.");
+    }
+    da_order order() { return da_order(opts.key("storage order")); }
+};
+
+// ------------------------------------------------------------------ kNN ----
+// Reference: source/core/nearest_neighbors/nearest_neighbors.{hpp,cpp}
+template <typename T> struct NN : public AlgBase {
+    // option-derived state (nearest_neighbors.cpp:295-352)
+    da_int n_neighbors = 5, algo = 3, metric = 0, weights = 0;
+    T p = 2;
+    bool up_to_date = false;
+    da_int locked_algo = -1, locked_metric = -1, locked_leaf = -1;
+    T locked_p = 0;
+    // data
+    da_int n_samples = 0, n_features = 0;
+    const T *X_host = nullptr;
+    da_int ldx_host = 0;
+    da_order data_order = column_major;
+    bool have_X = false, X_on_device = false;
+    const da_int *y_class = nullptr;
+    const T *y_reg = nullptr;
+    bool have_labels = false, have_targets = false;
+    std::vector<da_int> classes;
+    bool classes_done = false;
+    // device
+    int ld = 0;
+    DevBuf dX, dXn, dQ, dQn, dPartK, dPartI, dOutK, dOutI, dStage;
+    int xn_kind = -1; // which norms dXn holds: 0 squared, 1 eps1-norm
+
+    NN(ErrorRecord *e, CudaCtx *c, bool single);
+    da_status set_params();
+    da_status check_options_update();
+    da_status set_data(da_int n, da_int d, const T *X, da_int ldx);
+    da_status set_labels(da_int n, const da_int *y);
+    da_status set_targets(da_int n, const T *y);
+    da_status kneighbors(da_int nq, da_int d, const T *Xt, da_int ldt, da_int *n_ind, T *n_dist,
+                         da_int k, da_int return_distance);
+    da_status classes_api(da_int *n_classes, da_int *cls);
+    da_status predict_proba(da_int nq, da_int d, const T *Xt, da_int ldt, T *proba,
+                            da_nn_search_mode mode);
+    da_status predict(da_int nq, da_int d, const T *Xt, da_int ldt, da_int *y,
+                      da_nn_search_mode mode);
+    da_status predict_reg(da_int nq, da_int d, const T *Xt, da_int ldt, T *y,
+                          da_nn_search_mode mode);
+    void refresh() override { up_to_date = false; }
+
+    // core: q-major results (n_ind[q*k + r]) on the host
+    da_status kneighbors_compute(da_int nq, da_int d, const T *Xt, da_int ldt, da_order ord,
+                                 da_int k, std::vector<da_int> &ind, std::vector<T> *dist);
+    da_status ensure_device_data();
+    da_status validate_queries(da_int nq, da_int d, const T *Xt, da_int ldt);
+    da_status compute_proba(da_int nq, da_int d, const T *Xt, da_int ldt, std::vector<T> &proba);
+    da_status available_classes();
+};
+
+// --------------------------------------------------------------- k-means ---
+// Reference: source/core/clustering/kmeans/kmeans.{hpp,cpp}, kmeans_lloyd.hpp
+template <typename T> struct KMeans : public AlgBase {
+    da_int n_samples = 0, n_features = 0;
+    const T *A_host = nullptr;
+    da_int lda_host = 0;
+    da_order data_order = column_major;
+    bool initdone = false, centres_supplied = false;
+    std::vector<T> C_supplied; // column-major n_clusters x d
+    // options read at compute
+    da_int n_clusters = 1, n_init = 10, max_iter = 300, seed = 0, init_method = 1;
+    da_int algorithm = 0, empty_mode = 0, afk_samples = 50;
+    double tol = 1e-4;
+    std::mt19937_64 mt_gen;
+    // results
+    std::vector<T> best_centres; // column-major k x d
+    std::vector<da_int> best_labels;
+    bool best_labels_on_host = false;
+    double best_inertia = 0;
+    da_int best_n_iter = 0, best_lp_n_iter = 0;
+    bool warn_maxit = false;
+    // device
+    int ld = 0;
+    DevBuf dX, dXn, dC0, dC1, dCn, dL0, dL1, dCounts, dBlockCounts, dOffsets, dSorted,
+        dChunkSums, dSegStart, dScalars, dFlags, dPartials, dW, dKD, dCand, dStage, dY, dYL,
+        dBestL;
+    T *h_pin = nullptr;
+    void *h_small = nullptr; // pinned: flags + scalars
+
+    KMeans(ErrorRecord *e, CudaCtx *c, bool single);
+    ~KMeans() override;
+    void refresh() override;
+    da_status set_data(da_int n, da_int d, const T *A, da_int lda);
+    da_status set_init_centres(const T *C, da_int ldc);
+    da_status compute();
+    da_status read_options();
+    da_status initial_centres(T *C, da_int ldc);
+    da_status predict(da_int m, da_int d, const T *Y, da_int ldy, da_int *labels);
+    da_status transform(da_int m, da_int d, const T *X, da_int ldx, T *Xt, da_int ldxt);
+    da_status get_result_t(da_result q, da_int *dim, T *out);
+    da_status get_result(da_result q, da_int *dim, double *out) override;
+    da_status get_result(da_result q, da_int *dim, float *out) override;
+    da_status get_result_int(da_result q, da_int *dim, da_int *out) override;
+
+    // internals
+    da_status ensure_device_data();
+    da_status alloc_work();
+    da_status init_centres(T *dC);
+    da_status kmeans_plusplus(T *dC);
+    da_status afk_mcmc(std::vector<T> &Cc);
+    da_status run_lloyd(T *&dCcur, T *&dCprev, int *&dLcur, int *&dLprev, da_int &n_iter,
+                        int &converged, double &inertia, bool &empty_found);
+    da_status lloyd_step(const T *dCprev, T *dCnew, int *dL, const int *dLprev, bool update,
+                         double *h_scal, int *h_flags);
+    da_status split_empty(T *dC, int *dL, bool &split);
+};
+
+} // namespace b200
+
+// The opaque handle of the C ABI (source/include/aoclda_handle.h:98).
+struct _da_handle {
+    da_precision precision = da_unknown;
+    da_handle_type type = da_handle_uninitialized;
+    b200::ErrorRecord err;
+    b200::CudaCtx cuda;
+    std::unique_ptr<b200::AlgBase> alg;
+};

@@ -1,0 +1,161 @@
+// Host-callable launchers of the B200 kernels.  All pointers are DEVICE
+// pointers; every launcher enqueues on `stream` and returns the launch error.
+//
+// Device data layout (chosen for sm_100a, not taken from the reference):
+//   * a sample matrix is row-major, rows x ld with ld = d rounded up to a
+//     multiple of 4 elements (16-byte rows for fp32, 32-byte for fp64), pad
+//     columns are zero;
+//   * labels / indices are int32;
+//   * centroid sums are fp64.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace b200 {
+
+inline int pad4(int d) { return (d + 3) & ~3; }
+
+// Element-wise metric families of the direct (non-GEMM) distance engine.
+// The accumulation order of each family follows the AOCL-DA micro-kernels
+// (source/core/metrics/metrics_kernels.hpp).
+enum AccKind : int {
+    ACC_SQEUC = 0,     // sum (a-b)^2, two accumulators (metrics_kernels.hpp:419-496)
+    ACC_DOT = 1,       // sum a*b, one fma chain (cosine kernel, metrics_kernels.hpp:670-749)
+    ACC_MANHATTAN = 2, // sum |a-b|, one add chain (metrics_kernels.hpp:584-666)
+    ACC_MINKOWSKI = 3  // sum |a-b|^p, one add chain (metrics_kernels.hpp:752-827)
+};
+
+// Post-operation applied to an accumulated pair value.
+enum PostKind : int {
+    POST_NONE = 0,       // squared euclidean / manhattan: value as accumulated
+    POST_SQRT = 1,       // euclidean
+    POST_COSINE = 2,     // 1 - dot / (|x| |y|)
+    POST_GEMM_SQ = 3,    // |x|^2 + |y|^2 - 2 dot (GEMM-form squared euclidean)
+    POST_GEMM_SQRT = 4,  // sqrt of POST_GEMM_SQ (no clamp, as the reference)
+    POST_POW = 5,        // (sum)^(1/p)
+    POST_NEG = 6,        // -dot: inner product ranked largest-first
+    POST_GEMM_SQ_CLAMP = 7 // max(0, GEMM-form squared euclidean) -- kNN selection key
+};
+
+
+// ---------------------------------------------------------------- ingest --
+// Dense column-major (rows x cols, ld = rows) -> padded row-major (rows x ldo).
+template <typename T>
+cudaError_t launch_colmajor_to_rowmajor(const T *src, int rows, int cols, T *dst, int ldo,
+                                        cudaStream_t s);
+// Row-major (rows x ldo) -> dense column-major (rows x cols, ld = ldc).
+template <typename T>
+cudaError_t launch_rowmajor_to_colmajor(const T *src, int rows, int cols, int ldi, T *dst,
+                                        long ldc, cudaStream_t s);
+
+// ------------------------------------------------------------- row norms --
+// out[i] = sum_j x_ij^2 as a sequential fma chain in j (the order of the
+// reference's norm loops, euclidean_gemm_distance.cpp:65-95).
+template <typename T>
+cudaError_t launch_row_sqnorms(const T *X, int ld, int rows, int d, T *out, cudaStream_t s);
+// out[i] = ||x_i||_2 (accumulated in fp64), replaced by 1 when <= eps
+// (cosine_distance.cpp:117-146).
+template <typename T>
+cudaError_t launch_row_norms_eps1(const T *X, int ld, int rows, int d, T *out,
+                                  cudaStream_t s);
+
+// --------------------------------------------------------- pairwise tile --
+struct PairwiseArgs {
+    int acc;       // AccKind
+    int post;      // PostKind
+    int kc;        // KC slice length of the reference's blocking (multiple of 4)
+    double p;      // Minkowski exponent
+    bool x_is_y;   // cosine / gemm: diagonal forced to 0
+    bool out_rowmajor; // D row-major (m x n, ld = n) or column-major (ld = m)
+};
+// D(i,j) = dist(x_i, y_j), i < m (rows of X), j < n (rows of Y).
+template <typename T>
+cudaError_t launch_pairwise(const T *X, int ldx, int m, const T *Y, int ldy, int n, int d,
+                            const T *xn, const T *yn, const PairwiseArgs &a, T *D,
+                            cudaStream_t s);
+
+// ------------------------------------------------------------ kNN fused --
+struct KnnArgs {
+    int acc, post, kc;
+    double p;
+    int k;          // neighbours requested
+    int chunk_rows; // train rows per chunk (multiple of the tile width)
+    int n_chunks;
+};
+// Stage 1: per (query tile, train chunk) running top-k of the selection key,
+// written as sorted (key, index) lists: part_key[(q * n_chunks + c) * k + r].
+template <typename T>
+cudaError_t launch_knn_chunks(const T *Q, int ldq, int nq, const T *X, int ldx, int nx,
+                              int d, const T *qn, const T *xn, const KnnArgs &a,
+                              T *part_key, int *part_idx, int *err_flag, cudaStream_t s);
+// Stage 2: merge the n_chunks lists of every query into the final sorted
+// top-k; out_key receives the value returned to the user (sqrt applied for
+// euclidean, sign restored for inner product).
+template <typename T>
+cudaError_t launch_knn_merge(const T *part_key, const int *part_idx, int nq, int n_chunks,
+                             int k, int out_transform, T *out_key, int *out_idx,
+                             cudaStream_t s);
+// Which tile widths the fused kernel uses; chunk_rows must be a multiple.
+int knn_tile_rows_train(bool fp64);
+int knn_max_k(bool fp64);
+
+// ------------------------------------------------------------- k-means ---
+struct KmeansWork {
+    // per-iteration device scratch owned by the handle
+    int *labels;          // n
+    int *labels_prev;     // n
+    int *counts;          // k
+    int *block_counts;    // n_blocks * k
+    int *offsets;         // k + 1
+    int *sorted_rows;     // n
+    double *chunk_sums;   // n_seg_chunks_max * ld
+    int *seg_chunk_start; // k + 1  (first chunk of each cluster)
+    double *scalars;      // [0]=normc^2 [1]=shift^2 [2]=inertia ...
+    int *flags;           // [0]=labels changed [1]=n_empty
+};
+int kmeans_assign_block_rows();
+int kmeans_max_clusters_fused();
+// Lloyd assignment: label_i = argmin_j (|c_j|^2 - 2 x_i.c_j), ties -> lower j.
+// Also writes per-block label histograms (for the counting sort) and raises
+// flags[0] when a label differs from labels_prev (if labels_prev != null).
+template <typename T>
+cudaError_t launch_kmeans_assign(const T *X, int ldx, int n, int d, const T *C, int ldc,
+                                 int k, const T *cnorm, int *labels, const int *labels_prev,
+                                 int *block_counts, int *flags, cudaStream_t s);
+// Counting sort of rows by label: offsets (exclusive scan of counts) and a
+// stable scatter of row ids (rows of one cluster stay in ascending order).
+cudaError_t launch_kmeans_sort(const int *labels, int n, int k, const int *block_counts,
+                               int *counts, int *offsets, int *seg_chunk_start,
+                               int seg_rows, int *sorted_rows, int *flags, cudaStream_t s);
+// Deterministic centroid update: fp64 sums over fixed row chunks of every
+// cluster, combined in chunk order; C_new = sum / max(count,1) (an empty
+// cluster becomes the zero vector, kmeans_lloyd.hpp:364-377).  Also computes
+// |C_prev|_F^2 and |C_prev - C_new|_F^2 in fp64 into scalars[0], scalars[1].
+template <typename T>
+cudaError_t launch_kmeans_update(const T *X, int ldx, int n, int d, int k,
+                                 const int *sorted_rows, const int *offsets,
+                                 const int *seg_chunk_start, int seg_rows, double *chunk_sums,
+                                 const int *counts, const T *C_prev, T *C_new, int ldc,
+                                 double *scalars, int *flags, cudaStream_t s);
+// Squared row norms of the centres (sequential fma chain over features).
+template <typename T>
+cudaError_t launch_centre_norms(const T *C, int ldc, int k, int d, T *out, cudaStream_t s);
+// Inertia sum_i |x_i - c_{l_i}|^2 accumulated in fp64 (fixed block order).
+template <typename T>
+cudaError_t launch_kmeans_inertia(const T *X, int ldx, int n, int d, const T *C, int ldc,
+                                  const int *labels, double *block_partials, double *out,
+                                  cudaStream_t s);
+// k-means++ distances of every row to `t` candidate rows:
+// D[c*n + i] = (|x_i|^2 + |x_cand|^2) - 2 x_i.x_cand (GEMM form, no clamp).
+template <typename T>
+cudaError_t launch_kpp_dist(const T *X, int ldx, int n, int d, const T *xnorm,
+                            const int *cand, int t, T *D, cudaStream_t s);
+// For each candidate c: cost_c = sum_i max(0, min(w_i, D_ci)) (fp64, fixed order).
+template <typename T>
+cudaError_t launch_kpp_cost(const T *w, const T *D, int n, int t, double *block_partials,
+                            double *cost, cudaStream_t s);
+// w_i = max(0, min(w_i, D_ci)) for the chosen candidate (in place).
+template <typename T>
+cudaError_t launch_kpp_update(T *w, const T *Dc, int n, int chosen, cudaStream_t s);
+
+} // namespace b200

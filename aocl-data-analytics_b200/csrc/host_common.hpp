@@ -1,0 +1,401 @@
+// Host-side infrastructure of the B200 library: error recording, the option
+// registry, device buffers and the per-handle CUDA context.
+#pragma once
+#include "../../include/aoclda_b200.h"
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace b200 {
+
+// ------------------------------------------------------------------ errors --
+// Mirrors the record/warn behaviour of the reference error object
+// (source/core/utilities/da_error.hpp:163-260): the last status, message and
+// severity of a call are kept in the handle and cleared at the start of the
+// next public call.
+struct ErrorRecord {
+    da_status status = da_status_success;
+    da_severity severity = DA_NOTSET;
+    std::string message;
+    void clear() {
+        status = da_status_success;
+        severity = DA_NOTSET;
+        message.clear();
+    }
+    da_status error(da_status s, const std::string &m) {
+        status = s;
+        severity = DA_ERROR;
+        message = m;
+        return s;
+    }
+    da_status warn(da_status s, const std::string &m) {
+        status = s;
+        severity = DA_WARNING;
+        message = m;
+        return s;
+    }
+};
+
+// ----------------------------------------------------------------- options --
+// A typed registry with the same option names, bounds, defaults and status
+// codes as the reference (source/core/utilities/options.hpp:192-940).
+enum class LB { m_inf, greaterthan, greaterequal };
+enum class UB { p_inf, lessthan, lessequal };
+enum class OptKind { Int, Real, String };
+
+struct Option {
+    OptKind kind;
+    std::string name;
+    da_int ival = 0, ilo = 0, ihi = 0;
+    double rval = 0, rlo = 0, rhi = 0;
+    LB lb = LB::m_inf;
+    UB ub = UB::p_inf;
+    std::string sval;
+    std::vector<std::pair<std::string, da_int>> labels;
+};
+
+// trim, squeeze whitespace, lower case (options.hpp:192-202)
+inline std::string prep_str(const std::string &in) {
+    std::string out;
+    bool sp = false;
+    for (char c : in) {
+        if (std::isspace((unsigned char)c)) {
+            sp = true;
+            continue;
+        }
+        if (sp && !out.empty()) out.push_back(' ');
+        sp = false;
+        out.push_back((char)std::tolower((unsigned char)c));
+    }
+    return out;
+}
+
+class Registry {
+  public:
+    std::string errmsg;
+    bool single = false; // real options follow float semantics
+
+    void add_int(const std::string &n, da_int lo, LB lb, da_int hi, UB ub, da_int def) {
+        Option o;
+        o.kind = OptKind::Int;
+        o.name = n;
+        o.ilo = lo;
+        o.ihi = hi;
+        o.lb = lb;
+        o.ub = ub;
+        o.ival = def;
+        opts_[n] = o;
+    }
+    void add_real(const std::string &n, double lo, LB lb, double hi, UB ub, double def) {
+        Option o;
+        o.kind = OptKind::Real;
+        o.name = n;
+        o.rlo = lo;
+        o.rhi = hi;
+        o.lb = lb;
+        o.ub = ub;
+        o.rval = round_t(def);
+        opts_[n] = o;
+    }
+    void add_string(const std::string &n, std::vector<std::pair<std::string, da_int>> labels,
+                    const std::string &def) {
+        Option o;
+        o.kind = OptKind::String;
+        o.name = n;
+        o.labels = std::move(labels);
+        o.sval = def;
+        opts_[n] = o;
+    }
+    // Re-register an integer option's bounds (kmeans_options.hpp:153-170).
+    void rebound_int(const std::string &n, da_int lo, LB lb, da_int hi, UB ub) {
+        auto &o = opts_[n];
+        o.ilo = lo;
+        o.lb = lb;
+        o.ihi = hi;
+        o.ub = ub;
+    }
+
+    da_status set_int(const std::string &name, da_int v) {
+        Option *o = find(name);
+        if (!o) return da_status_option_not_found;
+        if (o->kind != OptKind::Int) return wrong_type(name);
+        if (!in_bounds((double)v, (double)o->ilo, o->lb, (double)o->ihi, o->ub)) {
+            errmsg = "Option '" + o->name + "': value out-of-bounds";
+            return da_status_option_invalid_value;
+        }
+        o->ival = v;
+        return da_status_success;
+    }
+    da_status set_real(const std::string &name, double v) {
+        Option *o = find(name);
+        if (!o) return da_status_option_not_found;
+        if (o->kind != OptKind::Real) return wrong_type(name);
+        v = round_t(v);
+        if (std::isnan(v)) {
+            errmsg = "Option '" + o->name + "': Invalid value.";
+            return da_status_option_invalid_value;
+        }
+        if (!in_bounds(v, o->rlo, o->lb, o->rhi, o->ub)) {
+            errmsg = "Option '" + o->name + "': value out-of-bounds";
+            return da_status_option_invalid_value;
+        }
+        o->rval = v;
+        return da_status_success;
+    }
+    da_status set_string(const std::string &name, const std::string &v) {
+        Option *o = find(name);
+        if (!o) return da_status_option_not_found;
+        if (o->kind != OptKind::String) return wrong_type(name);
+        for (auto &l : o->labels)
+            if (l.first == v) {
+                o->sval = v;
+                return da_status_success;
+            }
+        std::string t = prep_str(v);
+        for (auto &l : o->labels)
+            if (l.first == t) {
+                o->sval = t;
+                return da_status_success;
+            }
+        errmsg = "Unrecognized value '" + t + "' for option '" + o->name + "'.";
+        return da_status_option_invalid_value;
+    }
+    da_status get_int(const std::string &name, da_int &v) {
+        Option *o = find(name);
+        if (!o) return da_status_option_not_found;
+        if (o->kind != OptKind::Int) return wrong_type(name);
+        v = o->ival;
+        return da_status_success;
+    }
+    da_status get_real(const std::string &name, double &v) {
+        Option *o = find(name);
+        if (!o) return da_status_option_not_found;
+        if (o->kind != OptKind::Real) return wrong_type(name);
+        v = o->rval;
+        return da_status_success;
+    }
+    da_status get_string(const std::string &name, std::string &v, da_int *key = nullptr) {
+        Option *o = find(name);
+        if (!o) return da_status_option_not_found;
+        if (o->kind != OptKind::String) return wrong_type(name);
+        v = o->sval;
+        if (key)
+            for (auto &l : o->labels)
+                if (l.first == v) *key = l.second;
+        return da_status_success;
+    }
+    // convenience getters for internal use (the option must exist)
+    da_int i(const std::string &n) { return opts_.at(n).ival; }
+    double r(const std::string &n) { return opts_.at(n).rval; }
+    da_int key(const std::string &n) {
+        auto &o = opts_.at(n);
+        for (auto &l : o.labels)
+            if (l.first == o.sval) return l.second;
+        return -1;
+    }
+    void print() const {
+        for (auto &kv : opts_) {
+            const Option &o = kv.second;
+            if (o.kind == OptKind::Int)
+                std::printf("%s = %lld\n", o.name.c_str(), (long long)o.ival);
+            else if (o.kind == OptKind::Real)
+                std::printf("%s = %.17g\n", o.name.c_str(), o.rval);
+            else
+                std::printf("%s = %s\n", o.name.c_str(), o.sval.c_str());
+        }
+    }
+
+  private:
+    std::map<std::string, Option> opts_;
+    Option *find(const std::string &name) {
+        auto it = opts_.find(name);
+        if (it == opts_.end()) it = opts_.find(prep_str(name));
+        if (it == opts_.end()) {
+            errmsg = "Option '" + prep_str(name) + "' not found in the option registry";
+            return nullptr;
+        }
+        return &it->second;
+    }
+    da_status wrong_type(const std::string &name) {
+        errmsg = "Option setter for '" + name + "' was called with the wrong type";
+        return da_status_option_wrong_type;
+    }
+    double round_t(double v) const { return single ? (double)(float)v : v; }
+    static bool in_bounds(double v, double lo, LB lb, double hi, UB ub) {
+        if (lb == LB::greaterthan && !(v > lo)) return false;
+        if (lb == LB::greaterequal && !(v >= lo)) return false;
+        if (ub == UB::lessthan && !(v < hi)) return false;
+        if (ub == UB::lessequal && !(v <= hi)) return false;
+        return true;
+    }
+};
+
+// Options common to every handle (basic_handle_options.hpp:40-53).
+inline void register_common_options(Registry &r) {
+    r.add_string("storage order",
+                 {{"row-major", row_major},
+                  {"column-major", column_major},
+                  {"fortran", column_major},
+                  {"f", column_major},
+                  {"c", row_major}},
+                 "column-major");
+    r.add_string("check data", {{"yes", 1}, {"no", 0}}, "no");
+}
+
+// ---------------------------------------------------------- device buffers --
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    // grow-only allocation; returns false on failure
+    bool ensure(size_t b) {
+        if (b <= bytes && p) return true;
+        release();
+        if (b == 0) b = 16;
+        if (cudaMalloc(&p, b) != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            return false;
+        }
+        bytes = b;
+        return true;
+    }
+    template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+// Per-handle CUDA context: device, stream, kernel timing.
+struct CudaCtx {
+    int device = -1;
+    cudaStream_t stream = nullptr;     // stream all work is enqueued on
+    cudaStream_t own_stream = nullptr; // the handle's own stream
+    bool ready = false;
+    bool timing = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::map<std::string, std::pair<double, long>> ktime; // name -> (ms total, launches)
+
+    // Lazily bind to the current CUDA device.  Host-only calls (options,
+    // argument checks) never need a device; the first call that touches data
+    // does.  Fails loudly when no device is present: there is no CPU path.
+    da_status init(ErrorRecord &err) {
+        if (ready) return da_status_success;
+        int n = 0;
+        cudaError_t e = cudaGetDeviceCount(&n);
+        if (e != cudaSuccess || n == 0) {
+            cudaGetLastError();
+            return err.error(da_status_arch_not_supported,
+                             "No CUDA device is available: this library computes on "
+                             "NVIDIA B200 (sm_100a) GPUs only.");
+        }
+        cudaGetDevice(&device);
+        if (cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            return err.error(da_status_internal_error, "cudaStreamCreate failed.");
+        }
+        if (!stream) stream = own_stream;
+        cudaEventCreate(&ev0);
+        cudaEventCreate(&ev1);
+        ready = true;
+        return da_status_success;
+    }
+    ~CudaCtx() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+    // Time one launch with events on the handle's stream when timing is on.
+    template <typename F> cudaError_t timed(const char *name, F &&launch) {
+        if (!timing) return launch();
+        cudaEventRecord(ev0, stream);
+        cudaError_t e = launch();
+        cudaEventRecord(ev1, stream);
+        cudaEventSynchronize(ev1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        auto &t = ktime[name];
+        t.first += ms;
+        t.second += 1;
+        return e;
+    }
+};
+
+inline da_status cuda_status(ErrorRecord &err, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return da_status_success;
+    cudaGetLastError();
+    da_status s = (e == cudaErrorMemoryAllocation) ? da_status_memory_error
+                                                   : da_status_internal_error;
+    return err.error(s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define B200_TRY(expr, what)                                                                   \
+    do {                                                                                       \
+        cudaError_t _e = (expr);                                                               \
+        if (_e != cudaSuccess) return cuda_status(*this->err, _e, what);                       \
+    } while (0)
+
+// Validation of a 2-D user array (basic_handle.cpp:110-200 semantics).
+template <typename T>
+inline da_status check_2d(ErrorRecord &err, da_order order, da_int n_rows, da_int n_cols,
+                          const T *data, da_int ld, const char *rn, const char *cn,
+                          const char *dn, const char *ldn, da_int rmin = 1, da_int cmin = 1,
+                          bool check_nan = false) {
+    if (n_rows < rmin)
+        return err.error(da_status_invalid_array_dimension,
+                         std::string("The function was called with ") + rn + " = " +
+                             std::to_string(n_rows) + ". Constraint: " + rn +
+                             " >= " + std::to_string(rmin) + ".");
+    if (n_cols < cmin)
+        return err.error(da_status_invalid_array_dimension,
+                         std::string("The function was called with ") + cn + " = " +
+                             std::to_string(n_cols) + ". Constraint: " + cn +
+                             " >= " + std::to_string(cmin) + ".");
+    if (data == nullptr)
+        return err.error(da_status_invalid_pointer, std::string("The array ") + dn + " is null.");
+    if (order == column_major && ld < n_rows)
+        return err.error(da_status_invalid_leading_dimension,
+                         std::string("The function was called with ") + rn + " = " +
+                             std::to_string(n_rows) + " and " + ldn + " = " +
+                             std::to_string(ld) + ". Constraint: " + ldn + " >= " + rn + ".");
+    if (order == row_major && ld < n_cols)
+        return err.error(da_status_invalid_leading_dimension,
+                         std::string("The function was called with ") + cn + " = " +
+                             std::to_string(n_cols) + " and " + ldn + " = " +
+                             std::to_string(ld) + ". Constraint: " + ldn + " >= " + cn + ".");
+    if (check_nan) {
+        for (da_int j = 0; j < n_cols; ++j)
+            for (da_int i = 0; i < n_rows; ++i) {
+                T v = (order == column_major) ? data[i + (size_t)j * ld] : data[(size_t)i * ld + j];
+                if (std::isnan(v))
+                    return err.error(da_status_invalid_input,
+                                     std::string("The array ") + dn +
+                                         " contains at least one NaN.");
+            }
+    }
+    return da_status_success;
+}
+
+// Copy a user matrix (order, ld) into a device row-major matrix with padded
+// width ldo (zero pad columns).  `stage` is scratch for column-major input.
+template <typename T>
+cudaError_t upload_matrix(da_order order, da_int rows, da_int cols, const T *host, da_int ld,
+                          T *dst, int ldo, DevBuf &stage, cudaStream_t s);
+template <typename T>
+cudaError_t download_matrix(da_order order, da_int rows, da_int cols, const T *dev_rowmajor,
+                            int ldi, T *host, da_int ld, DevBuf &stage, cudaStream_t s);
+
+} // namespace b200

@@ -1,0 +1,825 @@
+// k-means (Lloyd) handle, host side.  Control flow, option semantics and
+// status codes follow source/core/clustering/kmeans/kmeans.cpp; every pass
+// over the data runs on the GPU (kmeans_simt.cu), the random draws of the
+// initialisation use the same std:: generators as the reference on the host.
+#include "alg.hpp"
+
+namespace b200 {
+
+enum { INIT_RANDOM = 0, INIT_KPP = 1, INIT_SUPPLIED = 2, INIT_RPART = 3, INIT_AFK = 4 };
+enum { ALG_LLOYD = 0, ALG_ELKAN = 1, ALG_HW = 2, ALG_MACQ = 3 };
+enum { EC_IGNORE = 0, EC_ERROR = 1, EC_SPLIT = 2 };
+static constexpr int SEG_ROWS = 64; // rows per fp64 partial-sum chunk
+
+template <typename T>
+KMeans<T>::KMeans(ErrorRecord *e, CudaCtx *c, bool single) {
+    err = e;
+    cuda = c;
+    opts.single = single;
+    register_common_options(opts);
+    // kmeans_options.hpp:46-137
+    const da_int imax = std::numeric_limits<da_int>::max();
+    opts.add_int("n_clusters", 1, LB::greaterequal, imax, UB::p_inf, 1);
+    opts.add_int("n_init", 1, LB::greaterequal, imax, UB::p_inf, 10);
+    opts.add_int("max_iter", 1, LB::greaterequal, imax, UB::p_inf, 300);
+    opts.add_int("low precision max_iter", 1, LB::greaterequal, imax, UB::p_inf, 200);
+    opts.add_int("seed", -1, LB::greaterequal, imax, UB::p_inf, 0);
+    opts.add_int("afk-mc2 samples", 1, LB::greaterequal, imax, UB::p_inf, 50);
+    opts.add_string("initialization method",
+                    {{"random", INIT_RANDOM},
+                     {"k-means++", INIT_KPP},
+                     {"supplied", INIT_SUPPLIED},
+                     {"random partitions", INIT_RPART},
+                     {"afk-mc2", INIT_AFK}},
+                    "k-means++");
+    opts.add_string("algorithm",
+                    {{"lloyd", ALG_LLOYD}, {"elkan", ALG_ELKAN}, {"hartigan-wong", ALG_HW},
+                     {"macqueen", ALG_MACQ}},
+                    "lloyd");
+    opts.add_string("mixed precision", {{"yes", 1}, {"no", 0}}, "no");
+    opts.add_string("empty clusters", {{"ignore", EC_IGNORE}, {"error", EC_ERROR}, {"split", EC_SPLIT}},
+                    "ignore");
+    opts.add_string("distance", {{"euclidean", 0}, {"cosine", 1}}, "euclidean");
+    opts.add_string("normalize data", {{"yes", 1}, {"no", 0}}, "yes");
+    opts.add_real("convergence tolerance", 0.0, LB::greaterequal, 0.0, UB::p_inf, 1.0e-4);
+    opts.add_real("low precision convergence tolerance", 0.0, LB::greaterequal, 0.0, UB::p_inf,
+                  1.0e-2);
+}
+
+template <typename T> KMeans<T>::~KMeans() {
+    if (h_small) cudaFreeHost(h_small);
+}
+
+template <typename T> void KMeans<T>::refresh() {
+    best_n_iter = 0;
+    best_inertia = 0;
+    best_lp_n_iter = 0;
+    warn_maxit = false;
+}
+
+// kmeans.cpp:249-293
+template <typename T>
+da_status KMeans<T>::set_data(da_int n, da_int d, const T *A, da_int lda) {
+    refresh();
+    const da_order ord = order();
+    da_status s = check_2d(*err, ord, n, d, A, lda, "n_samples", "n_features", "A", "lda", 1, 1,
+                           opts.key("check data") == 1);
+    if (s != da_status_success) return s;
+    A_host = A;
+    lda_host = lda;
+    data_order = ord;
+    n_samples = n;
+    n_features = d;
+    initdone = true;
+    model_trained = false;
+    dX.release();
+    // n_clusters is re-bounded by the number of samples (kmeans_options.hpp:153-170)
+    da_int kc = opts.i("n_clusters");
+    opts.rebound_int("n_clusters", 1, LB::greaterequal, n, UB::lessequal);
+    opts.set_int("n_clusters", std::min(kc, n));
+    if (cuda->init(*err) == da_status_success) {
+        s = ensure_device_data();
+        if (s != da_status_success) return s;
+    } else {
+        err->clear();
+    }
+    if (kc > n)
+        return err->warn(da_status_incompatible_options,
+                         "The requested number of clusters has been decreased from " +
+                             std::to_string(kc) + " to " + std::to_string(n) +
+                             " due to the size of the data array.");
+    return da_status_success;
+}
+
+template <typename T> da_status KMeans<T>::ensure_device_data() {
+    da_status s = cuda->init(*err);
+    if (s != da_status_success) return s;
+    if (dX.p) return da_status_success;
+    ld = pad4(n_features);
+    if (!dX.ensure((size_t)n_samples * ld * sizeof(T)) || !dXn.ensure((size_t)n_samples * sizeof(T)))
+        return err->error(da_status_memory_error, "Device memory allocation failed.");
+    B200_TRY(upload_matrix<T>(data_order, n_samples, n_features, A_host, lda_host, dX.as<T>(), ld,
+                              dStage, cuda->stream),
+             "upload of A");
+    B200_TRY(launch_row_sqnorms<T>(dX.as<T>(), ld, n_samples, n_features, dXn.as<T>(), cuda->stream),
+             "row norms");
+    return da_status_success;
+}
+
+// kmeans.cpp:295-348
+template <typename T> da_status KMeans<T>::set_init_centres(const T *C, da_int ldc) {
+    if (!initdone)
+        return err->error(da_status_no_data,
+                          "No data has been passed to the handle. Please call "
+                          "da_kmeans_set_data_s or da_kmeans_set_data_d.");
+    if (order() != data_order)
+        return err->error(da_status_incompatible_options,
+                          "The storage order option was changed after data was set.");
+    const da_int k = opts.i("n_clusters");
+    da_status s = check_2d(*err, data_order, k, n_features, C, ldc, "n_clusters", "n_features",
+                           "C", "ldc", 1, 1, opts.key("check data") == 1);
+    if (s != da_status_success) return s;
+    C_supplied.assign((size_t)k * n_features, T(0));
+    for (da_int j = 0; j < n_features; ++j)
+        for (da_int i = 0; i < k; ++i)
+            C_supplied[i + (size_t)j * k] =
+                data_order == column_major ? C[i + (size_t)j * ldc] : C[(size_t)i * ldc + j];
+    centres_supplied = true;
+    return da_status_success;
+}
+
+template <typename T> da_status KMeans<T>::alloc_work() {
+    const size_t n = n_samples, k = n_clusters;
+    const size_t nblk = (n + kmeans_assign_block_rows() - 1) / kmeans_assign_block_rows();
+    const size_t nchunks = n / SEG_ROWS + k + 1;
+    const size_t nfin = (k * n_features + 255) / 256;
+    bool ok = dC0.ensure(k * ld * sizeof(T)) && dC1.ensure(k * ld * sizeof(T)) &&
+              dCn.ensure(k * sizeof(T)) && dL0.ensure(n * sizeof(int)) &&
+              dL1.ensure(n * sizeof(int)) && dCounts.ensure(k * sizeof(int)) &&
+              dBlockCounts.ensure(nblk * k * sizeof(int)) &&
+              dOffsets.ensure((k + 1) * sizeof(int)) && dSorted.ensure(n * sizeof(int)) &&
+              dChunkSums.ensure(nchunks * ld * sizeof(double)) &&
+              dSegStart.ensure((k + 1) * sizeof(int)) &&
+              dScalars.ensure((8 + 2 * nfin) * sizeof(double)) && dFlags.ensure(8 * sizeof(int)) &&
+              dPartials.ensure(148 * 8 * 16 * sizeof(double));
+    if (!ok) return err->error(da_status_memory_error, "Device memory allocation failed.");
+    if (!h_small && cudaMallocHost(&h_small, 256) != cudaSuccess) {
+        cudaGetLastError();
+        return err->error(da_status_memory_error, "Pinned host allocation failed.");
+    }
+    if (cudaMemsetAsync(dC0.p, 0, k * ld * sizeof(T), cuda->stream) != cudaSuccess ||
+        cudaMemsetAsync(dC1.p, 0, k * ld * sizeof(T), cuda->stream) != cudaSuccess ||
+        cudaMemsetAsync(dL0.p, 0, n * sizeof(int), cuda->stream) != cudaSuccess ||
+        cudaMemsetAsync(dL1.p, 0, n * sizeof(int), cuda->stream) != cudaSuccess)
+        return cuda_status(*err, cudaGetLastError(), "memset");
+    return da_status_success;
+}
+
+// Column-major host centres (k x d) -> device row-major centres.
+template <typename T>
+static cudaError_t upload_centres(const std::vector<T> &Cc, int k, int d, int ld, T *dC,
+                                  cudaStream_t s) {
+    std::vector<T> rm((size_t)k * ld, T(0));
+    for (int i = 0; i < k; ++i)
+        for (int j = 0; j < d; ++j) rm[(size_t)i * ld + j] = Cc[i + (size_t)j * k];
+    cudaError_t e = cudaMemcpyAsync(dC, rm.data(), rm.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(s);
+}
+template <typename T>
+static cudaError_t download_centres(const T *dC, int k, int d, int ld, std::vector<T> &Cc,
+                                    cudaStream_t s) {
+    std::vector<T> rm((size_t)k * ld);
+    cudaError_t e = cudaMemcpyAsync(rm.data(), dC, rm.size() * sizeof(T), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(s);
+    Cc.assign((size_t)k * d, T(0));
+    for (int i = 0; i < k; ++i)
+        for (int j = 0; j < d; ++j) Cc[i + (size_t)j * k] = rm[(size_t)i * ld + j];
+    return e;
+}
+
+// Host element of the user's data array (A is kept alive by the caller, as
+// the reference's pointer-storing set_data requires).
+template <typename T> static inline T host_at(const KMeans<T> &km, da_int i, da_int j) {
+    return km.data_order == column_major ? km.A_host[i + (size_t)j * km.lda_host]
+                                         : km.A_host[(size_t)i * km.lda_host + j];
+}
+
+// kmeans.cpp:1524-1664 (distances on the device, draws on the host).
+template <typename T> da_status KMeans<T>::kmeans_plusplus(T *dC) {
+    cudaStream_t st = cuda->stream;
+    const da_int n = n_samples, k = n_clusters, d = n_features;
+    const da_int n_trials = 2 + (da_int)std::log(k);
+    if (!dW.ensure((size_t)n * sizeof(T)) || !dKD.ensure((size_t)n * (n_trials + 1) * sizeof(T)) ||
+        !dCand.ensure((size_t)(n_trials + 1) * sizeof(int)))
+        return err->error(da_status_memory_error, "Device memory allocation failed.");
+    std::vector<int> chosen(k, 0);
+    std::uniform_int_distribution<> dis_int(0, n - 1);
+    const int first = dis_int(mt_gen);
+    chosen[0] = first;
+    // works3: distances to the first centre, clamped
+    B200_TRY(cudaMemcpyAsync(dCand.p, &first, sizeof(int), cudaMemcpyHostToDevice, st), "copy");
+    B200_TRY(launch_kpp_dist<T>(dX.as<T>(), ld, n, d, dXn.as<T>(), dCand.as<int>(), 1, dW.as<T>(), st),
+             "k-means++ distances");
+    std::vector<T> w(n);
+    B200_TRY(cudaMemcpyAsync(w.data(), dW.p, n * sizeof(T), cudaMemcpyDeviceToHost, st), "copy");
+    B200_TRY(cudaStreamSynchronize(st), "k-means++");
+    w[first] = T(0);
+    bool coincident = true;
+    for (da_int i = 0; i < n; ++i) {
+        if (!std::isfinite(w[i]) || w[i] < T(0)) w[i] = T(0);
+        if (w[i] > T(0)) coincident = false;
+    }
+    if (coincident) {
+        for (da_int i = 0; i < k; ++i) chosen[i] = i;
+    } else {
+        B200_TRY(cudaMemcpyAsync(dW.p, w.data(), n * sizeof(T), cudaMemcpyHostToDevice, st), "copy");
+        std::vector<int> cand(n_trials);
+        std::vector<double> cost(n_trials);
+        for (da_int c = 1; c < k; ++c) {
+            std::discrete_distribution<> weighted_dis(w.begin(), w.end());
+            for (da_int t = 0; t < n_trials; ++t) cand[t] = weighted_dis(mt_gen);
+            B200_TRY(cudaMemcpyAsync(dCand.p, cand.data(), n_trials * sizeof(int),
+                                     cudaMemcpyHostToDevice, st), "copy");
+            B200_TRY(launch_kpp_dist<T>(dX.as<T>(), ld, n, d, dXn.as<T>(), dCand.as<int>(),
+                                        n_trials, dKD.as<T>(), st), "k-means++ distances");
+            B200_TRY(launch_kpp_cost<T>(dW.as<T>(), dKD.as<T>(), n, n_trials, dPartials.as<double>(),
+                                        dScalars.as<double>(), st), "k-means++ cost");
+            B200_TRY(cudaMemcpyAsync(cost.data(), dScalars.p, n_trials * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st), "copy");
+            B200_TRY(cudaStreamSynchronize(st), "k-means++");
+            int best = 0, best_t = -1;
+            double best_cost = std::numeric_limits<double>::infinity();
+            for (da_int t = 0; t < n_trials; ++t) {
+                bool repeat = false;
+                for (da_int u = 0; u < t; ++u)
+                    if (cand[u] == cand[t]) repeat = true;
+                if (repeat) continue;
+                if (std::isfinite(cost[t]) && cost[t] < best_cost) {
+                    best_cost = cost[t];
+                    best = cand[t];
+                    best_t = t;
+                }
+            }
+            if (best_t < 0) best_t = 0, best = cand[0];
+            chosen[c] = best;
+            B200_TRY(launch_kpp_update<T>(dW.as<T>(), dKD.as<T>() + (size_t)best_t * n, n, best, st),
+                     "k-means++ update");
+            B200_TRY(cudaMemcpyAsync(w.data(), dW.p, n * sizeof(T), cudaMemcpyDeviceToHost, st), "copy");
+            B200_TRY(cudaStreamSynchronize(st), "k-means++");
+        }
+    }
+    std::vector<T> Cc((size_t)k * d);
+    for (da_int c = 0; c < k; ++c)
+        for (da_int j = 0; j < d; ++j) Cc[c + (size_t)j * k] = host_at(*this, chosen[c], j);
+    B200_TRY(upload_centres<T>(Cc, k, d, ld, dC, st), "centres");
+    return da_status_success;
+}
+
+// kmeans.cpp:1667-1808 (AFK-MC^2), evaluated on the host from the caller's data.
+template <typename T> da_status KMeans<T>::afk_mcmc(std::vector<T> &Cc) {
+    const da_int n = n_samples, k = n_clusters, d = n_features;
+    std::vector<T> xn(n, T(0));
+    for (da_int i = 0; i < n; ++i)
+        for (da_int j = 0; j < d; ++j) xn[i] += host_at(*this, i, j) * host_at(*this, i, j);
+    std::uniform_int_distribution<> dis_int(0, n - 1);
+    const da_int c1 = dis_int(mt_gen);
+    Cc.assign((size_t)k * d, T(0));
+    for (da_int j = 0; j < d; ++j) Cc[(size_t)j * k] = host_at(*this, c1, j);
+    // d(x, c1)^2 in GEMM form
+    std::vector<T> w3(n), q(n);
+    T dot_c = T(0);
+    for (da_int j = 0; j < d; ++j) dot_c += host_at(*this, c1, j) * host_at(*this, c1, j);
+    T sum = T(0);
+    for (da_int i = 0; i < n; ++i) {
+        T s = T(0);
+        for (da_int j = 0; j < d; ++j) s += host_at(*this, i, j) * host_at(*this, c1, j);
+        T v = T(-2) * s + (xn[i] + dot_c);
+        w3[i] = std::max(T(0), v);
+        sum += w3[i];
+    }
+    const T inv2n = T(1) / T(2 * n);
+    for (da_int i = 0; i < n; ++i)
+        q[i] = (std::isfinite(sum) && sum > T(0)) ? T(0.5) * w3[i] / sum + inv2n : T(1) / T(n);
+    auto nearest = [&](da_int idx, da_int nc) {
+        T best = std::numeric_limits<T>::infinity();
+        for (da_int c = 0; c < nc; ++c) {
+            T dist = T(0);
+            for (da_int j = 0; j < d; ++j) {
+                T t = host_at(*this, idx, j) - Cc[c + (size_t)j * k];
+                dist += t * t;
+            }
+            if (dist < best) best = dist;
+        }
+        return best;
+    };
+    std::discrete_distribution<> q_dist(q.begin(), q.end());
+    std::uniform_real_distribution<T> unif(T(0), T(1));
+    for (da_int i = 1; i < k; ++i) {
+        da_int x = q_dist(mt_gen);
+        T dx = nearest(x, i);
+        for (da_int step = 0; step < afk_samples; ++step) {
+            da_int y = q_dist(mt_gen);
+            T dy = nearest(y, i);
+            T dxqy = dx * q[y];
+            if (dxqy == T(0) || (dy * q[x]) / dxqy > unif(mt_gen)) {
+                x = y;
+                dx = dy;
+            }
+        }
+        for (da_int j = 0; j < d; ++j) Cc[i + (size_t)j * k] = host_at(*this, x, j);
+    }
+    return da_status_success;
+}
+
+// kmeans.cpp:1400-1486
+template <typename T> da_status KMeans<T>::init_centres(T *dC) {
+    const da_int n = n_samples, k = n_clusters, d = n_features;
+    std::vector<T> Cc;
+    switch (init_method) {
+    case INIT_RANDOM: {
+        // selection sampling (da_std.hpp:102-118)
+        std::vector<da_int> pick;
+        da_int need = std::min(k, n), pop = n;
+        for (da_int i = 0; need > 0; ++i, --pop) {
+            std::uniform_int_distribution<da_int> dd(0, pop - 1);
+            if (dd(mt_gen) < need) {
+                pick.push_back(i);
+                --need;
+            }
+        }
+        Cc.assign((size_t)k * d, T(0));
+        for (da_int c = 0; c < k; ++c)
+            for (da_int j = 0; j < d; ++j) Cc[c + (size_t)j * k] = host_at(*this, pick[c], j);
+        break;
+    }
+    case INIT_RPART: {
+        std::uniform_int_distribution<> dis(0, k - 1);
+        std::vector<int> lab(n);
+        for (da_int i = 0; i < n; ++i) lab[i] = dis(mt_gen);
+        // means of the random partition, computed with the device update kernels
+        B200_TRY(cudaMemcpyAsync(dL0.p, lab.data(), n * sizeof(int), cudaMemcpyHostToDevice,
+                                 cuda->stream), "copy");
+        B200_TRY(launch_kmeans_sort(dL0.as<int>(), n, k, dBlockCounts.as<int>(), dCounts.as<int>(),
+                                    dOffsets.as<int>(), dSegStart.as<int>(), SEG_ROWS,
+                                    dSorted.as<int>(), dFlags.as<int>(), cuda->stream), "sort");
+        T *other = (dC == dC0.as<T>()) ? dC1.as<T>() : dC0.as<T>();
+        B200_TRY(launch_kmeans_update<T>(dX.as<T>(), ld, n, d, k, dSorted.as<int>(),
+                                         dOffsets.as<int>(), dSegStart.as<int>(), SEG_ROWS,
+                                         dChunkSums.as<double>(), dCounts.as<int>(), other, dC, ld,
+                                         dScalars.as<double>(), dFlags.as<int>(), cuda->stream),
+                 "update");
+        B200_TRY(cudaStreamSynchronize(cuda->stream), "init");
+        return da_status_success;
+    }
+    case INIT_KPP: return kmeans_plusplus(dC);
+    case INIT_AFK: {
+        da_status s = afk_mcmc(Cc);
+        if (s != da_status_success) return s;
+        break;
+    }
+    default: Cc = C_supplied; break;
+    }
+    B200_TRY(upload_centres<T>(Cc, k, d, ld, dC, cuda->stream), "centres");
+    return da_status_success;
+}
+
+// One Lloyd pass (kmeans_lloyd.hpp:106-271): assignment against dCprev and,
+// if `update`, the new centres in dCnew plus the shift norms.
+template <typename T>
+da_status KMeans<T>::lloyd_step(const T *dCprev, T *dCnew, int *dL, const int *dLprev, bool update,
+                                double *h_scal, int *h_flags) {
+    cudaStream_t st = cuda->stream;
+    const int n = n_samples, k = n_clusters, d = n_features;
+    B200_TRY(launch_centre_norms<T>(dCprev, ld, k, d, dCn.as<T>(), st), "centre norms");
+    B200_TRY(cudaMemsetAsync(dFlags.p, 0, 8 * sizeof(int), st), "memset");
+    B200_TRY(cuda->timed("kmeans_assign", [&] {
+        return launch_kmeans_assign<T>(dX.as<T>(), ld, n, d, dCprev, ld, k, dCn.as<T>(), dL,
+                                       dLprev, nullptr, dFlags.as<int>(), st);
+    }), "assign");
+    if (update) {
+        B200_TRY(cuda->timed("kmeans_sort", [&] {
+            return launch_kmeans_sort(dL, n, k, dBlockCounts.as<int>(), dCounts.as<int>(),
+                                      dOffsets.as<int>(), dSegStart.as<int>(), SEG_ROWS,
+                                      dSorted.as<int>(), dFlags.as<int>(), st);
+        }), "sort");
+        B200_TRY(cuda->timed("kmeans_update", [&] {
+            return launch_kmeans_update<T>(dX.as<T>(), ld, n, d, k, dSorted.as<int>(),
+                                           dOffsets.as<int>(), dSegStart.as<int>(), SEG_ROWS,
+                                           dChunkSums.as<double>(), dCounts.as<int>(), dCprev,
+                                           dCnew, ld, dScalars.as<double>(), dFlags.as<int>(), st);
+        }), "update");
+    }
+    if (h_scal) {
+        B200_TRY(cudaMemcpyAsync(h_scal, dScalars.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, st),
+                 "copy");
+    }
+    if (h_flags) {
+        B200_TRY(cudaMemcpyAsync(h_flags, dFlags.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st),
+                 "copy");
+    }
+    B200_TRY(cudaStreamSynchronize(st), "Lloyd iteration");
+    return da_status_success;
+}
+
+// Empty-cluster splitting (kmeans.cpp:1127-1330), on the host.
+template <typename T> da_status KMeans<T>::split_empty(T *dC, int *dL, bool &split) {
+    split = false;
+    const da_int n = n_samples, k = n_clusters, d = n_features;
+    std::vector<int> lab(n);
+    std::vector<T> Cc;
+    B200_TRY(cudaMemcpyAsync(lab.data(), dL, n * sizeof(int), cudaMemcpyDeviceToHost, cuda->stream),
+             "copy");
+    B200_TRY(download_centres<T>(dC, k, d, ld, Cc, cuda->stream), "copy");
+    std::vector<da_int> cnt(k, 0);
+    for (da_int i = 0; i < n; ++i) cnt[lab[i]]++;
+    da_int n_empty = 0;
+    for (da_int c = 0; c < k; ++c) n_empty += cnt[c] == 0;
+    if (n_empty == 0) return da_status_success;
+    std::vector<T> w(n);
+    auto dist_to = [&](da_int i, da_int c) {
+        T s = T(0);
+        for (da_int j = 0; j < d; ++j) {
+            T t = host_at(*this, i, j) - Cc[c + (size_t)j * k];
+            s += t * t;
+        }
+        return s;
+    };
+    for (da_int i = 0; i < n; ++i) w[i] = dist_to(i, lab[i]);
+    for (da_int c = 0; c < k; ++c) {
+        if (cnt[c] != 0) continue;
+        da_int bi = -1;
+        T bd = T(-1);
+        for (da_int i = 0; i < n; ++i)
+            if (cnt[lab[i]] > 1 && std::isfinite(w[i]) && w[i] > bd) {
+                bd = w[i];
+                bi = i;
+            }
+        if (bi < 0) break;
+        const da_int old = lab[bi], nold = cnt[old];
+        for (da_int j = 0; j < d; ++j) {
+            T &cv = Cc[old + (size_t)j * k];
+            cv = (cv * T(nold) - host_at(*this, bi, j)) / T(nold - 1);
+        }
+        for (da_int j = 0; j < d; ++j) Cc[c + (size_t)j * k] = host_at(*this, bi, j);
+        cnt[old] -= 1;
+        cnt[c] = 1;
+        lab[bi] = (int)c;
+        w[bi] = T(0);
+        if (n_empty > 1)
+            for (da_int i = 0; i < n; ++i)
+                if (lab[i] == old) w[i] = dist_to(i, old);
+    }
+    B200_TRY(upload_centres<T>(Cc, k, d, ld, dC, cuda->stream), "copy");
+    B200_TRY(cudaMemcpyAsync(dL, lab.data(), n * sizeof(int), cudaMemcpyHostToDevice, cuda->stream),
+             "copy");
+    B200_TRY(cudaStreamSynchronize(cuda->stream), "split");
+    split = true;
+    return da_status_success;
+}
+
+// perform_kmeans (kmeans.cpp:996-1058)
+template <typename T>
+da_status KMeans<T>::run_lloyd(T *&dCcur, T *&dCprev, int *&dLcur, int *&dLprev, da_int &n_iter,
+                               int &converged, double &inertia, bool &empty_found) {
+    double *h_scal = static_cast<double *>(h_small);
+    int *h_flags = reinterpret_cast<int *>(static_cast<char *>(h_small) + 64);
+    converged = 0;
+    empty_found = false;
+    da_int it = 0;
+    for (it = 0; it < max_iter; ++it) {
+        std::swap(dCprev, dCcur);
+        std::swap(dLprev, dLcur);
+        da_status s = lloyd_step(dCprev, dCcur, dLcur, dLprev, true, h_scal, h_flags);
+        if (s != da_status_success) return s;
+        if (empty_mode != EC_IGNORE && h_flags[1] > 0) {
+            if (empty_mode == EC_ERROR) {
+                empty_found = true;
+                return da_status_success;
+            }
+            bool split = false;
+            s = split_empty(dCcur, dLcur, split);
+            if (s != da_status_success) return s;
+            if (split) continue;
+        }
+        // convergence_test (kmeans.cpp:1359-1397)
+        int conv = 0;
+        if (it > 1 && h_flags[0] == 0) conv = 2;
+        if (conv == 0 && std::sqrt(h_scal[1]) < tol * std::sqrt(h_scal[0])) conv = 1;
+        converged = conv;
+        if (converged > 0) break;
+    }
+    n_iter = it;
+    if (converged == 1 || it == max_iter) {
+        // relabel against the final centres without updating them
+        std::swap(dLprev, dLcur);
+        da_status s = lloyd_step(dCcur, nullptr, dLcur, nullptr, false, nullptr, nullptr);
+        if (s != da_status_success) return s;
+    }
+    B200_TRY(launch_kmeans_inertia<T>(dX.as<T>(), ld, n_samples, n_features, dCcur, ld, dLcur,
+                                      dPartials.as<double>(), dScalars.as<double>() + 2,
+                                      cuda->stream), "inertia");
+    B200_TRY(cudaMemcpyAsync(h_scal + 2, dScalars.as<double>() + 2, sizeof(double),
+                             cudaMemcpyDeviceToHost, cuda->stream), "copy");
+    B200_TRY(cudaStreamSynchronize(cuda->stream), "inertia");
+    inertia = h_scal[2];
+    return da_status_success;
+}
+
+// Option reading and consistency checks of kmeans.cpp:359-458.
+template <typename T> da_status KMeans<T>::read_options() {
+    n_clusters = opts.i("n_clusters");
+    init_method = opts.key("initialization method");
+    n_init = opts.i("n_init");
+    max_iter = opts.i("max_iter");
+    tol = opts.r("convergence tolerance");
+    seed = opts.i("seed");
+    afk_samples = opts.i("afk-mc2 samples");
+    algorithm = opts.key("algorithm");
+    empty_mode = opts.key("empty clusters");
+    const bool spherical = opts.key("distance") == 1;
+    da_status warn_status = da_status_success;
+    std::string warn_msg;
+    if (n_init > 1 && init_method == INIT_SUPPLIED) {
+        warn_msg = "n_init was set to " + std::to_string(n_init) +
+                   " but the initialization method was set to 'supplied'. The k-means "
+                   "algorithm will only be run once.";
+        n_init = 1;
+        warn_status = da_status_incompatible_options;
+    }
+    if (algorithm == ALG_HW && (n_clusters == 1 || n_clusters >= n_samples))
+        return err->error(da_status_incompatible_options,
+                          "The Hartigan-Wong algorithm requires 1 < k < n_samples.");
+    if (spherical && algorithm == ALG_HW)
+        return err->error(da_status_incompatible_options,
+                          "Cosine distance is not compatible with the Hartigan-Wong algorithm. "
+                          "Please use Lloyd, Elkan, or MacQueen.");
+    if (algorithm == ALG_HW || algorithm == ALG_MACQ)
+        return err->error(da_status_not_implemented,
+                          "The B200 library implements Lloyd's algorithm (and Elkan, whose "
+                          "iterates are Lloyd's); Hartigan-Wong and MacQueen are not provided.");
+    if (spherical)
+        return err->error(da_status_not_implemented,
+                          "Spherical (cosine) k-means is not provided by the B200 library.");
+    if (n_clusters > n_samples)
+        return err->error(da_status_incompatible_options,
+                          "n_clusters = " + std::to_string(n_clusters) + ", and n_samples = " +
+                              std::to_string(n_samples) + ". Constraint: n_clusters <= n_samples.");
+    if (init_method == INIT_SUPPLIED && !centres_supplied)
+        return err->error(da_status_no_data,
+                          "The initialization method was set to 'supplied' but no initial "
+                          "centres have been provided.");
+    if (n_clusters > 12288)
+        return err->error(da_status_not_implemented,
+                          "More than 12288 clusters are not supported by the B200 library.");
+    if (warn_status != da_status_success) return err->warn(warn_status, warn_msg);
+    return da_status_success;
+}
+
+// kmeans.cpp:351-783
+template <typename T> da_status KMeans<T>::compute() {
+    if (!initdone)
+        return err->error(da_status_no_data,
+                          "No data has been passed to the handle. Please call "
+                          "da_kmeans_set_data_s or da_kmeans_set_data_d.");
+    if (order() != data_order)
+        return err->error(da_status_incompatible_options,
+                          "The storage order option was changed after data was set.");
+    da_status warn_status = da_status_success;
+    std::string warn_msg;
+    {
+        da_status s0 = read_options();
+        if (s0 != da_status_success && err->severity == DA_ERROR) return s0;
+        if (s0 != da_status_success) {
+            warn_status = s0;
+            warn_msg = err->message;
+            err->clear();
+        }
+    }
+    da_status s = ensure_device_data();
+    if (s != da_status_success) return s;
+    s = alloc_work();
+    if (s != da_status_success) return s;
+    if (init_method != INIT_SUPPLIED) {
+        if (seed == -1) {
+            std::random_device r;
+            seed = std::abs((da_int)r());
+        }
+        mt_gen.seed(seed);
+    }
+    best_inertia = std::numeric_limits<double>::infinity();
+    bool valid = false, first_valid = true;
+    for (da_int run = 0; run < n_init; ++run) {
+        T *dCcur = dC0.as<T>(), *dCprev = dC1.as<T>();
+        int *dLcur = dL0.as<int>(), *dLprev = dL1.as<int>();
+        s = init_centres(dCcur);
+        if (s != da_status_success) return s;
+        da_int n_iter = 0;
+        int converged = 0;
+        double inertia = 0;
+        bool empty = false;
+        s = run_lloyd(dCcur, dCprev, dLcur, dLprev, n_iter, converged, inertia, empty);
+        if (s != da_status_success) return s;
+        if (empty) continue;
+        valid = true;
+        if (inertia < best_inertia || first_valid) {
+            first_valid = false;
+            best_inertia = inertia;
+            best_n_iter = n_iter;
+            warn_maxit = converged == 0;
+            B200_TRY(download_centres<T>(dCcur, n_clusters, n_features, ld, best_centres,
+                                         cuda->stream), "copy");
+            // labels stay on the device until they are queried
+            if (!dBestL.ensure((size_t)n_samples * sizeof(int)))
+                return err->error(da_status_memory_error, "Device memory allocation failed.");
+            B200_TRY(cudaMemcpyAsync(dBestL.p, dLcur, n_samples * sizeof(int),
+                                     cudaMemcpyDeviceToDevice, cuda->stream), "copy");
+            B200_TRY(cudaStreamSynchronize(cuda->stream), "copy");
+            best_labels_on_host = false;
+        }
+    }
+    if (!valid)
+        return err->error(da_status_empty_clusters,
+                          "All " + std::to_string(n_init) +
+                              " run(s) of the k-means algorithm resulted in at least one empty "
+                              "cluster during the k-means iterations. A better set of initial "
+                              "cluster centers is needed.");
+    model_trained = true;
+    if (warn_maxit) return err->warn(da_status_maxit, "The maximum number of iterations was reached.");
+    if (warn_status != da_status_success) return err->warn(warn_status, warn_msg);
+    return da_status_success;
+}
+
+// Initial centres of the configured initialisation method (B200 extension).
+template <typename T> da_status KMeans<T>::initial_centres(T *C, da_int ldc) {
+    if (!initdone)
+        return err->error(da_status_no_data,
+                          "No data has been passed to the handle. Please call "
+                          "da_kmeans_set_data_s or da_kmeans_set_data_d.");
+    da_status s = read_options();
+    if (s != da_status_success && err->severity == DA_ERROR) return s;
+    err->clear();
+    if (C == nullptr) return err->error(da_status_invalid_pointer, "The array C is null.");
+    const da_order ord = order();
+    if ((ord == column_major && ldc < n_clusters) || (ord == row_major && ldc < n_features))
+        return err->error(da_status_invalid_leading_dimension, "ldc is too small.");
+    s = ensure_device_data();
+    if (s != da_status_success) return s;
+    s = alloc_work();
+    if (s != da_status_success) return s;
+    if (init_method != INIT_SUPPLIED) {
+        if (seed == -1) {
+            std::random_device r;
+            seed = std::abs((da_int)r());
+        }
+        mt_gen.seed(seed);
+    }
+    s = init_centres(dC0.as<T>());
+    if (s != da_status_success) return s;
+    std::vector<T> Cc;
+    B200_TRY(download_centres<T>(dC0.as<T>(), n_clusters, n_features, ld, Cc, cuda->stream), "copy");
+    for (da_int i = 0; i < n_clusters; ++i)
+        for (da_int j = 0; j < n_features; ++j)
+            C[ord == row_major ? (size_t)i * ldc + j : i + (size_t)j * ldc] =
+                Cc[i + (size_t)j * n_clusters];
+    return da_status_success;
+}
+
+// kmeans.cpp:894-993
+template <typename T>
+da_status KMeans<T>::predict(da_int m, da_int d, const T *Y, da_int ldy, da_int *labels) {
+    if (!model_trained)
+        return err->warn(da_status_no_data,
+                         "The k-means has not been computed. Please call da_kmeans_compute_s or "
+                         "da_kmeans_compute_d.");
+    if (d != n_features)
+        return err->error(da_status_invalid_input,
+                          "The function was called with k_features = " + std::to_string(d) +
+                              " but the k-means has been computed with " +
+                              std::to_string(n_features) + " features.");
+    da_status s = check_2d(*err, order(), m, d, Y, ldy, "k_samples", "k_features", "Y", "ldy", 1,
+                           1, opts.key("check data") == 1);
+    if (s != da_status_success) return s;
+    if (labels == nullptr) return err->error(da_status_invalid_pointer, "The array Y_labels is null.");
+    s = cuda->init(*err);
+    if (s != da_status_success) return s;
+    cudaStream_t st = cuda->stream;
+    if (!dY.ensure((size_t)m * ld * sizeof(T)) || !dYL.ensure((size_t)m * sizeof(int)) ||
+        !dC0.ensure((size_t)n_clusters * ld * sizeof(T)) || !dCn.ensure(n_clusters * sizeof(T)))
+        return err->error(da_status_memory_error, "Device memory allocation failed.");
+    B200_TRY(upload_matrix<T>(order(), m, d, Y, ldy, dY.as<T>(), ld, dStage, st), "upload");
+    B200_TRY(upload_centres<T>(best_centres, n_clusters, n_features, ld, dC0.as<T>(), st), "upload");
+    B200_TRY(launch_centre_norms<T>(dC0.as<T>(), ld, n_clusters, n_features, dCn.as<T>(), st), "norms");
+    B200_TRY(launch_kmeans_assign<T>(dY.as<T>(), ld, m, n_features, dC0.as<T>(), ld, n_clusters,
+                                     dCn.as<T>(), dYL.as<int>(), nullptr, nullptr, nullptr, st),
+             "assign");
+    std::vector<int> lab(m);
+    B200_TRY(cudaMemcpyAsync(lab.data(), dYL.p, m * sizeof(int), cudaMemcpyDeviceToHost, st), "copy");
+    B200_TRY(cudaStreamSynchronize(st), "predict");
+    for (da_int i = 0; i < m; ++i) labels[i] = lab[i];
+    return da_status_success;
+}
+
+// kmeans.cpp:786-891: X_transform_ij = |x_i - c_j| (GEMM form, no clamp).
+template <typename T>
+da_status KMeans<T>::transform(da_int m, da_int d, const T *X, da_int ldx, T *Xt, da_int ldxt) {
+    if (!model_trained)
+        return err->warn(da_status_no_data,
+                         "The k-means has not been computed. Please call da_kmeans_compute_s or "
+                         "da_kmeans_compute_d.");
+    if (d != n_features)
+        return err->error(da_status_invalid_input,
+                          "The function was called with m_features = " + std::to_string(d) +
+                              " but the k-means has been computed with " +
+                              std::to_string(n_features) + " features.");
+    da_status s = check_2d(*err, order(), m, d, X, ldx, "m_samples", "m_features", "X", "ldx", 1, 1,
+                           opts.key("check data") == 1);
+    if (s != da_status_success) return s;
+    s = check_2d(*err, order(), m, n_clusters, Xt, ldxt, "m_samples", "n_clusters", "X_transform",
+                 "ldx_transform", 1, 1, false);
+    if (s != da_status_success) return s;
+    s = cuda->init(*err);
+    if (s != da_status_success) return s;
+    cudaStream_t st = cuda->stream;
+    const size_t outn = (size_t)m * n_clusters;
+    if (!dY.ensure((size_t)m * ld * sizeof(T)) || !dYL.ensure((size_t)m * sizeof(T)) ||
+        !dC0.ensure((size_t)n_clusters * ld * sizeof(T)) || !dCn.ensure(n_clusters * sizeof(T)) ||
+        !dKD.ensure(outn * sizeof(T)))
+        return err->error(da_status_memory_error, "Device memory allocation failed.");
+    B200_TRY(upload_matrix<T>(order(), m, d, X, ldx, dY.as<T>(), ld, dStage, st), "upload");
+    B200_TRY(upload_centres<T>(best_centres, n_clusters, n_features, ld, dC0.as<T>(), st), "upload");
+    B200_TRY(launch_centre_norms<T>(dC0.as<T>(), ld, n_clusters, n_features, dCn.as<T>(), st), "norms");
+    B200_TRY(launch_row_sqnorms<T>(dY.as<T>(), ld, m, n_features, dYL.as<T>(), st), "norms");
+    PairwiseArgs a{ACC_DOT, POST_GEMM_SQRT, 256, 2.0, false, order() == row_major};
+    B200_TRY(launch_pairwise<T>(dY.as<T>(), ld, m, dC0.as<T>(), ld, n_clusters, n_features,
+                                dYL.as<T>(), dCn.as<T>(), a, dKD.as<T>(), st), "transform");
+    std::vector<T> out(outn);
+    B200_TRY(cudaMemcpyAsync(out.data(), dKD.p, outn * sizeof(T), cudaMemcpyDeviceToHost, st), "copy");
+    B200_TRY(cudaStreamSynchronize(st), "transform");
+    const bool rm = order() == row_major;
+    for (da_int i = 0; i < m; ++i)
+        for (da_int j = 0; j < n_clusters; ++j)
+            Xt[rm ? (size_t)i * ldxt + j : i + (size_t)j * ldxt] =
+                out[rm ? (size_t)i * n_clusters + j : i + (size_t)j * m];
+    return da_status_success;
+}
+
+// kmeans.cpp:146-224
+template <typename T> da_status KMeans<T>::get_result_t(da_result q, da_int *dim, T *out) {
+    if (!model_trained)
+        return err->warn(da_status_no_data,
+                         "k-means clustering has not yet been computed. Please call "
+                         "da_kmeans_compute_s or da_kmeans_compute_d before extracting results.");
+    switch (q) {
+    case da_rinfo:
+        if (*dim < 6) {
+            *dim = 6;
+            return err->warn(da_status_invalid_array_dimension,
+                             "The array is too small. Please provide an array of at least size: 6.");
+        }
+        out[0] = (T)n_samples;
+        out[1] = (T)n_features;
+        out[2] = (T)n_clusters;
+        out[3] = (T)best_n_iter;
+        out[4] = (T)best_inertia;
+        out[5] = (T)best_lp_n_iter;
+        return da_status_success;
+    case da_kmeans_cluster_centres: {
+        const da_int need = n_clusters * n_features;
+        if (*dim < need) {
+            *dim = need;
+            return err->warn(da_status_invalid_array_dimension,
+                             "The array is too small. Please provide an array of at least size: " +
+                                 std::to_string(need) + ".");
+        }
+        const bool rm = order() == row_major;
+        for (da_int i = 0; i < n_clusters; ++i)
+            for (da_int j = 0; j < n_features; ++j)
+                out[rm ? (size_t)i * n_features + j : i + (size_t)j * n_clusters] =
+                    best_centres[i + (size_t)j * n_clusters];
+        return da_status_success;
+    }
+    default:
+        return err->warn(da_status_unknown_query, "The requested result could not be found.");
+    }
+}
+template <typename T> da_status KMeans<T>::get_result(da_result q, da_int *dim, double *out) {
+    if constexpr (std::is_same_v<T, double>) return get_result_t(q, dim, (T *)out);
+    return err->error(da_status_wrong_type, "Wrong precision type.");
+}
+template <typename T> da_status KMeans<T>::get_result(da_result q, da_int *dim, float *out) {
+    if constexpr (std::is_same_v<T, float>) return get_result_t(q, dim, (T *)out);
+    return err->error(da_status_wrong_type, "Wrong precision type.");
+}
+template <typename T> da_status KMeans<T>::get_result_int(da_result q, da_int *dim, da_int *out) {
+    if (q == da_trained) return AlgBase::get_result_int(q, dim, out);
+    if (!model_trained)
+        return err->warn(da_status_no_data,
+                         "k-means clustering has not yet been computed. Please call "
+                         "da_kmeans_compute_s or da_kmeans_compute_d before extracting results.");
+    if (q == da_kmeans_labels) {
+        if (*dim < n_samples) {
+            *dim = n_samples;
+            return err->warn(da_status_invalid_array_dimension,
+                             "The array is too small. Please provide an array of at least size: " +
+                                 std::to_string(n_samples) + ".");
+        }
+        if (!best_labels_on_host) {
+            std::vector<int> lab(n_samples);
+            B200_TRY(cudaMemcpyAsync(lab.data(), dBestL.p, n_samples * sizeof(int),
+                                     cudaMemcpyDeviceToHost, cuda->stream), "copy");
+            B200_TRY(cudaStreamSynchronize(cuda->stream), "copy");
+            best_labels.assign(lab.begin(), lab.end());
+            best_labels_on_host = true;
+        }
+        for (da_int i = 0; i < n_samples; ++i) out[i] = best_labels[i];
+        return da_status_success;
+    }
+    return err->warn(da_status_unknown_query, "The requested result could not be found.");
+}
+
+template struct KMeans<float>;
+template struct KMeans<double>;
+
+} // namespace b200

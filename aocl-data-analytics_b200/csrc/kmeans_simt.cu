@@ -1,0 +1,487 @@
+// k-means (Lloyd) kernels for sm_100a: SIMT assignment with fused argmin,
+// deterministic counting-sort centroid update in fp64, k-means++ helpers.
+//
+// Reference algorithm (AOCL-DA):
+//   assignment  kmeans_lloyd.hpp:189-198 (W = -2 C A^T, then argmin_j W_ij + |c_j|^2
+//               in kmeans_kernels.cpp:209-234; strict '<', so ties keep the lower j)
+//   update      kmeans_lloyd.hpp:275-361 (sum of member rows), :364-405 (divide by
+//               max(count,1): an empty cluster becomes the zero vector)
+//   shift       kmeans.cpp:1334-1355, convergence kmeans.cpp:1359-1397
+//   inertia     kmeans.cpp:1061-1124
+//   k-means++   kmeans.cpp:1491-1664
+// Here sums, shift and inertia are accumulated in fp64 in a fixed order, so
+// every result is run-to-run deterministic and independent of scheduling.
+#include "b200_common.cuh"
+#include "b200_kernels.hpp"
+#include "simt_engine.cuh"
+
+namespace b200 {
+
+static constexpr int SORT_ROWS = 1024; // rows per counting-sort block
+
+int kmeans_assign_block_rows() { return SORT_ROWS; }
+int kmeans_max_clusters_fused() { return 1 << 20; }
+
+// ------------------------------------------------------------- assign ----
+// CTA = BM rows x all clusters (cluster tiles of BN), thread tile TM x TN.
+template <typename T>
+__global__ void __launch_bounds__(256)
+kmeans_assign_kernel(const T *X, int n, int ld, int d, const T *C, int k, const T *cnorm,
+                     int *labels, const int *labels_prev, int *flags) {
+    using Cf = SimtCfg<T>;
+    constexpr int TM = Cf::TM, TN = Cf::TN, BK = Cf::BK, BM = 16 * TM, BN = 16 * TN;
+    __shared__ __align__(16) Stage<T, BM, BN, BK> st[2];
+    __shared__ int changed;
+    const int tid = threadIdx.x, tm = tid / 16, tn = tid % 16;
+    const int i0 = blockIdx.x * BM;
+    if (tid == 0) changed = 0;
+
+    T best[TM];
+    int bidx[TM];
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+        best[i] = Lim<T>::inf();
+        bidx[i] = 0x7fffffff;
+    }
+    Acc<T, TM, TN> acc;
+    for (int j0 = 0; j0 < k; j0 += BN) {
+        compute_tile<T, ACC_DOT, TM, TN, BM, BN, BK>(st, X, ld, n, i0, C, ld, k, j0, d, 256,
+                                                     T(0), acc, tid);
+#pragma unroll
+        for (int j = 0; j < TN; ++j) {
+            const int gj = j0 + (j / 4) * 64 + tn * 4 + (j % 4);
+            if (gj >= k) continue;
+            const T cn = cnorm[gj];
+#pragma unroll
+            for (int i = 0; i < TM; ++i) {
+                // |c|^2 - 2 x.c: -2 s is exact, so this is the reference's
+                // fl(fl(-2 s) + |c|^2).
+                const T v = fma_rn(T(-2), acc.g1[i][j], cn);
+                if (key_less(v, gj, best[i], bidx[i])) {
+                    best[i] = v;
+                    bidx[i] = gj;
+                }
+            }
+        }
+    }
+    // reduce across the 16 lanes that share these rows (lanes tn = 0..15)
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+#pragma unroll
+        for (int off = 8; off >= 1; off >>= 1) {
+            const T ov = __shfl_xor_sync(0xffffffffu, best[i], off);
+            const int oi = __shfl_xor_sync(0xffffffffu, bidx[i], off);
+            if (key_less(ov, oi, best[i], bidx[i])) {
+                best[i] = ov;
+                bidx[i] = oi;
+            }
+        }
+    }
+    if (tn == 0) {
+        int ch = 0;
+#pragma unroll
+        for (int i = 0; i < TM; ++i) {
+            const int gi = i0 + tm * 4 + i;
+            if (gi < n) {
+                // NaN distances never win: fall back to cluster 0 as the
+                // reference's scalar kernel does (label initialised to 0).
+                const int lbl = (bidx[i] == 0x7fffffff) ? 0 : bidx[i];
+                labels[gi] = lbl;
+                if (labels_prev && labels_prev[gi] != lbl) ch = 1;
+            }
+        }
+        if (ch) changed = 1;
+    }
+    __syncthreads();
+    if (tid == 0 && changed && flags) atomicOr(&flags[0], 1);
+}
+
+template <typename T>
+cudaError_t launch_kmeans_assign(const T *X, int ldx, int n, int d, const T *C, int ldc, int k,
+                                 const T *cnorm, int *labels, const int *labels_prev,
+                                 int *block_counts, int *flags, cudaStream_t s) {
+    (void)block_counts;
+    if (ldx != ldc) return cudaErrorInvalidValue;
+    using Cf = SimtCfg<T>;
+    constexpr int BM = 16 * Cf::TM;
+    kmeans_assign_kernel<T><<<(n + BM - 1) / BM, 256, 0, s>>>(X, n, ldx, d, C, k, cnorm, labels,
+                                                              labels_prev, flags);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------- counting sort ---
+// (1) per SORT_ROWS block histogram of labels.
+__global__ void label_hist_kernel(const int *labels, int n, int k, int *block_counts) {
+    extern __shared__ int h[];
+    for (int j = threadIdx.x; j < k; j += blockDim.x) h[j] = 0;
+    __syncthreads();
+    const int r0 = blockIdx.x * SORT_ROWS;
+    const int r1 = min(n, r0 + SORT_ROWS);
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) atomicAdd(&h[labels[i]], 1);
+    __syncthreads();
+    for (int j = threadIdx.x; j < k; j += blockDim.x)
+        block_counts[(size_t)blockIdx.x * k + j] = h[j];
+}
+// (2) one warp per cluster: exclusive scan of its block counts (in place).
+__global__ void block_scan_kernel(int *block_counts, int nblocks, int k, int *counts) {
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (j >= k) return;
+    int carry = 0;
+    for (int b0 = 0; b0 < nblocks; b0 += 32) {
+        const int b = b0 + lane;
+        const int v = (b < nblocks) ? block_counts[(size_t)b * k + j] : 0;
+        int x = v;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= off) x += y;
+        }
+        if (b < nblocks) block_counts[(size_t)b * k + j] = carry + x - v;
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (lane == 0) counts[j] = carry;
+}
+// (3) single CTA: cluster offsets and per-cluster segment-chunk starts.
+__global__ void cluster_offsets_kernel(const int *counts, int k, int seg_rows, int *offsets,
+                                       int *seg_chunk_start, int *flags) {
+    __shared__ int s_off[1024], s_seg[1024];
+    int carry_off = 0, carry_seg = 0;
+    for (int j0 = 0; j0 < k; j0 += 1024) {
+        const int j = j0 + threadIdx.x;
+        const int c = (j < k) ? counts[j] : 0;
+        const int sc = (c + seg_rows - 1) / seg_rows;
+        s_off[threadIdx.x] = c;
+        s_seg[threadIdx.x] = sc;
+        __syncthreads();
+        // Hillis-Steele inclusive scan over 1024 entries
+        for (int off = 1; off < 1024; off <<= 1) {
+            int a = 0, b = 0;
+            if ((int)threadIdx.x >= off) {
+                a = s_off[threadIdx.x - off];
+                b = s_seg[threadIdx.x - off];
+            }
+            __syncthreads();
+            s_off[threadIdx.x] += a;
+            s_seg[threadIdx.x] += b;
+            __syncthreads();
+        }
+        if (j < k) {
+            offsets[j] = carry_off + s_off[threadIdx.x] - c;
+            seg_chunk_start[j] = carry_seg + s_seg[threadIdx.x] - sc;
+        }
+        const int tot_off = s_off[1023], tot_seg = s_seg[1023];
+        __syncthreads();
+        carry_off += tot_off;
+        carry_seg += tot_seg;
+    }
+    if (threadIdx.x == 0) {
+        offsets[k] = carry_off;
+        seg_chunk_start[k] = carry_seg;
+    }
+    // empty-cluster count
+    __shared__ int s_empty;
+    if (threadIdx.x == 0) s_empty = 0;
+    __syncthreads();
+    for (int j = threadIdx.x; j < k; j += blockDim.x)
+        if (counts[j] == 0) atomicAdd(&s_empty, 1);
+    __syncthreads();
+    if (threadIdx.x == 0 && flags) flags[1] = s_empty;
+}
+// (4) one warp per SORT_ROWS block: stable scatter of row ids.
+__global__ void label_scatter_kernel(const int *labels, int n, int k, const int *block_offsets,
+                                     const int *offsets, int *sorted_rows) {
+    extern __shared__ int ctr[];
+    const int b = blockIdx.x;
+    const int lane = threadIdx.x;
+    for (int j = lane; j < k; j += 32) ctr[j] = offsets[j] + block_offsets[(size_t)b * k + j];
+    __syncwarp();
+    const int r0 = b * SORT_ROWS;
+    const int r1 = min(n, r0 + SORT_ROWS);
+    for (int base = r0; base < r1; base += 32) {
+        const int i = base + lane;
+        const bool valid = i < r1;
+        const unsigned active = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+            const int lbl = labels[i];
+            const unsigned peers = __match_any_sync(active, lbl);
+            const unsigned lt = (1u << lane) - 1u;
+            const int pos = ctr[lbl] + __popc(peers & lt);
+            sorted_rows[pos] = i;
+            __syncwarp(active);
+            if ((__ffs(peers) - 1) == lane) ctr[lbl] += __popc(peers);
+        }
+        __syncwarp();
+    }
+}
+
+cudaError_t launch_kmeans_sort(const int *labels, int n, int k, const int *block_counts_in,
+                               int *counts, int *offsets, int *seg_chunk_start, int seg_rows,
+                               int *sorted_rows, int *flags, cudaStream_t s) {
+    int *block_counts = const_cast<int *>(block_counts_in);
+    const int nblocks = (n + SORT_ROWS - 1) / SORT_ROWS;
+    const size_t hs = (size_t)k * sizeof(int);
+    label_hist_kernel<<<nblocks, 256, hs, s>>>(labels, n, k, block_counts);
+    block_scan_kernel<<<(k * 32 + 255) / 256, 256, 0, s>>>(block_counts, nblocks, k, counts);
+    cluster_offsets_kernel<<<1, 1024, 0, s>>>(counts, k, seg_rows, offsets, seg_chunk_start,
+                                              flags);
+    label_scatter_kernel<<<nblocks, 32, hs, s>>>(labels, n, k, block_counts, offsets,
+                                                 sorted_rows);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------- update ----
+// One warp per (cluster, chunk of seg_rows sorted rows): fp64 sums in row order.
+template <typename T>
+__global__ void seg_sum_kernel(const T *X, int ld, int d, int k, const int *sorted_rows,
+                               const int *offsets, const int *seg_chunk_start, int seg_rows,
+                               double *chunk_sums) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int total = seg_chunk_start[k];
+    if (w >= total) return;
+    // cluster of chunk w: last j with seg_chunk_start[j] <= w
+    int lo = 0, hi = k - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (seg_chunk_start[mid] <= w) lo = mid;
+        else hi = mid - 1;
+    }
+    const int j = lo;
+    const int r_begin = offsets[j] + (w - seg_chunk_start[j]) * seg_rows;
+    const int r_end = min(offsets[j + 1], r_begin + seg_rows);
+    double *out = chunk_sums + (size_t)w * ld;
+    for (int d0 = 0; d0 < d; d0 += 128) {
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        const int c0 = d0 + lane, c1 = c0 + 32, c2 = c0 + 64, c3 = c0 + 96;
+        for (int r = r_begin; r < r_end; ++r) {
+            const T *x = X + (size_t)sorted_rows[r] * ld;
+            if (c0 < d) a0 += (double)x[c0];
+            if (c1 < d) a1 += (double)x[c1];
+            if (c2 < d) a2 += (double)x[c2];
+            if (c3 < d) a3 += (double)x[c3];
+        }
+        if (c0 < d) out[c0] = a0;
+        if (c1 < d) out[c1] = a1;
+        if (c2 < d) out[c2] = a2;
+        if (c3 < d) out[c3] = a3;
+    }
+}
+// One thread per (cluster, feature): combine the cluster's chunks in order,
+// divide, and emit per-block fp64 partials of |C_prev|^2 and |C_prev-C_new|^2.
+template <typename T>
+__global__ void centre_finalize_kernel(int k, int d, int ld, const int *counts,
+                                       const int *seg_chunk_start, const double *chunk_sums,
+                                       const T *C_prev, T *C_new, double *block_partials) {
+    __shared__ double s0[256], s1[256];
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double pn = 0.0, ps = 0.0;
+    if (e < k * d) {
+        const int j = e / d, f = e % d;
+        double sum = 0.0;
+        for (int c = seg_chunk_start[j]; c < seg_chunk_start[j + 1]; ++c)
+            sum += chunk_sums[(size_t)c * ld + f];
+        const int cnt = counts[j];
+        const T cn = T(sum / (double)(cnt > 0 ? cnt : 1));
+        const size_t o = (size_t)j * ld + f;
+        const T cp = C_prev[o];
+        C_new[o] = cn;
+        pn = (double)cp * (double)cp;
+        const double df = (double)cp - (double)cn;
+        ps = df * df;
+    }
+    s0[threadIdx.x] = pn;
+    s1[threadIdx.x] = ps;
+    __syncthreads();
+    for (int off = 128; off > 0; off >>= 1) {
+        if ((int)threadIdx.x < off) {
+            s0[threadIdx.x] += s0[threadIdx.x + off];
+            s1[threadIdx.x] += s1[threadIdx.x + off];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        block_partials[2 * blockIdx.x] = s0[0];
+        block_partials[2 * blockIdx.x + 1] = s1[0];
+    }
+}
+// Single warp: sum per-block partials in block order (deterministic).
+__global__ void sum_partials_kernel(const double *partials, int nblocks, int stride,
+                                    int nvals, double *out) {
+    const int lane = threadIdx.x;
+    for (int v = 0; v < nvals; ++v) {
+        double a = 0.0;
+        for (int b = lane; b < nblocks; b += 32) a += partials[(size_t)b * stride + v];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
+        if (lane == 0) out[v] = a;
+    }
+}
+
+template <typename T>
+cudaError_t launch_kmeans_update(const T *X, int ldx, int n, int d, int k,
+                                 const int *sorted_rows, const int *offsets,
+                                 const int *seg_chunk_start, int seg_rows, double *chunk_sums,
+                                 const int *counts, const T *C_prev, T *C_new, int ldc,
+                                 double *scalars, int *flags, cudaStream_t s) {
+    (void)flags;
+    (void)n;
+    if (ldx != ldc) return cudaErrorInvalidValue;
+    // chunk count upper bound: n / seg_rows + k
+    const int max_chunks = n / seg_rows + k + 1;
+    seg_sum_kernel<T><<<(max_chunks * 32 + 255) / 256, 256, 0, s>>>(
+        X, ldx, d, k, sorted_rows, offsets, seg_chunk_start, seg_rows, chunk_sums);
+    const int e = k * d;
+    const int nb = (e + 255) / 256;
+    // block partials live after the scalars block (scalars[8...])
+    double *partials = scalars + 8;
+    centre_finalize_kernel<T><<<nb, 256, 0, s>>>(k, d, ldc, counts, seg_chunk_start, chunk_sums,
+                                                 C_prev, C_new, partials);
+    sum_partials_kernel<<<1, 32, 0, s>>>(partials, nb, 2, 2, scalars);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------- centre norms ----
+template <typename T>
+cudaError_t launch_centre_norms(const T *C, int ldc, int k, int d, T *out, cudaStream_t s) {
+    return launch_row_sqnorms<T>(C, ldc, k, d, out, s);
+}
+
+// ------------------------------------------------------------ inertia ----
+template <typename T>
+__global__ void inertia_kernel(const T *X, int ld, int n, int d, const T *C, const int *labels,
+                               double *block_partials) {
+    __shared__ double sh[8];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double acc = 0.0;
+    // one warp per row (rows strided by the grid), lanes over features
+    const int gw = blockIdx.x * 8 + warp;
+    const int nw = gridDim.x * 8;
+    for (int i = gw; i < n; i += nw) {
+        const T *x = X + (size_t)i * ld;
+        const T *c = C + (size_t)labels[i] * ld;
+        double r = 0.0;
+        for (int f = lane; f < d; f += 32) {
+            const double t = (double)x[f] - (double)c[f];
+            r += t * t;
+        }
+        acc += r;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if (lane == 0) sh[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += sh[w];
+        block_partials[blockIdx.x] = t;
+    }
+}
+template <typename T>
+cudaError_t launch_kmeans_inertia(const T *X, int ldx, int n, int d, const T *C, int ldc,
+                                  const int *labels, double *block_partials, double *out,
+                                  cudaStream_t s) {
+    if (ldx != ldc) return cudaErrorInvalidValue;
+    const int nb = 148 * 8;
+    inertia_kernel<T><<<nb, 256, 0, s>>>(X, ldx, n, d, C, labels, block_partials);
+    sum_partials_kernel<<<1, 32, 0, s>>>(block_partials, nb, 1, 1, out);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ k-means++ --
+// D[c*n + i] = fl(-2 x_i.x_c + fl(|x_i|^2 + |x_c|^2)) -- the GEMM form of
+// euclidean_gemm_distance with precomputed norms (kmeans.cpp:1491-1521).
+template <typename T>
+__global__ void kpp_dist_kernel(const T *X, int ld, int n, int d, const T *xnorm,
+                                const int *cand, int t, T *D) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    T *cs = reinterpret_cast<T *>(sm);
+    for (int e = threadIdx.x; e < t * d; e += blockDim.x) {
+        const int c = e / d, f = e % d;
+        cs[e] = X[(size_t)cand[c] * ld + f];
+    }
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const T *x = X + (size_t)i * ld;
+    for (int c = 0; c < t; ++c) {
+        T s = T(0);
+        const T *y = cs + c * d;
+        for (int f = 0; f < d; ++f) s = fma_rn(x[f], y[f], s);
+        const T nn = add_rn(xnorm[i], xnorm[cand[c]]);
+        D[(size_t)c * n + i] = fma_rn(T(-2), s, nn);
+    }
+}
+template <typename T>
+cudaError_t launch_kpp_dist(const T *X, int ldx, int n, int d, const T *xnorm, const int *cand,
+                            int t, T *D, cudaStream_t s) {
+    const size_t sm = (size_t)t * d * sizeof(T);
+    kpp_dist_kernel<T><<<(n + 255) / 256, 256, sm, s>>>(X, ldx, n, d, xnorm, cand, t, D);
+    return cudaGetLastError();
+}
+template <typename T>
+__global__ void kpp_cost_kernel(const T *w, const T *D, int n, int t, double *block_partials) {
+    __shared__ double sh[256];
+    for (int c = 0; c < t; ++c) {
+        double a = 0.0;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+            T v = D[(size_t)c * n + i];
+            T wi = w[i];
+            T m = v < wi ? v : wi;
+            if (!(m > T(0))) m = T(0);
+            a += (double)m;
+        }
+        sh[threadIdx.x] = a;
+        __syncthreads();
+        for (int off = 128; off > 0; off >>= 1) {
+            if ((int)threadIdx.x < off) sh[threadIdx.x] += sh[threadIdx.x + off];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) block_partials[(size_t)blockIdx.x * t + c] = sh[0];
+        __syncthreads();
+    }
+}
+template <typename T>
+cudaError_t launch_kpp_cost(const T *w, const T *D, int n, int t, double *block_partials,
+                            double *cost, cudaStream_t s) {
+    const int nb = 148 * 4;
+    kpp_cost_kernel<T><<<nb, 256, 0, s>>>(w, D, n, t, block_partials);
+    sum_partials_kernel<<<1, 32, 0, s>>>(block_partials, nb, t, t, cost);
+    return cudaGetLastError();
+}
+template <typename T>
+__global__ void kpp_update_kernel(T *w, const T *Dc, int n, int chosen) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    T v = Dc[i], wi = w[i];
+    T m = v < wi ? v : wi;
+    if (!(m > T(0))) m = T(0);
+    w[i] = (i == chosen) ? T(0) : m;
+}
+template <typename T>
+cudaError_t launch_kpp_update(T *w, const T *Dc, int n, int chosen, cudaStream_t s) {
+    kpp_update_kernel<T><<<(n + 255) / 256, 256, 0, s>>>(w, Dc, n, chosen);
+    return cudaGetLastError();
+}
+
+#define B200_KM_INST(T)                                                                        \
+    template cudaError_t launch_kmeans_assign<T>(const T *, int, int, int, const T *, int, int, \
+                                                 const T *, int *, const int *, int *, int *,   \
+                                                 cudaStream_t);                                 \
+    template cudaError_t launch_kmeans_update<T>(const T *, int, int, int, int, const int *,    \
+                                                 const int *, const int *, int, double *,       \
+                                                 const int *, const T *, T *, int, double *,    \
+                                                 int *, cudaStream_t);                          \
+    template cudaError_t launch_centre_norms<T>(const T *, int, int, int, T *, cudaStream_t);   \
+    template cudaError_t launch_kmeans_inertia<T>(const T *, int, int, int, const T *, int,     \
+                                                  const int *, double *, double *,              \
+                                                  cudaStream_t);                                \
+    template cudaError_t launch_kpp_dist<T>(const T *, int, int, int, const T *, const int *,   \
+                                            int, T *, cudaStream_t);                            \
+    template cudaError_t launch_kpp_cost<T>(const T *, const T *, int, int, double *, double *, \
+                                            cudaStream_t);                                      \
+    template cudaError_t launch_kpp_update<T>(T *, const T *, int, int, cudaStream_t);
+B200_KM_INST(float)
+B200_KM_INST(double)
+
+} // namespace b200

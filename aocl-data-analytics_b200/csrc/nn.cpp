@@ -1,0 +1,535 @@
+// Brute-force k-nearest-neighbours handle (host side).  Argument checks,
+// option semantics and status codes follow
+// source/core/nearest_neighbors/nearest_neighbors.cpp; the distance tile and
+// the top-k selection run on the GPU (dist_simt.cu).
+#include "alg.hpp"
+
+namespace b200 {
+
+// metric ids of the "metric" option (aoclda_metrics.h:44-59)
+enum { M_EUC = 0, M_SQEUC = 1, M_MINK = 2, M_MANH = 3, M_COS = 4, M_EUC_GEMM = 5,
+       M_SQEUC_GEMM = 6, M_IP = 7 };
+// algorithm ids (nearest_neighbors_types.hpp:29)
+enum { A_BRUTE = 0, A_KD = 1, A_BALL = 2, A_AUTO = 3 };
+
+template <typename T>
+NN<T>::NN(ErrorRecord *e, CudaCtx *c, bool single) {
+    err = e;
+    cuda = c;
+    opts.single = single;
+    register_common_options(opts);
+    // nearest_neighbors_options.hpp:52-124
+    const da_int imax = std::numeric_limits<da_int>::max();
+    const da_int imin = std::numeric_limits<da_int>::min();
+    const double fmax = (double)std::numeric_limits<T>::max();
+    const double flow = (double)std::numeric_limits<T>::lowest();
+    opts.add_int("number of neighbors", 1, LB::greaterequal, imax, UB::p_inf, 5);
+    opts.add_int("leaf size", 1, LB::greaterequal, imax, UB::p_inf, 30);
+    opts.add_int("outlier label", imin, LB::m_inf, imax, UB::p_inf, 0);
+    opts.add_real("minkowski parameter", 0.0, LB::greaterthan, fmax, UB::p_inf, 2.0);
+    opts.add_real("radius", 0.0, LB::greaterequal, fmax, UB::p_inf, 1.0);
+    opts.add_real("outlier target", flow, LB::m_inf, fmax, UB::p_inf, 0.0);
+    opts.add_string("algorithm",
+                    {{"auto", A_AUTO}, {"brute", A_BRUTE}, {"kd tree", A_KD}, {"ball tree", A_BALL}},
+                    "auto");
+    opts.add_string("metric",
+                    {{"euclidean", M_EUC},
+                     {"l2", M_EUC},
+                     {"sqeuclidean", M_SQEUC},
+                     {"manhattan", M_MANH},
+                     {"l1", M_MANH},
+                     {"cityblock", M_MANH},
+                     {"cosine", M_COS},
+                     {"minkowski", M_MINK},
+                     {"sqeuclidean_gemm", M_SQEUC_GEMM},
+                     {"euclidean_gemm", M_EUC_GEMM},
+                     {"inner product", M_IP}},
+                    "euclidean");
+    opts.add_string("weights", {{"uniform", 0}, {"distance", 1}}, "uniform");
+    opts.add_string("outlier handling", {{"none", 0}, {"manual", 1}, {"most frequent", 2}},
+                    "none");
+    // B200 options (no counterpart in the reference):
+    //   "reference isa": which AOCL-DA build's KC blocking the squared-euclidean
+    //   summation order reproduces (avx512: KC=256/512, avx2: KC=64/32).
+    opts.add_string("reference isa", {{"avx512", 0}, {"avx2", 1}}, "avx512");
+}
+
+template <typename T> da_status NN<T>::set_params() {
+    n_neighbors = opts.i("number of neighbors");
+    algo = opts.key("algorithm");
+    metric = opts.key("metric");
+    weights = opts.key("weights");
+    p = (T)opts.r("minkowski parameter");
+    // Tree algorithms reject non-metric distances (nearest_neighbors.cpp:313-330).
+    if (algo == A_KD || algo == A_BALL) {
+        if (metric == M_COS || metric == M_SQEUC || metric == M_SQEUC_GEMM || metric == M_IP)
+            return err->error(da_status_incompatible_options,
+                              "The tree algorithms are not compatible with the cosine, squared "
+                              "Euclidean, or inner product distances.");
+        if (metric == M_MINK && p < T(1))
+            return err->error(da_status_incompatible_options,
+                              "Tree algorithms are not compatible with the Minkowski metric when "
+                              "0 < p < 1.");
+    }
+    up_to_date = true;
+    return da_status_success;
+}
+
+// nearest_neighbors.cpp:398-466: after set_data the tree-related options are
+// locked.  As in the reference, "number of neighbors", "metric", "weights" and
+// "minkowski parameter" are read when the training data are set
+// (set_params, nearest_neighbors.cpp:497-499) and not re-read afterwards.
+template <typename T> da_status NN<T>::check_options_update() {
+    const da_int a = opts.key("algorithm");
+    if (a == A_AUTO || a == A_KD || a == A_BALL) {
+        if (a != locked_algo || opts.i("leaf size") != locked_leaf)
+            return err->error(da_status_option_locked,
+                              "Options need to be set before calling set_training_data().");
+        if (a == A_AUTO &&
+            (opts.key("metric") != locked_metric || (T)opts.r("minkowski parameter") != locked_p))
+            return err->error(da_status_option_locked,
+                              "Options need to be set before calling set_training_data().");
+    }
+    return da_status_success;
+}
+
+template <typename T>
+da_status NN<T>::set_data(da_int n, da_int d, const T *X, da_int ldx) {
+    if (n_samples > 0 && n != n_samples)
+        return err->error(da_status_invalid_array_dimension,
+                          "n_samples = " + std::to_string(n) +
+                              " doesn't match the training data size " +
+                              std::to_string(n_samples) + ".");
+    const da_order ord = order();
+    da_status s = check_2d(*err, ord, n, d, X, ldx, "n_samples", "n_features", "X_train",
+                           "ldx_train", 1, 1, opts.key("check data") == 1);
+    if (s != da_status_success) return s;
+    n_samples = n;
+    n_features = d;
+    X_host = X;
+    ldx_host = ldx;
+    data_order = ord;
+    have_X = true;
+    X_on_device = false;
+    xn_kind = -1;
+    s = set_params();
+    if (s != da_status_success) return s;
+    locked_algo = algo;
+    locked_leaf = opts.i("leaf size");
+    locked_metric = metric;
+    locked_p = p;
+    // Upload now when a device is present (the reference keeps the user's
+    // pointer; an eager device copy is a safe superset of that contract).
+    if (cuda->init(*err) == da_status_success) {
+        s = ensure_device_data();
+        if (s != da_status_success) return s;
+    } else {
+        err->clear();
+    }
+    return da_status_success;
+}
+
+template <typename T> da_status NN<T>::ensure_device_data() {
+    da_status s = cuda->init(*err);
+    if (s != da_status_success) return s;
+    if (X_on_device) return da_status_success;
+    ld = pad4(n_features);
+    if (!dX.ensure((size_t)n_samples * ld * sizeof(T)))
+        return err->error(da_status_memory_error, "Device memory allocation failed.");
+    B200_TRY(upload_matrix<T>(data_order, n_samples, n_features, X_host, ldx_host, dX.as<T>(),
+                              ld, dStage, cuda->stream),
+             "upload of X_train");
+    X_on_device = true;
+    xn_kind = -1;
+    return da_status_success;
+}
+
+template <typename T> da_status NN<T>::set_labels(da_int n, const da_int *y) {
+    if (n_samples > 0 && n != n_samples)
+        return err->error(da_status_invalid_array_dimension,
+                          "n_samples = " + std::to_string(n) +
+                              " doesn't match the training data size " +
+                              std::to_string(n_samples) + ".");
+    if (n < 1)
+        return err->error(da_status_invalid_array_dimension,
+                          "The function was called with n_samples = " + std::to_string(n) +
+                              ". Constraint: n_samples >= 1.");
+    if (y == nullptr) return err->error(da_status_invalid_pointer, "The array y_train_class is null.");
+    n_samples = n;
+    y_class = y;
+    have_labels = true;
+    classes_done = false;
+    return da_status_success;
+}
+
+template <typename T> da_status NN<T>::set_targets(da_int n, const T *y) {
+    if (n_samples > 0 && n != n_samples)
+        return err->error(da_status_invalid_array_dimension,
+                          "n_samples = " + std::to_string(n) +
+                              " doesn't match the training data size " +
+                              std::to_string(n_samples) + ".");
+    if (n < 1)
+        return err->error(da_status_invalid_array_dimension,
+                          "The function was called with n_samples = " + std::to_string(n) +
+                              ". Constraint: n_samples >= 1.");
+    if (y == nullptr) return err->error(da_status_invalid_pointer, "The array y_train_reg is null.");
+    n_samples = n;
+    y_reg = y;
+    have_targets = true;
+    return da_status_success;
+}
+
+template <typename T>
+da_status NN<T>::validate_queries(da_int nq, da_int d, const T *Xt, da_int ldt) {
+    if (Xt == nullptr) return err->error(da_status_invalid_pointer, "X_test is not a valid pointer.");
+    if (d != n_features)
+        return err->error(da_status_invalid_array_dimension,
+                          "n_features = " + std::to_string(d) +
+                              " doesn't match the expected value " +
+                              std::to_string(n_features) + ".");
+    return check_2d(*err, order(), nq, d, Xt, ldt, "n_queries", "n_features", "X_test",
+                    "ldx_test", 1, 1, opts.key("check data") == 1);
+}
+
+// Run the fused distance + top-k kernels; ind/dist are q-major (q*k + r).
+template <typename T>
+da_status NN<T>::kneighbors_compute(da_int nq, da_int d, const T *Xt, da_int ldt, da_order ord,
+                                    da_int k, std::vector<da_int> &ind, std::vector<T> *dist) {
+    da_status s = ensure_device_data();
+    if (s != da_status_success) return s;
+    cudaStream_t st = cuda->stream;
+    // metric -> accumulation family, selection key and output transform
+    int acc = ACC_SQEUC, post = POST_NONE, tf = 0, norm_kind = -1;
+    switch (metric) {
+    case M_EUC: acc = ACC_SQEUC; post = POST_NONE; tf = 1; break;
+    case M_SQEUC: acc = ACC_SQEUC; post = POST_NONE; break;
+    case M_EUC_GEMM: acc = ACC_DOT; post = POST_GEMM_SQ_CLAMP; tf = 1; norm_kind = 0; break;
+    case M_SQEUC_GEMM: acc = ACC_DOT; post = POST_GEMM_SQ_CLAMP; norm_kind = 0; break;
+    case M_MANH: acc = ACC_MANHATTAN; break;
+    case M_COS: acc = ACC_DOT; post = POST_COSINE; norm_kind = 1; break;
+    case M_IP: acc = ACC_DOT; post = POST_NEG; tf = 2; break;
+    case M_MINK:
+        if (p == T(2)) { acc = ACC_SQEUC; tf = 1; }
+        else if (p == T(1)) { acc = ACC_MANHATTAN; }
+        else { acc = ACC_MINKOWSKI; post = POST_POW; }
+        break;
+    }
+    const bool fp64 = sizeof(T) == 8;
+    const int kc = opts.key("reference isa") == 1 ? (fp64 ? 32 : 64) : (fp64 ? 512 : 256);
+    // queries -> device
+    if (!dQ.ensure((size_t)nq * ld * sizeof(T)))
+        return err->error(da_status_memory_error, "Device memory allocation failed.");
+    B200_TRY(upload_matrix<T>(ord, nq, d, Xt, ldt, dQ.as<T>(), ld, dStage, st), "upload of X_test");
+    const T *qn = nullptr, *xn = nullptr;
+    if (norm_kind >= 0) {
+        if (!dQn.ensure((size_t)nq * sizeof(T)) || !dXn.ensure((size_t)n_samples * sizeof(T)))
+            return err->error(da_status_memory_error, "Device memory allocation failed.");
+        if (norm_kind == 0) {
+            B200_TRY(launch_row_sqnorms<T>(dQ.as<T>(), ld, nq, d, dQn.as<T>(), st), "norms");
+            if (xn_kind != 0)
+                B200_TRY(launch_row_sqnorms<T>(dX.as<T>(), ld, n_samples, d, dXn.as<T>(), st), "norms");
+        } else {
+            B200_TRY(launch_row_norms_eps1<T>(dQ.as<T>(), ld, nq, d, dQn.as<T>(), st), "norms");
+            if (xn_kind != 1)
+                B200_TRY(launch_row_norms_eps1<T>(dX.as<T>(), ld, n_samples, d, dXn.as<T>(), st), "norms");
+        }
+        xn_kind = norm_kind;
+        qn = dQn.as<T>();
+        xn = dXn.as<T>();
+    }
+    if (k > knn_max_k(fp64))
+        return err->error(da_status_not_implemented,
+                          "k = " + std::to_string(k) + " exceeds the largest supported number "
+                          "of neighbours per query (" + std::to_string(knn_max_k(fp64)) + ").");
+    // chunking of the training rows: enough CTAs to fill 148 SMs several times
+    const int BN = knn_tile_rows_train(fp64);
+    const int q_tiles = (int)((nq + 63) / 64);
+    const int max_chunks = std::max(1, (int)((n_samples + BN - 1) / BN));
+    int n_chunks = std::max(1, std::min(max_chunks, (148 * 8 + q_tiles - 1) / q_tiles));
+    int chunk_rows = (int)((n_samples + n_chunks - 1) / n_chunks);
+    chunk_rows = ((chunk_rows + BN - 1) / BN) * BN;
+    n_chunks = (int)((n_samples + chunk_rows - 1) / chunk_rows);
+    KnnArgs a{acc, post, kc, (double)p, (int)k, chunk_rows, n_chunks};
+    const size_t parts = (size_t)nq * n_chunks * k;
+    if (!dPartK.ensure(parts * sizeof(T)) || !dPartI.ensure(parts * sizeof(int)) ||
+        !dOutK.ensure((size_t)nq * k * sizeof(T)) || !dOutI.ensure((size_t)nq * k * sizeof(int)))
+        return err->error(da_status_memory_error, "Device memory allocation failed.");
+    B200_TRY(cuda->timed("knn_chunks", [&] {
+        return launch_knn_chunks<T>(dQ.as<T>(), ld, (int)nq, dX.as<T>(), ld, (int)n_samples,
+                                    (int)d, qn, xn, a, dPartK.as<T>(), dPartI.as<int>(), nullptr,
+                                    st);
+    }), "kNN distance kernel");
+    B200_TRY(cuda->timed("knn_merge", [&] {
+        return launch_knn_merge<T>(dPartK.as<T>(), dPartI.as<int>(), (int)nq, n_chunks, (int)k,
+                                   tf, dOutK.as<T>(), dOutI.as<int>(), st);
+    }), "kNN merge kernel");
+    ind.resize((size_t)nq * k);
+    std::vector<int> tmp((size_t)nq * k);
+    B200_TRY(cudaMemcpyAsync(tmp.data(), dOutI.p, tmp.size() * sizeof(int), cudaMemcpyDeviceToHost, st),
+             "download");
+    if (dist) {
+        dist->resize((size_t)nq * k);
+        B200_TRY(cudaMemcpyAsync(dist->data(), dOutK.p, dist->size() * sizeof(T),
+                                 cudaMemcpyDeviceToHost, st), "download");
+    }
+    B200_TRY(cudaStreamSynchronize(st), "kNN");
+    for (size_t i = 0; i < tmp.size(); ++i) ind[i] = (da_int)tmp[i];
+    return da_status_success;
+}
+
+// nearest_neighbors.cpp:940-1015
+template <typename T>
+da_status NN<T>::kneighbors(da_int nq, da_int d, const T *Xt, da_int ldt, da_int *n_ind,
+                            T *n_dist, da_int k, da_int return_distance) {
+    if (!have_X)
+        return err->error(da_status_no_data,
+                          "No training data have been set. Please call da_nn_set_data_s or "
+                          "da_nn_set_data_d.");
+    da_status s = check_options_update();
+    if (s != da_status_success) return s;
+    if (n_ind == nullptr) return err->error(da_status_invalid_pointer, "n_ind is not a valid pointer.");
+    s = validate_queries(nq, d, Xt, ldt);
+    if (s != da_status_success) return s;
+    if (k <= 0 && n_neighbors <= 0)
+        return err->error(da_status_invalid_input, "Number of requested neighbors must be positive.");
+    if (k <= 0) k = n_neighbors;
+    if (k > n_samples)
+        return err->error(da_status_invalid_input,
+                          "Number of requested neighbors must be at least as big as the number "
+                          "of samples.");
+    if (return_distance && n_dist == nullptr)
+        return err->error(da_status_invalid_pointer, "n_dist is not a valid pointer.");
+    std::vector<da_int> ind;
+    std::vector<T> dist;
+    s = kneighbors_compute(nq, d, Xt, ldt, order(), k, ind, return_distance ? &dist : nullptr);
+    if (s != da_status_success) return s;
+    // outputs: q-major for row-major storage, n_queries x k column-major otherwise
+    const bool cm = order() == column_major;
+    for (da_int q = 0; q < nq; ++q)
+        for (da_int r = 0; r < k; ++r) {
+            const size_t src = (size_t)q * k + r;
+            const size_t dst = cm ? (size_t)r * nq + q : src;
+            n_ind[dst] = ind[src];
+            if (return_distance) n_dist[dst] = dist[src];
+        }
+    return da_status_success;
+}
+
+template <typename T> da_status NN<T>::available_classes() {
+    if (!have_X)
+        return err->error(da_status_no_data,
+                          "No training data have been set. Please call da_nn_set_data_s or "
+                          "da_nn_set_data_d.");
+    if (!have_labels)
+        return err->error(da_status_no_data,
+                          "No classification labels have been set. Please call "
+                          "da_nn_set_labels_s or da_nn_set_labels_d.");
+    std::set<da_int> s(y_class, y_class + n_samples);
+    classes.assign(s.begin(), s.end());
+    classes_done = true;
+    return da_status_success;
+}
+
+template <typename T> da_status NN<T>::classes_api(da_int *n_classes, da_int *cls) {
+    if (n_classes == nullptr)
+        return err->error(da_status_invalid_pointer, "n_classes is not a valid pointer.");
+    if (!classes_done) {
+        da_status s = available_classes();
+        if (s != da_status_success) return s;
+    }
+    const da_int nc = (da_int)classes.size();
+    if (*n_classes <= 0 || cls == nullptr) {
+        *n_classes = nc;
+        return da_status_success;
+    }
+    if (*n_classes < nc) {
+        *n_classes = nc;
+        return err->error(da_status_invalid_array_dimension,
+                          "The classes array is too small, it must be at least " +
+                              std::to_string(nc) + ".");
+    }
+    for (da_int i = 0; i < nc; ++i) cls[i] = classes[i];
+    *n_classes = nc;
+    return da_status_success;
+}
+
+// Vote of predict_proba_compute_knn (nearest_neighbors.cpp:1166-1272):
+// proba is q-major (q * n_classes + c).
+template <typename T>
+da_status NN<T>::compute_proba(da_int nq, da_int d, const T *Xt, da_int ldt,
+                               std::vector<T> &proba) {
+    if (metric == M_IP && weights == 1)
+        return err->error(da_status_incompatible_options,
+                          "The inner product metric is not compatible with "
+                          "weights=\"distance\". Use weights=\"uniform\" instead.");
+    if (!classes_done) {
+        da_status s = available_classes();
+        if (s != da_status_success) return s;
+    }
+    const da_int k = n_neighbors;
+    if (k > n_samples)
+        return err->error(da_status_invalid_input,
+                          "Number of requested neighbors must be at least as big as the number "
+                          "of samples.");
+    std::vector<da_int> ind;
+    std::vector<T> dist;
+    da_status s = kneighbors_compute(nq, d, Xt, ldt, order(), k, ind, weights == 1 ? &dist : nullptr);
+    if (s != da_status_success) return s;
+    const da_int nc = (da_int)classes.size();
+    proba.assign((size_t)nq * nc, T(0));
+    for (da_int q = 0; q < nq; ++q) {
+        T den = T(0);
+        for (da_int c = 0; c < nc; ++c) {
+            T v = T(0);
+            for (da_int r = 0; r < k; ++r) {
+                const da_int lbl = y_class[ind[(size_t)q * k + r]];
+                if (lbl != classes[c]) continue;
+                if (weights == 0) v += T(1);
+                else {
+                    const T w = dist[(size_t)q * k + r];
+                    v += (w <= std::numeric_limits<T>::epsilon()) ? T(1) : T(1) / w;
+                }
+            }
+            proba[(size_t)q * nc + c] = v;
+            den += v;
+        }
+        for (da_int c = 0; c < nc; ++c) proba[(size_t)q * nc + c] /= den;
+    }
+    return da_status_success;
+}
+
+template <typename T>
+da_status NN<T>::predict_proba(da_int nq, da_int d, const T *Xt, da_int ldt, T *proba,
+                               da_nn_search_mode mode) {
+    if (!have_X)
+        return err->error(da_status_no_data,
+                          "No training data have been set. Please call da_nn_set_data_s or "
+                          "da_nn_set_data_d.");
+    if (!have_labels)
+        return err->error(da_status_no_data,
+                          "No classification labels have been set. Please call "
+                          "da_nn_set_labels_s or da_nn_set_labels_d.");
+    da_status s = check_options_update();
+    if (s != da_status_success) return s;
+    if (proba == nullptr) return err->error(da_status_invalid_pointer, "proba is not a valid pointer.");
+    if (nq < 1)
+        return err->error(da_status_invalid_array_dimension,
+                          "Number of queries must be greater than zero.");
+    if (d < 1)
+        return err->error(da_status_invalid_array_dimension,
+                          "Number of features must be greater than zero.");
+    s = validate_queries(nq, d, Xt, ldt);
+    if (s != da_status_success) return s;
+    if (mode != knn_search_mode)
+        return err->error(da_status_not_implemented,
+                          "Radius-neighbours search is not provided by the B200 library.");
+    std::vector<T> pr;
+    s = compute_proba(nq, d, Xt, ldt, pr);
+    if (s != da_status_success) return s;
+    const da_int nc = (da_int)classes.size();
+    const bool cm = order() == column_major;
+    for (da_int q = 0; q < nq; ++q)
+        for (da_int c = 0; c < nc; ++c)
+            proba[cm ? (size_t)c * nq + q : (size_t)q * nc + c] = pr[(size_t)q * nc + c];
+    return da_status_success;
+}
+
+template <typename T>
+da_status NN<T>::predict(da_int nq, da_int d, const T *Xt, da_int ldt, da_int *y,
+                         da_nn_search_mode mode) {
+    da_status s = check_options_update();
+    if (s != da_status_success) return s;
+    if (!have_X)
+        return err->error(da_status_no_data,
+                          "No training data have been set. Please call da_nn_set_data_s or "
+                          "da_nn_set_data_d.");
+    if (!have_labels)
+        return err->error(da_status_no_data,
+                          "No classification labels have been set. Please call "
+                          "da_nn_set_labels_s or da_nn_set_labels_d.");
+    if (y == nullptr) return err->error(da_status_invalid_pointer, "y_test is not a valid pointer.");
+    if (nq < 1)
+        return err->error(da_status_invalid_array_dimension, "n_queries must be greater than 0.");
+    s = validate_queries(nq, d, Xt, ldt);
+    if (s != da_status_success) return s;
+    if (mode != knn_search_mode)
+        return err->error(da_status_not_implemented,
+                          "Radius-neighbours search is not provided by the B200 library.");
+    std::vector<T> pr;
+    s = compute_proba(nq, d, Xt, ldt, pr);
+    if (s != da_status_success) return s;
+    const da_int nc = (da_int)classes.size();
+    for (da_int q = 0; q < nq; ++q) {
+        // first maximum (cblas_iamax semantics, nearest_neighbors.cpp:1566-1573)
+        da_int best = 0;
+        T bv = std::fabs(pr[(size_t)q * nc]);
+        for (da_int c = 1; c < nc; ++c) {
+            const T v = std::fabs(pr[(size_t)q * nc + c]);
+            if (v > bv) {
+                bv = v;
+                best = c;
+            }
+        }
+        y[q] = classes[best];
+    }
+    return da_status_success;
+}
+
+template <typename T>
+da_status NN<T>::predict_reg(da_int nq, da_int d, const T *Xt, da_int ldt, T *y,
+                             da_nn_search_mode mode) {
+    if (!have_X)
+        return err->error(da_status_no_data,
+                          "No training data have been set. Please call da_nn_set_data_s or "
+                          "da_nn_set_data_d.");
+    if (!have_targets)
+        return err->error(da_status_no_data,
+                          "No regression targets have been set. Please call "
+                          "da_nn_set_targets_s or da_nn_set_targets_d.");
+    da_status s = check_options_update();
+    if (s != da_status_success) return s;
+    if (y == nullptr) return err->error(da_status_invalid_pointer, "y_test is not a valid pointer.");
+    if (nq < 1)
+        return err->error(da_status_invalid_array_dimension, "n_queries must be greater than 0.");
+    s = validate_queries(nq, d, Xt, ldt);
+    if (s != da_status_success) return s;
+    if (mode != knn_search_mode)
+        return err->error(da_status_not_implemented,
+                          "Radius-neighbours search is not provided by the B200 library.");
+    if (metric == M_IP && weights == 1)
+        return err->error(da_status_incompatible_options,
+                          "The inner product metric is not compatible with "
+                          "weights=\"distance\". Use weights=\"uniform\" instead.");
+    const da_int k = n_neighbors;
+    if (k > n_samples)
+        return err->error(da_status_invalid_input,
+                          "Number of requested neighbors must be at least as big as the number "
+                          "of samples.");
+    std::vector<da_int> ind;
+    std::vector<T> dist;
+    s = kneighbors_compute(nq, d, Xt, ldt, order(), k, ind, weights == 1 ? &dist : nullptr);
+    if (s != da_status_success) return s;
+    // nearest_neighbors.cpp:1707-1747
+    for (da_int q = 0; q < nq; ++q) {
+        if (weights == 0) {
+            T sum = T(0);
+            for (da_int r = 0; r < k; ++r) sum += y_reg[ind[(size_t)q * k + r]];
+            y[q] = sum / T(k);
+        } else {
+            T num = T(0), den = T(0);
+            for (da_int r = 0; r < k; ++r) {
+                const T dv = dist[(size_t)q * k + r];
+                const T w = (dv <= std::numeric_limits<T>::epsilon()) ? T(1) : T(1) / dv;
+                num += y_reg[ind[(size_t)q * k + r]] * w;
+                den += w;
+            }
+            y[q] = num / den;
+        }
+    }
+    return da_status_success;
+}
+
+template struct NN<float>;
+template struct NN<double>;
+
+} // namespace b200

@@ -1,0 +1,44 @@
+/*
+ * aoclda_b200_ext.h -- B200-specific entry points of libaoclda_b200.so.
+ *
+ * None of these has a counterpart in the AOCL-DA C API; they expose what a
+ * GPU library needs beyond it (stream binding, kernel timing, access to the
+ * k-means initial centres).  Plain C types only.
+ */
+#ifndef AOCLDA_B200_EXT_H
+#define AOCLDA_B200_EXT_H
+
+#include "aoclda_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Bind the handle's work to a caller-owned CUDA stream (a cudaStream_t passed
+ * as void*); NULL restores the handle's own non-blocking stream.  Calls still
+ * return only after their results are complete. */
+da_status da_b200_set_stream(da_handle handle, void *stream);
+
+/* Kernel timing: when enabled, every launch of the named hot kernels is
+ * bracketed by CUDA events on the handle's stream and accumulated.  Intended
+ * for measurement (it serialises launches); off by default. */
+da_status da_b200_set_kernel_timing(da_handle handle, da_int enable);
+/* Total milliseconds and launch count accumulated for `kernel` ("knn_chunks",
+ * "knn_merge", "kmeans_assign", "kmeans_sort", "kmeans_update", ...). */
+da_status da_b200_get_kernel_time(da_handle handle, const char *kernel, double *total_ms,
+                                  da_int *launches);
+da_status da_b200_reset_kernel_time(da_handle handle);
+
+/* k-means: run only the configured initialisation method ("initialization
+ * method", "seed", "n_clusters") on the data set and write the n_clusters x
+ * n_features initial centres to C (storage order of the handle, leading
+ * dimension ldc).  The same centres are the starting point of
+ * da_kmeans_compute_? with n_init = 1. */
+da_status da_b200_kmeans_init_centres_d(da_handle handle, double *C, da_int ldc);
+da_status da_b200_kmeans_init_centres_s(da_handle handle, float *C, da_int ldc);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AOCLDA_B200_EXT_H */

@@ -1,0 +1,162 @@
+"""ctypes wrapper of liboracle.so, the CPU restatement of the reference path.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py as the checker.  The product never
+imports it.  Each wrapped function cites the AOCL-DA source it restates in
+oracle.c.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+METRICS = {"euclidean": 0, "sqeuclidean": 1, "minkowski": 2, "manhattan": 3, "cosine": 4,
+           "euclidean_gemm": 5, "sqeuclidean_gemm": 6, "inner product": 7}
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        _lib = C.CDLL(LIB)
+        P = C.c_void_p
+        i = C.c_int
+        for sfx, T in (("s", C.c_float), ("d", C.c_double)):
+            f = getattr(_lib, f"orc_pairwise_{sfx}")
+            f.argtypes = [i, i, i, P, P, P, T, i, i]
+            f.restype = None
+            f = getattr(_lib, f"orc_knn_{sfx}")
+            f.argtypes = [i, i, P, i, P, i, i, T, i, P, P]
+            f.restype = None
+            f = getattr(_lib, f"orc_kmeans_assign_{sfx}")
+            f.argtypes = [i, i, P, i, P, P, P]
+            f.restype = None
+            f = getattr(_lib, f"orc_kmeans_lloyd_{sfx}")
+            f.argtypes = [i, i, P, i, P, i, C.c_double, P, P, P, P]
+            f.restype = None
+        _lib.orc_kmeans_update_d.argtypes = [i, i, P, P, i, P, P]
+        _lib.orc_kmeans_update_d.restype = None
+        _lib.orc_kmeans_inertia_d.argtypes = [i, i, P, P, P]
+        _lib.orc_kmeans_inertia_d.restype = C.c_double
+        _lib.orc_kmeans_iteration_s.argtypes = [i, i, P, i, P, P]
+        _lib.orc_kmeans_iteration_s.restype = i
+        _lib.orc_knn_reference_ties_d.argtypes = [i, P, i, P]
+        _lib.orc_knn_reference_ties_d.restype = None
+        _lib.orc_num_threads.restype = i
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _sfx(dt):
+    return "d" if np.dtype(dt) == np.float64 else "s"
+
+
+def default_kc(dtype, isa="avx512"):
+    """KC slice length of the reference's packed blocking
+    (partitioning_infrastructure.hpp:45-59)."""
+    f64 = np.dtype(dtype) == np.float64
+    if isa == "avx2":
+        return 32 if f64 else 64
+    return 512 if f64 else 256
+
+
+def pairwise(X, Y=None, metric="euclidean", p=2.0, kc=None):
+    X = np.ascontiguousarray(X)
+    dt = X.dtype
+    Yc = None if Y is None else np.ascontiguousarray(Y, dtype=dt)
+    m, d = X.shape
+    n = m if Y is None else Yc.shape[0]
+    D = np.zeros((m, n), dtype=dt)
+    getattr(lib(), f"orc_pairwise_{_sfx(dt)}")(m, n, d, _p(X), _p(Yc), _p(D), p,
+                                               METRICS[metric], kc or default_kc(dt))
+    return D
+
+
+def knn(X, Q, k, metric="euclidean", p=2.0, kc=None):
+    """Exact top-k with ties to the lower index; returns (ind, dist) q-major."""
+    X = np.ascontiguousarray(X)
+    dt = X.dtype
+    Q = np.ascontiguousarray(Q, dtype=dt)
+    nx, d = X.shape
+    nq = Q.shape[0]
+    ind = np.zeros((nq, k), dtype=np.int32)
+    dist = np.zeros((nq, k), dtype=dt)
+    getattr(lib(), f"orc_knn_{_sfx(dt)}")(nx, d, _p(X), nq, _p(Q), k, METRICS[metric], p,
+                                          kc or default_kc(dt), _p(ind), _p(dist))
+    return ind, dist
+
+
+def kmeans_assign(X, Cn):
+    X = np.ascontiguousarray(X)
+    dt = X.dtype
+    Cn = np.ascontiguousarray(Cn, dtype=dt)
+    n, d = X.shape
+    lab = np.zeros(n, dtype=np.int32)
+    gap = np.zeros(n, dtype=np.float64)
+    getattr(lib(), f"orc_kmeans_assign_{_sfx(dt)}")(n, d, _p(X), Cn.shape[0], _p(Cn), _p(lab),
+                                                    _p(gap))
+    return lab, gap
+
+
+def kmeans_update(X, labels, k):
+    Xd = np.ascontiguousarray(X, dtype=np.float64)
+    n, d = Xd.shape
+    Cn = np.zeros((k, d), dtype=np.float64)
+    cnt = np.zeros(k, dtype=np.int32)
+    lab = np.ascontiguousarray(labels, dtype=np.int32)
+    lib().orc_kmeans_update_d(n, d, _p(Xd), _p(lab), k, _p(Cn), _p(cnt))
+    return Cn, cnt
+
+
+def kmeans_inertia(X, labels, Cn):
+    Xd = np.ascontiguousarray(X, dtype=np.float64)
+    n, d = Xd.shape
+    return lib().orc_kmeans_inertia_d(n, d, _p(Xd), _p(np.ascontiguousarray(labels, np.int32)),
+                                      _p(np.ascontiguousarray(Cn, np.float64)))
+
+
+def kmeans_lloyd(X, C0, max_iter=300, tol=1e-4):
+    X = np.ascontiguousarray(X)
+    dt = X.dtype
+    C0 = np.ascontiguousarray(C0, dtype=dt)
+    n, d = X.shape
+    k = C0.shape[0]
+    Cout = np.zeros_like(C0)
+    lab = np.zeros(n, dtype=np.int32)
+    nit = np.zeros(1, dtype=np.int32)
+    inertia = np.zeros(1, dtype=np.float64)
+    getattr(lib(), f"orc_kmeans_lloyd_{_sfx(dt)}")(n, d, _p(X), k, _p(C0), max_iter, tol,
+                                                   _p(Cout), _p(lab), _p(nit), _p(inertia))
+    return Cout, lab, int(nit[0]), float(inertia[0])
+
+
+def kmeans_iteration(X, C, labels):
+    """One Lloyd iteration in place (CPU baseline timing)."""
+    n, d = X.shape
+    return lib().orc_kmeans_iteration_s(n, d, _p(X), C.shape[0], _p(C), _p(labels))
+
+
+def knn_reference_ties(keys, k):
+    keys = np.ascontiguousarray(keys, dtype=np.float64)
+    ind = np.zeros(k, dtype=np.int32)
+    lib().orc_knn_reference_ties_d(len(keys), _p(keys), k, _p(ind))
+    return ind
+
+
+def num_threads():
+    return lib().orc_num_threads()

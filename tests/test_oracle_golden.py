@@ -1,0 +1,117 @@
+"""Pins the CPU oracle against the reference's own known-answer tests.
+
+The oracle (oracle/oracle.c) restates the AOCL-DA algorithms; before it is
+trusted as the checker of the GPU path it must reproduce the golden vectors
+of the reference's test-suite (converted by tests/golden/make_golden.py).
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+
+def classify_mismatch(X, Q, got, want, dist64):
+    """Indices that differ must be exact ties in fp64 distance."""
+    bad = 0
+    for q in range(len(got)):
+        if np.array_equal(got[q], want[q]):
+            continue
+        a = np.sort(dist64[q][got[q]])
+        b = np.sort(dist64[q][want[q]])
+        if not np.allclose(a, b, rtol=1e-12, atol=0):
+            bad += 1
+    return bad
+
+
+@pytest.mark.parametrize("tag", ["2092x2071x5", "2125x2068x20"])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_oracle_knn_golden_csv(orc, tag, dtype):
+    z = golden(f"nn_{tag}.npz")
+    X = z["X_train"].astype(dtype)
+    Q = z["X_test"].astype(dtype)
+    ind, dist = orc.knn(X, Q, 5, "euclidean")
+    eps = np.finfo(dtype).eps
+    # reference tolerance: 500 * eps (nearest_neighbors_tests.hpp:636)
+    np.testing.assert_allclose(dist, z["k_dist"], rtol=500 * eps, atol=500 * eps)
+    d64 = np.sqrt(((Q.astype(np.float64)[:, None, :] - X.astype(np.float64)[None]) ** 2).sum(-1))
+    assert classify_mismatch(X, Q, ind, z["k_ind"], d64) == 0
+
+
+def test_oracle_knn_small_hand_problem(orc):
+    z = golden("nn_small.npz")
+    for k, ki, kd in ((3, "kind3", "kdist3"), (4, "kind4", "kdist4")):
+        ind, dist = orc.knn(z["X_train"], z["X_test"], k, "euclidean")
+        # expected arrays are n_queries x k column-major
+        want_i = z[ki].reshape(k, 3).T
+        want_d = z[kd].reshape(k, 3).T
+        np.testing.assert_allclose(dist, want_d, rtol=40 * np.finfo(float).eps)
+        # identical except exact ties: q2's 4th neighbour is a tie between rows
+        # 0 and 2 (squared distance 38); the reference keeps the later row, the
+        # oracle the lower index
+        d64 = np.sqrt(((z["X_test"][:, None] - z["X_train"][None]) ** 2).sum(-1))
+        assert classify_mismatch(None, None, ind, want_i, d64) == 0
+        if k == 4:
+            assert (ind[2, 3], want_i[2, 3]) == (0, 2)
+
+
+def test_oracle_kmeans_lloyd80(orc):
+    z = golden("kmeans_lloyd80.npz")
+    C, lab, nit, inertia = orc.kmeans_lloyd(z["A"], z["C"], max_iter=30, tol=1e-4)
+    assert nit == int(z["expected_rinfo"][3])
+    np.testing.assert_array_equal(lab, z["expected_labels"])
+    np.testing.assert_allclose(C, z["expected_centres"], rtol=1e-4, atol=1e-5)
+    assert abs(inertia - z["expected_rinfo"][4]) < 1e-4
+
+
+def test_oracle_kmeans_lloyd80_single(orc):
+    z = golden("kmeans_lloyd80.npz")
+    C, lab, nit, inertia = orc.kmeans_lloyd(z["A"].astype(np.float32),
+                                            z["C"].astype(np.float32), max_iter=30, tol=1e-4)
+    assert nit == int(z["expected_rinfo"][3])
+    np.testing.assert_array_equal(lab, z["expected_labels"])
+    np.testing.assert_allclose(C, z["expected_centres"], rtol=1e-4, atol=1e-4)
+
+
+def test_oracle_sqeuclidean_order_matters(orc):
+    """The two-accumulator order is not the naive order: pin that the oracle
+    follows the reference's grouping (differs from a plain sequential sum on
+    some inputs) while agreeing with fp64 to rounding."""
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((64, 37)).astype(np.float32) * 10
+    Y = rng.standard_normal((48, 37)).astype(np.float32) * 10
+    D = orc.pairwise(X, Y, "sqeuclidean")
+    naive = np.zeros_like(D)
+    for i in range(64):
+        for j in range(48):
+            g = np.float32(0)
+            for t in range(37):
+                dd = np.float32(X[i, t] - Y[j, t])
+                g = np.float32(g + np.float32(dd * dd))
+            naive[i, j] = g
+    exact = ((X.astype(np.float64)[:, None] - Y.astype(np.float64)[None]) ** 2).sum(-1)
+    np.testing.assert_allclose(D, exact, rtol=1e-5)
+    assert not np.array_equal(D, naive)
+
+
+def test_oracle_kc_slicing(orc):
+    """d > KC: the slice boundary changes the summation order."""
+    rng = np.random.default_rng(4)
+    X = rng.standard_normal((8, 300)).astype(np.float32)
+    Y = rng.standard_normal((8, 300)).astype(np.float32)
+    a = orc.pairwise(X, Y, "sqeuclidean", kc=256)
+    b = orc.pairwise(X, Y, "sqeuclidean", kc=64)
+    exact = ((X.astype(np.float64)[:, None] - Y.astype(np.float64)[None]) ** 2).sum(-1)
+    np.testing.assert_allclose(a, exact, rtol=1e-5)
+    np.testing.assert_allclose(b, exact, rtol=1e-5)
+    assert not np.array_equal(a, b)
+
+
+def test_oracle_reference_tie_order(orc):
+    """The reference's running top-k keeps the LAST of equal distances at the
+    k boundary (<= replacement, nearest_neighbors_utils.hpp:206); the oracle's
+    knn() breaks ties to the lower index.  Both orders are reproduced."""
+    keys = np.array([5.0, 1.0, 3.0, 1.0, 3.0, 2.0])
+    ref = orc.knn_reference_ties(keys, 3)
+    assert list(ref) == [3, 1, 5]  # equal keys stay in buffer order
+    keys2 = np.array([1.0, 2.0, 2.0, 2.0])
+    assert list(orc.knn_reference_ties(keys2, 2)) == [0, 3]
