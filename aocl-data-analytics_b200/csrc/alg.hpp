@@ -116,7 +116,11 @@ template <typename T> struct KMeans : public AlgBase {
     int ld = 0;
     DevBuf dX, dXn, dC0, dC1, dCn, dL0, dL1, dCounts, dBlockCounts, dOffsets, dSorted,
         dChunkSums, dSegStart, dScalars, dFlags, dPartials, dW, dKD, dCand, dStage, dY, dYL,
-        dBestL;
+        dBestL, dXbf, dXnrm, dCbf, dCtmp, dTcScal, dAmb;
+    bool use_tc = false; // bf16 tensor-core assignment active for this compute
+    bool dXbf_stale = true;
+    int ldbf = 0;
+    da_int amb_last = 0;  // rows relabelled exactly in the last tensor-core pass
     T *h_pin = nullptr;
     void *h_small = nullptr; // pinned: flags + scalars
 
@@ -146,6 +150,8 @@ template <typename T> struct KMeans : public AlgBase {
     da_status lloyd_step(const T *dCprev, T *dCnew, int *dL, const int *dLprev, bool update,
                          double *h_scal, int *h_flags);
     da_status split_empty(T *dC, int *dL, bool &split);
+    da_status prepare_tc();
+    da_status assign(const T *dC, int *dL, const int *dLprev);
 };
 
 } // namespace b200

@@ -158,4 +158,25 @@ cudaError_t launch_kpp_cost(const T *w, const T *D, int n, int t, double *block_
 template <typename T>
 cudaError_t launch_kpp_update(T *w, const T *Dc, int n, int chosen, cudaStream_t s);
 
+// ------------------------------------------------- tensor-core k-means ---
+// 1 when the tcgen05 assignment handles (k clusters, d features).
+int tc_assign_supported(int k, int d);
+// fp32 row-major (ld) -> bf16 row-major with ldo = 64 * ceil(d/64), zero pad.
+cudaError_t launch_to_bf16(const float *X, int ld, int rows, int d, void *Y, int ldo,
+                           cudaStream_t s);
+// out[i] = |x_i| (fp32); *maxv = max_i |x_i| when maxv != null.
+cudaError_t launch_row_norm_max(const float *X, int ld, int rows, int d, float *out, float *maxv,
+                                cudaStream_t s);
+// BF16 tensor-core candidate assignment: certified rows get their exact fp32
+// label, the others are appended to amb_rows (*amb_count must be 0 on entry).
+cudaError_t launch_kmeans_assign_tc(const void *Xbf, int n, int ldbf, const void *Cbf, int k,
+                                    const float *cnorm, const float *xnorm, const float *cmax,
+                                    int *labels, const int *labels_prev, int *flags,
+                                    int *amb_rows, int *amb_count, int *err, cudaStream_t s);
+// Exact fp32 labels of the rows listed by the tensor-core pass.
+cudaError_t launch_kmeans_fixup(const float *X, int ld, int d, const float *C, int k,
+                                const float *cnorm, const int *amb_rows, const int *amb_count,
+                                int max_rows, int *labels, const int *labels_prev, int *flags,
+                                cudaStream_t s);
+
 } // namespace b200

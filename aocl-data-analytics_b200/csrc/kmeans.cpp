@@ -42,6 +42,10 @@ KMeans<T>::KMeans(ErrorRecord *e, CudaCtx *c, bool single) {
     opts.add_string("distance", {{"euclidean", 0}, {"cosine", 1}}, "euclidean");
     opts.add_string("normalize data", {{"yes", 1}, {"no", 0}}, "yes");
     opts.add_real("convergence tolerance", 0.0, LB::greaterequal, 0.0, UB::p_inf, 1.0e-4);
+    // B200 option (no counterpart in the reference): "bf16" runs the
+    // assignment on the tensor cores with a certified candidate pass whose
+    // labels equal the "plain" fp32 path's; fp64 data always use "plain".
+    opts.add_string("precision mode", {{"plain", 0}, {"bf16", 1}}, "bf16");
     opts.add_real("low precision convergence tolerance", 0.0, LB::greaterequal, 0.0, UB::p_inf,
                   1.0e-2);
 }
@@ -103,6 +107,7 @@ template <typename T> da_status KMeans<T>::ensure_device_data() {
              "upload of A");
     B200_TRY(launch_row_sqnorms<T>(dX.as<T>(), ld, n_samples, n_features, dXn.as<T>(), cuda->stream),
              "row norms");
+    dXbf_stale = true;
     return da_status_success;
 }
 
@@ -365,6 +370,69 @@ template <typename T> da_status KMeans<T>::init_centres(T *dC) {
     return da_status_success;
 }
 
+// Device state of the tensor-core assignment (fp32 data only): bf16 copy of
+// X, row norms |x_i|, bf16 centres, scalars and the relabel list.
+template <typename T> da_status KMeans<T>::prepare_tc() {
+    use_tc = false;
+    if constexpr (std::is_same_v<T, float>) {
+        if (opts.key("precision mode") != 1 || !tc_assign_supported(n_clusters, n_features))
+            return da_status_success;
+        const int nkb = (n_features + 63) / 64;
+        const int npad = (n_clusters + 15) & ~15;
+        const bool fresh = !dXbf.p || ldbf != nkb * 64;
+        ldbf = nkb * 64;
+        if (!dXbf.ensure((size_t)n_samples * ldbf * 2) || !dXnrm.ensure((size_t)n_samples * 4) ||
+            !dCbf.ensure((size_t)npad * ldbf * 2) || !dCtmp.ensure((size_t)npad * 4) ||
+            !dTcScal.ensure(64) || !dAmb.ensure((size_t)n_samples * 4))
+            return err->error(da_status_memory_error, "Device memory allocation failed.");
+        cudaStream_t st = cuda->stream;
+        if (fresh || dXbf_stale) {
+            B200_TRY(launch_to_bf16(dX.as<float>(), ld, n_samples, n_features, dXbf.p, ldbf, st),
+                     "bf16 copy");
+            B200_TRY(launch_row_norm_max(dX.as<float>(), ld, n_samples, n_features,
+                                         dXnrm.as<float>(), nullptr, st), "row norms");
+            dXbf_stale = false;
+        }
+        B200_TRY(cudaMemsetAsync(dCbf.p, 0, (size_t)npad * ldbf * 2, st), "memset");
+        B200_TRY(cudaMemsetAsync(dTcScal.p, 0, 64, st), "memset");
+        use_tc = true;
+    }
+    return da_status_success;
+}
+
+// Assignment of every row to its nearest centre (labels of the plain fp32
+// formula), on the tensor cores when use_tc, else on the CUDA cores.
+template <typename T> da_status KMeans<T>::assign(const T *dC, int *dL, const int *dLprev) {
+    cudaStream_t st = cuda->stream;
+    const int n = n_samples, k = n_clusters, d = n_features;
+    if constexpr (std::is_same_v<T, float>) {
+        if (use_tc) {
+            float *cmax = dTcScal.as<float>();
+            int *amb_cnt = reinterpret_cast<int *>(dTcScal.as<char>() + 16);
+            int *errf = reinterpret_cast<int *>(dTcScal.as<char>() + 20);
+            B200_TRY(launch_to_bf16(dC, ld, k, d, dCbf.p, ldbf, st), "bf16 centres");
+            B200_TRY(launch_row_norm_max(dC, ld, k, d, dCtmp.as<float>(), cmax, st), "centre norms");
+            B200_TRY(cudaMemsetAsync(amb_cnt, 0, sizeof(int), st), "memset");
+            B200_TRY(cuda->timed("kmeans_assign", [&] {
+                return launch_kmeans_assign_tc(dXbf.p, n, ldbf, dCbf.p, k, dCn.as<float>(),
+                                               dXnrm.as<float>(), cmax, dL, dLprev,
+                                               dFlags.as<int>(), dAmb.as<int>(), amb_cnt, errf, st);
+            }), "tensor-core assign");
+            B200_TRY(cuda->timed("kmeans_fixup", [&] {
+                return launch_kmeans_fixup(dX.as<float>(), ld, d, dC, k, dCn.as<float>(),
+                                           dAmb.as<int>(), amb_cnt, n, dL, dLprev,
+                                           dFlags.as<int>(), st);
+            }), "relabel");
+            return da_status_success;
+        }
+    }
+    B200_TRY(cuda->timed("kmeans_assign", [&] {
+        return launch_kmeans_assign<T>(dX.as<T>(), ld, n, d, dC, ld, k, dCn.as<T>(), dL, dLprev,
+                                       nullptr, dFlags.as<int>(), st);
+    }), "assign");
+    return da_status_success;
+}
+
 // One Lloyd pass (kmeans_lloyd.hpp:106-271): assignment against dCprev and,
 // if `update`, the new centres in dCnew plus the shift norms.
 template <typename T>
@@ -374,10 +442,10 @@ da_status KMeans<T>::lloyd_step(const T *dCprev, T *dCnew, int *dL, const int *d
     const int n = n_samples, k = n_clusters, d = n_features;
     B200_TRY(launch_centre_norms<T>(dCprev, ld, k, d, dCn.as<T>(), st), "centre norms");
     B200_TRY(cudaMemsetAsync(dFlags.p, 0, 8 * sizeof(int), st), "memset");
-    B200_TRY(cuda->timed("kmeans_assign", [&] {
-        return launch_kmeans_assign<T>(dX.as<T>(), ld, n, d, dCprev, ld, k, dCn.as<T>(), dL,
-                                       dLprev, nullptr, dFlags.as<int>(), st);
-    }), "assign");
+    {
+        da_status sa = assign(dCprev, dL, dLprev);
+        if (sa != da_status_success) return sa;
+    }
     if (update) {
         B200_TRY(cuda->timed("kmeans_sort", [&] {
             return launch_kmeans_sort(dL, n, k, dBlockCounts.as<int>(), dCounts.as<int>(),
@@ -399,7 +467,19 @@ da_status KMeans<T>::lloyd_step(const T *dCprev, T *dCnew, int *dL, const int *d
         B200_TRY(cudaMemcpyAsync(h_flags, dFlags.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st),
                  "copy");
     }
+    int tc_state[2] = {0, 0};
+    if (use_tc)
+        B200_TRY(cudaMemcpyAsync(tc_state, dTcScal.as<char>() + 16, 2 * sizeof(int),
+                                 cudaMemcpyDeviceToHost, st), "copy");
     B200_TRY(cudaStreamSynchronize(st), "Lloyd iteration");
+    (void)d;
+    if (use_tc) {
+        amb_last = tc_state[0];
+        if (tc_state[1] != 0)
+            return err->error(da_status_internal_error,
+                              "The tensor-core assignment kernel timed out waiting on a "
+                              "pipeline barrier (code " + std::to_string(tc_state[1]) + ").");
+    }
     return da_status_success;
 }
 
@@ -581,6 +661,8 @@ template <typename T> da_status KMeans<T>::compute() {
     if (s != da_status_success) return s;
     s = alloc_work();
     if (s != da_status_success) return s;
+    s = prepare_tc();
+    if (s != da_status_success) return s;
     if (init_method != INIT_SUPPLIED) {
         if (seed == -1) {
             std::random_device r;
@@ -627,7 +709,8 @@ template <typename T> da_status KMeans<T>::compute() {
                               "cluster centers is needed.");
     model_trained = true;
     if (warn_maxit) return err->warn(da_status_maxit, "The maximum number of iterations was reached.");
-    if (warn_status != da_status_success) return err->warn(warn_status, warn_msg);
+    // kmeans.cpp:413-420 only records this warning; compute() still succeeds
+    if (warn_status != da_status_success) err->warn(warn_status, warn_msg);
     return da_status_success;
 }
 

@@ -36,6 +36,11 @@ METRIC = "k-means Lloyd iterations/s (fp32, 1M x 64, k=256)"
 UNIT = "iters/s"
 
 
+def set_rows(rows):
+    global N
+    N = rows
+
+
 def _load(name, path):
     spec = importlib.util.spec_from_file_location(name, path)
     mod = importlib.util.module_from_spec(spec)
@@ -44,7 +49,8 @@ def _load(name, path):
     return mod
 
 
-def make_data(n=N, d=D, k=K, seed=SEED):
+def make_data(n=None, d=D, k=K, seed=SEED):
+    n = N if n is None else n
     rng = np.random.default_rng(seed)
     means = rng.uniform(-10.0, 10.0, (k, d))
     sig = rng.uniform(0.5, 2.0, k)
@@ -185,7 +191,7 @@ def run_reference(args):
 
 
 def config_dict(args):
-    return {"workload": "kmeans_lloyd_fp32_1Mx64_k256", "n_samples": N, "n_features": D,
+    return {"workload": f"kmeans_lloyd_fp32_{N}x64_k256", "n_samples": N, "n_features": D,
             "n_clusters": K, "init": "k-means++ seed 1 (computed once, supplied to every step)",
             "max_iter": MAX_ITER, "tol": TOL, "precision_path": "plain fp32 (SIMT)",
             "step": "one da_kmeans_compute_s = rinfo[3] Lloyd iterations",
@@ -199,8 +205,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--rows", type=int, default=N,
+                    help="rows of X (default 1,000,000; smaller only for profiling captures)")
     args = ap.parse_args()
+    set_rows(args.rows)
     if args.impl == "reference":
         return run_reference(args)
 
@@ -271,6 +281,21 @@ def main():
     simt_peak = 148 * 128 * 2 * 1.965e9 / 1e12
 
     # e2e: host (pinned) -> device every step, labels + centres back
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(ab, km, X, C0, stream, args, world)
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cb = cpu_baseline(X, C0, int(os.environ.get("BENCH_CPU_SAMPLE", "131072")), 2)
+    emit(args, rank, world, value, ms, n_iter, init_ms, kt, a_avg, achieved_tflops, bf16,
+         peak_src, flops, simt_peak, cb, e2e, clocks)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_e2e(ab, km, X, C0, stream, args, world):
+    import torch
     Xp = torch.empty((N, D), dtype=torch.float32, pin_memory=True).numpy()
     Xp[:] = X
     km2 = ab.KMeans(K, "s", order=ab.ROW_MAJOR, max_iter=MAX_ITER, n_init=1, seed=SEED)
@@ -302,11 +327,12 @@ def main():
     torch.cuda.synchronize()
     e2e_ms = f0.elapsed_time(f1)
     e2e_value = e2e_iters * world / (e2e_ms / 1e3)
+    return {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N * D * 4 + K * D * 4,
+            "d2h_bytes_per_step": N * 4 + K * D * 4 + 6 * 4}
 
-    cb = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        cb = cpu_baseline(X, C0, int(os.environ.get("BENCH_CPU_SAMPLE", "131072")), 2)
 
+def emit(args, rank, world, value, ms, n_iter, init_ms, kt, a_avg, achieved_tflops, bf16,
+         peak_src, flops, simt_peak, cb, e2e, clocks):
     launches_per_step = 9 * n_iter + 4
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -321,16 +347,12 @@ def main():
             "frac_of_simt_nominal": achieved_tflops / simt_peak,
             "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in kt.items()}},
         "cpu_baseline": cb,
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N * D * 4 + K * D * 4,
-                "d2h_bytes_per_step": N * 4 + K * D * 4 + 6 * 4},
+        "e2e": e2e,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
     }
     if rank == 0:
         print(json.dumps(out))
-    if world > 1:
-        torch.distributed.destroy_process_group()
-    return 0
 
 
 if __name__ == "__main__":

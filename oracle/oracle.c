@@ -279,6 +279,7 @@ void orc_kmeans_assign_s(int n, int d, const float *X, int k, const float *C, in
         for (int j = 0; j < k; ++j) {
             float v = fmaf(-2.0f, dot_s(x, C + (size_t)j * d, d), cn[j]);
             if (v < best) { best = v; bj = j; }
+            if (!gap64) continue;
             double e = 0;
             for (int f = 0; f < d; ++f) { double t = (double)x[f] - (double)C[(size_t)j * d + f]; e += t * t; }
             if (e < b1) { b2 = b1; b1 = e; } else if (e < b2) b2 = e;
@@ -300,6 +301,7 @@ void orc_kmeans_assign_d(int n, int d, const double *X, int k, const double *C, 
         for (int j = 0; j < k; ++j) {
             double v = fma(-2.0, dot_d(x, C + (size_t)j * d, d), cn[j]);
             if (v < best) { best = v; bj = j; }
+            if (!gap64) continue;
             double e = 0;
             for (int f = 0; f < d; ++f) { double t = x[f] - C[(size_t)j * d + f]; e += t * t; }
             if (e < b1) { b2 = b1; b1 = e; } else if (e < b2) b2 = e;
