@@ -96,6 +96,7 @@ def load(path=LIB_PATH):
         "da_b200_set_kernel_timing": (_P, da_int),
         "da_b200_get_kernel_time": (_P, C.c_char_p, C.POINTER(C.c_double), C.POINTER(da_int)),
         "da_b200_reset_kernel_time": (_P,),
+        "da_b200_get_stat": (_P, C.c_char_p, C.POINTER(C.c_double)),
         "da_b200_kmeans_init_centres_d": (_P, _P, da_int),
         "da_b200_kmeans_init_centres_s": (_P, _P, da_int),
     })
@@ -157,6 +158,11 @@ class Handle:
         n = da_int()
         self.L.da_b200_get_kernel_time(self.h, name.encode(), C.byref(ms), C.byref(n))
         return ms.value, n.value
+
+    def stat(self, name):
+        v = C.c_double()
+        self.L.da_b200_get_stat(self.h, name.encode(), C.byref(v))
+        return v.value
 
     def message(self):
         p = C.c_void_p()

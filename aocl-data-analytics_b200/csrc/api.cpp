@@ -525,6 +525,13 @@ da_status da_b200_get_kernel_time(da_handle h, const char *kernel, double *total
     *launches = (da_int)it->second.second;
     return da_status_success;
 }
+da_status da_b200_get_stat(da_handle h, const char *name, double *value) {
+    if (!h) return da_status_handle_not_initialized;
+    if (!name || !value) return da_status_invalid_pointer;
+    auto it = h->cuda.stats.find(name);
+    *value = it == h->cuda.stats.end() ? 0.0 : it->second;
+    return da_status_success;
+}
 da_status da_b200_reset_kernel_time(da_handle h) {
     if (!h) return da_status_handle_not_initialized;
     h->cuda.ktime.clear();

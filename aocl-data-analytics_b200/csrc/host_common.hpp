@@ -288,6 +288,7 @@ struct CudaCtx {
     bool timing = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::map<std::string, std::pair<double, long>> ktime; // name -> (ms total, launches)
+    std::map<std::string, double> stats;                  // named counters of the last call
 
     // Lazily bind to the current CUDA device.  Host-only calls (options,
     // argument checks) never need a device; the first call that touches data

@@ -475,6 +475,7 @@ da_status KMeans<T>::lloyd_step(const T *dCprev, T *dCnew, int *dL, const int *d
     (void)d;
     if (use_tc) {
         amb_last = tc_state[0];
+        cuda->stats["relabelled_rows"] = (double)amb_last;
         if (tc_state[1] != 0)
             return err->error(da_status_internal_error,
                               "The tensor-core assignment kernel timed out waiting on a "
@@ -663,6 +664,7 @@ template <typename T> da_status KMeans<T>::compute() {
     if (s != da_status_success) return s;
     s = prepare_tc();
     if (s != da_status_success) return s;
+    cuda->stats["tensor_core"] = use_tc ? 1.0 : 0.0;
     if (init_method != INIT_SUPPLIED) {
         if (seed == -1) {
             std::random_device r;

@@ -193,7 +193,7 @@ def run_reference(args):
 def config_dict(args):
     return {"workload": f"kmeans_lloyd_fp32_{N}x64_k256", "n_samples": N, "n_features": D,
             "n_clusters": K, "init": "k-means++ seed 1 (computed once, supplied to every step)",
-            "max_iter": MAX_ITER, "tol": TOL, "precision_path": "plain fp32 (SIMT)",
+            "max_iter": MAX_ITER, "tol": TOL,
             "step": "one da_kmeans_compute_s = rinfo[3] Lloyd iterations",
             "l2": "inputs (256 MB) larger than the 126 MB L2",
             "parallelism": f"replicas x{args.gpus}"}
@@ -202,11 +202,12 @@ def config_dict(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain fp32 comparison")
     ap.add_argument("--rows", type=int, default=N,
                     help="rows of X (default 1,000,000; smaller only for profiling captures)")
     args = ap.parse_args()
@@ -225,60 +226,113 @@ def main():
 
     X = make_data()
     stream = torch.cuda.current_stream()
-    km = ab.KMeans(K, "s", order=ab.ROW_MAJOR, max_iter=MAX_ITER, n_init=1, seed=SEED)
-    km.L.da_b200_set_stream(km.h, C.c_void_p(stream.cuda_stream))
-    km.set("convergence tolerance", TOL)
-    km.set_data(X)
+
+    def handle(mode):
+        km = ab.KMeans(K, "s", order=ab.ROW_MAJOR, max_iter=MAX_ITER, n_init=1, seed=SEED)
+        km.L.da_b200_set_stream(km.h, C.c_void_p(stream.cuda_stream))
+        km.set("convergence tolerance", TOL)
+        km.set("precision mode", mode)
+        km.set_data(X)
+        return km
+
+    km = handle("bf16")
     t0 = time.perf_counter()
     C0 = km.init_centres(K)
     init_ms = (time.perf_counter() - t0) * 1e3
-    km.set("initialization method", "supplied")
-    km.call("da_kmeans_set_init_centres_s", ab.ptr(C0), D)
 
-    def step():
-        km.call("da_kmeans_compute_s", ok=(0, 21))
-        return int(km.rinfo()[3])
+    def prepare(h):
+        h.set("initialization method", "supplied")
+        h.call("da_kmeans_set_init_centres_s", ab.ptr(C0), D)
 
-    for _ in range(args.warmup):
-        step()
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    clk = Clocks(local)
-    clk.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    iters = 0
-    for _ in range(args.steps):
-        iters += step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    clocks = clk.stop()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-        it = torch.tensor([iters], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(it)
-        iters_total = float(it.item())
-    else:
-        iters_total = iters
+    def step(h):
+        h.call("da_kmeans_compute_s", ok=(0, 21))
+        return int(h.rinfo()[3])
+
+    def timed(h, steps, warmup, sample_clocks=False):
+        for _ in range(warmup):
+            step(h)
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        clk = Clocks(local) if sample_clocks else None
+        if clk:
+            clk.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        iters = 0
+        for _ in range(steps):
+            iters += step(h)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clocks = clk.stop() if clk else None
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+            it = torch.tensor([iters], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(it)
+            iters_total = float(it.item())
+        else:
+            iters_total = iters
+        return ms, iters, iters_total, clocks
+
+    def kernel_times(h):
+        # separate pass: event timing serialises the launches
+        h.L.da_b200_set_kernel_timing(h.h, 1)
+        h.L.da_b200_reset_kernel_time(h.h)
+        step(h)
+        h.L.da_b200_set_kernel_timing(h.h, 0)
+        return {n: h.kernel_time(n) for n in
+                ("kmeans_assign", "kmeans_fixup", "kmeans_sort", "kmeans_update")}
+
+    prepare(km)
+    ms, iters, iters_total, clocks = timed(km, args.steps, args.warmup, sample_clocks=True)
     value = iters_total / (ms / 1e3)
     n_iter = iters // args.steps
+    relabelled = km.stat("relabelled_rows")
+    tensor_core = km.stat("tensor_core") == 1.0
+    kt = kernel_times(km)
 
-    # per-kernel device time (separate pass: timing serialises launches)
-    km.L.da_b200_set_kernel_timing(km.h, 1)
-    km.L.da_b200_reset_kernel_time(km.h)
-    step()
-    km.L.da_b200_set_kernel_timing(km.h, 0)
-    kt = {n: km.kernel_time(n) for n in ("kmeans_assign", "kmeans_sort", "kmeans_update")}
+    plain = None
+    if not args.no_plain:
+        kp = handle("plain")
+        prepare(kp)
+        psteps = max(2, args.steps // 10)
+        pms, piters, piters_total, _ = timed(kp, psteps, 1)
+        pkt = kernel_times(kp)
+        pa = pkt["kmeans_assign"]
+        plain = {"value": piters_total / (pms / 1e3), "unit": UNIT, "steps": psteps,
+                 "ms_per_step": pms / psteps,
+                 "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in pkt.items() if v[1]},
+                 "assign_tflops": 2.0 * N * K * D / (pa[0] / max(pa[1], 1) / 1e3) / 1e12}
+        kp.close()
+
     a_ms, a_n = kt["kmeans_assign"]
     a_avg = a_ms / max(a_n, 1)
     hbm, bf16, peak_src = load_peaks()
     flops = 2.0 * N * K * D
+    ldbf = 64 * ((D + 63) // 64)
+    traffic_alg = N * ldbf * 2 + N * 4 * 3  # bf16 X + labels, previous labels, |x|
     achieved_tflops = flops / (a_avg / 1e3) / 1e12
-    simt_peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    achieved_gbs = traffic_alg / (a_avg / 1e3) / 1e9
+    t_tensor = flops / (bf16 * 1e12)
+    t_hbm = traffic_alg / (hbm * 1e9)
+    if t_hbm >= t_tensor:
+        roof = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
+                "frac": achieved_gbs / hbm}
+    else:
+        roof = {"bound": "tensor", "achieved": achieved_tflops, "peak": bf16, "unit": "TFLOP/s",
+                "frac": achieved_tflops / bf16}
+    roof.update({"traffic": None, "peak_source": peak_src,
+                 "kernel": "kmeans_assign_tc_kernel (tcgen05 bf16, TMEM fp32)" if tensor_core
+                 else "kmeans_assign_kernel (SIMT fp32)",
+                 "algorithmic_flops_per_launch": flops,
+                 "algorithmic_bytes_per_launch": traffic_alg,
+                 "avg_launch_ms": a_avg, "tensor_tflops": achieved_tflops,
+                 "tensor_frac": achieved_tflops / bf16, "hbm_gbs": achieved_gbs,
+                 "hbm_frac": achieved_gbs / hbm,
+                 "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in kt.items() if v[1]}})
 
     # e2e: host (pinned) -> device every step, labels + centres back
     e2e = None
@@ -287,8 +341,25 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline(X, C0, int(os.environ.get("BENCH_CPU_SAMPLE", "131072")), 2)
-    emit(args, rank, world, value, ms, n_iter, init_ms, kt, a_avg, achieved_tflops, bf16,
-         peak_src, flops, simt_peak, cb, e2e, clocks)
+    extra = {"iterations_per_step": n_iter, "init_ms": init_ms,
+             "relabelled_rows_last_iteration": relabelled,
+             "precision_path": "bf16 tcgen05 candidate pass + exact fp32 relabel" if tensor_core
+             else "plain fp32 (SIMT)"}
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_dict(args) | extra,
+        "roofline": roof,
+        "cpu_baseline": cb,
+        "e2e": e2e,
+        "gpu_launches": (12 * n_iter + 6) * args.steps,
+        "clocks": clocks,
+        "plain_fp32": plain,
+        "speedup_vs_plain_fp32": (value / plain["value"]) if plain else None,
+    }
+    if rank == 0:
+        print(json.dumps(out))
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
@@ -302,6 +373,7 @@ def run_e2e(ab, km, X, C0, stream, args, world):
     km2.L.da_b200_set_stream(km2.h, C.c_void_p(stream.cuda_stream))
     km2.set("convergence tolerance", TOL)
     km2.set("initialization method", "supplied")
+    km2.set("precision mode", "bf16")
     lab_host = torch.empty(N, dtype=torch.int32, pin_memory=True).numpy()
     cen_host = np.zeros(K * D, dtype=np.float32)
 
@@ -329,30 +401,6 @@ def run_e2e(ab, km, X, C0, stream, args, world):
     e2e_value = e2e_iters * world / (e2e_ms / 1e3)
     return {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N * D * 4 + K * D * 4,
             "d2h_bytes_per_step": N * 4 + K * D * 4 + 6 * 4}
-
-
-def emit(args, rank, world, value, ms, n_iter, init_ms, kt, a_avg, achieved_tflops, bf16,
-         peak_src, flops, simt_peak, cb, e2e, clocks):
-    launches_per_step = 9 * n_iter + 4
-    out = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": config_dict(args) | {"iterations_per_step": n_iter, "init_ms": init_ms},
-        "roofline": {
-            "bound": "tensor", "achieved": achieved_tflops, "peak": bf16, "unit": "TFLOP/s",
-            "frac": achieved_tflops / bf16, "traffic": None, "peak_source": peak_src,
-            "kernel": "kmeans_assign_kernel (SIMT fp32)", "algorithmic_flops_per_launch": flops,
-            "avg_launch_ms": a_avg, "simt_fp32_nominal_tflops": simt_peak,
-            "frac_of_simt_nominal": achieved_tflops / simt_peak,
-            "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in kt.items()}},
-        "cpu_baseline": cb,
-        "e2e": e2e,
-        "gpu_launches": launches_per_step * args.steps,
-        "clocks": clocks,
-    }
-    if rank == 0:
-        print(json.dumps(out))
 
 
 if __name__ == "__main__":

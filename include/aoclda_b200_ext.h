@@ -29,6 +29,11 @@ da_status da_b200_get_kernel_time(da_handle handle, const char *kernel, double *
                                   da_int *launches);
 da_status da_b200_reset_kernel_time(da_handle handle);
 
+/* Named statistics of the last call: "relabelled_rows" (k-means rows of the
+ * last tensor-core assignment whose label needed the exact fp32 re-score),
+ * "tensor_core" (1 when the last k-means compute used the tensor cores). */
+da_status da_b200_get_stat(da_handle handle, const char *name, double *value);
+
 /* k-means: run only the configured initialisation method ("initialization
  * method", "seed", "n_clusters") on the data set and write the n_clusters x
  * n_features initial centres to C (storage order of the handle, leading
