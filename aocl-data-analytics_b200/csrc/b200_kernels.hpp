@@ -167,16 +167,20 @@ cudaError_t launch_to_bf16(const float *X, int ld, int rows, int d, void *Y, int
 // out[i] = |x_i| (fp32); *maxv = max_i |x_i| when maxv != null.
 cudaError_t launch_row_norm_max(const float *X, int ld, int rows, int d, float *out, float *maxv,
                                 cudaStream_t s);
-// BF16 tensor-core candidate assignment: certified rows get their exact fp32
-// label, the others are appended to amb_rows (*amb_count must be 0 on entry).
+// BF16 tensor-core candidate assignment: rows with a single candidate within
+// the error bound get their exact fp32 label; the others are appended to
+// amb_rows with up to 4 candidate clusters each (amb_ncand = 0: list
+// overflowed).  *amb_count must be 0 on entry.
 cudaError_t launch_kmeans_assign_tc(const void *Xbf, int n, int ldbf, const void *Cbf, int k,
                                     const float *cnorm, const float *xnorm, const float *cmax,
                                     int *labels, const int *labels_prev, int *flags,
-                                    int *amb_rows, int *amb_count, int *err, cudaStream_t s);
+                                    int *amb_rows, int *amb_cand, int *amb_ncand, int *amb_count,
+                                    int *err, cudaStream_t s);
 // Exact fp32 labels of the rows listed by the tensor-core pass.
-cudaError_t launch_kmeans_fixup(const float *X, int ld, int d, const float *C, int k,
-                                const float *cnorm, const int *amb_rows, const int *amb_count,
-                                int max_rows, int *labels, const int *labels_prev, int *flags,
-                                cudaStream_t s);
+cudaError_t launch_kmeans_rescore(const float *X, int ld, int d, const float *C, int k,
+                                  const float *cnorm, const int *amb_rows, const int *amb_cand,
+                                  const int *amb_ncand, const int *amb_count, int max_rows,
+                                  int *labels, const int *labels_prev, int *flags,
+                                  cudaStream_t s);
 
 } // namespace b200

@@ -383,7 +383,7 @@ template <typename T> da_status KMeans<T>::prepare_tc() {
         ldbf = nkb * 64;
         if (!dXbf.ensure((size_t)n_samples * ldbf * 2) || !dXnrm.ensure((size_t)n_samples * 4) ||
             !dCbf.ensure((size_t)npad * ldbf * 2) || !dCtmp.ensure((size_t)npad * 4) ||
-            !dTcScal.ensure(64) || !dAmb.ensure((size_t)n_samples * 4))
+            !dTcScal.ensure(64) || !dAmb.ensure((size_t)n_samples * 4 * 6))
             return err->error(da_status_memory_error, "Device memory allocation failed.");
         cudaStream_t st = cuda->stream;
         if (fresh || dXbf_stale) {
@@ -410,18 +410,22 @@ template <typename T> da_status KMeans<T>::assign(const T *dC, int *dL, const in
             float *cmax = dTcScal.as<float>();
             int *amb_cnt = reinterpret_cast<int *>(dTcScal.as<char>() + 16);
             int *errf = reinterpret_cast<int *>(dTcScal.as<char>() + 20);
+            int *amb_rows = dAmb.as<int>();
+            int *amb_ncand = amb_rows + n;
+            int *amb_cand = amb_rows + 2 * (size_t)n;
             B200_TRY(launch_to_bf16(dC, ld, k, d, dCbf.p, ldbf, st), "bf16 centres");
             B200_TRY(launch_row_norm_max(dC, ld, k, d, dCtmp.as<float>(), cmax, st), "centre norms");
             B200_TRY(cudaMemsetAsync(amb_cnt, 0, sizeof(int), st), "memset");
             B200_TRY(cuda->timed("kmeans_assign", [&] {
                 return launch_kmeans_assign_tc(dXbf.p, n, ldbf, dCbf.p, k, dCn.as<float>(),
                                                dXnrm.as<float>(), cmax, dL, dLprev,
-                                               dFlags.as<int>(), dAmb.as<int>(), amb_cnt, errf, st);
+                                               dFlags.as<int>(), amb_rows, amb_cand, amb_ncand,
+                                               amb_cnt, errf, st);
             }), "tensor-core assign");
-            B200_TRY(cuda->timed("kmeans_fixup", [&] {
-                return launch_kmeans_fixup(dX.as<float>(), ld, d, dC, k, dCn.as<float>(),
-                                           dAmb.as<int>(), amb_cnt, n, dL, dLprev,
-                                           dFlags.as<int>(), st);
+            B200_TRY(cuda->timed("kmeans_rescore", [&] {
+                return launch_kmeans_rescore(dX.as<float>(), ld, d, dC, k, dCn.as<float>(),
+                                             amb_rows, amb_cand, amb_ncand, amb_cnt, n, dL,
+                                             dLprev, dFlags.as<int>(), st);
             }), "relabel");
             return da_status_success;
         }

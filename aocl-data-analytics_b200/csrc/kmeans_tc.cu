@@ -29,6 +29,7 @@ using namespace tc;
 static constexpr int TC_BM = 128;       // rows per tile (UMMA M)
 static constexpr int TC_KB = 64;        // bf16 elements per 128-byte K block
 static constexpr int TC_THREADS = 320;  // 10 warps
+static constexpr int TC_MAXC = 4;       // candidates kept per uncertified row
 
 struct TcAssignArgs {
     int n, k, npad, nkb, stages, bufcols;
@@ -39,12 +40,14 @@ struct TcAssignArgs {
     const int *labels_prev;
     int *flags;          // [0] labels changed
     int *amb_rows;       // rows to relabel exactly
+    int *amb_cand;       // TC_MAXC candidate clusters per listed row
+    int *amb_ncand;      // number of candidates (0: scan every cluster)
     int *amb_count;
     int *err;            // set on a timed-out wait
     float delta;
 };
 
-struct __align__(8) TcShared {
+struct __align__(16) TcShared {
     uint64_t full[8], empty[8], tfull[2], tempty[2], bfull;
     uint32_t tmem_base;
     int abort_flag;
@@ -69,7 +72,9 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
     unsigned char *Bs = base;
     unsigned char *As = Bs + (size_t)nkb * b_bytes;
     TcShared *sh = reinterpret_cast<TcShared *>(As + (size_t)S * nkb * a_bytes);
-    float *cn_s = reinterpret_cast<float *>(sh + 1);
+    float *cn_s = reinterpret_cast<float *>(sh + 1);      // npad32 entries, +inf pad
+    const int npad32 = (a.npad + 31) & ~31;
+    int *cand_s = reinterpret_cast<int *>(cn_s + npad32); // [TC_THREADS][TC_MAXC]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ntiles = (a.n + TC_BM - 1) / TC_BM;
@@ -88,7 +93,8 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
         sh->changed = 0;
         fence_barrier_init();
     }
-    for (int j = threadIdx.x; j < a.npad; j += blockDim.x) cn_s[j] = j < a.k ? a.cnorm[j] : 0.f;
+    for (int j = threadIdx.x; j < npad32; j += blockDim.x)
+        cn_s[j] = j < a.k ? a.cnorm[j] : __int_as_float(0x7f800000);
     if (warp == 1) {
         tmem_alloc(&sh->tmem_base, 2u * a.bufcols);
         tmem_relinquish();
@@ -183,42 +189,70 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
             }
             if (*((volatile int *)&sh->abort_flag)) break;
             tc_fence_after();
-            float b1 = __int_as_float(0x7f800000), b2 = b1;
-            int i1 = 0x7fffffff;
             const uint32_t trow = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * a.bufcols);
+            const int r = t * TC_BM + row_in_tile;
+            const float xn = r < a.n ? a.xnorm[r] : 0.f;
+            // pass 1: smallest v_j = |c_j|^2 - 2 s_j (tree minimum per 32 columns)
+            float b1 = __int_as_float(0x7f800000);
             for (int c = 0; c < nchunks; ++c) {
                 float v[32];
                 tmem_ld32(trow + (uint32_t)(c * 32), v);
+                const float4 *cn4 = reinterpret_cast<const float4 *>(cn_s + c * 32);
 #pragma unroll
-                for (int u = 0; u < 32; ++u) {
-                    const int j = c * 32 + u;
-                    const float val = __fmaf_rn(-2.f, v[u], cn_s[j < a.npad ? j : 0]);
-                    if (j < a.k) {
-                        if (val < b1) {
-                            b2 = b1;
-                            b1 = val;
-                            i1 = j;
-                        } else {
-                            b2 = fminf(b2, val);
+                for (int u = 0; u < 8; ++u) {
+                    const float4 cc = cn4[u];
+                    v[4 * u + 0] = __fmaf_rn(-2.f, v[4 * u + 0], cc.x);
+                    v[4 * u + 1] = __fmaf_rn(-2.f, v[4 * u + 1], cc.y);
+                    v[4 * u + 2] = __fmaf_rn(-2.f, v[4 * u + 2], cc.z);
+                    v[4 * u + 3] = __fmaf_rn(-2.f, v[4 * u + 3], cc.w);
+                }
+#pragma unroll
+                for (int w = 16; w >= 1; w >>= 1)
+#pragma unroll
+                    for (int u = 0; u < w; ++u) v[u] = fminf(v[u], v[u + w]);
+                b1 = fminf(b1, v[0]);
+            }
+            // pass 2: every cluster within 2 eps of the minimum is a candidate
+            const float eps = 1.01f * (2.f * a.delta * xn * cmax +
+                                       1.1920929e-7f * (cmax * cmax + 2.f * xn * cmax));
+            const float tau = b1 + 2.f * eps;
+            int cnt = 0;
+            int *my = cand_s + threadIdx.x * TC_MAXC;
+            for (int c = 0; c < nchunks; ++c) {
+                float v[32];
+                tmem_ld32(trow + (uint32_t)(c * 32), v);
+                const float4 *cn4 = reinterpret_cast<const float4 *>(cn_s + c * 32);
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const float4 cc = cn4[u];
+                    const float w4[4] = {__fmaf_rn(-2.f, v[4 * u + 0], cc.x),
+                                         __fmaf_rn(-2.f, v[4 * u + 1], cc.y),
+                                         __fmaf_rn(-2.f, v[4 * u + 2], cc.z),
+                                         __fmaf_rn(-2.f, v[4 * u + 3], cc.w)};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        if (w4[e] <= tau) {
+                            if (cnt < TC_MAXC) my[cnt] = c * 32 + 4 * u + e;
+                            ++cnt;
                         }
                     }
                 }
             }
             tc_fence_before();
             mbar_arrive(&sh->tempty[b]);
-            const int r = t * TC_BM + row_in_tile;
             if (r < a.n) {
-                const float xn = a.xnorm[r];
-                const float eps = 1.01f * (2.f * a.delta * xn * cmax +
-                                           1.1920929e-7f * (cmax * cmax + 2.f * xn * cmax));
-                // NaN values fail the comparison and are relabelled exactly
-                const bool certain = (i1 != 0x7fffffff) && (b2 - b1 > 2.f * eps);
-                if (certain) {
-                    a.labels[r] = i1;
-                    if (a.labels_prev && a.labels_prev[r] != i1) changed = 1;
+                if (cnt == 1) {
+                    // a single candidate: the fp32 label is certified
+                    const int lbl = my[0];
+                    a.labels[r] = lbl;
+                    if (a.labels_prev && a.labels_prev[r] != lbl) changed = 1;
                 } else {
+                    // near-tie (or NaN): exact fp32 re-score of the candidates
                     const int pos = atomicAdd(a.amb_count, 1);
                     a.amb_rows[pos] = r;
+                    const int nc = (cnt >= 2 && cnt <= TC_MAXC) ? cnt : 0;
+                    a.amb_ncand[pos] = nc;
+                    for (int e = 0; e < nc; ++e) a.amb_cand[pos * TC_MAXC + e] = my[e];
                 }
             }
         }
@@ -233,45 +267,40 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
     }
 }
 
-// Exact fp32 relabelling of the uncertified rows: one warp per row, lanes over
-// clusters, the plain path's formula fl(|c|^2 - 2 x.c) with the dot as one
-// fma chain over the features; ties -> lower index.
-__global__ void kmeans_fixup_kernel(const float *X, int ld, int d, const float *C, int k,
-                                    const float *cnorm, const int *amb_rows, const int *amb_count,
-                                    int *labels, const int *labels_prev, int *flags) {
-    const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
+// Exact fp32 relabelling of the uncertified rows: the plain path's formula
+// fl(|c|^2 - 2 x.c) with the dot product as one fma chain over the features,
+// evaluated for the listed candidates (every cluster when the list
+// overflowed); ties -> lower index.  One thread per listed row.
+__global__ void kmeans_rescore_kernel(const float *X, int ld, int d, const float *C, int k,
+                                      const float *cnorm, const int *amb_rows,
+                                      const int *amb_cand, const int *amb_ncand,
+                                      const int *amb_count, int *labels, const int *labels_prev,
+                                      int *flags) {
     const int cnt = *amb_count;
-    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < cnt; w += nw) {
-    const int r = amb_rows[w];
-    const float *x = X + (size_t)r * ld;
-    float best = __int_as_float(0x7f800000);
-    int bi = 0x7fffffff;
-    for (int j = lane; j < k; j += 32) {
-        const float *c = C + (size_t)j * ld;
-        float s = 0.f;
-        for (int f = 0; f < d; ++f) s = __fmaf_rn(x[f], c[f], s);
-        const float v = __fmaf_rn(-2.f, s, cnorm[j]);
-        if (key_less(v, j, best, bi)) {
-            best = v;
-            bi = j;
+    int changed = 0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += gridDim.x * blockDim.x) {
+        const int r = amb_rows[e];
+        const float *x = X + (size_t)r * ld;
+        const int nc = amb_ncand[e];
+        float best = __int_as_float(0x7f800000);
+        int bi = 0x7fffffff;
+        const int m = nc > 0 ? nc : k;
+        for (int u = 0; u < m; ++u) {
+            const int j = nc > 0 ? amb_cand[e * TC_MAXC + u] : u;
+            const float *c = C + (size_t)j * ld;
+            float sdot = 0.f;
+            for (int f = 0; f < d; ++f) sdot = __fmaf_rn(x[f], c[f], sdot);
+            const float v = __fmaf_rn(-2.f, sdot, cnorm[j]);
+            if (key_less(v, j, best, bi)) {
+                best = v;
+                bi = j;
+            }
         }
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        const float ov = __shfl_xor_sync(0xffffffffu, best, off);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-        if (key_less(ov, oi, best, bi)) {
-            best = ov;
-            bi = oi;
-        }
-    }
-    if (lane == 0) {
         const int lbl = (bi == 0x7fffffff) ? 0 : bi;
         labels[r] = lbl;
-        if (labels_prev && labels_prev[r] != lbl && flags) atomicOr(&flags[0], 1);
+        if (labels_prev && labels_prev[r] != lbl) changed = 1;
     }
-    }
+    if (changed && flags) atomicOr(&flags[0], 1);
 }
 
 // fp32 (row-major, ld) -> bf16 (row-major, ldo = nkb*64), zero padded.
@@ -364,7 +393,8 @@ cudaError_t launch_row_norm_max(const float *X, int ld, int rows, int d, float *
 cudaError_t launch_kmeans_assign_tc(const void *Xbf, int n, int ldbf, const void *Cbf, int k,
                                     const float *cnorm, const float *xnorm, const float *cmax,
                                     int *labels, const int *labels_prev, int *flags,
-                                    int *amb_rows, int *amb_count, int *err, cudaStream_t s) {
+                                    int *amb_rows, int *amb_cand, int *amb_ncand, int *amb_count,
+                                    int *err, cudaStream_t s) {
     const int nkb = ldbf / TC_KB;
     const int npad = (k + 15) & ~15;
     CUtensorMap mx, mc;
@@ -374,7 +404,8 @@ cudaError_t launch_kmeans_assign_tc(const void *Xbf, int n, int ldbf, const void
     const size_t a_stage = (size_t)nkb * TC_BM * 128;
     int stages = (int)((150 * 1024 - b_bytes) / a_stage);
     stages = stages < 2 ? 2 : (stages > 6 ? 6 : stages);
-    const size_t smem = 1024 + b_bytes + stages * a_stage + sizeof(TcShared) + npad * 4 + 64;
+    const size_t smem = 1024 + b_bytes + stages * a_stage + sizeof(TcShared) +
+                        (size_t)((npad + 31) & ~31) * 4 + TC_THREADS * TC_MAXC * 4 + 64;
     int bufcols = 32;
     while (bufcols < npad) bufcols <<= 1;
     TcAssignArgs a;
@@ -391,6 +422,8 @@ cudaError_t launch_kmeans_assign_tc(const void *Xbf, int n, int ldbf, const void
     a.labels_prev = labels_prev;
     a.flags = flags;
     a.amb_rows = amb_rows;
+    a.amb_cand = amb_cand;
+    a.amb_ncand = amb_ncand;
     a.amb_count = amb_count;
     a.err = err;
     a.delta = 0.0078125f * (1.f + 0.0078125f) + (float)(nkb * TC_KB) * 4.76837158e-7f;
@@ -405,15 +438,22 @@ cudaError_t launch_kmeans_assign_tc(const void *Xbf, int n, int ldbf, const void
     return cudaGetLastError();
 }
 
-cudaError_t launch_kmeans_fixup(const float *X, int ld, int d, const float *C, int k,
-                                const float *cnorm, const int *amb_rows, const int *amb_count,
-                                int max_rows, int *labels, const int *labels_prev, int *flags,
-                                cudaStream_t s) {
+cudaError_t launch_kmeans_rescore(const float *X, int ld, int d, const float *C, int k,
+                                  const float *cnorm, const int *amb_rows, const int *amb_cand,
+                                  const int *amb_ncand, const int *amb_count, int max_rows,
+                                  int *labels, const int *labels_prev, int *flags,
+                                  cudaStream_t s) {
     if (max_rows <= 0) return cudaSuccess;
-    const long warps = max_rows < 148 * 64 ? max_rows : 148 * 64;
-    kmeans_fixup_kernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(
-        X, ld, d, C, k, cnorm, amb_rows, amb_count, labels, labels_prev, flags);
+    const int threads = max_rows < 148 * 1024 ? max_rows : 148 * 1024;
+    kmeans_rescore_kernel<<<(threads + 255) / 256, 256, 0, s>>>(
+        X, ld, d, C, k, cnorm, amb_rows, amb_cand, amb_ncand, amb_count, labels, labels_prev,
+        flags);
     return cudaGetLastError();
 }
 
+} // namespace b200
+
+namespace b200 {
+// The epilogue reads |c_j|^2 as float4 right after the barrier block.
+static_assert(sizeof(TcShared) % 16 == 0, "TcShared must keep the cnorm array 16-byte aligned");
 } // namespace b200

@@ -284,7 +284,7 @@ def main():
         step(h)
         h.L.da_b200_set_kernel_timing(h.h, 0)
         return {n: h.kernel_time(n) for n in
-                ("kmeans_assign", "kmeans_fixup", "kmeans_sort", "kmeans_update")}
+                ("kmeans_assign", "kmeans_rescore", "kmeans_sort", "kmeans_update")}
 
     prepare(km)
     ms, iters, iters_total, clocks = timed(km, args.steps, args.warmup, sample_clocks=True)
