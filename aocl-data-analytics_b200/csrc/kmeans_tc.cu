@@ -231,8 +231,9 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
                                          __fmaf_rn(-2.f, v[4 * u + 3], cc.w)};
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
-                        if (w4[e] <= tau) {
-                            if (cnt < TC_MAXC) my[cnt] = c * 32 + 4 * u + e;
+                        const int j = c * 32 + 4 * u + e;
+                        if (w4[e] <= tau && j < a.k) { // padded columns are never candidates
+                            if (cnt < TC_MAXC) my[cnt] = j;
                             ++cnt;
                         }
                     }
@@ -240,15 +241,23 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
             }
             tc_fence_before();
             mbar_arrive(&sh->tempty[b]);
-            if (r < a.n) {
-                if (cnt == 1) {
-                    // a single candidate: the fp32 label is certified
-                    const int lbl = my[0];
-                    a.labels[r] = lbl;
-                    if (a.labels_prev && a.labels_prev[r] != lbl) changed = 1;
-                } else {
-                    // near-tie (or NaN): exact fp32 re-score of the candidates
-                    const int pos = atomicAdd(a.amb_count, 1);
+            const bool valid = r < a.n;
+            if (valid && cnt == 1) {
+                // a single candidate: the fp32 label is certified
+                const int lbl = my[0];
+                a.labels[r] = lbl;
+                if (a.labels_prev && a.labels_prev[r] != lbl) changed = 1;
+            }
+            // near-ties (or NaN): appended, one atomic per warp, for the exact
+            // fp32 re-score of their candidates
+            const bool amb = valid && cnt != 1;
+            const unsigned mask = __ballot_sync(0xffffffffu, amb);
+            if (mask) {
+                int base0 = 0;
+                if (lane == 0) base0 = atomicAdd(a.amb_count, __popc(mask));
+                base0 = __shfl_sync(0xffffffffu, base0, 0);
+                if (amb) {
+                    const int pos = base0 + __popc(mask & ((1u << lane) - 1u));
                     a.amb_rows[pos] = r;
                     const int nc = (cnt >= 2 && cnt <= TC_MAXC) ? cnt : 0;
                     a.amb_ncand[pos] = nc;
@@ -270,35 +279,68 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
 // Exact fp32 relabelling of the uncertified rows: the plain path's formula
 // fl(|c|^2 - 2 x.c) with the dot product as one fma chain over the features,
 // evaluated for the listed candidates (every cluster when the list
-// overflowed); ties -> lower index.  One thread per listed row.
-__global__ void kmeans_rescore_kernel(const float *X, int ld, int d, const float *C, int k,
-                                      const float *cnorm, const int *amb_rows,
-                                      const int *amb_cand, const int *amb_ncand,
-                                      const int *amb_count, int *labels, const int *labels_prev,
-                                      int *flags) {
+// overflowed); ties -> lower index.  Each warp stages the centres and 32
+// listed rows in shared memory (coalesced loads, rows padded to d+1 floats so
+// the per-lane sequential dot products are bank-conflict free); one lane per
+// listed row.
+__global__ void __launch_bounds__(256)
+kmeans_rescore_kernel(const float *X, int ld, int d, const float *C, int k,
+                      const float *cnorm, const int *amb_rows, const int *amb_cand,
+                      const int *amb_ncand, const int *amb_count, int *labels,
+                      const int *labels_prev, int *flags, int c_in_smem) {
+    extern __shared__ float rs_smem[];
+    const int dp = d + 1;
+    float *cs = rs_smem;                                            // k x dp (optional)
+    float *xs = rs_smem + (c_in_smem ? (size_t)k * dp : 0) + (threadIdx.x >> 5) * 32 * dp;
+    const int lane = threadIdx.x & 31;
     const int cnt = *amb_count;
-    int changed = 0;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += gridDim.x * blockDim.x) {
-        const int r = amb_rows[e];
-        const float *x = X + (size_t)r * ld;
-        const int nc = amb_ncand[e];
-        float best = __int_as_float(0x7f800000);
-        int bi = 0x7fffffff;
-        const int m = nc > 0 ? nc : k;
-        for (int u = 0; u < m; ++u) {
-            const int j = nc > 0 ? amb_cand[e * TC_MAXC + u] : u;
-            const float *c = C + (size_t)j * ld;
-            float sdot = 0.f;
-            for (int f = 0; f < d; ++f) sdot = __fmaf_rn(x[f], c[f], sdot);
-            const float v = __fmaf_rn(-2.f, sdot, cnorm[j]);
-            if (key_less(v, j, best, bi)) {
-                best = v;
-                bi = j;
-            }
+    if (c_in_smem) {
+        for (int e = threadIdx.x; e < k * d; e += blockDim.x) {
+            const int j = e / d, f = e % d;
+            cs[j * dp + f] = C[(size_t)j * ld + f];
         }
-        const int lbl = (bi == 0x7fffffff) ? 0 : bi;
-        labels[r] = lbl;
-        if (labels_prev && labels_prev[r] != lbl) changed = 1;
+        __syncthreads();
+    }
+    int changed = 0;
+    const int warps_total = (gridDim.x * blockDim.x) >> 5;
+    for (int e0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; e0 < cnt;
+         e0 += warps_total * 32) {
+        const int ne = min(32, cnt - e0);
+        // coalesced staging of the (up to) 32 listed rows
+        for (int i = 0; i < ne; ++i) {
+            const float *x = X + (size_t)amb_rows[e0 + i] * ld;
+            for (int f = lane; f < d; f += 32) xs[i * dp + f] = x[f];
+        }
+        __syncwarp();
+        if (lane < ne) {
+            const int e = e0 + lane;
+            const int r = amb_rows[e];
+            const float *x = xs + lane * dp;
+            const int nc = amb_ncand[e];
+            float best = __int_as_float(0x7f800000);
+            int bi = 0x7fffffff;
+            const int m = nc > 0 ? nc : k;
+            for (int u = 0; u < m; ++u) {
+                const int j = nc > 0 ? amb_cand[e * TC_MAXC + u] : u;
+                float sdot = 0.f;
+                if (c_in_smem) {
+                    const float *c = cs + j * dp;
+                    for (int f = 0; f < d; ++f) sdot = __fmaf_rn(x[f], c[f], sdot);
+                } else {
+                    const float *c = C + (size_t)j * ld;
+                    for (int f = 0; f < d; ++f) sdot = __fmaf_rn(x[f], c[f], sdot);
+                }
+                const float v = __fmaf_rn(-2.f, sdot, cnorm[j]);
+                if (key_less(v, j, best, bi)) {
+                    best = v;
+                    bi = j;
+                }
+            }
+            const int lbl = (bi == 0x7fffffff) ? 0 : bi;
+            labels[r] = lbl;
+            if (labels_prev && labels_prev[r] != lbl) changed = 1;
+        }
+        __syncwarp();
     }
     if (changed && flags) atomicOr(&flags[0], 1);
 }
@@ -444,10 +486,18 @@ cudaError_t launch_kmeans_rescore(const float *X, int ld, int d, const float *C,
                                   int *labels, const int *labels_prev, int *flags,
                                   cudaStream_t s) {
     if (max_rows <= 0) return cudaSuccess;
-    const int threads = max_rows < 148 * 1024 ? max_rows : 148 * 1024;
-    kmeans_rescore_kernel<<<(threads + 255) / 256, 256, 0, s>>>(
-        X, ld, d, C, k, cnorm, amb_rows, amb_cand, amb_ncand, amb_count, labels, labels_prev,
-        flags);
+    const size_t xs_bytes = (size_t)8 * 32 * (d + 1) * 4;
+    const size_t cs_bytes = (size_t)k * (d + 1) * 4;
+    const int c_in_smem = (cs_bytes + xs_bytes <= 200 * 1024) ? 1 : 0;
+    const size_t smem = xs_bytes + (c_in_smem ? cs_bytes : 0);
+    if (smem > 220 * 1024) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(kmeans_rescore_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int blocks = min(148 * 2, (max_rows + 255) / 256);
+    kmeans_rescore_kernel<<<blocks, 256, smem, s>>>(X, ld, d, C, k, cnorm, amb_rows, amb_cand,
+                                                    amb_ncand, amb_count, labels, labels_prev,
+                                                    flags, c_in_smem);
     return cudaGetLastError();
 }
 
