@@ -116,9 +116,11 @@ template <typename T> struct KMeans : public AlgBase {
     int ld = 0;
     DevBuf dX, dXn, dC0, dC1, dCn, dL0, dL1, dCounts, dBlockCounts, dOffsets, dSorted,
         dChunkSums, dSegStart, dScalars, dFlags, dPartials, dW, dKD, dCand, dStage, dY, dYL,
-        dBestL, dXbf, dXnrm, dCbf, dCtmp, dTcScal, dAmb;
+        dBestL, dXh, dXl, dXnrm, dBh, dBl, dBaug, dAaug, dCtmp, dTcScal, dAmb;
+    int tc_split = 0;     // bf16 terms of the resident X copies (0: none)
     bool use_tc = false; // bf16 tensor-core assignment active for this compute
     bool dXbf_stale = true;
+    bool aaug_ready = false;
     int ldbf = 0;
     da_int amb_last = 0;  // rows relabelled exactly in the last tensor-core pass
     T *h_pin = nullptr;

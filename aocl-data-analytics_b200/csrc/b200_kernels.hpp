@@ -159,23 +159,32 @@ template <typename T>
 cudaError_t launch_kpp_update(T *w, const T *Dc, int n, int chosen, cudaStream_t s);
 
 // ------------------------------------------------- tensor-core k-means ---
-// 1 when the tcgen05 assignment handles (k clusters, d features).
-int tc_assign_supported(int k, int d);
-// fp32 row-major (ld) -> bf16 row-major with ldo = 64 * ceil(d/64), zero pad.
-cudaError_t launch_to_bf16(const float *X, int ld, int rows, int d, void *Y, int ldo,
-                           cudaStream_t s);
+// 1 when the tcgen05 assignment handles (k clusters, d features) with the
+// given bf16 split (1 or 3 terms).
+int tc_assign_supported(int k, int d, int split);
+// X fp32 (ld) -> Xh = bf16(x), Xl = bf16(x - Xh) (Xl may be null), row-major
+// with ldo = 64 * ceil(d / 64), zero padded.
+cudaError_t launch_split_bf16(const float *X, int ld, int rows, int d, void *Xh, void *Xl,
+                              int ldo, cudaStream_t s);
+// Centre operands of the tensor-core pass: B = -2 C as bf16 hi (+ lo), the
+// |c|^2 hi/lo pair (Baug, npad x 64) and, when Aaug_once != null, the constant
+// ones operand (128 x 64).
+cudaError_t launch_prep_centres(const float *C, int ld, int k, int d, int ldo,
+                                const float *cnorm, void *Bh, void *Bl, void *Baug,
+                                void *Aaug_once, cudaStream_t s);
 // out[i] = |x_i| (fp32); *maxv = max_i |x_i| when maxv != null.
 cudaError_t launch_row_norm_max(const float *X, int ld, int rows, int d, float *out, float *maxv,
                                 cudaStream_t s);
-// BF16 tensor-core candidate assignment: rows with a single candidate within
-// the error bound get their exact fp32 label; the others are appended to
-// amb_rows with up to 4 candidate clusters each (amb_ncand = 0: list
-// overflowed).  *amb_count must be 0 on entry.
-cudaError_t launch_kmeans_assign_tc(const void *Xbf, int n, int ldbf, const void *Cbf, int k,
-                                    const float *cnorm, const float *xnorm, const float *cmax,
-                                    int *labels, const int *labels_prev, int *flags,
-                                    int *amb_rows, int *amb_cand, int *amb_ncand, int *amb_count,
-                                    int *err, cudaStream_t s);
+// Tensor-core candidate assignment: rows with a single candidate within the
+// error bound get their exact fp32 label; the others are appended to amb_rows
+// with up to 4 candidate clusters each (amb_ncand = 0: scan all).  *amb_count
+// must be 0 on entry.
+cudaError_t launch_kmeans_assign_tc(int split, const void *Xh, const void *Xl, int n, int ldbf,
+                                    const void *Bh, const void *Bl, const void *Baug,
+                                    const void *Aaug, int k, const float *xnorm,
+                                    const float *cmax, int *labels, const int *labels_prev,
+                                    int *flags, int *amb_rows, int *amb_cand, int *amb_ncand,
+                                    int *amb_count, int *err, cudaStream_t s);
 // Exact fp32 labels of the rows listed by the tensor-core pass.
 cudaError_t launch_kmeans_rescore(const float *X, int ld, int d, const float *C, int k,
                                   const float *cnorm, const int *amb_rows, const int *amb_cand,

@@ -42,10 +42,11 @@ KMeans<T>::KMeans(ErrorRecord *e, CudaCtx *c, bool single) {
     opts.add_string("distance", {{"euclidean", 0}, {"cosine", 1}}, "euclidean");
     opts.add_string("normalize data", {{"yes", 1}, {"no", 0}}, "yes");
     opts.add_real("convergence tolerance", 0.0, LB::greaterequal, 0.0, UB::p_inf, 1.0e-4);
-    // B200 option (no counterpart in the reference): "bf16" runs the
-    // assignment on the tensor cores with a certified candidate pass whose
-    // labels equal the "plain" fp32 path's; fp64 data always use "plain".
-    opts.add_string("precision mode", {{"plain", 0}, {"bf16", 1}}, "bf16");
+    // B200 option (no counterpart in the reference): "bf16" / "bf16x3" run the
+    // assignment on the tensor cores (one bf16 term, or the three-term hi/lo
+    // split) with a certified candidate pass whose labels equal the "plain"
+    // fp32 path's; fp64 data always use "plain".
+    opts.add_string("precision mode", {{"plain", 0}, {"bf16", 1}, {"bf16x3", 3}}, "bf16x3");
     opts.add_real("low precision convergence tolerance", 0.0, LB::greaterequal, 0.0, UB::p_inf,
                   1.0e-2);
 }
@@ -375,25 +376,30 @@ template <typename T> da_status KMeans<T>::init_centres(T *dC) {
 template <typename T> da_status KMeans<T>::prepare_tc() {
     use_tc = false;
     if constexpr (std::is_same_v<T, float>) {
-        if (opts.key("precision mode") != 1 || !tc_assign_supported(n_clusters, n_features))
+        const int split = (int)opts.key("precision mode");
+        if (split == 0 || !tc_assign_supported(n_clusters, n_features, split))
             return da_status_success;
         const int nkb = (n_features + 63) / 64;
         const int npad = (n_clusters + 15) & ~15;
-        const bool fresh = !dXbf.p || ldbf != nkb * 64;
+        const bool fresh = tc_split != split || ldbf != nkb * 64 || dXbf_stale;
         ldbf = nkb * 64;
-        if (!dXbf.ensure((size_t)n_samples * ldbf * 2) || !dXnrm.ensure((size_t)n_samples * 4) ||
-            !dCbf.ensure((size_t)npad * ldbf * 2) || !dCtmp.ensure((size_t)npad * 4) ||
+        const size_t xb = (size_t)n_samples * ldbf * 2;
+        if (!dXh.ensure(xb) || (split == 3 && !dXl.ensure(xb)) ||
+            !dXnrm.ensure((size_t)n_samples * 4) || !dBh.ensure((size_t)npad * ldbf * 2) ||
+            !dBl.ensure((size_t)npad * ldbf * 2) || !dBaug.ensure((size_t)npad * 64 * 2) ||
+            !dAaug.ensure(128 * 64 * 2) || !dCtmp.ensure((size_t)npad * 4) ||
             !dTcScal.ensure(64) || !dAmb.ensure((size_t)n_samples * 4 * 6))
             return err->error(da_status_memory_error, "Device memory allocation failed.");
         cudaStream_t st = cuda->stream;
-        if (fresh || dXbf_stale) {
-            B200_TRY(launch_to_bf16(dX.as<float>(), ld, n_samples, n_features, dXbf.p, ldbf, st),
-                     "bf16 copy");
+        if (fresh) {
+            B200_TRY(launch_split_bf16(dX.as<float>(), ld, n_samples, n_features, dXh.p,
+                                       split == 3 ? dXl.p : nullptr, ldbf, st), "bf16 copy");
             B200_TRY(launch_row_norm_max(dX.as<float>(), ld, n_samples, n_features,
                                          dXnrm.as<float>(), nullptr, st), "row norms");
+            tc_split = split;
             dXbf_stale = false;
+            aaug_ready = false;
         }
-        B200_TRY(cudaMemsetAsync(dCbf.p, 0, (size_t)npad * ldbf * 2, st), "memset");
         B200_TRY(cudaMemsetAsync(dTcScal.p, 0, 64, st), "memset");
         use_tc = true;
     }
@@ -413,11 +419,16 @@ template <typename T> da_status KMeans<T>::assign(const T *dC, int *dL, const in
             int *amb_rows = dAmb.as<int>();
             int *amb_ncand = amb_rows + n;
             int *amb_cand = amb_rows + 2 * (size_t)n;
-            B200_TRY(launch_to_bf16(dC, ld, k, d, dCbf.p, ldbf, st), "bf16 centres");
+            const bool s3 = tc_split == 3;
+            B200_TRY(launch_prep_centres(dC, ld, k, d, ldbf, dCn.as<float>(), dBh.p,
+                                         s3 ? dBl.p : nullptr, dBaug.p,
+                                         aaug_ready ? nullptr : dAaug.p, st), "centre operands");
+            aaug_ready = true;
             B200_TRY(launch_row_norm_max(dC, ld, k, d, dCtmp.as<float>(), cmax, st), "centre norms");
             B200_TRY(cudaMemsetAsync(amb_cnt, 0, sizeof(int), st), "memset");
             B200_TRY(cuda->timed("kmeans_assign", [&] {
-                return launch_kmeans_assign_tc(dXbf.p, n, ldbf, dCbf.p, k, dCn.as<float>(),
+                return launch_kmeans_assign_tc(tc_split, dXh.p, s3 ? dXl.p : nullptr, n, ldbf,
+                                               dBh.p, s3 ? dBl.p : nullptr, dBaug.p, dAaug.p, k,
                                                dXnrm.as<float>(), cmax, dL, dLprev,
                                                dFlags.as<int>(), amb_rows, amb_cand, amb_ncand,
                                                amb_cnt, errf, st);

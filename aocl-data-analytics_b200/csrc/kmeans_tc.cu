@@ -1,22 +1,23 @@
 // Tensor-core (tcgen05) k-means assignment for sm_100a.
 //
-// S = X_bf16 * C_bf16^T is accumulated in fp32 in TMEM (128 rows per tile,
-// N = all clusters, <= 256), fed by 128-byte-swizzled TMA tiles.  The epilogue
-// forms v_j = |c_j|^2 - 2 s_j and keeps, per row, the smallest and the
-// second-smallest v.  The label of the plain fp32 path is certified when the
-// gap exceeds twice a rigorous bound on |v_bf16 - v_fp32|:
-//   eps_i = 2 delta |x_i| cmax + 2^-23 (cmax^2 + 2 |x_i| cmax),
-//   delta = 2^-7 (1 + 2^-7) + K 2^-21
-// (bf16 rounding of both operands: |x~c~ - xc| <= 2^-7 |xc|; fp32 accumulation
-// of the tensor core and of the plain path: K 2^-23 each; two fma roundings).
-// Rows whose gap is not certified are appended to a list and relabelled by
-// the exact fp32 kernel, so every label equals the plain path's label.
+// For a 128-row tile of X and all clusters (N <= 256) the MMA accumulates in
+// TMEM (fp32) directly the approximate Lloyd score
+//     v_j = |c_j|^2 - 2 x.c_j
+// using B = -2 C (exact scaling) split into bf16 hi/lo parts and one extra
+// K=16 MMA that adds |c_j|^2 (bf16 hi + lo) through a constant "ones" operand:
+//   SPLIT = 1:  Xh.Bh + 1.(cn_h + cn_l)
+//   SPLIT = 3:  Xh.Bh + Xh.Bl + Xl.Bh + 1.(cn_h + cn_l)     (X = Xh + Xl)
+// The epilogue finds b1 = min_j v_j (pass 1) and every cluster with
+// v_j <= b1 + 2 eps (pass 2).  eps is a rigorous bound on |v_tc - v_fp32|
+// (operand rounding, fp32 accumulation of the tensor core and of the plain
+// fp32 path, the bf16 split of |c|^2), so the plain path's label is among the
+// candidates; a single candidate IS that label.  Rows with several candidates
+// are appended to a list and re-scored exactly with the plain fp32 formula.
 //
 // Warp roles (320 threads): warp 0 TMA producer, warp 1 TMEM owner + MMA
-// issuer, warps 2-9 two epilogue warpgroups (each owns one TMEM buffer and
-// every other tile).
-// Accumulators are double-buffered in TMEM so MMA of tile t+1 overlaps the
-// epilogue of tile t.
+// issuer, warps 2-9 two epilogue warpgroups; group g owns TMEM accumulator g
+// and every other tile, so MMA of one tile overlaps the epilogue of another.
+// No TMA multicast; every wait is bounded.
 #include "b200_common.cuh"
 #include "b200_kernels.hpp"
 #include "tc_common.cuh"
@@ -33,9 +34,9 @@ static constexpr int TC_MAXC = 4;       // candidates kept per uncertified row
 
 struct TcAssignArgs {
     int n, k, npad, nkb, stages, bufcols;
-    const float *cnorm;  // k   (fp32, plain formula)
     const float *xnorm;  // n   (fp32 |x_i|)
     const float *cmax;   // 1   (max_j |c_j|)
+    float e1, e2;        // eps_i = e1 |x_i| cmax + e2 cmax^2
     int *labels;
     const int *labels_prev;
     int *flags;          // [0] labels changed
@@ -44,7 +45,6 @@ struct TcAssignArgs {
     int *amb_ncand;      // number of candidates (0: scan every cluster)
     int *amb_count;
     int *err;            // set on a timed-out wait
-    float delta;
 };
 
 struct __align__(16) TcShared {
@@ -53,28 +53,35 @@ struct __align__(16) TcShared {
     int abort_flag;
     int changed;
 };
+static_assert(sizeof(TcShared) % 16 == 0, "keeps the candidate scratch aligned");
 
 __device__ __forceinline__ void raise(int *abort_flag, int *err, int code) {
     *((volatile int *)abort_flag) = 1;
     atomicExch(err, code);
 }
 
+template <int SPLIT>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
-                        const __grid_constant__ CUtensorMap tmC, TcAssignArgs a) {
+kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
+                        const __grid_constant__ CUtensorMap tmXl,
+                        const __grid_constant__ CUtensorMap tmBh,
+                        const __grid_constant__ CUtensorMap tmBl,
+                        const __grid_constant__ CUtensorMap tmBaug,
+                        const __grid_constant__ CUtensorMap tmAaug, TcAssignArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    // 1024-byte alignment for the swizzled operand tiles
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    constexpr int NX = (SPLIT == 3) ? 2 : 1; // X operands per K block
     const int S = a.stages, nkb = a.nkb;
-    const uint32_t b_bytes = (uint32_t)a.npad * 128u;       // one K block of C
-    const uint32_t a_bytes = (uint32_t)TC_BM * 128u;        // one K block of a tile
-    unsigned char *Bs = base;
-    unsigned char *As = Bs + (size_t)nkb * b_bytes;
-    TcShared *sh = reinterpret_cast<TcShared *>(As + (size_t)S * nkb * a_bytes);
-    float *cn_s = reinterpret_cast<float *>(sh + 1);      // npad32 entries, +inf pad
-    const int npad32 = (a.npad + 31) & ~31;
-    int *cand_s = reinterpret_cast<int *>(cn_s + npad32); // [TC_THREADS][TC_MAXC]
+    const uint32_t b_bytes = (uint32_t)a.npad * 128u; // one K block of C
+    const uint32_t a_bytes = (uint32_t)TC_BM * 128u;  // one K block of a tile
+    unsigned char *Bh = base;
+    unsigned char *Bl = Bh + (size_t)nkb * b_bytes;                    // SPLIT == 3
+    unsigned char *Baug = Bl + (SPLIT == 3 ? (size_t)nkb * b_bytes : 0);
+    unsigned char *Aaug = Baug + b_bytes;
+    unsigned char *As = Aaug + a_bytes;                                // S stages
+    TcShared *sh = reinterpret_cast<TcShared *>(As + (size_t)S * NX * nkb * a_bytes);
+    int *cand_s = reinterpret_cast<int *>(sh + 1); // [TC_THREADS][TC_MAXC]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ntiles = (a.n + TC_BM - 1) / TC_BM;
@@ -93,8 +100,6 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
         sh->changed = 0;
         fence_barrier_init();
     }
-    for (int j = threadIdx.x; j < npad32; j += blockDim.x)
-        cn_s[j] = j < a.k ? a.cnorm[j] : __int_as_float(0x7f800000);
     if (warp == 1) {
         tmem_alloc(&sh->tmem_base, 2u * a.bufcols);
         tmem_relinquish();
@@ -107,31 +112,37 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
     if (warp == 0) {
         // ------------------------------------------------ TMA producer ----
         if (lane == 0) {
-            prefetch_tmap(&tmX);
-            prefetch_tmap(&tmC);
-            mbar_arrive_expect_tx(&sh->bfull, (uint32_t)nkb * b_bytes);
-            for (int kb = 0; kb < nkb; ++kb)
-                tma_load_2d(&tmC, &sh->bfull, Bs + (size_t)kb * b_bytes, kb * TC_KB, 0);
+            prefetch_tmap(&tmXh);
+            prefetch_tmap(&tmBh);
+            mbar_arrive_expect_tx(&sh->bfull, (uint32_t)(NX * nkb + 1) * b_bytes + a_bytes);
+            for (int kb = 0; kb < nkb; ++kb) {
+                tma_load_2d(&tmBh, &sh->bfull, Bh + (size_t)kb * b_bytes, kb * TC_KB, 0);
+                if (SPLIT == 3)
+                    tma_load_2d(&tmBl, &sh->bfull, Bl + (size_t)kb * b_bytes, kb * TC_KB, 0);
+            }
+            tma_load_2d(&tmBaug, &sh->bfull, Baug, 0, 0);
+            tma_load_2d(&tmAaug, &sh->bfull, Aaug, 0, 0);
             int it = 0;
             for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
                 const int s = it % S;
-                const uint32_t ph = (uint32_t)((it / S) & 1);
-                if (!mbar_wait(&sh->empty[s], ph ^ 1u)) {
+                if (!mbar_wait(&sh->empty[s], (uint32_t)(((it / S) & 1) ^ 1))) {
                     raise(&sh->abort_flag, a.err, 1);
                     break;
                 }
                 if (*((volatile int *)&sh->abort_flag)) break;
-                mbar_arrive_expect_tx(&sh->full[s], (uint32_t)nkb * a_bytes);
-                for (int kb = 0; kb < nkb; ++kb)
-                    tma_load_2d(&tmX, &sh->full[s], As + ((size_t)s * nkb + kb) * a_bytes,
-                                kb * TC_KB, t * TC_BM);
+                mbar_arrive_expect_tx(&sh->full[s], (uint32_t)(NX * nkb) * a_bytes);
+                unsigned char *st = As + (size_t)s * NX * nkb * a_bytes;
+                for (int kb = 0; kb < nkb; ++kb) {
+                    tma_load_2d(&tmXh, &sh->full[s], st + (size_t)kb * a_bytes, kb * TC_KB,
+                                t * TC_BM);
+                    if (SPLIT == 3)
+                        tma_load_2d(&tmXl, &sh->full[s], st + (size_t)(nkb + kb) * a_bytes,
+                                    kb * TC_KB, t * TC_BM);
+                }
             }
             // drain: every issued stage must have landed before exit
-            const int issued = it;
-            for (int u = (issued > S ? issued - S : 0); u < issued; ++u) {
-                const int s = u % S;
-                mbar_wait(&sh->full[s], (uint32_t)((u / S) & 1));
-            }
+            for (int u = (it > S ? it - S : 0); u < it; ++u)
+                mbar_wait(&sh->full[u % S], (uint32_t)((u / S) & 1));
         }
     } else if (warp == 1) {
         // ------------------------------------------------ MMA issuer ------
@@ -139,6 +150,7 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
             const uint32_t idesc = idesc_bf16_f32(TC_BM, a.npad);
             bool ok = mbar_wait(&sh->bfull, 0);
             if (!ok) raise(&sh->abort_flag, a.err, 2);
+            const uint32_t baug = smem_u32(Baug), aaug = smem_u32(Aaug);
             int it = 0;
             for (int t = blockIdx.x; ok && t < ntiles; t += gridDim.x, ++it) {
                 const int s = it % S, b = it & 1;
@@ -153,14 +165,28 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
                 if (*((volatile int *)&sh->abort_flag)) break;
                 tc_fence_after();
                 const uint32_t tacc = tbase + (uint32_t)(b * a.bufcols);
+                const unsigned char *st = As + (size_t)s * NX * nkb * a_bytes;
+                uint32_t acc = 0;
                 for (int kb = 0; kb < nkb; ++kb) {
-                    const uint32_t abase = smem_u32(As + ((size_t)s * nkb + kb) * a_bytes);
-                    const uint32_t bbase = smem_u32(Bs + (size_t)kb * b_bytes);
+                    const uint32_t xh = smem_u32(st + (size_t)kb * a_bytes);
+                    const uint32_t xl = smem_u32(st + (size_t)(nkb + kb) * a_bytes);
+                    const uint32_t bh = smem_u32(Bh + (size_t)kb * b_bytes);
+                    const uint32_t bl = smem_u32(Bl + (size_t)kb * b_bytes);
 #pragma unroll
-                    for (int kk = 0; kk < TC_KB / 16; ++kk)
-                        mma_f16_ss(tacc, desc_k_sw128(abase + kk * 32), desc_k_sw128(bbase + kk * 32),
-                                   idesc, (kb | kk) != 0);
+                    for (int kk = 0; kk < TC_KB / 16; ++kk) {
+                        mma_f16_ss(tacc, desc_k_sw128(xh + kk * 32), desc_k_sw128(bh + kk * 32),
+                                   idesc, acc);
+                        acc = 1;
+                        if (SPLIT == 3) {
+                            mma_f16_ss(tacc, desc_k_sw128(xh + kk * 32),
+                                       desc_k_sw128(bl + kk * 32), idesc, 1);
+                            mma_f16_ss(tacc, desc_k_sw128(xl + kk * 32),
+                                       desc_k_sw128(bh + kk * 32), idesc, 1);
+                        }
+                    }
                 }
+                // + |c_j|^2 (hi + lo) through the constant ones operand
+                mma_f16_ss(tacc, desc_k_sw128(aaug), desc_k_sw128(baug), idesc, 1);
                 mma_commit(&sh->empty[s]);
                 mma_commit(&sh->tfull[b]);
             }
@@ -171,14 +197,14 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
         }
     } else {
         // ------------------------------------------------ epilogue --------
-        // Group g (warps 2-5 / 6-9) owns TMEM buffer g and the local tiles
-        // it = g, g+2, ...; each thread owns one row (its TMEM lane) and scans
-        // all clusters.  The groups never wait on each other.
-        const int g = (warp - 2) / 4;
+        const int g = (warp - 2) / 4;      // accumulator / tile parity
         const int q = warp & 3;            // TMEM lane quarter of this warp
         const int row_in_tile = q * 32 + lane;
         const int nchunks = (a.npad + 31) / 32;
+        const int tail = a.npad - (nchunks - 1) * 32; // valid columns of the last chunk
         const float cmax = *a.cmax;
+        const float inf = __int_as_float(0x7f800000);
+        int *my = cand_s + threadIdx.x * TC_MAXC;
         int changed = 0;
         int it = g;
         for (int t = blockIdx.x + g * gridDim.x; t < ntiles; t += 2 * gridDim.x, it += 2) {
@@ -192,19 +218,16 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
             const uint32_t trow = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * a.bufcols);
             const int r = t * TC_BM + row_in_tile;
             const float xn = r < a.n ? a.xnorm[r] : 0.f;
-            // pass 1: smallest v_j = |c_j|^2 - 2 s_j (tree minimum per 32 columns)
-            float b1 = __int_as_float(0x7f800000);
+            // pass 1: b1 = min_j v_j (tree minimum per 32 columns).  All lanes
+            // execute every tcgen05.ld (warp-synchronous).
+            float b1 = inf;
             for (int c = 0; c < nchunks; ++c) {
                 float v[32];
                 tmem_ld32(trow + (uint32_t)(c * 32), v);
-                const float4 *cn4 = reinterpret_cast<const float4 *>(cn_s + c * 32);
+                if (c == nchunks - 1 && tail < 32) {
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const float4 cc = cn4[u];
-                    v[4 * u + 0] = __fmaf_rn(-2.f, v[4 * u + 0], cc.x);
-                    v[4 * u + 1] = __fmaf_rn(-2.f, v[4 * u + 1], cc.y);
-                    v[4 * u + 2] = __fmaf_rn(-2.f, v[4 * u + 2], cc.z);
-                    v[4 * u + 3] = __fmaf_rn(-2.f, v[4 * u + 3], cc.w);
+                    for (int u = 0; u < 32; ++u)
+                        if (u >= tail) v[u] = inf;
                 }
 #pragma unroll
                 for (int w = 16; w >= 1; w >>= 1)
@@ -212,45 +235,36 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
                     for (int u = 0; u < w; ++u) v[u] = fminf(v[u], v[u + w]);
                 b1 = fminf(b1, v[0]);
             }
-            // pass 2: every cluster within 2 eps of the minimum is a candidate
-            const float eps = 1.01f * (2.f * a.delta * xn * cmax +
-                                       1.1920929e-7f * (cmax * cmax + 2.f * xn * cmax));
+            // pass 2: clusters within 2 eps of the minimum
+            const float eps = a.e1 * xn * cmax + a.e2 * cmax * cmax;
             const float tau = b1 + 2.f * eps;
             int cnt = 0;
-            int *my = cand_s + threadIdx.x * TC_MAXC;
             for (int c = 0; c < nchunks; ++c) {
                 float v[32];
                 tmem_ld32(trow + (uint32_t)(c * 32), v);
-                const float4 *cn4 = reinterpret_cast<const float4 *>(cn_s + c * 32);
+                const int lim = (c == nchunks - 1) ? tail : 32;
+                uint32_t bits = 0;
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const float4 cc = cn4[u];
-                    const float w4[4] = {__fmaf_rn(-2.f, v[4 * u + 0], cc.x),
-                                         __fmaf_rn(-2.f, v[4 * u + 1], cc.y),
-                                         __fmaf_rn(-2.f, v[4 * u + 2], cc.z),
-                                         __fmaf_rn(-2.f, v[4 * u + 3], cc.w)};
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const int j = c * 32 + 4 * u + e;
-                        if (w4[e] <= tau && j < a.k) { // padded columns are never candidates
-                            if (cnt < TC_MAXC) my[cnt] = j;
-                            ++cnt;
-                        }
-                    }
+                for (int u = 0; u < 32; ++u)
+                    if (v[u] <= tau && u < lim) bits |= 1u << u;
+                while (bits) {
+                    const int u = __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    if (cnt < TC_MAXC) my[cnt] = c * 32 + u;
+                    ++cnt;
                 }
             }
             tc_fence_before();
             mbar_arrive(&sh->tempty[b]);
             const bool valid = r < a.n;
-            if (valid && cnt == 1) {
-                // a single candidate: the fp32 label is certified
+            const bool certain = valid && cnt == 1 && tau <= 3.0e38f && my[0] < a.k;
+            if (certain) {
                 const int lbl = my[0];
                 a.labels[r] = lbl;
                 if (a.labels_prev && a.labels_prev[r] != lbl) changed = 1;
             }
-            // near-ties (or NaN): appended, one atomic per warp, for the exact
-            // fp32 re-score of their candidates
-            const bool amb = valid && cnt != 1;
+            // several candidates (or non-finite scores): one atomic per warp
+            const bool amb = valid && !certain;
             const unsigned mask = __ballot_sync(0xffffffffu, amb);
             if (mask) {
                 int base0 = 0;
@@ -259,7 +273,9 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmX,
                 if (amb) {
                     const int pos = base0 + __popc(mask & ((1u << lane) - 1u));
                     a.amb_rows[pos] = r;
-                    const int nc = (cnt >= 2 && cnt <= TC_MAXC) ? cnt : 0;
+                    bool okc = cnt >= 2 && cnt <= TC_MAXC && tau <= 3.0e38f;
+                    for (int e = 0; e < cnt && e < TC_MAXC; ++e) okc = okc && my[e] < a.k;
+                    const int nc = okc ? cnt : 0;
                     a.amb_ncand[pos] = nc;
                     for (int e = 0; e < nc; ++e) a.amb_cand[pos * TC_MAXC + e] = my[e];
                 }
@@ -294,6 +310,7 @@ kmeans_rescore_kernel(const float *X, int ld, int d, const float *C, int k,
     float *xs = rs_smem + (c_in_smem ? (size_t)k * dp : 0) + (threadIdx.x >> 5) * 32 * dp;
     const int lane = threadIdx.x & 31;
     const int cnt = *amb_count;
+    if (cnt == 0) return;
     if (c_in_smem) {
         for (int e = threadIdx.x; e < k * d; e += blockDim.x) {
             const int j = e / d, f = e % d;
@@ -306,15 +323,14 @@ kmeans_rescore_kernel(const float *X, int ld, int d, const float *C, int k,
     for (int e0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; e0 < cnt;
          e0 += warps_total * 32) {
         const int ne = min(32, cnt - e0);
-        // coalesced staging of the (up to) 32 listed rows
+        const int myrow = lane < ne ? amb_rows[e0 + lane] : 0;
         for (int i = 0; i < ne; ++i) {
-            const float *x = X + (size_t)amb_rows[e0 + i] * ld;
+            const float *x = X + (size_t)__shfl_sync(0xffffffffu, myrow, i) * ld;
             for (int f = lane; f < d; f += 32) xs[i * dp + f] = x[f];
         }
         __syncwarp();
         if (lane < ne) {
             const int e = e0 + lane;
-            const int r = amb_rows[e];
             const float *x = xs + lane * dp;
             const int nc = amb_ncand[e];
             float best = __int_as_float(0x7f800000);
@@ -337,21 +353,58 @@ kmeans_rescore_kernel(const float *X, int ld, int d, const float *C, int k,
                 }
             }
             const int lbl = (bi == 0x7fffffff) ? 0 : bi;
-            labels[r] = lbl;
-            if (labels_prev && labels_prev[r] != lbl) changed = 1;
+            labels[myrow] = lbl;
+            if (labels_prev && labels_prev[myrow] != lbl) changed = 1;
         }
         __syncwarp();
     }
     if (changed && flags) atomicOr(&flags[0], 1);
 }
 
-// fp32 (row-major, ld) -> bf16 (row-major, ldo = nkb*64), zero padded.
-__global__ void to_bf16_kernel(const float *X, int ld, int rows, int d, __nv_bfloat16 *Y, int ldo) {
+// X (fp32, ld) -> Xh = bf16(x), Xl = bf16(x - Xh) (row-major, ldo), zero pad.
+__global__ void split_bf16_kernel(const float *X, int ld, int rows, int d, __nv_bfloat16 *Xh,
+                                  __nv_bfloat16 *Xl, int ldo) {
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t total = (size_t)rows * ldo;
-    if (e >= total) return;
+    if (e >= (size_t)rows * ldo) return;
     const int r = (int)(e / ldo), c = (int)(e % ldo);
-    Y[e] = __float2bfloat16_rn((c < d) ? X[(size_t)r * ld + c] : 0.f);
+    const float x = (c < d) ? X[(size_t)r * ld + c] : 0.f;
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    Xh[e] = h;
+    if (Xl) Xl[e] = __float2bfloat16_rn(x - __bfloat162float(h));
+}
+// Operands of the centres: B = -2 C split hi/lo (rows k..npad-1 zero) and the
+// |c|^2 column pair (cn_h, cn_l) of Baug (+inf for the padded rows).
+__global__ void prep_centres_kernel(const float *C, int ld, int k, int d, int npad, int ldo,
+                                    const float *cnorm, __nv_bfloat16 *Bh, __nv_bfloat16 *Bl,
+                                    __nv_bfloat16 *Baug) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < (size_t)npad * ldo) {
+        const int j = (int)(e / ldo), f = (int)(e % ldo);
+        const float x = (j < k && f < d) ? -2.f * C[(size_t)j * ld + f] : 0.f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        Bh[e] = h;
+        if (Bl) Bl[e] = __float2bfloat16_rn(x - __bfloat162float(h));
+    }
+    if (e < (size_t)npad * TC_KB) {
+        const int j = (int)(e / TC_KB), f = (int)(e % TC_KB);
+        __nv_bfloat16 v = __float2bfloat16_rn(0.f);
+        if (j < k) {
+            const __nv_bfloat16 h = __float2bfloat16_rn(cnorm[j]);
+            if (f == 0) v = h;
+            if (f == 1) v = __float2bfloat16_rn(cnorm[j] - __bfloat162float(h));
+        } else if (f == 0) {
+            v = __float2bfloat16_rn(__int_as_float(0x7f800000));
+        }
+        Baug[e] = v;
+    }
+}
+// The constant "ones" operand: 128 rows x 64, columns 0 and 1 equal to 1.
+__global__ void ones_aug_kernel(__nv_bfloat16 *A) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < TC_BM * TC_KB) {
+        const int f = e % TC_KB;
+        A[e] = __float2bfloat16_rn(f < 2 ? 1.f : 0.f);
+    }
 }
 // |x_i| (fp32 sqrt of the fma-chain squared norm) and, optionally, the max.
 __global__ void row_norm_max_kernel(const float *X, int ld, int rows, int d, float *out,
@@ -395,7 +448,7 @@ static EncodeTiledFn get_encode() {
 // 128-byte swizzle, zero fill out of bounds.
 static bool make_map_bf16(CUtensorMap *m, const void *ptr, int rows, int cols, int box_rows) {
     EncodeTiledFn enc = get_encode();
-    if (!enc) return false;
+    if (!enc || !ptr) return false;
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
     cuuint32_t box[2] = {(cuuint32_t)TC_KB, (cuuint32_t)box_rows};
@@ -406,19 +459,45 @@ static bool make_map_bf16(CUtensorMap *m, const void *ptr, int rows, int cols, i
            CUDA_SUCCESS;
 }
 
-int tc_assign_supported(int k, int d) {
+static size_t tc_smem_bytes(int split, int nkb, int npad, int stages) {
+    const int nx = split == 3 ? 2 : 1;
+    return 1024 + (size_t)(nx * nkb + 1) * npad * 128 + (size_t)TC_BM * 128 +
+           (size_t)stages * nx * nkb * TC_BM * 128 + sizeof(TcShared) +
+           (size_t)TC_THREADS * TC_MAXC * 4 + 64;
+}
+static int tc_stages(int split, int nkb, int npad) {
+    int s = 6;
+    while (s > 2 && tc_smem_bytes(split, nkb, npad, s) > 225 * 1024) --s;
+    return s;
+}
+
+int tc_assign_supported(int k, int d, int split) {
     if (k < 1 || k > 256) return 0;
     const int nkb = (d + TC_KB - 1) / TC_KB;
     const int npad = (k + 15) & ~15;
-    const size_t need = (size_t)nkb * npad * 128 + 2 * (size_t)nkb * TC_BM * 128 + 4096;
-    return need <= 200 * 1024 ? 1 : 0;
+    return tc_smem_bytes(split, nkb, npad, 2) <= 225 * 1024 ? 1 : 0;
 }
 
-cudaError_t launch_to_bf16(const float *X, int ld, int rows, int d, void *Y, int ldo,
-                           cudaStream_t s) {
+cudaError_t launch_split_bf16(const float *X, int ld, int rows, int d, void *Xh, void *Xl,
+                              int ldo, cudaStream_t s) {
     const size_t total = (size_t)rows * ldo;
-    to_bf16_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(
-        X, ld, rows, d, reinterpret_cast<__nv_bfloat16 *>(Y), ldo);
+    split_bf16_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(
+        X, ld, rows, d, reinterpret_cast<__nv_bfloat16 *>(Xh),
+        reinterpret_cast<__nv_bfloat16 *>(Xl), ldo);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prep_centres(const float *C, int ld, int k, int d, int ldo,
+                                const float *cnorm, void *Bh, void *Bl, void *Baug,
+                                void *Aaug_once, cudaStream_t s) {
+    const int npad = (k + 15) & ~15;
+    const size_t total = (size_t)npad * (ldo > TC_KB ? ldo : TC_KB);
+    prep_centres_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(
+        C, ld, k, d, npad, ldo, cnorm, reinterpret_cast<__nv_bfloat16 *>(Bh),
+        reinterpret_cast<__nv_bfloat16 *>(Bl), reinterpret_cast<__nv_bfloat16 *>(Baug));
+    if (Aaug_once)
+        ones_aug_kernel<<<(TC_BM * TC_KB + 255) / 256, 256, 0, s>>>(
+            reinterpret_cast<__nv_bfloat16 *>(Aaug_once));
     return cudaGetLastError();
 }
 
@@ -432,24 +511,44 @@ cudaError_t launch_row_norm_max(const float *X, int ld, int rows, int d, float *
     return cudaGetLastError();
 }
 
-cudaError_t launch_kmeans_assign_tc(const void *Xbf, int n, int ldbf, const void *Cbf, int k,
-                                    const float *cnorm, const float *xnorm, const float *cmax,
-                                    int *labels, const int *labels_prev, int *flags,
-                                    int *amb_rows, int *amb_cand, int *amb_ncand, int *amb_count,
-                                    int *err, cudaStream_t s) {
+cudaError_t launch_kmeans_assign_tc(int split, const void *Xh, const void *Xl, int n, int ldbf,
+                                    const void *Bh, const void *Bl, const void *Baug,
+                                    const void *Aaug, int k, const float *xnorm,
+                                    const float *cmax, int *labels, const int *labels_prev,
+                                    int *flags, int *amb_rows, int *amb_cand, int *amb_ncand,
+                                    int *amb_count, int *err, cudaStream_t s) {
     const int nkb = ldbf / TC_KB;
     const int npad = (k + 15) & ~15;
-    CUtensorMap mx, mc;
-    if (!make_map_bf16(&mx, Xbf, n, ldbf, TC_BM) || !make_map_bf16(&mc, Cbf, npad, ldbf, npad))
+    CUtensorMap mxh, mxl, mbh, mbl, mbaug, maaug;
+    const bool s3 = split == 3;
+    if (!make_map_bf16(&mxh, Xh, n, ldbf, TC_BM) || !make_map_bf16(&mbh, Bh, npad, ldbf, npad) ||
+        !make_map_bf16(&mbaug, Baug, npad, TC_KB, npad) ||
+        !make_map_bf16(&maaug, Aaug, TC_BM, TC_KB, TC_BM))
         return cudaErrorInvalidValue;
-    const size_t b_bytes = (size_t)nkb * npad * 128;
-    const size_t a_stage = (size_t)nkb * TC_BM * 128;
-    int stages = (int)((150 * 1024 - b_bytes) / a_stage);
-    stages = stages < 2 ? 2 : (stages > 6 ? 6 : stages);
-    const size_t smem = 1024 + b_bytes + stages * a_stage + sizeof(TcShared) +
-                        (size_t)((npad + 31) & ~31) * 4 + TC_THREADS * TC_MAXC * 4 + 64;
+    if (s3) {
+        if (!make_map_bf16(&mxl, Xl, n, ldbf, TC_BM) || !make_map_bf16(&mbl, Bl, npad, ldbf, npad))
+            return cudaErrorInvalidValue;
+    } else {
+        mxl = mxh;
+        mbl = mbh;
+    }
+    const int stages = tc_stages(split, nkb, npad);
+    const size_t smem = tc_smem_bytes(split, nkb, npad, stages);
     int bufcols = 32;
     while (bufcols < npad) bufcols <<= 1;
+    // Rigorous |v_tc - v_fp32| bound, eps = e1 |x| cmax + e2 cmax^2
+    // (products relative to |x| |-2c| = 2 |x||c|; u = 2^-24):
+    //   operand rounding   split 1: (2^-7 + 2^-16) . 2     split 3: 3.1 . 2^-16 . 2
+    //   tensor-core fp32 accumulation of K_total terms:    K_total 2^-23 (2 |x||c| + |c|^2)
+    //   plain fp32 fma chain and final fma:                2 Kp u |x||c| + u |v|
+    //   bf16 hi/lo split of |c|^2:                         2^-16 |c|^2
+    const double u = std::ldexp(1.0, -24);
+    const double kp = (double)nkb * TC_KB;
+    const double ktot = (s3 ? 3.0 : 1.0) * kp + 16.0;
+    const double prod = s3 ? 3.1 * std::ldexp(1.0, -16) * 2.0
+                           : (std::ldexp(1.0, -7) + std::ldexp(1.0, -16)) * 2.0;
+    const double e1 = 1.05 * (prod + ktot * 2.0 * u * 2.0 + 2.0 * kp * u + 2.0 * u);
+    const double e2 = 1.05 * (ktot * 2.0 * u + std::ldexp(1.0, -16) + u);
     TcAssignArgs a;
     a.n = n;
     a.k = k;
@@ -457,9 +556,10 @@ cudaError_t launch_kmeans_assign_tc(const void *Xbf, int n, int ldbf, const void
     a.nkb = nkb;
     a.stages = stages;
     a.bufcols = bufcols;
-    a.cnorm = cnorm;
     a.xnorm = xnorm;
     a.cmax = cmax;
+    a.e1 = (float)e1;
+    a.e2 = (float)e2;
     a.labels = labels;
     a.labels_prev = labels_prev;
     a.flags = flags;
@@ -468,15 +568,16 @@ cudaError_t launch_kmeans_assign_tc(const void *Xbf, int n, int ldbf, const void
     a.amb_ncand = amb_ncand;
     a.amb_count = amb_count;
     a.err = err;
-    a.delta = 0.0078125f * (1.f + 0.0078125f) + (float)(nkb * TC_KB) * 4.76837158e-7f;
-    cudaError_t e = cudaFuncSetAttribute(kmeans_assign_tc_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    auto kern = s3 ? kmeans_assign_tc_kernel<3> : kmeans_assign_tc_kernel<1>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
     if (e != cudaSuccess) return e;
     const int ntiles = (n + TC_BM - 1) / TC_BM;
-    int nsm = 148;
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const int grid = ntiles < nsm ? ntiles : nsm;
-    kmeans_assign_tc_kernel<<<grid, TC_THREADS, smem, s>>>(mx, mc, a);
+    kern<<<grid, TC_THREADS, smem, s>>>(mxh, mxl, mbh, mbl, mbaug, maaug, a);
     return cudaGetLastError();
 }
 
@@ -501,9 +602,4 @@ cudaError_t launch_kmeans_rescore(const float *X, int ld, int d, const float *C,
     return cudaGetLastError();
 }
 
-} // namespace b200
-
-namespace b200 {
-// The epilogue reads |c_j|^2 as float4 right after the barrier block.
-static_assert(sizeof(TcShared) % 16 == 0, "TcShared must keep the cnorm array 16-byte aligned");
 } // namespace b200

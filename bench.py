@@ -235,7 +235,8 @@ def main():
         km.set_data(X)
         return km
 
-    km = handle("bf16")
+    mode = os.environ.get("BENCH_MODE", "bf16x3")
+    km = handle(mode)
     t0 = time.perf_counter()
     C0 = km.init_centres(K)
     init_ms = (time.perf_counter() - t0) * 1e3
@@ -343,8 +344,8 @@ def main():
         cb = cpu_baseline(X, C0, int(os.environ.get("BENCH_CPU_SAMPLE", "131072")), 2)
     extra = {"iterations_per_step": n_iter, "init_ms": init_ms,
              "relabelled_rows_last_iteration": relabelled,
-             "precision_path": "bf16 tcgen05 candidate pass + exact fp32 relabel" if tensor_core
-             else "plain fp32 (SIMT)"}
+             "precision_path": (f"{mode} tcgen05 candidate pass + exact fp32 re-score of "
+                                "uncertified rows") if tensor_core else "plain fp32 (SIMT)"}
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -373,7 +374,7 @@ def run_e2e(ab, km, X, C0, stream, args, world):
     km2.L.da_b200_set_stream(km2.h, C.c_void_p(stream.cuda_stream))
     km2.set("convergence tolerance", TOL)
     km2.set("initialization method", "supplied")
-    km2.set("precision mode", "bf16")
+    km2.set("precision mode", os.environ.get("BENCH_MODE", "bf16x3"))
     lab_host = torch.empty(N, dtype=torch.int32, pin_memory=True).numpy()
     cen_host = np.zeros(K * D, dtype=np.float32)
 

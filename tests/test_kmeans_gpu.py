@@ -126,17 +126,19 @@ def test_kmeans_empty_cluster_modes(gpu, ab):
 @pytest.mark.parametrize("n,d,k", [(100000, 64, 256), (33333, 37, 100), (20000, 128, 64),
                                    (5000, 200, 16), (70000, 96, 250), (4000, 8, 3)])
 def test_kmeans_bf16_tensor_core_equals_plain(gpu, ab, n, d, k):
-    """The BF16 tensor-core candidate pass must return exactly the plain fp32
-    path's labels, centres, iteration count and inertia."""
+    """Both BF16 tensor-core candidate passes (one term, three-term split) must
+    return exactly the plain fp32 path's labels, centres, iteration count and
+    inertia."""
     rng = np.random.default_rng(n + k)
     A = gmm(rng, n, d, max(k // 2, 2))
     C0 = A[rng.choice(n, k, replace=False)].copy()
     out = {}
-    for mode in ("plain", "bf16"):
+    for mode in ("plain", "bf16", "bf16x3"):
         km = ab.KMeans(k, "s", order=0, max_iter=25, n_init=1)
         km.set("precision mode", mode)
         km.fit(A, C0=C0)
         out[mode] = (km.labels(n), km.centres(k, d), km.rinfo())
-    np.testing.assert_array_equal(out["plain"][0], out["bf16"][0])
-    np.testing.assert_array_equal(out["plain"][1], out["bf16"][1])
-    np.testing.assert_array_equal(out["plain"][2], out["bf16"][2])
+    for mode in ("bf16", "bf16x3"):
+        np.testing.assert_array_equal(out["plain"][0], out[mode][0])
+        np.testing.assert_array_equal(out["plain"][1], out[mode][1])
+        np.testing.assert_array_equal(out["plain"][2], out[mode][2])
