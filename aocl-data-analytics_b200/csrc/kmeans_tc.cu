@@ -60,6 +60,32 @@ __device__ __forceinline__ void raise(int *abort_flag, int *err, int code) {
     atomicExch(err, code);
 }
 
+// Minimum of the first `lim` of 32 accumulator values (a tree, for ILP).
+__device__ __forceinline__ float chunk_min(const uint32_t (&r)[32], int lim) {
+    float v[32];
+#pragma unroll
+    for (int u = 0; u < 32; ++u) v[u] = u < lim ? __uint_as_float(r[u]) : __int_as_float(0x7f800000);
+#pragma unroll
+    for (int w = 16; w >= 1; w >>= 1)
+#pragma unroll
+        for (int u = 0; u < w; ++u) v[u] = fminf(v[u], v[u + w]);
+    return v[0];
+}
+// Candidates of one 32-column chunk: columns with v <= tau (first TC_MAXC kept).
+__device__ __forceinline__ void collect(const uint32_t (&r)[32], int c, int lim, float tau,
+                                        int *my, int &cnt) {
+    uint32_t bits = 0;
+#pragma unroll
+    for (int u = 0; u < 32; ++u)
+        if (__uint_as_float(r[u]) <= tau && u < lim) bits |= 1u << u;
+    while (bits) {
+        const int u = __ffs(bits) - 1;
+        bits &= bits - 1;
+        if (cnt < TC_MAXC) my[cnt] = c * 32 + u;
+        ++cnt;
+    }
+}
+
 template <int SPLIT>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
@@ -219,39 +245,41 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
             const int r = t * TC_BM + row_in_tile;
             const float xn = r < a.n ? a.xnorm[r] : 0.f;
             // pass 1: b1 = min_j v_j (tree minimum per 32 columns).  All lanes
-            // execute every tcgen05.ld (warp-synchronous).
+            // execute every tcgen05.ld (warp-synchronous); the load of chunk
+            // c+1 is in flight while chunk c is reduced.
             float b1 = inf;
-            for (int c = 0; c < nchunks; ++c) {
-                float v[32];
-                tmem_ld32(trow + (uint32_t)(c * 32), v);
-                if (c == nchunks - 1 && tail < 32) {
-#pragma unroll
-                    for (int u = 0; u < 32; ++u)
-                        if (u >= tail) v[u] = inf;
+            {
+                uint32_t ra[32], rb[32];
+                tmem_ld32_issue(trow, ra);
+                tmem_ld_wait(ra);
+                for (int c = 0; c < nchunks; c += 2) {
+                    if (c + 1 < nchunks) tmem_ld32_issue(trow + (uint32_t)((c + 1) * 32), rb);
+                    b1 = fminf(b1, chunk_min(ra, c == nchunks - 1 ? tail : 32));
+                    if (c + 1 < nchunks) {
+                        tmem_ld_wait(rb);
+                        if (c + 2 < nchunks) tmem_ld32_issue(trow + (uint32_t)((c + 2) * 32), ra);
+                        b1 = fminf(b1, chunk_min(rb, c + 1 == nchunks - 1 ? tail : 32));
+                        if (c + 2 < nchunks) tmem_ld_wait(ra);
+                    }
                 }
-#pragma unroll
-                for (int w = 16; w >= 1; w >>= 1)
-#pragma unroll
-                    for (int u = 0; u < w; ++u) v[u] = fminf(v[u], v[u + w]);
-                b1 = fminf(b1, v[0]);
             }
             // pass 2: clusters within 2 eps of the minimum
             const float eps = a.e1 * xn * cmax + a.e2 * cmax * cmax;
             const float tau = b1 + 2.f * eps;
             int cnt = 0;
-            for (int c = 0; c < nchunks; ++c) {
-                float v[32];
-                tmem_ld32(trow + (uint32_t)(c * 32), v);
-                const int lim = (c == nchunks - 1) ? tail : 32;
-                uint32_t bits = 0;
-#pragma unroll
-                for (int u = 0; u < 32; ++u)
-                    if (v[u] <= tau && u < lim) bits |= 1u << u;
-                while (bits) {
-                    const int u = __ffs(bits) - 1;
-                    bits &= bits - 1;
-                    if (cnt < TC_MAXC) my[cnt] = c * 32 + u;
-                    ++cnt;
+            {
+                uint32_t ra[32], rb[32];
+                tmem_ld32_issue(trow, ra);
+                tmem_ld_wait(ra);
+                for (int c = 0; c < nchunks; c += 2) {
+                    if (c + 1 < nchunks) tmem_ld32_issue(trow + (uint32_t)((c + 1) * 32), rb);
+                    collect(ra, c, c == nchunks - 1 ? tail : 32, tau, my, cnt);
+                    if (c + 1 < nchunks) {
+                        tmem_ld_wait(rb);
+                        if (c + 2 < nchunks) tmem_ld32_issue(trow + (uint32_t)((c + 2) * 32), ra);
+                        collect(rb, c + 1, c + 1 == nchunks - 1 ? tail : 32, tau, my, cnt);
+                        if (c + 2 < nchunks) tmem_ld_wait(ra);
+                    }
                 }
             }
             tc_fence_before();
@@ -295,10 +323,8 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
 // Exact fp32 relabelling of the uncertified rows: the plain path's formula
 // fl(|c|^2 - 2 x.c) with the dot product as one fma chain over the features,
 // evaluated for the listed candidates (every cluster when the list
-// overflowed); ties -> lower index.  Each warp stages the centres and 32
-// listed rows in shared memory (coalesced loads, rows padded to d+1 floats so
-// the per-lane sequential dot products are bank-conflict free); one lane per
-// listed row.
+// overflowed); ties -> lower index.  One thread per listed row; the centres
+// are staged in shared memory (rows padded to d+1 floats).
 __global__ void __launch_bounds__(256)
 kmeans_rescore_kernel(const float *X, int ld, int d, const float *C, int k,
                       const float *cnorm, const int *amb_rows, const int *amb_cand,
@@ -306,57 +332,76 @@ kmeans_rescore_kernel(const float *X, int ld, int d, const float *C, int k,
                       const int *labels_prev, int *flags, int c_in_smem) {
     extern __shared__ float rs_smem[];
     const int dp = d + 1;
-    float *cs = rs_smem;                                            // k x dp (optional)
-    float *xs = rs_smem + (c_in_smem ? (size_t)k * dp : 0) + (threadIdx.x >> 5) * 32 * dp;
-    const int lane = threadIdx.x & 31;
+    float *cs = rs_smem; // k x dp (when c_in_smem)
     const int cnt = *amb_count;
     if (cnt == 0) return;
     if (c_in_smem) {
         for (int e = threadIdx.x; e < k * d; e += blockDim.x) {
-            const int j = e / d, f = e % d;
+            const int j = e / d, f = e - j * d;
             cs[j * dp + f] = C[(size_t)j * ld + f];
         }
         __syncthreads();
     }
     int changed = 0;
-    const int warps_total = (gridDim.x * blockDim.x) >> 5;
-    for (int e0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; e0 < cnt;
-         e0 += warps_total * 32) {
-        const int ne = min(32, cnt - e0);
-        const int myrow = lane < ne ? amb_rows[e0 + lane] : 0;
-        for (int i = 0; i < ne; ++i) {
-            const float *x = X + (size_t)__shfl_sync(0xffffffffu, myrow, i) * ld;
-            for (int f = lane; f < d; f += 32) xs[i * dp + f] = x[f];
-        }
-        __syncwarp();
-        if (lane < ne) {
-            const int e = e0 + lane;
-            const float *x = xs + lane * dp;
-            const int nc = amb_ncand[e];
-            float best = __int_as_float(0x7f800000);
-            int bi = 0x7fffffff;
-            const int m = nc > 0 ? nc : k;
-            for (int u = 0; u < m; ++u) {
-                const int j = nc > 0 ? amb_cand[e * TC_MAXC + u] : u;
-                float sdot = 0.f;
-                if (c_in_smem) {
-                    const float *c = cs + j * dp;
-                    for (int f = 0; f < d; ++f) sdot = __fmaf_rn(x[f], c[f], sdot);
-                } else {
-                    const float *c = C + (size_t)j * ld;
-                    for (int f = 0; f < d; ++f) sdot = __fmaf_rn(x[f], c[f], sdot);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += gridDim.x * blockDim.x) {
+        const int r = amb_rows[e];
+        const float *x = X + (size_t)r * ld;
+        const int nc = amb_ncand[e];
+        float best = __int_as_float(0x7f800000);
+        int bi = 0x7fffffff;
+        if (nc > 0) {
+            // up to TC_MAXC candidates: x streamed once in 16-float chunks,
+            // each candidate's dot kept as its own sequential fma chain
+            int jj[TC_MAXC];
+            float sd[TC_MAXC];
+#pragma unroll
+            for (int u = 0; u < TC_MAXC; ++u) {
+                jj[u] = u < nc ? amb_cand[e * TC_MAXC + u] : amb_cand[e * TC_MAXC];
+                sd[u] = 0.f;
+            }
+            for (int f0 = 0; f0 < d; f0 += 16) {
+                float xv[16];
+#pragma unroll
+                for (int q = 0; q < 16; q += 4) {
+                    if (f0 + q < ld) {
+                        const float4 t = __ldg(reinterpret_cast<const float4 *>(x + f0 + q));
+                        xv[q] = t.x; xv[q + 1] = t.y; xv[q + 2] = t.z; xv[q + 3] = t.w;
+                    } else {
+                        xv[q] = xv[q + 1] = xv[q + 2] = xv[q + 3] = 0.f;
+                    }
                 }
+                const int fe = min(16, d - f0);
+#pragma unroll
+                for (int u = 0; u < TC_MAXC; ++u) {
+                    const float *c = c_in_smem ? cs + jj[u] * dp : C + (size_t)jj[u] * ld;
+                    for (int q = 0; q < fe; ++q) sd[u] = __fmaf_rn(xv[q], c[f0 + q], sd[u]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < TC_MAXC; ++u) {
+                if (u < nc) {
+                    const float v = __fmaf_rn(-2.f, sd[u], cnorm[jj[u]]);
+                    if (key_less(v, jj[u], best, bi)) {
+                        best = v;
+                        bi = jj[u];
+                    }
+                }
+            }
+        } else {
+            for (int j = 0; j < k; ++j) {
+                const float *c = c_in_smem ? cs + j * dp : C + (size_t)j * ld;
+                float sdot = 0.f;
+                for (int f = 0; f < d; ++f) sdot = __fmaf_rn(x[f], c[f], sdot);
                 const float v = __fmaf_rn(-2.f, sdot, cnorm[j]);
                 if (key_less(v, j, best, bi)) {
                     best = v;
                     bi = j;
                 }
             }
-            const int lbl = (bi == 0x7fffffff) ? 0 : bi;
-            labels[myrow] = lbl;
-            if (labels_prev && labels_prev[myrow] != lbl) changed = 1;
         }
-        __syncwarp();
+        const int lbl = (bi == 0x7fffffff) ? 0 : bi;
+        labels[r] = lbl;
+        if (labels_prev && labels_prev[r] != lbl) changed = 1;
     }
     if (changed && flags) atomicOr(&flags[0], 1);
 }
@@ -587,10 +632,9 @@ cudaError_t launch_kmeans_rescore(const float *X, int ld, int d, const float *C,
                                   int *labels, const int *labels_prev, int *flags,
                                   cudaStream_t s) {
     if (max_rows <= 0) return cudaSuccess;
-    const size_t xs_bytes = (size_t)8 * 32 * (d + 1) * 4;
     const size_t cs_bytes = (size_t)k * (d + 1) * 4;
-    const int c_in_smem = (cs_bytes + xs_bytes <= 200 * 1024) ? 1 : 0;
-    const size_t smem = xs_bytes + (c_in_smem ? cs_bytes : 0);
+    const int c_in_smem = (cs_bytes <= 200 * 1024) ? 1 : 0;
+    const size_t smem = c_in_smem ? cs_bytes : 0;
     if (smem > 220 * 1024) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(kmeans_rescore_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
