@@ -60,24 +60,26 @@ __device__ __forceinline__ void raise(int *abort_flag, int *err, int code) {
     atomicExch(err, code);
 }
 
-// Minimum of the first `lim` of 32 accumulator values (a tree, for ILP).
-__device__ __forceinline__ float chunk_min(const uint32_t (&r)[32], int lim) {
-    float v[32];
-#pragma unroll
-    for (int u = 0; u < 32; ++u) v[u] = u < lim ? __uint_as_float(r[u]) : __int_as_float(0x7f800000);
+// Minimum of 32 accumulator values (a tree: one FMNMX per value, full ILP).
+__device__ __forceinline__ float chunk_min32(float (&v)[32]) {
 #pragma unroll
     for (int w = 16; w >= 1; w >>= 1)
 #pragma unroll
         for (int u = 0; u < w; ++u) v[u] = fminf(v[u], v[u + w]);
     return v[0];
 }
-// Candidates of one 32-column chunk: columns with v <= tau (first TC_MAXC kept).
-__device__ __forceinline__ void collect(const uint32_t (&r)[32], int c, int lim, float tau,
-                                        int *my, int &cnt) {
+// Bit u set when v[u] <= tau: one FSET (all-ones / zero) and one LOP3 per value.
+__device__ __forceinline__ uint32_t le_mask32(const float (&v)[32], float tau) {
     uint32_t bits = 0;
 #pragma unroll
-    for (int u = 0; u < 32; ++u)
-        if (__uint_as_float(r[u]) <= tau && u < lim) bits |= 1u << u;
+    for (int u = 0; u < 32; ++u) {
+        uint32_t t;
+        asm("set.le.u32.f32 %0, %1, %2;" : "=r"(t) : "f"(v[u]), "f"(tau));
+        bits |= t & (1u << u);
+    }
+    return bits;
+}
+__device__ __forceinline__ void collect_bits(uint32_t bits, int c, int *my, int &cnt) {
     while (bits) {
         const int u = __ffs(bits) - 1;
         bits &= bits - 1;
@@ -245,42 +247,29 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
             const int r = t * TC_BM + row_in_tile;
             const float xn = r < a.n ? a.xnorm[r] : 0.f;
             // pass 1: b1 = min_j v_j (tree minimum per 32 columns).  All lanes
-            // execute every tcgen05.ld (warp-synchronous); the load of chunk
-            // c+1 is in flight while chunk c is reduced.
+            // execute every tcgen05.ld (warp-synchronous); columns beyond npad
+            // in the last chunk are masked (warp-uniform branch).
             float b1 = inf;
-            {
-                uint32_t ra[32], rb[32];
-                tmem_ld32_issue(trow, ra);
-                tmem_ld_wait(ra);
-                for (int c = 0; c < nchunks; c += 2) {
-                    if (c + 1 < nchunks) tmem_ld32_issue(trow + (uint32_t)((c + 1) * 32), rb);
-                    b1 = fminf(b1, chunk_min(ra, c == nchunks - 1 ? tail : 32));
-                    if (c + 1 < nchunks) {
-                        tmem_ld_wait(rb);
-                        if (c + 2 < nchunks) tmem_ld32_issue(trow + (uint32_t)((c + 2) * 32), ra);
-                        b1 = fminf(b1, chunk_min(rb, c + 1 == nchunks - 1 ? tail : 32));
-                        if (c + 2 < nchunks) tmem_ld_wait(ra);
-                    }
+            for (int c = 0; c < nchunks; ++c) {
+                float v[32];
+                tmem_ld32(trow + (uint32_t)(c * 32), v);
+                if (c == nchunks - 1 && tail < 32) {
+#pragma unroll
+                    for (int u = 0; u < 32; ++u)
+                        if (u >= tail) v[u] = inf;
                 }
+                b1 = fminf(b1, chunk_min32(v));
             }
             // pass 2: clusters within 2 eps of the minimum
             const float eps = a.e1 * xn * cmax + a.e2 * cmax * cmax;
             const float tau = b1 + 2.f * eps;
             int cnt = 0;
-            {
-                uint32_t ra[32], rb[32];
-                tmem_ld32_issue(trow, ra);
-                tmem_ld_wait(ra);
-                for (int c = 0; c < nchunks; c += 2) {
-                    if (c + 1 < nchunks) tmem_ld32_issue(trow + (uint32_t)((c + 1) * 32), rb);
-                    collect(ra, c, c == nchunks - 1 ? tail : 32, tau, my, cnt);
-                    if (c + 1 < nchunks) {
-                        tmem_ld_wait(rb);
-                        if (c + 2 < nchunks) tmem_ld32_issue(trow + (uint32_t)((c + 2) * 32), ra);
-                        collect(rb, c + 1, c + 1 == nchunks - 1 ? tail : 32, tau, my, cnt);
-                        if (c + 2 < nchunks) tmem_ld_wait(ra);
-                    }
-                }
+            for (int c = 0; c < nchunks; ++c) {
+                float v[32];
+                tmem_ld32(trow + (uint32_t)(c * 32), v);
+                uint32_t bits = le_mask32(v, tau);
+                if (c == nchunks - 1 && tail < 32) bits &= (1u << tail) - 1u;
+                collect_bits(bits, c, my, cnt);
             }
             tc_fence_before();
             mbar_arrive(&sh->tempty[b]);
