@@ -116,11 +116,16 @@ template <typename T> struct KMeans : public AlgBase {
     int ld = 0;
     DevBuf dX, dXn, dC0, dC1, dCn, dL0, dL1, dCounts, dBlockCounts, dOffsets, dSorted,
         dChunkSums, dSegStart, dScalars, dFlags, dPartials, dW, dKD, dCand, dStage, dY, dYL,
-        dBestL, dXh, dXl, dXnrm, dBh, dBl, dBaug, dAaug, dCtmp, dTcScal, dAmb;
+        dBestL, dXh, dXl, dXnrm, dBh, dBl, dBaug, dAaug, dCtmp, dTcScal, dAmb, dFxScale,
+        dFxAcc, dFxTicket;
     int tc_split = 0;     // bf16 terms of the resident X copies (0: none)
     bool use_tc = false; // bf16 tensor-core assignment active for this compute
     bool dXbf_stale = true;
     bool aaug_ready = false;
+    bool fx_stale = true;  // fixed-point scales need recomputing (new data)
+    bool fx_data_ok = false; // data finite (scales valid)
+    bool use_fx = false;   // fixed-point centroid update active for this compute
+    int fx_parity = 0;
     int ldbf = 0;
     da_int amb_last = 0;  // rows relabelled exactly in the last tensor-core pass
     T *h_pin = nullptr;
@@ -153,6 +158,7 @@ template <typename T> struct KMeans : public AlgBase {
                          double *h_scal, int *h_flags);
     da_status split_empty(T *dC, int *dL, bool &split);
     da_status prepare_tc();
+    da_status prepare_fx();
     da_status assign(const T *dC, int *dL, const int *dLprev);
 };
 

@@ -508,6 +508,7 @@ da_status da_b200_set_stream(da_handle h, void *stream) {
 }
 da_status da_b200_set_kernel_timing(da_handle h, da_int enable) {
     if (!h) return da_status_handle_not_initialized;
+    if (!enable) h->cuda.flush_timing();
     h->cuda.timing = enable != 0;
     return da_status_success;
 }
@@ -515,6 +516,7 @@ da_status da_b200_get_kernel_time(da_handle h, const char *kernel, double *total
                                   da_int *launches) {
     if (!h) return da_status_handle_not_initialized;
     if (!kernel || !total_ms || !launches) return da_status_invalid_pointer;
+    h->cuda.flush_timing();
     auto it = h->cuda.ktime.find(kernel);
     if (it == h->cuda.ktime.end()) {
         *total_ms = 0;
@@ -534,6 +536,7 @@ da_status da_b200_get_stat(da_handle h, const char *name, double *value) {
 }
 da_status da_b200_reset_kernel_time(da_handle h) {
     if (!h) return da_status_handle_not_initialized;
+    h->cuda.flush_timing();
     h->cuda.ktime.clear();
     return da_status_success;
 }

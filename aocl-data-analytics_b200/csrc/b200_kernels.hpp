@@ -137,6 +137,25 @@ cudaError_t launch_kmeans_update(const T *X, int ldx, int n, int d, int k,
                                  const int *seg_chunk_start, int seg_rows, double *chunk_sums,
                                  const int *counts, const T *C_prev, T *C_new, int ldc,
                                  double *scalars, int *flags, cudaStream_t s);
+// Fixed-point centroid update for fp32 data (order-independent integer sums,
+// so deterministic without sorting): supported when the shared-memory
+// accumulators (k x d int64) fit.  launch_col_absmax gives the per-feature
+// max |x| (as float bits) and a non-finite flag, from which the host derives
+// scale[f] = 2^s_f (fp32) and inv_scale[f] = 2^-s_f (fp64), with
+// n max|x_f| 2^s_f < 2^62 and max|x_f| 2^s_f < 2^44.  accum (fx_accum_bytes) holds
+// two sets of global sums and counts used alternately (parity): the update
+// of parity p reads set p and clears set 1-p, so both must be zero before
+// the first call.  ticket is a zero-initialised counter left at zero.
+int fx_update_supported(int k, int d);
+size_t fx_accum_bytes(int k, int d);
+cudaError_t launch_col_absmax(const float *X, int ld, int n, int d, unsigned *colmax,
+                              int *nonfinite, cudaStream_t s);
+cudaError_t launch_kmeans_update_fx(const float *X, int ld, int n, int d, int k,
+                                    const int *labels, const float *scale,
+                                    const double *inv_scale, void *accum, int parity,
+                                    const float *C_prev, float *C_new, int *counts,
+                                    double *block_partials, double *scalars, int *flags,
+                                    unsigned *ticket, cudaStream_t s);
 // Squared row norms of the centres (sequential fma chain over features).
 template <typename T>
 cudaError_t launch_centre_norms(const T *C, int ldc, int k, int d, T *out, cudaStream_t s);
@@ -182,7 +201,7 @@ cudaError_t launch_row_norm_max(const float *X, int ld, int rows, int d, float *
 cudaError_t launch_kmeans_assign_tc(int split, const void *Xh, const void *Xl, int n, int ldbf,
                                     const void *Bh, const void *Bl, const void *Baug,
                                     const void *Aaug, int k, const float *xnorm,
-                                    const float *cmax, int *labels, const int *labels_prev,
+                                    const float *cnorm, int *labels, const int *labels_prev,
                                     int *flags, int *amb_rows, int *amb_cand, int *amb_ncand,
                                     int *amb_count, int *err, cudaStream_t s);
 // Exact fp32 labels of the rows listed by the tensor-core pass.

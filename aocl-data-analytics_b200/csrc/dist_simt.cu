@@ -380,14 +380,29 @@ cudaError_t launch_knn_merge(const T *part_key, const int *part_idx, int nq, int
 }
 
 // ------------------------------------------------------------ row norms ---
+// Squared norms as one sequential fma chain per row.  A block of 256 threads
+// takes 32 rows: 64-feature slabs of them are staged in shared memory with
+// coalesced loads (rows padded to 65 words), then 32 threads carry the chains.
 template <typename T>
-__global__ void row_sqnorms_kernel(const T *X, int ld, int rows, int d, T *out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= rows) return;
-    const T *x = X + (size_t)i * ld;
+__global__ void __launch_bounds__(256) row_sqnorms_kernel(const T *X, int ld, int rows, int d,
+                                                          T *out) {
+    __shared__ T slab[32][65];
+    const int r0 = blockIdx.x * 32;
+    const int nr = min(32, rows - r0);
     T s = T(0);
-    for (int j = 0; j < d; ++j) s = fma_rn(x[j], x[j], s);
-    out[i] = s;
+    for (int f0 = 0; f0 < d; f0 += 64) {
+        const int nf = min(64, d - f0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < 32 * 64; e += 256) {
+            const int i = e >> 6, f = e & 63;
+            if (i < nr && f < nf) slab[i][f] = X[(size_t)(r0 + i) * ld + f0 + f];
+        }
+        __syncthreads();
+        if ((int)threadIdx.x < nr)
+            for (int f = 0; f < nf; ++f)
+                s = fma_rn(slab[threadIdx.x][f], slab[threadIdx.x][f], s);
+    }
+    if ((int)threadIdx.x < nr) out[r0 + threadIdx.x] = s;
 }
 template <typename T>
 __global__ void row_norms_eps1_kernel(const T *X, int ld, int rows, int d, T eps, T *out) {
@@ -401,7 +416,8 @@ __global__ void row_norms_eps1_kernel(const T *X, int ld, int rows, int d, T eps
 }
 template <typename T>
 cudaError_t launch_row_sqnorms(const T *X, int ld, int rows, int d, T *out, cudaStream_t s) {
-    row_sqnorms_kernel<T><<<(rows + 255) / 256, 256, 0, s>>>(X, ld, rows, d, out);
+    if (rows <= 0) return cudaSuccess;
+    row_sqnorms_kernel<T><<<(rows + 31) / 32, 256, 0, s>>>(X, ld, rows, d, out);
     return cudaGetLastError();
 }
 template <typename T>

@@ -286,7 +286,15 @@ struct CudaCtx {
     cudaStream_t own_stream = nullptr; // the handle's own stream
     bool ready = false;
     bool timing = false;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // Kernel timing: one event pair per timed launch, recorded without
+    // synchronising (so that the pair brackets the launch as it runs among
+    // its neighbours) and folded into ktime by flush_timing().
+    struct TimedLaunch {
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        std::string name;
+    };
+    std::vector<TimedLaunch> tpool;
+    size_t tused = 0;
     std::map<std::string, std::pair<double, long>> ktime; // name -> (ms total, launches)
     std::map<std::string, double> stats;                  // named counters of the last call
 
@@ -309,28 +317,47 @@ struct CudaCtx {
             return err.error(da_status_internal_error, "cudaStreamCreate failed.");
         }
         if (!stream) stream = own_stream;
-        cudaEventCreate(&ev0);
-        cudaEventCreate(&ev1);
         ready = true;
         return da_status_success;
     }
     ~CudaCtx() {
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
+        for (auto &t : tpool) {
+            if (t.ev0) cudaEventDestroy(t.ev0);
+            if (t.ev1) cudaEventDestroy(t.ev1);
+        }
         if (own_stream) cudaStreamDestroy(own_stream);
+    }
+    // Fold the recorded launches into ktime (waits for the last of them).
+    void flush_timing() {
+        if (tused == 0) return;
+        cudaEventSynchronize(tpool[tused - 1].ev1);
+        for (size_t i = 0; i < tused; ++i) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, tpool[i].ev0, tpool[i].ev1) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            auto &t = ktime[tpool[i].name];
+            t.first += ms;
+            t.second += 1;
+        }
+        tused = 0;
     }
     // Time one launch with events on the handle's stream when timing is on.
     template <typename F> cudaError_t timed(const char *name, F &&launch) {
         if (!timing) return launch();
-        cudaEventRecord(ev0, stream);
+        if (tused == 1024) flush_timing();
+        if (tused == tpool.size()) {
+            TimedLaunch t;
+            cudaEventCreate(&t.ev0);
+            cudaEventCreate(&t.ev1);
+            tpool.push_back(t);
+        }
+        TimedLaunch &t = tpool[tused++];
+        t.name = name;
+        cudaEventRecord(t.ev0, stream);
         cudaError_t e = launch();
-        cudaEventRecord(ev1, stream);
-        cudaEventSynchronize(ev1);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, ev0, ev1);
-        auto &t = ktime[name];
-        t.first += ms;
-        t.second += 1;
+        cudaEventRecord(t.ev1, stream);
         return e;
     }
 };

@@ -109,6 +109,7 @@ template <typename T> da_status KMeans<T>::ensure_device_data() {
     B200_TRY(launch_row_sqnorms<T>(dX.as<T>(), ld, n_samples, n_features, dXn.as<T>(), cuda->stream),
              "row norms");
     dXbf_stale = true;
+    fx_stale = true;
     return da_status_success;
 }
 
@@ -371,6 +372,71 @@ template <typename T> da_status KMeans<T>::init_centres(T *dC) {
     return da_status_success;
 }
 
+// Fixed-point centroid update (fp32 data): per-feature scales 2^s_f with
+// n * max_i |x_if| * 2^s_f < 2^62 (computed once per data set), partial-sum
+// buffers for one CTA per SM.  Data holding inf or NaN keep the sorted fp64
+// update.
+template <typename T> da_status KMeans<T>::prepare_fx() {
+    use_fx = false;
+    if constexpr (std::is_same_v<T, float>) {
+        const int n = n_samples, k = n_clusters, d = n_features;
+        if (!fx_update_supported(k, d)) return da_status_success;
+        cudaStream_t st = cuda->stream;
+        const size_t accb = fx_accum_bytes(k, d);
+        if (!dFxScale.ensure((size_t)2 * d * sizeof(double) + (size_t)d * 4 + 16) ||
+            !dFxAcc.ensure(accb))
+            return err->error(da_status_memory_error, "Device memory allocation failed.");
+        // both accumulator sets start at zero (each update clears the other)
+        B200_TRY(cudaMemsetAsync(dFxAcc.p, 0, accb, st), "memset");
+        fx_parity = 0;
+        if (!dFxTicket.p) {
+            if (!dFxTicket.ensure(16))
+                return err->error(da_status_memory_error, "Device memory allocation failed.");
+            B200_TRY(cudaMemsetAsync(dFxTicket.p, 0, 16, st), "memset");
+        }
+        if (fx_stale) {
+            double *scale = dFxScale.as<double>();
+            unsigned *colmax = reinterpret_cast<unsigned *>(scale + 2 * d);
+            int *nonfinite = reinterpret_cast<int *>(colmax + d);
+            B200_TRY(launch_col_absmax(dX.as<float>(), ld, n, d, colmax, nonfinite, st),
+                     "column maxima");
+            std::vector<unsigned> hmax(d + 1);
+            B200_TRY(cudaMemcpyAsync(hmax.data(), colmax, (d + 1) * sizeof(unsigned),
+                                     cudaMemcpyDeviceToHost, st), "copy");
+            B200_TRY(cudaStreamSynchronize(st), "column maxima");
+            fx_data_ok = hmax[d] == 0;
+            if (fx_data_ok) {
+                // scale[f] = 2^s_f as fp32 (bytes 0..4d), inv_scale[f] = 2^-s_f as
+                // fp64 (from byte 8d); s_f keeps n max|x| 2^s_f < 2^62 and
+                // max|x| 2^s_f < 2^44 (the quantiser's range), and 2^s_f within
+                // the fp32 range
+                int L = 0;
+                while ((1LL << L) < (long long)n) ++L;
+                std::vector<float> scf(d);
+                std::vector<double> inv(d);
+                for (int f = 0; f < d; ++f) {
+                    float m;
+                    std::memcpy(&m, &hmax[f], sizeof(float));
+                    int E = 0;
+                    if (m > 0.f) std::frexp((double)m, &E); // m < 2^E
+                    int sf = std::min(62 - L, 44) - E;
+                    sf = std::max(-126, std::min(127, sf));
+                    scf[f] = std::ldexp(1.0f, sf);
+                    inv[f] = std::ldexp(1.0, -sf);
+                }
+                B200_TRY(cudaMemcpyAsync(scale, scf.data(), d * sizeof(float),
+                                         cudaMemcpyHostToDevice, st), "copy");
+                B200_TRY(cudaMemcpyAsync(scale + d, inv.data(), d * sizeof(double),
+                                         cudaMemcpyHostToDevice, st), "copy");
+                B200_TRY(cudaStreamSynchronize(st), "scales");
+            }
+            fx_stale = false;
+        }
+        use_fx = fx_data_ok;
+    }
+    return da_status_success;
+}
+
 // Device state of the tensor-core assignment (fp32 data only): bf16 copy of
 // X, row norms |x_i|, bf16 centres, scalars and the relabel list.
 template <typename T> da_status KMeans<T>::prepare_tc() {
@@ -413,7 +479,6 @@ template <typename T> da_status KMeans<T>::assign(const T *dC, int *dL, const in
     const int n = n_samples, k = n_clusters, d = n_features;
     if constexpr (std::is_same_v<T, float>) {
         if (use_tc) {
-            float *cmax = dTcScal.as<float>();
             int *amb_cnt = reinterpret_cast<int *>(dTcScal.as<char>() + 16);
             int *errf = reinterpret_cast<int *>(dTcScal.as<char>() + 20);
             int *amb_rows = dAmb.as<int>();
@@ -424,12 +489,11 @@ template <typename T> da_status KMeans<T>::assign(const T *dC, int *dL, const in
                                          s3 ? dBl.p : nullptr, dBaug.p,
                                          aaug_ready ? nullptr : dAaug.p, st), "centre operands");
             aaug_ready = true;
-            B200_TRY(launch_row_norm_max(dC, ld, k, d, dCtmp.as<float>(), cmax, st), "centre norms");
             B200_TRY(cudaMemsetAsync(amb_cnt, 0, sizeof(int), st), "memset");
             B200_TRY(cuda->timed("kmeans_assign", [&] {
                 return launch_kmeans_assign_tc(tc_split, dXh.p, s3 ? dXl.p : nullptr, n, ldbf,
                                                dBh.p, s3 ? dBl.p : nullptr, dBaug.p, dAaug.p, k,
-                                               dXnrm.as<float>(), cmax, dL, dLprev,
+                                               dXnrm.as<float>(), dCn.as<float>(), dL, dLprev,
                                                dFlags.as<int>(), amb_rows, amb_cand, amb_ncand,
                                                amb_cnt, errf, st);
             }), "tensor-core assign");
@@ -461,7 +525,19 @@ da_status KMeans<T>::lloyd_step(const T *dCprev, T *dCnew, int *dL, const int *d
         da_status sa = assign(dCprev, dL, dLprev);
         if (sa != da_status_success) return sa;
     }
-    if (update) {
+    if (update && use_fx) {
+        if constexpr (std::is_same_v<T, float>) {
+            const double *scale = dFxScale.as<double>();
+            B200_TRY(cuda->timed("kmeans_update", [&] {
+                return launch_kmeans_update_fx(
+                    dX.as<float>(), ld, n, d, k, dL, reinterpret_cast<const float *>(scale),
+                    scale + d, dFxAcc.p, fx_parity,
+                    dCprev, dCnew, dCounts.as<int>(), dScalars.as<double>() + 8,
+                    dScalars.as<double>(), dFlags.as<int>(), dFxTicket.as<unsigned>(), st);
+            }), "update");
+            fx_parity ^= 1;
+        }
+    } else if (update) {
         B200_TRY(cuda->timed("kmeans_sort", [&] {
             return launch_kmeans_sort(dL, n, k, dBlockCounts.as<int>(), dCounts.as<int>(),
                                       dOffsets.as<int>(), dSegStart.as<int>(), SEG_ROWS,
@@ -679,7 +755,10 @@ template <typename T> da_status KMeans<T>::compute() {
     if (s != da_status_success) return s;
     s = prepare_tc();
     if (s != da_status_success) return s;
+    s = prepare_fx();
+    if (s != da_status_success) return s;
     cuda->stats["tensor_core"] = use_tc ? 1.0 : 0.0;
+    cuda->stats["fixed_point_update"] = use_fx ? 1.0 : 0.0;
     if (init_method != INIT_SUPPLIED) {
         if (seed == -1) {
             std::random_device r;

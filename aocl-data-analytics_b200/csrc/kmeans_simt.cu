@@ -484,4 +484,256 @@ cudaError_t launch_kpp_update(T *w, const T *Dc, int n, int chosen, cudaStream_t
 B200_KM_INST(float)
 B200_KM_INST(double)
 
+
+// ------------------------------------------- fixed-point update (fp32 X) ---
+// Centroid sums as exact 64-bit integer sums of fixed-point features: feature
+// f of a row becomes q = round(x * 2^s_f), with s_f chosen once per data set
+// so that n * max_i |x_if| * 2^s_f < 2^62 and max_i |x_if| * 2^s_f < 2^44.  Integer addition is associative,
+// so the sums (and the centres) do not depend on the order in which rows are
+// added: one streaming pass over X with shared-memory accumulators, no sort.
+// The rounding error per term is at most 2^-(s_f+1) = max_i |x_if| 2^-(E+1)
+// with E = min(62 - L, 44) (n <= 2^L): for n >= 2^18 that is 2^-(63-L) of the
+// column maximum, below the error of an fp64 running sum over the same rows.
+namespace {
+constexpr int FX_SMEM_LIMIT = 200 * 1024;
+constexpr int FX_THREADS = 1024;
+constexpr int FX_ROWS = 8; // rows in flight per warp
+} // namespace
+
+size_t fx_update_smem(int k, int d) {
+    return (size_t)k * d * 8 + (size_t)k * 4 + (size_t)d * 4;
+}
+int fx_update_supported(int k, int d) { return fx_update_smem(k, d) <= FX_SMEM_LIMIT ? 1 : 0; }
+
+__global__ void col_absmax_kernel(const float *X, int ld, int n, int d, unsigned *colmax,
+                                  int *nonfinite) {
+    extern __shared__ unsigned cm[];
+    for (int f = threadIdx.x; f < d; f += blockDim.x) cm[f] = 0u;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    int bad = 0;
+    for (int r = blockIdx.x * nw + warp; r < n; r += gridDim.x * nw) {
+        const float *x = X + (size_t)r * ld;
+        for (int f = lane; f < d; f += 32) {
+            const unsigned b = __float_as_uint(x[f]) & 0x7fffffffu;
+            if (b >= 0x7f800000u) bad = 1;
+            else atomicMax(&cm[f], b);
+        }
+    }
+    if (bad) *nonfinite = 1;
+    __syncthreads();
+    for (int f = threadIdx.x; f < d; f += blockDim.x) atomicMax(&colmax[f], cm[f]);
+}
+
+cudaError_t launch_col_absmax(const float *X, int ld, int n, int d, unsigned *colmax,
+                              int *nonfinite, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(colmax, 0, (size_t)d * sizeof(unsigned), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(nonfinite, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    const int blocks = max(1, min(148 * 4, (n + 31) / 32));
+    col_absmax_kernel<<<blocks, 256, (size_t)d * sizeof(unsigned), s>>>(X, ld, n, d, colmax,
+                                                                         nonfinite);
+    return cudaGetLastError();
+}
+
+// q = round(x * 2^s) for |x * 2^s| < 2^44, on the FMA pipe: y = x * 2^s is
+// exact; yh = y rounded to a multiple of 2^22 (add/subtract 1.5 * 2^45) and
+// yl = y - yh (exact, |yl| <= 2^21); both halves become int32 through the
+// 1.5 * 2^23 magic constant (exact for |v| < 2^22).  Rounding is to nearest
+// (ties to even at each step; any fixed rule keeps the sums deterministic).
+__device__ __forceinline__ long long fx_quant(float x, float sc) {
+    const float y = __fmul_rn(x, sc);
+    const float yh = __fsub_rn(__fadd_rn(y, 52776558133248.f), 52776558133248.f);
+    const float yl = __fsub_rn(y, yh);
+    const int hi = __float_as_int(__fmaf_rn(yh, 2.384185791015625e-07f, 12582912.f)) - 0x4B400000;
+    const int lo = __float_as_int(__fadd_rn(yl, 12582912.f)) - 0x4B400000;
+    return ((long long)hi << 22) + lo;
+}
+
+// acc += q (64-bit, in shared memory) as two 32-bit atomics: the low word's
+// atomic returns its old value, from which this addition's carry into the
+// high word is exact whatever the interleaving of the other threads' adds.
+__device__ __forceinline__ void fx_add(unsigned long long *acc, long long q) {
+    unsigned *w = reinterpret_cast<unsigned *>(acc);
+    const unsigned l = (unsigned)q, h = (unsigned)((unsigned long long)q >> 32);
+    const unsigned o = atomicAdd(w, l);
+    atomicAdd(w + 1, h + (o + l < o ? 1u : 0u));
+}
+
+// One CTA per SM, each over a contiguous range of rows: warp per row (lanes
+// over feature pairs when VEC2), FX_ROWS rows in flight; integer atomics into
+// shared memory; the CTA's sums and counts are then added (integer
+// reductions, so the order of the CTAs does not matter) into the global
+// accumulators gsum / gcnt.
+template <bool VEC2>
+__global__ void __launch_bounds__(FX_THREADS, 1)
+fx_update_kernel(const float *X, int ld, int n, int d, int k, const int *labels,
+                 const float *scale, unsigned long long *gsum, int *gcnt) {
+    extern __shared__ __align__(16) unsigned char fx_smem[];
+    unsigned long long *acc = reinterpret_cast<unsigned long long *>(fx_smem);
+    int *cnt = reinterpret_cast<int *>(acc + (size_t)k * d);
+    float *sc = reinterpret_cast<float *>(cnt + k);
+    const int kd = k * d;
+    for (int e = threadIdx.x; e < kd; e += blockDim.x) acc[e] = 0ull;
+    for (int j = threadIdx.x; j < k; j += blockDim.x) cnt[j] = 0;
+    for (int f = threadIdx.x; f < d; f += blockDim.x) sc[f] = scale[f];
+    __syncthreads();
+    const long long per = ((long long)n + gridDim.x - 1) / gridDim.x;
+    const int r0 = (int)min((long long)n, per * blockIdx.x);
+    const int r1 = (int)min((long long)n, per * (blockIdx.x + 1));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int rb = r0 + warp * FX_ROWS; rb < r1; rb += nw * FX_ROWS) {
+        const int lv = lane < FX_ROWS && rb + lane < r1 ? labels[rb + lane] : -1;
+        int lab[FX_ROWS];
+#pragma unroll
+        for (int u = 0; u < FX_ROWS; ++u) lab[u] = __shfl_sync(0xffffffffu, lv, u);
+        if (VEC2) {
+            for (int f = 2 * lane; f < d; f += 64) {
+                float2 xv[FX_ROWS];
+#pragma unroll
+                for (int u = 0; u < FX_ROWS; ++u)
+                    xv[u] = rb + u < r1
+                                ? *reinterpret_cast<const float2 *>(X + (size_t)(rb + u) * ld + f)
+                                : make_float2(0.f, 0.f);
+                const float s0 = sc[f], s1 = sc[f + 1];
+#pragma unroll
+                for (int u = 0; u < FX_ROWS; ++u) {
+                    if (lab[u] >= 0) {
+                        unsigned long long *a = acc + (size_t)lab[u] * d + f;
+                        fx_add(a, fx_quant(xv[u].x, s0));
+                        fx_add(a + 1, fx_quant(xv[u].y, s1));
+                    }
+                }
+            }
+        } else {
+            for (int f = lane; f < d; f += 32) {
+                float xv[FX_ROWS];
+#pragma unroll
+                for (int u = 0; u < FX_ROWS; ++u)
+                    xv[u] = rb + u < r1 ? X[(size_t)(rb + u) * ld + f] : 0.f;
+                const float s0 = sc[f];
+#pragma unroll
+                for (int u = 0; u < FX_ROWS; ++u)
+                    if (lab[u] >= 0) fx_add(acc + (size_t)lab[u] * d + f, fx_quant(xv[u], s0));
+            }
+        }
+        if (lv >= 0) atomicAdd(&cnt[lv], 1);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kd; e += blockDim.x)
+        if (acc[e]) atomicAdd(&gsum[e], acc[e]);
+    for (int j = threadIdx.x; j < k; j += blockDim.x)
+        if (cnt[j]) atomicAdd(&gcnt[j], cnt[j]);
+}
+
+// One thread per (cluster, feature): the mean from the global sums, and fp64
+// block partials of |C_prev|^2 and |C_prev - C_new|^2; the last block to
+// finish sums the block partials in block order (deterministic) into
+// scalars[0..1] and re-arms the ticket.  The other accumulator pair
+// (nsum / ncnt, used by the next update) is cleared here.
+__global__ void __launch_bounds__(256)
+fx_finalize_kernel(int k, int d, int ld, const unsigned long long *gsum, const int *gcnt,
+                   unsigned long long *nsum, int *ncnt, const double *inv_scale,
+                   const float *C_prev, float *C_new, int *counts, double *block_partials,
+                   double *scalars, int *flags, unsigned *ticket) {
+    __shared__ double s0[256], s1[256];
+    __shared__ bool last;
+    const int kd = k * d;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double pn = 0.0, ps = 0.0;
+    if (e < kd) {
+        const int j = e / d, f = e - j * d;
+        const long long S = (long long)gsum[e];
+        const int c = gcnt[j];
+        nsum[e] = 0ull;
+        if (f == 0) ncnt[j] = 0;
+        const double mean = ((double)S * inv_scale[f]) / (double)(c > 0 ? c : 1);
+        const float cn = (float)mean;
+        const size_t o = (size_t)j * ld + f;
+        const float cp = C_prev[o];
+        C_new[o] = cn;
+        pn = (double)cp * (double)cp;
+        const double df = (double)cp - (double)cn;
+        ps = df * df;
+        if (f == 0) {
+            if (counts) counts[j] = c;
+            if (c == 0 && flags) atomicAdd(&flags[1], 1);
+        }
+    }
+    s0[threadIdx.x] = pn;
+    s1[threadIdx.x] = ps;
+    __syncthreads();
+    for (int off = 128; off > 0; off >>= 1) {
+        if ((int)threadIdx.x < off) {
+            s0[threadIdx.x] += s0[threadIdx.x + off];
+            s1[threadIdx.x] += s1[threadIdx.x + off];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        block_partials[2 * blockIdx.x] = s0[0];
+        block_partials[2 * blockIdx.x + 1] = s1[0];
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x < 32) {
+        __threadfence();
+        const int lane = threadIdx.x;
+        for (int v = 0; v < 2; ++v) {
+            double a = 0.0;
+            for (int b = lane; b < (int)gridDim.x; b += 32)
+                a += __ldcg(&block_partials[2 * b + v]);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
+            if (lane == 0) scalars[v] = a;
+        }
+        if (lane == 0) *ticket = 0u;
+    }
+}
+
+cudaError_t launch_kmeans_update_fx(const float *X, int ld, int n, int d, int k,
+                                    const int *labels, const float *scale,
+                                    const double *inv_scale, void *accum, int parity,
+                                    const float *C_prev, float *C_new, int *counts,
+                                    double *block_partials, double *scalars, int *flags,
+                                    unsigned *ticket, cudaStream_t s) {
+    const size_t smem = fx_update_smem(k, d);
+    if (smem > (size_t)FX_SMEM_LIMIT) return cudaErrorInvalidValue;
+    thread_local int smem_set[16] = {};
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (dev < 0 || dev >= 16 || smem_set[dev] < (int)smem) {
+        cudaError_t e = cudaFuncSetAttribute(fx_update_kernel<true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(fx_update_kernel<false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 16) smem_set[dev] = (int)smem;
+    }
+    const size_t kd = (size_t)k * d;
+    unsigned long long *sum[2] = {static_cast<unsigned long long *>(accum),
+                                  static_cast<unsigned long long *>(accum) + kd};
+    int *cnt[2] = {reinterpret_cast<int *>(sum[1] + kd),
+                   reinterpret_cast<int *>(sum[1] + kd) + k};
+    const int p = parity & 1;
+    const bool vec2 = d % 2 == 0 && ld % 2 == 0 && (reinterpret_cast<uintptr_t>(X) & 7) == 0;
+    if (vec2)
+        fx_update_kernel<true><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale,
+                                                             sum[p], cnt[p]);
+    else
+        fx_update_kernel<false><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale,
+                                                              sum[p], cnt[p]);
+    const int nb = (int)((kd + 255) / 256);
+    fx_finalize_kernel<<<nb, 256, 0, s>>>(k, d, ld, sum[p], cnt[p], sum[1 - p], cnt[1 - p],
+                                          inv_scale, C_prev, C_new, counts, block_partials,
+                                          scalars, flags, ticket);
+    return cudaGetLastError();
+}
+
+size_t fx_accum_bytes(int k, int d) { return (size_t)2 * k * d * 8 + (size_t)2 * k * 4; }
+
 } // namespace b200

@@ -35,8 +35,8 @@ static constexpr int TC_MAXC = 4;       // candidates kept per uncertified row
 struct TcAssignArgs {
     int n, k, npad, nkb, stages, bufcols;
     const float *xnorm;  // n   (fp32 |x_i|)
-    const float *cmax;   // 1   (max_j |c_j|)
-    float e1, e2;        // eps_i = e1 |x_i| cmax + e2 cmax^2
+    const float *cnorm;  // k   (fp32 |c_j|^2, the plain path's values)
+    float e1, e2;        // eps_i = e1 |x_i| cmax + e2 cmax^2, cmax = max_j |c_j|
     int *labels;
     const int *labels_prev;
     int *flags;          // [0] labels changed
@@ -60,32 +60,76 @@ __device__ __forceinline__ void raise(int *abort_flag, int *err, int code) {
     atomicExch(err, code);
 }
 
-// Minimum of 32 accumulator values (a tree: one FMNMX per value, full ILP).
-__device__ __forceinline__ float chunk_min32(float (&v)[32]) {
-#pragma unroll
-    for (int w = 16; w >= 1; w >>= 1)
-#pragma unroll
-        for (int u = 0; u < w; ++u) v[u] = fminf(v[u], v[u + w]);
-    return v[0];
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
 }
-// Bit u set when v[u] <= tau: one FSET (all-ones / zero) and one LOP3 per value.
-__device__ __forceinline__ uint32_t le_mask32(const float (&v)[32], float tau) {
-    uint32_t bits = 0;
+// min(b, v[0..31]) with three-input minima (16 ALU instructions).
+__device__ __forceinline__ float chunk_min32(float b, const float (&v)[32]) {
+    float m[11];
 #pragma unroll
-    for (int u = 0; u < 32; ++u) {
-        uint32_t t;
-        asm("set.le.u32.f32 %0, %1, %2;" : "=r"(t) : "f"(v[u]), "f"(tau));
-        bits |= t & (1u << u);
-    }
-    return bits;
+    for (int i = 0; i < 10; ++i) m[i] = min3f(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+    m[10] = min3f(v[30], v[31], b);
+    const float a0 = min3f(m[0], m[1], m[2]), a1 = min3f(m[3], m[4], m[5]);
+    const float a2 = min3f(m[6], m[7], m[8]), a3 = fminf(m[9], m[10]);
+    return fminf(min3f(a0, a1, a2), a3);
 }
-__device__ __forceinline__ void collect_bits(uint32_t bits, int c, int *my, int &cnt) {
-    while (bits) {
-        const int u = __ffs(bits) - 1;
-        bits &= bits - 1;
-        if (cnt < TC_MAXC) my[cnt] = c * 32 + u;
-        ++cnt;
+__device__ __forceinline__ void mask_tail(float (&v)[32], int valid) {
+    if (valid < 32) {
+#pragma unroll
+        for (int u = 0; u < 32; ++u)
+            if (u >= valid) v[u] = __int_as_float(0x7f800000);
     }
+}
+// Exact 0/1 indicator of v < tau' on the FMA pipe: with S a power of two such
+// that |tau'| S lies in [2^25, 2^26), T = tau' S is exact and any v < tau'
+// gives (tau' - v) S >= 2 (float spacing near tau'), so the saturated fma is
+// exactly 1; v >= tau' (or NaN) gives 0.
+__device__ __forceinline__ float below_ind(float v, float negS, float T) {
+    float r;
+    asm("fma.rn.sat.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(v), "f"(negS), "f"(T));
+    return r;
+}
+
+// sum over u of below_ind(v[u]) * (4096 + u): four independent fma chains,
+// every partial sum an integer below 2^24 (exact).
+__device__ __forceinline__ float chunk_weight(const float (&v)[32], float negS, float T) {
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll
+    for (int u = 0; u < 32; u += 4) {
+        a0 = __fmaf_rn(below_ind(v[u], negS, T), (float)(4096 + u), a0);
+        a1 = __fmaf_rn(below_ind(v[u + 1], negS, T), (float)(4096 + u + 1), a1);
+        a2 = __fmaf_rn(below_ind(v[u + 2], negS, T), (float)(4096 + u + 2), a2);
+        a3 = __fmaf_rn(below_ind(v[u + 3], negS, T), (float)(4096 + u + 3), a3);
+    }
+    return (a0 + a1) + (a2 + a3);
+}
+
+// Account for one chunk's weighted count w = 4096 n + (sum of the n indices
+// within the chunk): a single candidate is recorded directly (index
+// 32 c + u); several (rare) are found from the chunk's values, still in
+// registers, with one compare per value.
+__device__ __forceinline__ void note_chunk(float w, const float (&v)[32], float tau, int c,
+                                           int *my, int &cnt, int &lab) {
+    const int iw = (int)w;
+    const int n = iw >> 12;
+    if (n == 1) {
+        lab = c * 32 + (iw & 4095);
+        if (cnt < TC_MAXC) my[cnt] = lab;
+    } else if (n > 1 && cnt < TC_MAXC) {
+        uint32_t bits = 0;
+#pragma unroll
+        for (int u = 0; u < 32; ++u) bits |= (v[u] < tau ? 1u : 0u) << u;
+        int m = cnt;
+        while (bits) {
+            const int u = __ffs(bits) - 1;
+            bits &= bits - 1;
+            if (m < TC_MAXC) my[m] = c * 32 + u;
+            ++m;
+        }
+    }
+    cnt += n;
 }
 
 template <int SPLIT>
@@ -230,7 +274,11 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
         const int row_in_tile = q * 32 + lane;
         const int nchunks = (a.npad + 31) / 32;
         const int tail = a.npad - (nchunks - 1) * 32; // valid columns of the last chunk
-        const float cmax = *a.cmax;
+        float cm = 0.f;
+        for (int j = lane; j < a.k; j += 32) cm = fmaxf(cm, a.cnorm[j]);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) cm = fmaxf(cm, __shfl_xor_sync(0xffffffffu, cm, off));
+        const float cmax = __fsqrt_rn(cm);
         const float inf = __int_as_float(0x7f800000);
         int *my = cand_s + threadIdx.x * TC_MAXC;
         int changed = 0;
@@ -246,37 +294,50 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
             const uint32_t trow = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * a.bufcols);
             const int r = t * TC_BM + row_in_tile;
             const float xn = r < a.n ? a.xnorm[r] : 0.f;
-            // pass 1: b1 = min_j v_j (tree minimum per 32 columns).  All lanes
-            // execute every tcgen05.ld (warp-synchronous); columns beyond npad
-            // in the last chunk are masked (warp-uniform branch).
+            // pass 1: b1 = min_j v_j.  All lanes execute every tcgen05.ld
+            // (warp-synchronous), two 32-column chunks per wait; columns
+            // beyond npad in the last chunk are masked (warp-uniform).
             float b1 = inf;
-            for (int c = 0; c < nchunks; ++c) {
-                float v[32];
-                tmem_ld32(trow + (uint32_t)(c * 32), v);
-                if (c == nchunks - 1 && tail < 32) {
-#pragma unroll
-                    for (int u = 0; u < 32; ++u)
-                        if (u >= tail) v[u] = inf;
+            for (int c = 0; c < nchunks; c += 2) {
+                float v0[32], v1[32];
+                tmem_ld64(trow + (uint32_t)(c * 32), c + 1 < nchunks, v0, v1);
+                mask_tail(v0, c == nchunks - 1 ? tail : 32);
+                b1 = chunk_min32(b1, v0);
+                if (c + 1 < nchunks) {
+                    mask_tail(v1, c + 1 == nchunks - 1 ? tail : 32);
+                    b1 = chunk_min32(b1, v1);
                 }
-                b1 = fminf(b1, chunk_min32(v));
             }
-            // pass 2: clusters within 2 eps of the minimum
+            // pass 2: the clusters with v_j < tau' (tau' = b1 + 2 eps, nudged
+            // up so the strict test keeps every v_j <= b1 + 2 eps), on the FMA
+            // pipe: per 32-column chunk a_c = sum over them of (4096 + u),
+            // exact in fp32, = 4096 n_c + (sum of their u) with that sum < 4096.
             const float eps = a.e1 * xn * cmax + a.e2 * cmax * cmax;
-            const float tau = b1 + 2.f * eps;
-            int cnt = 0;
-            for (int c = 0; c < nchunks; ++c) {
-                float v[32];
-                tmem_ld32(trow + (uint32_t)(c * 32), v);
-                uint32_t bits = le_mask32(v, tau);
-                if (c == nchunks - 1 && tail < 32) bits &= (1u << tail) - 1u;
-                collect_bits(bits, c, my, cnt);
+            const float tau0 = b1 + 2.f * eps;
+            const float taup = tau0 + fabsf(tau0) * 9.5367431640625e-7f + 1e-30f;
+            const int ex = (int)((__float_as_uint(taup) >> 23) & 0xFF) - 127;
+            const bool finite_tau = (ex > -90) && (ex < 100) && (taup == taup);
+            const int sexp = finite_tau ? 25 - ex : 0;
+            const float S = __int_as_float((uint32_t)(sexp + 127) << 23);
+            const float negS = -S, T = taup * S;
+            int cnt = 0, lab = -1;
+            for (int c = 0; c < nchunks; c += 2) {
+                float v0[32], v1[32];
+                tmem_ld64(trow + (uint32_t)(c * 32), c + 1 < nchunks, v0, v1);
+                mask_tail(v0, c == nchunks - 1 ? tail : 32);
+                note_chunk(chunk_weight(v0, negS, T), v0, taup, c, my, cnt, lab);
+                if (c + 1 < nchunks) {
+                    mask_tail(v1, c + 1 == nchunks - 1 ? tail : 32);
+                    note_chunk(chunk_weight(v1, negS, T), v1, taup, c + 1, my, cnt, lab);
+                }
             }
+            if (!finite_tau) cnt = 0;
             tc_fence_before();
             mbar_arrive(&sh->tempty[b]);
             const bool valid = r < a.n;
-            const bool certain = valid && cnt == 1 && tau <= 3.0e38f && my[0] < a.k;
+            const bool certain = valid && cnt == 1 && lab >= 0 && lab < a.k;
             if (certain) {
-                const int lbl = my[0];
+                const int lbl = lab;
                 a.labels[r] = lbl;
                 if (a.labels_prev && a.labels_prev[r] != lbl) changed = 1;
             }
@@ -290,8 +351,10 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
                 if (amb) {
                     const int pos = base0 + __popc(mask & ((1u << lane) - 1u));
                     a.amb_rows[pos] = r;
-                    bool okc = cnt >= 2 && cnt <= TC_MAXC && tau <= 3.0e38f;
-                    for (int e = 0; e < cnt && e < TC_MAXC; ++e) okc = okc && my[e] < a.k;
+                    // candidate list, or 0: exact scan of every cluster
+                    bool okc = cnt >= 2 && cnt <= TC_MAXC;
+                    for (int e = 0; e < TC_MAXC; ++e)
+                        if (e < cnt) okc = okc && my[e] >= 0 && my[e] < a.k;
                     const int nc = okc ? cnt : 0;
                     a.amb_ncand[pos] = nc;
                     for (int e = 0; e < nc; ++e) a.amb_cand[pos * TC_MAXC + e] = my[e];
@@ -310,89 +373,180 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
 }
 
 // Exact fp32 relabelling of the uncertified rows: the plain path's formula
-// fl(|c|^2 - 2 x.c) with the dot product as one fma chain over the features,
-// evaluated for the listed candidates (every cluster when the list
-// overflowed); ties -> lower index.  One thread per listed row; the centres
-// are staged in shared memory (rows padded to d+1 floats).
+// fl(|c|^2 - 2 x.c), the dot product as one sequential fma chain over the
+// features (exactly the plain path's order); ties -> lower index.  Each warp
+// takes 32 listed rows and stages them in shared memory (coalesced; rows
+// padded to dp floats so that per-lane row reads do not conflict).  A row with
+// a candidate list (2..TC_MAXC clusters) is re-scored by its lane over those
+// clusters only; rows listed without candidates are then scanned over every
+// cluster by the whole warp (lanes over clusters, the row broadcast).  The
+// centres are staged once per block in shared memory (same padding) when
+// they fit, else read from global memory.  VEC: d, ld and dp multiples of 4
+// (16-byte rows), read as float4.
+template <bool VEC>
 __global__ void __launch_bounds__(256)
-kmeans_rescore_kernel(const float *X, int ld, int d, const float *C, int k,
+kmeans_rescore_kernel(const float *X, int ld, int d, int dp, const float *C, int k,
                       const float *cnorm, const int *amb_rows, const int *amb_cand,
                       const int *amb_ncand, const int *amb_count, int *labels,
                       const int *labels_prev, int *flags, int c_in_smem) {
-    extern __shared__ float rs_smem[];
-    const int dp = d + 1;
-    float *cs = rs_smem; // k x dp (when c_in_smem)
+    extern __shared__ __align__(16) float rs_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwb = blockDim.x >> 5;
+    float *cs = rs_smem;
+    float *xw = rs_smem + (c_in_smem ? (size_t)k * dp : 0) + (size_t)warp * 32 * dp;
     const int cnt = *amb_count;
     if (cnt == 0) return;
     if (c_in_smem) {
-        for (int e = threadIdx.x; e < k * d; e += blockDim.x) {
-            const int j = e / d, f = e - j * d;
-            cs[j * dp + f] = C[(size_t)j * ld + f];
+        if (VEC) {
+            const int q4 = d >> 2;
+            for (int e = threadIdx.x; e < k * q4; e += blockDim.x) {
+                const int j = e / q4, f4 = e - j * q4;
+                *reinterpret_cast<float4 *>(cs + (size_t)j * dp + 4 * f4) =
+                    *reinterpret_cast<const float4 *>(C + (size_t)j * ld + 4 * f4);
+            }
+        } else {
+            for (int e = threadIdx.x; e < k * d; e += blockDim.x) {
+                const int j = e / d, f = e - j * d;
+                cs[(size_t)j * dp + f] = C[(size_t)j * ld + f];
+            }
         }
         __syncthreads();
     }
+    const float *cbase = c_in_smem ? cs : C;
+    const int cst = c_in_smem ? dp : ld;
+    const float inf = __int_as_float(0x7f800000);
     int changed = 0;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += gridDim.x * blockDim.x) {
-        const int r = amb_rows[e];
-        const float *x = X + (size_t)r * ld;
-        const int nc = amb_ncand[e];
-        float best = __int_as_float(0x7f800000);
-        int bi = 0x7fffffff;
-        if (nc > 0) {
-            // up to TC_MAXC candidates: x streamed once in 16-float chunks,
-            // each candidate's dot kept as its own sequential fma chain
-            int jj[TC_MAXC];
-            float sd[TC_MAXC];
-#pragma unroll
-            for (int u = 0; u < TC_MAXC; ++u) {
-                jj[u] = u < nc ? amb_cand[e * TC_MAXC + u] : amb_cand[e * TC_MAXC];
-                sd[u] = 0.f;
-            }
-            for (int f0 = 0; f0 < d; f0 += 16) {
-                float xv[16];
-#pragma unroll
-                for (int q = 0; q < 16; q += 4) {
-                    if (f0 + q < ld) {
-                        const float4 t = __ldg(reinterpret_cast<const float4 *>(x + f0 + q));
-                        xv[q] = t.x; xv[q + 1] = t.y; xv[q + 2] = t.z; xv[q + 3] = t.w;
-                    } else {
-                        xv[q] = xv[q + 1] = xv[q + 2] = xv[q + 3] = 0.f;
-                    }
-                }
-                const int fe = min(16, d - f0);
-#pragma unroll
-                for (int u = 0; u < TC_MAXC; ++u) {
-                    const float *c = c_in_smem ? cs + jj[u] * dp : C + (size_t)jj[u] * ld;
-                    for (int q = 0; q < fe; ++q) sd[u] = __fmaf_rn(xv[q], c[f0 + q], sd[u]);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < TC_MAXC; ++u) {
-                if (u < nc) {
-                    const float v = __fmaf_rn(-2.f, sd[u], cnorm[jj[u]]);
-                    if (key_less(v, jj[u], best, bi)) {
-                        best = v;
-                        bi = jj[u];
-                    }
-                }
+    const int nw = gridDim.x * nwb;
+    for (int e0 = (blockIdx.x * nwb + warp) * 32; e0 < cnt; e0 += nw * 32) {
+        const int e = e0 + lane;
+        const int nc = e < cnt ? amb_ncand[e] : -1;
+        const int r = e < cnt ? amb_rows[e] : 0;
+        const int nrows = min(32, cnt - e0);
+        __syncwarp();
+        if (VEC) {
+            const int q4 = d >> 2;
+            for (int t = lane; t < nrows * q4; t += 32) {
+                const int i = t / q4, f4 = t - i * q4;
+                const int ri = amb_rows[e0 + i];
+                *reinterpret_cast<float4 *>(xw + (size_t)i * dp + 4 * f4) =
+                    *reinterpret_cast<const float4 *>(X + (size_t)ri * ld + 4 * f4);
             }
         } else {
-            for (int j = 0; j < k; ++j) {
-                const float *c = c_in_smem ? cs + j * dp : C + (size_t)j * ld;
-                float sdot = 0.f;
-                for (int f = 0; f < d; ++f) sdot = __fmaf_rn(x[f], c[f], sdot);
-                const float v = __fmaf_rn(-2.f, sdot, cnorm[j]);
-                if (key_less(v, j, best, bi)) {
-                    best = v;
-                    bi = j;
-                }
+            for (int t = lane; t < nrows * d; t += 32) {
+                const int i = t / d, f = t - i * d;
+                xw[(size_t)i * dp + f] = X[(size_t)amb_rows[e0 + i] * ld + f];
             }
         }
-        const int lbl = (bi == 0x7fffffff) ? 0 : bi;
-        labels[r] = lbl;
-        if (labels_prev && labels_prev[r] != lbl) changed = 1;
+        __syncwarp();
+        if (nc > 0) {
+            int cj[TC_MAXC];
+            const float *cp[TC_MAXC];
+            float sd[TC_MAXC];
+#pragma unroll
+            for (int q = 0; q < TC_MAXC; ++q) {
+                cj[q] = amb_cand[(size_t)e * TC_MAXC + (q < nc ? q : 0)];
+                cp[q] = cbase + (size_t)cj[q] * cst;
+                sd[q] = 0.f;
+            }
+            const float *xr = xw + (size_t)lane * dp;
+            if (VEC) {
+                for (int f = 0; f < d; f += 4) {
+                    const float4 xv = *reinterpret_cast<const float4 *>(xr + f);
+#pragma unroll
+                    for (int q = 0; q < TC_MAXC; ++q) {
+                        const float4 cv = *reinterpret_cast<const float4 *>(cp[q] + f);
+                        sd[q] = __fmaf_rn(xv.x, cv.x, sd[q]);
+                        sd[q] = __fmaf_rn(xv.y, cv.y, sd[q]);
+                        sd[q] = __fmaf_rn(xv.z, cv.z, sd[q]);
+                        sd[q] = __fmaf_rn(xv.w, cv.w, sd[q]);
+                    }
+                }
+            } else {
+                for (int f = 0; f < d; ++f) {
+                    const float xf = xr[f];
+#pragma unroll
+                    for (int q = 0; q < TC_MAXC; ++q) sd[q] = __fmaf_rn(xf, cp[q][f], sd[q]);
+                }
+            }
+            float best = inf;
+            int bi = 0x7fffffff;
+#pragma unroll
+            for (int q = 0; q < TC_MAXC; ++q) {
+                if (q < nc) {
+                    const float v = __fmaf_rn(-2.f, sd[q], cnorm[cj[q]]);
+                    if (key_less(v, cj[q], best, bi)) {
+                        best = v;
+                        bi = cj[q];
+                    }
+                }
+            }
+            const int lbl = (bi == 0x7fffffff) ? cj[0] : bi;
+            labels[r] = lbl;
+            if (labels_prev && labels_prev[r] != lbl) changed = 1;
+        }
+        unsigned full = __ballot_sync(0xffffffffu, nc == 0);
+        while (full) {
+            const int src = __ffs(full) - 1;
+            full &= full - 1;
+            const float *xr = xw + (size_t)src * dp;
+            float best = inf;
+            int bi = 0x7fffffff;
+            // four clusters per lane at a time (independent fma chains)
+            for (int j0 = lane; j0 < k; j0 += 128) {
+                const float *c[4];
+                float sd[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const int j = min(j0 + 32 * t, k - 1);
+                    c[t] = cbase + (size_t)j * cst;
+                }
+                if (VEC) {
+                    for (int f = 0; f < d; f += 4) {
+                        const float4 xv = *reinterpret_cast<const float4 *>(xr + f);
+#pragma unroll
+                        for (int t = 0; t < 4; ++t) {
+                            const float4 cv = *reinterpret_cast<const float4 *>(c[t] + f);
+                            sd[t] = __fmaf_rn(xv.x, cv.x, sd[t]);
+                            sd[t] = __fmaf_rn(xv.y, cv.y, sd[t]);
+                            sd[t] = __fmaf_rn(xv.z, cv.z, sd[t]);
+                            sd[t] = __fmaf_rn(xv.w, cv.w, sd[t]);
+                        }
+                    }
+                } else {
+                    for (int f = 0; f < d; ++f) {
+                        const float xf = xr[f];
+#pragma unroll
+                        for (int t = 0; t < 4; ++t) sd[t] = __fmaf_rn(xf, c[t][f], sd[t]);
+                    }
+                }
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const int j = j0 + 32 * t;
+                    if (j < k) {
+                        const float v = __fmaf_rn(-2.f, sd[t], cnorm[j]);
+                        if (key_less(v, j, best, bi)) {
+                            best = v;
+                            bi = j;
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const float ov = __shfl_xor_sync(0xffffffffu, best, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                if (key_less(ov, oi, best, bi)) {
+                    best = ov;
+                    bi = oi;
+                }
+            }
+            if (lane == src) {
+                const int lbl = (bi == 0x7fffffff) ? 0 : bi;
+                labels[r] = lbl;
+                if (labels_prev && labels_prev[r] != lbl) changed = 1;
+            }
+        }
     }
-    if (changed && flags) atomicOr(&flags[0], 1);
+    if (__any_sync(0xffffffffu, changed) && lane == 0 && flags) atomicOr(&flags[0], 1);
 }
 
 // X (fp32, ld) -> Xh = bf16(x), Xl = bf16(x - Xh) (row-major, ldo), zero pad.
@@ -548,23 +702,49 @@ cudaError_t launch_row_norm_max(const float *X, int ld, int rows, int d, float *
 cudaError_t launch_kmeans_assign_tc(int split, const void *Xh, const void *Xl, int n, int ldbf,
                                     const void *Bh, const void *Bl, const void *Baug,
                                     const void *Aaug, int k, const float *xnorm,
-                                    const float *cmax, int *labels, const int *labels_prev,
+                                    const float *cnorm, int *labels, const int *labels_prev,
                                     int *flags, int *amb_rows, int *amb_cand, int *amb_ncand,
                                     int *amb_count, int *err, cudaStream_t s) {
     const int nkb = ldbf / TC_KB;
     const int npad = (k + 15) & ~15;
-    CUtensorMap mxh, mxl, mbh, mbl, mbaug, maaug;
     const bool s3 = split == 3;
-    if (!make_map_bf16(&mxh, Xh, n, ldbf, TC_BM) || !make_map_bf16(&mbh, Bh, npad, ldbf, npad) ||
-        !make_map_bf16(&mbaug, Baug, npad, TC_KB, npad) ||
-        !make_map_bf16(&maaug, Aaug, TC_BM, TC_KB, TC_BM))
-        return cudaErrorInvalidValue;
-    if (s3) {
-        if (!make_map_bf16(&mxl, Xl, n, ldbf, TC_BM) || !make_map_bf16(&mbl, Bl, npad, ldbf, npad))
+    int dev = 0;
+    cudaGetDevice(&dev);
+    // The tensor maps depend only on the buffers and shapes, which stay the
+    // same over the iterations of a fit: encode them once per configuration.
+    struct MapCache {
+        const void *p[6];
+        int n, ldbf, k, split, dev;
+        CUtensorMap m[6];
+        bool ok;
+    };
+    thread_local MapCache mc = {{nullptr}, -1, -1, -1, -1, -1, {}, false};
+    const void *ptrs[6] = {Xh, Xl, Bh, Bl, Baug, Aaug};
+    bool hit = mc.ok && mc.n == n && mc.ldbf == ldbf && mc.k == k && mc.split == split &&
+               mc.dev == dev;
+    for (int i = 0; i < 6 && hit; ++i) hit = mc.p[i] == ptrs[i];
+    if (!hit) {
+        mc.ok = false;
+        if (!make_map_bf16(&mc.m[0], Xh, n, ldbf, TC_BM) ||
+            !make_map_bf16(&mc.m[2], Bh, npad, ldbf, npad) ||
+            !make_map_bf16(&mc.m[4], Baug, npad, TC_KB, npad) ||
+            !make_map_bf16(&mc.m[5], Aaug, TC_BM, TC_KB, TC_BM))
             return cudaErrorInvalidValue;
-    } else {
-        mxl = mxh;
-        mbl = mbh;
+        if (s3) {
+            if (!make_map_bf16(&mc.m[1], Xl, n, ldbf, TC_BM) ||
+                !make_map_bf16(&mc.m[3], Bl, npad, ldbf, npad))
+                return cudaErrorInvalidValue;
+        } else {
+            mc.m[1] = mc.m[0];
+            mc.m[3] = mc.m[2];
+        }
+        for (int i = 0; i < 6; ++i) mc.p[i] = ptrs[i];
+        mc.n = n;
+        mc.ldbf = ldbf;
+        mc.k = k;
+        mc.split = split;
+        mc.dev = dev;
+        mc.ok = true;
     }
     const int stages = tc_stages(split, nkb, npad);
     const size_t smem = tc_smem_bytes(split, nkb, npad, stages);
@@ -591,7 +771,7 @@ cudaError_t launch_kmeans_assign_tc(int split, const void *Xh, const void *Xl, i
     a.stages = stages;
     a.bufcols = bufcols;
     a.xnorm = xnorm;
-    a.cmax = cmax;
+    a.cnorm = cnorm;
     a.e1 = (float)e1;
     a.e2 = (float)e2;
     a.labels = labels;
@@ -603,15 +783,19 @@ cudaError_t launch_kmeans_assign_tc(int split, const void *Xh, const void *Xl, i
     a.amb_count = amb_count;
     a.err = err;
     auto kern = s3 ? kmeans_assign_tc_kernel<3> : kmeans_assign_tc_kernel<1>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
+    thread_local int smem_set[2][16] = {};
+    int *set = (dev >= 0 && dev < 16) ? &smem_set[s3 ? 1 : 0][dev] : nullptr;
+    if (!set || *set < (int)smem) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        if (set) *set = (int)smem;
+    }
     const int ntiles = (n + TC_BM - 1) / TC_BM;
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
+    int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const int grid = ntiles < nsm ? ntiles : nsm;
-    kern<<<grid, TC_THREADS, smem, s>>>(mxh, mxl, mbh, mbl, mbaug, maaug, a);
+    kern<<<grid, TC_THREADS, smem, s>>>(mc.m[0], mc.m[1], mc.m[2], mc.m[3], mc.m[4], mc.m[5], a);
     return cudaGetLastError();
 }
 
@@ -621,17 +805,42 @@ cudaError_t launch_kmeans_rescore(const float *X, int ld, int d, const float *C,
                                   int *labels, const int *labels_prev, int *flags,
                                   cudaStream_t s) {
     if (max_rows <= 0) return cudaSuccess;
-    const size_t cs_bytes = (size_t)k * (d + 1) * 4;
-    const int c_in_smem = (cs_bytes <= 200 * 1024) ? 1 : 0;
-    const size_t smem = c_in_smem ? cs_bytes : 0;
-    if (smem > 220 * 1024) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(kmeans_rescore_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    const int blocks = min(148 * 2, (max_rows + 255) / 256);
-    kmeans_rescore_kernel<<<blocks, 256, smem, s>>>(X, ld, d, C, k, cnorm, amb_rows, amb_cand,
-                                                    amb_ncand, amb_count, labels, labels_prev,
-                                                    flags, c_in_smem);
+    const bool vec = (d % 4 == 0) && (ld % 4 == 0) &&
+                     ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(C)) & 15) == 0;
+    // padded row length: an odd number of 16-byte (VEC) or 4-byte words
+    const int dp = vec ? ((d / 4) % 2 == 1 ? d : d + 4) : (d | 1);
+    const size_t limit = 220 * 1024;
+    const size_t cs_bytes = (size_t)k * dp * 4, xw_bytes = (size_t)32 * dp * 4;
+    int warps = 8, c_in_smem = 1;
+    while (warps > 1 && cs_bytes + warps * xw_bytes > limit) warps >>= 1;
+    if (cs_bytes + warps * xw_bytes > limit) {
+        c_in_smem = 0;
+        warps = 8;
+        while (warps > 1 && warps * xw_bytes > limit) warps >>= 1;
+        if (warps * xw_bytes > limit) return cudaErrorInvalidValue;
+    }
+    const size_t smem = (c_in_smem ? cs_bytes : 0) + warps * xw_bytes;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int per_sm = max(1, (int)(228 * 1024 / (smem + 1024)));
+    const int blocks = max(1, min(nsm * per_sm, (max_rows + 32 * warps - 1) / (32 * warps)));
+    cudaError_t e;
+    if (vec) {
+        e = cudaFuncSetAttribute(kmeans_rescore_kernel<true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kmeans_rescore_kernel<true><<<blocks, 32 * warps, smem, s>>>(
+            X, ld, d, dp, C, k, cnorm, amb_rows, amb_cand, amb_ncand, amb_count, labels,
+            labels_prev, flags, c_in_smem);
+    } else {
+        e = cudaFuncSetAttribute(kmeans_rescore_kernel<false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kmeans_rescore_kernel<false><<<blocks, 32 * warps, smem, s>>>(
+            X, ld, d, dp, C, k, cnorm, amb_rows, amb_cand, amb_ncand, amb_count, labels,
+            labels_prev, flags, c_in_smem);
+    }
     return cudaGetLastError();
 }
 

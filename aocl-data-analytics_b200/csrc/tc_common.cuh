@@ -140,6 +140,32 @@ __device__ __forceinline__ void tmem_ld_wait(uint32_t (&r)[32]) {
                  : "memory");
 }
 
+// Two 32-column loads (the second only when `two`, a warp-uniform flag)
+// completed by a single wait.  The empty asm after the wait ties the second
+// array's registers to it, so no use of them is scheduled before the wait.
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, bool two, float (&v0)[32],
+                                          float (&v1)[32]) {
+    uint32_t r0[32], r1[32];
+    tmem_ld32_issue(taddr, r0);
+    if (two) tmem_ld32_issue(taddr + 32u, r1);
+    tmem_ld_wait(r0);
+    asm volatile(""
+                 : "+r"(r1[0]), "+r"(r1[1]), "+r"(r1[2]), "+r"(r1[3]), "+r"(r1[4]), "+r"(r1[5]),
+                   "+r"(r1[6]), "+r"(r1[7]), "+r"(r1[8]), "+r"(r1[9]), "+r"(r1[10]),
+                   "+r"(r1[11]), "+r"(r1[12]), "+r"(r1[13]), "+r"(r1[14]), "+r"(r1[15]),
+                   "+r"(r1[16]), "+r"(r1[17]), "+r"(r1[18]), "+r"(r1[19]), "+r"(r1[20]),
+                   "+r"(r1[21]), "+r"(r1[22]), "+r"(r1[23]), "+r"(r1[24]), "+r"(r1[25]),
+                   "+r"(r1[26]), "+r"(r1[27]), "+r"(r1[28]), "+r"(r1[29]), "+r"(r1[30]),
+                   "+r"(r1[31])
+                 :
+                 : "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        v0[i] = __uint_as_float(r0[i]);
+        v1[i] = __uint_as_float(r1[i]);
+    }
+}
+
 // Shared-memory matrix descriptor: K-major operand, 128-byte swizzle, rows of
 // 128 bytes in 8-row (1024-byte) atoms (SBO = 1024 B, LBO unused = 16 B).
 __device__ __forceinline__ uint64_t desc_k_sw128(uint32_t smem_addr) {
