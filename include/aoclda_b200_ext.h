@@ -42,6 +42,33 @@ da_status da_b200_get_stat(da_handle handle, const char *name, double *value);
 da_status da_b200_kmeans_init_centres_d(da_handle handle, double *C, da_int ldc);
 da_status da_b200_kmeans_init_centres_s(da_handle handle, float *C, da_int ldc);
 
+/* No counterpart in the AOCL-DA API.  Brute-force euclidean k nearest
+ * neighbours for callers that cannot allocate device memory (code running
+ * inside a device allocator or memory-pool callback, real-time pipelines that
+ * forbid allocation after start-up, hosts whose device memory another
+ * framework has reserved).  It allocates nothing: its working memory is one
+ * fixed array of DA_B200_KNN_NOALLOC_SCRATCH_BYTES in the library's device
+ * code, held on every GPU that loads the library until the process exits.
+ *
+ * X (n x d), Q (nq x d): row-major fp32 device arrays with the same leading
+ * dimension ld (a multiple of 4, ld >= d), 16-byte aligned, each holding
+ * rows x ld elements.  Results, on the device: dist (nq x k, row-major) and
+ * ind (nq x k, 0-based training-row indices), the same neighbours and
+ * distances, bit for bit, as da_nn_kneighbors_s with metric "euclidean" on
+ * row-major data; ties between equal distances go to the lower index.
+ * 1 <= k <= min(n, 256).  nq * k * 8 + 256 bytes must fit in the scratch
+ * array (else da_status_invalid_array_dimension).
+ *
+ * The work is enqueued on `stream` (a cudaStream_t; NULL = legacy default
+ * stream) and the call returns without waiting for it.  The first call on a
+ * device looks up the scratch array's address; make it before any stream
+ * capture on that device.  Calls share the scratch array: calls whose work
+ * overlaps on the GPU race on it. */
+#define DA_B200_KNN_NOALLOC_SCRATCH_BYTES (32u << 20)
+da_status da_b200_knn_euclidean_noalloc_s(const float *X, da_int n, const float *Q, da_int nq,
+                                          da_int d, da_int ld, da_int k, float *dist,
+                                          da_int *ind, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
