@@ -29,7 +29,8 @@ using namespace tc;
 
 static constexpr int TC_BM = 128;       // rows per tile (UMMA M)
 static constexpr int TC_KB = 64;        // bf16 elements per 128-byte K block
-static constexpr int TC_THREADS = 320;  // 10 warps
+static constexpr int TC_EPI_WARPS = 16; // 2 accumulators x 2 column halves x 4 lane quarters
+static constexpr int TC_THREADS = 64 + 32 * TC_EPI_WARPS; // + producer and MMA warps
 static constexpr int TC_MAXC = 4;       // candidates kept per uncertified row
 
 struct TcAssignArgs {
@@ -75,6 +76,11 @@ __device__ __forceinline__ float chunk_min32(float b, const float (&v)[32]) {
     const float a2 = min3f(m[6], m[7], m[8]), a3 = fminf(m[9], m[10]);
     return fminf(min3f(a0, a1, a2), a3);
 }
+// Named barrier of `count` threads (whole warps).
+__device__ __forceinline__ void named_bar_sync(int id, int count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
 __device__ __forceinline__ void mask_tail(float (&v)[32], int valid) {
     if (valid < 32) {
 #pragma unroll
@@ -154,6 +160,10 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
     unsigned char *As = Aaug + a_bytes;                                // S stages
     TcShared *sh = reinterpret_cast<TcShared *>(As + (size_t)S * NX * nkb * a_bytes);
     int *cand_s = reinterpret_cast<int *>(sh + 1); // [TC_THREADS][TC_MAXC]
+    float *xb1 = reinterpret_cast<float *>(cand_s + TC_THREADS * TC_MAXC); // pair exchange
+    int *xcnt = reinterpret_cast<int *>(xb1 + TC_THREADS);
+    int *xlab = xcnt + TC_THREADS;
+    int *xok = xlab + TC_THREADS;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ntiles = (a.n + TC_BM - 1) / TC_BM;
@@ -165,7 +175,7 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&sh->tfull[b], 1);
-            mbar_init(&sh->tempty[b], 128);
+            mbar_init(&sh->tempty[b], 8 * 32);
         }
         mbar_init(&sh->bfull, 1);
         sh->abort_flag = 0;
@@ -269,11 +279,21 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
         }
     } else {
         // ------------------------------------------------ epilogue --------
-        const int g = (warp - 2) / 4;      // accumulator / tile parity
-        const int q = warp & 3;            // TMEM lane quarter of this warp
+        // 16 warps: accumulator (tile parity) g, column half h, TMEM lane
+        // quarter q.  The two warps of a (g, q) pair read the same 32 rows,
+        // one half of the columns each, and exchange per-row results through
+        // shared memory at a named barrier of the pair.
+        const int e = warp - 2;
+        const int g = e >> 3;
+        const int h = (e >> 2) & 1;
+        const int q = warp & 3;
+        const int partner = (int)threadIdx.x + (h == 0 ? 128 : -128);
+        const int bar_id = 1 + g * 4 + q;
         const int row_in_tile = q * 32 + lane;
         const int nchunks = (a.npad + 31) / 32;
         const int tail = a.npad - (nchunks - 1) * 32; // valid columns of the last chunk
+        const int c_lo = h == 0 ? 0 : (nchunks + 1) / 2;
+        const int c_hi = h == 0 ? (nchunks + 1) / 2 : nchunks;
         float cm = 0.f;
         for (int j = lane; j < a.k; j += 32) cm = fmaxf(cm, a.cnorm[j]);
 #pragma unroll
@@ -285,29 +305,32 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
         int it = g;
         for (int t = blockIdx.x + g * gridDim.x; t < ntiles; t += 2 * gridDim.x, it += 2) {
             const int b = g;
-            if (!mbar_wait(&sh->tfull[b], (uint32_t)((it >> 1) & 1))) {
-                raise(&sh->abort_flag, a.err, 5);
-                break;
-            }
-            if (*((volatile int *)&sh->abort_flag)) break;
-            tc_fence_after();
+            bool ok = mbar_wait(&sh->tfull[b], (uint32_t)((it >> 1) & 1));
+            if (!ok) raise(&sh->abort_flag, a.err, 5);
+            ok = ok && !*((volatile int *)&sh->abort_flag);
+            ok = __all_sync(0xffffffffu, ok); // warp-uniform from here on
             const uint32_t trow = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * a.bufcols);
             const int r = t * TC_BM + row_in_tile;
             const float xn = r < a.n ? a.xnorm[r] : 0.f;
-            // pass 1: b1 = min_j v_j.  All lanes execute every tcgen05.ld
-            // (warp-synchronous), two 32-column chunks per wait; columns
-            // beyond npad in the last chunk are masked (warp-uniform).
+            // pass 1: this half's min_j v_j.  All lanes execute every
+            // tcgen05.ld (warp-synchronous); columns beyond npad in the last
+            // chunk are masked (warp-uniform).
             float b1 = inf;
-            for (int c = 0; c < nchunks; c += 2) {
-                float v0[32], v1[32];
-                tmem_ld64(trow + (uint32_t)(c * 32), c + 1 < nchunks, v0, v1);
-                mask_tail(v0, c == nchunks - 1 ? tail : 32);
-                b1 = chunk_min32(b1, v0);
-                if (c + 1 < nchunks) {
-                    mask_tail(v1, c + 1 == nchunks - 1 ? tail : 32);
-                    b1 = chunk_min32(b1, v1);
+            if (ok) {
+                tc_fence_after();
+                for (int c = c_lo; c < c_hi; ++c) {
+                    float v[32];
+                    tmem_ld32(trow + (uint32_t)(c * 32), v);
+                    mask_tail(v, c == nchunks - 1 ? tail : 32);
+                    b1 = chunk_min32(b1, v);
                 }
             }
+            xb1[threadIdx.x] = b1;
+            xok[threadIdx.x] = ok ? 1 : 0;
+            named_bar_sync(bar_id, 64);
+            // both warps of the pair see the same two flags: they stop together
+            if (!(ok && xok[partner])) break;
+            b1 = fminf(b1, xb1[partner]);
             // pass 2: the clusters with v_j < tau' (tau' = b1 + 2 eps, nudged
             // up so the strict test keeps every v_j <= b1 + 2 eps), on the FMA
             // pipe: per 32-column chunk a_c = sum over them of (4096 + u),
@@ -321,19 +344,25 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
             const float S = __int_as_float((uint32_t)(sexp + 127) << 23);
             const float negS = -S, T = taup * S;
             int cnt = 0, lab = -1;
-            for (int c = 0; c < nchunks; c += 2) {
-                float v0[32], v1[32];
-                tmem_ld64(trow + (uint32_t)(c * 32), c + 1 < nchunks, v0, v1);
-                mask_tail(v0, c == nchunks - 1 ? tail : 32);
-                note_chunk(chunk_weight(v0, negS, T), v0, taup, c, my, cnt, lab);
-                if (c + 1 < nchunks) {
-                    mask_tail(v1, c + 1 == nchunks - 1 ? tail : 32);
-                    note_chunk(chunk_weight(v1, negS, T), v1, taup, c + 1, my, cnt, lab);
-                }
+            for (int c = c_lo; c < c_hi; ++c) {
+                float v[32];
+                tmem_ld32(trow + (uint32_t)(c * 32), v);
+                mask_tail(v, c == nchunks - 1 ? tail : 32);
+                note_chunk(chunk_weight(v, negS, T), v, taup, c, my, cnt, lab);
             }
-            if (!finite_tau) cnt = 0;
+            xcnt[threadIdx.x] = cnt;
+            xlab[threadIdx.x] = lab;
             tc_fence_before();
             mbar_arrive(&sh->tempty[b]);
+            named_bar_sync(bar_id, 64);
+            if (h != 0) continue;
+            // merge the two halves (the h = 0 warp writes the results)
+            const int cnt1 = xcnt[partner];
+            const int *my1 = cand_s + partner * TC_MAXC;
+            if (cnt == 0 && cnt1 == 1) lab = xlab[partner];
+            for (int u = 0; u < TC_MAXC; ++u)
+                if (u < cnt1 && cnt + u < TC_MAXC) my[cnt + u] = my1[u];
+            cnt = finite_tau ? cnt + cnt1 : 0;
             const bool valid = r < a.n;
             const bool certain = valid && cnt == 1 && lab >= 0 && lab < a.k;
             if (certain) {
@@ -353,11 +382,11 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
                     a.amb_rows[pos] = r;
                     // candidate list, or 0: exact scan of every cluster
                     bool okc = cnt >= 2 && cnt <= TC_MAXC;
-                    for (int e = 0; e < TC_MAXC; ++e)
-                        if (e < cnt) okc = okc && my[e] >= 0 && my[e] < a.k;
+                    for (int u = 0; u < TC_MAXC; ++u)
+                        if (u < cnt) okc = okc && my[u] >= 0 && my[u] < a.k;
                     const int nc = okc ? cnt : 0;
                     a.amb_ncand[pos] = nc;
-                    for (int e = 0; e < nc; ++e) a.amb_cand[pos * TC_MAXC + e] = my[e];
+                    for (int u = 0; u < nc; ++u) a.amb_cand[pos * TC_MAXC + u] = my[u];
                 }
             }
         }
@@ -651,7 +680,7 @@ static size_t tc_smem_bytes(int split, int nkb, int npad, int stages) {
     const int nx = split == 3 ? 2 : 1;
     return 1024 + (size_t)(nx * nkb + 1) * npad * 128 + (size_t)TC_BM * 128 +
            (size_t)stages * nx * nkb * TC_BM * 128 + sizeof(TcShared) +
-           (size_t)TC_THREADS * TC_MAXC * 4 + 64;
+           (size_t)TC_THREADS * (TC_MAXC + 4) * 4 + 64;
 }
 static int tc_stages(int split, int nkb, int npad) {
     int s = 6;
