@@ -489,7 +489,7 @@ template <typename T> da_status KMeans<T>::assign(const T *dC, int *dL, const in
                                          s3 ? dBl.p : nullptr, dBaug.p,
                                          aaug_ready ? nullptr : dAaug.p, st), "centre operands");
             aaug_ready = true;
-            B200_TRY(cudaMemsetAsync(amb_cnt, 0, sizeof(int), st), "memset");
+            B200_TRY(cudaMemsetAsync(amb_cnt, 0, 3 * sizeof(int), st), "memset");
             B200_TRY(cuda->timed("kmeans_assign", [&] {
                 return launch_kmeans_assign_tc(tc_split, dXh.p, s3 ? dXl.p : nullptr, n, ldbf,
                                                dBh.p, s3 ? dBl.p : nullptr, dBaug.p, dAaug.p, k,
@@ -558,15 +558,16 @@ da_status KMeans<T>::lloyd_step(const T *dCprev, T *dCnew, int *dL, const int *d
         B200_TRY(cudaMemcpyAsync(h_flags, dFlags.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st),
                  "copy");
     }
-    int tc_state[2] = {0, 0};
+    int tc_state[3] = {0, 0, 0};
     if (use_tc)
-        B200_TRY(cudaMemcpyAsync(tc_state, dTcScal.as<char>() + 16, 2 * sizeof(int),
+        B200_TRY(cudaMemcpyAsync(tc_state, dTcScal.as<char>() + 16, 3 * sizeof(int),
                                  cudaMemcpyDeviceToHost, st), "copy");
     B200_TRY(cudaStreamSynchronize(st), "Lloyd iteration");
     (void)d;
     if (use_tc) {
         amb_last = tc_state[0];
         cuda->stats["relabelled_rows"] = (double)amb_last;
+        cuda->stats["full_scan_rows"] = (double)tc_state[2];
         if (tc_state[1] != 0)
             return err->error(da_status_internal_error,
                               "The tensor-core assignment kernel timed out waiting on a "

@@ -497,11 +497,12 @@ B200_KM_INST(double)
 namespace {
 constexpr int FX_SMEM_LIMIT = 200 * 1024;
 constexpr int FX_THREADS = 1024;
-constexpr int FX_ROWS = 8; // rows in flight per warp
+constexpr int FX_ROWS = 8;     // rows in flight per warp
+constexpr int FX_BATCH = 8192; // rows sorted by label per pass of a CTA
 } // namespace
 
 size_t fx_update_smem(int k, int d) {
-    return (size_t)k * d * 8 + (size_t)k * 4 + (size_t)d * 4;
+    return (size_t)k * d * 8 + (size_t)FX_BATCH * 4 + (size_t)(2 * k + 2) * 4 + (size_t)d * 4;
 }
 int fx_update_supported(int k, int d) { return fx_update_smem(k, d) <= FX_SMEM_LIMIT ? 1 : 0; }
 
@@ -560,70 +561,122 @@ __device__ __forceinline__ void fx_add(unsigned long long *acc, long long q) {
     atomicAdd(w + 1, h + (o + l < o ? 1u : 0u));
 }
 
-// One CTA per SM, each over a contiguous range of rows: warp per row (lanes
-// over feature pairs when VEC2), FX_ROWS rows in flight; integer atomics into
-// shared memory; the CTA's sums and counts are then added (integer
-// reductions, so the order of the CTAs does not matter) into the global
-// accumulators gsum / gcnt.
+// Add a run's register sums into the shared accumulators (two 32-bit
+// atomics with an exact carry; other warps may flush into the same cluster).
+__device__ __forceinline__ void fx_flush(unsigned long long *acc, int d, int j, int f,
+                                         long long &s0, long long &s1, bool two) {
+    if (f < d) fx_add(acc + (size_t)j * d + f, s0);
+    if (two && f + 1 < d) fx_add(acc + (size_t)j * d + f + 1, s1);
+    s0 = 0;
+    s1 = 0;
+}
+
+// One CTA per SM over a contiguous range of rows, in batches of FX_BATCH:
+// the batch's rows are bucketed by label in shared memory (counting sort; the
+// order inside a bucket does not matter, the sums are integers), then each
+// warp walks an equal share of the bucketed list, keeping the running sums of
+// the current cluster in registers (lanes over feature pairs) and adding them
+// to the CTA's shared accumulators only when the cluster changes.  The CTA's
+// sums and counts are finally added (integer reductions, order-free) into the
+// global accumulators gsum / gcnt.
 template <bool VEC2>
 __global__ void __launch_bounds__(FX_THREADS, 1)
 fx_update_kernel(const float *X, int ld, int n, int d, int k, const int *labels,
                  const float *scale, unsigned long long *gsum, int *gcnt) {
     extern __shared__ __align__(16) unsigned char fx_smem[];
     unsigned long long *acc = reinterpret_cast<unsigned long long *>(fx_smem);
-    int *cnt = reinterpret_cast<int *>(acc + (size_t)k * d);
-    float *sc = reinterpret_cast<float *>(cnt + k);
+    int *list = reinterpret_cast<int *>(acc + (size_t)k * d); // FX_BATCH row ids
+    int *off = list + FX_BATCH;                                  // k + 1 bucket starts
+    int *cur = off + k + 1;                                      // k + 1 cursors / counts
+    float *sc = reinterpret_cast<float *>(cur + k + 1);
     const int kd = k * d;
     for (int e = threadIdx.x; e < kd; e += blockDim.x) acc[e] = 0ull;
-    for (int j = threadIdx.x; j < k; j += blockDim.x) cnt[j] = 0;
     for (int f = threadIdx.x; f < d; f += blockDim.x) sc[f] = scale[f];
-    __syncthreads();
     const long long per = ((long long)n + gridDim.x - 1) / gridDim.x;
     const int r0 = (int)min((long long)n, per * blockIdx.x);
     const int r1 = (int)min((long long)n, per * (blockIdx.x + 1));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int rb = r0 + warp * FX_ROWS; rb < r1; rb += nw * FX_ROWS) {
-        const int lv = lane < FX_ROWS && rb + lane < r1 ? labels[rb + lane] : -1;
-        int lab[FX_ROWS];
+    for (int b0 = r0; b0 < r1; b0 += FX_BATCH) {
+        const int nb = min(FX_BATCH, r1 - b0);
+        for (int j = threadIdx.x; j <= k; j += blockDim.x) cur[j] = 0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) atomicAdd(&cur[labels[b0 + i]], 1);
+        __syncthreads();
+        if (warp == 0) { // exclusive scan of the counts -> bucket starts
+            int carry = 0;
+            for (int j0 = 0; j0 < k; j0 += 32) {
+                const int j = j0 + lane;
+                const int c = j < k ? cur[j] : 0;
+                if (c > 0) atomicAdd(&gcnt[j], c);
+                int x = c;
 #pragma unroll
-        for (int u = 0; u < FX_ROWS; ++u) lab[u] = __shfl_sync(0xffffffffu, lv, u);
-        if (VEC2) {
-            for (int f = 2 * lane; f < d; f += 64) {
-                float2 xv[FX_ROWS];
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= o) x += y;
+                }
+                if (j < k) off[j] = carry + x - c;
+                carry += __shfl_sync(0xffffffffu, x, 31);
+            }
+            if (lane == 0) off[k] = carry;
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < k; j += blockDim.x) cur[j] = off[j];
+        __syncthreads();
+        for (int i = threadIdx.x; i < nb; i += blockDim.x)
+            list[atomicAdd(&cur[labels[b0 + i]], 1)] = b0 + i;
+        __syncthreads();
+        // this warp's share of the bucketed list
+        const int p0 = (int)((long long)nb * warp / nw), p1 = (int)((long long)nb * (warp + 1) / nw);
+        if (p0 < p1) {
+            int j0 = 0; // bucket holding position p0: last j with off[j] <= p0
+            {
+                int lo = 0, hi = k - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (off[mid] <= p0) lo = mid;
+                    else hi = mid - 1;
+                }
+                j0 = lo;
+            }
+            const int fstep = VEC2 ? 64 : 32;
+            for (int fb = 0; fb < d; fb += fstep) {
+                const int f = fb + (VEC2 ? 2 * lane : lane);
+                const float s0 = f < d ? sc[f] : 0.f;
+                const float s1 = VEC2 && f + 1 < d ? sc[f + 1] : 0.f;
+                int j = j0;
+                int jend = off[j + 1];
+                long long a0 = 0, a1 = 0;
+                for (int p = p0; p < p1; p += FX_ROWS) {
+                    float2 xv[FX_ROWS];
 #pragma unroll
-                for (int u = 0; u < FX_ROWS; ++u)
-                    xv[u] = rb + u < r1
-                                ? *reinterpret_cast<const float2 *>(X + (size_t)(rb + u) * ld + f)
-                                : make_float2(0.f, 0.f);
-                const float s0 = sc[f], s1 = sc[f + 1];
+                    for (int u = 0; u < FX_ROWS; ++u) {
+                        xv[u] = make_float2(0.f, 0.f);
+                        if (p + u < p1 && f < d) {
+                            const float *xr = X + (size_t)list[p + u] * ld + f;
+                            if (VEC2) xv[u] = *reinterpret_cast<const float2 *>(xr);
+                            else xv[u].x = *xr;
+                        }
+                    }
 #pragma unroll
-                for (int u = 0; u < FX_ROWS; ++u) {
-                    if (lab[u] >= 0) {
-                        unsigned long long *a = acc + (size_t)lab[u] * d + f;
-                        fx_add(a, fx_quant(xv[u].x, s0));
-                        fx_add(a + 1, fx_quant(xv[u].y, s1));
+                    for (int u = 0; u < FX_ROWS; ++u) {
+                        if (p + u < p1) {
+                            while (p + u >= jend) { // next non-empty bucket
+                                fx_flush(acc, d, j, f, a0, a1, VEC2);
+                                ++j;
+                                jend = off[j + 1];
+                            }
+                            a0 += fx_quant(xv[u].x, s0);
+                            if (VEC2) a1 += fx_quant(xv[u].y, s1);
+                        }
                     }
                 }
-            }
-        } else {
-            for (int f = lane; f < d; f += 32) {
-                float xv[FX_ROWS];
-#pragma unroll
-                for (int u = 0; u < FX_ROWS; ++u)
-                    xv[u] = rb + u < r1 ? X[(size_t)(rb + u) * ld + f] : 0.f;
-                const float s0 = sc[f];
-#pragma unroll
-                for (int u = 0; u < FX_ROWS; ++u)
-                    if (lab[u] >= 0) fx_add(acc + (size_t)lab[u] * d + f, fx_quant(xv[u], s0));
+                fx_flush(acc, d, j, f, a0, a1, VEC2);
             }
         }
-        if (lv >= 0) atomicAdd(&cnt[lv], 1);
+        __syncthreads();
     }
-    __syncthreads();
     for (int e = threadIdx.x; e < kd; e += blockDim.x)
         if (acc[e]) atomicAdd(&gsum[e], acc[e]);
-    for (int j = threadIdx.x; j < k; j += blockDim.x)
-        if (cnt[j]) atomicAdd(&gcnt[j], cnt[j]);
 }
 
 // One thread per (cluster, feature): the mean from the global sums, and fp64

@@ -44,7 +44,7 @@ struct TcAssignArgs {
     int *amb_rows;       // rows to relabel exactly
     int *amb_cand;       // TC_MAXC candidate clusters per listed row
     int *amb_ncand;      // number of candidates (0: scan every cluster)
-    int *amb_count;
+    int *amb_count;      // [0] listed rows, [2] of them without a candidate list
     int *err;            // set on a timed-out wait
 };
 
@@ -387,6 +387,8 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
                     const int nc = okc ? cnt : 0;
                     a.amb_ncand[pos] = nc;
                     for (int u = 0; u < nc; ++u) a.amb_cand[pos * TC_MAXC + u] = my[u];
+                    const unsigned fullm = __ballot_sync(mask, nc == 0);
+                    if (fullm && lane == __ffs(mask) - 1) atomicAdd(a.amb_count + 2, __popc(fullm));
                 }
             }
         }
@@ -451,18 +453,34 @@ kmeans_rescore_kernel(const float *X, int ld, int d, int dp, const float *C, int
         const int r = e < cnt ? amb_rows[e] : 0;
         const int nrows = min(32, cnt - e0);
         __syncwarp();
-        if (VEC) {
-            const int q4 = d >> 2;
-            for (int t = lane; t < nrows * q4; t += 32) {
-                const int i = t / q4, f4 = t - i * q4;
-                const int ri = amb_rows[e0 + i];
-                *reinterpret_cast<float4 *>(xw + (size_t)i * dp + 4 * f4) =
-                    *reinterpret_cast<const float4 *>(X + (size_t)ri * ld + 4 * f4);
-            }
-        } else {
-            for (int t = lane; t < nrows * d; t += 32) {
-                const int i = t / d, f = t - i * d;
-                xw[(size_t)i * dp + f] = X[(size_t)amb_rows[e0 + i] * ld + f];
+        // stage the warp's rows: row ids come from the lanes (shuffles), and
+        // eight loads per lane are issued before their stores, so the loads
+        // of different rows overlap
+        {
+            const int w4 = VEC ? (d >> 2) : d; // 16-byte (VEC) or 4-byte words per row
+            const int tot = nrows * w4;
+            for (int t0 = 0; t0 < tot; t0 += 256) {
+                float4 buf[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int t = t0 + 32 * u + lane;
+                    const int i = min(t / w4, 31);
+                    const int ri = __shfl_sync(0xffffffffu, r, i);
+                    if (t < tot) {
+                        const int c = t - i * w4;
+                        if (VEC) buf[u] = *reinterpret_cast<const float4 *>(X + (size_t)ri * ld + 4 * c);
+                        else buf[u].x = X[(size_t)ri * ld + c];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int t = t0 + 32 * u + lane;
+                    if (t < tot) {
+                        const int i = t / w4, c = t - i * w4;
+                        if (VEC) *reinterpret_cast<float4 *>(xw + (size_t)i * dp + 4 * c) = buf[u];
+                        else xw[(size_t)i * dp + c] = buf[u].x;
+                    }
+                }
             }
         }
         __syncwarp();

@@ -292,6 +292,7 @@ def main():
     value = iters_total / (ms / 1e3)
     n_iter = iters // args.steps
     relabelled = km.stat("relabelled_rows")
+    full_scan = km.stat("full_scan_rows")
     tensor_core = km.stat("tensor_core") == 1.0
     kt = kernel_times(km)
 
@@ -344,6 +345,7 @@ def main():
         cb = cpu_baseline(X, C0, int(os.environ.get("BENCH_CPU_SAMPLE", "131072")), 2)
     extra = {"iterations_per_step": n_iter, "init_ms": init_ms,
              "relabelled_rows_last_iteration": relabelled,
+             "full_scan_rows_last_iteration": full_scan,
              "precision_path": (f"{mode} tcgen05 candidate pass + exact fp32 re-score of "
                                 "uncertified rows") if tensor_core else "plain fp32 (SIMT)"}
     out = {
