@@ -305,13 +305,15 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
         int it = g;
         for (int t = blockIdx.x + g * gridDim.x; t < ntiles; t += 2 * gridDim.x, it += 2) {
             const int b = g;
+            // row data first, so that their loads overlap the wait
+            const int r = t * TC_BM + row_in_tile;
+            const float xn = r < a.n ? a.xnorm[r] : 0.f;
+            const int lprev = (h == 0 && a.labels_prev && r < a.n) ? a.labels_prev[r] : -1;
             bool ok = mbar_wait(&sh->tfull[b], (uint32_t)((it >> 1) & 1));
             if (!ok) raise(&sh->abort_flag, a.err, 5);
             ok = ok && !*((volatile int *)&sh->abort_flag);
             ok = __all_sync(0xffffffffu, ok); // warp-uniform from here on
             const uint32_t trow = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * a.bufcols);
-            const int r = t * TC_BM + row_in_tile;
-            const float xn = r < a.n ? a.xnorm[r] : 0.f;
             // pass 1: this half's min_j v_j.  All lanes execute every
             // tcgen05.ld (warp-synchronous); columns beyond npad in the last
             // chunk are masked (warp-uniform).
@@ -368,7 +370,7 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
             if (certain) {
                 const int lbl = lab;
                 a.labels[r] = lbl;
-                if (a.labels_prev && a.labels_prev[r] != lbl) changed = 1;
+                if (a.labels_prev && lprev != lbl) changed = 1;
             }
             // several candidates (or non-finite scores): one atomic per warp
             const bool amb = valid && !certain;
@@ -427,17 +429,28 @@ kmeans_rescore_kernel(const float *X, int ld, int d, int dp, const float *C, int
     const int cnt = *amb_count;
     if (cnt == 0) return;
     if (c_in_smem) {
-        if (VEC) {
-            const int q4 = d >> 2;
-            for (int e = threadIdx.x; e < k * q4; e += blockDim.x) {
-                const int j = e / q4, f4 = e - j * q4;
-                *reinterpret_cast<float4 *>(cs + (size_t)j * dp + 4 * f4) =
-                    *reinterpret_cast<const float4 *>(C + (size_t)j * ld + 4 * f4);
+        // eight loads per thread in flight before their stores
+        const int w4 = VEC ? (d >> 2) : d;
+        const int tot = k * w4;
+        for (int t0 = 0; t0 < tot; t0 += 8 * (int)blockDim.x) {
+            float4 buf[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int t = t0 + u * (int)blockDim.x + (int)threadIdx.x;
+                if (t < tot) {
+                    const int j = t / w4, c = t - j * w4;
+                    if (VEC) buf[u] = *reinterpret_cast<const float4 *>(C + (size_t)j * ld + 4 * c);
+                    else buf[u].x = C[(size_t)j * ld + c];
+                }
             }
-        } else {
-            for (int e = threadIdx.x; e < k * d; e += blockDim.x) {
-                const int j = e / d, f = e - j * d;
-                cs[(size_t)j * dp + f] = C[(size_t)j * ld + f];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int t = t0 + u * (int)blockDim.x + (int)threadIdx.x;
+                if (t < tot) {
+                    const int j = t / w4, c = t - j * w4;
+                    if (VEC) *reinterpret_cast<float4 *>(cs + (size_t)j * dp + 4 * c) = buf[u];
+                    else cs[(size_t)j * dp + c] = buf[u].x;
+                }
             }
         }
         __syncthreads();
