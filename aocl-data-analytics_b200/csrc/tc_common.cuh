@@ -113,59 +113,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Split form for software pipelining: issue the load, use other registers,
-// then wait.  The wait takes the destination registers as read-write operands
-// so that no use of them can be scheduled before it.
-__device__ __forceinline__ void tmem_ld32_issue(uint32_t taddr, uint32_t (&r)[32]) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                 "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-                   "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
-                   "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]),
-                   "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-                   "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
-                   "=r"(r[30]), "=r"(r[31])
-                 : "r"(taddr));
-}
-__device__ __forceinline__ void tmem_ld_wait(uint32_t (&r)[32]) {
-    asm volatile("tcgen05.wait::ld.sync.aligned;"
-                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
-                   "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
-                   "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]),
-                   "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
-                   "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]),
-                   "+r"(r[30]), "+r"(r[31])
-                 :
-                 : "memory");
-}
-
-// Two 32-column loads (the second only when `two`, a warp-uniform flag)
-// completed by a single wait.  The empty asm after the wait ties the second
-// array's registers to it, so no use of them is scheduled before the wait.
-__device__ __forceinline__ void tmem_ld64(uint32_t taddr, bool two, float (&v0)[32],
-                                          float (&v1)[32]) {
-    uint32_t r0[32], r1[32];
-    tmem_ld32_issue(taddr, r0);
-    if (two) tmem_ld32_issue(taddr + 32u, r1);
-    tmem_ld_wait(r0);
-    asm volatile(""
-                 : "+r"(r1[0]), "+r"(r1[1]), "+r"(r1[2]), "+r"(r1[3]), "+r"(r1[4]), "+r"(r1[5]),
-                   "+r"(r1[6]), "+r"(r1[7]), "+r"(r1[8]), "+r"(r1[9]), "+r"(r1[10]),
-                   "+r"(r1[11]), "+r"(r1[12]), "+r"(r1[13]), "+r"(r1[14]), "+r"(r1[15]),
-                   "+r"(r1[16]), "+r"(r1[17]), "+r"(r1[18]), "+r"(r1[19]), "+r"(r1[20]),
-                   "+r"(r1[21]), "+r"(r1[22]), "+r"(r1[23]), "+r"(r1[24]), "+r"(r1[25]),
-                   "+r"(r1[26]), "+r"(r1[27]), "+r"(r1[28]), "+r"(r1[29]), "+r"(r1[30]),
-                   "+r"(r1[31])
-                 :
-                 : "memory");
-#pragma unroll
-    for (int i = 0; i < 32; ++i) {
-        v0[i] = __uint_as_float(r0[i]);
-        v1[i] = __uint_as_float(r1[i]);
-    }
-}
-
 // Shared-memory matrix descriptor: K-major operand, 128-byte swizzle, rows of
 // 128 bytes in 8-row (1024-byte) atoms (SBO = 1024 B, LBO unused = 16 B).
 __device__ __forceinline__ uint64_t desc_k_sw128(uint32_t smem_addr) {
