@@ -499,6 +499,7 @@ constexpr int FX_SMEM_LIMIT = 200 * 1024;
 constexpr int FX_THREADS = 1024;
 constexpr int FX_ROWS = 8;     // rows in flight per warp
 constexpr int FX_BATCH = 8192; // rows sorted by label per pass of a CTA
+static_assert(FX_BATCH / (FX_THREADS / 32) + 1 <= 511, "run sums must fit in int32");
 } // namespace
 
 size_t fx_update_smem(int k, int d) {
@@ -537,20 +538,6 @@ cudaError_t launch_col_absmax(const float *X, int ld, int n, int d, unsigned *co
     return cudaGetLastError();
 }
 
-// q = round(x * 2^s) for |x * 2^s| < 2^44, on the FMA pipe: y = x * 2^s is
-// exact; yh = y rounded to a multiple of 2^22 (add/subtract 1.5 * 2^45) and
-// yl = y - yh (exact, |yl| <= 2^21); both halves become int32 through the
-// 1.5 * 2^23 magic constant (exact for |v| < 2^22).  Rounding is to nearest
-// (ties to even at each step; any fixed rule keeps the sums deterministic).
-__device__ __forceinline__ long long fx_quant(float x, float sc) {
-    const float y = __fmul_rn(x, sc);
-    const float yh = __fsub_rn(__fadd_rn(y, 52776558133248.f), 52776558133248.f);
-    const float yl = __fsub_rn(y, yh);
-    const int hi = __float_as_int(__fmaf_rn(yh, 2.384185791015625e-07f, 12582912.f)) - 0x4B400000;
-    const int lo = __float_as_int(__fadd_rn(yl, 12582912.f)) - 0x4B400000;
-    return ((long long)hi << 22) + lo;
-}
-
 // acc += q (64-bit, in shared memory) as two 32-bit atomics: the low word's
 // atomic returns its old value, from which this addition's carry into the
 // high word is exact whatever the interleaving of the other threads' adds.
@@ -563,12 +550,38 @@ __device__ __forceinline__ void fx_add(unsigned long long *acc, long long q) {
 
 // Add a run's register sums into the shared accumulators (two 32-bit
 // atomics with an exact carry; other warps may flush into the same cluster).
+// Run sums of q = round(x * 2^s) split as q = hi * 2^22 + lo, both parts
+// accumulated as raw float bits of hi + 1.5 * 2^23 and lo + 1.5 * 2^23 in
+// wrapping 32-bit registers (four FMA-pipe operations and two integer adds
+// per value):
+//   t  = fma(x, 2^(s-22), 1.5 * 2^23)   = 1.5 * 2^23 + round(x 2^(s-22))
+//   nh = fma(t, -2^22, 1.5 * 2^45)      = -hi * 2^22               (exact)
+//   yl = fma(x, 2^s, nh)                = x 2^s - hi * 2^22        (exact, |yl| <= 2^21)
+//   lo = yl + 1.5 * 2^23                 (rounds yl to an integer)
+// With |x 2^s| < 2^44 and at most 511 rows per run, the unbiased sums fit in
+// int32 (|sum hi| < 2^31, |sum lo| < 2^30).
+struct FxRun {
+    unsigned h0 = 0, l0 = 0, h1 = 0, l1 = 0;
+    unsigned n = 0;
+};
+__device__ __forceinline__ void fx_acc(float x, float s22, float s, unsigned &h, unsigned &l) {
+    const float t = __fmaf_rn(x, s22, 12582912.f);
+    const float nh = __fmaf_rn(t, -4194304.f, 52776558133248.f);
+    const float yl = __fmaf_rn(x, s, nh);
+    h += __float_as_uint(t);
+    l += __float_as_uint(__fadd_rn(yl, 12582912.f));
+}
+__device__ __forceinline__ long long fx_run_sum(unsigned h, unsigned l, unsigned n) {
+    const int hs = (int)(h - n * 0x4B400000u), ls = (int)(l - n * 0x4B400000u);
+    return ((long long)hs << 22) + ls;
+}
 __device__ __forceinline__ void fx_flush(unsigned long long *acc, int d, int j, int f,
-                                         long long &s0, long long &s1, bool two) {
-    if (f < d) fx_add(acc + (size_t)j * d + f, s0);
-    if (two && f + 1 < d) fx_add(acc + (size_t)j * d + f + 1, s1);
-    s0 = 0;
-    s1 = 0;
+                                         FxRun &run, bool two) {
+    if (run.n) {
+        if (f < d) fx_add(acc + (size_t)j * d + f, fx_run_sum(run.h0, run.l0, run.n));
+        if (two && f + 1 < d) fx_add(acc + (size_t)j * d + f + 1, fx_run_sum(run.h1, run.l1, run.n));
+    }
+    run = FxRun();
 }
 
 // One CTA per SM over a contiguous range of rows, in batches of FX_BATCH:
@@ -643,9 +656,10 @@ fx_update_kernel(const float *X, int ld, int n, int d, int k, const int *labels,
                 const int f = fb + (VEC2 ? 2 * lane : lane);
                 const float s0 = f < d ? sc[f] : 0.f;
                 const float s1 = VEC2 && f + 1 < d ? sc[f + 1] : 0.f;
+                const float s0_22 = s0 * 2.384185791015625e-07f, s1_22 = s1 * 2.384185791015625e-07f;
                 int j = j0;
                 int jend = off[j + 1];
-                long long a0 = 0, a1 = 0;
+                FxRun run;
                 for (int p = p0; p < p1; p += FX_ROWS) {
                     float2 xv[FX_ROWS];
 #pragma unroll
@@ -661,16 +675,17 @@ fx_update_kernel(const float *X, int ld, int n, int d, int k, const int *labels,
                     for (int u = 0; u < FX_ROWS; ++u) {
                         if (p + u < p1) {
                             while (p + u >= jend) { // next non-empty bucket
-                                fx_flush(acc, d, j, f, a0, a1, VEC2);
+                                fx_flush(acc, d, j, f, run, VEC2);
                                 ++j;
                                 jend = off[j + 1];
                             }
-                            a0 += fx_quant(xv[u].x, s0);
-                            if (VEC2) a1 += fx_quant(xv[u].y, s1);
+                            fx_acc(xv[u].x, s0_22, s0, run.h0, run.l0);
+                            if (VEC2) fx_acc(xv[u].y, s1_22, s1, run.h1, run.l1);
+                            ++run.n;
                         }
                     }
                 }
-                fx_flush(acc, d, j, f, a0, a1, VEC2);
+                fx_flush(acc, d, j, f, run, VEC2);
             }
         }
         __syncthreads();
