@@ -99,6 +99,24 @@ cudaError_t launch_knn_merge(const T *part_key, const int *part_idx, int nq, int
 int knn_tile_rows_train(bool fp64);
 int knn_max_k(bool fp64);
 
+// ---------------------------------------------- kNN tensor-core pass ---
+// fp32 euclidean / squared euclidean: bf16x3 tcgen05 candidate pass with a
+// certified threshold per query, exact re-score of the survivors in the plain
+// kernel's order.  Results (q-major, as launch_knn_merge) equal the plain
+// path's; queries the pass cannot certify are flagged in `fallback`
+// (*n_fallback of them) for the plain path.
+int knn_tc_supported(int nx, int d, int k);
+size_t knn_tc_list_cap();                   // list entries per query
+size_t knn_tc_query_bytes(int nq, int d);   // size of qbuf
+int *knn_tc_counts(void *qbuf, int nq, int d); // per-query list lengths inside qbuf
+cudaError_t launch_knn_tc_train_prep(const float *X, int ld, int nx, int d, void *Xh, void *Xl,
+                                     int ldbf, float *xnorm2, float *xmax, cudaStream_t s);
+cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const float *xnorm2,
+                          const float *xmax, int nx, int ld, int ldbf, int d, const float *Q,
+                          int nq, int k, int kc, int take_sqrt, void *qbuf, void *list,
+                          int *fallback, int *n_fallback, int *err, float *out_key,
+                          int *out_idx, cudaStream_t s);
+
 // ------------------------------------------------------------- k-means ---
 struct KmeansWork {
     // per-iteration device scratch owned by the handle

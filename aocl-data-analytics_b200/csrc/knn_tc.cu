@@ -1,0 +1,662 @@
+// Brute-force kNN (euclidean / squared euclidean, fp32 data) with a bf16
+// tensor-core candidate pass and an exact fp32 re-score.
+//
+// Ranking value of train row j for query q: v'_j = |x_j|^2 - 2 x_j.q (the
+// squared distance minus the query's own |q|^2).  The tcgen05 pass computes
+// v'_tc from three bf16 products (x = xh + xl, -2q = qh + ql:
+// xh.qh + xh.ql + xl.qh) accumulated in fp32 in TMEM, plus the fp32 |x_j|^2.
+// A rigorous bound |v'_tc - v'_plain| <= eps_q (v'_plain: the plain path's
+// fp32 squared distance, in the reference's accumulation order, minus |q|^2)
+// gives the certificate: every row of the plain top-k has
+// v'_tc <= v'_tc(k) + 2 eps_q, where v'_tc(k) is the k-th smallest v'_tc.
+//
+// Every query keeps a threshold theta_q >= v'_tc(k) + 2 eps_q, shared by all
+// CTAs through global memory (atomicMin of order-preserving bits).  The
+// epilogue appends every (v'_tc, j) with v'_tc < theta_q to the query's list;
+// at every window boundary of the list, a warp lowers theta_q to (k-th
+// smallest value of a complete window) + 2 eps_q -- the window's k-th
+// smallest is never below the global one, so theta_q stays a valid bound
+// while it tightens.  theta_q starts from an exact pre-pass over the first
+// TK_PRE_ROWS training rows (the k-th smallest plain distance there bounds
+// the global one).  The finalize kernel re-scores the listed rows
+// with v'_tc < theta_q exactly (the plain kernel's formula and order) and
+// keeps the k best by (distance, index): the plain path's neighbours.
+#include "b200_common.cuh"
+#include "b200_kernels.hpp"
+#include "tc_common.cuh"
+#include <cuda_bf16.h>
+#include <cmath>
+
+namespace b200 {
+
+using namespace tc;
+
+namespace {
+
+constexpr int TK_BM = 128;         // train rows per tile (UMMA M, TMEM lanes)
+constexpr int TK_BN = 256;         // queries per tile (UMMA N, TMEM columns)
+constexpr int TK_KB = 64;          // bf16 elements per 128-byte K block
+constexpr int TK_THREADS = 320;    // TMA warp, MMA warp, 8 epilogue warps
+constexpr int TK_WIN_MAX = 512;    // list entries per threshold refresh (256 when k <= 128)
+constexpr int TK_PRE_ROWS = 4096;  // training rows of the threshold pre-pass
+constexpr int TK_CHUNK_TILES = 64; // train tiles per work item
+constexpr int TK_FIN_MAX = 2048;   // candidates re-scored per query (more: fallback)
+
+struct KnnTcArgs {
+    int nx, nq, k, nkb, stages, n_qtiles, n_xtiles, n_items, cap, win;
+    const float *xnorm;   // nx: fp32 |x_j|^2
+    const float *margin;  // n_qtiles * TK_BN: 2 eps_q (nudged up)
+    unsigned *theta;      // n_qtiles * TK_BN: threshold, order-preserving bits
+    int *cnt;             // n_qtiles * TK_BN: entries appended
+    int2 *list;           // nq * cap: (value bits, train row)
+    int *err;
+};
+
+struct __align__(16) TkShared {
+    uint64_t full[8], empty[8], tfull[2], tempty[2], bfull, bempty;
+    uint32_t tmem_base;
+    int abort_flag;
+};
+
+__device__ __forceinline__ unsigned ord_bits(float f) {
+    const unsigned b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float ord_float(unsigned o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
+__device__ __forceinline__ float nudge_up(float t) {
+    return t + fabsf(t) * 9.5367431640625e-7f + 1e-30f;
+}
+__device__ __forceinline__ void tk_raise(int *abort_flag, int *err, int code) {
+    *((volatile int *)abort_flag) = 1;
+    atomicExch(err, code);
+}
+
+// Ascending bitonic sort of 512 floats held 16 per lane (element i = 16 lane + e).
+__device__ __forceinline__ void warp_sort512(float (&a)[16]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int size = 2; size <= 512; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            if (stride >= 16) {
+                const int lx = stride >> 4;
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    const float o = __shfl_xor_sync(0xffffffffu, a[e], lx);
+                    const int i = lane * 16 + e;
+                    const bool asc = (i & size) == 0, lower = (i & stride) == 0;
+                    a[e] = (asc == lower) ? fminf(a[e], o) : fmaxf(a[e], o);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    if ((e & stride) == 0) {
+                        const int j = e ^ stride;
+                        const int i = lane * 16 + e;
+                        const bool asc = (i & size) == 0;
+                        const float lo = fminf(a[e], a[j]), hi = fmaxf(a[e], a[j]);
+                        a[e] = asc ? lo : hi;
+                        a[j] = asc ? hi : lo;
+                    }
+                }
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(TK_THREADS, 1)
+knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
+              const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
+              KnnTcArgs a) {
+    extern __shared__ __align__(1024) unsigned char tk_raw[];
+    unsigned char *base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(tk_raw) + 1023) & ~uintptr_t(1023));
+    const int S = a.stages, nkb = a.nkb;
+    constexpr uint32_t kB = TK_BN * 128u; // one K block of the query tile (32 KB)
+    constexpr uint32_t kA = TK_BM * 128u; // one K block of a train tile (16 KB)
+    unsigned char *Bh = base;
+    unsigned char *Bl = Bh + (size_t)nkb * kB;
+    unsigned char *As = Bl + (size_t)nkb * kB; // S stages of (Ah, Al) for one K block
+    float *th_w = reinterpret_cast<float *>(As + (size_t)S * 2 * kA); // 8 warps x TK_BN
+    TkShared *sh = reinterpret_cast<TkShared *>(th_w + 8 * TK_BN);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&sh->full[s], 1);
+            mbar_init(&sh->empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&sh->tfull[b], 1);
+            mbar_init(&sh->tempty[b], 4 * 32);
+        }
+        mbar_init(&sh->bfull, 1);
+        mbar_init(&sh->bempty, 1);
+        sh->abort_flag = 0;
+        fence_barrier_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(&sh->tmem_base, 2u * TK_BN);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = sh->tmem_base;
+
+    if (warp == 0) {
+        // ---------------------------------------------------- TMA producer --
+        if (lane == 0) {
+            prefetch_tmap(&tmAh);
+            prefetch_tmap(&tmBh);
+            int us = 0, ii = 0;
+            bool ok = true;
+            for (int item = blockIdx.x; ok && item < a.n_items; item += gridDim.x, ++ii) {
+                const int xc = item / a.n_qtiles, qt = item % a.n_qtiles;
+                if (ii > 0 && !mbar_wait(&sh->bempty, (uint32_t)((ii - 1) & 1))) {
+                    tk_raise(&sh->abort_flag, a.err, 11);
+                    break;
+                }
+                mbar_arrive_expect_tx(&sh->bfull, (uint32_t)(2 * nkb) * kB);
+                for (int kb = 0; kb < nkb; ++kb) {
+                    tma_load_2d(&tmBh, &sh->bfull, Bh + (size_t)kb * kB, kb * TK_KB, qt * TK_BN);
+                    tma_load_2d(&tmBl, &sh->bfull, Bl + (size_t)kb * kB, kb * TK_KB, qt * TK_BN);
+                }
+                const int x0 = xc * TK_CHUNK_TILES, x1 = min(a.n_xtiles, x0 + TK_CHUNK_TILES);
+                for (int xt = x0; ok && xt < x1; ++xt) {
+                    for (int kb = 0; kb < nkb; ++kb, ++us) {
+                        const int s = us % S;
+                        if (!mbar_wait(&sh->empty[s], (uint32_t)(((us / S) & 1) ^ 1))) {
+                            tk_raise(&sh->abort_flag, a.err, 12);
+                            ok = false;
+                            break;
+                        }
+                        if (*((volatile int *)&sh->abort_flag)) {
+                            ok = false;
+                            break;
+                        }
+                        unsigned char *st = As + (size_t)s * 2 * kA;
+                        mbar_arrive_expect_tx(&sh->full[s], 2 * kA);
+                        tma_load_2d(&tmAh, &sh->full[s], st, kb * TK_KB, xt * TK_BM);
+                        tma_load_2d(&tmAl, &sh->full[s], st + kA, kb * TK_KB, xt * TK_BM);
+                    }
+                }
+            }
+            // every issued stage must have landed before exit
+            for (int u = (us > S ? us - S : 0); u < us; ++u)
+                mbar_wait(&sh->full[u % S], (uint32_t)((u / S) & 1));
+        }
+    } else if (warp == 1) {
+        // ---------------------------------------------------- MMA issuer ----
+        if (lane == 0) {
+            const uint32_t idesc = idesc_bf16_f32(TK_BM, TK_BN);
+            int us = 0, tc = 0, ii = 0;
+            bool ok = true;
+            for (int item = blockIdx.x; ok && item < a.n_items; item += gridDim.x, ++ii) {
+                const int xc = item / a.n_qtiles;
+                if (!mbar_wait(&sh->bfull, (uint32_t)(ii & 1))) {
+                    tk_raise(&sh->abort_flag, a.err, 13);
+                    break;
+                }
+                const int x0 = xc * TK_CHUNK_TILES, x1 = min(a.n_xtiles, x0 + TK_CHUNK_TILES);
+                for (int xt = x0; ok && xt < x1; ++xt, ++tc) {
+                    const int b = tc & 1;
+                    if (!mbar_wait(&sh->tempty[b], (uint32_t)(((tc >> 1) & 1) ^ 1))) {
+                        tk_raise(&sh->abort_flag, a.err, 14);
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t tacc = tbase + (uint32_t)(b * TK_BN);
+                    uint32_t acc = 0;
+                    for (int kb = 0; kb < nkb; ++kb, ++us) {
+                        const int s = us % S;
+                        if (!mbar_wait(&sh->full[s], (uint32_t)((us / S) & 1))) {
+                            tk_raise(&sh->abort_flag, a.err, 15);
+                            ok = false;
+                            break;
+                        }
+                        if (*((volatile int *)&sh->abort_flag)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t ah = smem_u32(As + (size_t)s * 2 * kA);
+                        const uint32_t al = ah + kA;
+                        const uint32_t bh = smem_u32(Bh + (size_t)kb * kB);
+                        const uint32_t bl = smem_u32(Bl + (size_t)kb * kB);
+#pragma unroll
+                        for (int kk = 0; kk < TK_KB / 16; ++kk) {
+                            mma_f16_ss(tacc, desc_k_sw128(ah + kk * 32), desc_k_sw128(bh + kk * 32),
+                                       idesc, acc);
+                            acc = 1;
+                            mma_f16_ss(tacc, desc_k_sw128(ah + kk * 32), desc_k_sw128(bl + kk * 32),
+                                       idesc, 1);
+                            mma_f16_ss(tacc, desc_k_sw128(al + kk * 32), desc_k_sw128(bh + kk * 32),
+                                       idesc, 1);
+                        }
+                        mma_commit(&sh->empty[s]);
+                    }
+                    if (!ok) break;
+                    mma_commit(&sh->tfull[b]);
+                }
+                mma_commit(&sh->bempty);
+            }
+            // the accumulators of the last tiles must be complete before the
+            // TMEM is released
+            for (int u = (tc > 2 ? tc - 2 : 0); u < tc; ++u)
+                mbar_wait(&sh->tfull[u & 1], (uint32_t)((u >> 1) & 1));
+        }
+    } else {
+        // ---------------------------------------------------- epilogue ------
+        const int e = warp - 2;
+        const int g = e >> 2;     // accumulator buffer / tile parity
+        const int q = warp & 3;   // TMEM lane quarter
+        float *thw = th_w + e * TK_BN;
+        const float inf = __int_as_float(0x7f800000);
+        int tc = 0;
+        bool ok = true;
+        for (int item = blockIdx.x; ok && item < a.n_items; item += gridDim.x) {
+            const int xc = item / a.n_qtiles, qt = item % a.n_qtiles;
+            const int x0 = xc * TK_CHUNK_TILES, x1 = min(a.n_xtiles, x0 + TK_CHUNK_TILES);
+            for (int xt = x0; xt < x1; ++xt, ++tc) {
+                if ((tc & 1) != g) continue;
+                const int b = g;
+                const int row = xt * TK_BM + q * 32 + lane;
+                const float xn = row < a.nx ? a.xnorm[row] : inf;
+                unsigned tb[TK_BN / 32];
+#pragma unroll
+                for (int u = 0; u < TK_BN / 32; ++u) tb[u] = a.theta[qt * TK_BN + u * 32 + lane];
+                bool w = mbar_wait(&sh->tfull[b], (uint32_t)((tc >> 1) & 1));
+                if (!w) tk_raise(&sh->abort_flag, a.err, 16);
+                w = w && !*((volatile int *)&sh->abort_flag);
+                if (!__all_sync(0xffffffffu, w)) {
+                    ok = false;
+                    break;
+                }
+#pragma unroll
+                for (int u = 0; u < TK_BN / 32; ++u) thw[u * 32 + lane] = ord_float(tb[u]);
+                __syncwarp();
+                tc_fence_after();
+                const uint32_t trow = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TK_BN);
+                for (int c = 0; c < TK_BN / 32; ++c) {
+                    float v[32];
+                    tmem_ld32(trow + (uint32_t)(c * 32), v);
+                    float m = inf;
+#pragma unroll
+                    for (int u = 0; u < 32; ++u)
+                        m = fminf(m, __fadd_rn(v[u], xn) - thw[c * 32 + u]);
+                    if (!__any_sync(0xffffffffu, m < 0.f)) continue;
+                    // rare: some value below its query's threshold
+                    for (int u = 0; u < 32; ++u) {
+                        const int col = c * 32 + u;
+                        const float sv = __fadd_rn(v[u], xn);
+                        const bool pred = sv < thw[col];
+                        const unsigned mask = __ballot_sync(0xffffffffu, pred);
+                        if (!mask) continue;
+                        const int gq = qt * TK_BN + col;
+                        const int leader = __ffs(mask) - 1, nadd = __popc(mask);
+                        int base0 = 0;
+                        if (lane == leader) base0 = atomicAdd(&a.cnt[gq], nadd);
+                        base0 = __shfl_sync(0xffffffffu, base0, leader);
+                        if (pred) {
+                            const int pos = base0 + __popc(mask & ((1u << lane) - 1u));
+                            if (pos < a.cap)
+                                a.list[(size_t)gq * a.cap + pos] = make_int2(__float_as_int(sv), row);
+                        }
+                        // Crossing a window boundary: lower theta with the k-th
+                        // smallest value of the window before the one just
+                        // completed (its entries have been written by now; one
+                        // still in flight reads as +inf, which only loosens the
+                        // bound).
+                        const int w_end = ((base0 + nadd) / a.win) * a.win;
+                        if (w_end > base0 && w_end >= 2 * a.win && w_end <= a.cap) {
+                            __syncwarp();
+                            const int2 *lw = a.list + (size_t)gq * a.cap + (w_end - 2 * a.win);
+                            const int per = a.win >> 5; // 8 or 16 per lane
+                            float s16[16];
+#pragma unroll
+                            for (int t = 0; t < 16; ++t) {
+                                // first word of the entry, past L1 (other SMs write it)
+                                s16[t] = t < per ? __int_as_float(__ldcg(&lw[lane * per + t].x))
+                                                 : __int_as_float(0x7f800000);
+                            }
+                            warp_sort512(s16);
+                            float kth = 0.f;
+#pragma unroll
+                            for (int t = 0; t < 16; ++t)
+                                if (t == (a.k - 1) % 16) kth = s16[t];
+                            kth = __shfl_sync(0xffffffffu, kth, (a.k - 1) / 16);
+                            const float thn = nudge_up(kth + a.margin[gq]);
+                            if (thn < thw[col]) {
+                                if (lane == 0) {
+                                    atomicMin(&a.theta[gq], ord_bits(thn));
+                                    thw[col] = thn;
+                                }
+                            }
+                            __syncwarp();
+                        }
+                    }
+                }
+                tc_fence_before();
+                mbar_arrive(&sh->tempty[b]);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tbase, 2u * TK_BN);
+    }
+}
+
+// -2q split into bf16 hi / lo (rows nq..nq_pad-1 zero), the query norms |q|
+// and the margins 2 eps_q; thresholds +inf (padded queries -inf), counts 0.
+__global__ void knn_tc_prep_queries(const float *Q, int ld, int nq, int d, int nq_pad, int ldo,
+                                    __nv_bfloat16 *Qh, __nv_bfloat16 *Ql, float e1, float e2,
+                                    const float *xmax, float *margin, unsigned *theta, int *cnt,
+                                    float *qsq) {
+    const int qi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (qi >= nq_pad) return;
+    float s = 0.f;
+    for (int f = lane; f < ldo; f += 32) {
+        const float x = (qi < nq && f < d) ? Q[(size_t)qi * ld + f] : 0.f;
+        s = __fmaf_rn(x, x, s);
+        const float y = -2.f * x;
+        const __nv_bfloat16 h = __float2bfloat16_rn(y);
+        Qh[(size_t)qi * ldo + f] = h;
+        Ql[(size_t)qi * ldo + f] = __float2bfloat16_rn(y - __bfloat162float(h));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) {
+        const float qn = sqrtf(s) * 1.0001f;
+        const float xm = *xmax;
+        const float eps = e1 * xm * qn + e2 * (xm * xm + qn * qn);
+        margin[qi] = nudge_up(2.f * eps);
+        theta[qi] = qi < nq ? ord_bits(__int_as_float(0x7f800000)) : ord_bits(-__int_as_float(0x7f800000));
+        cnt[qi] = 0;
+        qsq[qi] = s;
+    }
+}
+
+// theta_q from the pre-pass: p = k-th smallest plain squared distance over a
+// subset of the rows; theta_q = p - |q|^2 + 4 eps_q >= v'_tc(k) + 2 eps_q
+// (k rows with plain value <= p have v'_tc <= p - |q|^2 + eps_q; the fp32
+// |q|^2 is within eps_q of |q|^2).
+__global__ void knn_tc_init_theta(const float *pre_key, int k, int nq, const float *qsq,
+                                  const float *margin, unsigned *theta) {
+    const int qi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (qi >= nq) return;
+    const float pk = pre_key[(size_t)qi * k + (k - 1)];
+    const float t = nudge_up(pk - qsq[qi] + 2.f * margin[qi]);
+    if (t == t) theta[qi] = ord_bits(t);
+}
+
+__global__ void knn_tc_fill_list(int2 *list, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) list[i] = make_int2(0x7f800000, 0x7fffffff);
+}
+
+// The plain path's squared euclidean distance of one pair, in its exact
+// accumulation order: per group of 4 dims, dims 4t, 4t+1 into g1 and
+// 4t+2, 4t+3 into g2 (fma of the rounded difference), g1 += g2 at the end of
+// every kc-block and of the last full group; remaining dims into g1.
+__device__ __forceinline__ float sqeuc_ref(const float *x, const float *q, int d, int kc) {
+    const int d4 = d & ~3;
+    float g1 = 0.f, g2 = 0.f;
+    for (int kg = 0; kg < d4; kg += 4) {
+        const float t0 = __fsub_rn(q[kg], x[kg]), t1 = __fsub_rn(q[kg + 1], x[kg + 1]);
+        const float t2 = __fsub_rn(q[kg + 2], x[kg + 2]), t3 = __fsub_rn(q[kg + 3], x[kg + 3]);
+        g1 = __fmaf_rn(t0, t0, g1);
+        g1 = __fmaf_rn(t1, t1, g1);
+        g2 = __fmaf_rn(t2, t2, g2);
+        g2 = __fmaf_rn(t3, t3, g2);
+        if (((kg + 4) % kc) == 0 || (kg + 4) == d4) {
+            g1 = __fadd_rn(g1, g2);
+            g2 = 0.f;
+        }
+    }
+    for (int f = d4; f < d; ++f) {
+        const float t = __fsub_rn(q[f], x[f]);
+        g1 = __fmaf_rn(t, t, g1);
+    }
+    return g1;
+}
+
+// One block per query: the listed rows with v'_tc < theta_q, their exact
+// distances, sorted by (distance, index); the first k are written (sqrt for
+// euclidean).  A query whose list overflowed, or with more than TK_FIN_MAX
+// survivors, is flagged for the plain path (*n_fallback).
+__global__ void __launch_bounds__(256)
+knn_tc_finalize(const float *X, const float *Q, int ld, int d, int kc, int k, int cap,
+                const unsigned *theta, const int *cnt, const int2 *list, int take_sqrt,
+                float *out_key, int *out_idx, int *fallback, int *n_fallback) {
+    __shared__ float skey[TK_FIN_MAX];
+    __shared__ int sidx[TK_FIN_MAX];
+    __shared__ int scount;
+    extern __shared__ float qs[];
+    const int qi = blockIdx.x;
+    const int n = cnt[qi];
+    const float th = ord_float(theta[qi]);
+    if (threadIdx.x == 0) scount = 0;
+    for (int f = threadIdx.x; f < d; f += blockDim.x) qs[f] = Q[(size_t)qi * ld + f];
+    __syncthreads();
+    if (n > cap) {
+        if (threadIdx.x == 0) {
+            fallback[qi] = 1;
+            atomicAdd(n_fallback, 1);
+        }
+        return;
+    }
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        const int2 ev = list[(size_t)qi * cap + e];
+        if (__int_as_float(ev.x) < th) {
+            const int p = atomicAdd(&scount, 1);
+            if (p < TK_FIN_MAX) sidx[p] = ev.y;
+        }
+    }
+    __syncthreads();
+    const int m = scount;
+    if (m > TK_FIN_MAX || m < k) {
+        if (threadIdx.x == 0) {
+            fallback[qi] = 1;
+            atomicAdd(n_fallback, 1);
+        }
+        return;
+    }
+    int np2 = 1;
+    while (np2 < m) np2 <<= 1;
+    for (int e = threadIdx.x; e < np2; e += blockDim.x) {
+        if (e < m) {
+            skey[e] = sqeuc_ref(X + (size_t)sidx[e] * ld, qs, d, kc);
+        } else {
+            skey[e] = __int_as_float(0x7f800000);
+            sidx[e] = 0x7fffffff;
+        }
+    }
+    __syncthreads();
+    // bitonic sort of (key, index) pairs, ascending
+    for (int size = 2; size <= np2; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < np2; i += blockDim.x) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const bool asc = (i & size) == 0;
+                    const float ki = skey[i], kj = skey[j];
+                    const int ii = sidx[i], ij = sidx[j];
+                    const bool gt = key_less(kj, ij, ki, ii); // (i) > (j)
+                    if (gt == asc) {
+                        skey[i] = kj;
+                        skey[j] = ki;
+                        sidx[i] = ij;
+                        sidx[j] = ii;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int r = threadIdx.x; r < k; r += blockDim.x) {
+        const float kv = skey[r];
+        out_key[(size_t)qi * k + r] = take_sqrt ? __fsqrt_rn(kv) : kv;
+        out_idx[(size_t)qi * k + r] = sidx[r];
+    }
+}
+
+__global__ void max_value_kernel(const float *v, int n, float *out) {
+    float m = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        m = fmaxf(m, v[i]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(out), __float_as_int(m));
+}
+__global__ void sqrt_inplace_kernel(float *v) { *v = sqrtf(*v) * 1.0001f; }
+
+size_t tk_smem_bytes(int nkb, int stages) {
+    return 1024 + (size_t)nkb * 2 * TK_BN * 128 + (size_t)stages * 2 * TK_BM * 128 +
+           (size_t)8 * TK_BN * 4 + sizeof(TkShared) + 64;
+}
+
+} // namespace
+
+int knn_tc_supported(int nx, int d, int k) {
+    if (k < 1 || k > 256 || nx < k || d < 1) return 0;
+    const int nkb = (d + TK_KB - 1) / TK_KB;
+    return tk_smem_bytes(nkb, 2) <= 225 * 1024 ? 1 : 0;
+}
+
+size_t knn_tc_list_cap() { return 8192; }
+
+cudaError_t launch_knn_tc_train_prep(const float *X, int ld, int nx, int d, void *Xh, void *Xl,
+                                     int ldbf, float *xnorm2, float *xmax, cudaStream_t s) {
+    cudaError_t e = launch_split_bf16(X, ld, nx, d, Xh, Xl, ldbf, s);
+    if (e != cudaSuccess) return e;
+    e = launch_row_sqnorms<float>(X, ld, nx, d, xnorm2, s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(xmax, 0, sizeof(float), s);
+    if (e != cudaSuccess) return e;
+    max_value_kernel<<<148 * 4, 256, 0, s>>>(xnorm2, nx, xmax);
+    sqrt_inplace_kernel<<<1, 1, 0, s>>>(xmax);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const float *xnorm2,
+                          const float *xmax, int nx, int ld, int ldbf, int d, const float *Q,
+                          int nq, int k, int kc, int take_sqrt, void *qbuf, void *list,
+                          int *fallback, int *n_fallback, int *err, float *out_key,
+                          int *out_idx, cudaStream_t s) {
+    const int nkb = ldbf / TK_KB;
+    const int n_qtiles = (nq + TK_BN - 1) / TK_BN, nq_pad = n_qtiles * TK_BN;
+    const int n_xtiles = (nx + TK_BM - 1) / TK_BM;
+    const int n_xchunks = (n_xtiles + TK_CHUNK_TILES - 1) / TK_CHUNK_TILES;
+    const int cap = (int)knn_tc_list_cap();
+    // query-side buffers carved from qbuf (knn_tc_query_bytes)
+    unsigned char *p = static_cast<unsigned char *>(qbuf);
+    __nv_bfloat16 *Qh = reinterpret_cast<__nv_bfloat16 *>(p);
+    __nv_bfloat16 *Ql = Qh + (size_t)nq_pad * ldbf;
+    float *margin = reinterpret_cast<float *>(Ql + (size_t)nq_pad * ldbf);
+    unsigned *theta = reinterpret_cast<unsigned *>(margin + nq_pad);
+    int *cnt = reinterpret_cast<int *>(theta + nq_pad);
+    float *qsq = reinterpret_cast<float *>(cnt + nq_pad);
+    // |v'_tc - v'_plain| <= e1 |x||q| + e2 (|x|^2 + |q|^2)  (u = 2^-24):
+    //   bf16 hi/lo split of x and of -2q, dropped lo.lo term: 3.1 2^-16 |x||2q|
+    //   fp32 accumulation of K_total = 3 Kp products in the tensor core
+    //   (allowing truncation): 2 K_total u |x||2q|
+    //   fp32 |x|^2 (Kp-term fma chain) and the final add: (Kp + 2) u |x|^2, u |2xq|
+    //   the plain path's direct-difference sum: (d + 4) u (|x| + |q|)^2
+    const double u = std::ldexp(1.0, -24);
+    const double kp = (double)nkb * TK_KB, ktot = 3.0 * kp;
+    const double e1 = 1.1 * (3.1 * std::ldexp(1.0, -16) * 2.0 + 2.0 * ktot * u * 2.0 + 2.0 * u +
+                             (d + 4.0) * u * 2.0);
+    const double e2 = 1.1 * ((kp + 2.0) * u + (d + 4.0) * u * 2.0 + 2.0 * u);
+    {
+        const int wpb = 8;
+        knn_tc_prep_queries<<<(nq_pad + wpb - 1) / wpb, wpb * 32, 0, s>>>(
+            Q, ld, nq, d, nq_pad, ldbf, Qh, Ql, (float)e1, (float)e2, xmax, margin, theta, cnt, qsq);
+        // exact pre-pass over the first training rows (plain kernels; its
+        // partial lists live in the candidate list buffer, its merged keys in
+        // the output arrays, both overwritten below)
+        const int pre = std::min(nx, TK_PRE_ROWS);
+        if (pre >= k) {
+            const int BN = knn_tile_rows_train(false);
+            int n_chunks = std::max(1, std::min((pre + BN - 1) / BN, 8));
+            int chunk_rows = ((pre + n_chunks - 1) / n_chunks + BN - 1) / BN * BN;
+            n_chunks = (pre + chunk_rows - 1) / chunk_rows;
+            KnnArgs pa{ACC_SQEUC, POST_NONE, kc, 2.0, k, chunk_rows, n_chunks};
+            float *pk = static_cast<float *>(list);
+            int *pi = reinterpret_cast<int *>(pk + (size_t)nq * n_chunks * k);
+            cudaError_t e = launch_knn_chunks<float>(Q, ld, nq, X, ld, pre, d, nullptr, nullptr, pa,
+                                                     pk, pi, nullptr, s);
+            if (e == cudaSuccess)
+                e = launch_knn_merge<float>(pk, pi, nq, n_chunks, k, 0, out_key, out_idx, s);
+            if (e != cudaSuccess) return e;
+            knn_tc_init_theta<<<(nq + 255) / 256, 256, 0, s>>>(out_key, k, nq, qsq, margin, theta);
+        }
+        const size_t nl = (size_t)nq * cap;
+        knn_tc_fill_list<<<(unsigned)((nl + 255) / 256), 256, 0, s>>>(static_cast<int2 *>(list), nl);
+        cudaError_t e = cudaMemsetAsync(fallback, 0, (size_t)nq * sizeof(int), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(n_fallback, 0, sizeof(int), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), s);
+        if (e != cudaSuccess) return e;
+    }
+    CUtensorMap mah, mal, mbh, mbl;
+    if (!make_map_bf16_rows(&mah, Xh, nx, ldbf, TK_BM) ||
+        !make_map_bf16_rows(&mal, Xl, nx, ldbf, TK_BM) ||
+        !make_map_bf16_rows(&mbh, Qh, nq_pad, ldbf, TK_BN) ||
+        !make_map_bf16_rows(&mbl, Ql, nq_pad, ldbf, TK_BN))
+        return cudaErrorInvalidValue;
+    int stages = 8;
+    while (stages > 2 && tk_smem_bytes(nkb, stages) > 225 * 1024) --stages;
+    const size_t smem = tk_smem_bytes(nkb, stages);
+    cudaError_t e =
+        cudaFuncSetAttribute(knn_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    KnnTcArgs a;
+    a.nx = nx;
+    a.nq = nq;
+    a.k = k;
+    a.nkb = nkb;
+    a.stages = stages;
+    a.n_qtiles = n_qtiles;
+    a.n_xtiles = n_xtiles;
+    a.n_items = n_qtiles * n_xchunks;
+    a.cap = cap;
+    a.win = k <= 128 ? 256 : 512;
+    a.xnorm = xnorm2;
+    a.margin = margin;
+    a.theta = theta;
+    a.cnt = cnt;
+    a.list = static_cast<int2 *>(list);
+    a.err = err;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = std::min(nsm, a.n_items);
+    knn_tc_kernel<<<grid, TK_THREADS, smem, s>>>(mah, mal, mbh, mbl, a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    knn_tc_finalize<<<nq, 256, (size_t)d * sizeof(float), s>>>(
+        X, Q, ld, d, kc, k, cap, theta, cnt, static_cast<const int2 *>(list), take_sqrt, out_key,
+        out_idx, fallback, n_fallback);
+    return cudaGetLastError();
+}
+
+int *knn_tc_counts(void *qbuf, int nq, int d) {
+    const int nkb = (d + TK_KB - 1) / TK_KB;
+    const size_t nq_pad = (size_t)((nq + TK_BN - 1) / TK_BN) * TK_BN;
+    unsigned char *p = static_cast<unsigned char *>(qbuf) + nq_pad * nkb * TK_KB * 2 * 2;
+    return reinterpret_cast<int *>(p + nq_pad * 8);
+}
+
+size_t knn_tc_query_bytes(int nq, int d) {
+    const int nkb = (d + TK_KB - 1) / TK_KB;
+    const size_t nq_pad = (size_t)((nq + TK_BN - 1) / TK_BN) * TK_BN;
+    return nq_pad * nkb * TK_KB * 2 * 2 + nq_pad * 16 + 256;
+}
+
+} // namespace b200

@@ -52,6 +52,10 @@ NN<T>::NN(ErrorRecord *e, CudaCtx *c, bool single) {
     //   "reference isa": which AOCL-DA build's KC blocking the squared-euclidean
     //   summation order reproduces (avx512: KC=256/512, avx2: KC=64/32).
     opts.add_string("reference isa", {{"avx512", 0}, {"avx2", 1}}, "avx512");
+    //   "precision mode": "bf16x3" lets large fp32 euclidean searches run a
+    //   tensor-core candidate pass with an exact re-score (same neighbours and
+    //   distances as "plain", the SIMT fp32 path).
+    opts.add_string("precision mode", {{"plain", 0}, {"bf16x3", 3}}, "bf16x3");
 }
 
 template <typename T> da_status NN<T>::set_params() {
@@ -141,6 +145,83 @@ template <typename T> da_status NN<T>::ensure_device_data() {
              "upload of X_train");
     X_on_device = true;
     xn_kind = -1;
+    tc_train_ready = false;
+    return da_status_success;
+}
+
+// Tensor-core candidate pass + exact re-score (knn_tc.cu) into dOutK / dOutI,
+// in query batches that bound the candidate lists' memory.  Any query the
+// pass could not certify sends the whole call to the plain path (done =
+// false).
+template <typename T>
+da_status NN<T>::kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_sqrt, bool &done) {
+    done = false;
+    if constexpr (std::is_same_v<T, float>) {
+        cudaStream_t st = cuda->stream;
+        const int nkb = (int)((d + 63) / 64);
+        if (!tc_train_ready || tc_ldbf != nkb * 64) {
+            tc_ldbf = nkb * 64;
+            const size_t xb = (size_t)n_samples * tc_ldbf * 2;
+            if (!dXh.ensure(xb) || !dXl.ensure(xb) || !dXsq.ensure((size_t)n_samples * 4) ||
+                !dTkScal.ensure(64))
+                return err->error(da_status_memory_error, "Device memory allocation failed.");
+            B200_TRY(launch_knn_tc_train_prep(dX.as<float>(), ld, (int)n_samples, (int)d, dXh.p,
+                                              dXl.p, tc_ldbf, dXsq.as<float>(),
+                                              dTkScal.as<float>(), st),
+                     "tensor-core training copies");
+            tc_train_ready = true;
+        }
+        const da_int QB = 16384;
+        const da_int qb = std::min(nq, QB);
+        if (!dTkQ.ensure(knn_tc_query_bytes((int)qb, (int)d)) ||
+            !dTkList.ensure((size_t)qb * knn_tc_list_cap() * 8) ||
+            !dTkFlag.ensure((size_t)qb * sizeof(int)) ||
+            !dOutK.ensure((size_t)nq * k * sizeof(float)) ||
+            !dOutI.ensure((size_t)nq * k * sizeof(int)))
+            return err->error(da_status_memory_error, "Device memory allocation failed.");
+        int *n_fb = reinterpret_cast<int *>(dTkScal.as<char>() + 16);
+        int *errf = n_fb + 1;
+        int h_state[2] = {0, 0};
+        for (da_int q0 = 0; q0 < nq; q0 += QB) {
+            const da_int nb = std::min(QB, nq - q0);
+            B200_TRY(cuda->timed("knn_tc", [&] {
+                return launch_knn_tc(dX.as<float>(), dXh.p, dXl.p, dXsq.as<float>(),
+                                     dTkScal.as<float>(), (int)n_samples, ld, tc_ldbf, (int)d,
+                                     dQ.as<float>() + (size_t)q0 * ld, (int)nb, (int)k, kc,
+                                     take_sqrt ? 1 : 0, dTkQ.p, dTkList.p, dTkFlag.as<int>(),
+                                     n_fb, errf, dOutK.as<float>() + (size_t)q0 * k,
+                                     dOutI.as<int>() + (size_t)q0 * k, st);
+            }), "kNN tensor-core pass");
+            B200_TRY(cudaMemcpyAsync(h_state, n_fb, 2 * sizeof(int), cudaMemcpyDeviceToHost, st),
+                     "copy");
+            std::vector<int> lens((size_t)nb);
+            B200_TRY(cudaMemcpyAsync(lens.data(), knn_tc_counts(dTkQ.p, (int)nb, (int)d),
+                                     lens.size() * sizeof(int), cudaMemcpyDeviceToHost, st),
+                     "copy");
+            B200_TRY(cudaStreamSynchronize(st), "kNN tensor-core pass");
+            double mx = 0, sum = 0;
+            for (int v : lens) {
+                mx = std::max(mx, (double)v);
+                sum += v;
+            }
+            cuda->stats["knn_tc_max_list"] = std::max(cuda->stats["knn_tc_max_list"], mx);
+            cuda->stats["knn_tc_mean_list"] = sum / std::max<double>(1.0, (double)nb);
+            if (h_state[1] != 0)
+                return err->error(da_status_internal_error,
+                                  "The tensor-core kNN kernel timed out waiting on a pipeline "
+                                  "barrier (code " + std::to_string(h_state[1]) + ").");
+            cuda->stats["knn_tc_fallback_queries"] += (double)h_state[0];
+            if (h_state[0] != 0) return da_status_success; // plain path for the whole call
+        }
+        cuda->stats["tensor_core"] = 1.0;
+        done = true;
+    } else {
+        (void)nq;
+        (void)d;
+        (void)k;
+        (void)kc;
+        (void)take_sqrt;
+    }
     return da_status_success;
 }
 
@@ -220,49 +301,62 @@ da_status NN<T>::kneighbors_compute(da_int nq, da_int d, const T *Xt, da_int ldt
     if (!dQ.ensure((size_t)nq * ld * sizeof(T)))
         return err->error(da_status_memory_error, "Device memory allocation failed.");
     B200_TRY(upload_matrix<T>(ord, nq, d, Xt, ldt, dQ.as<T>(), ld, dStage, st), "upload of X_test");
-    const T *qn = nullptr, *xn = nullptr;
-    if (norm_kind >= 0) {
-        if (!dQn.ensure((size_t)nq * sizeof(T)) || !dXn.ensure((size_t)n_samples * sizeof(T)))
-            return err->error(da_status_memory_error, "Device memory allocation failed.");
-        if (norm_kind == 0) {
-            B200_TRY(launch_row_sqnorms<T>(dQ.as<T>(), ld, nq, d, dQn.as<T>(), st), "norms");
-            if (xn_kind != 0)
-                B200_TRY(launch_row_sqnorms<T>(dX.as<T>(), ld, n_samples, d, dXn.as<T>(), st), "norms");
-        } else {
-            B200_TRY(launch_row_norms_eps1<T>(dQ.as<T>(), ld, nq, d, dQn.as<T>(), st), "norms");
-            if (xn_kind != 1)
-                B200_TRY(launch_row_norms_eps1<T>(dX.as<T>(), ld, n_samples, d, dXn.as<T>(), st), "norms");
-        }
-        xn_kind = norm_kind;
-        qn = dQn.as<T>();
-        xn = dXn.as<T>();
+    cuda->stats["tensor_core"] = 0.0;
+    cuda->stats["knn_tc_fallback_queries"] = 0.0;
+    bool tc_done = false;
+    const bool tc_metric =
+        metric == M_EUC || metric == M_SQEUC || (metric == M_MINK && p == T(2));
+    if (!fp64 && tc_metric && opts.key("precision mode") != 0 &&
+        knn_tc_supported((int)n_samples, (int)d, (int)k) && n_samples >= 65536 &&
+        (double)n_samples * (double)nq * (double)d >= 4.0e9) {
+        s = kneighbors_tc(nq, d, k, kc, metric != M_SQEUC, tc_done);
+        if (s != da_status_success) return s;
     }
-    if (k > knn_max_k(fp64))
-        return err->error(da_status_not_implemented,
-                          "k = " + std::to_string(k) + " exceeds the largest supported number "
-                          "of neighbours per query (" + std::to_string(knn_max_k(fp64)) + ").");
-    // chunking of the training rows: enough CTAs to fill 148 SMs several times
-    const int BN = knn_tile_rows_train(fp64);
-    const int q_tiles = (int)((nq + 63) / 64);
-    const int max_chunks = std::max(1, (int)((n_samples + BN - 1) / BN));
-    int n_chunks = std::max(1, std::min(max_chunks, (148 * 8 + q_tiles - 1) / q_tiles));
-    int chunk_rows = (int)((n_samples + n_chunks - 1) / n_chunks);
-    chunk_rows = ((chunk_rows + BN - 1) / BN) * BN;
-    n_chunks = (int)((n_samples + chunk_rows - 1) / chunk_rows);
-    KnnArgs a{acc, post, kc, (double)p, (int)k, chunk_rows, n_chunks};
-    const size_t parts = (size_t)nq * n_chunks * k;
-    if (!dPartK.ensure(parts * sizeof(T)) || !dPartI.ensure(parts * sizeof(int)) ||
-        !dOutK.ensure((size_t)nq * k * sizeof(T)) || !dOutI.ensure((size_t)nq * k * sizeof(int)))
-        return err->error(da_status_memory_error, "Device memory allocation failed.");
-    B200_TRY(cuda->timed("knn_chunks", [&] {
-        return launch_knn_chunks<T>(dQ.as<T>(), ld, (int)nq, dX.as<T>(), ld, (int)n_samples,
-                                    (int)d, qn, xn, a, dPartK.as<T>(), dPartI.as<int>(), nullptr,
-                                    st);
-    }), "kNN distance kernel");
-    B200_TRY(cuda->timed("knn_merge", [&] {
-        return launch_knn_merge<T>(dPartK.as<T>(), dPartI.as<int>(), (int)nq, n_chunks, (int)k,
-                                   tf, dOutK.as<T>(), dOutI.as<int>(), st);
-    }), "kNN merge kernel");
+    if (!tc_done) {
+        const T *qn = nullptr, *xn = nullptr;
+        if (norm_kind >= 0) {
+            if (!dQn.ensure((size_t)nq * sizeof(T)) || !dXn.ensure((size_t)n_samples * sizeof(T)))
+                return err->error(da_status_memory_error, "Device memory allocation failed.");
+            if (norm_kind == 0) {
+                B200_TRY(launch_row_sqnorms<T>(dQ.as<T>(), ld, nq, d, dQn.as<T>(), st), "norms");
+                if (xn_kind != 0)
+                    B200_TRY(launch_row_sqnorms<T>(dX.as<T>(), ld, n_samples, d, dXn.as<T>(), st), "norms");
+            } else {
+                B200_TRY(launch_row_norms_eps1<T>(dQ.as<T>(), ld, nq, d, dQn.as<T>(), st), "norms");
+                if (xn_kind != 1)
+                    B200_TRY(launch_row_norms_eps1<T>(dX.as<T>(), ld, n_samples, d, dXn.as<T>(), st), "norms");
+            }
+            xn_kind = norm_kind;
+            qn = dQn.as<T>();
+            xn = dXn.as<T>();
+        }
+        if (k > knn_max_k(fp64))
+            return err->error(da_status_not_implemented,
+                              "k = " + std::to_string(k) + " exceeds the largest supported number "
+                              "of neighbours per query (" + std::to_string(knn_max_k(fp64)) + ").");
+        // chunking of the training rows: enough CTAs to fill 148 SMs several times
+        const int BN = knn_tile_rows_train(fp64);
+        const int q_tiles = (int)((nq + 63) / 64);
+        const int max_chunks = std::max(1, (int)((n_samples + BN - 1) / BN));
+        int n_chunks = std::max(1, std::min(max_chunks, (148 * 8 + q_tiles - 1) / q_tiles));
+        int chunk_rows = (int)((n_samples + n_chunks - 1) / n_chunks);
+        chunk_rows = ((chunk_rows + BN - 1) / BN) * BN;
+        n_chunks = (int)((n_samples + chunk_rows - 1) / chunk_rows);
+        KnnArgs a{acc, post, kc, (double)p, (int)k, chunk_rows, n_chunks};
+        const size_t parts = (size_t)nq * n_chunks * k;
+        if (!dPartK.ensure(parts * sizeof(T)) || !dPartI.ensure(parts * sizeof(int)) ||
+            !dOutK.ensure((size_t)nq * k * sizeof(T)) || !dOutI.ensure((size_t)nq * k * sizeof(int)))
+            return err->error(da_status_memory_error, "Device memory allocation failed.");
+        B200_TRY(cuda->timed("knn_chunks", [&] {
+            return launch_knn_chunks<T>(dQ.as<T>(), ld, (int)nq, dX.as<T>(), ld, (int)n_samples,
+                                        (int)d, qn, xn, a, dPartK.as<T>(), dPartI.as<int>(), nullptr,
+                                        st);
+        }), "kNN distance kernel");
+        B200_TRY(cuda->timed("knn_merge", [&] {
+            return launch_knn_merge<T>(dPartK.as<T>(), dPartI.as<int>(), (int)nq, n_chunks, (int)k,
+                                       tf, dOutK.as<T>(), dOutI.as<int>(), st);
+        }), "kNN merge kernel");
+    }
     ind.resize((size_t)nq * k);
     std::vector<int> tmp((size_t)nq * k);
     B200_TRY(cudaMemcpyAsync(tmp.data(), dOutI.p, tmp.size() * sizeof(int), cudaMemcpyDeviceToHost, st),
