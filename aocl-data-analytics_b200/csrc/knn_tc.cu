@@ -73,6 +73,14 @@ __device__ __forceinline__ void tk_raise(int *abort_flag, int *err, int code) {
     atomicExch(err, code);
 }
 
+// v[u] for a runtime u without dynamic register indexing (selects).
+__device__ __forceinline__ float pick32(const float (&v)[32], int u) {
+    float r = v[0];
+#pragma unroll
+    for (int i = 1; i < 32; ++i) r = (u == i) ? v[i] : r;
+    return r;
+}
+
 // Ascending bitonic sort of 512 floats held 16 per lane (element i = 16 lane + e).
 __device__ __forceinline__ void warp_sort512(float (&a)[16]) {
     const int lane = threadIdx.x & 31;
@@ -288,19 +296,30 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                     for (int u = 0; u < 32; ++u)
                         m = fminf(m, __fadd_rn(v[u], xn) - thw[c * 32 + u]);
                     if (!__any_sync(0xffffffffu, m < 0.f)) continue;
-                    // rare: some value below its query's threshold
+                    // rare: some values below their query's threshold.  First
+                    // the columns that have any (statically indexed, so v stays
+                    // in registers), and every such column's list slots reserved
+                    // at once (lane u reserves for column u).
+                    unsigned colbits = 0, mymask = 0;
+#pragma unroll
                     for (int u = 0; u < 32; ++u) {
+                        const unsigned mk =
+                            __ballot_sync(0xffffffffu, __fadd_rn(v[u], xn) < thw[c * 32 + u]);
+                        colbits |= (mk ? 1u : 0u) << u;
+                        if (lane == u) mymask = mk;
+                    }
+                    int mybase = 0;
+                    if (mymask) mybase = atomicAdd(&a.cnt[qt * TK_BN + c * 32 + lane], __popc(mymask));
+                    while (colbits) {
+                        const int u = __ffs(colbits) - 1;
+                        colbits &= colbits - 1;
                         const int col = c * 32 + u;
-                        const float sv = __fadd_rn(v[u], xn);
-                        const bool pred = sv < thw[col];
-                        const unsigned mask = __ballot_sync(0xffffffffu, pred);
-                        if (!mask) continue;
                         const int gq = qt * TK_BN + col;
-                        const int leader = __ffs(mask) - 1, nadd = __popc(mask);
-                        int base0 = 0;
-                        if (lane == leader) base0 = atomicAdd(&a.cnt[gq], nadd);
-                        base0 = __shfl_sync(0xffffffffu, base0, leader);
-                        if (pred) {
+                        const unsigned mask = __shfl_sync(0xffffffffu, mymask, u);
+                        const int base0 = __shfl_sync(0xffffffffu, mybase, u);
+                        const int nadd = __popc(mask);
+                        if ((mask >> lane) & 1u) {
+                            const float sv = __fadd_rn(pick32(v, u), xn);
                             const int pos = base0 + __popc(mask & ((1u << lane) - 1u));
                             if (pos < a.cap)
                                 a.list[(size_t)gq * a.cap + pos] = make_int2(__float_as_int(sv), row);
