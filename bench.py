@@ -208,6 +208,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain fp32 comparison")
+    ap.add_argument("--no-knn", action="store_true", help="skip the kNN (4.04M x 128) leg")
+    ap.add_argument("--knn-only", action="store_true",
+                    help="run only the kNN leg (profiling captures) and print its JSON")
+    ap.add_argument("--knn-rows", type=int, default=4_000_000)
+    ap.add_argument("--knn-queries", type=int, default=10_000)
+    ap.add_argument("--knn-plain", type=int, default=1,
+                    help="with --knn-only: also run the plain path (1) or not (0)")
     ap.add_argument("--rows", type=int, default=N,
                     help="rows of X (default 1,000,000; smaller only for profiling captures)")
     args = ap.parse_args()
@@ -223,6 +230,11 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     ab = _load("aoclda_b200", os.path.join(PKG, "aoclda_b200.py"))
+    if args.knn_only:
+        if rank == 0:
+            print(json.dumps(run_knn(ab, nx=args.knn_rows, nq=args.knn_queries,
+                                     plain=bool(args.knn_plain))))
+        return 0
 
     X = make_data()
     stream = torch.cuda.current_stream()
@@ -315,7 +327,10 @@ def main():
     hbm, bf16, peak_src = load_peaks()
     flops = 2.0 * N * K * D
     ldbf = 64 * ((D + 63) // 64)
-    traffic_alg = N * ldbf * 2 + N * 4 * 3  # bf16 X + labels, previous labels, |x|
+    terms = 2 if os.environ.get("BENCH_MODE", "bf16x3") == "bf16x3" else 1
+    # bf16 copies of X read by the MMA (hi and lo for bf16x3) + labels,
+    # previous labels and |x|
+    traffic_alg = N * ldbf * 2 * terms + N * 4 * 3
     achieved_tflops = flops / (a_avg / 1e3) / 1e12
     achieved_gbs = traffic_alg / (a_avg / 1e3) / 1e9
     t_tensor = flops / (bf16 * 1e12)
@@ -343,6 +358,9 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline(X, C0, int(os.environ.get("BENCH_CPU_SAMPLE", "131072")), 2)
+    knn = None
+    if rank == 0 and world == 1 and not args.no_knn:
+        knn = run_knn(ab)
     extra = {"iterations_per_step": n_iter, "init_ms": init_ms,
              "relabelled_rows_last_iteration": relabelled,
              "full_scan_rows_last_iteration": full_scan,
@@ -356,16 +374,68 @@ def main():
         "roofline": roof,
         "cpu_baseline": cb,
         "e2e": e2e,
-        "gpu_launches": (12 * n_iter + 6) * args.steps,
+        "gpu_launches": (6 * n_iter + 8) * args.steps,
         "clocks": clocks,
         "plain_fp32": plain,
         "speedup_vs_plain_fp32": (value / plain["value"]) if plain else None,
+        "knn": knn,
     }
     if rank == 0:
         print(json.dumps(out))
+        sys.stdout.flush()
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def run_knn(ab, nx=4_000_000, nq=10_000, d=128, k=100, comps=1024, seed=3, reps=3, plain=True):
+    """Brute-force kNN, fp32 euclidean: 4,000,000 x 128 training rows from a
+    1,024-component Gaussian mixture (the k-means recipe) plus 1% exact
+    duplicate rows (ties), 10,000 queries from the same mixture, k = 100.
+    Each timed call is one da_nn_kneighbors_s over all queries with host
+    arrays (queries up, indices and distances down).  The tensor-core path
+    (bf16x3 candidate pass + exact re-score) and the plain fp32 path must
+    return identical indices and distances."""
+    rng = np.random.default_rng(seed)
+    means = rng.uniform(-10.0, 10.0, (comps, d)).astype(np.float32)
+    sig = rng.uniform(0.5, 2.0, comps).astype(np.float32)
+    w = rng.dirichlet(np.ones(comps))
+    lab = rng.choice(comps, nx, p=w)
+    X = means[lab] + rng.standard_normal((nx, d), dtype=np.float32) * sig[lab, None]
+    X = np.concatenate([X, X[rng.integers(0, nx, nx // 100)]])
+    ql = rng.choice(comps, nq, p=w)
+    Q = means[ql] + rng.standard_normal((nq, d), dtype=np.float32) * sig[ql, None]
+    res = {}
+    for mode in ("bf16x3", "plain") if plain else ("bf16x3",):
+        nn = ab.KNN("s", order=ab.ROW_MAJOR, metric="euclidean", precision_mode=mode).fit(X)
+        nn.kneighbors(Q[:512], k)
+        nn.L.da_b200_set_kernel_timing(nn.h, 1)
+        ts = []
+        for _ in range(reps if mode == "bf16x3" else 1):
+            t = time.perf_counter()
+            ind, dist = nn.kneighbors(Q, k)
+            ts.append(time.perf_counter() - t)
+        kern = {}
+        for name in ("knn_tc", "knn_chunks", "knn_merge"):
+            ms_, n_ = nn.kernel_time(name)
+            if n_:
+                kern[name] = ms_ / n_
+        res[mode] = {"s": min(ts), "ind": ind, "dist": dist, "tc": nn.stat("tensor_core"),
+                     "kernel_ms": kern, "list_mean": nn.stat("knn_tc_mean_list")}
+        nn.close()
+    tc, pl = res["bf16x3"], res.get("plain")
+    flops = 2.0 * (nx + nx // 100) * nq * d
+    return {"workload": f"knn_fp32_euclidean_{nx + nx // 100}x{d}_q{nq}_k{k}",
+            "unit": "queries/s", "qps": nq / tc["s"],
+            "plain_qps": nq / pl["s"] if pl else None,
+            "speedup_vs_plain_fp32": pl["s"] / tc["s"] if pl else None,
+            "identical_to_plain": bool(np.array_equal(tc["ind"], pl["ind"]) and
+                                       np.array_equal(tc["dist"], pl["dist"])) if pl else None,
+            "tensor_core": tc["tc"] == 1.0, "kernel_ms": tc["kernel_ms"],
+            "plain_kernel_ms": pl["kernel_ms"] if pl else None,
+            "tensor_tflops_algorithmic": flops / (tc["kernel_ms"].get("knn_tc", float("nan")) / 1e3) / 1e12,
+            "candidate_list_mean": tc["list_mean"],
+            "timing": "wall clock of one da_nn_kneighbors_s call with host arrays (best of 3)"}
 
 
 def run_e2e(ab, km, X, C0, stream, args, world):
