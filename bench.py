@@ -341,7 +341,16 @@ def main():
     else:
         roof = {"bound": "tensor", "achieved": achieved_tflops, "peak": bf16, "unit": "TFLOP/s",
                 "frac": achieved_tflops / bf16}
-    roof.update({"traffic": None, "peak_source": peak_src,
+    traffic, traffic_src = None, None
+    prof = os.path.join(ROOT, "profiles", "kmeans_tc_kernels_600kx64_k256_ncu.md")
+    if tensor_core and N == 1_000_000 and os.path.exists(prof):
+        import re
+        m = re.search(r"dram_bytes_per_launch_scaled_to_1000000_rows: (\d+)", open(prof).read())
+        if m:
+            traffic = int(m.group(1))
+            traffic_src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at "
+                           "600,000 rows, scaled by rows (profiles/kmeans_tc_kernels_600kx64_k256_ncu.md)")
+    roof.update({"traffic": traffic, "traffic_source": traffic_src, "peak_source": peak_src,
                  "kernel": "kmeans_assign_tc_kernel (tcgen05 bf16, TMEM fp32)" if tensor_core
                  else "kmeans_assign_kernel (SIMT fp32)",
                  "algorithmic_flops_per_launch": flops,
