@@ -372,3 +372,35 @@ def pairwise_distances(X, Y=None, metric="euclidean", p=2.0, prec="d", order=COL
         order, m, n, k, ptr(X), _ld(X, order), ptr(Y), _ld(Y, order) if Y is not None else 0,
         ptr(D), ldd, p, METRICS[metric])
     return st, D
+
+
+def kmeans_batched(Xs, C0s, max_iter=300, tol=1e-4):
+    """da_b200_kmeans_batched_s over lists of fp32 data sets and initial
+    centres (row-major); returns a list of dicts with centres, labels,
+    n_iter, inertia and converged for every data set."""
+    L = lib()
+    m = len(Xs)
+    Xs = [np.ascontiguousarray(x, dtype=np.float32) for x in Xs]
+    C0s = [np.ascontiguousarray(c, dtype=np.float32) for c in C0s]
+    ns = (da_int * m)(*[x.shape[0] for x in Xs])
+    ds = (da_int * m)(*[x.shape[1] for x in Xs])
+    ks = (da_int * m)(*[c.shape[0] for c in C0s])
+    lds = (da_int * m)(*[x.shape[1] for x in Xs])
+    fp = C.POINTER(C.c_float)
+    A = (fp * m)(*[x.ctypes.data_as(fp) for x in Xs])
+    C0 = (fp * m)(*[c.ctypes.data_as(fp) for c in C0s])
+    outs = [np.zeros_like(c) for c in C0s]
+    labs = [np.zeros(x.shape[0], dtype=np.int32) for x in Xs]
+    CO = (fp * m)(*[o.ctypes.data_as(fp) for o in outs])
+    ip = C.POINTER(da_int)
+    LO = (ip * m)(*[l.ctypes.data_as(ip) for l in labs])
+    nit = (da_int * m)()
+    inert = (C.c_double * m)()
+    conv = (da_int * m)()
+    st = L.da_b200_kmeans_batched_s(m, ns, ds, ks, A, lds, C0, max_iter, C.c_double(tol), CO, LO,
+                                    nit, inert, conv, None)
+    if st != SUCCESS:
+        raise DAError(st, "da_b200_kmeans_batched_s")
+    return [{"centres": outs[i], "labels": labs[i], "n_iter": int(nit[i]),
+             "inertia": float(inert[i]), "converged": int(conv[i])} for i in range(m)]
+

@@ -42,6 +42,30 @@ da_status da_b200_get_stat(da_handle handle, const char *name, double *value);
 da_status da_b200_kmeans_init_centres_d(da_handle handle, double *C, da_int ldc);
 da_status da_b200_kmeans_init_centres_s(da_handle handle, float *C, da_int ldc);
 
+/* No counterpart in the AOCL-DA API.  Lloyd k-means on n_inst independent
+ * fp32 data sets at once (different n, d and k): instance i has n_samples[i]
+ * rows of n_features[i] values (row-major host array A[i], leading dimension
+ * lda[i]) and n_clusters[i] initial centres (row-major k x d host array
+ * C_init[i]).  Every instance gives exactly what da_kmeans_compute_s gives
+ * for that data with "precision mode" = "plain", "initialization method" =
+ * "supplied", n_init = 1, the same max_iter and convergence tolerance, and
+ * "empty clusters" = "ignore": centres (C_out[i], k x d row-major), labels
+ * (labels_out[i]), iteration count, convergence code (0: max_iter reached,
+ * 1: centre shift below tol, 2: labels unchanged) and inertia (fp64 sum, to
+ * within rounding).  All instances advance together on the device, each
+ * Lloyd iteration one pass over (instance, tile) work tables, the whole fit
+ * one CUDA graph.  Limits: k <= n and k * d <= 8192 per instance; finite
+ * data (else da_status_invalid_input).  `stream`: a cudaStream_t the inputs
+ * are uploaded on (NULL: the legacy default stream); the call returns when
+ * the results are on the host. */
+da_status da_b200_kmeans_batched_s(da_int n_inst, const da_int *n_samples,
+                                   const da_int *n_features, const da_int *n_clusters,
+                                   const float *const *A, const da_int *lda,
+                                   const float *const *C_init, da_int max_iter, double tol,
+                                   float *const *C_out, da_int *const *labels_out,
+                                   da_int *n_iter, double *inertia, da_int *converged,
+                                   void *stream);
+
 /* No counterpart in the AOCL-DA API.  Brute-force euclidean k nearest
  * neighbours for callers that cannot allocate device memory (code running
  * inside a device allocator or memory-pool callback, real-time pipelines that
