@@ -397,6 +397,7 @@ extern "C" da_status da_b200_kmeans_batched_s(da_int n_inst, const da_int *n_sam
                                               double tol, float *const *C_out,
                                               da_int *const *labels_out, da_int *n_iter,
                                               double *inertia, da_int *converged, void *stream) {
+    if (sizeof(da_int) != sizeof(int)) return da_status_not_implemented;
     if (n_inst < 1) return da_status_invalid_array_dimension;
     if (!n_samples || !n_features || !n_clusters || !A || !lda || !C_init || !C_out ||
         !labels_out || !n_iter || !inertia || !converged)
@@ -475,23 +476,16 @@ extern "C" da_status da_b200_kmeans_batched_s(da_int n_inst, const da_int *n_sam
         cudaGetLastError();
         return da_status_memory_error;
     }
-    // upload (rows padded to ld), initial centres into Cb0
+    // upload: rows padded to ld by the copy engine, initial centres into Cb0
     {
-        std::vector<float> stage;
+        ok(cudaMemsetAsync(X.p, 0, xo * sizeof(float), s));
+        ok(cudaMemsetAsync(Cb0.p, 0, co * sizeof(float), s));
         for (da_int i = 0; i < n_inst && e == cudaSuccess; ++i) {
             const KbInst &I = hi[i];
-            stage.assign((size_t)I.n * I.ld, 0.f);
-            for (int r = 0; r < I.n; ++r)
-                std::memcpy(&stage[(size_t)r * I.ld], A[i] + (size_t)r * lda[i], I.d * sizeof(float));
-            ok(cudaMemcpyAsync(X.p + I.xo, stage.data(), stage.size() * sizeof(float),
-                               cudaMemcpyHostToDevice, s));
-            ok(cudaStreamSynchronize(s));
-            stage.assign((size_t)I.k * I.ld, 0.f);
-            for (int j = 0; j < I.k; ++j)
-                std::memcpy(&stage[(size_t)j * I.ld], C_init[i] + (size_t)j * I.d, I.d * sizeof(float));
-            ok(cudaMemcpyAsync(Cb0.p + I.co, stage.data(), stage.size() * sizeof(float),
-                               cudaMemcpyHostToDevice, s));
-            ok(cudaStreamSynchronize(s));
+            ok(cudaMemcpy2DAsync(X.p + I.xo, (size_t)I.ld * 4, A[i], (size_t)lda[i] * 4,
+                                 (size_t)I.d * 4, I.n, cudaMemcpyHostToDevice, s));
+            ok(cudaMemcpy2DAsync(Cb0.p + I.co, (size_t)I.ld * 4, C_init[i], (size_t)I.d * 4,
+                                 (size_t)I.d * 4, I.k, cudaMemcpyHostToDevice, s));
         }
         ok(cudaMemsetAsync(Cb1.p, 0, co * sizeof(float), s));
         ok(cudaMemsetAsync(Lb0.p, 0, lo * sizeof(int), s));
@@ -561,23 +555,17 @@ extern "C" da_status da_b200_kmeans_batched_s(da_int n_inst, const da_int *n_sam
     std::vector<double> hin(n_inst);
     ok(cudaMemcpy(fin.data(), inst.p, fin.size() * sizeof(KbInst), cudaMemcpyDeviceToHost));
     ok(cudaMemcpy(hin.data(), inert.p, hin.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    std::vector<float> cbuf;
-    std::vector<int> lbuf;
     for (da_int i = 0; i < n_inst && e == cudaSuccess; ++i) {
         const KbInst &I = fin[i];
-        cbuf.resize((size_t)I.k * I.ld);
-        ok(cudaMemcpy(cbuf.data(), (I.fc ? Cb1.p : Cb0.p) + I.co, cbuf.size() * sizeof(float),
-                      cudaMemcpyDeviceToHost));
-        for (int j = 0; j < I.k; ++j)
-            std::memcpy(C_out[i] + (size_t)j * I.d, &cbuf[(size_t)j * I.ld], I.d * sizeof(float));
-        lbuf.resize(I.n);
-        ok(cudaMemcpy(lbuf.data(), (I.fl ? Lb1.p : Lb0.p) + I.lo, lbuf.size() * sizeof(int),
-                      cudaMemcpyDeviceToHost));
-        for (int r = 0; r < I.n; ++r) labels_out[i][r] = (da_int)lbuf[r];
+        ok(cudaMemcpy2DAsync(C_out[i], (size_t)I.d * 4, (I.fc ? Cb1.p : Cb0.p) + I.co,
+                             (size_t)I.ld * 4, (size_t)I.d * 4, I.k, cudaMemcpyDeviceToHost, cs));
+        ok(cudaMemcpyAsync(labels_out[i], (I.fl ? Lb1.p : Lb0.p) + I.lo, (size_t)I.n * sizeof(int),
+                           cudaMemcpyDeviceToHost, cs));
         n_iter[i] = I.n_iter;
         inertia[i] = hin[i];
         converged[i] = I.conv;
     }
+    ok(cudaStreamSynchronize(cs));
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (ev) cudaEventDestroy(ev);

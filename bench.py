@@ -209,6 +209,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain fp32 comparison")
     ap.add_argument("--no-knn", action="store_true", help="skip the kNN (4.04M x 128) leg")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched k-means (512 data sets) leg")
     ap.add_argument("--knn-only", action="store_true",
                     help="run only the kNN leg (profiling captures) and print its JSON")
     ap.add_argument("--knn-rows", type=int, default=4_000_000)
@@ -370,6 +372,9 @@ def main():
     knn = None
     if rank == 0 and world == 1 and not args.no_knn:
         knn = run_knn(ab)
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = run_batched(ab)
     extra = {"iterations_per_step": n_iter, "init_ms": init_ms,
              "relabelled_rows_last_iteration": relabelled,
              "full_scan_rows_last_iteration": full_scan,
@@ -388,6 +393,7 @@ def main():
         "plain_fp32": plain,
         "speedup_vs_plain_fp32": (value / plain["value"]) if plain else None,
         "knn": knn,
+        "kmeans_batched": batched,
     }
     if rank == 0:
         print(json.dumps(out))
@@ -445,6 +451,53 @@ def run_knn(ab, nx=4_000_000, nq=10_000, d=128, k=100, comps=1024, seed=3, reps=
             "tensor_tflops_algorithmic": flops / (tc["kernel_ms"].get("knn_tc", float("nan")) / 1e3) / 1e12,
             "candidate_list_mean": tc["list_mean"],
             "timing": "wall clock of one da_nn_kneighbors_s call with host arrays (best of 3)"}
+
+
+def run_batched(ab, count=512, max_iter=30, tol=1e-4, seed=4):
+    """Batched k-means: 512 independent fp32 data sets, n lognormal(ln 20000,
+    1) clipped to [1000, 200000], d uniform in {16, 32, 64, 128}, k uniform in
+    [8, 64], each a Gaussian mixture with k components (the k-means recipe),
+    initial centres k distinct rows, 30 Lloyd iterations at most (tol 1e-4).
+    One da_b200_kmeans_batched_s call (host arrays in and out) against one
+    da_kmeans_compute_s call per data set (precision mode plain, the
+    semantics the batched path reproduces); results must be identical."""
+    rng = np.random.default_rng(seed)
+    Xs, C0s = [], []
+    for _ in range(count):
+        n = int(np.clip(rng.lognormal(np.log(20000), 1.0), 1000, 200000))
+        d = int(rng.choice([16, 32, 64, 128]))
+        k = int(rng.integers(8, 65))
+        means = rng.uniform(-10.0, 10.0, (k, d)).astype(np.float32)
+        sig = rng.uniform(0.5, 2.0, k).astype(np.float32)
+        w = rng.dirichlet(np.ones(k))
+        lab = rng.choice(k, n, p=w)
+        X = means[lab] + rng.standard_normal((n, d), dtype=np.float32) * sig[lab, None]
+        Xs.append(np.ascontiguousarray(X))
+        C0s.append(X[rng.choice(n, k, replace=False)].copy())
+    ab.kmeans_batched(Xs[:4], C0s[:4], max_iter=max_iter, tol=tol)  # warm-up
+    t = time.perf_counter()
+    out = ab.kmeans_batched(Xs, C0s, max_iter=max_iter, tol=tol)
+    tb = time.perf_counter() - t
+    same = True
+    t = time.perf_counter()
+    for X, C0, r in zip(Xs, C0s, out):
+        km = ab.KMeans(C0.shape[0], "s", order=ab.ROW_MAJOR, max_iter=max_iter, n_init=1)
+        km.set("convergence tolerance", tol)
+        km.set("precision mode", "plain")
+        km.fit(X, C0)
+        same = same and int(km.rinfo()[3]) == r["n_iter"] and \
+            np.array_equal(km.labels(X.shape[0]), r["labels"])
+        km.close()
+    ts = time.perf_counter() - t
+    iters = sum(r["n_iter"] for r in out)
+    rows = sum(x.shape[0] for x in Xs)
+    return {"workload": f"kmeans_batched_fp32_{count}_instances_{rows}_rows_maxit{max_iter}",
+            "unit": "Lloyd iterations/s (summed over instances)",
+            "value": iters / tb, "batched_s": tb, "per_instance_calls_s": ts,
+            "speedup_vs_per_instance_calls": ts / tb, "identical_to_single": bool(same),
+            "total_iterations": iters,
+            "timing": "wall clock of the public calls with host arrays; the per-instance "
+                      "time includes labels download and comparison per call"}
 
 
 def run_e2e(ab, km, X, C0, stream, args, world):
