@@ -1,0 +1,206 @@
+"""Request loop over device-resident kNN indexes and k-means models.
+
+The training set of the kNN index and the centres of the k-means models stay
+in device memory for the life of the server (one library handle per worker).
+Requests -- a kNN search (queries, k) or a k-means predict (model, queries)
+-- are queued as they arrive.  Each worker thread repeatedly takes the
+pending requests of its kind that fit its share of the device-memory budget
+and its query cap (continuous batching: requests that arrive while a batch
+runs join the next one) and serves them with ONE library call: for kNN the
+queries are concatenated and searched with the largest k asked for; every
+request gets the prefix it asked for, which is exactly its own search because
+results are ordered by (distance, index).  Several kNN workers run their
+batches at the same time, each on its own handle, so their device work
+overlaps.  Every request records when it was submitted and completed;
+`latency_summary` gives p50 / p99.
+
+The library calls release the Python interpreter lock (ctypes), so the worker
+threads' device work proceeds concurrently.
+"""
+import collections
+import threading
+import time
+
+import numpy as np
+
+# device bytes per query of a kNN batch: the query row, its candidate list of
+# the tensor-core pass (8,192 entries of 8 bytes) and its outputs (k <= 256)
+KNN_LIST_BYTES = 8192 * 8
+KNN_OUT_BYTES = 256 * 8
+
+
+class Request:
+    __slots__ = ("kind", "queries", "k", "model", "t_submit", "t_done", "result", "_done")
+
+    def __init__(self, kind, queries, k=None, model=None):
+        if kind not in ("knn", "predict"):
+            raise ValueError("kind must be 'knn' or 'predict'")
+        self.kind = kind
+        self.queries = np.ascontiguousarray(queries, dtype=np.float32)
+        self.k = k
+        self.model = model
+        self.t_submit = None
+        self.t_done = None
+        self.result = None
+        self._done = threading.Event()
+
+    def wait(self, timeout=None):
+        return self._done.wait(timeout)
+
+    @property
+    def latency(self):
+        return None if self.t_done is None else self.t_done - self.t_submit
+
+
+class Server:
+    """kNN index X (n x d, fp32, euclidean) and k-means models given as
+    {name: (training rows, initial centres)}, fitted at start-up.  `workers`
+    kNN worker threads (one handle each) and one predict worker."""
+
+    def __init__(self, ab, X, models=None, workers=2, max_batch_queries=1024,
+                 hbm_budget=16 << 30, precision_mode="bf16x3"):
+        self.ab = ab
+        self.X = np.ascontiguousarray(X, dtype=np.float32)
+        self.d = self.X.shape[1]
+        self.max_batch_queries = max_batch_queries
+        self.hbm_budget = hbm_budget
+        self.cv = threading.Condition()
+        self.pending = {"knn": collections.deque(), "predict": collections.deque()}
+        self.stopping = False
+        self.completed = []
+        self.batches = []          # (kind, requests, queries) of every library call
+        self.knn_handles = []
+        for _ in range(workers):
+            h = ab.KNN("s", order=ab.ROW_MAJOR, metric="euclidean",
+                       precision_mode=precision_mode)
+            h.fit(self.X)
+            # one call so that the device-side copies exist before the first request
+            h.kneighbors(self.X[:1], 1)
+            self.knn_handles.append(h)
+        self.models = {}
+        for name, (Xm, C0) in (models or {}).items():
+            km = ab.KMeans(C0.shape[0], "s", order=ab.ROW_MAJOR, max_iter=50, n_init=1)
+            km.fit(Xm, C0)
+            self.models[name] = km
+        self.bytes_per_query = self.d * 4 + KNN_LIST_BYTES + KNN_OUT_BYTES
+        self.threads = [threading.Thread(target=self._knn_worker, args=(w,), daemon=True)
+                        for w in range(workers)]
+        self.threads.append(threading.Thread(target=self._predict_worker, daemon=True))
+        for t in self.threads:
+            t.start()
+
+    # ------------------------------------------------------------ clients --
+    def submit(self, req):
+        if req.kind == "predict" and req.model not in self.models:
+            raise KeyError(f"unknown model {req.model!r}")
+        if req.kind == "knn" and not (1 <= req.k <= 256):
+            raise ValueError("k must be in [1, 256]")
+        req.t_submit = time.perf_counter()
+        with self.cv:
+            self.pending[req.kind].append(req)
+            self.cv.notify_all()
+        return req
+
+    def close(self):
+        with self.cv:
+            self.stopping = True
+            self.cv.notify_all()
+        for t in self.threads:
+            t.join()
+        for h in self.knn_handles:
+            h.close()
+        for km in self.models.values():
+            km.close()
+
+    # ------------------------------------------------------------ workers --
+    def _take(self, kind, cap_queries, cap_bytes, per_query_bytes, same_model=False):
+        """Oldest pending requests of `kind` within the caps (at least one);
+        blocks until one is pending, None once the server stops."""
+        with self.cv:
+            while not self.pending[kind] and not self.stopping:
+                self.cv.wait()
+            q = self.pending[kind]
+            if not q:
+                return None
+            batch, nq = [], 0
+            model = q[0].model
+            i = 0
+            while i < len(q):
+                r = q[i]
+                m = r.queries.shape[0]
+                if same_model and r.model != model:
+                    i += 1
+                    continue
+                if batch and (nq + m > cap_queries or (nq + m) * per_query_bytes > cap_bytes):
+                    break
+                batch.append(r)
+                nq += m
+                del q[i]
+            return batch
+
+    def _finish(self, kind, batch, nq):
+        t = time.perf_counter()
+        for r in batch:
+            r.t_done = t
+            r._done.set()
+        with self.cv:
+            self.completed.extend(batch)
+            self.batches.append((kind, len(batch), nq))
+
+    def _knn_worker(self, w):
+        h = self.knn_handles[w]
+        share = self.hbm_budget // len(self.knn_handles)
+        while True:
+            batch = self._take("knn", self.max_batch_queries, share, self.bytes_per_query)
+            if batch is None:
+                return
+            Q = batch[0].queries if len(batch) == 1 else np.concatenate([r.queries for r in batch])
+            kmax = max(r.k for r in batch)
+            ind, dist = h.kneighbors(Q, kmax)
+            o = 0
+            for r in batch:
+                m = r.queries.shape[0]
+                r.result = (ind[o:o + m, :r.k].copy(), dist[o:o + m, :r.k].copy())
+                o += m
+            self._finish("knn", batch, Q.shape[0])
+
+    def _predict_worker(self):
+        while True:
+            batch = self._take("predict", 1 << 30, 1 << 62, 1, same_model=True)
+            if batch is None:
+                return
+            km = self.models[batch[0].model]
+            Q = batch[0].queries if len(batch) == 1 else np.concatenate([r.queries for r in batch])
+            lab = km.predict(Q)
+            o = 0
+            for r in batch:
+                m = r.queries.shape[0]
+                r.result = lab[o:o + m].copy()
+                o += m
+            self._finish("predict", batch, Q.shape[0])
+
+
+def latency_summary(reqs):
+    lat = np.array([r.latency for r in reqs if r.latency is not None])
+    if lat.size == 0:
+        return {"requests": 0}
+    return {"requests": int(lat.size), "p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "p99_ms": float(np.percentile(lat, 99) * 1e3), "max_ms": float(lat.max() * 1e3)}
+
+
+def replay(server, trace, rng_queries):
+    """Submit requests at the trace's arrival offsets (seconds from now):
+    trace = [(t, kind, size, k_or_model)], queries drawn by rng_queries(size).
+    Returns the submitted requests once all are complete."""
+    reqs = []
+    t0 = time.perf_counter()
+    for t, kind, size, arg in trace:
+        while time.perf_counter() - t0 < t:
+            time.sleep(0)
+        Q = rng_queries(size)
+        r = Request(kind, Q, k=arg if kind == "knn" else None,
+                    model=arg if kind == "predict" else None)
+        reqs.append(server.submit(r))
+    for r in reqs:
+        r.wait()
+    return reqs
