@@ -109,6 +109,11 @@ int knn_tc_supported(int nx, int d, int k);
 size_t knn_tc_list_cap();                   // list entries per query
 size_t knn_tc_query_bytes(int nq, int d);   // size of qbuf
 int *knn_tc_counts(void *qbuf, int nq, int d); // per-query list lengths inside qbuf
+// dst[i] = src[idx[i]] (rows of ld floats); out[idx[i]] = (key, ind)[i] (rows of k)
+cudaError_t launch_rows_gather(const float *src, int ld, const int *idx, int m, float *dst,
+                               cudaStream_t s);
+cudaError_t launch_results_scatter(const float *key, const int *ind, const int *idx, int m, int k,
+                                   float *out_key, int *out_idx, cudaStream_t s);
 cudaError_t launch_knn_tc_train_prep(const float *X, int ld, int nx, int d, void *Xh, void *Xl,
                                      int ldbf, float *xnorm2, float *xmax, cudaStream_t s);
 cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const float *xnorm2,

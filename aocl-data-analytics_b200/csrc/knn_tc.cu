@@ -13,10 +13,10 @@
 // Every query keeps a threshold theta_q >= v'_tc(k) + 2 eps_q, shared by all
 // CTAs through global memory (atomicMin of order-preserving bits).  The
 // epilogue appends every (v'_tc, j) with v'_tc < theta_q to the query's list;
-// at every window boundary of the list, a warp lowers theta_q to (k-th
-// smallest value of a complete window) + 2 eps_q -- the window's k-th
-// smallest is never below the global one, so theta_q stays a valid bound
-// while it tightens.  theta_q starts from an exact pre-pass over the first
+// at every window boundary of the list, a warp merges a complete window into
+// the query's smallest listed values and lowers theta_q to their k-th
+// + 2 eps_q -- k distinct listed rows, so never below the global k-th:
+// theta_q stays a valid bound while it tightens.  theta_q starts from an exact pre-pass over the first
 // TK_PRE_ROWS training rows (the k-th smallest plain distance there bounds
 // the global one).  The finalize kernel re-scores the listed rows
 // with v'_tc < theta_q exactly (the plain kernel's formula and order) and
@@ -37,18 +37,21 @@ constexpr int TK_BM = 128;         // train rows per tile (UMMA M, TMEM lanes)
 constexpr int TK_BN = 256;         // queries per tile (UMMA N, TMEM columns)
 constexpr int TK_KB = 64;          // bf16 elements per 128-byte K block
 constexpr int TK_THREADS = 320;    // TMA warp, MMA warp, 8 epilogue warps
-constexpr int TK_WIN_MAX = 512;    // list entries per threshold refresh (256 when k <= 128)
 constexpr int TK_PRE_ROWS = 4096;  // training rows of the threshold pre-pass
+constexpr int TK_BEST = 256;       // smallest listed values kept per query (>= k)
+constexpr int TK_WIN = 128;        // list entries merged into them per refresh
 constexpr int TK_CHUNK_TILES = 64; // train tiles per work item
 constexpr int TK_FIN_MAX = 2048;   // candidates re-scored per query (more: fallback)
 
 struct KnnTcArgs {
-    int nx, nq, k, nkb, stages, n_qtiles, n_xtiles, n_items, cap, win;
+    int nx, nq, k, nkb, stages, n_qtiles, n_xtiles, n_items, cap;
     const float *xnorm;   // nx: fp32 |x_j|^2
     const float *margin;  // n_qtiles * TK_BN: 2 eps_q (nudged up)
     unsigned *theta;      // n_qtiles * TK_BN: threshold, order-preserving bits
     int *cnt;             // n_qtiles * TK_BN: entries appended
     int2 *list;           // nq * cap: (value bits, train row)
+    float *best;          // n_qtiles * TK_BN * TK_BEST: smallest listed values so far
+    int *lock;            // n_qtiles * TK_BN: refresh of `best` in progress
     int *err;
 };
 
@@ -324,35 +327,50 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                             if (pos < a.cap)
                                 a.list[(size_t)gq * a.cap + pos] = make_int2(__float_as_int(sv), row);
                         }
-                        // Crossing a window boundary: lower theta with the k-th
-                        // smallest value of the window before the one just
-                        // completed (its entries have been written by now; one
-                        // still in flight reads as +inf, which only loosens the
-                        // bound).
-                        const int w_end = ((base0 + nadd) / a.win) * a.win;
-                        if (w_end > base0 && w_end >= 2 * a.win && w_end <= a.cap) {
+                        // Crossing a window boundary: merge the window before the
+                        // one just completed (its entries have been written by
+                        // now; one still in flight reads as +inf) into the
+                        // query's smallest listed values, and lower theta to
+                        // their k-th + 2 eps.  They are distinct listed rows, so
+                        // their k-th is never below the global k-th.  One warp
+                        // at a time per query (a refresh that finds another in
+                        // progress is skipped: a later one catches up).
+                        const int w_end = ((base0 + nadd) / TK_WIN) * TK_WIN;
+                        if (w_end > base0 && w_end >= 2 * TK_WIN && w_end <= a.cap) {
                             __syncwarp();
-                            const int2 *lw = a.list + (size_t)gq * a.cap + (w_end - 2 * a.win);
-                            const int per = a.win >> 5; // 8 or 16 per lane
-                            float s16[16];
+                            int got = 0;
+                            if (lane == 0) got = atomicCAS(&a.lock[gq], 0, 1) == 0;
+                            got = __shfl_sync(0xffffffffu, got, 0);
+                            if (got) {
+                                __threadfence();
+                                float *bq = a.best + (size_t)gq * TK_BEST;
+                                const int2 *lw = a.list + (size_t)gq * a.cap + (w_end - 2 * TK_WIN);
+                                float s16[16];
 #pragma unroll
-                            for (int t = 0; t < 16; ++t) {
-                                // first word of the entry, past L1 (other SMs write it)
-                                s16[t] = t < per ? __int_as_float(__ldcg(&lw[lane * per + t].x))
-                                                 : __int_as_float(0x7f800000);
-                            }
-                            warp_sort512(s16);
-                            float kth = 0.f;
+                                for (int t = 0; t < 8; ++t) s16[t] = __ldcg(&bq[lane * 8 + t]);
 #pragma unroll
-                            for (int t = 0; t < 16; ++t)
-                                if (t == (a.k - 1) % 16) kth = s16[t];
-                            kth = __shfl_sync(0xffffffffu, kth, (a.k - 1) / 16);
-                            const float thn = nudge_up(kth + a.margin[gq]);
-                            if (thn < thw[col]) {
-                                if (lane == 0) {
+                                for (int t = 0; t < 4; ++t)
+                                    s16[8 + t] = __int_as_float(__ldcg(&lw[lane * 4 + t].x));
+#pragma unroll
+                                for (int t = 12; t < 16; ++t) s16[t] = __int_as_float(0x7f800000);
+                                warp_sort512(s16);
+                                if (lane < TK_BEST / 16) {
+#pragma unroll
+                                    for (int t = 0; t < 16; ++t) __stcg(&bq[lane * 16 + t], s16[t]);
+                                }
+                                float kth = 0.f;
+#pragma unroll
+                                for (int t = 0; t < 16; ++t)
+                                    if (t == (a.k - 1) % 16) kth = s16[t];
+                                kth = __shfl_sync(0xffffffffu, kth, (a.k - 1) / 16);
+                                const float thn = nudge_up(kth + a.margin[gq]);
+                                if (thn < thw[col] && lane == 0) {
                                     atomicMin(&a.theta[gq], ord_bits(thn));
                                     thw[col] = thn;
                                 }
+                                __threadfence();
+                                __syncwarp();
+                                if (lane == 0) atomicExch(&a.lock[gq], 0);
                             }
                             __syncwarp();
                         }
@@ -413,6 +431,11 @@ __global__ void knn_tc_init_theta(const float *pre_key, int k, int nq, const flo
     const float pk = pre_key[(size_t)qi * k + (k - 1)];
     const float t = nudge_up(pk - qsq[qi] + 2.f * margin[qi]);
     if (t == t) theta[qi] = ord_bits(t);
+}
+
+__global__ void knn_tc_fill_best(float *best, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) best[i] = __int_as_float(0x7f800000);
 }
 
 __global__ void knn_tc_fill_list(int2 *list, size_t n) {
@@ -549,7 +572,7 @@ int knn_tc_supported(int nx, int d, int k) {
     return tk_smem_bytes(nkb, 2) <= 225 * 1024 ? 1 : 0;
 }
 
-size_t knn_tc_list_cap() { return 8192; }
+size_t knn_tc_list_cap() { return 16384; }
 
 cudaError_t launch_knn_tc_train_prep(const float *X, int ld, int nx, int d, void *Xh, void *Xl,
                                      int ldbf, float *xnorm2, float *xmax, cudaStream_t s) {
@@ -582,6 +605,8 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     unsigned *theta = reinterpret_cast<unsigned *>(margin + nq_pad);
     int *cnt = reinterpret_cast<int *>(theta + nq_pad);
     float *qsq = reinterpret_cast<float *>(cnt + nq_pad);
+    int *lock = reinterpret_cast<int *>(qsq + nq_pad);
+    float *best = reinterpret_cast<float *>(lock + nq_pad);
     // |v'_tc - v'_plain| <= e1 |x||q| + e2 (|x|^2 + |q|^2)  (u = 2^-24):
     //   bf16 hi/lo split of x and of -2q, dropped lo.lo term: 3.1 2^-16 |x||2q|
     //   fp32 accumulation of K_total = 3 Kp products in the tensor core
@@ -618,7 +643,10 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
         }
         const size_t nl = (size_t)nq * cap;
         knn_tc_fill_list<<<(unsigned)((nl + 255) / 256), 256, 0, s>>>(static_cast<int2 *>(list), nl);
-        cudaError_t e = cudaMemsetAsync(fallback, 0, (size_t)nq * sizeof(int), s);
+        const size_t nb = (size_t)nq_pad * TK_BEST;
+        knn_tc_fill_best<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(best, nb);
+        cudaError_t e = cudaMemsetAsync(lock, 0, (size_t)nq_pad * sizeof(int), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(fallback, 0, (size_t)nq * sizeof(int), s);
         if (e == cudaSuccess) e = cudaMemsetAsync(n_fallback, 0, sizeof(int), s);
         if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), s);
         if (e != cudaSuccess) return e;
@@ -645,12 +673,13 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     a.n_xtiles = n_xtiles;
     a.n_items = n_qtiles * n_xchunks;
     a.cap = cap;
-    a.win = k <= 128 ? 256 : 512;
     a.xnorm = xnorm2;
     a.margin = margin;
     a.theta = theta;
     a.cnt = cnt;
     a.list = static_cast<int2 *>(list);
+    a.best = best;
+    a.lock = lock;
     a.err = err;
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
@@ -665,6 +694,37 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     return cudaGetLastError();
 }
 
+__global__ void rows_gather_kernel(const float *src, int ld, const int *idx, int m, float *dst) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (size_t)m * ld) return;
+    const int i = (int)(e / ld), c = (int)(e % ld);
+    dst[e] = src[(size_t)idx[i] * ld + c];
+}
+__global__ void results_scatter_kernel(const float *key, const int *ind, const int *idx, int m,
+                                       int k, float *out_key, int *out_idx) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (size_t)m * k) return;
+    const int i = (int)(e / k), r = (int)(e % k);
+    out_key[(size_t)idx[i] * k + r] = key[e];
+    out_idx[(size_t)idx[i] * k + r] = ind[e];
+}
+
+cudaError_t launch_rows_gather(const float *src, int ld, const int *idx, int m, float *dst,
+                               cudaStream_t s) {
+    const size_t n = (size_t)m * ld;
+    if (n == 0) return cudaSuccess;
+    rows_gather_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, ld, idx, m, dst);
+    return cudaGetLastError();
+}
+cudaError_t launch_results_scatter(const float *key, const int *ind, const int *idx, int m, int k,
+                                   float *out_key, int *out_idx, cudaStream_t s) {
+    const size_t n = (size_t)m * k;
+    if (n == 0) return cudaSuccess;
+    results_scatter_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(key, ind, idx, m, k,
+                                                                        out_key, out_idx);
+    return cudaGetLastError();
+}
+
 int *knn_tc_counts(void *qbuf, int nq, int d) {
     const int nkb = (d + TK_KB - 1) / TK_KB;
     const size_t nq_pad = (size_t)((nq + TK_BN - 1) / TK_BN) * TK_BN;
@@ -675,7 +735,7 @@ int *knn_tc_counts(void *qbuf, int nq, int d) {
 size_t knn_tc_query_bytes(int nq, int d) {
     const int nkb = (d + TK_KB - 1) / TK_KB;
     const size_t nq_pad = (size_t)((nq + TK_BN - 1) / TK_BN) * TK_BN;
-    return nq_pad * nkb * TK_KB * 2 * 2 + nq_pad * 16 + 256;
+    return nq_pad * nkb * TK_KB * 2 * 2 + nq_pad * 20 + nq_pad * TK_BEST * 4 + 256;
 }
 
 } // namespace b200

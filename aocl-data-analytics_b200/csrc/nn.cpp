@@ -211,7 +211,51 @@ da_status NN<T>::kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_
                                   "The tensor-core kNN kernel timed out waiting on a pipeline "
                                   "barrier (code " + std::to_string(h_state[1]) + ").");
             cuda->stats["knn_tc_fallback_queries"] += (double)h_state[0];
-            if (h_state[0] != 0) return da_status_success; // plain path for the whole call
+            if (h_state[0] != 0) {
+                // the queries the pass could not certify: the plain path on
+                // just those rows (gathered, searched, scattered back)
+                std::vector<int> flags((size_t)nb), idx;
+                B200_TRY(cudaMemcpyAsync(flags.data(), dTkFlag.p, flags.size() * sizeof(int),
+                                         cudaMemcpyDeviceToHost, st), "copy");
+                B200_TRY(cudaStreamSynchronize(st), "copy");
+                for (int i = 0; i < (int)nb; ++i)
+                    if (flags[i]) idx.push_back(i);
+                const int m = (int)idx.size();
+                const int BN = knn_tile_rows_train(false);
+                const int q_tiles = (m + 63) / 64;
+                const int max_chunks = std::max(1, (int)((n_samples + BN - 1) / BN));
+                int n_chunks = std::max(1, std::min(max_chunks, (148 * 8 + q_tiles - 1) / q_tiles));
+                int chunk_rows = (int)((n_samples + n_chunks - 1) / n_chunks);
+                chunk_rows = ((chunk_rows + BN - 1) / BN) * BN;
+                n_chunks = (int)((n_samples + chunk_rows - 1) / chunk_rows);
+                // scratch inside the (now free) candidate-list buffer
+                const size_t parts = (size_t)m * n_chunks * k;
+                const size_t need = (size_t)m * 4 + (size_t)m * ld * 4 + parts * 8 +
+                                    (size_t)m * k * 8 + 1024;
+                if (!dTkList.ensure(need))
+                    return err->error(da_status_memory_error, "Device memory allocation failed.");
+                char *p = dTkList.as<char>();
+                int *didx = reinterpret_cast<int *>(p);
+                float *qsub = reinterpret_cast<float *>(p + ((size_t)m * 4 + 255) / 256 * 256);
+                float *pk = qsub + (size_t)m * ld;
+                int *pi = reinterpret_cast<int *>(pk + parts);
+                float *ok = reinterpret_cast<float *>(pi + parts);
+                int *oi = reinterpret_cast<int *>(ok + (size_t)m * k);
+                KnnArgs pa{ACC_SQEUC, POST_NONE, kc, 2.0, (int)k, chunk_rows, n_chunks};
+                B200_TRY(cudaMemcpyAsync(didx, idx.data(), (size_t)m * 4, cudaMemcpyHostToDevice,
+                                         st), "copy");
+                B200_TRY(launch_rows_gather(dQ.as<float>() + (size_t)q0 * ld, ld, didx, m, qsub,
+                                            st), "gather");
+                B200_TRY(launch_knn_chunks<float>(qsub, ld, m, dX.as<float>(), ld,
+                                                  (int)n_samples, (int)d, nullptr, nullptr, pa, pk,
+                                                  pi, nullptr, st), "kNN distance kernel");
+                B200_TRY(launch_knn_merge<float>(pk, pi, m, n_chunks, (int)k, take_sqrt ? 1 : 0,
+                                                 ok, oi, st), "kNN merge kernel");
+                B200_TRY(launch_results_scatter(ok, oi, didx, m, (int)k,
+                                                dOutK.as<float>() + (size_t)q0 * k,
+                                                dOutI.as<int>() + (size_t)q0 * k, st), "scatter");
+                B200_TRY(cudaStreamSynchronize(st), "kNN fallback");
+            }
         }
         cuda->stats["tensor_core"] = 1.0;
         done = true;

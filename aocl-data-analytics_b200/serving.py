@@ -24,8 +24,8 @@ import time
 import numpy as np
 
 # device bytes per query of a kNN batch: the query row, its candidate list of
-# the tensor-core pass (8,192 entries of 8 bytes) and its outputs (k <= 256)
-KNN_LIST_BYTES = 8192 * 8
+# the tensor-core pass (16,384 entries of 8 bytes) and its outputs (k <= 256)
+KNN_LIST_BYTES = 16384 * 8
 KNN_OUT_BYTES = 256 * 8
 
 
@@ -68,7 +68,8 @@ class Server:
         self.pending = {"knn": collections.deque(), "predict": collections.deque()}
         self.stopping = False
         self.completed = []
-        self.batches = []          # (kind, requests, queries) of every library call
+        self.batches = []          # (kind, requests, queries, seconds) of every library call
+        self.fallback_queries = 0  # kNN queries the tensor-core pass handed to the plain path
         self.knn_handles = []
         for _ in range(workers):
             h = ab.KNN("s", order=ab.ROW_MAJOR, metric="euclidean",
@@ -138,14 +139,14 @@ class Server:
                 del q[i]
             return batch
 
-    def _finish(self, kind, batch, nq):
+    def _finish(self, kind, batch, nq, secs):
         t = time.perf_counter()
         for r in batch:
             r.t_done = t
             r._done.set()
         with self.cv:
             self.completed.extend(batch)
-            self.batches.append((kind, len(batch), nq))
+            self.batches.append((kind, len(batch), nq, secs))
 
     def _knn_worker(self, w):
         h = self.knn_handles[w]
@@ -156,13 +157,19 @@ class Server:
                 return
             Q = batch[0].queries if len(batch) == 1 else np.concatenate([r.queries for r in batch])
             kmax = max(r.k for r in batch)
+            t0 = time.perf_counter()
             ind, dist = h.kneighbors(Q, kmax)
+            secs = time.perf_counter() - t0
+            nfb = int(h.stat("knn_tc_fallback_queries"))
+            if nfb:
+                with self.cv:
+                    self.fallback_queries += nfb
             o = 0
             for r in batch:
                 m = r.queries.shape[0]
                 r.result = (ind[o:o + m, :r.k].copy(), dist[o:o + m, :r.k].copy())
                 o += m
-            self._finish("knn", batch, Q.shape[0])
+            self._finish("knn", batch, Q.shape[0], secs)
 
     def _predict_worker(self):
         while True:
@@ -171,13 +178,15 @@ class Server:
                 return
             km = self.models[batch[0].model]
             Q = batch[0].queries if len(batch) == 1 else np.concatenate([r.queries for r in batch])
+            t0 = time.perf_counter()
             lab = km.predict(Q)
+            secs = time.perf_counter() - t0
             o = 0
             for r in batch:
                 m = r.queries.shape[0]
                 r.result = lab[o:o + m].copy()
                 o += m
-            self._finish("predict", batch, Q.shape[0])
+            self._finish("predict", batch, Q.shape[0], secs)
 
 
 def latency_summary(reqs):
@@ -195,8 +204,11 @@ def replay(server, trace, rng_queries):
     reqs = []
     t0 = time.perf_counter()
     for t, kind, size, arg in trace:
-        while time.perf_counter() - t0 < t:
-            time.sleep(0)
+        # sleep (not spin) until the arrival time, leaving the interpreter
+        # lock to the workers
+        wait = t - (time.perf_counter() - t0)
+        if wait > 0:
+            time.sleep(wait)
         Q = rng_queries(size)
         r = Request(kind, Q, k=arg if kind == "knn" else None,
                     model=arg if kind == "predict" else None)

@@ -211,6 +211,10 @@ def main():
     ap.add_argument("--no-knn", action="store_true", help="skip the kNN (4.04M x 128) leg")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched k-means (512 data sets) leg")
+    ap.add_argument("--no-serve", action="store_true",
+                    help="skip the serving leg (8M x 96 index, 64 k-means models)")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="run only the serving leg and print its JSON")
     ap.add_argument("--knn-only", action="store_true",
                     help="run only the kNN leg (profiling captures) and print its JSON")
     ap.add_argument("--knn-rows", type=int, default=4_000_000)
@@ -232,6 +236,10 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     ab = _load("aoclda_b200", os.path.join(PKG, "aoclda_b200.py"))
+    if args.serve_only:
+        if rank == 0:
+            print(json.dumps(run_serving(ab)))
+        return 0
     if args.knn_only:
         if rank == 0:
             print(json.dumps(run_knn(ab, nx=args.knn_rows, nq=args.knn_queries,
@@ -375,6 +383,9 @@ def main():
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = run_batched(ab)
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        serving = run_serving(ab)
     extra = {"iterations_per_step": n_iter, "init_ms": init_ms,
              "relabelled_rows_last_iteration": relabelled,
              "full_scan_rows_last_iteration": full_scan,
@@ -394,6 +405,7 @@ def main():
         "speedup_vs_plain_fp32": (value / plain["value"]) if plain else None,
         "knn": knn,
         "kmeans_batched": batched,
+        "serving": serving,
     }
     if rank == 0:
         print(json.dumps(out))
@@ -451,6 +463,73 @@ def run_knn(ab, nx=4_000_000, nq=10_000, d=128, k=100, comps=1024, seed=3, reps=
             "tensor_tflops_algorithmic": flops / (tc["kernel_ms"].get("knn_tc", float("nan")) / 1e3) / 1e12,
             "candidate_list_mean": tc["list_mean"],
             "timing": "wall clock of one da_nn_kneighbors_s call with host arrays (best of 3)"}
+
+
+def run_serving(ab, nx=8_000_000, d=96, comps=2048, n_models=64, rates=(1000.0, 2000.0),
+                seconds=2.0, seed=5):
+    """Serving: a resident kNN index of 8,000,000 x 96 fp32 rows from a
+    2,048-component Gaussian mixture (the k-means recipe) and 64 k-means
+    models (d = 96, 256 centres, each fitted on 20,000 rows of its own
+    mixture).  A seeded trace of Poisson arrivals at 2,000 requests/s for 2 s:
+    per-request query count lognormal(ln 16, 1.5) clipped to [1, 4096],
+    k uniform in {1, 10, 100}, one request in five a predict on a random
+    model.  Served by the continuous-batching loop (two kNN workers, at most
+    512 queries per library call); p50 / p99 latency (submit to completion)
+    and queries/s at 1,000 and 2,000 requests/s for the tensor-core kNN path,
+    and at 1,000 requests/s for the plain fp32 path (which cannot keep up, so
+    its queue grows)."""
+    sv = _load("aoclda_serving", os.path.join(PKG, "serving.py"))
+    rng = np.random.default_rng(seed)
+    means = rng.uniform(-10.0, 10.0, (comps, d)).astype(np.float32)
+    sig = rng.uniform(0.5, 2.0, comps).astype(np.float32)
+    w = rng.dirichlet(np.ones(comps))
+    lab = rng.choice(comps, nx, p=w)
+    X = means[lab] + rng.standard_normal((nx, d), dtype=np.float32) * sig[lab, None]
+    models = {}
+    for m in range(n_models):
+        mm = rng.uniform(-10.0, 10.0, (256, d)).astype(np.float32)
+        lm = rng.integers(0, 256, 20_000)
+        Xm = mm[lm] + rng.standard_normal((20_000, d), dtype=np.float32)
+        models[m] = (Xm, Xm[rng.choice(20_000, 256, replace=False)].copy())
+    def make_trace(rate, trng):
+        trace, t = [], 0.0
+        while t < seconds:
+            t += trng.exponential(1.0 / rate)
+            size = int(np.clip(trng.lognormal(np.log(16), 1.5), 1, 4096))
+            if trng.random() < 0.2:
+                trace.append((t, "predict", size, int(trng.integers(0, n_models))))
+            else:
+                trace.append((t, "knn", size, int(trng.choice([1, 10, 100]))))
+        return trace
+
+    qrng = np.random.default_rng(seed + 1)
+
+    def queries(size):
+        li = qrng.choice(comps, size, p=w)
+        return means[li] + qrng.standard_normal((size, d), dtype=np.float32) * sig[li, None]
+
+    out = {"workload": f"serve_fp32_index_{nx}x{d}_{n_models}_models_poisson_{seconds:g}s"}
+    for mode, mode_rates in (("bf16x3", rates), ("plain", rates[:1])):
+        server = sv.Server(ab, X, models=models, workers=2, max_batch_queries=512,
+                           precision_mode=mode)
+        for rate in mode_rates:
+            server.batches.clear()
+            trace = make_trace(rate, np.random.default_rng(seed + int(rate)))
+            t0 = time.perf_counter()
+            reqs = sv.replay(server, trace, queries)
+            wall = time.perf_counter() - t0
+            small = [r for r in reqs if r.queries.shape[0] <= 256]
+            nq = sum(r.queries.shape[0] for r in reqs)
+            kb = [b for b in server.batches if b[0] == "knn"]
+            out[f"{mode}_{int(rate)}rps"] = {
+                "requests": len(reqs), "all": sv.latency_summary(reqs),
+                "requests_1_256_queries": sv.latency_summary(small),
+                "queries_per_s": nq / wall, "knn_calls": len(kb),
+                "mean_queries_per_knn_call": float(np.mean([b[2] for b in kb])) if kb else 0.0,
+                "mean_knn_call_ms": float(np.mean([b[3] for b in kb]) * 1e3) if kb else 0.0,
+                "plain_fallback_queries": server.fallback_queries}
+        server.close()
+    return out
 
 
 def run_batched(ab, count=512, max_iter=30, tol=1e-4, seed=4):

@@ -44,3 +44,21 @@ def test_knn_tc_equals_plain(gpu, ab, nx, nq, d, k, metric, order):
     assert ttc == 1.0 and fb == 0.0
     np.testing.assert_array_equal(td, pd)
     np.testing.assert_array_equal(ti, pi)
+
+
+def test_knn_tc_fallback_queries(gpu, ab):
+    """Queries whose candidates the tensor-core pass cannot resolve (here: 5,000
+    copies of one row at the query's own position, more exact ties than its
+    re-score holds) are searched on the plain path alone; all results still
+    equal the plain path's."""
+    rng = np.random.default_rng(11)
+    nx, nq, d, k = 200_000, 600, 64, 10
+    X = mixture(rng, nx, d, comps=64)
+    X[rng.choice(nx, 5000, replace=False)] = X[0]
+    Q = mixture(rng, nq, d, comps=64)
+    Q[[3, 77, 500]] = X[0]
+    pi, pd, _, _ = run(ab, X, Q, k, "euclidean", "plain", 0)
+    ti, td, ttc, fb = run(ab, X, Q, k, "euclidean", "bf16x3", 0)
+    assert ttc == 1.0 and fb >= 3.0
+    np.testing.assert_array_equal(td, pd)
+    np.testing.assert_array_equal(ti, pi)

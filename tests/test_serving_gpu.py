@@ -51,7 +51,7 @@ def test_serving_results_alone_and_in_the_mix(gpu, ab):
                 trace.append((t, "knn", size, int(rng.choice([1, 10, 100]))))
         reqs = sv.replay(server, trace, queries)
         assert all(r.result is not None for r in reqs)
-        assert max(nb for kind, nb, _ in server.batches if kind == "knn") > 1
+        assert max(b[1] for b in server.batches if b[0] == "knn") > 1
         summary = sv.latency_summary(reqs)
         assert summary["requests"] == len(reqs)
     finally:
