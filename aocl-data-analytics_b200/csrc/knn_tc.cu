@@ -37,11 +37,12 @@ constexpr int TK_BM = 128;         // train rows per tile (UMMA M, TMEM lanes)
 constexpr int TK_BN = 256;         // queries per tile (UMMA N, TMEM columns)
 constexpr int TK_KB = 64;          // bf16 elements per 128-byte K block
 constexpr int TK_THREADS = 320;    // TMA warp, MMA warp, 8 epilogue warps
-constexpr int TK_PRE_ROWS = 4096;  // training rows of the threshold pre-pass
+constexpr int TK_PRE_ROWS = 16384; // training rows of the threshold pre-pass (small batches;
+                                   // 4,096 from 2,048 queries up)
 constexpr int TK_BEST = 256;       // smallest listed values kept per query (>= k)
 constexpr int TK_WIN = 128;        // list entries merged into them per refresh
 constexpr int TK_CHUNK_TILES = 64; // train tiles per work item
-constexpr int TK_FIN_MAX = 2048;   // candidates re-scored per query (more: fallback)
+constexpr int TK_FIN_MAX = 8192;   // candidates re-scored per query (more: fallback)
 
 struct KnnTcArgs {
     int nx, nq, k, nkb, stages, n_qtiles, n_xtiles, n_items, cap;
@@ -338,8 +339,12 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                         const int w_end = ((base0 + nadd) / TK_WIN) * TK_WIN;
                         if (w_end > base0 && w_end >= 2 * TK_WIN && w_end <= a.cap) {
                             __syncwarp();
+                            // a short, bounded wait for the lock (its holder never
+                            // waits, so it is released within a refresh time)
                             int got = 0;
-                            if (lane == 0) got = atomicCAS(&a.lock[gq], 0, 1) == 0;
+                            if (lane == 0)
+                                for (int t = 0; t < 256 && !got; ++t)
+                                    got = atomicCAS(&a.lock[gq], 0, 1) == 0;
                             got = __shfl_sync(0xffffffffu, got, 0);
                             if (got) {
                                 __threadfence();
@@ -477,20 +482,24 @@ __global__ void __launch_bounds__(256)
 knn_tc_finalize(const float *X, const float *Q, int ld, int d, int kc, int k, int cap,
                 const unsigned *theta, const int *cnt, const int2 *list, int take_sqrt,
                 float *out_key, int *out_idx, int *fallback, int *n_fallback) {
-    __shared__ float skey[TK_FIN_MAX];
-    __shared__ int sidx[TK_FIN_MAX];
     __shared__ int scount;
-    extern __shared__ float qs[];
+    extern __shared__ __align__(16) float fin_smem[];
+    float *skey = fin_smem;                                  // TK_FIN_MAX
+    int *sidx = reinterpret_cast<int *>(skey + TK_FIN_MAX);  // TK_FIN_MAX
+    float *qs = reinterpret_cast<float *>(sidx + TK_FIN_MAX); // d
     const int qi = blockIdx.x;
     const int n = cnt[qi];
     const float th = ord_float(theta[qi]);
     if (threadIdx.x == 0) scount = 0;
     for (int f = threadIdx.x; f < d; f += blockDim.x) qs[f] = Q[(size_t)qi * ld + f];
     __syncthreads();
+    // fallback reasons counted at n_fallback[2..4]: list overflow, more
+    // survivors than the re-score holds, fewer survivors than k
     if (n > cap) {
         if (threadIdx.x == 0) {
             fallback[qi] = 1;
             atomicAdd(n_fallback, 1);
+            atomicAdd(n_fallback + 2, 1);
         }
         return;
     }
@@ -507,6 +516,7 @@ knn_tc_finalize(const float *X, const float *Q, int ld, int d, int kc, int k, in
         if (threadIdx.x == 0) {
             fallback[qi] = 1;
             atomicAdd(n_fallback, 1);
+            atomicAdd(n_fallback + (m > TK_FIN_MAX ? 3 : 4), 1);
         }
         return;
     }
@@ -625,10 +635,12 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
         // exact pre-pass over the first training rows (plain kernels; its
         // partial lists live in the candidate list buffer, its merged keys in
         // the output arrays, both overwritten below)
-        const int pre = std::min(nx, TK_PRE_ROWS);
+        // exact pre-pass rows: its cost grows with the batch, while large
+        // batches tighten their thresholds quickly on their own
+        const int pre = std::min(nx, nq >= 2048 ? 4096 : TK_PRE_ROWS);
         if (pre >= k) {
             const int BN = knn_tile_rows_train(false);
-            int n_chunks = std::max(1, std::min((pre + BN - 1) / BN, 8));
+            int n_chunks = std::max(1, std::min((pre + BN - 1) / BN, 16));
             int chunk_rows = ((pre + n_chunks - 1) / n_chunks + BN - 1) / BN * BN;
             n_chunks = (pre + chunk_rows - 1) / chunk_rows;
             KnnArgs pa{ACC_SQEUC, POST_NONE, kc, 2.0, k, chunk_rows, n_chunks};
@@ -648,6 +660,7 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
         cudaError_t e = cudaMemsetAsync(lock, 0, (size_t)nq_pad * sizeof(int), s);
         if (e == cudaSuccess) e = cudaMemsetAsync(fallback, 0, (size_t)nq * sizeof(int), s);
         if (e == cudaSuccess) e = cudaMemsetAsync(n_fallback, 0, sizeof(int), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(n_fallback + 2, 0, 3 * sizeof(int), s);
         if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), s);
         if (e != cudaSuccess) return e;
     }
@@ -688,7 +701,10 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     knn_tc_kernel<<<grid, TK_THREADS, smem, s>>>(mah, mal, mbh, mbl, a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    knn_tc_finalize<<<nq, 256, (size_t)d * sizeof(float), s>>>(
+    const size_t fsm = (size_t)TK_FIN_MAX * 8 + (size_t)d * sizeof(float);
+    e = cudaFuncSetAttribute(knn_tc_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm);
+    if (e != cudaSuccess) return e;
+    knn_tc_finalize<<<nq, 256, fsm, s>>>(
         X, Q, ld, d, kc, k, cap, theta, cnt, static_cast<const int2 *>(list), take_sqrt, out_key,
         out_idx, fallback, n_fallback);
     return cudaGetLastError();

@@ -181,7 +181,7 @@ da_status NN<T>::kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_
             return err->error(da_status_memory_error, "Device memory allocation failed.");
         int *n_fb = reinterpret_cast<int *>(dTkScal.as<char>() + 16);
         int *errf = n_fb + 1;
-        int h_state[2] = {0, 0};
+        int h_state[5] = {0, 0, 0, 0, 0};
         for (da_int q0 = 0; q0 < nq; q0 += QB) {
             const da_int nb = std::min(QB, nq - q0);
             B200_TRY(cuda->timed("knn_tc", [&] {
@@ -192,7 +192,7 @@ da_status NN<T>::kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_
                                      n_fb, errf, dOutK.as<float>() + (size_t)q0 * k,
                                      dOutI.as<int>() + (size_t)q0 * k, st);
             }), "kNN tensor-core pass");
-            B200_TRY(cudaMemcpyAsync(h_state, n_fb, 2 * sizeof(int), cudaMemcpyDeviceToHost, st),
+            B200_TRY(cudaMemcpyAsync(h_state, n_fb, 5 * sizeof(int), cudaMemcpyDeviceToHost, st),
                      "copy");
             std::vector<int> lens((size_t)nb);
             B200_TRY(cudaMemcpyAsync(lens.data(), knn_tc_counts(dTkQ.p, (int)nb, (int)d),
@@ -211,6 +211,9 @@ da_status NN<T>::kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_
                                   "The tensor-core kNN kernel timed out waiting on a pipeline "
                                   "barrier (code " + std::to_string(h_state[1]) + ").");
             cuda->stats["knn_tc_fallback_queries"] += (double)h_state[0];
+            cuda->stats["knn_tc_fallback_list_overflow"] += (double)h_state[2];
+            cuda->stats["knn_tc_fallback_many_survivors"] += (double)h_state[3];
+            cuda->stats["knn_tc_fallback_few_survivors"] += (double)h_state[4];
             if (h_state[0] != 0) {
                 // the queries the pass could not certify: the plain path on
                 // just those rows (gathered, searched, scattered back)
@@ -224,7 +227,10 @@ da_status NN<T>::kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_
                 const int BN = knn_tile_rows_train(false);
                 const int q_tiles = (m + 63) / 64;
                 const int max_chunks = std::max(1, (int)((n_samples + BN - 1) / BN));
-                int n_chunks = std::max(1, std::min(max_chunks, (148 * 8 + q_tiles - 1) / q_tiles));
+                // enough CTAs to fill the GPU, but at most ~16K partial entries per query
+                // (the merge ranks every entry against every chunk list)
+                int n_chunks = std::max(1, std::min({max_chunks, (148 * 8 + q_tiles - 1) / q_tiles,
+                                                     std::max(8, 16384 / (int)k)}));
                 int chunk_rows = (int)((n_samples + n_chunks - 1) / n_chunks);
                 chunk_rows = ((chunk_rows + BN - 1) / BN) * BN;
                 n_chunks = (int)((n_samples + chunk_rows - 1) / chunk_rows);
@@ -347,12 +353,15 @@ da_status NN<T>::kneighbors_compute(da_int nq, da_int d, const T *Xt, da_int ldt
     B200_TRY(upload_matrix<T>(ord, nq, d, Xt, ldt, dQ.as<T>(), ld, dStage, st), "upload of X_test");
     cuda->stats["tensor_core"] = 0.0;
     cuda->stats["knn_tc_fallback_queries"] = 0.0;
+    cuda->stats["knn_tc_fallback_list_overflow"] = 0.0;
+    cuda->stats["knn_tc_fallback_many_survivors"] = 0.0;
+    cuda->stats["knn_tc_fallback_few_survivors"] = 0.0;
     bool tc_done = false;
     const bool tc_metric =
         metric == M_EUC || metric == M_SQEUC || (metric == M_MINK && p == T(2));
     if (!fp64 && tc_metric && opts.key("precision mode") != 0 &&
         knn_tc_supported((int)n_samples, (int)d, (int)k) && n_samples >= 65536 &&
-        (double)n_samples * (double)nq * (double)d >= 4.0e9) {
+        (double)n_samples * (double)std::max<da_int>(nq, 256) * (double)d >= 4.0e9) {
         s = kneighbors_tc(nq, d, k, kc, metric != M_SQEUC, tc_done);
         if (s != da_status_success) return s;
     }
@@ -382,7 +391,10 @@ da_status NN<T>::kneighbors_compute(da_int nq, da_int d, const T *Xt, da_int ldt
         const int BN = knn_tile_rows_train(fp64);
         const int q_tiles = (int)((nq + 63) / 64);
         const int max_chunks = std::max(1, (int)((n_samples + BN - 1) / BN));
-        int n_chunks = std::max(1, std::min(max_chunks, (148 * 8 + q_tiles - 1) / q_tiles));
+        // enough CTAs to fill the GPU, but at most ~16K partial entries per query
+        // (the merge ranks every entry against every chunk list)
+        int n_chunks = std::max(1, std::min({max_chunks, (148 * 8 + q_tiles - 1) / q_tiles,
+                                             std::max(8, 16384 / (int)k)}));
         int chunk_rows = (int)((n_samples + n_chunks - 1) / n_chunks);
         chunk_rows = ((chunk_rows + BN - 1) / BN) * BN;
         n_chunks = (int)((n_samples + chunk_rows - 1) / chunk_rows);

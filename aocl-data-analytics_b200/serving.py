@@ -58,7 +58,7 @@ class Server:
     kNN worker threads (one handle each) and one predict worker."""
 
     def __init__(self, ab, X, models=None, workers=2, max_batch_queries=1024,
-                 hbm_budget=16 << 30, precision_mode="bf16x3"):
+                 max_request_queries=4096, hbm_budget=16 << 30, precision_mode="bf16x3"):
         self.ab = ab
         self.X = np.ascontiguousarray(X, dtype=np.float32)
         self.d = self.X.shape[1]
@@ -75,8 +75,11 @@ class Server:
             h = ab.KNN("s", order=ab.ROW_MAJOR, metric="euclidean",
                        precision_mode=precision_mode)
             h.fit(self.X)
-            # one call so that the device-side copies exist before the first request
-            h.kneighbors(self.X[:1], 1)
+            # one call of the largest batch: the device copies and every
+            # per-call buffer reach their final size now, so that no request
+            # waits for a device allocation (which also stalls other work)
+            warm = max(max_batch_queries, max_request_queries)
+            h.kneighbors(self.X[np.arange(warm) % self.X.shape[0]], 256)
             self.knn_handles.append(h)
         self.models = {}
         for name, (Xm, C0) in (models or {}).items():

@@ -465,7 +465,7 @@ def run_knn(ab, nx=4_000_000, nq=10_000, d=128, k=100, comps=1024, seed=3, reps=
             "timing": "wall clock of one da_nn_kneighbors_s call with host arrays (best of 3)"}
 
 
-def run_serving(ab, nx=8_000_000, d=96, comps=2048, n_models=64, rates=(1000.0, 2000.0),
+def run_serving(ab, nx=8_000_000, d=96, comps=2048, n_models=64, rates=(250.0, 1000.0, 2000.0),
                 seconds=2.0, seed=5):
     """Serving: a resident kNN index of 8,000,000 x 96 fp32 rows from a
     2,048-component Gaussian mixture (the k-means recipe) and 64 k-means
@@ -475,8 +475,8 @@ def run_serving(ab, nx=8_000_000, d=96, comps=2048, n_models=64, rates=(1000.0, 
     k uniform in {1, 10, 100}, one request in five a predict on a random
     model.  Served by the continuous-batching loop (two kNN workers, at most
     512 queries per library call); p50 / p99 latency (submit to completion)
-    and queries/s at 1,000 and 2,000 requests/s for the tensor-core kNN path,
-    and at 1,000 requests/s for the plain fp32 path (which cannot keep up, so
+    and queries/s at 250, 1,000 and 2,000 requests/s for the tensor-core path,
+    and at 250 requests/s for the plain fp32 path (which cannot keep up, so
     its queue grows)."""
     sv = _load("aoclda_serving", os.path.join(PKG, "serving.py"))
     rng = np.random.default_rng(seed)

@@ -47,14 +47,14 @@ def test_knn_tc_equals_plain(gpu, ab, nx, nq, d, k, metric, order):
 
 
 def test_knn_tc_fallback_queries(gpu, ab):
-    """Queries whose candidates the tensor-core pass cannot resolve (here: 5,000
+    """Queries whose candidates the tensor-core pass cannot resolve (here: 10,000
     copies of one row at the query's own position, more exact ties than its
     re-score holds) are searched on the plain path alone; all results still
     equal the plain path's."""
     rng = np.random.default_rng(11)
     nx, nq, d, k = 200_000, 600, 64, 10
     X = mixture(rng, nx, d, comps=64)
-    X[rng.choice(nx, 5000, replace=False)] = X[0]
+    X[rng.choice(nx, 10000, replace=False)] = X[0]
     Q = mixture(rng, nq, d, comps=64)
     Q[[3, 77, 500]] = X[0]
     pi, pd, _, _ = run(ab, X, Q, k, "euclidean", "plain", 0)
