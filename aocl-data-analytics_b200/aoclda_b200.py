@@ -99,6 +99,12 @@ def load(path=LIB_PATH):
         "da_b200_get_stat": (_P, C.c_char_p, C.POINTER(C.c_double)),
         "da_b200_kmeans_init_centres_d": (_P, _P, da_int),
         "da_b200_kmeans_init_centres_s": (_P, _P, da_int),
+        "da_b200_kmeans_shard_colmax_s": (_P, _P),
+        "da_b200_kmeans_shard_begin_s": (_P, _P, da_int, _P),
+        "da_b200_kmeans_shard_partial_s": (_P, _P),
+        "da_b200_kmeans_shard_finalize_s": (_P, _P, _P, _P),
+        "da_b200_kmeans_shard_inertia_s": (_P, da_int, C.POINTER(C.c_double)),
+        "da_b200_kmeans_shard_result_s": (_P, _P, _P),
     })
     for name, args in sig.items():
         f = getattr(lib, name)

@@ -166,6 +166,18 @@ template <typename T> struct KMeans : public AlgBase {
     da_status split_empty(T *dC, int *dL, bool &split);
     da_status prepare_tc();
     da_status prepare_fx();
+    // Lloyd steps of a shard of a data set split across processes: the
+    // current centres are dC0 / dC1 by shard_c, the current labels dL0 / dL1
+    // by shard_l
+    int shard_c = 0, shard_l = 0;
+    bool shard_ready = false;
+    da_status shard_colmax(float *colmax);
+    da_status shard_begin(const float *colmax_global, da_int n_global, const float *C);
+    da_status shard_partial(long long *acc);
+    da_status shard_finalize(const long long *acc, double *scalars, da_int *flags);
+    da_status shard_relabel(double *inertia, bool assign_first);
+    da_status shard_result(float *centres, da_int *labels);
+    da_status shard_tc_check();
     da_status assign(const T *dC, int *dL, const int *dLprev);
 };
 

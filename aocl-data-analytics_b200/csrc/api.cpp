@@ -540,6 +540,26 @@ da_status da_b200_reset_kernel_time(da_handle h) {
     h->cuda.ktime.clear();
     return da_status_success;
 }
+da_status da_b200_kmeans_shard_colmax_s(da_handle h, float *colmax) {
+    KM_CALL(float, h, shard_colmax(colmax));
+}
+da_status da_b200_kmeans_shard_begin_s(da_handle h, const float *colmax_global,
+                                       da_int n_global, const float *centres) {
+    KM_CALL(float, h, shard_begin(colmax_global, n_global, centres));
+}
+da_status da_b200_kmeans_shard_partial_s(da_handle h, long long *acc) {
+    KM_CALL(float, h, shard_partial(acc));
+}
+da_status da_b200_kmeans_shard_finalize_s(da_handle h, const long long *acc, double *scalars,
+                                          da_int *flags) {
+    KM_CALL(float, h, shard_finalize(acc, scalars, flags));
+}
+da_status da_b200_kmeans_shard_inertia_s(da_handle h, da_int relabel, double *inertia) {
+    KM_CALL(float, h, shard_relabel(inertia, relabel != 0));
+}
+da_status da_b200_kmeans_shard_result_s(da_handle h, float *centres, da_int *labels) {
+    KM_CALL(float, h, shard_result(centres, labels));
+}
 da_status da_b200_kmeans_init_centres_d(da_handle h, double *C, da_int ldc) {
     KM_CALL(double, h, initial_centres(C, ldc));
 }

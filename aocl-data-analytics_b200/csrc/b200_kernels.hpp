@@ -179,6 +179,22 @@ cudaError_t launch_kmeans_update_fx(const float *X, int ld, int n, int d, int k,
                                     const float *C_prev, float *C_new, int *counts,
                                     double *block_partials, double *scalars, int *flags,
                                     unsigned *ticket, cudaStream_t s);
+// One shard's share of a data set split across processes, packed for one
+// integer all-reduce: acc[0, k*d) the fixed-point sums (two's complement,
+// from zero), acc[k*d, k*d+k) the counts, acc[k*d+k] = (*changed != 0).
+// counts is int scratch of k entries.
+cudaError_t launch_kmeans_sums_fx(const float *X, int ld, int n, int d, int k, const int *labels,
+                                  const float *scale, long long *acc, int *counts,
+                                  const int *changed, cudaStream_t s);
+// New centres from the all-reduced acc (layout above): the single-device
+// finalize with int64 counts; flags[1] += empty clusters.
+cudaError_t launch_kmeans_finalize_shards(int k, int d, int ld, const long long *acc,
+                                          const double *inv_scale, const float *C_prev,
+                                          float *C_new, double *block_partials, double *scalars,
+                                          int *flags, unsigned *ticket, cudaStream_t s);
+// Raises (never lowers) func's dynamic shared-memory limit on the current
+// device, once per size (thread-safe).
+cudaError_t ensure_smem_limit(const void *func, size_t smem);
 // Squared row norms of the centres (sequential fma chain over features).
 template <typename T>
 cudaError_t launch_centre_norms(const T *C, int ldc, int k, int d, T *out, cudaStream_t s);

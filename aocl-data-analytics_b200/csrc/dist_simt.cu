@@ -18,6 +18,29 @@
 #include "b200_common.cuh"
 #include "b200_kernels.hpp"
 #include "simt_engine.cuh"
+#include <map>
+#include <mutex>
+
+namespace b200 {
+// Raises (never lowers) a kernel's dynamic shared-memory limit on the current
+// device.  The limit belongs to the function and device for the whole
+// process, so callers on several threads that need different sizes must not
+// lower it under one another; a larger limit does not change a launch that
+// asks for less.
+cudaError_t ensure_smem_limit(const void *func, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> g(mu);
+    size_t &have = done[{func, dev}];
+    if (have >= smem) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) have = smem;
+    return e;
+}
+} // namespace b200
 
 namespace b200 {
 
@@ -286,8 +309,7 @@ static cudaError_t launch_knn_chunks_t(const T *Q, int nq, const T *X, int nx, i
     constexpr int BM = 16 * C::TM, BN = 16 * C::TN, BK = C::BK;
     const size_t smem = 2 * sizeof(Stage<T, BM, BN, BK>) + sizeof(TopkSmem<T, BM, KCAP, BN>);
     auto kern = knn_chunk_kernel<T, ACC, KCAP>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(kern), smem);
     if (e != cudaSuccess) return e;
     dim3 grid((nq + BM - 1) / BM, a.n_chunks);
     const T p = T(a.p);

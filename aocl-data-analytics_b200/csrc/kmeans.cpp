@@ -999,6 +999,260 @@ template <typename T> da_status KMeans<T>::get_result_int(da_result q, da_int *d
     return err->warn(da_status_unknown_query, "The requested result could not be found.");
 }
 
+// ------------------------------------------------- sharded Lloyd steps ----
+// A data set split over processes, one shard per handle (one GPU each).  The
+// caller runs the Lloyd loop of run_lloyd: per iteration shard_partial
+// (assignment + the shard's fixed-point centroid sums, counts and
+// label-change flag, packed into one int64 device buffer), ONE integer
+// all-reduce of that buffer over the processes (exact in any order), then
+// shard_finalize (the new centres from the global sums, identical on every
+// process, and the shift / norm scalars of the convergence test).  With the
+// global column maxima and row count every shard quantises with the scales
+// the whole data set would use on one device, so the reduced sums, the
+// centres and the convergence decisions equal the single-handle ones bit for
+// bit.
+template <typename T> da_status KMeans<T>::shard_colmax(float *colmax) {
+    if constexpr (!std::is_same_v<T, float>) {
+        (void)colmax;
+        return err->error(da_status_not_implemented, "Sharded k-means steps are fp32 only.");
+    } else {
+        if (!initdone)
+            return err->error(da_status_no_data, "No data has been passed to the handle.");
+        if (!colmax) return err->error(da_status_invalid_pointer, "colmax is null.");
+        da_status s = ensure_device_data();
+        if (s != da_status_success) return s;
+        const int d = n_features;
+        if (!dFxScale.ensure((size_t)2 * d * sizeof(double) + (size_t)d * 4 + 16))
+            return err->error(da_status_memory_error, "Device memory allocation failed.");
+        unsigned *cm = reinterpret_cast<unsigned *>(dFxScale.as<double>() + 2 * d);
+        int *nonfinite = reinterpret_cast<int *>(cm + d);
+        cudaStream_t st = cuda->stream;
+        B200_TRY(launch_col_absmax(dX.as<float>(), ld, n_samples, d, cm, nonfinite, st), "maxima");
+        std::vector<unsigned> h(d + 1);
+        B200_TRY(cudaMemcpyAsync(h.data(), cm, (d + 1) * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                 st), "copy");
+        B200_TRY(cudaStreamSynchronize(st), "maxima");
+        if (h[d])
+            return err->error(da_status_invalid_input, "The data hold inf or NaN values.");
+        std::memcpy(colmax, h.data(), d * sizeof(float));
+        fx_stale = true; // the scale buffer now holds other values
+        return da_status_success;
+    }
+}
+
+template <typename T>
+da_status KMeans<T>::shard_begin(const float *colmax_global, da_int n_global, const float *C) {
+    if constexpr (!std::is_same_v<T, float>) {
+        (void)colmax_global, (void)n_global, (void)C;
+        return err->error(da_status_not_implemented, "Sharded k-means steps are fp32 only.");
+    } else {
+        shard_ready = false;
+        if (!initdone)
+            return err->error(da_status_no_data, "No data has been passed to the handle.");
+        if (!colmax_global || !C)
+            return err->error(da_status_invalid_pointer, "A required array is null.");
+        if (n_global < n_samples)
+            return err->error(da_status_invalid_input, "n_global is below the shard's rows.");
+        da_status s = read_options();
+        if (s != da_status_success && err->severity == DA_ERROR) return s;
+        err->clear();
+        const int k = n_clusters, d = n_features;
+        if (!fx_update_supported(k, d))
+            return err->error(da_status_not_implemented,
+                              "n_clusters * n_features is too large for the sharded update.");
+        for (int f = 0; f < d; ++f)
+            if (!(colmax_global[f] >= 0.f) || std::isinf(colmax_global[f]))
+                return err->error(da_status_invalid_input,
+                                  "The column maxima must be finite and non-negative.");
+        s = ensure_device_data();
+        if (s != da_status_success) return s;
+        s = alloc_work();
+        if (s != da_status_success) return s;
+        s = prepare_tc();
+        if (s != da_status_success) return s;
+        if (!dFxScale.ensure((size_t)2 * d * sizeof(double) + (size_t)d * 4 + 16) ||
+            !dFxAcc.ensure((size_t)k * 4) || !dFxTicket.ensure(16))
+            return err->error(da_status_memory_error, "Device memory allocation failed.");
+        cudaStream_t st = cuda->stream;
+        // the scales of prepare_fx, from the whole data set's maxima and rows
+        int L = 0;
+        while ((1LL << L) < (long long)n_global) ++L;
+        std::vector<float> scf(d);
+        std::vector<double> inv(d);
+        for (int f = 0; f < d; ++f) {
+            int E = 0;
+            if (colmax_global[f] > 0.f) std::frexp((double)colmax_global[f], &E);
+            int sf = std::min(62 - L, 44) - E;
+            sf = std::max(-126, std::min(127, sf));
+            scf[f] = std::ldexp(1.0f, sf);
+            inv[f] = std::ldexp(1.0, -sf);
+        }
+        double *scale = dFxScale.as<double>();
+        B200_TRY(cudaMemcpyAsync(scale, scf.data(), d * sizeof(float), cudaMemcpyHostToDevice, st),
+                 "copy");
+        B200_TRY(cudaMemcpyAsync(scale + d, inv.data(), d * sizeof(double),
+                                 cudaMemcpyHostToDevice, st), "copy");
+        B200_TRY(cudaMemsetAsync(dFxTicket.p, 0, 16, st), "memset");
+        std::vector<float> Cp((size_t)k * ld, 0.f);
+        for (int j = 0; j < k; ++j)
+            std::memcpy(&Cp[(size_t)j * ld], C + (size_t)j * d, d * sizeof(float));
+        B200_TRY(cudaMemcpyAsync(dC0.p, Cp.data(), Cp.size() * sizeof(float),
+                                 cudaMemcpyHostToDevice, st), "copy");
+        B200_TRY(cudaStreamSynchronize(st), "sharded start");
+        fx_stale = true; // the scales are the whole data set's, not this shard's
+        shard_c = 0;
+        shard_l = 0;
+        shard_ready = true;
+        return da_status_success;
+    }
+}
+
+// Assignment of the shard's rows to the current centres (labels into the
+// other label buffer, flag = any label changed) and the packed sums.
+template <typename T> da_status KMeans<T>::shard_partial(long long *acc) {
+    if constexpr (!std::is_same_v<T, float>) {
+        (void)acc;
+        return err->error(da_status_not_implemented, "Sharded k-means steps are fp32 only.");
+    } else {
+        if (!shard_ready)
+            return err->error(da_status_no_data, "da_b200_kmeans_shard_begin_s has not run.");
+        if (!acc) return err->error(da_status_invalid_pointer, "acc is null.");
+        const int k = n_clusters, d = n_features;
+        cudaStream_t st = cuda->stream;
+        float *Ccur = (shard_c ? dC1 : dC0).template as<float>();
+        shard_l ^= 1;
+        int *Lcur = (shard_l ? dL1 : dL0).template as<int>();
+        int *Lprev = (shard_l ? dL0 : dL1).template as<int>();
+        B200_TRY(launch_centre_norms<float>(Ccur, ld, k, d, dCn.as<float>(), st), "centre norms");
+        B200_TRY(cudaMemsetAsync(dFlags.p, 0, 8 * sizeof(int), st), "memset");
+        da_status s = assign(Ccur, Lcur, Lprev);
+        if (s != da_status_success) return s;
+        B200_TRY(cuda->timed("kmeans_update", [&] {
+            return launch_kmeans_sums_fx(dX.as<float>(), ld, n_samples, d, k, Lcur,
+                                         reinterpret_cast<const float *>(dFxScale.as<double>()),
+                                         acc, dFxAcc.as<int>(), dFlags.as<int>(), st);
+        }), "sums");
+        return da_status_success;
+    }
+}
+
+template <typename T> da_status KMeans<T>::shard_tc_check() {
+    if (!use_tc) return da_status_success;
+    int tc_state[3] = {0, 0, 0};
+    B200_TRY(cudaMemcpyAsync(tc_state, dTcScal.as<char>() + 16, 3 * sizeof(int),
+                             cudaMemcpyDeviceToHost, cuda->stream), "copy");
+    B200_TRY(cudaStreamSynchronize(cuda->stream), "copy");
+    cuda->stats["relabelled_rows"] = (double)tc_state[0];
+    cuda->stats["full_scan_rows"] = (double)tc_state[2];
+    if (tc_state[1] != 0)
+        return err->error(da_status_internal_error,
+                          "The tensor-core assignment kernel timed out waiting on a pipeline "
+                          "barrier (code " + std::to_string(tc_state[1]) + ").");
+    return da_status_success;
+}
+
+template <typename T>
+da_status KMeans<T>::shard_finalize(const long long *acc, double *scalars, da_int *flags) {
+    if constexpr (!std::is_same_v<T, float>) {
+        (void)acc, (void)scalars, (void)flags;
+        return err->error(da_status_not_implemented, "Sharded k-means steps are fp32 only.");
+    } else {
+        if (!shard_ready)
+            return err->error(da_status_no_data, "da_b200_kmeans_shard_begin_s has not run.");
+        if (!acc || !scalars || !flags)
+            return err->error(da_status_invalid_pointer, "A required array is null.");
+        const int k = n_clusters, d = n_features;
+        cudaStream_t st = cuda->stream;
+        float *Ccur = (shard_c ? dC1 : dC0).template as<float>();
+        float *Cnew = (shard_c ? dC0 : dC1).template as<float>();
+        const double *scale = dFxScale.as<double>();
+        B200_TRY(cudaMemsetAsync(dFlags.as<int>() + 1, 0, sizeof(int), st), "memset");
+        B200_TRY(launch_kmeans_finalize_shards(k, d, ld, acc, scale + d, Ccur, Cnew,
+                                               dScalars.as<double>() + 8, dScalars.as<double>(),
+                                               dFlags.as<int>(), dFxTicket.as<unsigned>(), st),
+                 "centres");
+        double *h_scal = static_cast<double *>(h_small);
+        long long *h_chg = reinterpret_cast<long long *>(static_cast<char *>(h_small) + 64);
+        int *h_empty = reinterpret_cast<int *>(static_cast<char *>(h_small) + 72);
+        B200_TRY(cudaMemcpyAsync(h_scal, dScalars.p, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                 st), "copy");
+        B200_TRY(cudaMemcpyAsync(h_chg, acc + (size_t)k * d + k, sizeof(long long),
+                                 cudaMemcpyDeviceToHost, st), "copy");
+        B200_TRY(cudaMemcpyAsync(h_empty, dFlags.as<int>() + 1, sizeof(int),
+                                 cudaMemcpyDeviceToHost, st), "copy");
+        B200_TRY(cudaStreamSynchronize(st), "Lloyd iteration");
+        shard_c ^= 1;
+        scalars[0] = h_scal[0];
+        scalars[1] = h_scal[1];
+        flags[0] = *h_chg != 0;
+        flags[1] = *h_empty;
+        return shard_tc_check();
+    }
+}
+
+template <typename T> da_status KMeans<T>::shard_relabel(double *inertia, bool assign_first) {
+    if constexpr (!std::is_same_v<T, float>) {
+        (void)inertia, (void)assign_first;
+        return err->error(da_status_not_implemented, "Sharded k-means steps are fp32 only.");
+    } else {
+        if (!shard_ready)
+            return err->error(da_status_no_data, "da_b200_kmeans_shard_begin_s has not run.");
+        if (!inertia) return err->error(da_status_invalid_pointer, "inertia is null.");
+        const int k = n_clusters, d = n_features;
+        cudaStream_t st = cuda->stream;
+        float *Ccur = (shard_c ? dC1 : dC0).template as<float>();
+        if (assign_first) {
+            shard_l ^= 1;
+            B200_TRY(launch_centre_norms<float>(Ccur, ld, k, d, dCn.as<float>(), st),
+                     "centre norms");
+            B200_TRY(cudaMemsetAsync(dFlags.p, 0, 8 * sizeof(int), st), "memset");
+            da_status s = assign(Ccur, (shard_l ? dL1 : dL0).template as<int>(), nullptr);
+            if (s != da_status_success) return s;
+        }
+        int *Lcur = (shard_l ? dL1 : dL0).template as<int>();
+        B200_TRY(launch_kmeans_inertia<float>(dX.as<float>(), ld, n_samples, d, Ccur, ld, Lcur,
+                                              dPartials.as<double>(), dScalars.as<double>() + 2,
+                                              st), "inertia");
+        double *h = static_cast<double *>(h_small) + 2;
+        B200_TRY(cudaMemcpyAsync(h, dScalars.as<double>() + 2, sizeof(double),
+                                 cudaMemcpyDeviceToHost, st), "copy");
+        B200_TRY(cudaStreamSynchronize(st), "inertia");
+        *inertia = *h;
+        return assign_first ? shard_tc_check() : da_status_success;
+    }
+}
+
+template <typename T> da_status KMeans<T>::shard_result(float *centres, da_int *labels) {
+    if constexpr (!std::is_same_v<T, float>) {
+        (void)centres, (void)labels;
+        return err->error(da_status_not_implemented, "Sharded k-means steps are fp32 only.");
+    } else {
+        if (!shard_ready)
+            return err->error(da_status_no_data, "da_b200_kmeans_shard_begin_s has not run.");
+        const int k = n_clusters, d = n_features;
+        cudaStream_t st = cuda->stream;
+        std::vector<float> Cp;
+        std::vector<int> h;
+        if (centres) {
+            Cp.resize((size_t)k * ld);
+            B200_TRY(cudaMemcpyAsync(Cp.data(), (shard_c ? dC1 : dC0).p, Cp.size() * sizeof(float),
+                                     cudaMemcpyDeviceToHost, st), "copy");
+        }
+        if (labels) {
+            h.resize(n_samples);
+            B200_TRY(cudaMemcpyAsync(h.data(), (shard_l ? dL1 : dL0).p, h.size() * sizeof(int),
+                                     cudaMemcpyDeviceToHost, st), "copy");
+        }
+        B200_TRY(cudaStreamSynchronize(st), "copy");
+        if (centres)
+            for (int j = 0; j < k; ++j)
+                std::memcpy(centres + (size_t)j * d, &Cp[(size_t)j * ld], d * sizeof(float));
+        if (labels)
+            for (da_int i = 0; i < n_samples; ++i) labels[i] = (da_int)h[i];
+        return da_status_success;
+    }
+}
+
 template struct KMeans<float>;
 template struct KMeans<double>;
 

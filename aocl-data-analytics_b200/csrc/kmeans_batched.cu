@@ -516,7 +516,7 @@ extern "C" da_status da_b200_kmeans_batched_s(da_int n_inst, const da_int *n_sam
     for (const KbInst &I : hi) max_k = std::max(max_k, I.k);
     const size_t usmem = max_smem_kd * 8 + (size_t)KB_BATCH * 4 + (size_t)2 * (max_k + 1) * 4 +
                          (size_t)max_d * 4 + 16;
-    ok(cudaFuncSetAttribute(kb_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)usmem));
+    ok(ensure_smem_limit(reinterpret_cast<const void *>(kb_update), usmem));
     // The whole fit as one CUDA graph: max_iter iterations of four launches
     // (finished instances skip their work), the final relabelling and the
     // inertia; replayed once.

@@ -653,9 +653,12 @@ fx_update_kernel(const float *X, int ld, int n, int d, int k, const int *labels,
 // block partials of |C_prev|^2 and |C_prev - C_new|^2; the last block to
 // finish sums the block partials in block order (deterministic) into
 // scalars[0..1] and re-arms the ticket.  The other accumulator pair
-// (nsum / ncnt, used by the next update) is cleared here.
+// (nsum / ncnt, used by the next update) is cleared here when given.
+// Counts are int (one device's accumulators) or int64 (the sum over the
+// shards of a data set split across processes).
+template <typename CT>
 __global__ void __launch_bounds__(256)
-fx_finalize_kernel(int k, int d, int ld, const unsigned long long *gsum, const int *gcnt,
+fx_finalize_kernel(int k, int d, int ld, const unsigned long long *gsum, const CT *gcnt,
                    unsigned long long *nsum, int *ncnt, const double *inv_scale,
                    const float *C_prev, float *C_new, int *counts, double *block_partials,
                    double *scalars, int *flags, unsigned *ticket) {
@@ -667,9 +670,9 @@ fx_finalize_kernel(int k, int d, int ld, const unsigned long long *gsum, const i
     if (e < kd) {
         const int j = e / d, f = e - j * d;
         const long long S = (long long)gsum[e];
-        const int c = gcnt[j];
-        nsum[e] = 0ull;
-        if (f == 0) ncnt[j] = 0;
+        const long long c = (long long)gcnt[j];
+        if (nsum) nsum[e] = 0ull;
+        if (ncnt && f == 0) ncnt[j] = 0;
         const double mean = ((double)S * inv_scale[f]) / (double)(c > 0 ? c : 1);
         const float cn = (float)mean;
         const size_t o = (size_t)j * ld + f;
@@ -679,7 +682,7 @@ fx_finalize_kernel(int k, int d, int ld, const unsigned long long *gsum, const i
         const double df = (double)cp - (double)cn;
         ps = df * df;
         if (f == 0) {
-            if (counts) counts[j] = c;
+            if (counts) counts[j] = (int)c;
             if (c == 0 && flags) atomicAdd(&flags[1], 1);
         }
     }
@@ -715,6 +718,13 @@ fx_finalize_kernel(int k, int d, int ld, const unsigned long long *gsum, const i
     }
 }
 
+static cudaError_t fx_smem_limit(size_t smem) {
+    cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(fx_update_kernel<true>), smem);
+    if (e == cudaSuccess)
+        e = ensure_smem_limit(reinterpret_cast<const void *>(fx_update_kernel<false>), smem);
+    return e;
+}
+
 cudaError_t launch_kmeans_update_fx(const float *X, int ld, int n, int d, int k,
                                     const int *labels, const float *scale,
                                     const double *inv_scale, void *accum, int parity,
@@ -723,20 +733,11 @@ cudaError_t launch_kmeans_update_fx(const float *X, int ld, int n, int d, int k,
                                     unsigned *ticket, cudaStream_t s) {
     const size_t smem = fx_update_smem(k, d);
     if (smem > (size_t)FX_SMEM_LIMIT) return cudaErrorInvalidValue;
-    thread_local int smem_set[16] = {};
+    cudaError_t e = fx_smem_limit(smem);
+    if (e != cudaSuccess) return e;
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (dev < 0 || dev >= 16 || smem_set[dev] < (int)smem) {
-        cudaError_t e = cudaFuncSetAttribute(fx_update_kernel<true>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(fx_update_kernel<false>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 16) smem_set[dev] = (int)smem;
-    }
     const size_t kd = (size_t)k * d;
     unsigned long long *sum[2] = {static_cast<unsigned long long *>(accum),
                                   static_cast<unsigned long long *>(accum) + kd};
@@ -751,9 +752,53 @@ cudaError_t launch_kmeans_update_fx(const float *X, int ld, int n, int d, int k,
         fx_update_kernel<false><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale,
                                                               sum[p], cnt[p]);
     const int nb = (int)((kd + 255) / 256);
-    fx_finalize_kernel<<<nb, 256, 0, s>>>(k, d, ld, sum[p], cnt[p], sum[1 - p], cnt[1 - p],
-                                          inv_scale, C_prev, C_new, counts, block_partials,
-                                          scalars, flags, ticket);
+    fx_finalize_kernel<int><<<nb, 256, 0, s>>>(k, d, ld, sum[p], cnt[p], sum[1 - p], cnt[1 - p],
+                                               inv_scale, C_prev, C_new, counts, block_partials,
+                                               scalars, flags, ticket);
+    return cudaGetLastError();
+}
+
+// acc[k*d + j] = counts[j]; acc[k*d + k] = the label-change flag.
+__global__ void fx_pack_counts_kernel(int k, int kd, const int *counts, const int *changed,
+                                      long long *acc) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < k) acc[kd + j] = (long long)counts[j];
+    if (j == k) acc[kd + k] = changed ? (long long)(*changed != 0) : 0ll;
+}
+
+cudaError_t launch_kmeans_sums_fx(const float *X, int ld, int n, int d, int k, const int *labels,
+                                  const float *scale, long long *acc, int *counts,
+                                  const int *changed, cudaStream_t s) {
+    unsigned long long *sums = reinterpret_cast<unsigned long long *>(acc);
+    const size_t smem = fx_update_smem(k, d);
+    if (smem > (size_t)FX_SMEM_LIMIT) return cudaErrorInvalidValue;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = fx_smem_limit(smem);
+    if (e == cudaSuccess) e = cudaMemsetAsync(sums, 0, (size_t)k * d * 8, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(counts, 0, (size_t)k * 4, s);
+    if (e != cudaSuccess) return e;
+    const bool vec2 = d % 2 == 0 && ld % 2 == 0 && (reinterpret_cast<uintptr_t>(X) & 7) == 0;
+    if (vec2)
+        fx_update_kernel<true><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale, sums,
+                                                             counts);
+    else
+        fx_update_kernel<false><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale, sums,
+                                                              counts);
+    fx_pack_counts_kernel<<<(k + 1 + 255) / 256, 256, 0, s>>>(k, k * d, counts, changed, acc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_kmeans_finalize_shards(int k, int d, int ld, const long long *acc,
+                                          const double *inv_scale, const float *C_prev,
+                                          float *C_new, double *block_partials, double *scalars,
+                                          int *flags, unsigned *ticket, cudaStream_t s) {
+    const size_t kd = (size_t)k * d;
+    const int nb = (int)((kd + 255) / 256);
+    fx_finalize_kernel<long long><<<nb, 256, 0, s>>>(
+        k, d, ld, reinterpret_cast<const unsigned long long *>(acc), acc + kd, nullptr, nullptr,
+        inv_scale, C_prev, C_new, nullptr, block_partials, scalars, flags, ticket);
     return cudaGetLastError();
 }
 

@@ -843,13 +843,9 @@ cudaError_t launch_kmeans_assign_tc(int split, const void *Xh, const void *Xl, i
     a.amb_count = amb_count;
     a.err = err;
     auto kern = s3 ? kmeans_assign_tc_kernel<3> : kmeans_assign_tc_kernel<1>;
-    thread_local int smem_set[2][16] = {};
-    int *set = (dev >= 0 && dev < 16) ? &smem_set[s3 ? 1 : 0][dev] : nullptr;
-    if (!set || *set < (int)smem) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
+    {
+        cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(kern), smem);
         if (e != cudaSuccess) return e;
-        if (set) *set = (int)smem;
     }
     const int ntiles = (n + TC_BM - 1) / TC_BM;
     int nsm = 148;
@@ -887,15 +883,13 @@ cudaError_t launch_kmeans_rescore(const float *X, int ld, int d, const float *C,
     const int blocks = max(1, min(nsm * per_sm, (max_rows + 32 * warps - 1) / (32 * warps)));
     cudaError_t e;
     if (vec) {
-        e = cudaFuncSetAttribute(kmeans_rescore_kernel<true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = ensure_smem_limit(reinterpret_cast<const void *>(kmeans_rescore_kernel<true>), smem);
         if (e != cudaSuccess) return e;
         kmeans_rescore_kernel<true><<<blocks, 32 * warps, smem, s>>>(
             X, ld, d, dp, C, k, cnorm, amb_rows, amb_cand, amb_ncand, amb_count, labels,
             labels_prev, flags, c_in_smem);
     } else {
-        e = cudaFuncSetAttribute(kmeans_rescore_kernel<false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = ensure_smem_limit(reinterpret_cast<const void *>(kmeans_rescore_kernel<false>), smem);
         if (e != cudaSuccess) return e;
         kmeans_rescore_kernel<false><<<blocks, 32 * warps, smem, s>>>(
             X, ld, d, dp, C, k, cnorm, amb_rows, amb_cand, amb_ncand, amb_count, labels,

@@ -673,8 +673,7 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     int stages = 8;
     while (stages > 2 && tk_smem_bytes(nkb, stages) > 225 * 1024) --stages;
     const size_t smem = tk_smem_bytes(nkb, stages);
-    cudaError_t e =
-        cudaFuncSetAttribute(knn_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(knn_tc_kernel), smem);
     if (e != cudaSuccess) return e;
     KnnTcArgs a;
     a.nx = nx;
@@ -702,7 +701,7 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const size_t fsm = (size_t)TK_FIN_MAX * 8 + (size_t)d * sizeof(float);
-    e = cudaFuncSetAttribute(knn_tc_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm);
+    e = ensure_smem_limit(reinterpret_cast<const void *>(knn_tc_finalize), fsm);
     if (e != cudaSuccess) return e;
     knn_tc_finalize<<<nq, 256, fsm, s>>>(
         X, Q, ld, d, kc, k, cap, theta, cnt, static_cast<const int2 *>(list), take_sqrt, out_key,

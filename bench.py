@@ -247,7 +247,8 @@ def main():
         return 0
 
     X = make_data()
-    stream = torch.cuda.current_stream()
+    # the library's calls and the timing events share one (non-default) stream
+    stream = torch.cuda.Stream()
 
     def handle(mode):
         km = ab.KMeans(K, "s", order=ab.ROW_MAJOR, max_iter=MAX_ITER, n_init=1, seed=SEED)

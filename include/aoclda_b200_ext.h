@@ -42,6 +42,47 @@ da_status da_b200_get_stat(da_handle handle, const char *name, double *value);
 da_status da_b200_kmeans_init_centres_d(da_handle handle, double *C, da_int ldc);
 da_status da_b200_kmeans_init_centres_s(da_handle handle, float *C, da_int ldc);
 
+/* No counterpart in the AOCL-DA API.  Steps of a k-means (Lloyd) fit of one
+ * fp32 data set split row-wise over several handles (one per process / GPU),
+ * for a caller that runs the Lloyd loop of da_kmeans_compute_s and reduces
+ * one integer buffer over the processes per iteration.  Every handle holds
+ * its shard (da_kmeans_set_data_s) and the same options.  The results --
+ * labels, centres, iteration count -- equal those of da_kmeans_compute_s
+ * on the unsplit data with supplied initial centres and n_init = 1 (the
+ * inertia to fp64 rounding: the shards' inertias are added).
+ *
+ * da_b200_kmeans_shard_colmax_s: max |x| per feature over the shard
+ *   (n_features floats); the caller takes the element-wise maximum.
+ * da_b200_kmeans_shard_begin_s: starts a fit from the initial centres
+ *   (k x d row-major, host) with the whole data set's column maxima and row
+ *   count, which fix the fixed-point scales of the centroid sums.
+ * da_b200_kmeans_shard_partial_s: assigns the shard's rows to the current
+ *   centres (the plain fp32 labels) and writes, on the handle's stream, into
+ *   the caller's DEVICE buffer acc of DA_B200_KMEANS_SHARD_ACC_LEN(k, d)
+ *   int64: [0, k*d) the fixed-point centroid sums, [k*d, k*d+k) the counts,
+ *   [k*d+k] = 1 if a label changed since the previous partial step.  The
+ *   element-wise sum of acc over all shards (an integer all-reduce, exact in
+ *   any order) is the unsplit data's.
+ * da_b200_kmeans_shard_finalize_s: the new centres from the reduced acc
+ *   (centre j, feature f = (double)sum * 2^-s_f / max(count, 1) rounded to
+ *   fp32, s_f = min(62 - L, 44) - E_f clamped to [-126, 127], n <= 2^L,
+ *   colmax[f] < 2^E_f); scalars[0] = sum |C_old|^2, scalars[1] =
+ *   sum |C_old - C_new|^2 (fp64, a fixed order); flags[0] = any label
+ *   changed on any shard, flags[1] = empty clusters.  Synchronises.
+ * da_b200_kmeans_shard_inertia_s: the shard's inertia against the current
+ *   centres (fp64), with relabel != 0 after a new assignment to them.
+ * da_b200_kmeans_shard_result_s: current centres (k x d row-major) and the
+ *   shard's labels; either pointer may be null. */
+#define DA_B200_KMEANS_SHARD_ACC_LEN(k, d) ((size_t)(k) * (size_t)(d) + (size_t)(k) + 1u)
+da_status da_b200_kmeans_shard_colmax_s(da_handle handle, float *colmax);
+da_status da_b200_kmeans_shard_begin_s(da_handle handle, const float *colmax_global,
+                                       da_int n_global, const float *centres);
+da_status da_b200_kmeans_shard_partial_s(da_handle handle, long long *acc);
+da_status da_b200_kmeans_shard_finalize_s(da_handle handle, const long long *acc,
+                                          double *scalars, da_int *flags);
+da_status da_b200_kmeans_shard_inertia_s(da_handle handle, da_int relabel, double *inertia);
+da_status da_b200_kmeans_shard_result_s(da_handle handle, float *centres, da_int *labels);
+
 /* No counterpart in the AOCL-DA API.  Lloyd k-means on n_inst independent
  * fp32 data sets at once (different n, d and k): instance i has n_samples[i]
  * rows of n_features[i] values (row-major host array A[i], leading dimension
