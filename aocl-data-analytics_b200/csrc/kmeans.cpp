@@ -1100,6 +1100,8 @@ da_status KMeans<T>::shard_begin(const float *colmax_global, da_int n_global, co
                                  cudaMemcpyHostToDevice, st), "copy");
         B200_TRY(cudaStreamSynchronize(st), "sharded start");
         fx_stale = true; // the scales are the whole data set's, not this shard's
+        cuda->stats["tensor_core"] = use_tc ? 1.0 : 0.0;
+        cuda->stats["fixed_point_update"] = 1.0;
         shard_c = 0;
         shard_l = 0;
         shard_ready = true;

@@ -12,6 +12,13 @@ matrix; the metric is Lloyd iterations per second.  `value` keeps X resident
 in HBM (set once); `e2e` re-uploads X from pinned host memory and reads the
 labels and centres back inside every step.
 
+With --gpus N > 1 (one rank per GPU under torch.distributed.run) the data
+set is split across the ranks: every rank holds a copy of the 1,000,000 x
+64 set as its shard (weak scaling: the job clusters N x 1,000,000 rows), the
+ranks exchange their integer centroid sums in one NCCL all-reduce per Lloyd
+iteration, and `value` is N x the fit's Lloyd iterations per second.
+--sharded runs that path on one GPU too.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
 import argparse
@@ -89,7 +96,7 @@ class Clocks:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu),
                  "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -202,7 +209,7 @@ def config_dict(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
@@ -221,6 +228,9 @@ def main():
     ap.add_argument("--knn-queries", type=int, default=10_000)
     ap.add_argument("--knn-plain", type=int, default=1,
                     help="with --knn-only: also run the plain path (1) or not (0)")
+    ap.add_argument("--sharded", action="store_true",
+                    help="run the split-data path (every rank's shard, one NCCL all-reduce per "
+                         "Lloyd iteration) also on one GPU; it is the path for --gpus > 1")
     ap.add_argument("--rows", type=int, default=N,
                     help="rows of X (default 1,000,000; smaller only for profiling captures)")
     args = ap.parse_args()
@@ -231,11 +241,24 @@ def main():
     import torch
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    if world > 1:
+    if world > 1 or args.sharded:
         import torch.distributed as dist
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        kw = {}
+        if world == 1:
+            import socket
+            with socket.socket() as sk:
+                sk.bind(("127.0.0.1", 0))
+                kw = {"init_method": f"tcp://127.0.0.1:{sk.getsockname()[1]}", "rank": 0,
+                      "world_size": 1}
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local), **kw)
     ab = _load("aoclda_b200", os.path.join(PKG, "aoclda_b200.py"))
+    if world > 1 or args.sharded:
+        try:
+            return run_sharded(ab, args, rank, world, local)
+        finally:
+            torch.distributed.destroy_process_group()
     if args.serve_only:
         if rank == 0:
             print(json.dumps(run_serving(ab)))
@@ -411,8 +434,113 @@ def main():
     if rank == 0:
         print(json.dumps(out))
         sys.stdout.flush()
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_sharded(ab, args, rank, world, local):
+    """k-means over a data set split across the ranks (weak scaling): every
+    rank holds a copy of the 1,000,000 x 64 set as its shard, so the job
+    clusters world x 1,000,000 rows; per Lloyd iteration every rank assigns
+    its rows and writes its integer centroid sums (sharded.py), ONE NCCL
+    all-reduce of k*d + k + 1 int64 follows, and every rank computes the
+    same centres.  value = world x Lloyd iterations / s (the single-GPU unit:
+    iterations over 1,000,000 rows); e2e re-uploads the shard from pinned
+    host memory and reads labels and centres back in every step."""
+    import torch
+    sd = _load("aoclda_sharded", os.path.join(PKG, "sharded.py"))
+    comm = sd.TorchComm()
+    X = make_data()
+    mode = os.environ.get("BENCH_MODE", "bf16x3")
+    # the k-means++ centres of the single-GPU workload, from rank 0
+    C0 = np.zeros((K, D), dtype=np.float32)
+    if rank == 0:
+        km0 = ab.KMeans(K, "s", order=ab.ROW_MAJOR, max_iter=MAX_ITER, n_init=1, seed=SEED)
+        km0.set_data(X)
+        C0 = km0.init_centres(K)
+        km0.close()
+    c0 = torch.from_numpy(np.ascontiguousarray(C0)).cuda()
+    torch.distributed.broadcast(c0, 0)
+    C0 = c0.cpu().numpy()
+    shard = sd.DeviceKMeansShard(ab, X, K, precision_mode=mode)
+    stream = shard.stream
+
+    def step():
+        return sd.kmeans_fit([shard], C0, comm, max_iter=MAX_ITER, tol=TOL)["n_iter"]
+
+    def timed(fn, steps, warmup, sample_clocks=False):
+        for _ in range(warmup):
+            fn()
+        torch.distributed.barrier()
+        torch.cuda.synchronize()
+        clk = Clocks(local) if sample_clocks else None
+        if clk:
+            clk.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        iters = 0
+        for _ in range(steps):
+            iters += fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clocks = clk.stop() if clk else None
+        t = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item()), iters, clocks
+
+    ms, iters, clocks = timed(step, args.steps, args.warmup, sample_clocks=True)
+    n_iter = iters // args.steps
+    value = world * iters / (ms / 1e3)
+    # kernel times of one step (event timing serialises the launches)
+    L = shard.km.L
+    L.da_b200_set_kernel_timing(shard.km.h, 1)
+    L.da_b200_reset_kernel_time(shard.km.h)
+    step()
+    L.da_b200_set_kernel_timing(shard.km.h, 0)
+    kt = {n: shard.km.kernel_time(n) for n in ("kmeans_assign", "kmeans_rescore", "kmeans_update")}
+    a_ms, a_n = kt["kmeans_assign"]
+    a_avg = a_ms / max(a_n, 1)
+    hbm, bf16, peak_src = load_peaks()
+    flops = 2.0 * N * K * D
+    tensor_core = shard.km.stat("tensor_core") == 1.0
+    achieved = flops / (a_avg / 1e3) / 1e12
+    roof = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
+            "frac": achieved / bf16, "traffic": None, "peak_source": peak_src,
+            "kernel": "kmeans_assign_tc_kernel (tcgen05 bf16, TMEM fp32)" if tensor_core
+            else "kmeans_assign_kernel (SIMT fp32)", "avg_launch_ms": a_avg,
+            "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in kt.items() if v[1]}}
+
+    e2e = None
+    if not args.no_e2e:
+        Xp = torch.empty((N, D), dtype=torch.float32, pin_memory=True).numpy()
+        Xp[:] = X
+
+        def e2e_step():
+            shard.km.set_data(Xp)
+            it = sd.kmeans_fit([shard], C0, comm, max_iter=MAX_ITER, tol=TOL)["n_iter"]
+            shard.result()
+            return it
+
+        ems, eiters, _ = timed(e2e_step, args.steps, max(1, min(args.warmup, 2)))
+        e2e = {"value": world * eiters / (ems / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": N * D * 4 + K * D * 4 + D * 4,
+               "d2h_bytes_per_step": N * 4 + K * D * 4 + D * 4}
+    shard.close()
+    cfg = config_dict(args) | {
+        "workload": f"kmeans_lloyd_fp32_{N}x64_k256_split_over_{world}_ranks",
+        "n_samples_total": N * world,
+        "parallelism": f"data split over {world} ranks (one shard each, every shard a copy of "
+                       f"the {N} x 64 set); one NCCL all-reduce of k*d+k+1 int64 per Lloyd "
+                       "iteration",
+        "iterations_per_step": n_iter,
+        "step": "one sharded Lloyd fit (sharded.kmeans_fit) = n_iter iterations on every rank"}
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": cfg, "roofline": roof, "cpu_baseline": None, "e2e": e2e,
+           "gpu_launches": (7 * n_iter + 10) * args.steps, "clocks": clocks}
+    if rank == 0:
+        print(json.dumps(out))
+        sys.stdout.flush()
     return 0
 
 
