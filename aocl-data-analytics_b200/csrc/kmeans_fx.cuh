@@ -52,4 +52,26 @@ __device__ __forceinline__ void fx_flush(unsigned long long *acc, int d, int j, 
     run = FxRun();
 }
 
+// The same run sums for VW consecutive features of one lane.
+template <int VW> struct FxRunV {
+    unsigned h[VW], l[VW];
+    unsigned n;
+    __device__ __forceinline__ void reset() {
+#pragma unroll
+        for (int v = 0; v < VW; ++v) h[v] = l[v] = 0u;
+        n = 0u;
+    }
+};
+template <int VW>
+__device__ __forceinline__ void fx_flush_v(unsigned long long *acc, int d, int j, int f,
+                                           FxRunV<VW> &run) {
+    if (run.n) {
+#pragma unroll
+        for (int v = 0; v < VW; ++v)
+            if (f + v < d)
+                fx_add(acc + (size_t)j * d + f + v, fx_run_sum(run.h[v], run.l[v], run.n));
+    }
+    run.reset();
+}
+
 } // namespace b200

@@ -498,7 +498,8 @@ B200_KM_INST(double)
 namespace {
 constexpr int FX_SMEM_LIMIT = 200 * 1024;
 constexpr int FX_THREADS = 1024;
-constexpr int FX_ROWS = 8;     // rows in flight per warp
+constexpr int FX_ROWS = 8;     // rows in flight per warp (1 or 2 features per lane)
+constexpr int FX_ROWS_V4 = 6;  // rows in flight per sub-warp (4 features per lane)
 constexpr int FX_BATCH = 8192; // rows sorted by label per pass of a CTA
 static_assert(FX_BATCH / (FX_THREADS / 32) + 1 <= 511, "run sums must fit in int32");
 } // namespace
@@ -543,14 +544,17 @@ cudaError_t launch_col_absmax(const float *X, int ld, int n, int d, unsigned *co
 // the batch's rows are bucketed by label in shared memory (counting sort; the
 // order inside a bucket does not matter, the sums are integers), then each
 // warp walks an equal share of the bucketed list, keeping the running sums of
-// the current cluster in registers (lanes over feature pairs) and adding them
-// to the CTA's shared accumulators only when the cluster changes.  The CTA's
-// sums and counts are finally added (integer reductions, order-free) into the
-// global accumulators gsum / gcnt.
-template <bool VEC2>
+// the current cluster in registers and adding them to the CTA's shared
+// accumulators only when the cluster changes.  Lanes hold VW consecutive
+// features (one vector load per row); with VW = 4 and d <= 128 a row takes
+// `sub_w` lanes (the next power of two >= d / 4) and the warp's 32 / sub_w
+// sub-warps walk separate parts of its share, so one warp instruction serves
+// several rows.  The CTA's sums and counts are finally added (integer
+// reductions, order-free) into the global accumulators gsum / gcnt.
+template <int VW>
 __global__ void __launch_bounds__(FX_THREADS, 1)
 fx_update_kernel(const float *X, int ld, int n, int d, int k, const int *labels,
-                 const float *scale, unsigned long long *gsum, int *gcnt) {
+                 const float *scale, unsigned long long *gsum, int *gcnt, int sub_w) {
     extern __shared__ __align__(16) unsigned char fx_smem[];
     unsigned long long *acc = reinterpret_cast<unsigned long long *>(fx_smem);
     int *list = reinterpret_cast<int *>(acc + (size_t)k * d); // FX_BATCH row ids
@@ -564,6 +568,8 @@ fx_update_kernel(const float *X, int ld, int n, int d, int k, const int *labels,
     const int r0 = (int)min((long long)n, per * blockIdx.x);
     const int r1 = (int)min((long long)n, per * (blockIdx.x + 1));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int W = VW == 4 ? sub_w : 32;
+    const int R = 32 / W, sub = lane / W, sl = lane - sub * W;
     for (int b0 = r0; b0 < r1; b0 += FX_BATCH) {
         const int nb = min(FX_BATCH, r1 - b0);
         for (int j = threadIdx.x; j <= k; j += blockDim.x) cur[j] = 0;
@@ -593,8 +599,10 @@ fx_update_kernel(const float *X, int ld, int n, int d, int k, const int *labels,
         for (int i = threadIdx.x; i < nb; i += blockDim.x)
             list[atomicAdd(&cur[labels[b0 + i]], 1)] = b0 + i;
         __syncthreads();
-        // this warp's share of the bucketed list
-        const int p0 = (int)((long long)nb * warp / nw), p1 = (int)((long long)nb * (warp + 1) / nw);
+        // this sub-warp's part of the warp's share of the bucketed list
+        const int w0 = (int)((long long)nb * warp / nw), w1 = (int)((long long)nb * (warp + 1) / nw);
+        const int p0 = w0 + (int)((long long)(w1 - w0) * sub / R);
+        const int p1 = w0 + (int)((long long)(w1 - w0) * (sub + 1) / R);
         if (p0 < p1) {
             int j0 = 0; // bucket holding position p0: last j with off[j] <= p0
             {
@@ -606,47 +614,92 @@ fx_update_kernel(const float *X, int ld, int n, int d, int k, const int *labels,
                 }
                 j0 = lo;
             }
-            const int fstep = VEC2 ? 64 : 32;
-            for (int fb = 0; fb < d; fb += fstep) {
-                const int f = fb + (VEC2 ? 2 * lane : lane);
-                const float s0 = f < d ? sc[f] : 0.f;
-                const float s1 = VEC2 && f + 1 < d ? sc[f + 1] : 0.f;
-                const float s0_22 = s0 * 2.384185791015625e-07f, s1_22 = s1 * 2.384185791015625e-07f;
+            for (int fb = 0; fb < d; fb += VW * W) {
+                const int f = fb + VW * sl;
+                float sv[VW], sv22[VW];
+#pragma unroll
+                for (int v = 0; v < VW; ++v) {
+                    sv[v] = f + v < d ? sc[f + v] : 0.f;
+                    sv22[v] = sv[v] * 2.384185791015625e-07f;
+                }
                 int j = j0;
                 int jend = off[j + 1];
-                FxRun run;
-                for (int p = p0; p < p1; p += FX_ROWS) {
-                    float2 xv[FX_ROWS];
+                FxRunV<VW> run;
+                run.reset();
+                constexpr int NR = VW == 4 ? FX_ROWS_V4 : FX_ROWS;
+                for (int p = p0; p < p1; p += NR) {
+                    float xv[NR][VW];
 #pragma unroll
-                    for (int u = 0; u < FX_ROWS; ++u) {
-                        xv[u] = make_float2(0.f, 0.f);
+                    for (int u = 0; u < NR; ++u) {
+#pragma unroll
+                        for (int v = 0; v < VW; ++v) xv[u][v] = 0.f;
                         if (p + u < p1 && f < d) {
                             const float *xr = X + (size_t)list[p + u] * ld + f;
-                            if (VEC2) xv[u] = *reinterpret_cast<const float2 *>(xr);
-                            else xv[u].x = *xr;
+                            if (VW == 4) {
+                                const float4 t = *reinterpret_cast<const float4 *>(xr);
+                                xv[u][0] = t.x, xv[u][1] = t.y, xv[u][VW > 2 ? 2 : 0] = t.z,
+                                xv[u][VW > 3 ? 3 : 0] = t.w;
+                            } else if (VW == 2) {
+                                const float2 t = *reinterpret_cast<const float2 *>(xr);
+                                xv[u][0] = t.x, xv[u][VW > 1 ? 1 : 0] = t.y;
+                            } else {
+                                xv[u][0] = *xr;
+                            }
                         }
                     }
 #pragma unroll
-                    for (int u = 0; u < FX_ROWS; ++u) {
+                    for (int u = 0; u < NR; ++u) {
                         if (p + u < p1) {
                             while (p + u >= jend) { // next non-empty bucket
-                                fx_flush(acc, d, j, f, run, VEC2);
+                                fx_flush_v<VW>(acc, d, j, f, run);
                                 ++j;
                                 jend = off[j + 1];
                             }
-                            fx_acc(xv[u].x, s0_22, s0, run.h0, run.l0);
-                            if (VEC2) fx_acc(xv[u].y, s1_22, s1, run.h1, run.l1);
+#pragma unroll
+                            for (int v = 0; v < VW; ++v)
+                                fx_acc(xv[u][v], sv22[v], sv[v], run.h[v], run.l[v]);
                             ++run.n;
                         }
                     }
                 }
-                fx_flush(acc, d, j, f, run, VEC2);
+                fx_flush_v<VW>(acc, d, j, f, run);
             }
         }
         __syncthreads();
     }
     for (int e = threadIdx.x; e < kd; e += blockDim.x)
         if (acc[e]) atomicAdd(&gsum[e], acc[e]);
+}
+
+// Vector width and sub-warp width of the update for X's layout.
+static void fx_shape(const float *X, int ld, int d, int &vw, int &sub_w) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(X);
+    sub_w = 32;
+    if (d % 4 == 0 && ld % 4 == 0 && (a & 15) == 0 && d <= 128) {
+        vw = 4;
+        sub_w = 1;
+        while (sub_w * 4 < d) sub_w <<= 1;
+    } else if (d % 2 == 0 && ld % 2 == 0 && (a & 7) == 0) {
+        vw = 2;
+    } else {
+        vw = 1;
+    }
+}
+
+static void fx_launch(const float *X, int ld, int n, int d, int k, const int *labels,
+                      const float *scale, unsigned long long *sums, int *counts, int nsm,
+                      size_t smem, cudaStream_t s) {
+    int vw = 1, sub_w = 32;
+    fx_shape(X, ld, d, vw, sub_w);
+    if (vw == 4)
+        fx_update_kernel<4><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale, sums,
+                                                          counts, sub_w);
+    else if (vw == 2)
+        fx_update_kernel<2><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale, sums,
+                                                          counts, sub_w);
+    else
+        fx_update_kernel<1><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale, sums,
+                                                          counts, sub_w);
 }
 
 // One thread per (cluster, feature): the mean from the global sums, and fp64
@@ -719,9 +772,11 @@ fx_finalize_kernel(int k, int d, int ld, const unsigned long long *gsum, const C
 }
 
 static cudaError_t fx_smem_limit(size_t smem) {
-    cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(fx_update_kernel<true>), smem);
+    cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(fx_update_kernel<4>), smem);
     if (e == cudaSuccess)
-        e = ensure_smem_limit(reinterpret_cast<const void *>(fx_update_kernel<false>), smem);
+        e = ensure_smem_limit(reinterpret_cast<const void *>(fx_update_kernel<2>), smem);
+    if (e == cudaSuccess)
+        e = ensure_smem_limit(reinterpret_cast<const void *>(fx_update_kernel<1>), smem);
     return e;
 }
 
@@ -744,13 +799,7 @@ cudaError_t launch_kmeans_update_fx(const float *X, int ld, int n, int d, int k,
     int *cnt[2] = {reinterpret_cast<int *>(sum[1] + kd),
                    reinterpret_cast<int *>(sum[1] + kd) + k};
     const int p = parity & 1;
-    const bool vec2 = d % 2 == 0 && ld % 2 == 0 && (reinterpret_cast<uintptr_t>(X) & 7) == 0;
-    if (vec2)
-        fx_update_kernel<true><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale,
-                                                             sum[p], cnt[p]);
-    else
-        fx_update_kernel<false><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale,
-                                                              sum[p], cnt[p]);
+    fx_launch(X, ld, n, d, k, labels, scale, sum[p], cnt[p], nsm, smem, s);
     const int nb = (int)((kd + 255) / 256);
     fx_finalize_kernel<int><<<nb, 256, 0, s>>>(k, d, ld, sum[p], cnt[p], sum[1 - p], cnt[1 - p],
                                                inv_scale, C_prev, C_new, counts, block_partials,
@@ -779,13 +828,7 @@ cudaError_t launch_kmeans_sums_fx(const float *X, int ld, int n, int d, int k, c
     if (e == cudaSuccess) e = cudaMemsetAsync(sums, 0, (size_t)k * d * 8, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(counts, 0, (size_t)k * 4, s);
     if (e != cudaSuccess) return e;
-    const bool vec2 = d % 2 == 0 && ld % 2 == 0 && (reinterpret_cast<uintptr_t>(X) & 7) == 0;
-    if (vec2)
-        fx_update_kernel<true><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale, sums,
-                                                             counts);
-    else
-        fx_update_kernel<false><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale, sums,
-                                                              counts);
+    fx_launch(X, ld, n, d, k, labels, scale, sums, counts, nsm, smem, s);
     fx_pack_counts_kernel<<<(k + 1 + 255) / 256, 256, 0, s>>>(k, k * d, counts, changed, acc);
     return cudaGetLastError();
 }

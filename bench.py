@@ -734,16 +734,20 @@ def run_e2e(ab, km, X, C0, stream, args, world):
         e2e_step()
     torch.cuda.synchronize()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
     f0.record(stream)
     e2e_iters = 0
     for _ in range(args.steps):
         e2e_iters += e2e_step()
     f1.record(stream)
     torch.cuda.synchronize()
+    wall_ms = (time.perf_counter() - t0) * 1e3
     e2e_ms = f0.elapsed_time(f1)
     e2e_value = e2e_iters * world / (e2e_ms / 1e3)
     return {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N * D * 4 + K * D * 4,
-            "d2h_bytes_per_step": N * 4 + K * D * 4 + 6 * 4}
+            "d2h_bytes_per_step": N * 4 + K * D * 4 + 6 * 4, "ms_per_step": e2e_ms / args.steps,
+            "host_wall_ms_per_step": wall_ms / args.steps,
+            "iterations_per_step": e2e_iters / args.steps}
 
 
 if __name__ == "__main__":
