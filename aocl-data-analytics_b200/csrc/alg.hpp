@@ -128,6 +128,7 @@ template <typename T> struct KMeans : public AlgBase {
     int tc_split = 0;     // bf16 terms of the resident X copies (0: none)
     bool use_tc = false; // bf16 tensor-core assignment active for this compute
     bool dXbf_stale = true;
+    bool dx_loaded = false; // dX holds the current data set
     bool aaug_ready = false;
     bool fx_stale = true;  // fixed-point scales need recomputing (new data)
     bool fx_data_ok = false; // data finite (scales valid)
@@ -137,6 +138,12 @@ template <typename T> struct KMeans : public AlgBase {
     da_int amb_last = 0;  // rows relabelled exactly in the last tensor-core pass
     T *h_pin = nullptr;
     void *h_small = nullptr; // pinned: flags + scalars
+    // Lloyd iterations 1.. as one CUDA graph (a WHILE node whose body is one
+    // iteration in place); rebuilt when a pointer or size it holds changes
+    cudaGraph_t loop_graph = nullptr;
+    cudaGraphExec_t loop_exec = nullptr;
+    std::vector<uintptr_t> loop_key;
+    DevBuf dLoop;
 
     KMeans(ErrorRecord *e, CudaCtx *c, bool single);
     ~KMeans() override;
@@ -164,6 +171,9 @@ template <typename T> struct KMeans : public AlgBase {
     da_status lloyd_step(const T *dCprev, T *dCnew, int *dL, const int *dLprev, bool update,
                          double *h_scal, int *h_flags);
     da_status split_empty(T *dC, int *dL, bool &split);
+    da_status lloyd_graph(T *dC, int *dL, da_int &n_iter, int &converged, bool &ran);
+    bool build_loop_graph(T *dC, int *dL);
+    void drop_loop_graph();
     da_status prepare_tc();
     da_status prepare_fx();
     // Lloyd steps of a shard of a data set split across processes: the

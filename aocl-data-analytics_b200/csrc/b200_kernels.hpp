@@ -179,6 +179,24 @@ cudaError_t launch_kmeans_update_fx(const float *X, int ld, int n, int d, int k,
                                     const float *C_prev, float *C_new, int *counts,
                                     double *block_partials, double *scalars, int *flags,
                                     unsigned *ticket, cudaStream_t s);
+// Device state of a Lloyd loop run as a CUDA graph (WHILE node): the next
+// iteration's index, the limits, and the outcome written by the finalize.
+struct LloydLoopState {
+    int it;       // index of the iteration the next finalize ends
+    int max_iter;
+    int conv;     // 0, 1 (centre shift below tol), 2 (no label changed)
+    int n_iter;   // the host loop's iteration count at its end
+    double tol;
+};
+// One Lloyd update inside the graph loop: sums into accumulator set 0
+// (cleared first), new centres in place in C, the convergence test of
+// iteration ls->it, and cudaGraphSetConditional(cond, 0) when the loop ends.
+cudaError_t launch_kmeans_update_fx_loop(const float *X, int ld, int n, int d, int k,
+                                         const int *labels, const float *scale,
+                                         const double *inv_scale, void *accum, float *C,
+                                         int *counts, double *block_partials, double *scalars,
+                                         int *flags, unsigned *ticket, LloydLoopState *ls,
+                                         unsigned long long cond, cudaStream_t s);
 // One shard's share of a data set split across processes, packed for one
 // integer all-reduce: acc[0, k*d) the fixed-point sums (two's complement,
 // from zero), acc[k*d, k*d+k) the counts, acc[k*d+k] = (*changed != 0).

@@ -52,6 +52,7 @@ KMeans<T>::KMeans(ErrorRecord *e, CudaCtx *c, bool single) {
 }
 
 template <typename T> KMeans<T>::~KMeans() {
+    drop_loop_graph();
     if (h_small) cudaFreeHost(h_small);
 }
 
@@ -77,7 +78,9 @@ da_status KMeans<T>::set_data(da_int n, da_int d, const T *A, da_int lda) {
     n_features = d;
     initdone = true;
     model_trained = false;
-    dX.release();
+    // the device copy is refreshed on the next use, in the same allocation
+    // when it is large enough (no free / malloc per new data set)
+    dx_loaded = false;
     // n_clusters is re-bounded by the number of samples (kmeans_options.hpp:153-170)
     da_int kc = opts.i("n_clusters");
     opts.rebound_int("n_clusters", 1, LB::greaterequal, n, UB::lessequal);
@@ -99,7 +102,7 @@ da_status KMeans<T>::set_data(da_int n, da_int d, const T *A, da_int lda) {
 template <typename T> da_status KMeans<T>::ensure_device_data() {
     da_status s = cuda->init(*err);
     if (s != da_status_success) return s;
-    if (dX.p) return da_status_success;
+    if (dx_loaded && dX.p) return da_status_success;
     ld = pad4(n_features);
     if (!dX.ensure((size_t)n_samples * ld * sizeof(T)) || !dXn.ensure((size_t)n_samples * sizeof(T)))
         return err->error(da_status_memory_error, "Device memory allocation failed.");
@@ -110,6 +113,7 @@ template <typename T> da_status KMeans<T>::ensure_device_data() {
              "row norms");
     dXbf_stale = true;
     fx_stale = true;
+    dx_loaded = true;
     return da_status_success;
 }
 
@@ -632,6 +636,141 @@ template <typename T> da_status KMeans<T>::split_empty(T *dC, int *dL, bool &spl
     return da_status_success;
 }
 
+// ------------------------------------------- Lloyd loop as a CUDA graph ----
+// Iterations 1.. of run_lloyd (fp32 on the tensor cores, fixed-point update,
+// empty clusters ignored, no kernel timing) as one graph launch: a WHILE conditional node
+// whose body is one Lloyd iteration working in place on the centres dC and
+// the labels dL (every kernel reads a row's or element's old value before
+// the same thread writes the new one), with the convergence test on the
+// device (fx_finalize_kernel), so the host waits once per fit instead of
+// once per iteration.  The decisions are the host loop's: the same fp64
+// scalars, the same comparisons.
+template <typename T> void KMeans<T>::drop_loop_graph() {
+    if (loop_exec) cudaGraphExecDestroy(loop_exec);
+    if (loop_graph) cudaGraphDestroy(loop_graph);
+    loop_exec = nullptr;
+    loop_graph = nullptr;
+    loop_key.clear();
+}
+
+template <typename T> bool KMeans<T>::build_loop_graph(T *dC, int *dL) {
+    if constexpr (!std::is_same_v<T, float>) {
+        (void)dC, (void)dL;
+        return false;
+    } else {
+        cudaStream_t st = cuda->stream;
+        const int n = n_samples, k = n_clusters, d = n_features;
+        cudaGraph_t g = nullptr;
+        if (cudaGraphCreate(&g, 0) != cudaSuccess) return false;
+        cudaGraphConditionalHandle cond = 0;
+        cudaGraphNodeParams p = {};
+        cudaGraphNode_t node;
+        bool ok = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault) ==
+                  cudaSuccess;
+        if (ok) {
+            p.type = cudaGraphNodeTypeConditional;
+            p.conditional.handle = cond;
+            p.conditional.type = cudaGraphCondTypeWhile;
+            p.conditional.size = 1;
+            ok = cudaGraphAddNode(&node, g, nullptr, 0, &p) == cudaSuccess;
+        }
+        cudaGraph_t body = ok ? p.conditional.phGraph_out[0] : nullptr;
+        if (ok)
+            ok = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            bool launched = launch_centre_norms<float>(dC, ld, k, d, dCn.as<float>(), st) ==
+                                cudaSuccess &&
+                            cudaMemsetAsync(dFlags.p, 0, 8 * sizeof(int), st) == cudaSuccess;
+            launched = launched && assign(dC, dL, dL) == da_status_success;
+            const double *scale = dFxScale.as<double>();
+            launched = launched &&
+                       launch_kmeans_update_fx_loop(
+                           dX.as<float>(), ld, n, d, k, dL, reinterpret_cast<const float *>(scale),
+                           scale + d, dFxAcc.p, dC, dCounts.as<int>(), dScalars.as<double>() + 8,
+                           dScalars.as<double>(), dFlags.as<int>(), dFxTicket.as<unsigned>(),
+                           dLoop.as<LloydLoopState>(), (unsigned long long)cond,
+                           st) == cudaSuccess;
+            cudaGraph_t captured = nullptr;
+            const bool ended = cudaStreamEndCapture(st, &captured) == cudaSuccess;
+            ok = launched && ended;
+        }
+        if (ok) ok = cudaGraphInstantiate(&loop_exec, g, 0) == cudaSuccess;
+        if (!ok) {
+            cudaGetLastError();
+            err->clear();
+            loop_exec = nullptr;
+            cudaGraphDestroy(g);
+            return false;
+        }
+        loop_graph = g;
+        return true;
+    }
+}
+
+template <typename T>
+da_status KMeans<T>::lloyd_graph(T *dC, int *dL, da_int &n_iter_out, int &converged, bool &ran) {
+    ran = false;
+    if constexpr (!std::is_same_v<T, float>) {
+        (void)dC, (void)dL, (void)n_iter_out, (void)converged;
+        return da_status_success;
+    } else {
+        cudaStream_t st = cuda->stream;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+            cudaGetLastError();
+            return da_status_success; // the caller captures: run the host loop
+        }
+        if (!dLoop.ensure(sizeof(LloydLoopState))) return da_status_success;
+        const std::vector<uintptr_t> key = {
+            (uintptr_t)st, (uintptr_t)dC, (uintptr_t)dL, (uintptr_t)dX.p, (uintptr_t)dCn.p,
+            (uintptr_t)dFlags.p, (uintptr_t)dFxAcc.p, (uintptr_t)dFxScale.p,
+            (uintptr_t)dScalars.p, (uintptr_t)dCounts.p, (uintptr_t)dFxTicket.p,
+            (uintptr_t)dLoop.p, (uintptr_t)dXh.p, (uintptr_t)dXl.p, (uintptr_t)dXnrm.p,
+            (uintptr_t)dBh.p, (uintptr_t)dBl.p, (uintptr_t)dBaug.p, (uintptr_t)dAaug.p,
+            (uintptr_t)dCtmp.p, (uintptr_t)dTcScal.p, (uintptr_t)dAmb.p, (uintptr_t)n_samples,
+            (uintptr_t)n_clusters, (uintptr_t)n_features, (uintptr_t)ld, (uintptr_t)use_tc,
+            (uintptr_t)tc_split, (uintptr_t)ldbf};
+        if (!loop_exec || key != loop_key) {
+            drop_loop_graph();
+            if (!build_loop_graph(dC, dL)) return da_status_success;
+            loop_key = key;
+        }
+        char *hb = static_cast<char *>(h_small);
+        LloydLoopState *hs = reinterpret_cast<LloydLoopState *>(hb + 128);
+        LloydLoopState *ho = reinterpret_cast<LloydLoopState *>(hb + 160);
+        int *tc_state = reinterpret_cast<int *>(hb + 192);
+        *hs = LloydLoopState{1, (int)max_iter, 0, 0, (double)tol};
+        tc_state[0] = tc_state[1] = tc_state[2] = 0;
+        B200_TRY(cudaMemcpyAsync(dLoop.p, hs, sizeof(LloydLoopState), cudaMemcpyHostToDevice, st),
+                 "copy");
+        B200_TRY(cudaGraphLaunch(loop_exec, st), "Lloyd loop graph");
+        B200_TRY(cudaMemcpyAsync(ho, dLoop.p, sizeof(LloydLoopState), cudaMemcpyDeviceToHost, st),
+                 "copy");
+        if (use_tc)
+            B200_TRY(cudaMemcpyAsync(tc_state, dTcScal.as<char>() + 16, 3 * sizeof(int),
+                                     cudaMemcpyDeviceToHost, st), "copy");
+        // both accumulator sets zero again for the host-loop steps that follow
+        B200_TRY(cudaMemsetAsync(dFxAcc.p, 0, fx_accum_bytes(n_clusters, n_features), st),
+                 "memset");
+        B200_TRY(cudaStreamSynchronize(st), "Lloyd loop graph");
+        fx_parity = 0;
+        if (use_tc) {
+            amb_last = tc_state[0];
+            cuda->stats["relabelled_rows"] = (double)amb_last;
+            cuda->stats["full_scan_rows"] = (double)tc_state[2];
+            if (tc_state[1] != 0)
+                return err->error(da_status_internal_error,
+                                  "The tensor-core assignment kernel timed out waiting on a "
+                                  "pipeline barrier (code " + std::to_string(tc_state[1]) + ").");
+        }
+        n_iter_out = ho->n_iter;
+        converged = ho->conv;
+        ran = true;
+        return da_status_success;
+    }
+}
+
 // perform_kmeans (kmeans.cpp:996-1058)
 template <typename T>
 da_status KMeans<T>::run_lloyd(T *&dCcur, T *&dCprev, int *&dLcur, int *&dLprev, da_int &n_iter,
@@ -640,8 +779,22 @@ da_status KMeans<T>::run_lloyd(T *&dCcur, T *&dCprev, int *&dLcur, int *&dLprev,
     int *h_flags = reinterpret_cast<int *>(static_cast<char *>(h_small) + 64);
     converged = 0;
     empty_found = false;
+    // iterations 1.. as one graph launch where the loop allows it
+    const bool graph = use_fx && use_tc && empty_mode == EC_IGNORE && !cuda->timing;
     da_int it = 0;
     for (it = 0; it < max_iter; ++it) {
+        if (graph && it == 1) {
+            bool ran = false;
+            da_int nit = 0;
+            int conv = 0;
+            da_status s = lloyd_graph(dCcur, dLcur, nit, conv, ran);
+            if (s != da_status_success) return s;
+            if (ran) {
+                converged = conv;
+                it = nit;
+                break;
+            }
+        }
         std::swap(dCprev, dCcur);
         std::swap(dLprev, dLcur);
         da_status s = lloyd_step(dCprev, dCcur, dLcur, dLprev, true, h_scal, h_flags);

@@ -87,8 +87,9 @@ kmeans_assign_kernel(const T *X, int n, int ld, int d, const T *C, int k, const 
                 // NaN distances never win: fall back to cluster 0 as the
                 // reference's scalar kernel does (label initialised to 0).
                 const int lbl = (bidx[i] == 0x7fffffff) ? 0 : bidx[i];
-                labels[gi] = lbl;
+                // read before the write: labels may be labels_prev (in place)
                 if (labels_prev && labels_prev[gi] != lbl) ch = 1;
+                labels[gi] = lbl;
             }
         }
         if (ch) changed = 1;
@@ -709,12 +710,18 @@ static void fx_launch(const float *X, int ld, int n, int d, int k, const int *la
 // (nsum / ncnt, used by the next update) is cleared here when given.
 // Counts are int (one device's accumulators) or int64 (the sum over the
 // shards of a data set split across processes).
+//
+// With `ls` (the Lloyd loop run as a CUDA graph), the last block also makes
+// the convergence test of the host loop for iteration ls->it -- no label
+// changed after iteration 1, or |C_prev - C_new| < tol |C_prev| -- and ends
+// the graph's WHILE node (cond) when it passes or max_iter is reached.
 template <typename CT>
 __global__ void __launch_bounds__(256)
 fx_finalize_kernel(int k, int d, int ld, const unsigned long long *gsum, const CT *gcnt,
                    unsigned long long *nsum, int *ncnt, const double *inv_scale,
                    const float *C_prev, float *C_new, int *counts, double *block_partials,
-                   double *scalars, int *flags, unsigned *ticket) {
+                   double *scalars, int *flags, unsigned *ticket, LloydLoopState *ls,
+                   unsigned long long cond) {
     __shared__ double s0[256], s1[256];
     __shared__ bool last;
     const int kd = k * d;
@@ -759,6 +766,7 @@ fx_finalize_kernel(int k, int d, int ld, const unsigned long long *gsum, const C
     if (last && threadIdx.x < 32) {
         __threadfence();
         const int lane = threadIdx.x;
+        double sv[2];
         for (int v = 0; v < 2; ++v) {
             double a = 0.0;
             for (int b = lane; b < (int)gridDim.x; b += 32)
@@ -766,8 +774,21 @@ fx_finalize_kernel(int k, int d, int ld, const unsigned long long *gsum, const C
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
             if (lane == 0) scalars[v] = a;
+            sv[v] = a;
         }
         if (lane == 0) *ticket = 0u;
+        if (ls && lane == 0) {
+            const int it = ls->it;
+            int conv = 0;
+            if (it > 1 && *((volatile int *)flags) == 0) conv = 2;
+            if (conv == 0 && sqrt(sv[1]) < ls->tol * sqrt(sv[0])) conv = 1;
+            const int next = it + 1;
+            const bool stop = conv > 0 || next >= ls->max_iter;
+            ls->conv = conv;
+            ls->n_iter = conv > 0 ? it : next;
+            ls->it = next;
+            if (stop) cudaGraphSetConditional(cond, 0);
+        }
     }
 }
 
@@ -803,7 +824,35 @@ cudaError_t launch_kmeans_update_fx(const float *X, int ld, int n, int d, int k,
     const int nb = (int)((kd + 255) / 256);
     fx_finalize_kernel<int><<<nb, 256, 0, s>>>(k, d, ld, sum[p], cnt[p], sum[1 - p], cnt[1 - p],
                                                inv_scale, C_prev, C_new, counts, block_partials,
-                                               scalars, flags, ticket);
+                                               scalars, flags, ticket, nullptr, 0ull);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_kmeans_update_fx_loop(const float *X, int ld, int n, int d, int k,
+                                         const int *labels, const float *scale,
+                                         const double *inv_scale, void *accum, float *C,
+                                         int *counts, double *block_partials, double *scalars,
+                                         int *flags, unsigned *ticket, LloydLoopState *ls,
+                                         unsigned long long cond, cudaStream_t s) {
+    const size_t smem = fx_update_smem(k, d);
+    if (smem > (size_t)FX_SMEM_LIMIT) return cudaErrorInvalidValue;
+    cudaError_t e = fx_smem_limit(smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const size_t kd = (size_t)k * d;
+    unsigned long long *sum = static_cast<unsigned long long *>(accum);
+    int *cnt = reinterpret_cast<int *>(sum + 2 * kd);
+    e = cudaMemsetAsync(sum, 0, kd * 8, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, (size_t)k * 4, s);
+    if (e != cudaSuccess) return e;
+    fx_launch(X, ld, n, d, k, labels, scale, sum, cnt, nsm, smem, s);
+    const int nb = (int)((kd + 255) / 256);
+    // in place: each element's old value is read by the thread that writes it
+    fx_finalize_kernel<int><<<nb, 256, 0, s>>>(k, d, ld, sum, cnt, nullptr, nullptr, inv_scale,
+                                               C, C, counts, block_partials, scalars, flags,
+                                               ticket, ls, cond);
     return cudaGetLastError();
 }
 
@@ -841,7 +890,7 @@ cudaError_t launch_kmeans_finalize_shards(int k, int d, int ld, const long long 
     const int nb = (int)((kd + 255) / 256);
     fx_finalize_kernel<long long><<<nb, 256, 0, s>>>(
         k, d, ld, reinterpret_cast<const unsigned long long *>(acc), acc + kd, nullptr, nullptr,
-        inv_scale, C_prev, C_new, nullptr, block_partials, scalars, flags, ticket);
+        inv_scale, C_prev, C_new, nullptr, block_partials, scalars, flags, ticket, nullptr, 0ull);
     return cudaGetLastError();
 }
 

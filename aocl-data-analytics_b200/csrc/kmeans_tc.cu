@@ -540,8 +540,9 @@ kmeans_rescore_kernel(const float *X, int ld, int d, int dp, const float *C, int
                 }
             }
             const int lbl = (bi == 0x7fffffff) ? cj[0] : bi;
-            labels[r] = lbl;
+            // read before the write: labels may be labels_prev (in place)
             if (labels_prev && labels_prev[r] != lbl) changed = 1;
+            labels[r] = lbl;
         }
         unsigned full = __ballot_sync(0xffffffffu, nc == 0);
         while (full) {
@@ -601,8 +602,8 @@ kmeans_rescore_kernel(const float *X, int ld, int d, int dp, const float *C, int
             }
             if (lane == src) {
                 const int lbl = (bi == 0x7fffffff) ? 0 : bi;
-                labels[r] = lbl;
                 if (labels_prev && labels_prev[r] != lbl) changed = 1;
+                labels[r] = lbl;
             }
         }
     }
