@@ -34,7 +34,7 @@ using namespace tc;
 namespace {
 
 constexpr int TK_BM = 128;         // train rows per tile (UMMA M, TMEM lanes)
-constexpr int TK_BN = 256;         // queries per tile (UMMA N, TMEM columns)
+constexpr int TK_BN = 256;         // queries per tile (UMMA N, TMEM columns), at most
 constexpr int TK_KB = 64;          // bf16 elements per 128-byte K block
 constexpr int TK_THREADS = 320;    // TMA warp, MMA warp, 8 epilogue warps
 constexpr int TK_PRE_ROWS = 16384; // training rows of the threshold pre-pass (small batches;
@@ -47,12 +47,12 @@ constexpr int TK_FIN_MAX = 8192;   // candidates re-scored per query (more: fall
 struct KnnTcArgs {
     int nx, nq, k, nkb, stages, n_qtiles, n_xtiles, n_items, cap;
     const float *xnorm;   // nx: fp32 |x_j|^2
-    const float *margin;  // n_qtiles * TK_BN: 2 eps_q (nudged up)
-    unsigned *theta;      // n_qtiles * TK_BN: threshold, order-preserving bits
-    int *cnt;             // n_qtiles * TK_BN: entries appended
+    const float *margin;  // n_qtiles * BN: 2 eps_q (nudged up)
+    unsigned *theta;      // n_qtiles * BN: threshold, order-preserving bits
+    int *cnt;             // n_qtiles * BN: entries appended
     int2 *list;           // nq * cap: (value bits, train row)
-    float *best;          // n_qtiles * TK_BN * TK_BEST: smallest listed values so far
-    int *lock;            // n_qtiles * TK_BN: refresh of `best` in progress
+    float *best;          // n_qtiles * BN * TK_BEST: smallest listed values so far
+    int *lock;            // n_qtiles * BN: refresh of `best` in progress
     int *err;
 };
 
@@ -118,6 +118,9 @@ __device__ __forceinline__ void warp_sort512(float (&a)[16]) {
     }
 }
 
+// BN: queries per tile (UMMA N, TMEM columns per accumulator): 64, 128 or
+// 256, the smallest that holds a small batch (less tensor work per train tile).
+template <int BN>
 __global__ void __launch_bounds__(TK_THREADS, 1)
 knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
               const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
@@ -126,13 +129,13 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(tk_raw) + 1023) & ~uintptr_t(1023));
     const int S = a.stages, nkb = a.nkb;
-    constexpr uint32_t kB = TK_BN * 128u; // one K block of the query tile (32 KB)
+    constexpr uint32_t kB = BN * 128u; // one K block of the query tile
     constexpr uint32_t kA = TK_BM * 128u; // one K block of a train tile (16 KB)
     unsigned char *Bh = base;
     unsigned char *Bl = Bh + (size_t)nkb * kB;
     unsigned char *As = Bl + (size_t)nkb * kB; // S stages of (Ah, Al) for one K block
-    float *th_w = reinterpret_cast<float *>(As + (size_t)S * 2 * kA); // 8 warps x TK_BN
-    TkShared *sh = reinterpret_cast<TkShared *>(th_w + 8 * TK_BN);
+    float *th_w = reinterpret_cast<float *>(As + (size_t)S * 2 * kA); // 8 warps x BN
+    TkShared *sh = reinterpret_cast<TkShared *>(th_w + 8 * BN);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -150,7 +153,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
         fence_barrier_init();
     }
     if (warp == 1) {
-        tmem_alloc(&sh->tmem_base, 2u * TK_BN);
+        tmem_alloc(&sh->tmem_base, 2u * BN);
         tmem_relinquish();
     }
     tc_fence_before();
@@ -173,8 +176,8 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                 }
                 mbar_arrive_expect_tx(&sh->bfull, (uint32_t)(2 * nkb) * kB);
                 for (int kb = 0; kb < nkb; ++kb) {
-                    tma_load_2d(&tmBh, &sh->bfull, Bh + (size_t)kb * kB, kb * TK_KB, qt * TK_BN);
-                    tma_load_2d(&tmBl, &sh->bfull, Bl + (size_t)kb * kB, kb * TK_KB, qt * TK_BN);
+                    tma_load_2d(&tmBh, &sh->bfull, Bh + (size_t)kb * kB, kb * TK_KB, qt * BN);
+                    tma_load_2d(&tmBl, &sh->bfull, Bl + (size_t)kb * kB, kb * TK_KB, qt * BN);
                 }
                 const int x0 = xc * TK_CHUNK_TILES, x1 = min(a.n_xtiles, x0 + TK_CHUNK_TILES);
                 for (int xt = x0; ok && xt < x1; ++xt) {
@@ -203,7 +206,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
     } else if (warp == 1) {
         // ---------------------------------------------------- MMA issuer ----
         if (lane == 0) {
-            const uint32_t idesc = idesc_bf16_f32(TK_BM, TK_BN);
+            const uint32_t idesc = idesc_bf16_f32(TK_BM, BN);
             int us = 0, tc = 0, ii = 0;
             bool ok = true;
             for (int item = blockIdx.x; ok && item < a.n_items; item += gridDim.x, ++ii) {
@@ -220,7 +223,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                         ok = false;
                         break;
                     }
-                    const uint32_t tacc = tbase + (uint32_t)(b * TK_BN);
+                    const uint32_t tacc = tbase + (uint32_t)(b * BN);
                     uint32_t acc = 0;
                     for (int kb = 0; kb < nkb; ++kb, ++us) {
                         const int s = us % S;
@@ -265,7 +268,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
         const int e = warp - 2;
         const int g = e >> 2;     // accumulator buffer / tile parity
         const int q = warp & 3;   // TMEM lane quarter
-        float *thw = th_w + e * TK_BN;
+        float *thw = th_w + e * BN;
         const float inf = __int_as_float(0x7f800000);
         int tc = 0;
         bool ok = true;
@@ -277,9 +280,9 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                 const int b = g;
                 const int row = xt * TK_BM + q * 32 + lane;
                 const float xn = row < a.nx ? a.xnorm[row] : inf;
-                unsigned tb[TK_BN / 32];
+                unsigned tb[BN / 32];
 #pragma unroll
-                for (int u = 0; u < TK_BN / 32; ++u) tb[u] = a.theta[qt * TK_BN + u * 32 + lane];
+                for (int u = 0; u < BN / 32; ++u) tb[u] = a.theta[qt * BN + u * 32 + lane];
                 bool w = mbar_wait(&sh->tfull[b], (uint32_t)((tc >> 1) & 1));
                 if (!w) tk_raise(&sh->abort_flag, a.err, 16);
                 w = w && !*((volatile int *)&sh->abort_flag);
@@ -288,11 +291,11 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                     break;
                 }
 #pragma unroll
-                for (int u = 0; u < TK_BN / 32; ++u) thw[u * 32 + lane] = ord_float(tb[u]);
+                for (int u = 0; u < BN / 32; ++u) thw[u * 32 + lane] = ord_float(tb[u]);
                 __syncwarp();
                 tc_fence_after();
-                const uint32_t trow = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TK_BN);
-                for (int c = 0; c < TK_BN / 32; ++c) {
+                const uint32_t trow = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN);
+                for (int c = 0; c < BN / 32; ++c) {
                     float v[32];
                     tmem_ld32(trow + (uint32_t)(c * 32), v);
                     float m = inf;
@@ -313,12 +316,12 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                         if (lane == u) mymask = mk;
                     }
                     int mybase = 0;
-                    if (mymask) mybase = atomicAdd(&a.cnt[qt * TK_BN + c * 32 + lane], __popc(mymask));
+                    if (mymask) mybase = atomicAdd(&a.cnt[qt * BN + c * 32 + lane], __popc(mymask));
                     while (colbits) {
                         const int u = __ffs(colbits) - 1;
                         colbits &= colbits - 1;
                         const int col = c * 32 + u;
-                        const int gq = qt * TK_BN + col;
+                        const int gq = qt * BN + col;
                         const unsigned mask = __shfl_sync(0xffffffffu, mymask, u);
                         const int base0 = __shfl_sync(0xffffffffu, mybase, u);
                         const int nadd = __popc(mask);
@@ -390,7 +393,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        tmem_dealloc(tbase, 2u * TK_BN);
+        tmem_dealloc(tbase, 2u * BN);
     }
 }
 
@@ -569,9 +572,9 @@ __global__ void max_value_kernel(const float *v, int n, float *out) {
 }
 __global__ void sqrt_inplace_kernel(float *v) { *v = sqrtf(*v) * 1.0001f; }
 
-size_t tk_smem_bytes(int nkb, int stages) {
-    return 1024 + (size_t)nkb * 2 * TK_BN * 128 + (size_t)stages * 2 * TK_BM * 128 +
-           (size_t)8 * TK_BN * 4 + sizeof(TkShared) + 64;
+size_t tk_smem_bytes(int nkb, int stages, int bn = TK_BN) {
+    return 1024 + (size_t)nkb * 2 * bn * 128 + (size_t)stages * 2 * TK_BM * 128 +
+           (size_t)8 * bn * 4 + sizeof(TkShared) + 64;
 }
 
 } // namespace
@@ -603,7 +606,10 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
                           int *fallback, int *n_fallback, int *err, float *out_key,
                           int *out_idx, cudaStream_t s) {
     const int nkb = ldbf / TK_KB;
-    const int n_qtiles = (nq + TK_BN - 1) / TK_BN, nq_pad = n_qtiles * TK_BN;
+    // query tile width: small batches use a narrower MMA (the train rows are
+    // read once either way; the tensor work and the epilogue scale with it)
+    const int bn = nq <= 64 ? 64 : nq <= 128 ? 128 : TK_BN;
+    const int n_qtiles = (nq + bn - 1) / bn, nq_pad = n_qtiles * bn;
     const int n_xtiles = (nx + TK_BM - 1) / TK_BM;
     const int n_xchunks = (n_xtiles + TK_CHUNK_TILES - 1) / TK_CHUNK_TILES;
     const int cap = (int)knn_tc_list_cap();
@@ -667,13 +673,14 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     CUtensorMap mah, mal, mbh, mbl;
     if (!make_map_bf16_rows(&mah, Xh, nx, ldbf, TK_BM) ||
         !make_map_bf16_rows(&mal, Xl, nx, ldbf, TK_BM) ||
-        !make_map_bf16_rows(&mbh, Qh, nq_pad, ldbf, TK_BN) ||
-        !make_map_bf16_rows(&mbl, Ql, nq_pad, ldbf, TK_BN))
+        !make_map_bf16_rows(&mbh, Qh, nq_pad, ldbf, bn) ||
+        !make_map_bf16_rows(&mbl, Ql, nq_pad, ldbf, bn))
         return cudaErrorInvalidValue;
     int stages = 8;
-    while (stages > 2 && tk_smem_bytes(nkb, stages) > 225 * 1024) --stages;
-    const size_t smem = tk_smem_bytes(nkb, stages);
-    cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(knn_tc_kernel), smem);
+    while (stages > 2 && tk_smem_bytes(nkb, stages, bn) > 225 * 1024) --stages;
+    const size_t smem = tk_smem_bytes(nkb, stages, bn);
+    auto kern = bn == 64 ? knn_tc_kernel<64> : bn == 128 ? knn_tc_kernel<128> : knn_tc_kernel<TK_BN>;
+    cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(kern), smem);
     if (e != cudaSuccess) return e;
     KnnTcArgs a;
     a.nx = nx;
@@ -697,7 +704,7 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const int grid = std::min(nsm, a.n_items);
-    knn_tc_kernel<<<grid, TK_THREADS, smem, s>>>(mah, mal, mbh, mbl, a);
+    kern<<<grid, TK_THREADS, smem, s>>>(mah, mal, mbh, mbl, a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const size_t fsm = (size_t)TK_FIN_MAX * 8 + (size_t)d * sizeof(float);

@@ -30,7 +30,8 @@ KNN_OUT_BYTES = 256 * 8
 
 
 class Request:
-    __slots__ = ("kind", "queries", "k", "model", "t_submit", "t_done", "result", "_done")
+    __slots__ = ("kind", "queries", "k", "model", "t_submit", "t_start", "t_done", "result",
+                 "_done")
 
     def __init__(self, kind, queries, k=None, model=None):
         if kind not in ("knn", "predict"):
@@ -40,6 +41,7 @@ class Request:
         self.k = k
         self.model = model
         self.t_submit = None
+        self.t_start = None  # when a worker took it into a batch
         self.t_done = None
         self.result = None
         self._done = threading.Event()
@@ -128,6 +130,7 @@ class Server:
                 return None
             batch, nq = [], 0
             model = q[0].model
+            now = time.perf_counter()
             i = 0
             while i < len(q):
                 r = q[i]
@@ -137,6 +140,7 @@ class Server:
                     continue
                 if batch and (nq + m > cap_queries or (nq + m) * per_query_bytes > cap_bytes):
                     break
+                r.t_start = now
                 batch.append(r)
                 nq += m
                 del q[i]
@@ -193,11 +197,20 @@ class Server:
 
 
 def latency_summary(reqs):
-    lat = np.array([r.latency for r in reqs if r.latency is not None])
-    if lat.size == 0:
+    """p50 / p99 / max of submit-to-completion latency, and its two parts:
+    queueing (submit to the start of its batch) and service (batch start to
+    completion)."""
+    done = [r for r in reqs if r.latency is not None]
+    if not done:
         return {"requests": 0}
-    return {"requests": int(lat.size), "p50_ms": float(np.percentile(lat, 50) * 1e3),
-            "p99_ms": float(np.percentile(lat, 99) * 1e3), "max_ms": float(lat.max() * 1e3)}
+    lat = np.array([r.latency for r in done])
+    wait = np.array([r.t_start - r.t_submit for r in done])
+    serve = np.array([r.t_done - r.t_start for r in done])
+    ms = lambda a, q: float(np.percentile(a, q) * 1e3)  # noqa: E731
+    return {"requests": int(lat.size), "p50_ms": ms(lat, 50), "p99_ms": ms(lat, 99),
+            "max_ms": float(lat.max() * 1e3), "queue_p50_ms": ms(wait, 50),
+            "queue_p99_ms": ms(wait, 99), "service_p50_ms": ms(serve, 50),
+            "service_p99_ms": ms(serve, 99)}
 
 
 def replay(server, trace, rng_queries):

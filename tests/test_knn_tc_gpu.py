@@ -30,6 +30,9 @@ def run(ab, X, Q, k, metric, mode, order):
     (150_000, 300, 100, 10, "sqeuclidean", 0),
     (140_000, 1_025, 32, 1, "euclidean", 1),
     (130_000, 600, 64, 256, "euclidean", 0),
+    (300_000, 40, 64, 10, "euclidean", 0),       # 64-query tiles
+    (180_000, 100, 96, 100, "sqeuclidean", 0),   # 128-query tiles
+    (300_000, 1, 64, 1, "euclidean", 1),
 ])
 def test_knn_tc_equals_plain(gpu, ab, nx, nq, d, k, metric, order):
     rng = np.random.default_rng(nx + nq + d + k)
