@@ -3,10 +3,15 @@
 The training set of the kNN index and the centres of the k-means models stay
 in device memory for the life of the server (one library handle per worker).
 Requests -- a kNN search (queries, k) or a k-means predict (model, queries)
--- are queued as they arrive.  Each worker thread repeatedly takes the
-pending requests of its kind that fit its share of the device-memory budget
-and its query cap (continuous batching: requests that arrive while a batch
-runs join the next one) and serves them with ONE library call: for kNN the
+-- are queued as they arrive; a kNN request with more queries than one call
+takes is split into parts of at most that many (each part is searched on its
+own; the request completes with its last part).  Each worker thread
+repeatedly takes pending requests of its kind that fit its share of the
+device-memory budget and its query cap -- requests waiting longer than
+`aging_ms` first, then small ones (at most `small_queries` queries), then
+the rest, oldest first within each class -- (continuous batching: requests
+that arrive while a batch runs join the next one) and serves them with ONE
+library call: for kNN the
 queries are concatenated and searched with the largest k asked for; every
 request gets the prefix it asked for, which is exactly its own search because
 results are ordered by (distance, index).  Several kNN workers run their
@@ -31,7 +36,7 @@ KNN_OUT_BYTES = 256 * 8
 
 class Request:
     __slots__ = ("kind", "queries", "k", "model", "t_submit", "t_start", "t_done", "result",
-                 "_done")
+                 "_done", "parent", "offset", "parts_left")
 
     def __init__(self, kind, queries, k=None, model=None):
         if kind not in ("knn", "predict"):
@@ -45,6 +50,9 @@ class Request:
         self.t_done = None
         self.result = None
         self._done = threading.Event()
+        self.parent = None      # for a part: the request it belongs to
+        self.offset = 0         # for a part: its first query in the parent
+        self.parts_left = 0
 
     def wait(self, timeout=None):
         return self._done.wait(timeout)
@@ -60,8 +68,11 @@ class Server:
     kNN worker threads (one handle each) and one predict worker."""
 
     def __init__(self, ab, X, models=None, workers=2, max_batch_queries=1024,
-                 max_request_queries=4096, hbm_budget=16 << 30, precision_mode="bf16x3"):
+                 max_request_queries=4096, hbm_budget=16 << 30, precision_mode="bf16x3",
+                 small_queries=256, aging_ms=20.0):
         self.ab = ab
+        self.small_queries = small_queries
+        self.aging = aging_ms / 1e3
         self.X = np.ascontiguousarray(X, dtype=np.float32)
         self.d = self.X.shape[1]
         self.max_batch_queries = max_batch_queries
@@ -79,14 +90,22 @@ class Server:
             h.fit(self.X)
             # one call of the largest batch: the device copies and every
             # per-call buffer reach their final size now, so that no request
-            # waits for a device allocation (which also stalls other work)
+            # waits for a device allocation (which also stalls other work);
+            # then calls of the other shapes a request can take (query tile
+            # widths, k), so that every kernel they launch is loaded now
             warm = max(max_batch_queries, max_request_queries)
             h.kneighbors(self.X[np.arange(warm) % self.X.shape[0]], 256)
+            for nq in (1, 64, 128, 256, min(warm, 512)):
+                for kk in (1, 10, 100):
+                    h.kneighbors(self.X[np.arange(nq) % self.X.shape[0]], kk)
             self.knn_handles.append(h)
         self.models = {}
         for name, (Xm, C0) in (models or {}).items():
             km = ab.KMeans(C0.shape[0], "s", order=ab.ROW_MAJOR, max_iter=50, n_init=1)
             km.fit(Xm, C0)
+            # one predict of the largest request: its device buffers are
+            # allocated now (an allocation later would stall every stream)
+            km.predict(np.zeros((max_request_queries, Xm.shape[1]), dtype=np.float32))
             self.models[name] = km
         self.bytes_per_query = self.d * 4 + KNN_LIST_BYTES + KNN_OUT_BYTES
         self.threads = [threading.Thread(target=self._knn_worker, args=(w,), daemon=True)
@@ -102,8 +121,19 @@ class Server:
         if req.kind == "knn" and not (1 <= req.k <= 256):
             raise ValueError("k must be in [1, 256]")
         req.t_submit = time.perf_counter()
+        parts = [req]
+        nq = req.queries.shape[0]
+        if req.kind == "knn" and nq > self.max_batch_queries:
+            req.result = (np.empty((nq, req.k), dtype=np.int32),
+                          np.empty((nq, req.k), dtype=np.float32))
+            parts = []
+            for o in range(0, nq, self.max_batch_queries):
+                part = Request("knn", req.queries[o:o + self.max_batch_queries], k=req.k)
+                part.t_submit, part.parent, part.offset = req.t_submit, req, o
+                parts.append(part)
+            req.parts_left = len(parts)
         with self.cv:
-            self.pending[req.kind].append(req)
+            self.pending[req.kind].extend(parts)
             self.cv.notify_all()
         return req
 
@@ -128,32 +158,46 @@ class Server:
             q = self.pending[kind]
             if not q:
                 return None
-            batch, nq = [], 0
-            model = q[0].model
             now = time.perf_counter()
-            i = 0
-            while i < len(q):
-                r = q[i]
+            # aged requests, then small ones, then the rest (oldest first in each)
+            def rank(r):
+                aged = now - r.t_submit >= self.aging
+                return (not aged, r.queries.shape[0] > self.small_queries, r.t_submit)
+            order = sorted(q, key=rank)
+            model = order[0].model
+            batch, nq = [], 0
+            for r in order:
                 m = r.queries.shape[0]
                 if same_model and r.model != model:
-                    i += 1
                     continue
                 if batch and (nq + m > cap_queries or (nq + m) * per_query_bytes > cap_bytes):
                     break
                 r.t_start = now
                 batch.append(r)
                 nq += m
-                del q[i]
+            taken = set(map(id, batch))
+            self.pending[kind] = collections.deque(r for r in q if id(r) not in taken)
             return batch
 
     def _finish(self, kind, batch, nq, secs):
         t = time.perf_counter()
-        for r in batch:
-            r.t_done = t
-            r._done.set()
+        done = []
         with self.cv:
-            self.completed.extend(batch)
+            for r in batch:
+                p = r.parent
+                if p is None:
+                    r.t_done = t
+                    done.append(r)
+                    continue
+                p.t_start = r.t_start if p.t_start is None else min(p.t_start, r.t_start)
+                p.parts_left -= 1
+                if p.parts_left == 0:
+                    p.t_done = t
+                    done.append(p)
+            self.completed.extend(done)
             self.batches.append((kind, len(batch), nq, secs))
+        for r in done:
+            r._done.set()
 
     def _knn_worker(self, w):
         h = self.knn_handles[w]
@@ -174,7 +218,12 @@ class Server:
             o = 0
             for r in batch:
                 m = r.queries.shape[0]
-                r.result = (ind[o:o + m, :r.k].copy(), dist[o:o + m, :r.k].copy())
+                if r.parent is None:
+                    r.result = (ind[o:o + m, :r.k].copy(), dist[o:o + m, :r.k].copy())
+                else:  # a part: its rows of the parent's result
+                    pi, pd = r.parent.result
+                    pi[r.offset:r.offset + m] = ind[o:o + m, :r.k]
+                    pd[r.offset:r.offset + m] = dist[o:o + m, :r.k]
                 o += m
             self._finish("knn", batch, Q.shape[0], secs)
 

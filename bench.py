@@ -603,7 +603,9 @@ def run_serving(ab, nx=8_000_000, d=96, comps=2048, n_models=64, rates=(250.0, 1
     per-request query count lognormal(ln 16, 1.5) clipped to [1, 4096],
     k uniform in {1, 10, 100}, one request in five a predict on a random
     model.  Served by the continuous-batching loop (two kNN workers, at most
-    512 queries per library call); p50 / p99 latency (submit to completion)
+    512 queries per library call, larger requests split into parts, small and
+    long-waiting requests first), after 0.5 s of unmeasured traffic at the
+    same rate; p50 / p99 latency (submit to completion)
     and queries/s at 250, 1,000 and 2,000 requests/s for the tensor-core path,
     and at 250 requests/s for the plain fp32 path (which cannot keep up, so
     its queue grows)."""
@@ -642,6 +644,10 @@ def run_serving(ab, nx=8_000_000, d=96, comps=2048, n_models=64, rates=(250.0, 1
         server = sv.Server(ab, X, models=models, workers=2, max_batch_queries=512,
                            precision_mode=mode)
         for rate in mode_rates:
+            # half a second of the same traffic first (not measured): the
+            # measured trace starts from a serving steady state
+            sv.replay(server, make_trace(rate, np.random.default_rng(seed + 7 * int(rate)))[
+                : max(1, int(rate * 0.5))], queries)
             server.batches.clear()
             trace = make_trace(rate, np.random.default_rng(seed + int(rate)))
             t0 = time.perf_counter()
@@ -650,9 +656,15 @@ def run_serving(ab, nx=8_000_000, d=96, comps=2048, n_models=64, rates=(250.0, 1
             small = [r for r in reqs if r.queries.shape[0] <= 256]
             nq = sum(r.queries.shape[0] for r in reqs)
             kb = [b for b in server.batches if b[0] == "knn"]
+            pb = [b for b in server.batches if b[0] == "predict"]
             out[f"{mode}_{int(rate)}rps"] = {
                 "requests": len(reqs), "all": sv.latency_summary(reqs),
                 "requests_1_256_queries": sv.latency_summary(small),
+                "knn_1_256_queries": sv.latency_summary([r for r in small if r.kind == "knn"]),
+                "predict_1_256_queries": sv.latency_summary(
+                    [r for r in small if r.kind == "predict"]),
+                "predict_calls": len(pb),
+                "mean_predict_call_ms": float(np.mean([b[3] for b in pb]) * 1e3) if pb else 0.0,
                 "queries_per_s": nq / wall, "knn_calls": len(kb),
                 "mean_queries_per_knn_call": float(np.mean([b[2] for b in kb])) if kb else 0.0,
                 "mean_knn_call_ms": float(np.mean([b[3] for b in kb]) * 1e3) if kb else 0.0,

@@ -40,7 +40,7 @@ def test_knn_tc_equals_plain(gpu, ab, nx, nq, d, k, metric, order):
     dup = rng.integers(0, nx, nx // 100)       # 1% exact duplicates -> ties
     X[rng.integers(0, nx, dup.size)] = X[dup]
     Q = mixture(rng, nq, d, comps=64)
-    Q[:5] = X[:5]                               # queries that hit training rows
+    Q[:min(5, nq)] = X[:min(5, nq)]             # queries that hit training rows
     pi, pd, ptc, _ = run(ab, X, Q, k, metric, "plain", order)
     ti, td, ttc, fb = run(ab, X, Q, k, metric, "bf16x3", order)
     assert ptc == 0.0

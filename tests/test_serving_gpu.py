@@ -4,7 +4,7 @@ are batched together) and some paced, served by two kNN workers and a predict
 worker over device-resident data.  Every request's result must be exactly
 what the same request gives alone (its own library call on its own handle):
 a kNN request batched with others is searched with a larger k and gets the
-prefix it asked for."""
+prefix it asked for, and one larger than a call takes is served in parts."""
 import numpy as np
 import pytest
 
@@ -29,7 +29,8 @@ def test_serving_results_alone_and_in_the_mix(gpu, ab):
     for m in range(3):
         Xm = mixture(rng, 20_000, d, 32)
         models[f"m{m}"] = (Xm, Xm[rng.choice(Xm.shape[0], 32, replace=False)].copy())
-    server = sv.Server(ab, X, models=models, workers=2, max_batch_queries=1024)
+    # calls of at most 128 queries: the larger requests are split into parts
+    server = sv.Server(ab, X, models=models, workers=2, max_batch_queries=128)
     try:
         def queries(size):
             return mixture(rng, size, d, 128)
@@ -51,6 +52,7 @@ def test_serving_results_alone_and_in_the_mix(gpu, ab):
                 trace.append((t, "knn", size, int(rng.choice([1, 10, 100]))))
         reqs = sv.replay(server, trace, queries)
         assert all(r.result is not None for r in reqs)
+        assert any(r.kind == "knn" and r.queries.shape[0] > 128 for r in reqs)
         assert max(b[1] for b in server.batches if b[0] == "knn") > 1
         summary = sv.latency_summary(reqs)
         assert summary["requests"] == len(reqs)
