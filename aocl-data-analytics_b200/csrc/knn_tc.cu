@@ -43,6 +43,7 @@ constexpr int TK_BEST = 256;       // smallest listed values kept per query (>= 
 constexpr int TK_WIN = 128;        // list entries merged into them per refresh
 constexpr int TK_CHUNK_TILES = 64; // train tiles per work item
 constexpr int TK_FIN_MAX = 8192;   // candidates re-scored per query (more: fallback)
+constexpr int TK_STASH = 4;        // values below threshold held per lane before reserving
 
 struct KnnTcArgs {
     int nx, nq, k, nkb, stages, n_qtiles, n_xtiles, n_items, cap;
@@ -135,7 +136,9 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
     unsigned char *Bl = Bh + (size_t)nkb * kB;
     unsigned char *As = Bl + (size_t)nkb * kB; // S stages of (Ah, Al) for one K block
     float *th_w = reinterpret_cast<float *>(As + (size_t)S * 2 * kA); // 8 warps x BN
-    TkShared *sh = reinterpret_cast<TkShared *>(th_w + 8 * BN);
+    int *col_w = reinterpret_cast<int *>(th_w + 8 * BN);                // 8 warps x BN
+    int2 *stash_w = reinterpret_cast<int2 *>(col_w + 8 * BN); // 8 warps x 32 lanes x TK_STASH
+    TkShared *sh = reinterpret_cast<TkShared *>(stash_w + 8 * 32 * TK_STASH);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -152,6 +155,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
         sh->abort_flag = 0;
         fence_barrier_init();
     }
+    for (int i = threadIdx.x; i < 8 * BN; i += blockDim.x) col_w[i] = 0;
     if (warp == 1) {
         tmem_alloc(&sh->tmem_base, 2u * BN);
         tmem_relinquish();
@@ -269,7 +273,104 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
         const int g = e >> 2;     // accumulator buffer / tile parity
         const int q = warp & 3;   // TMEM lane quarter
         float *thw = th_w + e * BN;
+        int *colcnt = col_w + e * BN;                          // zero between flushes
+        int2 *stash = stash_w + (size_t)(e * 32 + lane) * TK_STASH; // (column, value bits)
+        int ns = 0;
         const float inf = __int_as_float(0x7f800000);
+        // Reserve list slots for the stashed values (one global atomic per
+        // query column, all columns at once), write them, and merge the list
+        // windows they complete into the queries' best values (threshold
+        // refresh).  Warp-cooperative; `row` is this lane's train row.
+        auto flush = [&](int qt_, int row_) {
+            if (!__any_sync(0xffffffffu, ns > 0)) return;
+            for (int i = 0; i < ns; ++i) {
+                const int col = stash[i].x & 0xFFFF;
+                const int rank = atomicAdd(&colcnt[col], 1);
+                stash[i].x = col | (rank << 16);
+            }
+            __syncwarp();
+            int nn[BN / 32], bb[BN / 32];
+#pragma unroll
+            for (int j = 0; j < BN / 32; ++j) {
+                const int col = j * 32 + lane;
+                nn[j] = colcnt[col];
+                bb[j] = nn[j] > 0 ? atomicAdd(&a.cnt[qt_ * BN + col], nn[j]) : 0;
+            }
+#pragma unroll
+            for (int j = 0; j < BN / 32; ++j) colcnt[j * 32 + lane] = bb[j];
+            __syncwarp();
+            for (int i = 0; i < ns; ++i) {
+                const int col = stash[i].x & 0xFFFF, rank = stash[i].x >> 16;
+                const int pos = colcnt[col] + rank;
+                if (pos < a.cap)
+                    a.list[(size_t)(qt_ * BN + col) * a.cap + pos] = make_int2(stash[i].y, row_);
+            }
+            ns = 0;
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < BN / 32; ++j) colcnt[j * 32 + lane] = 0;
+#pragma unroll
+            for (int j = 0; j < BN / 32; ++j) {
+                // Crossing a window boundary: merge the window before the one
+                // just completed (its entries have been written by now; one
+                // still in flight reads as +inf) into the query's smallest
+                // listed values, and lower theta to their k-th + 2 eps.  They
+                // are distinct listed rows, so their k-th is never below the
+                // global k-th.  One warp at a time per query (a refresh that
+                // finds another in progress is skipped: a later one catches up).
+                const int w_mine = ((bb[j] + nn[j]) / TK_WIN) * TK_WIN;
+                const bool cross = nn[j] > 0 && w_mine > bb[j] && w_mine >= 2 * TK_WIN &&
+                                   w_mine <= a.cap;
+                unsigned todo = __ballot_sync(0xffffffffu, cross);
+                while (todo) {
+                    const int src = __ffs(todo) - 1;
+                    todo &= todo - 1;
+                    const int col = j * 32 + src;
+                    const int gq = qt_ * BN + col;
+                    const int w_end = __shfl_sync(0xffffffffu, w_mine, src);
+                    __threadfence();
+                    // a short, bounded wait for the lock (its holder never
+                    // waits, so it is released within a refresh time)
+                    int got = 0;
+                    if (lane == 0)
+                        for (int t = 0; t < 256 && !got; ++t)
+                            got = atomicCAS(&a.lock[gq], 0, 1) == 0;
+                    got = __shfl_sync(0xffffffffu, got, 0);
+                    if (got) {
+                        __threadfence();
+                        float *bq = a.best + (size_t)gq * TK_BEST;
+                        const int2 *lw = a.list + (size_t)gq * a.cap + (w_end - 2 * TK_WIN);
+                        float s16[16];
+#pragma unroll
+                        for (int t = 0; t < 8; ++t) s16[t] = __ldcg(&bq[lane * 8 + t]);
+#pragma unroll
+                        for (int t = 0; t < 4; ++t)
+                            s16[8 + t] = __int_as_float(__ldcg(&lw[lane * 4 + t].x));
+#pragma unroll
+                        for (int t = 12; t < 16; ++t) s16[t] = __int_as_float(0x7f800000);
+                        warp_sort512(s16);
+                        if (lane < TK_BEST / 16) {
+#pragma unroll
+                            for (int t = 0; t < 16; ++t) __stcg(&bq[lane * 16 + t], s16[t]);
+                        }
+                        float kth = 0.f;
+#pragma unroll
+                        for (int t = 0; t < 16; ++t)
+                            if (t == (a.k - 1) % 16) kth = s16[t];
+                        kth = __shfl_sync(0xffffffffu, kth, (a.k - 1) / 16);
+                        const float thn = nudge_up(kth + a.margin[gq]);
+                        if (thn < thw[col] && lane == 0) {
+                            atomicMin(&a.theta[gq], ord_bits(thn));
+                            thw[col] = thn;
+                        }
+                        __threadfence();
+                        __syncwarp();
+                        if (lane == 0) atomicExch(&a.lock[gq], 0);
+                    }
+                    __syncwarp();
+                }
+            }
+        };
         int tc = 0;
         bool ok = true;
         for (int item = blockIdx.x; ok && item < a.n_items; item += gridDim.x) {
@@ -295,6 +396,9 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                 __syncwarp();
                 tc_fence_after();
                 const uint32_t trow = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN);
+                // pass over the tile: values below their query's threshold
+                // go to this lane's stash (column, value); the list slots are
+                // reserved per tile, after the accumulator is released
                 for (int c = 0; c < BN / 32; ++c) {
                     float v[32];
                     tmem_ld32(trow + (uint32_t)(c * 32), v);
@@ -303,89 +407,23 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                     for (int u = 0; u < 32; ++u)
                         m = fminf(m, __fadd_rn(v[u], xn) - thw[c * 32 + u]);
                     if (!__any_sync(0xffffffffu, m < 0.f)) continue;
-                    // rare: some values below their query's threshold.  First
-                    // the columns that have any (statically indexed, so v stays
-                    // in registers), and every such column's list slots reserved
-                    // at once (lane u reserves for column u).
-                    unsigned colbits = 0, mymask = 0;
+                    unsigned bits = 0;
 #pragma unroll
-                    for (int u = 0; u < 32; ++u) {
-                        const unsigned mk =
-                            __ballot_sync(0xffffffffu, __fadd_rn(v[u], xn) < thw[c * 32 + u]);
-                        colbits |= (mk ? 1u : 0u) << u;
-                        if (lane == u) mymask = mk;
-                    }
-                    int mybase = 0;
-                    if (mymask) mybase = atomicAdd(&a.cnt[qt * BN + c * 32 + lane], __popc(mymask));
-                    while (colbits) {
-                        const int u = __ffs(colbits) - 1;
-                        colbits &= colbits - 1;
-                        const int col = c * 32 + u;
-                        const int gq = qt * BN + col;
-                        const unsigned mask = __shfl_sync(0xffffffffu, mymask, u);
-                        const int base0 = __shfl_sync(0xffffffffu, mybase, u);
-                        const int nadd = __popc(mask);
-                        if ((mask >> lane) & 1u) {
-                            const float sv = __fadd_rn(pick32(v, u), xn);
-                            const int pos = base0 + __popc(mask & ((1u << lane) - 1u));
-                            if (pos < a.cap)
-                                a.list[(size_t)gq * a.cap + pos] = make_int2(__float_as_int(sv), row);
+                    for (int u = 0; u < 32; ++u)
+                        bits |= (__fadd_rn(v[u], xn) < thw[c * 32 + u] ? 1u : 0u) << u;
+                    while (__any_sync(0xffffffffu, bits != 0)) {
+                        while (bits && ns < TK_STASH) {
+                            const int u = __ffs(bits) - 1;
+                            bits &= bits - 1;
+                            stash[ns++] = make_int2(c * 32 + u, __float_as_int(__fadd_rn(pick32(v, u), xn)));
                         }
-                        // Crossing a window boundary: merge the window before the
-                        // one just completed (its entries have been written by
-                        // now; one still in flight reads as +inf) into the
-                        // query's smallest listed values, and lower theta to
-                        // their k-th + 2 eps.  They are distinct listed rows, so
-                        // their k-th is never below the global k-th.  One warp
-                        // at a time per query (a refresh that finds another in
-                        // progress is skipped: a later one catches up).
-                        const int w_end = ((base0 + nadd) / TK_WIN) * TK_WIN;
-                        if (w_end > base0 && w_end >= 2 * TK_WIN && w_end <= a.cap) {
-                            __syncwarp();
-                            // a short, bounded wait for the lock (its holder never
-                            // waits, so it is released within a refresh time)
-                            int got = 0;
-                            if (lane == 0)
-                                for (int t = 0; t < 256 && !got; ++t)
-                                    got = atomicCAS(&a.lock[gq], 0, 1) == 0;
-                            got = __shfl_sync(0xffffffffu, got, 0);
-                            if (got) {
-                                __threadfence();
-                                float *bq = a.best + (size_t)gq * TK_BEST;
-                                const int2 *lw = a.list + (size_t)gq * a.cap + (w_end - 2 * TK_WIN);
-                                float s16[16];
-#pragma unroll
-                                for (int t = 0; t < 8; ++t) s16[t] = __ldcg(&bq[lane * 8 + t]);
-#pragma unroll
-                                for (int t = 0; t < 4; ++t)
-                                    s16[8 + t] = __int_as_float(__ldcg(&lw[lane * 4 + t].x));
-#pragma unroll
-                                for (int t = 12; t < 16; ++t) s16[t] = __int_as_float(0x7f800000);
-                                warp_sort512(s16);
-                                if (lane < TK_BEST / 16) {
-#pragma unroll
-                                    for (int t = 0; t < 16; ++t) __stcg(&bq[lane * 16 + t], s16[t]);
-                                }
-                                float kth = 0.f;
-#pragma unroll
-                                for (int t = 0; t < 16; ++t)
-                                    if (t == (a.k - 1) % 16) kth = s16[t];
-                                kth = __shfl_sync(0xffffffffu, kth, (a.k - 1) / 16);
-                                const float thn = nudge_up(kth + a.margin[gq]);
-                                if (thn < thw[col] && lane == 0) {
-                                    atomicMin(&a.theta[gq], ord_bits(thn));
-                                    thw[col] = thn;
-                                }
-                                __threadfence();
-                                __syncwarp();
-                                if (lane == 0) atomicExch(&a.lock[gq], 0);
-                            }
-                            __syncwarp();
-                        }
+                        // some lane's stash is full: reserve and write now
+                        if (__any_sync(0xffffffffu, bits != 0)) flush(qt, row);
                     }
                 }
                 tc_fence_before();
                 mbar_arrive(&sh->tempty[b]);
+                flush(qt, row);
             }
         }
     }
@@ -574,7 +612,7 @@ __global__ void sqrt_inplace_kernel(float *v) { *v = sqrtf(*v) * 1.0001f; }
 
 size_t tk_smem_bytes(int nkb, int stages, int bn = TK_BN) {
     return 1024 + (size_t)nkb * 2 * bn * 128 + (size_t)stages * 2 * TK_BM * 128 +
-           (size_t)8 * bn * 4 + sizeof(TkShared) + 64;
+           (size_t)8 * bn * 4 * 2 + (size_t)8 * 32 * TK_STASH * 8 + sizeof(TkShared) + 64;
 }
 
 } // namespace
