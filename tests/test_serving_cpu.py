@@ -1,0 +1,128 @@
+"""The serving loop's host logic (aocl-data-analytics_b200/serving.py) on
+CPU, over a stand-in for the library binding that answers with numpy:
+requests larger than one call are split into parts and reassembled, kNN
+requests batched together each get their own k-prefix, predict requests are
+batched per model, and the latency summary splits queueing and service."""
+import os
+import threading
+import time
+
+import numpy as np
+
+from conftest import PKG, _load
+
+
+class FakeKNN:
+    def __init__(self, prec, order=None, **options):
+        self.calls = []
+
+    def fit(self, X):
+        self.X = np.asarray(X, dtype=np.float64)
+        return self
+
+    def kneighbors(self, Q, k):
+        self.calls.append(Q.shape[0])
+        d2 = ((np.asarray(Q, dtype=np.float64)[:, None, :] - self.X[None]) ** 2).sum(-1)
+        idx = np.broadcast_to(np.arange(self.X.shape[0]), d2.shape)
+        o = np.lexsort((idx, d2), axis=-1)[:, :k]
+        return o.astype(np.int32), np.sqrt(np.take_along_axis(d2, o, 1)).astype(np.float32)
+
+    def stat(self, name):
+        return 0.0
+
+    def close(self):
+        pass
+
+
+class FakeKMeans:
+    def __init__(self, k, prec, order=None, **options):
+        self.k = k
+
+    def fit(self, X, C0):
+        self.C = np.asarray(C0, dtype=np.float64)
+        return self
+
+    def predict(self, Q):
+        d2 = ((np.asarray(Q, dtype=np.float64)[:, None, :] - self.C[None]) ** 2).sum(-1)
+        return np.argmin(d2, axis=1).astype(np.int32)
+
+    def close(self):
+        pass
+
+
+class FakeAB:
+    ROW_MAJOR = 1
+    KNN = FakeKNN
+    KMeans = FakeKMeans
+
+
+def test_serving_split_batch_and_prefixes():
+    sv = _load("aoclda_serving_cpu", os.path.join(PKG, "serving.py"))
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((400, 5)).astype(np.float32)
+    Xm = rng.standard_normal((100, 5)).astype(np.float32)
+    models = {"m": (Xm, Xm[:7].copy())}
+    server = sv.Server(FakeAB(), X, models=models, workers=2, max_batch_queries=16,
+                       max_request_queries=64)
+    try:
+        reqs = []
+        for i, (size, k) in enumerate([(3, 1), (40, 10), (1, 100), (16, 7), (33, 256), (5, 2)]):
+            reqs.append(server.submit(sv.Request("knn", rng.standard_normal((size, 5)), k=k)))
+            if i % 2:
+                reqs.append(server.submit(sv.Request("predict", rng.standard_normal((size, 5)),
+                                                     model="m")))
+        for r in reqs:
+            assert r.wait(30)
+        ref_knn = FakeKNN("s").fit(X)
+        ref_km = FakeKMeans(7, "s").fit(Xm, Xm[:7])
+        for r in reqs:
+            assert r.t_submit <= r.t_start <= r.t_done
+            if r.kind == "knn":
+                ind, dist = ref_knn.kneighbors(r.queries, r.k)
+                np.testing.assert_array_equal(r.result[0], ind)
+                np.testing.assert_array_equal(r.result[1], dist)
+            else:
+                np.testing.assert_array_equal(r.result, ref_km.predict(r.queries))
+        # every kNN call stays within the cap; the 40- and 33-query
+        # requests were served in parts
+        assert max(b[2] for b in server.batches if b[0] == "knn") <= 16
+        assert sum(1 for b in server.batches if b[0] == "knn") >= 6
+        s = sv.latency_summary(reqs)
+        assert s["requests"] == len(reqs)
+        for key in ("p50_ms", "p99_ms", "queue_p99_ms", "service_p99_ms"):
+            assert s[key] >= 0.0
+    finally:
+        server.close()
+
+
+def test_serving_small_requests_first():
+    """With one worker held busy, a small request submitted after a large one
+    is taken first."""
+    sv = _load("aoclda_serving_cpu2", os.path.join(PKG, "serving.py"))
+    gate = threading.Event()
+
+    class SlowKNN(FakeKNN):
+        def kneighbors(self, Q, k):
+            if Q.shape[0] == 2:  # the blocking request
+                gate.wait(10)
+            return super().kneighbors(Q, k)
+
+    class AB(FakeAB):
+        KNN = SlowKNN
+
+    rng = np.random.default_rng(4)
+    X = rng.standard_normal((300, 4)).astype(np.float32)
+    server = sv.Server(AB(), X, workers=1, max_batch_queries=512, max_request_queries=512,
+                       small_queries=8, aging_ms=10_000.0)
+    try:
+        block = server.submit(sv.Request("knn", rng.standard_normal((2, 4)), k=1))
+        time.sleep(0.2)                        # the worker is now inside the blocking call
+        large = server.submit(sv.Request("knn", rng.standard_normal((300, 4)), k=1))
+        small = server.submit(sv.Request("knn", rng.standard_normal((5, 4)), k=1))
+        gate.set()
+        for r in (block, large, small):
+            assert r.wait(30)
+        assert small.t_start <= large.t_start
+    finally:
+        gate.set()
+        server.close()
