@@ -64,9 +64,10 @@ template <typename T> struct NN : public AlgBase {
     int ld = 0;
     DevBuf dX, dXn, dQ, dQn, dPartK, dPartI, dOutK, dOutI, dStage;
     int xn_kind = -1; // which norms dXn holds: 0 squared, 1 eps1-norm
-    // tensor-core candidate pass (fp32 euclidean): bf16 hi/lo copies of the
-    // training rows, their fp32 |x|^2 and max |x|; per-call query buffers
-    DevBuf dXh, dXl, dXsq, dTkScal, dTkQ, dTkList, dTkFlag;
+    // tensor-core candidate pass (fp32 euclidean, cosine): bf16 hi/lo copies
+    // of the training rows, their fp32 |x|^2 and max |x|, 1 / |x| (cosine);
+    // per-call query buffers
+    DevBuf dXh, dXl, dXsq, dTkScal, dTkQ, dTkList, dTkFlag, dXinv;
     bool tc_train_ready = false;
     int tc_ldbf = 0;
 
@@ -93,7 +94,8 @@ template <typename T> struct NN : public AlgBase {
     da_status ensure_device_data();
     da_status validate_queries(da_int nq, da_int d, const T *Xt, da_int ldt);
     // tensor-core path; `done` false when the plain path must run instead
-    da_status kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_sqrt, bool &done);
+    da_status kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_sqrt, bool cosine,
+                            bool &done);
     da_status compute_proba(da_int nq, da_int d, const T *Xt, da_int ldt, std::vector<T> &proba);
     da_status available_classes();
 };

@@ -100,7 +100,7 @@ int knn_tile_rows_train(bool fp64);
 int knn_max_k(bool fp64);
 
 // ---------------------------------------------- kNN tensor-core pass ---
-// fp32 euclidean / squared euclidean: bf16x3 tcgen05 candidate pass with a
+// fp32 euclidean / squared euclidean / cosine: bf16x3 tcgen05 candidate pass with a
 // certified threshold per query, exact re-score of the survivors in the plain
 // kernel's order.  Results (q-major, as launch_knn_merge) equal the plain
 // path's; queries the pass cannot certify are flagged in `fallback`
@@ -116,11 +116,18 @@ cudaError_t launch_results_scatter(const float *key, const int *ind, const int *
                                    float *out_key, int *out_idx, cudaStream_t s);
 cudaError_t launch_knn_tc_train_prep(const float *X, int ld, int nx, int d, void *Xh, void *Xl,
                                      int ldbf, float *xnorm2, float *xmax, cudaStream_t s);
+// Cosine distance instead (the plain path's value 1 - x.q / (|x| |q|)): the
+// plain path's norms of the training rows (xnorm) and of this batch's queries
+// (qnorm), and the reciprocals of the former (xinv, launch_recip).
+struct KnnTcCosine {
+    const float *xnorm, *xinv, *qnorm;
+};
+cudaError_t launch_recip(const float *v, int n, float *out, cudaStream_t s);
 cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const float *xnorm2,
                           const float *xmax, int nx, int ld, int ldbf, int d, const float *Q,
                           int nq, int k, int kc, int take_sqrt, void *qbuf, void *list,
                           int *fallback, int *n_fallback, int *err, float *out_key,
-                          int *out_idx, cudaStream_t s);
+                          int *out_idx, cudaStream_t s, const KnnTcCosine *cosine = nullptr);
 
 // ------------------------------------------------------------- k-means ---
 struct KmeansWork {

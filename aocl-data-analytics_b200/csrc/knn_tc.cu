@@ -119,9 +119,16 @@ __device__ __forceinline__ void warp_sort512(float (&a)[16]) {
     }
 }
 
+// The ranking value of a train row: squared euclidean |x|^2 - 2 x.q (xs =
+// |x|^2), or cosine -2 x.q / |x| with q normalised (xs = 1 / |x|), which is
+// 2 (cosine distance - 1).
+template <bool COS> __device__ __forceinline__ float tk_val(float v, float xs) {
+    return COS ? __fmul_rn(v, xs) : __fadd_rn(v, xs);
+}
+
 // BN: queries per tile (UMMA N, TMEM columns per accumulator): 64, 128 or
 // 256, the smallest that holds a small batch (less tensor work per train tile).
-template <int BN>
+template <int BN, bool COS>
 __global__ void __launch_bounds__(TK_THREADS, 1)
 knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
               const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
@@ -380,7 +387,8 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                 if ((tc & 1) != g) continue;
                 const int b = g;
                 const int row = xt * TK_BM + q * 32 + lane;
-                const float xn = row < a.nx ? a.xnorm[row] : inf;
+                // rows past the end never pass (+inf, or NaN for cosine)
+                const float xn = row < a.nx ? a.xnorm[row] : (COS ? __int_as_float(0x7fc00000) : inf);
                 unsigned tb[BN / 32];
 #pragma unroll
                 for (int u = 0; u < BN / 32; ++u) tb[u] = a.theta[qt * BN + u * 32 + lane];
@@ -405,17 +413,17 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                     float m = inf;
 #pragma unroll
                     for (int u = 0; u < 32; ++u)
-                        m = fminf(m, __fadd_rn(v[u], xn) - thw[c * 32 + u]);
+                        m = fminf(m, tk_val<COS>(v[u], xn) - thw[c * 32 + u]);
                     if (!__any_sync(0xffffffffu, m < 0.f)) continue;
                     unsigned bits = 0;
 #pragma unroll
                     for (int u = 0; u < 32; ++u)
-                        bits |= (__fadd_rn(v[u], xn) < thw[c * 32 + u] ? 1u : 0u) << u;
+                        bits |= (tk_val<COS>(v[u], xn) < thw[c * 32 + u] ? 1u : 0u) << u;
                     while (__any_sync(0xffffffffu, bits != 0)) {
                         while (bits && ns < TK_STASH) {
                             const int u = __ffs(bits) - 1;
                             bits &= bits - 1;
-                            stash[ns++] = make_int2(c * 32 + u, __float_as_int(__fadd_rn(pick32(v, u), xn)));
+                            stash[ns++] = make_int2(c * 32 + u, __float_as_int(tk_val<COS>(pick32(v, u), xn)));
                         }
                         // some lane's stash is full: reserve and write now
                         if (__any_sync(0xffffffffu, bits != 0)) flush(qt, row);
@@ -437,18 +445,21 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
 
 // -2q split into bf16 hi / lo (rows nq..nq_pad-1 zero), the query norms |q|
 // and the margins 2 eps_q; thresholds +inf (padded queries -inf), counts 0.
+// Cosine (qnorm: the plain path's query norms): -2 q / |q| instead, and the
+// margin 2 e1 for every query.
 __global__ void knn_tc_prep_queries(const float *Q, int ld, int nq, int d, int nq_pad, int ldo,
                                     __nv_bfloat16 *Qh, __nv_bfloat16 *Ql, float e1, float e2,
                                     const float *xmax, float *margin, unsigned *theta, int *cnt,
-                                    float *qsq) {
+                                    float *qsq, const float *qnorm) {
     const int qi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (qi >= nq_pad) return;
+    const float qinv = (qnorm && qi < nq) ? __frcp_rn(qnorm[qi]) : 1.f;
     float s = 0.f;
     for (int f = lane; f < ldo; f += 32) {
         const float x = (qi < nq && f < d) ? Q[(size_t)qi * ld + f] : 0.f;
         s = __fmaf_rn(x, x, s);
-        const float y = -2.f * x;
+        const float y = qnorm ? -2.f * __fmul_rn(x, qinv) : -2.f * x;
         const __nv_bfloat16 h = __float2bfloat16_rn(y);
         Qh[(size_t)qi * ldo + f] = h;
         Ql[(size_t)qi * ldo + f] = __float2bfloat16_rn(y - __bfloat162float(h));
@@ -457,8 +468,8 @@ __global__ void knn_tc_prep_queries(const float *Q, int ld, int nq, int d, int n
     for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
     if (lane == 0) {
         const float qn = sqrtf(s) * 1.0001f;
-        const float xm = *xmax;
-        const float eps = e1 * xm * qn + e2 * (xm * xm + qn * qn);
+        const float xm = qnorm ? 0.f : *xmax;
+        const float eps = qnorm ? e1 : e1 * xm * qn + e2 * (xm * xm + qn * qn);
         margin[qi] = nudge_up(2.f * eps);
         theta[qi] = qi < nq ? ord_bits(__int_as_float(0x7f800000)) : ord_bits(-__int_as_float(0x7f800000));
         cnt[qi] = 0;
@@ -470,12 +481,14 @@ __global__ void knn_tc_prep_queries(const float *Q, int ld, int nq, int d, int n
 // subset of the rows; theta_q = p - |q|^2 + 4 eps_q >= v'_tc(k) + 2 eps_q
 // (k rows with plain value <= p have v'_tc <= p - |q|^2 + eps_q; the fp32
 // |q|^2 is within eps_q of |q|^2).
+// Cosine: p is a plain cosine distance and theta_q = 2 (p - 1) + 4 eps.
 __global__ void knn_tc_init_theta(const float *pre_key, int k, int nq, const float *qsq,
-                                  const float *margin, unsigned *theta) {
+                                  const float *margin, unsigned *theta, int cosm) {
     const int qi = blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= nq) return;
     const float pk = pre_key[(size_t)qi * k + (k - 1)];
-    const float t = nudge_up(pk - qsq[qi] + 2.f * margin[qi]);
+    const float t = cosm ? nudge_up(2.f * (pk - 1.f) + 2.f * margin[qi])
+                         : nudge_up(pk - qsq[qi] + 2.f * margin[qi]);
     if (t == t) theta[qi] = ord_bits(t);
 }
 
@@ -519,10 +532,20 @@ __device__ __forceinline__ float sqeuc_ref(const float *x, const float *q, int d
 // distances, sorted by (distance, index); the first k are written (sqrt for
 // euclidean).  A query whose list overflowed, or with more than TK_FIN_MAX
 // survivors, is flagged for the plain path (*n_fallback).
+// The plain path's cosine distance 1 - g / (|x| |q|), g one sequential fma
+// chain over the features, the norms the plain path's.
+__device__ __forceinline__ float cos_ref(const float *x, const float *q, int d, float xn,
+                                         float qn) {
+    float g = 0.f;
+    for (int f = 0; f < d; ++f) g = __fmaf_rn(x[f], q[f], g);
+    return __fsub_rn(1.f, __fdiv_rn(g, __fmul_rn(xn, qn)));
+}
+
 __global__ void __launch_bounds__(256)
 knn_tc_finalize(const float *X, const float *Q, int ld, int d, int kc, int k, int cap,
                 const unsigned *theta, const int *cnt, const int2 *list, int take_sqrt,
-                float *out_key, int *out_idx, int *fallback, int *n_fallback) {
+                float *out_key, int *out_idx, int *fallback, int *n_fallback,
+                const float *xnp, const float *qnp) {
     __shared__ int scount;
     extern __shared__ __align__(16) float fin_smem[];
     float *skey = fin_smem;                                  // TK_FIN_MAX
@@ -565,7 +588,8 @@ knn_tc_finalize(const float *X, const float *Q, int ld, int d, int kc, int k, in
     while (np2 < m) np2 <<= 1;
     for (int e = threadIdx.x; e < np2; e += blockDim.x) {
         if (e < m) {
-            skey[e] = sqeuc_ref(X + (size_t)sidx[e] * ld, qs, d, kc);
+            skey[e] = xnp ? cos_ref(X + (size_t)sidx[e] * ld, qs, d, xnp[sidx[e]], qnp[qi])
+                          : sqeuc_ref(X + (size_t)sidx[e] * ld, qs, d, kc);
         } else {
             skey[e] = __int_as_float(0x7f800000);
             sidx[e] = 0x7fffffff;
@@ -625,6 +649,16 @@ int knn_tc_supported(int nx, int d, int k) {
 
 size_t knn_tc_list_cap() { return 16384; }
 
+__global__ void recip_kernel(const float *v, int n, float *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = __frcp_rn(v[i]);
+}
+cudaError_t launch_recip(const float *v, int n, float *out, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    recip_kernel<<<(n + 255) / 256, 256, 0, s>>>(v, n, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_knn_tc_train_prep(const float *X, int ld, int nx, int d, void *Xh, void *Xl,
                                      int ldbf, float *xnorm2, float *xmax, cudaStream_t s) {
     cudaError_t e = launch_split_bf16(X, ld, nx, d, Xh, Xl, ldbf, s);
@@ -642,7 +676,7 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
                           const float *xmax, int nx, int ld, int ldbf, int d, const float *Q,
                           int nq, int k, int kc, int take_sqrt, void *qbuf, void *list,
                           int *fallback, int *n_fallback, int *err, float *out_key,
-                          int *out_idx, cudaStream_t s) {
+                          int *out_idx, cudaStream_t s, const KnnTcCosine *cosine) {
     const int nkb = ldbf / TK_KB;
     // query tile width: small batches use a narrower MMA (the train rows are
     // read once either way; the tensor work and the epilogue scale with it)
@@ -672,10 +706,19 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     const double e1 = 1.1 * (3.1 * std::ldexp(1.0, -16) * 2.0 + 2.0 * ktot * u * 2.0 + 2.0 * u +
                              (d + 4.0) * u * 2.0);
     const double e2 = 1.1 * ((kp + 2.0) * u + (d + 4.0) * u * 2.0 + 2.0 * u);
+    // cosine, r = -2 x.q / (|x| |q|) = 2 (distance - 1), |x|, |q| the plain
+    // path's norms: bf16 hi/lo split and fp32 accumulation as above on unit-
+    // scale products, the scalings by 1/|q| and 1/|x| (4 u), and twice the
+    // plain distance's own error (d fma terms, the product, division and
+    // subtraction: (d + 6) u)
+    const double ec = 1.1 * (2.0 * (3.1 * std::ldexp(1.0, -16) + 2.0 * ktot * u + 4.0 * u) +
+                             2.0 * (d + 6.0) * u);
+    const bool cosm = cosine != nullptr;
     {
         const int wpb = 8;
         knn_tc_prep_queries<<<(nq_pad + wpb - 1) / wpb, wpb * 32, 0, s>>>(
-            Q, ld, nq, d, nq_pad, ldbf, Qh, Ql, (float)e1, (float)e2, xmax, margin, theta, cnt, qsq);
+            Q, ld, nq, d, nq_pad, ldbf, Qh, Ql, (float)(cosm ? ec : e1), (float)e2, xmax, margin,
+            theta, cnt, qsq, cosm ? cosine->qnorm : nullptr);
         // exact pre-pass over the first training rows (plain kernels; its
         // partial lists live in the candidate list buffer, its merged keys in
         // the output arrays, both overwritten below)
@@ -687,15 +730,19 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
             int n_chunks = std::max(1, std::min((pre + BN - 1) / BN, 16));
             int chunk_rows = ((pre + n_chunks - 1) / n_chunks + BN - 1) / BN * BN;
             n_chunks = (pre + chunk_rows - 1) / chunk_rows;
-            KnnArgs pa{ACC_SQEUC, POST_NONE, kc, 2.0, k, chunk_rows, n_chunks};
+            KnnArgs pa{cosm ? ACC_DOT : ACC_SQEUC, cosm ? POST_COSINE : POST_NONE, kc, 2.0, k,
+                       chunk_rows, n_chunks};
             float *pk = static_cast<float *>(list);
             int *pi = reinterpret_cast<int *>(pk + (size_t)nq * n_chunks * k);
-            cudaError_t e = launch_knn_chunks<float>(Q, ld, nq, X, ld, pre, d, nullptr, nullptr, pa,
-                                                     pk, pi, nullptr, s);
+            cudaError_t e = launch_knn_chunks<float>(Q, ld, nq, X, ld, pre, d,
+                                                     cosm ? cosine->qnorm : nullptr,
+                                                     cosm ? cosine->xnorm : nullptr, pa, pk, pi,
+                                                     nullptr, s);
             if (e == cudaSuccess)
                 e = launch_knn_merge<float>(pk, pi, nq, n_chunks, k, 0, out_key, out_idx, s);
             if (e != cudaSuccess) return e;
-            knn_tc_init_theta<<<(nq + 255) / 256, 256, 0, s>>>(out_key, k, nq, qsq, margin, theta);
+            knn_tc_init_theta<<<(nq + 255) / 256, 256, 0, s>>>(out_key, k, nq, qsq, margin, theta,
+                                                               cosm ? 1 : 0);
         }
         const size_t nl = (size_t)nq * cap;
         knn_tc_fill_list<<<(unsigned)((nl + 255) / 256), 256, 0, s>>>(static_cast<int2 *>(list), nl);
@@ -717,7 +764,10 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     int stages = 8;
     while (stages > 2 && tk_smem_bytes(nkb, stages, bn) > 225 * 1024) --stages;
     const size_t smem = tk_smem_bytes(nkb, stages, bn);
-    auto kern = bn == 64 ? knn_tc_kernel<64> : bn == 128 ? knn_tc_kernel<128> : knn_tc_kernel<TK_BN>;
+    auto kern = cosm ? (bn == 64 ? knn_tc_kernel<64, true> : bn == 128 ? knn_tc_kernel<128, true>
+                                                                       : knn_tc_kernel<TK_BN, true>)
+                     : (bn == 64 ? knn_tc_kernel<64, false> : bn == 128 ? knn_tc_kernel<128, false>
+                                                                        : knn_tc_kernel<TK_BN, false>);
     cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(kern), smem);
     if (e != cudaSuccess) return e;
     KnnTcArgs a;
@@ -730,7 +780,7 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     a.n_xtiles = n_xtiles;
     a.n_items = n_qtiles * n_xchunks;
     a.cap = cap;
-    a.xnorm = xnorm2;
+    a.xnorm = cosm ? cosine->xinv : xnorm2;
     a.margin = margin;
     a.theta = theta;
     a.cnt = cnt;
@@ -749,8 +799,9 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     e = ensure_smem_limit(reinterpret_cast<const void *>(knn_tc_finalize), fsm);
     if (e != cudaSuccess) return e;
     knn_tc_finalize<<<nq, 256, fsm, s>>>(
-        X, Q, ld, d, kc, k, cap, theta, cnt, static_cast<const int2 *>(list), take_sqrt, out_key,
-        out_idx, fallback, n_fallback);
+        X, Q, ld, d, kc, k, cap, theta, cnt, static_cast<const int2 *>(list),
+        cosm ? 0 : take_sqrt, out_key, out_idx, fallback, n_fallback,
+        cosm ? cosine->xnorm : nullptr, cosm ? cosine->qnorm : nullptr);
     return cudaGetLastError();
 }
 

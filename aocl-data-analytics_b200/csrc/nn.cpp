@@ -154,10 +154,26 @@ template <typename T> da_status NN<T>::ensure_device_data() {
 // pass could not certify sends the whole call to the plain path (done =
 // false).
 template <typename T>
-da_status NN<T>::kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_sqrt, bool &done) {
+da_status NN<T>::kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_sqrt,
+                                bool cosine, bool &done) {
     done = false;
     if constexpr (std::is_same_v<T, float>) {
         cudaStream_t st = cuda->stream;
+        if (cosine) {
+            // the plain path's norms of the training rows and queries, and the
+            // reciprocals of the former
+            if (!dQn.ensure((size_t)nq * sizeof(T)) || !dXn.ensure((size_t)n_samples * sizeof(T)) ||
+                !dXinv.ensure((size_t)n_samples * sizeof(float)))
+                return err->error(da_status_memory_error, "Device memory allocation failed.");
+            B200_TRY(launch_row_norms_eps1<float>(dQ.as<float>(), ld, (int)nq, (int)d,
+                                                  dQn.as<float>(), st), "norms");
+            if (xn_kind != 1)
+                B200_TRY(launch_row_norms_eps1<float>(dX.as<float>(), ld, (int)n_samples, (int)d,
+                                                      dXn.as<float>(), st), "norms");
+            xn_kind = 1;
+            B200_TRY(launch_recip(dXn.as<float>(), (int)n_samples, dXinv.as<float>(), st),
+                     "norms");
+        }
         const int nkb = (int)((d + 63) / 64);
         if (!tc_train_ready || tc_ldbf != nkb * 64) {
             tc_ldbf = nkb * 64;
@@ -184,13 +200,16 @@ da_status NN<T>::kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_
         int h_state[5] = {0, 0, 0, 0, 0};
         for (da_int q0 = 0; q0 < nq; q0 += QB) {
             const da_int nb = std::min(QB, nq - q0);
+            const KnnTcCosine cs{dXn.as<float>(), dXinv.as<float>(),
+                                 cosine ? dQn.as<float>() + q0 : nullptr};
             B200_TRY(cuda->timed("knn_tc", [&] {
                 return launch_knn_tc(dX.as<float>(), dXh.p, dXl.p, dXsq.as<float>(),
                                      dTkScal.as<float>(), (int)n_samples, ld, tc_ldbf, (int)d,
                                      dQ.as<float>() + (size_t)q0 * ld, (int)nb, (int)k, kc,
                                      take_sqrt ? 1 : 0, dTkQ.p, dTkList.p, dTkFlag.as<int>(),
                                      n_fb, errf, dOutK.as<float>() + (size_t)q0 * k,
-                                     dOutI.as<int>() + (size_t)q0 * k, st);
+                                     dOutI.as<int>() + (size_t)q0 * k, st,
+                                     cosine ? &cs : nullptr);
             }), "kNN tensor-core pass");
             B200_TRY(cudaMemcpyAsync(h_state, n_fb, 5 * sizeof(int), cudaMemcpyDeviceToHost, st),
                      "copy");
@@ -237,7 +256,7 @@ da_status NN<T>::kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_
                 // scratch inside the (now free) candidate-list buffer
                 const size_t parts = (size_t)m * n_chunks * k;
                 const size_t need = (size_t)m * 4 + (size_t)m * ld * 4 + parts * 8 +
-                                    (size_t)m * k * 8 + 1024;
+                                    (size_t)m * k * 8 + (size_t)m * 4 + 1280;
                 if (!dTkList.ensure(need))
                     return err->error(da_status_memory_error, "Device memory allocation failed.");
                 char *p = dTkList.as<char>();
@@ -247,16 +266,24 @@ da_status NN<T>::kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_
                 int *pi = reinterpret_cast<int *>(pk + parts);
                 float *ok = reinterpret_cast<float *>(pi + parts);
                 int *oi = reinterpret_cast<int *>(ok + (size_t)m * k);
-                KnnArgs pa{ACC_SQEUC, POST_NONE, kc, 2.0, (int)k, chunk_rows, n_chunks};
+                float *qnsub = reinterpret_cast<float *>(oi + (size_t)m * k);
+                KnnArgs pa{cosine ? ACC_DOT : ACC_SQEUC, cosine ? POST_COSINE : POST_NONE, kc, 2.0,
+                           (int)k, chunk_rows, n_chunks};
                 B200_TRY(cudaMemcpyAsync(didx, idx.data(), (size_t)m * 4, cudaMemcpyHostToDevice,
                                          st), "copy");
                 B200_TRY(launch_rows_gather(dQ.as<float>() + (size_t)q0 * ld, ld, didx, m, qsub,
                                             st), "gather");
+                if (cosine)
+                    B200_TRY(launch_rows_gather(dQn.as<float>() + q0, 1, didx, m, qnsub, st),
+                             "gather");
                 B200_TRY(launch_knn_chunks<float>(qsub, ld, m, dX.as<float>(), ld,
-                                                  (int)n_samples, (int)d, nullptr, nullptr, pa, pk,
+                                                  (int)n_samples, (int)d,
+                                                  cosine ? qnsub : nullptr,
+                                                  cosine ? dXn.as<float>() : nullptr, pa, pk,
                                                   pi, nullptr, st), "kNN distance kernel");
-                B200_TRY(launch_knn_merge<float>(pk, pi, m, n_chunks, (int)k, take_sqrt ? 1 : 0,
-                                                 ok, oi, st), "kNN merge kernel");
+                B200_TRY(launch_knn_merge<float>(pk, pi, m, n_chunks, (int)k,
+                                                 take_sqrt && !cosine ? 1 : 0, ok, oi, st),
+                         "kNN merge kernel");
                 B200_TRY(launch_results_scatter(ok, oi, didx, m, (int)k,
                                                 dOutK.as<float>() + (size_t)q0 * k,
                                                 dOutI.as<int>() + (size_t)q0 * k, st), "scatter");
@@ -271,6 +298,7 @@ da_status NN<T>::kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_
         (void)k;
         (void)kc;
         (void)take_sqrt;
+        (void)cosine;
     }
     return da_status_success;
 }
@@ -357,12 +385,13 @@ da_status NN<T>::kneighbors_compute(da_int nq, da_int d, const T *Xt, da_int ldt
     cuda->stats["knn_tc_fallback_many_survivors"] = 0.0;
     cuda->stats["knn_tc_fallback_few_survivors"] = 0.0;
     bool tc_done = false;
-    const bool tc_metric =
-        metric == M_EUC || metric == M_SQEUC || (metric == M_MINK && p == T(2));
+    const bool tc_metric = metric == M_EUC || metric == M_SQEUC || metric == M_COS ||
+                           (metric == M_MINK && p == T(2));
     if (!fp64 && tc_metric && opts.key("precision mode") != 0 &&
         knn_tc_supported((int)n_samples, (int)d, (int)k) && n_samples >= 65536 &&
         (double)n_samples * (double)std::max<da_int>(nq, 256) * (double)d >= 4.0e9) {
-        s = kneighbors_tc(nq, d, k, kc, metric != M_SQEUC, tc_done);
+        s = kneighbors_tc(nq, d, k, kc, metric != M_SQEUC && metric != M_COS, metric == M_COS,
+                          tc_done);
         if (s != da_status_success) return s;
     }
     if (!tc_done) {

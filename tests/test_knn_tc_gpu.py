@@ -1,5 +1,6 @@
 """The tensor-core kNN path (bf16x3 candidate pass with a certified per-query
-threshold, exact re-score) against the plain fp32 SIMT path on the same data:
+threshold, exact re-score; euclidean, squared euclidean and cosine) against
+the plain fp32 SIMT path on the same data:
 neighbour indices and distances must be identical (bit for bit), including
 rows duplicated to force exact ties.  Sizes are large enough that the
 library chooses the tensor-core pass (it reports it through the
@@ -33,6 +34,8 @@ def run(ab, X, Q, k, metric, mode, order):
     (300_000, 40, 64, 10, "euclidean", 0),       # 64-query tiles
     (180_000, 100, 96, 100, "sqeuclidean", 0),   # 128-query tiles
     (300_000, 1, 64, 1, "euclidean", 1),
+    (200_000, 700, 128, 100, "cosine", 0),
+    (300_000, 40, 64, 10, "cosine", 1),
 ])
 def test_knn_tc_equals_plain(gpu, ab, nx, nq, d, k, metric, order):
     rng = np.random.default_rng(nx + nq + d + k)
