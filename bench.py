@@ -544,14 +544,16 @@ def run_sharded(ab, args, rank, world, local):
     return 0
 
 
-def run_knn(ab, nx=4_000_000, nq=10_000, d=128, k=100, comps=1024, seed=3, reps=3, plain=True):
-    """Brute-force kNN, fp32 euclidean: 4,000,000 x 128 training rows from a
-    1,024-component Gaussian mixture (the k-means recipe) plus 1% exact
-    duplicate rows (ties), 10,000 queries from the same mixture, k = 100.
-    Each timed call is one da_nn_kneighbors_s over all queries with host
+def run_knn(ab, nx=4_000_000, nq=10_000, d=128, k=100, comps=1024, seed=3, reps=3, plain=True,
+            metrics=("euclidean", "cosine")):
+    """Brute-force kNN, fp32 euclidean and cosine: 4,000,000 x 128 training
+    rows from a 1,024-component Gaussian mixture (the k-means recipe) plus 1%
+    exact duplicate rows (ties), 10,000 queries from the same mixture, k =
+    100.  Each timed call is one da_nn_kneighbors_s over all queries with host
     arrays (queries up, indices and distances down).  The tensor-core path
     (bf16x3 candidate pass + exact re-score) and the plain fp32 path must
-    return identical indices and distances."""
+    return identical indices and distances.  The top-level keys are the
+    euclidean results; the cosine ones are under "cosine"."""
     rng = np.random.default_rng(seed)
     means = rng.uniform(-10.0, 10.0, (comps, d)).astype(np.float32)
     sig = rng.uniform(0.5, 2.0, comps).astype(np.float32)
@@ -561,27 +563,31 @@ def run_knn(ab, nx=4_000_000, nq=10_000, d=128, k=100, comps=1024, seed=3, reps=
     X = np.concatenate([X, X[rng.integers(0, nx, nx // 100)]])
     ql = rng.choice(comps, nq, p=w)
     Q = means[ql] + rng.standard_normal((nq, d), dtype=np.float32) * sig[ql, None]
-    res = {}
-    for mode in ("bf16x3", "plain") if plain else ("bf16x3",):
-        nn = ab.KNN("s", order=ab.ROW_MAJOR, metric="euclidean", precision_mode=mode).fit(X)
-        nn.kneighbors(Q[:512], k)
-        nn.L.da_b200_set_kernel_timing(nn.h, 1)
-        ts = []
-        for _ in range(reps if mode == "bf16x3" else 1):
-            t = time.perf_counter()
-            ind, dist = nn.kneighbors(Q, k)
-            ts.append(time.perf_counter() - t)
-        kern = {}
-        for name in ("knn_tc", "knn_chunks", "knn_merge"):
-            ms_, n_ = nn.kernel_time(name)
-            if n_:
-                kern[name] = ms_ / n_
-        res[mode] = {"s": min(ts), "ind": ind, "dist": dist, "tc": nn.stat("tensor_core"),
-                     "kernel_ms": kern, "list_mean": nn.stat("knn_tc_mean_list")}
-        nn.close()
-    tc, pl = res["bf16x3"], res.get("plain")
-    flops = 2.0 * (nx + nx // 100) * nq * d
-    return {"workload": f"knn_fp32_euclidean_{nx + nx // 100}x{d}_q{nq}_k{k}",
+    out = {}
+    for metric in metrics:
+        res = {}
+        for mode in ("bf16x3", "plain") if plain else ("bf16x3",):
+            nn = ab.KNN("s", order=ab.ROW_MAJOR, metric=metric, precision_mode=mode).fit(X)
+            nn.kneighbors(Q[:512], k)
+            nn.L.da_b200_set_kernel_timing(nn.h, 1)
+            ts = []
+            for _ in range(reps if mode == "bf16x3" else 1):
+                t = time.perf_counter()
+                ind, dist = nn.kneighbors(Q, k)
+                ts.append(time.perf_counter() - t)
+            kern = {}
+            for name in ("knn_tc", "knn_chunks", "knn_merge"):
+                ms_, n_ = nn.kernel_time(name)
+                if n_:
+                    kern[name] = ms_ / n_
+            res[mode] = {"s": min(ts), "ind": ind, "dist": dist, "tc": nn.stat("tensor_core"),
+                         "kernel_ms": kern, "list_mean": nn.stat("knn_tc_mean_list"),
+                         "fallback": nn.stat("knn_tc_fallback_queries")}
+            nn.close()
+        tc, pl = res["bf16x3"], res.get("plain")
+        flops = 2.0 * (nx + nx // 100) * nq * d
+        out[metric] = {
+            "workload": f"knn_fp32_{metric}_{nx + nx // 100}x{d}_q{nq}_k{k}",
             "unit": "queries/s", "qps": nq / tc["s"],
             "plain_qps": nq / pl["s"] if pl else None,
             "speedup_vs_plain_fp32": pl["s"] / tc["s"] if pl else None,
@@ -589,9 +595,12 @@ def run_knn(ab, nx=4_000_000, nq=10_000, d=128, k=100, comps=1024, seed=3, reps=
                                        np.array_equal(tc["dist"], pl["dist"])) if pl else None,
             "tensor_core": tc["tc"] == 1.0, "kernel_ms": tc["kernel_ms"],
             "plain_kernel_ms": pl["kernel_ms"] if pl else None,
-            "tensor_tflops_algorithmic": flops / (tc["kernel_ms"].get("knn_tc", float("nan")) / 1e3) / 1e12,
-            "candidate_list_mean": tc["list_mean"],
+            "tensor_tflops_algorithmic":
+                flops / (tc["kernel_ms"].get("knn_tc", float("nan")) / 1e3) / 1e12,
+            "candidate_list_mean": tc["list_mean"], "plain_fallback_queries": tc["fallback"],
             "timing": "wall clock of one da_nn_kneighbors_s call with host arrays (best of 3)"}
+    first = out[metrics[0]]
+    return dict(first, **{m: out[m] for m in metrics[1:]})
 
 
 def run_serving(ab, nx=8_000_000, d=96, comps=2048, n_models=64, rates=(250.0, 1000.0, 2000.0),
