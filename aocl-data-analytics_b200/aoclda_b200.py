@@ -99,6 +99,8 @@ def load(path=LIB_PATH):
         "da_b200_get_stat": (_P, C.c_char_p, C.POINTER(C.c_double)),
         "da_b200_kmeans_init_centres_d": (_P, _P, da_int),
         "da_b200_kmeans_init_centres_s": (_P, _P, da_int),
+        "da_handle_save_model": (_P, C.c_char_p),
+        "da_handle_load_model": (h, C.c_char_p),
         "da_b200_kmeans_shard_colmax_s": (_P, _P),
         "da_b200_kmeans_shard_begin_s": (_P, _P, da_int, _P),
         "da_b200_kmeans_shard_partial_s": (_P, _P),
@@ -152,6 +154,25 @@ class Handle:
     def close(self):
         if self.h:
             self.L.da_handle_destroy(C.byref(self.h))
+
+    def save_model(self, path):
+        """da_handle_save_model: options and trained state to a file."""
+        return self.call("da_handle_save_model", str(path).encode())
+
+    @classmethod
+    def load_model(cls, path, prec):
+        """da_handle_load_model into a new object of this class; `prec` ("s"
+        or "d") must be the precision the model was saved with."""
+        L = lib()
+        h = C.c_void_p()
+        st = L.da_handle_load_model(C.byref(h), str(path).encode())
+        if st != SUCCESS:
+            raise DAError(st, "da_handle_load_model")
+        obj = cls.__new__(cls)
+        obj.L, obj.h, obj.prec = L, h, prec
+        obj.dtype = np.float64 if prec == "d" else np.float32
+        obj.order = ROW_MAJOR if obj.get_string("storage order") == "row-major" else COLUMN_MAJOR
+        return obj
 
     def __del__(self):
         try:

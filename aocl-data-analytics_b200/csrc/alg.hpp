@@ -38,6 +38,15 @@ struct AlgBase {
         return err->warn(da_status_unknown_query, "The requested result could not be found.");
     }
     da_order order() { return da_order(opts.key("storage order")); }
+    // model persistence: the algorithm's state after its options
+    virtual da_status save_state(ByteWriter &w) {
+        (void)w;
+        return err->error(da_status_not_implemented, "This handle cannot be saved.");
+    }
+    virtual da_status load_state(ByteReader &r) {
+        (void)r;
+        return err->error(da_status_not_implemented, "This handle cannot be loaded.");
+    }
 };
 
 // ------------------------------------------------------------------ kNN ----
@@ -87,6 +96,12 @@ template <typename T> struct NN : public AlgBase {
     da_status predict_reg(da_int nq, da_int d, const T *Xt, da_int ldt, T *y,
                           da_nn_search_mode mode);
     void refresh() override { up_to_date = false; }
+    // model persistence: the training rows (and labels / targets) are copied
+    // into the file; a loaded handle owns them (X_own, y_own, t_own)
+    std::vector<T> X_own, t_own;
+    std::vector<da_int> y_own;
+    da_status save_state(ByteWriter &w) override;
+    da_status load_state(ByteReader &r) override;
 
     // core: q-major results (n_ind[q*k + r]) on the host
     da_status kneighbors_compute(da_int nq, da_int d, const T *Xt, da_int ldt, da_order ord,
@@ -148,6 +163,9 @@ template <typename T> struct KMeans : public AlgBase {
     DevBuf dLoop;
 
     KMeans(ErrorRecord *e, CudaCtx *c, bool single);
+    // model persistence: the fitted centres, labels and run information
+    da_status save_state(ByteWriter &w) override;
+    da_status load_state(ByteReader &r) override;
     ~KMeans() override;
     void refresh() override;
     da_status set_data(da_int n, da_int d, const T *A, da_int lda);

@@ -270,6 +270,90 @@ void da_handle_refresh(da_handle handle) {
     if (handle && handle->alg) handle->alg->refresh();
 }
 
+// ------------------------------------------------------ model persistence --
+// da_handle_public.cpp:295-345 (file forms).  Layout: the 12-byte magic,
+// uint32 format version, int32 handle type, int32 precision, the options
+// (Registry::save), the algorithm's state (save_state), and the 64-bit
+// FNV-1a hash of everything before it.
+static const char kModelMagic[12] = {'A', 'O', 'C', 'L', 'D', 'A', '-', 'B', '2', '0', '0', '\n'};
+static const uint32_t kModelVersion = 1;
+static uint64_t fnv1a(const char *p, size_t n) {
+    uint64_t h = 1469598103934665603ull;
+    for (size_t i = 0; i < n; ++i) {
+        h ^= (unsigned char)p[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+da_status da_handle_save_model(da_handle h, const char *file_name) {
+    if (!h) return da_status_invalid_pointer;
+    h->err.clear();
+    if (!file_name) return h->err.error(da_status_invalid_pointer, "file_name cannot be null.");
+    if (!h->alg) return h->err.error(da_status_invalid_input, "The handle is not initialized.");
+    ByteWriter w;
+    w.b.insert(w.b.end(), kModelMagic, kModelMagic + sizeof(kModelMagic));
+    w.put<uint32_t>(kModelVersion);
+    w.put<int32_t>((int32_t)h->type);
+    w.put<int32_t>((int32_t)h->precision);
+    h->alg->opts.save(w);
+    da_status s = h->alg->save_state(w);
+    if (s != da_status_success) return s;
+    w.put<uint64_t>(fnv1a(w.b.data(), w.b.size()));
+    std::FILE *f = std::fopen(file_name, "wb");
+    if (!f) return h->err.error(da_status_io_error, "Cannot open the file for writing.");
+    const size_t wrote = std::fwrite(w.b.data(), 1, w.b.size(), f);
+    const int closed = std::fclose(f);
+    if (wrote != w.b.size() || closed != 0)
+        return h->err.error(da_status_io_error, "Writing the model file failed.");
+    return da_status_success;
+}
+
+da_status da_handle_load_model(da_handle *handle, const char *file_name) {
+    if (!handle || *handle || !file_name) return da_status_invalid_pointer;
+    std::vector<char> buf;
+    {
+        std::FILE *f = std::fopen(file_name, "rb");
+        if (!f) return da_status_io_error;
+        char tmp[1 << 16];
+        size_t got;
+        while ((got = std::fread(tmp, 1, sizeof(tmp), f)) > 0) buf.insert(buf.end(), tmp, tmp + got);
+        const bool bad = std::ferror(f) != 0;
+        std::fclose(f);
+        if (bad) return da_status_io_error;
+    }
+    const size_t head = sizeof(kModelMagic) + 4 + 4 + 4;
+    if (buf.size() < head + 8 || std::memcmp(buf.data(), kModelMagic, sizeof(kModelMagic)) != 0)
+        return da_status_invalid_file_data;
+    uint64_t sum;
+    std::memcpy(&sum, buf.data() + buf.size() - 8, 8);
+    if (sum != fnv1a(buf.data(), buf.size() - 8)) return da_status_invalid_file_data;
+    ByteReader r;
+    r.p = buf.data();
+    r.n = buf.size() - 8;
+    r.pos = sizeof(kModelMagic);
+    if (r.get<uint32_t>() != kModelVersion) return da_status_version_mismatch;
+    const int32_t type = r.get<int32_t>(), prec = r.get<int32_t>();
+    if ((type != (int32_t)da_handle_nn && type != (int32_t)da_handle_kmeans) ||
+        (prec != (int32_t)da_single && prec != (int32_t)da_double))
+        return da_status_invalid_file_data;
+    da_handle h = nullptr;
+    da_status s = handle_init(&h, (da_handle_type)type, (da_precision)prec);
+    if (s != da_status_success) return s;
+    if (!h->alg->opts.load(r)) {
+        delete h;
+        return da_status_invalid_file_data;
+    }
+    s = h->alg->load_state(r);
+    if (s == da_status_success && (!r.ok || r.pos != r.n)) s = da_status_invalid_file_data;
+    if (s != da_status_success) {
+        delete h;
+        return s;
+    }
+    *handle = h;
+    return da_status_success;
+}
+
 // ---------------------------------------------------------------- options --
 // options_public.cpp:32-123
 da_status da_options_set_int(da_handle h, const char *option, da_int value) {

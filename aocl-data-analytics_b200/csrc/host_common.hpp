@@ -7,6 +7,7 @@
 #include <cctype>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <limits>
 #include <map>
@@ -77,6 +78,64 @@ inline std::string prep_str(const std::string &in) {
     }
     return out;
 }
+
+// Little byte streams of the model files (da_handle_save_model /
+// da_handle_load_model): plain values in host byte order, strings and arrays
+// with a 64-bit length; the reader fails (ok = false) instead of reading past
+// the end.
+struct ByteWriter {
+    std::vector<char> b;
+    template <typename V> void put(const V &v) {
+        const char *p = reinterpret_cast<const char *>(&v);
+        b.insert(b.end(), p, p + sizeof(V));
+    }
+    void put_str(const std::string &s) {
+        put<uint64_t>(s.size());
+        b.insert(b.end(), s.begin(), s.end());
+    }
+    template <typename V> void put_vec(const V *p, size_t n) {
+        put<uint64_t>(n);
+        const char *c = reinterpret_cast<const char *>(p);
+        b.insert(b.end(), c, c + n * sizeof(V));
+    }
+};
+struct ByteReader {
+    const char *p = nullptr;
+    size_t n = 0, pos = 0;
+    bool ok = true;
+    template <typename V> V get() {
+        V v{};
+        if (!ok || n - pos < sizeof(V)) {
+            ok = false;
+            return v;
+        }
+        std::memcpy(&v, p + pos, sizeof(V));
+        pos += sizeof(V);
+        return v;
+    }
+    std::string get_str() {
+        const uint64_t len = get<uint64_t>();
+        if (!ok || n - pos < len) {
+            ok = false;
+            return std::string();
+        }
+        std::string s(p + pos, p + pos + len);
+        pos += len;
+        return s;
+    }
+    template <typename V> std::vector<V> get_vec() {
+        const uint64_t len = get<uint64_t>();
+        std::vector<V> v;
+        if (!ok || len > (n - pos) / sizeof(V)) {
+            ok = false;
+            return v;
+        }
+        v.resize(len);
+        std::memcpy(v.data(), p + pos, len * sizeof(V));
+        pos += len * sizeof(V);
+        return v;
+    }
+};
 
 class Registry {
   public:
@@ -200,6 +259,36 @@ class Registry {
         for (auto &l : o.labels)
             if (l.first == o.sval) return l.second;
         return -1;
+    }
+    // every option's current value (name, kind, value)
+    void save(ByteWriter &w) const {
+        w.put<uint64_t>(opts_.size());
+        for (auto &kv : opts_) {
+            const Option &o = kv.second;
+            w.put_str(o.name);
+            w.put<int32_t>((int32_t)o.kind);
+            if (o.kind == OptKind::Int) w.put<int64_t>((int64_t)o.ival);
+            else if (o.kind == OptKind::Real) w.put<double>(o.rval);
+            else w.put_str(o.sval);
+        }
+    }
+    // values written by save(), through the checking setters; false on a
+    // malformed stream, an unknown option or a value the setter rejects
+    bool load(ByteReader &r) {
+        const uint64_t cnt = r.get<uint64_t>();
+        for (uint64_t i = 0; r.ok && i < cnt; ++i) {
+            const std::string name = r.get_str();
+            const int32_t kind = r.get<int32_t>();
+            if (!r.ok) return false;
+            Option *o = find(name);
+            if (!o || (int32_t)o->kind != kind) return false;
+            da_status s;
+            if (o->kind == OptKind::Int) s = set_int(name, (da_int)r.get<int64_t>());
+            else if (o->kind == OptKind::Real) s = set_real(name, r.get<double>());
+            else s = set_string(name, r.get_str());
+            if (!r.ok || s != da_status_success) return false;
+        }
+        return r.ok;
     }
     void print() const {
         for (auto &kv : opts_) {

@@ -1408,6 +1408,62 @@ template <typename T> da_status KMeans<T>::shard_result(float *centres, da_int *
     }
 }
 
+// Model persistence: sizes, the run information, the centres (column-major
+// k x d) and the labels of the best run.  A loaded handle predicts and
+// transforms and answers the result queries; a new fit needs data again.
+template <typename T> da_status KMeans<T>::save_state(ByteWriter &w) {
+    if (!model_trained)
+        return err->error(da_status_no_data,
+                          "k-means clustering has not yet been computed. Please call "
+                          "da_kmeans_compute_s or da_kmeans_compute_d before saving the model.");
+    std::vector<da_int> lab((size_t)n_samples);
+    da_int dim = n_samples;
+    da_status s = get_result_int(da_kmeans_labels, &dim, lab.data());
+    if (s != da_status_success) return s;
+    w.put<int64_t>(n_samples);
+    w.put<int64_t>(n_features);
+    w.put<int64_t>(n_clusters);
+    w.put<int32_t>((int32_t)data_order);
+    w.put<int64_t>(best_n_iter);
+    w.put<int64_t>(best_lp_n_iter);
+    w.put<double>(best_inertia);
+    w.put<int32_t>(warn_maxit ? 1 : 0);
+    w.put_vec(best_centres.data(), best_centres.size());
+    w.put_vec(lab.data(), lab.size());
+    return da_status_success;
+}
+
+template <typename T> da_status KMeans<T>::load_state(ByteReader &r) {
+    const int64_t n = r.get<int64_t>(), d = r.get<int64_t>(), k = r.get<int64_t>();
+    const int32_t ord = r.get<int32_t>();
+    const int64_t nit = r.get<int64_t>(), lpit = r.get<int64_t>();
+    const double inertia = r.get<double>();
+    const int32_t wm = r.get<int32_t>();
+    std::vector<T> cen = r.get_vec<T>();
+    std::vector<da_int> lab = r.get_vec<da_int>();
+    if (!r.ok || n < 1 || d < 1 || k < 1 || k > n || cen.size() != (size_t)(k * d) ||
+        lab.size() != (size_t)n)
+        return err->error(da_status_invalid_file_data, "The model file is corrupted.");
+    for (da_int v : lab)
+        if (v < 0 || v >= k)
+            return err->error(da_status_invalid_file_data, "The model file is corrupted.");
+    n_samples = (da_int)n;
+    n_features = (da_int)d;
+    n_clusters = (da_int)k;
+    data_order = (da_order)ord;
+    best_n_iter = (da_int)nit;
+    best_lp_n_iter = (da_int)lpit;
+    best_inertia = inertia;
+    warn_maxit = wm != 0;
+    best_centres = std::move(cen);
+    best_labels = std::move(lab);
+    best_labels_on_host = true;
+    ld = pad4(n_features);
+    initdone = false;
+    model_trained = true;
+    return da_status_success;
+}
+
 template struct KMeans<float>;
 template struct KMeans<double>;
 

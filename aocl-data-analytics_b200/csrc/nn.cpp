@@ -133,6 +133,58 @@ da_status NN<T>::set_data(da_int n, da_int d, const T *X, da_int ldx) {
     return da_status_success;
 }
 
+// Model persistence: the training rows in their storage order (dense), then
+// the labels and targets when set.  Loading replays set_data / set_labels /
+// set_targets on the handle's own copies (the options were loaded first).
+template <typename T> da_status NN<T>::save_state(ByteWriter &w) {
+    if (!have_X)
+        return err->error(da_status_no_data,
+                          "No training data have been set. Please call da_nn_set_data_s or "
+                          "da_nn_set_data_d before saving the model.");
+    const bool rm = data_order == row_major;
+    std::vector<T> X((size_t)n_samples * n_features);
+    for (da_int i = 0; i < n_samples; ++i)
+        for (da_int j = 0; j < n_features; ++j)
+            X[rm ? (size_t)i * n_features + j : i + (size_t)j * n_samples] =
+                X_host[rm ? (size_t)i * ldx_host + j : i + (size_t)j * ldx_host];
+    w.put<int64_t>(n_samples);
+    w.put<int64_t>(n_features);
+    w.put<int32_t>((int32_t)data_order);
+    w.put_vec(X.data(), X.size());
+    w.put<int32_t>(have_labels ? 1 : 0);
+    if (have_labels) w.put_vec(y_class, (size_t)n_samples);
+    w.put<int32_t>(have_targets ? 1 : 0);
+    if (have_targets) w.put_vec(y_reg, (size_t)n_samples);
+    return da_status_success;
+}
+
+template <typename T> da_status NN<T>::load_state(ByteReader &r) {
+    const int64_t n = r.get<int64_t>(), d = r.get<int64_t>();
+    const int32_t ord = r.get<int32_t>();
+    X_own = r.get_vec<T>();
+    if (!r.ok || n < 1 || d < 1 || X_own.size() != (size_t)(n * d) || ord != (int32_t)order())
+        return err->error(da_status_invalid_file_data, "The model file is corrupted.");
+    da_status s = set_data((da_int)n, (da_int)d, X_own.data(),
+                           ord == row_major ? (da_int)d : (da_int)n);
+    if (s != da_status_success) return s;
+    if (r.get<int32_t>()) {
+        y_own = r.get_vec<da_int>();
+        if (!r.ok || y_own.size() != (size_t)n)
+            return err->error(da_status_invalid_file_data, "The model file is corrupted.");
+        s = set_labels((da_int)n, y_own.data());
+        if (s != da_status_success) return s;
+    }
+    if (r.get<int32_t>()) {
+        t_own = r.get_vec<T>();
+        if (!r.ok || t_own.size() != (size_t)n)
+            return err->error(da_status_invalid_file_data, "The model file is corrupted.");
+        s = set_targets((da_int)n, t_own.data());
+        if (s != da_status_success) return s;
+    }
+    if (!r.ok) return err->error(da_status_invalid_file_data, "The model file is corrupted.");
+    return da_status_success;
+}
+
 template <typename T> da_status NN<T>::ensure_device_data() {
     da_status s = cuda->init(*err);
     if (s != da_status_success) return s;

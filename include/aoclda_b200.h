@@ -73,6 +73,9 @@ enum da_status_ {
     da_status_option_invalid_bounds = 403,
     da_status_option_invalid_value = 404,
     da_status_outlier_warning = 700,
+    da_status_serialization_error = 800,
+    da_status_invalid_file_data = 801,
+    da_status_version_mismatch = 802,
     da_status_empty_clusters = 900
 };
 typedef enum da_status_ da_status;
@@ -147,6 +150,18 @@ da_status da_handle_get_error_message(da_handle handle, char **message);
 da_status da_handle_get_error_severity(da_handle handle, da_severity *severity);
 /* source/include/aoclda_handle.h:153 */
 void da_handle_refresh(da_handle handle);
+/* source/include/aoclda_handle.h:177 -- a trained kNN (training data set)
+ * or k-means (computed) handle to a file: its options and its state (kNN:
+ * the training rows and labels / targets; k-means: centres, labels, run
+ * information).  The file format is this library's own (a magic string,
+ * format version 1, handle type, precision, options, state, FNV-1a
+ * checksum), not the reference's. */
+da_status da_handle_save_model(da_handle handle, const char *file_name);
+/* source/include/aoclda_handle.h:201 -- a new handle (*handle must be null)
+ * from a file written by da_handle_save_model: da_status_io_error when it
+ * cannot be read, da_status_invalid_file_data when it is not a model file or
+ * is corrupted, da_status_version_mismatch for another format version. */
+da_status da_handle_load_model(da_handle *handle, const char *file_name);
 
 /* ======================================================================== */
 /* Options                                                                   */
