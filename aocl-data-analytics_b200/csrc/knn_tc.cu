@@ -47,6 +47,7 @@ constexpr int TK_STASH = 4;        // values below threshold held per lane befor
 
 struct KnnTcArgs {
     int nx, nq, k, nkb, stages, n_qtiles, n_xtiles, n_items, cap;
+    int kk_last; // K steps of 16 in the last K block (the rest are zero columns)
     const float *xnorm;   // nx: fp32 |x_j|^2
     const float *margin;  // n_qtiles * BN: 2 eps_q (nudged up)
     unsigned *theta;      // n_qtiles * BN: threshold, order-preserving bits
@@ -252,8 +253,10 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                         const uint32_t al = ah + kA;
                         const uint32_t bh = smem_u32(Bh + (size_t)kb * kB);
                         const uint32_t bl = smem_u32(Bl + (size_t)kb * kB);
+                        const int nkk = kb == nkb - 1 ? a.kk_last : TK_KB / 16;
 #pragma unroll
                         for (int kk = 0; kk < TK_KB / 16; ++kk) {
+                            if (kk >= nkk) break;
                             mma_f16_ss(tacc, desc_k_sw128(ah + kk * 32), desc_k_sw128(bh + kk * 32),
                                        idesc, acc);
                             acc = 1;
@@ -677,7 +680,11 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
                           int nq, int k, int kc, int take_sqrt, void *qbuf, void *list,
                           int *fallback, int *n_fallback, int *err, float *out_key,
                           int *out_idx, cudaStream_t s, const KnnTcCosine *cosine) {
-    const int nkb = ldbf / TK_KB;
+    // ldbf: the bf16 rows' length (d rounded up to 8, at least 64); the MMA
+    // runs nkb K blocks of 64, the last with only the 16-column steps that
+    // hold data (the tensor maps zero-fill the columns past ldbf)
+    const int nkb = (ldbf + TK_KB - 1) / TK_KB;
+    const int kk_last = (d - (nkb - 1) * TK_KB + 15) / 16;
     // query tile width: small batches use a narrower MMA (the train rows are
     // read once either way; the tensor work and the epilogue scale with it)
     const int bn = nq <= 64 ? 64 : nq <= 128 ? 128 : TK_BN;
@@ -685,16 +692,20 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     const int n_xtiles = (nx + TK_BM - 1) / TK_BM;
     const int n_xchunks = (n_xtiles + TK_CHUNK_TILES - 1) / TK_CHUNK_TILES;
     const int cap = (int)knn_tc_list_cap();
-    // query-side buffers carved from qbuf (knn_tc_query_bytes)
+    // query-side buffers carved from qbuf with the region sizes of
+    // knn_tc_query_bytes / knn_tc_counts (256-query padding, 64-column K
+    // blocks), whatever the tile width
+    const size_t nq_alloc = (size_t)((nq + TK_BN - 1) / TK_BN) * TK_BN;
+    const size_t qrow = (size_t)nkb * TK_KB;
     unsigned char *p = static_cast<unsigned char *>(qbuf);
     __nv_bfloat16 *Qh = reinterpret_cast<__nv_bfloat16 *>(p);
-    __nv_bfloat16 *Ql = Qh + (size_t)nq_pad * ldbf;
-    float *margin = reinterpret_cast<float *>(Ql + (size_t)nq_pad * ldbf);
-    unsigned *theta = reinterpret_cast<unsigned *>(margin + nq_pad);
-    int *cnt = reinterpret_cast<int *>(theta + nq_pad);
-    float *qsq = reinterpret_cast<float *>(cnt + nq_pad);
-    int *lock = reinterpret_cast<int *>(qsq + nq_pad);
-    float *best = reinterpret_cast<float *>(lock + nq_pad);
+    __nv_bfloat16 *Ql = Qh + nq_alloc * qrow;
+    float *margin = reinterpret_cast<float *>(Ql + nq_alloc * qrow);
+    unsigned *theta = reinterpret_cast<unsigned *>(margin + nq_alloc);
+    int *cnt = reinterpret_cast<int *>(theta + nq_alloc);
+    float *qsq = reinterpret_cast<float *>(cnt + nq_alloc);
+    int *lock = reinterpret_cast<int *>(qsq + nq_alloc);
+    float *best = reinterpret_cast<float *>(lock + nq_alloc);
     // |v'_tc - v'_plain| <= e1 |x||q| + e2 (|x|^2 + |q|^2)  (u = 2^-24):
     //   bf16 hi/lo split of x and of -2q, dropped lo.lo term: 3.1 2^-16 |x||2q|
     //   fp32 accumulation of K_total = 3 Kp products in the tensor core
@@ -775,6 +786,7 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     a.nq = nq;
     a.k = k;
     a.nkb = nkb;
+    a.kk_last = kk_last;
     a.stages = stages;
     a.n_qtiles = n_qtiles;
     a.n_xtiles = n_xtiles;

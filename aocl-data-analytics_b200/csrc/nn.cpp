@@ -226,9 +226,11 @@ da_status NN<T>::kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_
             B200_TRY(launch_recip(dXn.as<float>(), (int)n_samples, dXinv.as<float>(), st),
                      "norms");
         }
-        const int nkb = (int)((d + 63) / 64);
-        if (!tc_train_ready || tc_ldbf != nkb * 64) {
-            tc_ldbf = nkb * 64;
+        // bf16 rows of d rounded up to 8 (at least 64): no padded K block is
+        // stored or read (the tensor maps zero-fill past the row)
+        const int ldbf = d <= 64 ? 64 : (int)((d + 7) / 8 * 8);
+        if (!tc_train_ready || tc_ldbf != ldbf) {
+            tc_ldbf = ldbf;
             const size_t xb = (size_t)n_samples * tc_ldbf * 2;
             if (!dXh.ensure(xb) || !dXl.ensure(xb) || !dXsq.ensure((size_t)n_samples * 4) ||
                 !dTkScal.ensure(64))

@@ -154,7 +154,9 @@ inline EncodeTiledFn tensor_map_encoder() {
 inline bool make_map_bf16_rows(CUtensorMap *m, const void *ptr, int rows, int cols,
                                int box_rows) {
     EncodeTiledFn enc = tensor_map_encoder();
-    if (!enc || !ptr || box_rows > 256 || cols % 64 != 0) return false;
+    // rows of any multiple of 8 elements (16 bytes) from 64 up; a 64-column
+    // box past the last column reads zeros
+    if (!enc || !ptr || box_rows > 256 || cols % 8 != 0 || cols < 64) return false;
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
     cuuint32_t box[2] = {64u, (cuuint32_t)box_rows};
