@@ -1,6 +1,6 @@
 /*
  * oracle.c -- CPU restatement of the AOCL-DA distance / kNN / k-means hot
- * path.  TEST INFRASTRUCTURE ONLY: the checker used by tests/, smoke() and
+ * path.  TEST INFRASTRUCTURE ONLY: the reference used by tests/, smoke() and
  * the cpu_baseline leg of bench.py.  The product (libaoclda_b200.so) never
  * links, loads or calls this code.
  *

@@ -1,7 +1,8 @@
 """ctypes wrapper of liboracle.so, the CPU restatement of the reference path.
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
-cpu_baseline / reference legs of bench.py as the checker.  The product never
+cpu_baseline / reference legs of bench.py, to check results and to time the
+CPU algorithm.  The product never
 imports it.  Each wrapped function cites the AOCL-DA source it restates in
 oracle.c.
 """

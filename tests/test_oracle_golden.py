@@ -1,7 +1,7 @@
 """Pins the CPU oracle against the reference's own known-answer tests.
 
 The oracle (oracle/oracle.c) restates the AOCL-DA algorithms; before it is
-trusted as the checker of the GPU path it must reproduce the golden vectors
+trusted to check the GPU path it must reproduce the golden vectors
 of the reference's test-suite (converted by tests/golden/make_golden.py).
 """
 import numpy as np
