@@ -32,6 +32,8 @@ RINFO = 1
 TRAINED = 2
 KMEANS_CENTRES = 501
 KMEANS_LABELS = 502
+RNN_COUNT, RNN_OFFSETS, RNN_INDICES, RNN_DISTANCES = 601, 602, 603, 604
+RNN_INDICES_INDEX, RNN_DISTANCES_INDEX = 605, 606
 # metrics (aoclda_metrics.h)
 METRICS = {"euclidean": 0, "sqeuclidean": 1, "minkowski": 2, "manhattan": 3, "cosine": 4,
            "euclidean_gemm": 5, "sqeuclidean_gemm": 6, "inner product": 7}
@@ -70,6 +72,8 @@ def load(path=LIB_PATH):
         "da_nn_set_targets_d": (_P, da_int, _P), "da_nn_set_targets_s": (_P, da_int, _P),
         "da_nn_kneighbors_d": (_P, da_int, da_int, _P, da_int, _P, _P, da_int, da_int),
         "da_nn_kneighbors_s": (_P, da_int, da_int, _P, da_int, _P, _P, da_int, da_int),
+        "da_nn_radius_neighbors_d": (_P, da_int, da_int, _P, da_int, C.c_double, da_int, da_int),
+        "da_nn_radius_neighbors_s": (_P, da_int, da_int, _P, da_int, C.c_float, da_int, da_int),
         "da_nn_classes_d": (_P, C.POINTER(da_int), _P), "da_nn_classes_s": (_P, C.POINTER(da_int), _P),
         "da_nn_classifier_predict_proba_d": (_P, da_int, da_int, _P, da_int, _P, C.c_int),
         "da_nn_classifier_predict_proba_s": (_P, da_int, da_int, _P, da_int, _P, C.c_int),
@@ -273,6 +277,31 @@ class KNN(Handle):
         self.call(f"da_nn_kneighbors_{self.prec}", nq, d, ptr(Q), _ld(Q, self.order), ptr(ind),
                   ptr(dist) if return_distance else None, k, int(return_distance))
         return ind, dist
+
+    def radius_neighbors(self, Q, radius, return_distance=True, sort_results=False):
+        """da_nn_radius_neighbors: returns (count[n_q + 1], offsets[n_q + 1],
+        indices, distances or None) from the result queries."""
+        Q = _as(Q, self.dtype, self.order)
+        nq, d = Q.shape
+        self.call(f"da_nn_radius_neighbors_{self.prec}", nq, d, ptr(Q), _ld(Q, self.order), radius,
+                  int(return_distance), int(sort_results))
+        cnt = self.result_int(RNN_COUNT, nq + 1)
+        off = self.result_int(RNN_OFFSETS, nq + 1)
+        total = int(cnt[nq])
+        ind = self.result_int(RNN_INDICES, max(total, 1))[:total]
+        dist = None
+        if return_distance:
+            out = np.zeros(max(total, 1), dtype=self.dtype)
+            dim = da_int(out.size)
+            self.call(f"da_handle_get_result_{self.prec}", RNN_DISTANCES, C.byref(dim), ptr(out))
+            dist = out[:total]
+        return cnt, off, ind, dist
+
+    def result_int(self, query, size):
+        out = np.zeros(size, dtype=np.int32)
+        dim = da_int(size)
+        self.call("da_handle_get_result_int", query, C.byref(dim), ptr(out))
+        return out
 
     def classes(self):
         n = da_int(0)

@@ -100,6 +100,20 @@ template <typename T> struct NN : public AlgBase {
     // into the file; a loaded handle owns them (X_own, y_own, t_own)
     std::vector<T> X_own, t_own;
     std::vector<da_int> y_own;
+    // radius search (nearest_neighbors.cpp:1915-2068, 2070-2247): per query
+    // its count and start in the flat index / value arrays; values as
+    // computed (squared for euclidean), the square root taken on extraction
+    std::vector<da_int> rnn_count, rnn_idx;
+    std::vector<long long> rnn_start;
+    std::vector<T> rnn_val;
+    bool rnn_dist = false, rnn_squares = false;
+    DevBuf dD, dRc, dRs, dRi, dRv;
+    da_status radius_neighbors(da_int nq, da_int d, const T *Xt, da_int ldt, T radius,
+                               da_int return_distance, da_int sort_results);
+    da_status get_result(da_result q, da_int *dim, double *out) override;
+    da_status get_result(da_result q, da_int *dim, float *out) override;
+    da_status get_result_int(da_result q, da_int *dim, da_int *out) override;
+    da_status radius_values(da_result q, da_int *dim, T *out);
     da_status save_state(ByteWriter &w) override;
     da_status load_state(ByteReader &r) override;
 

@@ -504,6 +504,14 @@ da_status da_nn_kneighbors_s(da_handle h, da_int nq, da_int d, const float *X, d
                              da_int *n_ind, float *n_dist, da_int k, da_int rd) {
     NN_CALL(float, h, kneighbors(nq, d, X, ldx, n_ind, n_dist, k, rd));
 }
+da_status da_nn_radius_neighbors_d(da_handle h, da_int nq, da_int d, const double *X, da_int ldx,
+                                   double radius, da_int rd, da_int sort) {
+    NN_CALL(double, h, radius_neighbors(nq, d, X, ldx, radius, rd, sort));
+}
+da_status da_nn_radius_neighbors_s(da_handle h, da_int nq, da_int d, const float *X, da_int ldx,
+                                   float radius, da_int rd, da_int sort) {
+    NN_CALL(float, h, radius_neighbors(nq, d, X, ldx, radius, rd, sort));
+}
 da_status da_nn_classes_d(da_handle h, da_int *nc, da_int *c) { NN_CALL(double, h, classes_api(nc, c)); }
 da_status da_nn_classes_s(da_handle h, da_int *nc, da_int *c) { NN_CALL(float, h, classes_api(nc, c)); }
 da_status da_nn_classifier_predict_proba_d(da_handle h, da_int nq, da_int d, const double *X,

@@ -74,6 +74,16 @@ cudaError_t launch_pairwise(const T *X, int ldx, int m, const T *Y, int ldy, int
                             const T *xn, const T *yn, const PairwiseArgs &a, T *D,
                             cudaStream_t s);
 
+// Radius neighbours from a block of distances D (rows x n, row-major, ld):
+// per row the count of D <= thr, then the ordered compaction (index order)
+// of those (column, value) pairs at out offsets start[row].
+template <typename T>
+cudaError_t launch_radius_count(const T *D, int rows, int n, size_t ld, T thr, int *cnt,
+                                cudaStream_t s);
+template <typename T>
+cudaError_t launch_radius_emit(const T *D, int rows, int n, size_t ld, T thr,
+                               const long long *start, int *idx, T *val, cudaStream_t s);
+
 // ------------------------------------------------------------ kNN fused --
 struct KnnArgs {
     int acc, post, kc;

@@ -513,4 +513,82 @@ cudaError_t launch_rowmajor_to_colmajor(const T *src, int rows, int cols, int ld
 B200_INST(float)
 B200_INST(double)
 
+// ------------------------------------------------------ radius search ---
+// nearest_neighbors.cpp:2070-2247 keeps, per query, the training rows with
+// D <= (squared) radius.  One block per row of a distance block: a count
+// pass, then an ordered compaction (block-wide exclusive scans over tiles of
+// blockDim columns), so each row's hits come out in index order.
+template <typename T>
+__global__ void radius_count_kernel(const T *D, int n, size_t ld, T thr, int *cnt) {
+    const T *row = D + (size_t)blockIdx.x * ld;
+    int c = 0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) c += row[j] <= thr ? 1 : 0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+    __shared__ int ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
+        cnt[blockIdx.x] = t;
+    }
+}
+template <typename T>
+__global__ void radius_emit_kernel(const T *D, int n, size_t ld, T thr, const long long *start,
+                                   int *idx, T *val) {
+    const T *row = D + (size_t)blockIdx.x * ld;
+    __shared__ int ws[33];
+    long long base = start[blockIdx.x];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int j0 = 0; j0 < n; j0 += blockDim.x) {
+        const int j = j0 + threadIdx.x;
+        const T v = j < n ? row[j] : T(0);
+        const int f = (j < n && v <= thr) ? 1 : 0;
+        const unsigned b = __ballot_sync(0xffffffffu, f);
+        const int inw = __popc(b & ((1u << lane) - 1u));
+        if (lane == 0) ws[w] = __popc(b);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int q = 0; q < nw; ++q) {
+                const int c = ws[q];
+                ws[q] = t;
+                t += c;
+            }
+            ws[32] = t;
+        }
+        __syncthreads();
+        if (f) {
+            const long long pos = base + ws[w] + inw;
+            idx[pos] = j;
+            val[pos] = v;
+        }
+        base += ws[32];
+        __syncthreads();
+    }
+}
+template <typename T>
+cudaError_t launch_radius_count(const T *D, int rows, int n, size_t ld, T thr, int *cnt,
+                                cudaStream_t s) {
+    if (rows <= 0) return cudaSuccess;
+    radius_count_kernel<T><<<rows, 512, 0, s>>>(D, n, ld, thr, cnt);
+    return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_radius_emit(const T *D, int rows, int n, size_t ld, T thr,
+                               const long long *start, int *idx, T *val, cudaStream_t s) {
+    if (rows <= 0) return cudaSuccess;
+    radius_emit_kernel<T><<<rows, 512, 0, s>>>(D, n, ld, thr, start, idx, val);
+    return cudaGetLastError();
+}
+template cudaError_t launch_radius_count<float>(const float *, int, int, size_t, float, int *,
+                                                cudaStream_t);
+template cudaError_t launch_radius_count<double>(const double *, int, int, size_t, double, int *,
+                                                 cudaStream_t);
+template cudaError_t launch_radius_emit<float>(const float *, int, int, size_t, float,
+                                               const long long *, int *, float *, cudaStream_t);
+template cudaError_t launch_radius_emit<double>(const double *, int, int, size_t, double,
+                                                const long long *, int *, double *, cudaStream_t);
+
 } // namespace b200

@@ -511,6 +511,261 @@ da_status NN<T>::kneighbors_compute(da_int nq, da_int d, const T *Xt, da_int ldt
 }
 
 // nearest_neighbors.cpp:940-1015
+// Radius neighbours, brute force (nearest_neighbors.cpp:1915-2068 and the
+// brute-force search :2070-2247): the distance block of the kNN path's
+// metric plan (squared for euclidean, compared with radius^2), the rows
+// within the radius in index order per query, then (sort_results) a stable
+// sort by distance as sorted_n_dist_n_ind (nearest_neighbors_utils.hpp:73-101).
+template <typename T>
+da_status NN<T>::radius_neighbors(da_int nq, da_int d, const T *Xt, da_int ldt, T r,
+                                  da_int return_distance, da_int sort_results) {
+    if (!return_distance && sort_results)
+        return err->error(da_status_invalid_input,
+                          "Cannot sort results if distances are not returned.");
+    if (!have_X)
+        return err->error(da_status_no_data,
+                          "No training data have been set. Please call da_nn_set_data_s or "
+                          "da_nn_set_data_d.");
+    da_status s = check_options_update();
+    if (s != da_status_success) return s;
+    if (metric == M_IP)
+        return err->error(da_status_incompatible_options,
+                          "The inner product metric is not compatible with radius neighbors. "
+                          "Use da_nn_kneighbors to find the k most similar training vectors by "
+                          "inner product.");
+    s = validate_queries(nq, d, Xt, ldt);
+    if (s != da_status_success) return s;
+    if (r < T(0)) r = (T)opts.r("radius");
+    model_trained = false;
+    rnn_count.assign((size_t)nq, 0);
+    rnn_start.assign((size_t)nq, 0);
+    rnn_idx.clear();
+    rnn_val.clear();
+    s = ensure_device_data();
+    if (s != da_status_success) return s;
+    cudaStream_t st = cuda->stream;
+    int acc = ACC_SQEUC, post = POST_NONE, tf = 0, norm_kind = -1;
+    switch (metric) {
+    case M_EUC: acc = ACC_SQEUC; tf = 1; break;
+    case M_SQEUC: acc = ACC_SQEUC; break;
+    case M_EUC_GEMM: acc = ACC_DOT; post = POST_GEMM_SQ_CLAMP; tf = 1; norm_kind = 0; break;
+    case M_SQEUC_GEMM: acc = ACC_DOT; post = POST_GEMM_SQ_CLAMP; norm_kind = 0; break;
+    case M_MANH: acc = ACC_MANHATTAN; break;
+    case M_COS: acc = ACC_DOT; post = POST_COSINE; norm_kind = 1; break;
+    case M_MINK:
+        if (p == T(2)) { acc = ACC_SQEUC; tf = 1; }
+        else if (p == T(1)) { acc = ACC_MANHATTAN; }
+        else { acc = ACC_MINKOWSKI; post = POST_POW; }
+        break;
+    }
+    rnn_squares = tf == 1;
+    rnn_dist = return_distance != 0;
+    const T thr = rnn_squares ? r * r : r;
+    const bool fp64 = sizeof(T) == 8;
+    const int kc = opts.key("reference isa") == 1 ? (fp64 ? 32 : 64) : (fp64 ? 512 : 256);
+    if (!dQ.ensure((size_t)nq * ld * sizeof(T)))
+        return err->error(da_status_memory_error, "Device memory allocation failed.");
+    B200_TRY(upload_matrix<T>(order(), nq, d, Xt, ldt, dQ.as<T>(), ld, dStage, st), "upload of X_test");
+    const T *qn = nullptr, *xn = nullptr;
+    if (norm_kind >= 0) {
+        if (!dQn.ensure((size_t)nq * sizeof(T)) || !dXn.ensure((size_t)n_samples * sizeof(T)))
+            return err->error(da_status_memory_error, "Device memory allocation failed.");
+        if (norm_kind == 0) {
+            B200_TRY(launch_row_sqnorms<T>(dQ.as<T>(), ld, nq, d, dQn.as<T>(), st), "norms");
+            if (xn_kind != 0)
+                B200_TRY(launch_row_sqnorms<T>(dX.as<T>(), ld, n_samples, d, dXn.as<T>(), st), "norms");
+        } else {
+            B200_TRY(launch_row_norms_eps1<T>(dQ.as<T>(), ld, nq, d, dQn.as<T>(), st), "norms");
+            if (xn_kind != 1)
+                B200_TRY(launch_row_norms_eps1<T>(dX.as<T>(), ld, n_samples, d, dXn.as<T>(), st), "norms");
+        }
+        xn_kind = norm_kind;
+        qn = dQn.as<T>();
+        xn = dXn.as<T>();
+    }
+    // query blocks whose distance rows fit in 256 MB
+    const size_t n = (size_t)n_samples;
+    const da_int B = (da_int)std::max<size_t>(1, std::min<size_t>((size_t)nq, (256u << 20) / (n * sizeof(T))));
+    if (!dD.ensure((size_t)B * n * sizeof(T)) || !dRc.ensure((size_t)B * sizeof(int)) ||
+        !dRs.ensure((size_t)B * sizeof(long long)))
+        return err->error(da_status_memory_error, "Device memory allocation failed.");
+    std::vector<int> cnt((size_t)B);
+    std::vector<long long> start((size_t)B);
+    const PairwiseArgs pa{acc, post, kc, (double)p, false, true};
+    for (da_int q0 = 0; q0 < nq; q0 += B) {
+        const int b = (int)std::min<da_int>(B, nq - q0);
+        B200_TRY(launch_pairwise<T>(dQ.as<T>() + (size_t)q0 * ld, ld, b, dX.as<T>(), ld,
+                                    (int)n, (int)d, qn ? qn + q0 : nullptr, xn, pa, dD.as<T>(), st),
+                 "distance kernel");
+        B200_TRY(launch_radius_count<T>(dD.as<T>(), b, (int)n, n, thr, dRc.as<int>(), st), "count");
+        B200_TRY(cudaMemcpyAsync(cnt.data(), dRc.p, (size_t)b * sizeof(int),
+                                 cudaMemcpyDeviceToHost, st), "copy");
+        B200_TRY(cudaStreamSynchronize(st), "radius search");
+        long long tot = 0;
+        for (int i = 0; i < b; ++i) {
+            start[i] = tot;
+            tot += cnt[i];
+        }
+        const size_t base = rnn_idx.size();
+        for (int i = 0; i < b; ++i) {
+            rnn_count[(size_t)q0 + i] = (da_int)cnt[i];
+            rnn_start[(size_t)q0 + i] = (long long)base + start[i];
+        }
+        if (tot == 0) continue;
+        if (!dRi.ensure((size_t)tot * sizeof(int)) || !dRv.ensure((size_t)tot * sizeof(T)))
+            return err->error(da_status_memory_error, "Device memory allocation failed.");
+        B200_TRY(cudaMemcpyAsync(dRs.p, start.data(), (size_t)b * sizeof(long long),
+                                 cudaMemcpyHostToDevice, st), "copy");
+        B200_TRY(launch_radius_emit<T>(dD.as<T>(), b, (int)n, n, thr, dRs.as<long long>(),
+                                       dRi.as<int>(), dRv.as<T>(), st), "compaction");
+        rnn_idx.resize(base + (size_t)tot);
+        rnn_val.resize(base + (size_t)tot);
+        std::vector<int> ii((size_t)tot);
+        B200_TRY(cudaMemcpyAsync(ii.data(), dRi.p, (size_t)tot * sizeof(int),
+                                 cudaMemcpyDeviceToHost, st), "copy");
+        B200_TRY(cudaMemcpyAsync(rnn_val.data() + base, dRv.p, (size_t)tot * sizeof(T),
+                                 cudaMemcpyDeviceToHost, st), "copy");
+        B200_TRY(cudaStreamSynchronize(st), "radius search");
+        for (size_t i = 0; i < (size_t)tot; ++i) rnn_idx[base + i] = (da_int)ii[i];
+    }
+    if (sort_results) {
+        std::vector<da_int> perm, ti;
+        std::vector<T> tv;
+        for (da_int q = 0; q < nq; ++q) {
+            const size_t o = (size_t)rnn_start[q], m = (size_t)rnn_count[q];
+            perm.resize(m);
+            for (size_t i = 0; i < m; ++i) perm[i] = (da_int)i;
+            std::stable_sort(perm.begin(), perm.end(), [&](da_int a, da_int b) {
+                return rnn_val[o + a] < rnn_val[o + b];
+            });
+            ti.assign(rnn_idx.begin() + o, rnn_idx.begin() + o + m);
+            tv.assign(rnn_val.begin() + o, rnn_val.begin() + o + m);
+            for (size_t i = 0; i < m; ++i) {
+                rnn_idx[o + i] = ti[perm[i]];
+                rnn_val[o + i] = tv[perm[i]];
+            }
+        }
+    }
+    model_trained = true;
+    return da_status_success;
+}
+
+// Result queries of the radius search (nearest_neighbors.cpp:118-260).
+template <typename T> da_status NN<T>::radius_values(da_result q, da_int *dim, T *out) {
+    if (!model_trained)
+        return err->warn(da_status_no_data,
+                         "Radius neighbors have not been computed. Please call "
+                         "da_nn_radius_neighbors_s or da_nn_radius_neighbors_d first.");
+    if (q != da_nn_radius_neighbors_distances && q != da_nn_radius_neighbors_distances_index)
+        return err->warn(da_status_unknown_query, "The requested result could not be found.");
+    if (!rnn_dist)
+        return err->warn(da_status_no_data,
+                         "Distances were not requested during radius neighbors computation. "
+                         "Please set return_distance to true in da_nn_radius_neighbors_s or "
+                         "da_nn_radius_neighbors_d call.");
+    const da_int nq = (da_int)rnn_count.size();
+    auto put = [&](da_int qi, T *dst) {
+        const size_t o = (size_t)rnn_start[qi];
+        for (da_int i = 0; i < rnn_count[qi]; ++i)
+            dst[i] = rnn_squares ? std::sqrt(rnn_val[o + i]) : rnn_val[o + i];
+    };
+    if (q == da_nn_radius_neighbors_distances_index) {
+        const da_int qi = (da_int)out[0];
+        if (qi < 0 || qi >= nq)
+            return err->warn(da_status_invalid_input,
+                             "The provided index is out of bounds. It should be in the range [0, " +
+                                 std::to_string(nq - 1) + "].");
+        if (rnn_count[qi] > *dim) {
+            *dim = rnn_count[qi];
+            return err->warn(da_status_invalid_array_dimension,
+                             "The array is too small. Please provide an array of at least size: " +
+                                 std::to_string(rnn_count[qi]) + ".");
+        }
+        put(qi, out);
+        return da_status_success;
+    }
+    const da_int total = (da_int)rnn_val.size();
+    if (total > *dim) {
+        *dim = total;
+        return err->warn(da_status_invalid_array_dimension,
+                         "The array is too small. Please provide an array of at least size: " +
+                             std::to_string(total) + ".");
+    }
+    da_int a = 0;
+    for (da_int qi = 0; qi < nq; ++qi) {
+        put(qi, out + a);
+        a += rnn_count[qi];
+    }
+    return da_status_success;
+}
+template <typename T> da_status NN<T>::get_result(da_result q, da_int *dim, double *out) {
+    if constexpr (std::is_same_v<T, double>) return radius_values(q, dim, out);
+    (void)q, (void)dim, (void)out;
+    return err->error(da_status_wrong_type, "Wrong precision type.");
+}
+template <typename T> da_status NN<T>::get_result(da_result q, da_int *dim, float *out) {
+    if constexpr (std::is_same_v<T, float>) return radius_values(q, dim, out);
+    (void)q, (void)dim, (void)out;
+    return err->error(da_status_wrong_type, "Wrong precision type.");
+}
+template <typename T> da_status NN<T>::get_result_int(da_result q, da_int *dim, da_int *out) {
+    if (q == da_trained) return AlgBase::get_result_int(q, dim, out);
+    if (!model_trained)
+        return err->warn(da_status_no_data,
+                         "Radius neighbors have not been computed. Please call "
+                         "da_nn_radius_neighbors first.");
+    const da_int nq = (da_int)rnn_count.size();
+    const da_int total = (da_int)rnn_idx.size();
+    switch (q) {
+    case da_nn_radius_neighbors_count:
+    case da_nn_radius_neighbors_offsets: {
+        if (nq + 1 > *dim) {
+            *dim = nq + 1;
+            return err->warn(da_status_invalid_array_dimension,
+                             "The array is too small. Please provide an array of at least size: " +
+                                 std::to_string(nq + 1) + ".");
+        }
+        da_int off = 0;
+        for (da_int i = 0; i < nq; ++i) {
+            if (q == da_nn_radius_neighbors_count) out[i] = rnn_count[i];
+            else out[i] = rnn_count[i] > 0 ? off : -1;
+            off += rnn_count[i];
+        }
+        out[nq] = off;
+        return da_status_success;
+    }
+    case da_nn_radius_neighbors_indices_index: {
+        const da_int qi = out[0];
+        if (qi < 0 || qi >= nq)
+            return err->warn(da_status_invalid_input,
+                             "The provided index is out of bounds. It should be in the range [0, " +
+                                 std::to_string(nq - 1) + "].");
+        if (rnn_count[qi] > *dim) {
+            *dim = rnn_count[qi];
+            return err->warn(da_status_invalid_array_dimension,
+                             "The array is too small. Please provide an array of at least size: " +
+                                 std::to_string(rnn_count[qi]) + ".");
+        }
+        for (da_int i = 0; i < rnn_count[qi]; ++i) out[i] = rnn_idx[(size_t)rnn_start[qi] + i];
+        return da_status_success;
+    }
+    case da_nn_radius_neighbors_indices: {
+        if (total > *dim) {
+            *dim = total;
+            return err->warn(da_status_invalid_array_dimension,
+                             "The array is too small. Please provide an array of at least size: " +
+                                 std::to_string(total) + ".");
+        }
+        da_int a = 0;
+        for (da_int qi = 0; qi < nq; ++qi)
+            for (da_int i = 0; i < rnn_count[qi]; ++i) out[a++] = rnn_idx[(size_t)rnn_start[qi] + i];
+        return da_status_success;
+    }
+    default:
+        return err->warn(da_status_unknown_query, "The requested result could not be found.");
+    }
+}
+
 template <typename T>
 da_status NN<T>::kneighbors(da_int nq, da_int d, const T *Xt, da_int ldt, da_int *n_ind,
                             T *n_dist, da_int k, da_int return_distance) {

@@ -109,7 +109,13 @@ enum da_result_ {
     da_rinfo = 1,
     da_trained = 2,
     da_kmeans_cluster_centres = 501,
-    da_kmeans_labels = 502
+    da_kmeans_labels = 502,
+    da_nn_radius_neighbors_count = 601,
+    da_nn_radius_neighbors_offsets = 602,
+    da_nn_radius_neighbors_indices = 603,
+    da_nn_radius_neighbors_distances = 604,
+    da_nn_radius_neighbors_indices_index = 605,
+    da_nn_radius_neighbors_distances_index = 606
 };
 typedef enum da_result_ da_result;
 
@@ -227,6 +233,17 @@ da_status da_nn_kneighbors_d(da_handle handle, da_int n_queries, da_int n_featur
 da_status da_nn_kneighbors_s(da_handle handle, da_int n_queries, da_int n_features,
                              const float *X_test, da_int ldx_test, da_int *n_ind,
                              float *n_dist, da_int k, da_int return_distance);
+/* source/include/aoclda_nearest_neighbors.h:188 -- brute force on the GPU;
+ * per query the training rows within `radius` in index order (sort_results:
+ * stable by distance); the results through da_handle_get_result_? /
+ * _int with the da_nn_radius_neighbors_* queries */
+da_status da_nn_radius_neighbors_d(da_handle handle, da_int n_queries, da_int n_features,
+                                   const double *X_test, da_int ldx_test, double radius,
+                                   da_int return_distance, da_int sort_results);
+/* source/include/aoclda_nearest_neighbors.h:191 */
+da_status da_nn_radius_neighbors_s(da_handle handle, da_int n_queries, da_int n_features,
+                                   const float *X_test, da_int ldx_test, float radius,
+                                   da_int return_distance, da_int sort_results);
 /* source/include/aoclda_nearest_neighbors.h:214 */
 da_status da_nn_classes_d(da_handle handle, da_int *n_classes, da_int *classes);
 /* source/include/aoclda_nearest_neighbors.h:215 */

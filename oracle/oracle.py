@@ -102,6 +102,28 @@ def knn(X, Q, k, metric="euclidean", p=2.0, kc=None):
     return ind, dist
 
 
+def radius(X, Q, r, metric="euclidean", p=2.0, sort=False, kc=None):
+    """Radius neighbours (nearest_neighbors.cpp:1915-2068, brute force
+    :2070-2247): per query the training rows with distance <= r -- squared
+    distances against r^2 for euclidean and minkowski p = 2 -- in index order,
+    or (sort) stably sorted by that distance (nearest_neighbors_utils.hpp:
+    73-101); distances returned with the square root taken for those metrics.
+    Returns a list of (indices, distances) per query."""
+    sq = metric == "euclidean" or (metric == "minkowski" and p == 2.0)
+    inner = "sqeuclidean" if sq else metric
+    D = pairwise(Q, X, inner, p, kc)
+    thr = np.asarray(r * r if sq else r, dtype=D.dtype)
+    out = []
+    for row in D:
+        idx = np.nonzero(row <= thr)[0]
+        val = row[idx]
+        if sort:
+            o = np.argsort(val, kind="stable")
+            idx, val = idx[o], val[o]
+        out.append((idx.astype(np.int32), np.sqrt(val) if sq else val))
+    return out
+
+
 def kmeans_assign(X, Cn):
     X = np.ascontiguousarray(X)
     dt = X.dtype
