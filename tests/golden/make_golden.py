@@ -11,7 +11,8 @@ It converts, without retyping any value:
     tests/unit_tests/nearest_neighbors/nearest_neighbors_tests.hpp:588-760,
     tolerance 500*eps), into nn_<samples>x<queries>x<features>.npz;
   * the 6x3 / 3x3 hand-computed kNN problem of nearest_neighbors_tests.hpp
-    (X_train/X_test at :450-464, expected indices and distances at :97-144),
+    (X_train/X_test at :450-464, expected indices and distances at :97-144,
+    radius-5 neighbours at :147-160),
     parsed from the C++ initialiser lists, into nn_small.npz;
   * the Lloyd "larger data matrix" k-means case of
     tests/unit_tests/kmeans/kmeans_test_data.hpp:444-526 into kmeans_lloyd80.npz.
@@ -67,9 +68,35 @@ def nn_small():
     y_reg = init_lists(text, "y_train_regression")[0]
     kinds = init_lists(text, "kind")
     kdists = init_lists(text, "kdist")
+    # the radius-5 expectations of get_expected_radius_ind_radius_dist
+    # (:147-160; sorted results): euclidean, then squared euclidean
+    blk = text[text.index("void get_expected_radius_ind_radius_dist"):]
+    blk = blk[:blk.index("template <typename T>")]
+
+    def ragged(after):
+        lists = []
+        pat = re.escape(after) + r"\s*=\s*std::vector<std::vector<[^>]*>>\(\{(.*?)\}\);"
+        for m in re.finditer(pat, blk, re.S):
+            rows = re.findall(r"\{([^{}]*)\}", m.group(1))
+            lists.append([[float(v) for v in r.split(",") if v.strip()] for r in rows])
+        return lists
+
+    rind, rdist = ragged("param.expected_radius_ind"), ragged("param.expected_radius_dist")
+
+    def flat(rows):
+        return np.array([v for r in rows for v in r])
+
+    def cnts(rows):
+        return np.array([len(r) for r in rows], dtype=np.int32)
+
+    radius = dict(radius=np.array([5.0]),
+                  rad_euc_ind=flat(rind[0]).astype(np.int32), rad_euc_cnt=cnts(rind[0]),
+                  rad_euc_dist=flat(rdist[0]),
+                  rad_sq_ind=flat(rind[1]).astype(np.int32), rad_sq_cnt=cnts(rind[1]),
+                  rad_sq_dist=flat(rdist[1]))
     # the first two lists are the k=3 and k=4 euclidean expectations (:97-144)
     np.savez_compressed(
-        os.path.join(OUT, "nn_small.npz"),
+        os.path.join(OUT, "nn_small.npz"), **radius,
         X_train=X_train.reshape(3, 6).T.copy(),  # column-major 6 x 3
         X_test=X_test.reshape(3, 3).T.copy(),    # column-major 3 x 3
         y_class=y_class.astype(np.int32), y_reg=y_reg,

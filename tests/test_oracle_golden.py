@@ -115,3 +115,18 @@ def test_oracle_reference_tie_order(orc):
     assert list(ref) == [3, 1, 5]  # equal keys stay in buffer order
     keys2 = np.array([1.0, 2.0, 2.0, 2.0])
     assert list(orc.knn_reference_ties(keys2, 2)) == [0, 3]
+
+
+def test_oracle_radius_hand_problem(orc):
+    """The radius-5 neighbours of the reference's hand problem (sorted
+    results): euclidean and squared euclidean."""
+    z = golden("nn_small.npz")
+    r = float(z["radius"][0])
+    for metric, pre in (("euclidean", "rad_euc"), ("sqeuclidean", "rad_sq")):
+        got = orc.radius(z["X_train"], z["X_test"], r, metric, sort=True)
+        o = 0
+        for q, c in enumerate(z[pre + "_cnt"]):
+            np.testing.assert_array_equal(got[q][0], z[pre + "_ind"][o:o + c])
+            np.testing.assert_allclose(got[q][1], z[pre + "_dist"][o:o + c],
+                                       rtol=40 * np.finfo(float).eps)
+            o += c

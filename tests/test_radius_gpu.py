@@ -76,3 +76,17 @@ def test_radius_result_queries(gpu, ab):
     dim = ab.da_int(dbuf.size)
     assert L.da_handle_get_result_d(nn.h, ab.RNN_DISTANCES, C.byref(dim), ab.ptr(dbuf)) == 20
     nn.close()
+
+
+def test_radius_hand_problem(gpu, ab):
+    """The reference's own radius-5 expectations on its hand problem."""
+    from conftest import golden
+    z = golden("nn_small.npz")
+    r = float(z["radius"][0])
+    for metric, pre in (("euclidean", "rad_euc"), ("sqeuclidean", "rad_sq")):
+        nn = ab.KNN("d", algorithm="brute", metric=metric).fit(z["X_train"])
+        cnt, off, ind, dist = nn.radius_neighbors(z["X_test"], r, True, True)
+        np.testing.assert_array_equal(cnt[:-1], z[pre + "_cnt"])
+        np.testing.assert_array_equal(ind, z[pre + "_ind"])
+        np.testing.assert_allclose(dist, z[pre + "_dist"], rtol=40 * np.finfo(float).eps)
+        nn.close()
