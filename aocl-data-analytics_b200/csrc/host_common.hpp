@@ -198,10 +198,6 @@ class Registry {
         if (!o) return da_status_option_not_found;
         if (o->kind != OptKind::Real) return wrong_type(name);
         v = round_t(v);
-        if (std::isnan(v)) {
-            errmsg = "Option '" + o->name + "': Invalid value.";
-            return da_status_option_invalid_value;
-        }
         if (!in_bounds(v, o->rlo, o->lb, o->rhi, o->ub)) {
             errmsg = "Option '" + o->name + "': value out-of-bounds";
             return da_status_option_invalid_value;
@@ -318,11 +314,14 @@ class Registry {
         return da_status_option_wrong_type;
     }
     double round_t(double v) const { return single ? (double)(float)v : v; }
+    // A value is rejected only when a bound comparison holds (options.hpp:
+    // 266-276, the setter validating without the NaN check of checkall), so
+    // a NaN real value is accepted, as the "outlier target" option needs.
     static bool in_bounds(double v, double lo, LB lb, double hi, UB ub) {
-        if (lb == LB::greaterthan && !(v > lo)) return false;
-        if (lb == LB::greaterequal && !(v >= lo)) return false;
-        if (ub == UB::lessthan && !(v < hi)) return false;
-        if (ub == UB::lessequal && !(v <= hi)) return false;
+        if (lb == LB::greaterthan && v <= lo) return false;
+        if (lb == LB::greaterequal && v < lo) return false;
+        if (ub == UB::lessthan && v >= hi) return false;
+        if (ub == UB::lessequal && v > hi) return false;
         return true;
     }
 };

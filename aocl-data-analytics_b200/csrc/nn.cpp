@@ -3,6 +3,7 @@
 // source/core/nearest_neighbors/nearest_neighbors.cpp; the distance tile and
 // the top-k selection run on the GPU (dist_simt.cu).
 #include "alg.hpp"
+#include <map>
 
 namespace b200 {
 
@@ -11,6 +12,8 @@ enum { M_EUC = 0, M_SQEUC = 1, M_MINK = 2, M_MANH = 3, M_COS = 4, M_EUC_GEMM = 5
        M_SQEUC_GEMM = 6, M_IP = 7 };
 // algorithm ids (nearest_neighbors_types.hpp:29)
 enum { A_BRUTE = 0, A_KD = 1, A_BALL = 2, A_AUTO = 3 };
+// "outlier handling" ids (nearest_neighbors_types.hpp)
+enum { OH_NONE = 0, OH_MANUAL = 1, OH_MOST_FREQUENT = 2 };
 
 template <typename T>
 NN<T>::NN(ErrorRecord *e, CudaCtx *c, bool single) {
@@ -46,7 +49,8 @@ NN<T>::NN(ErrorRecord *e, CudaCtx *c, bool single) {
                      {"inner product", M_IP}},
                     "euclidean");
     opts.add_string("weights", {{"uniform", 0}, {"distance", 1}}, "uniform");
-    opts.add_string("outlier handling", {{"none", 0}, {"manual", 1}, {"most frequent", 2}},
+    opts.add_string("outlier handling",
+                    {{"none", OH_NONE}, {"manual", OH_MANUAL}, {"most frequent", OH_MOST_FREQUENT}},
                     "none");
     // B200 options (no counterpart in the reference):
     //   "reference isa": which AOCL-DA build's KC blocking the squared-euclidean
@@ -510,37 +514,20 @@ da_status NN<T>::kneighbors_compute(da_int nq, da_int d, const T *Xt, da_int ldt
     return da_status_success;
 }
 
-// nearest_neighbors.cpp:940-1015
-// Radius neighbours, brute force (nearest_neighbors.cpp:1915-2068 and the
-// brute-force search :2070-2247): the distance block of the kNN path's
-// metric plan (squared for euclidean, compared with radius^2), the rows
-// within the radius in index order per query, then (sort_results) a stable
-// sort by distance as sorted_n_dist_n_ind (nearest_neighbors_utils.hpp:73-101).
+// Core of the radius search (radius_neighbors_compute, nearest_neighbors.cpp:
+// 1983-2068): per query its count and start in the flat index / value arrays,
+// rows in index order; values (only when want_val) as computed, squared for
+// euclidean (`squares`).  Options and queries are validated by the caller.
 template <typename T>
-da_status NN<T>::radius_neighbors(da_int nq, da_int d, const T *Xt, da_int ldt, T r,
-                                  da_int return_distance, da_int sort_results) {
-    if (!return_distance && sort_results)
-        return err->error(da_status_invalid_input,
-                          "Cannot sort results if distances are not returned.");
-    if (!have_X)
-        return err->error(da_status_no_data,
-                          "No training data have been set. Please call da_nn_set_data_s or "
-                          "da_nn_set_data_d.");
-    da_status s = check_options_update();
-    if (s != da_status_success) return s;
-    if (metric == M_IP)
-        return err->error(da_status_incompatible_options,
-                          "The inner product metric is not compatible with radius neighbors. "
-                          "Use da_nn_kneighbors to find the k most similar training vectors by "
-                          "inner product.");
-    s = validate_queries(nq, d, Xt, ldt);
-    if (s != da_status_success) return s;
-    if (r < T(0)) r = (T)opts.r("radius");
-    model_trained = false;
-    rnn_count.assign((size_t)nq, 0);
-    rnn_start.assign((size_t)nq, 0);
-    rnn_idx.clear();
-    rnn_val.clear();
+da_status NN<T>::radius_compute(da_int nq, da_int d, const T *Xt, da_int ldt, T r, bool want_val,
+                                std::vector<da_int> &cnt_out, std::vector<long long> &start_out,
+                                std::vector<da_int> &idx_out, std::vector<T> &val_out,
+                                bool &squares) {
+    da_status s;
+    cnt_out.assign((size_t)nq, 0);
+    start_out.assign((size_t)nq, 0);
+    idx_out.clear();
+    val_out.clear();
     s = ensure_device_data();
     if (s != da_status_success) return s;
     cudaStream_t st = cuda->stream;
@@ -552,14 +539,14 @@ da_status NN<T>::radius_neighbors(da_int nq, da_int d, const T *Xt, da_int ldt, 
     case M_SQEUC_GEMM: acc = ACC_DOT; post = POST_GEMM_SQ_CLAMP; norm_kind = 0; break;
     case M_MANH: acc = ACC_MANHATTAN; break;
     case M_COS: acc = ACC_DOT; post = POST_COSINE; norm_kind = 1; break;
+    case M_IP: acc = ACC_DOT; break; // radius predict only: rows with dot <= r
     case M_MINK:
         if (p == T(2)) { acc = ACC_SQEUC; tf = 1; }
         else if (p == T(1)) { acc = ACC_MANHATTAN; }
         else { acc = ACC_MINKOWSKI; post = POST_POW; }
         break;
     }
-    rnn_squares = tf == 1;
-    rnn_dist = return_distance != 0;
+    squares = tf == 1;
     const T thr = rnn_squares ? r * r : r;
     const bool fp64 = sizeof(T) == 8;
     const int kc = opts.key("reference isa") == 1 ? (fp64 ? 32 : 64) : (fp64 ? 512 : 256);
@@ -606,10 +593,10 @@ da_status NN<T>::radius_neighbors(da_int nq, da_int d, const T *Xt, da_int ldt, 
             start[i] = tot;
             tot += cnt[i];
         }
-        const size_t base = rnn_idx.size();
+        const size_t base = idx_out.size();
         for (int i = 0; i < b; ++i) {
-            rnn_count[(size_t)q0 + i] = (da_int)cnt[i];
-            rnn_start[(size_t)q0 + i] = (long long)base + start[i];
+            cnt_out[(size_t)q0 + i] = (da_int)cnt[i];
+            start_out[(size_t)q0 + i] = (long long)base + start[i];
         }
         if (tot == 0) continue;
         if (!dRi.ensure((size_t)tot * sizeof(int)) || !dRv.ensure((size_t)tot * sizeof(T)))
@@ -618,16 +605,51 @@ da_status NN<T>::radius_neighbors(da_int nq, da_int d, const T *Xt, da_int ldt, 
                                  cudaMemcpyHostToDevice, st), "copy");
         B200_TRY(launch_radius_emit<T>(dD.as<T>(), b, (int)n, n, thr, dRs.as<long long>(),
                                        dRi.as<int>(), dRv.as<T>(), st), "compaction");
-        rnn_idx.resize(base + (size_t)tot);
-        rnn_val.resize(base + (size_t)tot);
+        idx_out.resize(base + (size_t)tot);
+        if (want_val) val_out.resize(base + (size_t)tot);
         std::vector<int> ii((size_t)tot);
         B200_TRY(cudaMemcpyAsync(ii.data(), dRi.p, (size_t)tot * sizeof(int),
                                  cudaMemcpyDeviceToHost, st), "copy");
-        B200_TRY(cudaMemcpyAsync(rnn_val.data() + base, dRv.p, (size_t)tot * sizeof(T),
-                                 cudaMemcpyDeviceToHost, st), "copy");
+        if (want_val)
+            B200_TRY(cudaMemcpyAsync(val_out.data() + base, dRv.p, (size_t)tot * sizeof(T),
+                                     cudaMemcpyDeviceToHost, st), "copy");
         B200_TRY(cudaStreamSynchronize(st), "radius search");
-        for (size_t i = 0; i < (size_t)tot; ++i) rnn_idx[base + i] = (da_int)ii[i];
+        for (size_t i = 0; i < (size_t)tot; ++i) idx_out[base + i] = (da_int)ii[i];
     }
+    return da_status_success;
+}
+
+// nearest_neighbors.cpp:940-1015
+// Radius neighbours, brute force (nearest_neighbors.cpp:1915-2068 and the
+// brute-force search :2070-2247): the distance block of the kNN path's
+// metric plan (squared for euclidean, compared with radius^2), the rows
+// within the radius in index order per query, then (sort_results) a stable
+// sort by distance as sorted_n_dist_n_ind (nearest_neighbors_utils.hpp:73-101).
+template <typename T>
+da_status NN<T>::radius_neighbors(da_int nq, da_int d, const T *Xt, da_int ldt, T r,
+                                  da_int return_distance, da_int sort_results) {
+    if (!return_distance && sort_results)
+        return err->error(da_status_invalid_input,
+                          "Cannot sort results if distances are not returned.");
+    if (!have_X)
+        return err->error(da_status_no_data,
+                          "No training data have been set. Please call da_nn_set_data_s or "
+                          "da_nn_set_data_d.");
+    da_status s = check_options_update();
+    if (s != da_status_success) return s;
+    if (metric == M_IP)
+        return err->error(da_status_incompatible_options,
+                          "The inner product metric is not compatible with radius neighbors. "
+                          "Use da_nn_kneighbors to find the k most similar training vectors by "
+                          "inner product.");
+    s = validate_queries(nq, d, Xt, ldt);
+    if (s != da_status_success) return s;
+    if (r < T(0)) r = (T)opts.r("radius");
+    model_trained = false;
+    s = radius_compute(nq, d, Xt, ldt, r, return_distance || sort_results, rnn_count, rnn_start,
+                       rnn_idx, rnn_val, rnn_squares);
+    if (s != da_status_success) return s;
+    rnn_dist = return_distance != 0;
     if (sort_results) {
         std::vector<da_int> perm, ti;
         std::vector<T> tv;
@@ -886,6 +908,97 @@ da_status NN<T>::compute_proba(da_int nq, da_int d, const T *Xt, da_int ldt,
     return da_status_success;
 }
 
+// Radius-mode vote (predict_proba_compute_rnn, nearest_neighbors.cpp:1280-1479):
+// the rows within the "radius" option of each query vote for their labels,
+// with weight 1 (uniform) or 1 / distance (distance; 1 at distance <= eps).
+// A query with no row within the radius is an error under outlier handling
+// "none"; "manual" gives it probability 1 for the "outlier label" (all zero
+// and a warning when that label is not a training label), "most frequent"
+// probability 1 for the most frequent training label.  proba is q-major.
+template <typename T>
+da_status NN<T>::compute_proba_rnn(da_int nq, da_int d, const T *Xt, da_int ldt,
+                                   std::vector<T> &proba) {
+    if (metric == M_IP && weights == 1)
+        return err->error(da_status_incompatible_options,
+                          "The inner product metric is not compatible with "
+                          "weights=\"distance\". Use weights=\"uniform\" instead.");
+    if (!classes_done) {
+        da_status s = available_classes();
+        if (s != da_status_success) return s;
+    }
+    const da_int oh = opts.key("outlier handling");
+    const da_int nc = (da_int)classes.size();
+    const da_int mf = oh == OH_MOST_FREQUENT ? most_frequent_label() : 0;
+    da_int manual_idx = -1;
+    if (oh == OH_MANUAL) {
+        auto it = std::lower_bound(classes.begin(), classes.end(), (da_int)opts.i("outlier label"));
+        if (it != classes.end() && *it == (da_int)opts.i("outlier label"))
+            manual_idx = (da_int)(it - classes.begin());
+    }
+    std::vector<da_int> cnt, idx;
+    std::vector<long long> start;
+    std::vector<T> val;
+    bool squares = false;
+    da_status s = radius_compute(nq, d, Xt, ldt, (T)opts.r("radius"), weights == 1, cnt, start,
+                                 idx, val, squares);
+    if (s != da_status_success) return s;
+    proba.assign((size_t)nq * nc, T(0));
+    bool outliers = false;
+    for (da_int q = 0; q < nq; ++q) {
+        T *pq = proba.data() + (size_t)q * nc;
+        const size_t o = (size_t)start[q], m = (size_t)cnt[q];
+        if (m == 0) {
+            if (oh == OH_NONE)
+                return err->error(da_status_operation_failed,
+                                  "Failed to compute probabilities for query " + std::to_string(q) +
+                                      " since it does not have any neighbors within the "
+                                      "specified radius.");
+            if (oh == OH_MANUAL) {
+                outliers = true;
+                if (manual_idx != -1) pq[manual_idx] = T(1);
+            } else {
+                for (da_int c = 0; c < nc; ++c) pq[c] = classes[c] == mf ? T(1) : T(0);
+            }
+            continue;
+        }
+        // per class, the neighbours' weights in neighbour order
+        for (size_t i = 0; i < m; ++i) {
+            const da_int c = (da_int)(std::lower_bound(classes.begin(), classes.end(),
+                                                       y_class[idx[o + i]]) - classes.begin());
+            pq[c] += weights == 0 ? T(1) : radius_weight(val[o + i], squares);
+        }
+        T den = T(0);
+        for (da_int c = 0; c < nc; ++c) den += pq[c];
+        for (da_int c = 0; c < nc; ++c) pq[c] /= den;
+    }
+    if (oh == OH_MANUAL && outliers && manual_idx == -1)
+        return err->warn(da_status_outlier_warning,
+                         "The manually set outlier label is not present in the training labels. "
+                         "Setting probabilities to 0.0.");
+    return da_status_success;
+}
+
+// most_frequent_element (nearest_neighbors.cpp:1037-1058): the most frequent
+// training label, the smallest of equally frequent ones.
+template <typename T> da_int NN<T>::most_frequent_label() {
+    std::map<da_int, da_int> freq;
+    for (da_int i = 0; i < n_samples; ++i) freq[y_class[i]]++;
+    da_int best = y_class[0], top = 0;
+    for (const auto &f : freq)
+        if (f.second > top) {
+            top = f.second;
+            best = f.first;
+        }
+    return best;
+}
+
+// get_weights (nearest_neighbors.cpp:1021-1033) of one radius neighbour; the
+// stored value is squared for euclidean.
+template <typename T> T NN<T>::radius_weight(T v, bool squares) {
+    const T w = squares ? std::sqrt(v) : v;
+    return w <= std::numeric_limits<T>::epsilon() ? T(1) : T(1) / w;
+}
+
 template <typename T>
 da_status NN<T>::predict_proba(da_int nq, da_int d, const T *Xt, da_int ldt, T *proba,
                                da_nn_search_mode mode) {
@@ -908,18 +1021,19 @@ da_status NN<T>::predict_proba(da_int nq, da_int d, const T *Xt, da_int ldt, T *
                           "Number of features must be greater than zero.");
     s = validate_queries(nq, d, Xt, ldt);
     if (s != da_status_success) return s;
-    if (mode != knn_search_mode)
-        return err->error(da_status_not_implemented,
-                          "Radius-neighbours search is not provided by the B200 library.");
+    if (mode != knn_search_mode && mode != radius_search_mode)
+        return err->error(da_status_invalid_input,
+                          "Unknown search mode: " + std::to_string((int)mode) + ".");
     std::vector<T> pr;
-    s = compute_proba(nq, d, Xt, ldt, pr);
-    if (s != da_status_success) return s;
+    s = mode == knn_search_mode ? compute_proba(nq, d, Xt, ldt, pr)
+                                : compute_proba_rnn(nq, d, Xt, ldt, pr);
+    if (s != da_status_success && s != da_status_outlier_warning) return s;
     const da_int nc = (da_int)classes.size();
     const bool cm = order() == column_major;
     for (da_int q = 0; q < nq; ++q)
         for (da_int c = 0; c < nc; ++c)
             proba[cm ? (size_t)c * nq + q : (size_t)q * nc + c] = pr[(size_t)q * nc + c];
-    return da_status_success;
+    return s;
 }
 
 template <typename T>
@@ -940,13 +1054,20 @@ da_status NN<T>::predict(da_int nq, da_int d, const T *Xt, da_int ldt, da_int *y
         return err->error(da_status_invalid_array_dimension, "n_queries must be greater than 0.");
     s = validate_queries(nq, d, Xt, ldt);
     if (s != da_status_success) return s;
-    if (mode != knn_search_mode)
-        return err->error(da_status_not_implemented,
-                          "Radius-neighbours search is not provided by the B200 library.");
+    if (mode != knn_search_mode && mode != radius_search_mode)
+        return err->error(da_status_invalid_input,
+                          "Unknown search mode: " + std::to_string((int)mode) + ".");
     std::vector<T> pr;
-    s = compute_proba(nq, d, Xt, ldt, pr);
-    if (s != da_status_success) return s;
+    s = mode == knn_search_mode ? compute_proba(nq, d, Xt, ldt, pr)
+                                : compute_proba_rnn(nq, d, Xt, ldt, pr);
+    if (s != da_status_success && s != da_status_outlier_warning) return s;
     const da_int nc = (da_int)classes.size();
+    // radius mode with outlier handling: an all-zero row (a query without
+    // neighbours) takes the outlier label or the most frequent label
+    // (nearest_neighbors.cpp:1566-1599)
+    const da_int oh = mode == knn_search_mode ? OH_NONE : opts.key("outlier handling");
+    const da_int fill = oh == OH_MANUAL ? (da_int)opts.i("outlier label")
+                        : oh == OH_MOST_FREQUENT ? most_frequent_label() : 0;
     for (da_int q = 0; q < nq; ++q) {
         // first maximum (cblas_iamax semantics, nearest_neighbors.cpp:1566-1573)
         da_int best = 0;
@@ -958,9 +1079,9 @@ da_status NN<T>::predict(da_int nq, da_int d, const T *Xt, da_int ldt, da_int *y
                 best = c;
             }
         }
-        y[q] = classes[best];
+        y[q] = (oh != OH_NONE && pr[(size_t)q * nc + best] == T(0)) ? fill : classes[best];
     }
-    return da_status_success;
+    return s;
 }
 
 template <typename T>
@@ -981,13 +1102,14 @@ da_status NN<T>::predict_reg(da_int nq, da_int d, const T *Xt, da_int ldt, T *y,
         return err->error(da_status_invalid_array_dimension, "n_queries must be greater than 0.");
     s = validate_queries(nq, d, Xt, ldt);
     if (s != da_status_success) return s;
-    if (mode != knn_search_mode)
-        return err->error(da_status_not_implemented,
-                          "Radius-neighbours search is not provided by the B200 library.");
+    if (mode != knn_search_mode && mode != radius_search_mode)
+        return err->error(da_status_invalid_input,
+                          "Unknown search mode: " + std::to_string((int)mode) + ".");
     if (metric == M_IP && weights == 1)
         return err->error(da_status_incompatible_options,
                           "The inner product metric is not compatible with "
                           "weights=\"distance\". Use weights=\"uniform\" instead.");
+    if (mode == radius_search_mode) return predict_reg_rnn(nq, d, Xt, ldt, y);
     const da_int k = n_neighbors;
     if (k > n_samples)
         return err->error(da_status_invalid_input,
@@ -1014,6 +1136,69 @@ da_status NN<T>::predict_reg(da_int nq, da_int d, const T *Xt, da_int ldt, T *y,
             y[q] = num / den;
         }
     }
+    return da_status_success;
+}
+
+// Radius-mode regression (predict_targets_rnn, nearest_neighbors.cpp:1763-1909):
+// the mean target of the rows within the radius (uniform) or their
+// 1 / distance weighted mean (distance).  A query without neighbours is an
+// error under outlier handling "none"; it takes the mean training target
+// under "most frequent" and the "outlier target" (with a warning) under
+// "manual".
+template <typename T>
+da_status NN<T>::predict_reg_rnn(da_int nq, da_int d, const T *Xt, da_int ldt, T *y) {
+    const da_int oh = opts.key("outlier handling");
+    T mean_target = T(0);
+    if (oh == OH_MOST_FREQUENT) {
+        for (da_int i = 0; i < n_samples; ++i) mean_target += y_reg[i];
+        mean_target /= T(n_samples);
+    }
+    const T manual_target = (T)opts.r("outlier target");
+    std::vector<da_int> cnt, idx;
+    std::vector<long long> start;
+    std::vector<T> val;
+    bool squares = false;
+    da_status s = radius_compute(nq, d, Xt, ldt, (T)opts.r("radius"), weights == 1, cnt, start,
+                                 idx, val, squares);
+    if (s != da_status_success) return s;
+    bool outliers = false;
+    for (da_int q = 0; q < nq; ++q) {
+        const size_t o = (size_t)start[q], m = (size_t)cnt[q];
+        if (m == 0) {
+            if (oh == OH_NONE)
+                return err->error(da_status_operation_failed,
+                                  std::string(weights == 0 ? "Failed to compute targets for query "
+                                                           : "Failed to predict targets for query ") +
+                                      std::to_string(q) +
+                                      " since it does not have any neighbors within the "
+                                      "specified radius.");
+            if (oh == OH_MOST_FREQUENT) {
+                y[q] = mean_target;
+            } else {
+                outliers = true;
+                y[q] = manual_target;
+            }
+            continue;
+        }
+        if (weights == 0) {
+            T sum = T(0);
+            for (size_t i = 0; i < m; ++i) sum += y_reg[idx[o + i]];
+            y[q] = sum / T(m);
+        } else {
+            T num = T(0), den = T(0);
+            for (size_t i = 0; i < m; ++i) {
+                const T w = radius_weight(val[o + i], squares);
+                num += y_reg[idx[o + i]] * w;
+                den += w;
+            }
+            y[q] = num / den;
+        }
+    }
+    if (oh == OH_MANUAL && outliers)
+        return err->warn(da_status_outlier_warning,
+                         "One or more samples have no neighbors within the specified radius. "
+                         "Setting the corresponding targets to " + std::to_string(manual_target) +
+                             ".");
     return da_status_success;
 }
 
