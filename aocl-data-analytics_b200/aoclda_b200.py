@@ -18,15 +18,17 @@ SUCCESS = 0
 STATUS = {
     0: "success", 1: "internal_error", 2: "memory_error", 3: "invalid_pointer",
     4: "invalid_input", 5: "not_implemented", 7: "wrong_type", 9: "invalid_handle_type",
-    10: "handle_not_initialized", 13: "incompatible_options", 15: "invalid_leading_dimension",
+    10: "handle_not_initialized", 13: "incompatible_options", 14: "operation_failed",
+    15: "invalid_leading_dimension",
     17: "invalid_array_dimension", 18: "unknown_query", 20: "no_data", 21: "maxit",
     25: "arch_not_supported", 400: "option_not_found", 401: "option_locked",
     402: "option_wrong_type", 403: "option_invalid_bounds", 404: "option_invalid_value",
-    900: "empty_clusters",
+    700: "outlier_warning", 900: "empty_clusters",
 }
 # handle types (aoclda_handle.h)
 HANDLE_KMEANS = 3
 HANDLE_NN = 8
+HANDLE_APPROX_NN = 11
 # results (aoclda_result.h)
 RINFO = 1
 TRAINED = 2
@@ -34,6 +36,9 @@ KMEANS_CENTRES = 501
 KMEANS_LABELS = 502
 RNN_COUNT, RNN_OFFSETS, RNN_INDICES, RNN_DISTANCES = 601, 602, 603, 604
 RNN_INDICES_INDEX, RNN_DISTANCES_INDEX = 605, 606
+KNN_SEARCH, RADIUS_SEARCH = 0, 1  # da_nn_search_mode
+OUTLIER_WARNING = 700
+APPROX_NN_CENTROIDS, APPROX_NN_LIST_SIZES = 801, 802
 # metrics (aoclda_metrics.h)
 METRICS = {"euclidean": 0, "sqeuclidean": 1, "minkowski": 2, "manhattan": 3, "cosine": 4,
            "euclidean_gemm": 5, "sqeuclidean_gemm": 6, "inner product": 7}
@@ -74,6 +79,14 @@ def load(path=LIB_PATH):
         "da_nn_kneighbors_s": (_P, da_int, da_int, _P, da_int, _P, _P, da_int, da_int),
         "da_nn_radius_neighbors_d": (_P, da_int, da_int, _P, da_int, C.c_double, da_int, da_int),
         "da_nn_radius_neighbors_s": (_P, da_int, da_int, _P, da_int, C.c_float, da_int, da_int),
+        "da_approx_nn_set_training_data_d": (_P, da_int, da_int, _P, da_int),
+        "da_approx_nn_set_training_data_s": (_P, da_int, da_int, _P, da_int),
+        "da_approx_nn_train_d": (_P,), "da_approx_nn_train_s": (_P,),
+        "da_approx_nn_add_d": (_P, da_int, da_int, _P, da_int),
+        "da_approx_nn_add_s": (_P, da_int, da_int, _P, da_int),
+        "da_approx_nn_train_and_add_d": (_P,), "da_approx_nn_train_and_add_s": (_P,),
+        "da_approx_nn_kneighbors_d": (_P, da_int, da_int, _P, da_int, _P, _P, da_int, da_int),
+        "da_approx_nn_kneighbors_s": (_P, da_int, da_int, _P, da_int, _P, _P, da_int, da_int),
         "da_nn_classes_d": (_P, C.POINTER(da_int), _P), "da_nn_classes_s": (_P, C.POINTER(da_int), _P),
         "da_nn_classifier_predict_proba_d": (_P, da_int, da_int, _P, da_int, _P, C.c_int),
         "da_nn_classifier_predict_proba_s": (_P, da_int, da_int, _P, da_int, _P, C.c_int),
@@ -310,28 +323,101 @@ class KNN(Handle):
         self.call(f"da_nn_classes_{self.prec}", C.byref(n), ptr(out))
         return out
 
-    def predict_proba(self, Q):
+    # predict_proba / predict / predict_reg: `mode` is KNN_SEARCH (the
+    # "number of neighbors" nearest rows) or RADIUS_SEARCH (the rows within
+    # the "radius" option); status 700 (outlier warning) is kept in
+    # self.last_status with the results
+
+    def predict_proba(self, Q, mode=KNN_SEARCH):
         Q = _as(Q, self.dtype, self.order)
         nq, d = Q.shape
         nc = len(self.classes())
         pr = np.zeros((nq, nc), dtype=self.dtype, order="F" if self.order == COLUMN_MAJOR else "C")
-        self.call(f"da_nn_classifier_predict_proba_{self.prec}", nq, d, ptr(Q), _ld(Q, self.order),
-                  ptr(pr), 0)
+        self.last_status = self.call(f"da_nn_classifier_predict_proba_{self.prec}", nq, d, ptr(Q),
+                                     _ld(Q, self.order), ptr(pr), mode,
+                                     ok=(SUCCESS, OUTLIER_WARNING))
         return pr
 
-    def predict(self, Q):
+    def predict(self, Q, mode=KNN_SEARCH):
         Q = _as(Q, self.dtype, self.order)
         nq, d = Q.shape
         y = np.zeros(nq, dtype=np.int32)
-        self.call(f"da_nn_classifier_predict_{self.prec}", nq, d, ptr(Q), _ld(Q, self.order), ptr(y), 0)
+        self.last_status = self.call(f"da_nn_classifier_predict_{self.prec}", nq, d, ptr(Q),
+                                     _ld(Q, self.order), ptr(y), mode,
+                                     ok=(SUCCESS, OUTLIER_WARNING))
         return y
 
-    def predict_reg(self, Q):
+    def predict_reg(self, Q, mode=KNN_SEARCH):
         Q = _as(Q, self.dtype, self.order)
         nq, d = Q.shape
         y = np.zeros(nq, dtype=self.dtype)
-        self.call(f"da_nn_regressor_predict_{self.prec}", nq, d, ptr(Q), _ld(Q, self.order), ptr(y), 0)
+        self.last_status = self.call(f"da_nn_regressor_predict_{self.prec}", nq, d, ptr(Q),
+                                     _ld(Q, self.order), ptr(y), mode,
+                                     ok=(SUCCESS, OUTLIER_WARNING))
         return y
+
+
+class ApproxNN(Handle):
+    """IVF-flat approximate neighbours through da_approx_nn_* (host arrays,
+    C-ABI calls)."""
+
+    def __init__(self, prec="d", order=COLUMN_MAJOR, **options):
+        super().__init__(HANDLE_APPROX_NN, prec)
+        self.order = order
+        if order == ROW_MAJOR:
+            self.set("storage order", "row-major")
+        # option names: "n_list", "n_probe", "k-means_iter", "seed", "metric",
+        # "algorithm" as they are; number_of_neighbors / train_fraction spelled
+        # with underscores for keyword use
+        names = {"number_of_neighbors": "number of neighbors", "train_fraction": "train fraction",
+                 "kmeans_iter": "k-means_iter"}
+        for k, v in options.items():
+            st = self.set(names.get(k, k), v)
+            if st != SUCCESS:
+                raise DAError(st, f"option {k}")
+
+    def set_training_data(self, X):
+        self.X = _as(X, self.dtype, self.order)
+        n, d = self.X.shape
+        self.call(f"da_approx_nn_set_training_data_{self.prec}", n, d, ptr(self.X),
+                  _ld(self.X, self.order))
+        return self
+
+    def train(self):
+        self.call(f"da_approx_nn_train_{self.prec}")
+        return self
+
+    def add(self, X):
+        A = _as(X, self.dtype, self.order)  # the index keeps its own copy of the rows
+        n, d = A.shape
+        self.call(f"da_approx_nn_add_{self.prec}", n, d, ptr(A), _ld(A, self.order))
+        return self
+
+    def train_and_add(self):
+        self.call(f"da_approx_nn_train_and_add_{self.prec}")
+        return self
+
+    def kneighbors(self, Q, k, return_distance=True):
+        Q = _as(Q, self.dtype, self.order)
+        nq, d = Q.shape
+        o = "F" if self.order == COLUMN_MAJOR else "C"
+        ind = np.zeros((nq, k), dtype=np.int32, order=o)
+        dist = np.zeros((nq, k), dtype=self.dtype, order=o)
+        self.call(f"da_approx_nn_kneighbors_{self.prec}", nq, d, ptr(Q), _ld(Q, self.order),
+                  ptr(ind), ptr(dist) if return_distance else None, k, int(return_distance))
+        return ind, (dist if return_distance else None)
+
+    def result(self, query, size):
+        out = np.zeros(size, dtype=self.dtype)
+        dim = da_int(size)
+        self.call(f"da_handle_get_result_{self.prec}", query, C.byref(dim), ptr(out))
+        return out
+
+    def list_sizes(self, n_list):
+        out = np.zeros(n_list, dtype=np.int32)
+        dim = da_int(n_list)
+        self.call("da_handle_get_result_int", APPROX_NN_LIST_SIZES, C.byref(dim), ptr(out))
+        return out
 
 
 class KMeans(Handle):

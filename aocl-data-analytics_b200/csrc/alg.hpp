@@ -4,6 +4,7 @@
 #pragma once
 #include "b200_kernels.hpp"
 #include "host_common.hpp"
+#include <memory>
 #include <random>
 #include <set>
 
@@ -126,6 +127,15 @@ template <typename T> struct NN : public AlgBase {
     da_status kneighbors_tc(da_int nq, da_int d, da_int k, int kc, bool take_sqrt, bool cosine,
                             bool &done);
     da_status compute_proba(da_int nq, da_int d, const T *Xt, da_int ldt, std::vector<T> &proba);
+    // radius mode of predict / predict_proba (outlier handling as the reference)
+    da_status radius_compute(da_int nq, da_int d, const T *Xt, da_int ldt, T r, bool want_val,
+                             std::vector<da_int> &cnt, std::vector<long long> &start,
+                             std::vector<da_int> &idx, std::vector<T> &val, bool &squares);
+    da_status compute_proba_rnn(da_int nq, da_int d, const T *Xt, da_int ldt,
+                                std::vector<T> &proba);
+    da_status predict_reg_rnn(da_int nq, da_int d, const T *Xt, da_int ldt, T *y);
+    da_int most_frequent_label();
+    static T radius_weight(T v, bool squares);
     da_status available_classes();
 };
 
@@ -223,6 +233,53 @@ template <typename T> struct KMeans : public AlgBase {
     da_status shard_result(float *centres, da_int *labels);
     da_status shard_tc_check();
     da_status assign(const T *dC, int *dL, const int *dLprev);
+};
+
+// ---------------------------------------------------- IVF-flat (approx) ---
+// Reference: source/core/approximate_neighbors/approximate_neighbors.{hpp,cpp}
+// The coarse quantiser is this library's k-means (Lloyd, random-samples
+// initialisation, one run) on the GPU; the coarse probe and the assignment of
+// added rows are GPU kNN searches over the centroids (squared GEMM-form
+// distances); the inverted lists are one list-ordered device array scanned by
+// launch_ivf_scan.
+template <typename T> struct IVF : public AlgBase {
+    // options read at train (approximate_neighbors.cpp:233-274)
+    da_int n_list = 1, n_probe = 1, max_iter = 10, seed = 0, algo = 0, metric = 1;
+    da_int internal_seed = 0, kmeans_iter = 0;
+    T train_fraction = T(1);
+    bool train_data_set = false, data_added = false;
+    // training data (user memory)
+    da_int n_samples = 0, n_features = 0, ldx_train = 0;
+    const T *X_train = nullptr;
+    da_order data_order = column_major;
+    // the index: centroids (row-major n_list x d), per-list rows (row-major),
+    // their squared norms and global indices, in insertion order
+    std::vector<T> centroids;
+    std::vector<std::vector<T>> list_rows, list_norms;
+    std::vector<std::vector<da_int>> list_ids;
+    std::vector<da_int> list_sizes;
+    da_int n_index = 0;
+    std::unique_ptr<NN<T>> coarse; // kNN over the centroids
+    // device copy of the lists (rebuilt after every add)
+    int ld = 0;
+    bool lists_on_device = false;
+    DevBuf dX, dXn, dGid, dOff, dQ, dQn, dProbe, dOutD, dOutI, dStage;
+
+    IVF(ErrorRecord *e, CudaCtx *c, bool single);
+    void refresh() override {}
+    da_status check_options_update();
+    da_status set_training_data(da_int n, da_int d, const T *X, da_int ldx);
+    da_status train();
+    da_status add(da_int n, da_int d, const T *X, da_int ldx);
+    da_status train_and_add();
+    da_status kneighbors(da_int nq, da_int d, const T *Xt, da_int ldt, da_int *n_ind, T *n_dist,
+                         da_int k, da_int return_distance);
+    da_status get_result(da_result q, da_int *dim, double *out) override;
+    da_status get_result(da_result q, da_int *dim, float *out) override;
+    da_status get_result_int(da_result q, da_int *dim, da_int *out) override;
+    da_status result_values(da_result q, da_int *dim, T *out);
+    da_status make_coarse();
+    da_status upload_lists();
 };
 
 } // namespace b200

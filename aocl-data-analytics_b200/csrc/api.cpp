@@ -73,9 +73,12 @@ template <typename T> NN<T> *as_nn(da_handle h) {
 template <typename T> KMeans<T> *as_km(da_handle h) {
     return dynamic_cast<KMeans<T> *>(h->alg.get());
 }
+template <typename T> IVF<T> *as_ivf(da_handle h) {
+    return dynamic_cast<IVF<T> *>(h->alg.get());
+}
 
-// da_handle_init (da_handle_public.cpp:34-197): only the two handle types of
-// this library's path are accepted.
+// da_handle_init (da_handle_public.cpp:34-197): only the handle types of
+// this library's path (kNN, k-means, IVF-flat) are accepted.
 da_status handle_init(da_handle *handle, da_handle_type type, da_precision prec) {
     if (handle == nullptr) return da_status_invalid_input;
     *handle = nullptr;
@@ -97,6 +100,10 @@ da_status handle_init(da_handle *handle, da_handle_type type, da_precision prec)
         case da_handle_kmeans:
             if (single) h->alg.reset(new KMeans<float>(&h->err, &h->cuda, true));
             else h->alg.reset(new KMeans<double>(&h->err, &h->cuda, false));
+            break;
+        case da_handle_approx_nn:
+            if (single) h->alg.reset(new IVF<float>(&h->err, &h->cuda, true));
+            else h->alg.reset(new IVF<double>(&h->err, &h->cuda, false));
             break;
         case da_handle_uninitialized:
             break;
@@ -135,6 +142,20 @@ da_status handle_init(da_handle *handle, da_handle_type type, da_precision prec)
             return (h)->err.error(da_status_invalid_handle_type,                              \
                                   "handle was not initialized with "                          \
                                   "handle_type=da_handle_kmeans or handle is invalid.");      \
+        return _a->call;                                                                      \
+    } while (0)
+
+#define IVF_CALL(T, h, call)                                                                  \
+    do {                                                                                      \
+        if (!(h)) return da_status_handle_not_initialized;                                    \
+        (h)->err.clear();                                                                     \
+        da_status _s = check_precision<T>(h);                                                 \
+        if (_s != da_status_success) return _s;                                               \
+        auto *_a = as_ivf<T>(h);                                                              \
+        if (!_a)                                                                              \
+            return (h)->err.error(da_status_invalid_handle_type,                              \
+                                  "handle was not initialized with "                          \
+                                  "handle_type=da_handle_approx_nn or handle is invalid.");   \
         return _a->call;                                                                      \
     } while (0)
 
@@ -511,6 +532,36 @@ da_status da_nn_radius_neighbors_d(da_handle h, da_int nq, da_int d, const doubl
 da_status da_nn_radius_neighbors_s(da_handle h, da_int nq, da_int d, const float *X, da_int ldx,
                                    float radius, da_int rd, da_int sort) {
     NN_CALL(float, h, radius_neighbors(nq, d, X, ldx, radius, rd, sort));
+}
+
+// IVF-flat (approximate_neighbors_public.cpp:30-127)
+da_status da_approx_nn_set_training_data_d(da_handle h, da_int n, da_int d, const double *X,
+                                           da_int ldx) {
+    IVF_CALL(double, h, set_training_data(n, d, X, ldx));
+}
+da_status da_approx_nn_set_training_data_s(da_handle h, da_int n, da_int d, const float *X,
+                                           da_int ldx) {
+    IVF_CALL(float, h, set_training_data(n, d, X, ldx));
+}
+da_status da_approx_nn_train_d(da_handle h) { IVF_CALL(double, h, train()); }
+da_status da_approx_nn_train_s(da_handle h) { IVF_CALL(float, h, train()); }
+da_status da_approx_nn_add_d(da_handle h, da_int n, da_int d, const double *X, da_int ldx) {
+    IVF_CALL(double, h, add(n, d, X, ldx));
+}
+da_status da_approx_nn_add_s(da_handle h, da_int n, da_int d, const float *X, da_int ldx) {
+    IVF_CALL(float, h, add(n, d, X, ldx));
+}
+da_status da_approx_nn_train_and_add_d(da_handle h) { IVF_CALL(double, h, train_and_add()); }
+da_status da_approx_nn_train_and_add_s(da_handle h) { IVF_CALL(float, h, train_and_add()); }
+da_status da_approx_nn_kneighbors_d(da_handle h, da_int nq, da_int d, const double *X,
+                                    da_int ldx, da_int *n_ind, double *n_dist, da_int k,
+                                    da_int rd) {
+    IVF_CALL(double, h, kneighbors(nq, d, X, ldx, n_ind, n_dist, k, rd));
+}
+da_status da_approx_nn_kneighbors_s(da_handle h, da_int nq, da_int d, const float *X,
+                                    da_int ldx, da_int *n_ind, float *n_dist, da_int k,
+                                    da_int rd) {
+    IVF_CALL(float, h, kneighbors(nq, d, X, ldx, n_ind, n_dist, k, rd));
 }
 da_status da_nn_classes_d(da_handle h, da_int *nc, da_int *c) { NN_CALL(double, h, classes_api(nc, c)); }
 da_status da_nn_classes_s(da_handle h, da_int *nc, da_int *c) { NN_CALL(float, h, classes_api(nc, c)); }

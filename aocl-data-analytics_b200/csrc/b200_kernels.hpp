@@ -230,6 +230,20 @@ cudaError_t launch_kmeans_finalize_shards(int k, int d, int ld, const long long 
 // Raises (never lowers) func's dynamic shared-memory limit on the current
 // device, once per size (thread-safe).
 cudaError_t ensure_smem_limit(const void *func, size_t smem);
+
+// ------------------------------------------------------------ IVF-flat ---
+// Scan of the probed inverted lists (squared GEMM-form distances, exact
+// top-k in (distance, global index) order).  X: list-ordered rows (ld a
+// multiple of 4), xn their squared norms, gid their global indices, loff the
+// n_list + 1 row offsets of the lists; probe: n_probe list ids per query.
+// Outputs q-major (q * k + r): index -1 / distance +inf for empty slots,
+// square root of non-negative values when take_sqrt.
+size_t ivf_scan_smem(int k, bool fp64);
+template <typename T>
+cudaError_t launch_ivf_scan(const T *Q, const T *qn, int ld, int nq, const int *probe,
+                            int n_probe, const long long *loff, const T *X, const T *xn,
+                            const int *gid, int k, int take_sqrt, T *out_d, int *out_i,
+                            cudaStream_t s);
 // Squared row norms of the centres (sequential fma chain over features).
 template <typename T>
 cudaError_t launch_centre_norms(const T *C, int ldc, int k, int d, T *out, cudaStream_t s);

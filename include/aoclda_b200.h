@@ -115,7 +115,9 @@ enum da_result_ {
     da_nn_radius_neighbors_indices = 603,
     da_nn_radius_neighbors_distances = 604,
     da_nn_radius_neighbors_indices_index = 605,
-    da_nn_radius_neighbors_distances_index = 606
+    da_nn_radius_neighbors_distances_index = 606,
+    da_approx_nn_cluster_centroids = 801,
+    da_approx_nn_list_sizes = 802
 };
 typedef enum da_result_ da_result;
 
@@ -276,6 +278,42 @@ da_status da_nn_regressor_predict_d(da_handle handle, da_int n_queries, da_int n
 da_status da_nn_regressor_predict_s(da_handle handle, da_int n_queries, da_int n_features,
                                     const float *X_test, da_int ldx_test, float *y_test,
                                     da_nn_search_mode search_mode);
+
+/* ======================================================================== */
+/* IVF-flat approximate neighbours (handle type da_handle_approx_nn; options  */
+/* "n_list", "n_probe", "k-means_iter", "seed", "train fraction",            */
+/* "number of neighbors", "algorithm", "metric": euclidean / sqeuclidean)    */
+/* ======================================================================== */
+/* source/include/aoclda_approximate_neighbors.h:64 */
+da_status da_approx_nn_set_training_data_d(da_handle handle, da_int n_samples,
+                                           da_int n_features, const double *X_train,
+                                           da_int ldx_train);
+/* source/include/aoclda_approximate_neighbors.h:68 */
+da_status da_approx_nn_set_training_data_s(da_handle handle, da_int n_samples,
+                                           da_int n_features, const float *X_train,
+                                           da_int ldx_train);
+/* source/include/aoclda_approximate_neighbors.h:98 */
+da_status da_approx_nn_train_d(da_handle handle);
+/* source/include/aoclda_approximate_neighbors.h:100 */
+da_status da_approx_nn_train_s(da_handle handle);
+/* source/include/aoclda_approximate_neighbors.h:127 */
+da_status da_approx_nn_add_d(da_handle handle, da_int n_samples_add, da_int n_features,
+                             const double *X_add, da_int ldx_add);
+/* source/include/aoclda_approximate_neighbors.h:130 */
+da_status da_approx_nn_add_s(da_handle handle, da_int n_samples_add, da_int n_features,
+                             const float *X_add, da_int ldx_add);
+/* source/include/aoclda_approximate_neighbors.h:152 */
+da_status da_approx_nn_train_and_add_d(da_handle handle);
+/* source/include/aoclda_approximate_neighbors.h:154 */
+da_status da_approx_nn_train_and_add_s(da_handle handle);
+/* source/include/aoclda_approximate_neighbors.h:184 */
+da_status da_approx_nn_kneighbors_d(da_handle handle, da_int n_queries, da_int n_features,
+                                    const double *X_test, da_int ldx_test, da_int *n_ind,
+                                    double *n_dist, da_int k, da_int return_distance);
+/* source/include/aoclda_approximate_neighbors.h:188 */
+da_status da_approx_nn_kneighbors_s(da_handle handle, da_int n_queries, da_int n_features,
+                                    const float *X_test, da_int ldx_test, da_int *n_ind,
+                                    float *n_dist, da_int k, da_int return_distance);
 
 /* ======================================================================== */
 /* k-means (Lloyd)                                                           */

@@ -124,6 +124,153 @@ def radius(X, Q, r, metric="euclidean", p=2.0, sort=False, kc=None):
     return out
 
 
+def _radius_weights(dist, weights, dt):
+    """get_weights (nearest_neighbors.cpp:1021-1033): 1, or 1 / distance with
+    1 at distance <= eps."""
+    if weights == "uniform":
+        return [dt.type(1)] * len(dist)
+    eps = np.finfo(dt).eps
+    return [dt.type(1) if v <= eps else dt.type(1) / v for v in dist]
+
+
+def _most_frequent(y):
+    """most_frequent_element (nearest_neighbors.cpp:1037-1058): ties to the
+    smallest label."""
+    vals, cnt = np.unique(np.asarray(y), return_counts=True)
+    return int(vals[np.argmax(cnt)])
+
+
+def radius_predict_proba(X, y, Q, r, metric="euclidean", p=2.0, weights="uniform",
+                         outlier="none", outlier_label=0):
+    """Radius-mode class probabilities (predict_proba_compute_rnn,
+    nearest_neighbors.cpp:1280-1479): per query, per class (sorted labels),
+    the weights of its radius neighbours in index order, divided by their sum
+    over the classes.  Returns (proba[nq, nc], warning); raises
+    LookupError(query) where the reference fails (outlier "none", a query
+    without neighbours).  Under "manual" the outlier label's column gets 1
+    (the reference indexes that row by the label's value, which coincides for
+    labels 0..nc-1)."""
+    dt = np.asarray(X).dtype
+    classes = np.unique(np.asarray(y))
+    nc = len(classes)
+    pos = {int(c): i for i, c in enumerate(classes)}
+    mf = _most_frequent(y) if outlier == "most frequent" else None
+    mi = pos.get(int(outlier_label), -1)
+    proba = np.zeros((len(Q), nc), dtype=dt)
+    warn = False
+    for q, (idx, dist) in enumerate(radius(X, Q, r, metric, p)):
+        if len(idx) == 0:
+            if outlier == "none":
+                raise LookupError(q)
+            if outlier == "manual":
+                warn = True
+                if mi != -1:
+                    proba[q, mi] = 1
+            else:
+                proba[q, pos[mf]] = 1
+            continue
+        w = _radius_weights(dist, weights, dt)
+        acc = [dt.type(0)] * nc
+        for j, i in enumerate(idx):
+            c = pos[int(y[i])]
+            acc[c] = dt.type(acc[c] + w[j])
+        den = dt.type(0)
+        for c in range(nc):
+            den = dt.type(den + acc[c])
+        for c in range(nc):
+            proba[q, c] = dt.type(acc[c] / den)
+    return proba, warn and outlier == "manual" and mi == -1
+
+
+def radius_predict(X, y, Q, r, metric="euclidean", p=2.0, weights="uniform", outlier="none",
+                   outlier_label=0):
+    """Radius-mode labels (nearest_neighbors.cpp:1540-1603): the first largest
+    probability's class; with outlier handling an all-zero row takes the
+    outlier label or the most frequent label."""
+    proba, _ = radius_predict_proba(X, y, Q, r, metric, p, weights, outlier, outlier_label)
+    classes = np.unique(np.asarray(y))
+    best = np.argmax(np.abs(proba), axis=1)
+    lab = classes[best].astype(np.int32)
+    if outlier != "none":
+        fill = outlier_label if outlier == "manual" else _most_frequent(y)
+        lab[proba[np.arange(len(Q)), best] == 0] = fill
+    return lab
+
+
+def radius_predict_reg(X, t, Q, r, metric="euclidean", p=2.0, weights="uniform", outlier="none",
+                       outlier_target=0.0):
+    """Radius-mode regression (predict_targets_rnn, nearest_neighbors.cpp:
+    1763-1909): the mean target of the radius neighbours, or their weighted
+    mean; a query without neighbours takes the mean training target ("most
+    frequent") or the outlier target ("manual"), or fails ("none": raises
+    LookupError(query)).  Returns (y, warning)."""
+    dt = np.asarray(X).dtype
+    t = np.asarray(t, dtype=dt)
+    out = np.zeros(len(Q), dtype=dt)
+    warn = False
+    for q, (idx, dist) in enumerate(radius(X, Q, r, metric, p)):
+        if len(idx) == 0:
+            if outlier == "none":
+                raise LookupError(q)
+            if outlier == "most frequent":
+                out[q] = t.astype(np.float64).mean()
+            else:
+                warn = True
+                out[q] = outlier_target
+            continue
+        w = _radius_weights(dist, weights, dt)
+        num = den = dt.type(0)
+        for j, i in enumerate(idx):
+            num = dt.type(num + t[i] * w[j])
+            den = dt.type(den + w[j])
+        out[q] = num / den
+    return out, warn
+
+
+def _gemm_sq(A, B):
+    """|a|^2 + |b|^2 - 2 a.b in fp64 (the GEMM form of the squared euclidean
+    distance used throughout the IVF-flat index)."""
+    A = np.asarray(A, dtype=np.float64)
+    B = np.asarray(B, dtype=np.float64)
+    return (A * A).sum(1)[:, None] + (B * B).sum(1)[None, :] - 2.0 * A @ B.T
+
+
+def ivf_lists(C, X):
+    """add_ivfflat (approximate_neighbors.cpp:565-842): every row joins the
+    list of its nearest centroid (first minimum), after the rows already
+    there.  Returns the list of every row."""
+    return np.argmin(_gemm_sq(X, C), axis=1).astype(np.int32)
+
+
+def ivf_kneighbors(C, X, Q, k, n_probe, metric="sqeuclidean", lists=None):
+    """IVF-flat search (approximate_neighbors.cpp:971-1344): per query the
+    n_probe nearest centroids (lower index on ties), then the k nearest index
+    rows of those lists in (distance, index) order; index -1 / distance +inf
+    where the lists hold fewer than k rows; euclidean returns the square root
+    of non-negative values.  Distances in fp64.  Returns (ind, dist, probes),
+    q-major."""
+    lists = ivf_lists(C, X) if lists is None else lists
+    dc = _gemm_sq(Q, C)
+    nq = len(Q)
+    ind = np.full((nq, k), -1, dtype=np.int32)
+    dist = np.full((nq, k), np.inf)
+    probes = np.zeros((nq, n_probe), dtype=np.int32)
+    for q in range(nq):
+        pr = np.lexsort((np.arange(len(C)), dc[q]))[:n_probe]
+        probes[q] = pr
+        rows = np.nonzero(np.isin(lists, pr))[0]
+        if len(rows) == 0:
+            continue
+        dq = _gemm_sq(Q[q:q + 1], X[rows])[0]
+        o = np.lexsort((rows, dq))[:k]
+        ind[q, :len(o)] = rows[o]
+        dist[q, :len(o)] = dq[o]
+    if metric == "euclidean":
+        pos = dist >= 0
+        dist[pos] = np.sqrt(dist[pos])
+    return ind, dist, probes
+
+
 def kmeans_assign(X, Cn):
     X = np.ascontiguousarray(X)
     dt = X.dtype

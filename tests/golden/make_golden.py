@@ -14,6 +14,16 @@ It converts, without retyping any value:
     (X_train/X_test at :450-464, expected indices and distances at :97-144,
     radius-5 neighbours at :147-160),
     parsed from the C++ initialiser lists, into nn_small.npz;
+  * the radius-mode predict expectations: those of the same hand problem with
+    the "radius" option 21 (get_proba_radius / get_labels_radius /
+    get_targets_radius, nearest_neighbors_tests.hpp:317-424), and the
+    OutlierTesting and AccuracyTestingZeroData_radius cases of
+    nearest_neighbors_public.cpp (:337-432, :462-608), into
+    nn_radius_predict.npz;
+  * the squared-euclidean functionality cases of the IVF-flat tests
+    (tests/unit_tests/approximate_neighbors/ann_tests.hpp:395-1260: data,
+    n_list / n_probe / k, storage order, leading dimensions, expected
+    neighbour indices and squared distances), into ann_functionality.npz;
   * the Lloyd "larger data matrix" k-means case of
     tests/unit_tests/kmeans/kmeans_test_data.hpp:444-526 into kmeans_lloyd80.npz.
 The d=130 set cannot be converted: its inputs are absent from the tree.
@@ -104,6 +114,109 @@ def nn_small():
         kind4=kinds[1].astype(np.int32), kdist4=kdists[1])
 
 
+def _values(body):
+    out = []
+    for v in body.replace("\n", " ").split(","):
+        v = v.strip()
+        if v:
+            out.append(np.nan if "quiet_NaN" in v else float(v))
+    return np.array(out)
+
+
+def assigned_lists(text, name):
+    """Initialisers of `name` in declarations and assignments: `name{...}`,
+    `name = {...}`, `name = std::vector<T>({...})`, in source order."""
+    pat = (r"\b" + re.escape(name) +
+           r"\s*(?:=\s*)?(?:std::vector<[^>]*>\s*\(\s*)?\{([^{}]*)\}")
+    return [_values(m.group(1)) for m in re.finditer(pat, text)]
+
+
+def nn_radius_predict():
+    hpp = open(os.path.join(UT, "nearest_neighbors", "nearest_neighbors_tests.hpp")).read()
+    cpp = open(os.path.join(UT, "nearest_neighbors", "nearest_neighbors_public.cpp")).read()
+    out = {}
+    # hand problem, "radius" option 21: uniform / distance x euclidean / squared
+    rc = re.search(r"T radius_constructor = ([0-9.]+);", hpp[hpp.index("get_targets_radius"):])
+    out["hand_radius"] = np.array([float(rc.group(1))])
+    for fn, name, key in (("get_proba_radius", "proba", "proba"),
+                          ("get_labels_radius", "expected_labels_radius", "labels"),
+                          ("get_targets_radius", "expected_targets_radius", "targets")):
+        blk = hpp[hpp.index("void " + fn):]
+        blk = blk[:blk.index("template <typename T>")]
+        lists = init_lists(blk, name)
+        assert len(lists) == 4, (fn, len(lists))
+        for (w, m), v in zip((("uniform", "euc"), ("uniform", "sq"), ("distance", "euc"),
+                              ("distance", "sq")), lists):
+            out[f"hand_{key}_{w}_{m}"] = v
+    # OutlierTesting: radius 4, weights distance; most frequent, manual (-999, -123),
+    # manual (1, NaN)
+    blk = cpp[cpp.index("TYPED_TEST(NearestNeighborsTest, OutlierTesting)"):]
+    blk = blk[:blk.index("TYPED_TEST(", 10)]
+    one = lambda n: init_lists(blk, n)[0]
+    out.update(out_X_train=one("X_train").reshape(3, 6).T.copy(),  # column-major 6 x 3
+               out_X_test=one("X_test").reshape(3, 3).T.copy(),
+               out_y_class=one("y_train_class").astype(np.int32),
+               out_y_reg=one("y_train_regression"))
+    for name, key in (("expected_targets", "targets"), ("expected_proba", "proba"),
+                      ("expected_labels", "labels")):
+        lists = assigned_lists(blk, name)
+        assert len(lists) == 3, (name, len(lists))
+        for i, v in enumerate(lists):
+            out[f"out_{key}_{i}"] = v
+    # AccuracyTestingZeroData_radius: all-zero rows, radius 0.5, weights distance
+    blk = cpp[cpp.index("AccuracyTestingZeroData_radius"):]
+    blk = blk[:blk.index("TYPED_TEST(")]
+    out.update(zero_y_class=init_lists(blk, "y_train_class")[0].astype(np.int32),
+               zero_y_reg=init_lists(blk, "y_train_regression")[0],
+               zero_proba=assigned_lists(blk, "expected_proba")[0],
+               zero_labels=assigned_lists(blk, "expected_labels")[0].astype(np.int32),
+               zero_target=np.array([float(re.search(
+                   r"expected_targets\(n_queries, ([0-9.]+)\)", blk).group(1))]))
+    np.savez_compressed(os.path.join(OUT, "nn_radius_predict.npz"), **out)
+
+
+def ann_functionality():
+    text = open(os.path.join(UT, "approximate_neighbors", "ann_tests.hpp")).read()
+    out, names = {}, []
+    for m in re.finditer(r"template <typename T> void (\w+)\(std::vector<ANNParamType<T>> &params\) \{",
+                         text):
+        body = text[m.end():]
+        if "params.push_back(test);" not in body:
+            continue
+        body = body[:body.index("params.push_back(test);")]
+        ctor = re.search(r'ANNParamType<T> test\((\d+), (\d+), (\d+), "([^"]+)", "([^"]+)", "([^"]+)"\)',
+                         body)
+        if ctor is None or ctor.group(4) != "sqeuclidean":
+            continue
+        nlist, nprobe, k = (int(ctor.group(i)) for i in (1, 2, 3))
+        vals = {"n_features": None, "n_samples": None, "n_queries": None, "ldx_train": None,
+                "ldx_test": None, "kmeans_iter": 10, "train_fraction": 1.0, "seed": 0}
+        for a in re.finditer(r"test\.(\w+) = ([^;]+);", body):
+            key, expr = a.group(1), a.group(2).strip()
+            if key not in vals:
+                continue
+            ref = re.fullmatch(r"test\.(\w+)", expr)
+            vals[key] = vals[ref.group(1)] if ref else float(expr)
+        lists = {n: assigned_lists(body, n) for n in ("X_train", "X_test", "expected_kind",
+                                                      "expected_kdist")}
+        if not lists["X_train"] or not lists["X_test"] or not lists["expected_kdist"]:
+            continue
+        i = len(names)
+        names.append(m.group(1))
+        row = ctor.group(6) == "row-major"
+        out[f"c{i}_meta"] = np.array([nlist, nprobe, k, vals["n_features"], vals["n_samples"],
+                                      vals["n_queries"], vals["ldx_train"], vals["ldx_test"],
+                                      vals["kmeans_iter"], int(row), vals["train_fraction"],
+                                      vals["seed"]], dtype=np.float64)
+        out[f"c{i}_X_train"] = lists["X_train"][0]
+        out[f"c{i}_X_test"] = lists["X_test"][0]
+        out[f"c{i}_kdist"] = lists["expected_kdist"][0]
+        if lists["expected_kind"]:
+            out[f"c{i}_kind"] = lists["expected_kind"][0].astype(np.int32)
+    out["names"] = np.array(names)
+    np.savez_compressed(os.path.join(OUT, "ann_functionality.npz"), **out)
+
+
 def kmeans_lloyd80():
     text = open(os.path.join(UT, "kmeans", "kmeans_test_data.hpp")).read()
     start = text.index("GetLargeBaseData")
@@ -126,6 +239,8 @@ if __name__ == "__main__":
     nn_large(2092, 2071, 5)
     nn_large(2125, 2068, 20)
     nn_small()
+    nn_radius_predict()
+    ann_functionality()
     kmeans_lloyd80()
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):

@@ -130,3 +130,106 @@ def test_oracle_radius_hand_problem(orc):
             np.testing.assert_allclose(got[q][1], z[pre + "_dist"][o:o + c],
                                        rtol=40 * np.finfo(float).eps)
             o += c
+
+
+@pytest.mark.parametrize("weights", ["uniform", "distance"])
+@pytest.mark.parametrize("group", ["euc", "sq"])
+def test_oracle_radius_predict_hand_problem(orc, weights, group):
+    """Radius-mode predict of the hand problem with the "radius" option 21
+    (the reference's get_proba_radius / get_labels_radius /
+    get_targets_radius)."""
+    z, g = golden("nn_small.npz"), golden("nn_radius_predict.npz")
+    r = float(g["hand_radius"][0])
+    metric = {"euc": "euclidean", "sq": "sqeuclidean"}[group]
+    X, Q, y, t = z["X_train"], z["X_test"], z["y_class"], z["y_reg"]
+    pr, warn = orc.radius_predict_proba(X, y, Q, r, metric, weights=weights)
+    want = g[f"hand_proba_{weights}_{group}"].reshape(3, 3).T  # column-major n_q x n_classes
+    np.testing.assert_allclose(pr, want, rtol=100 * np.finfo(float).eps, atol=1e-15)
+    assert not warn
+    lab = orc.radius_predict(X, y, Q, r, metric, weights=weights)
+    np.testing.assert_array_equal(lab, g[f"hand_labels_{weights}_{group}"].astype(np.int32))
+    tg, _ = orc.radius_predict_reg(X, t, Q, r, metric, weights=weights)
+    np.testing.assert_allclose(tg, g[f"hand_targets_{weights}_{group}"],
+                               rtol=100 * np.finfo(float).eps)
+
+
+def test_oracle_radius_predict_outliers(orc):
+    """The reference's OutlierTesting: radius 4, distance weights; query 2
+    has no neighbour.  "most frequent", then "manual" with label -999 (not a
+    training label: zero probabilities and a warning) and target -123, then
+    "manual" with label 1 and target NaN."""
+    g = golden("nn_radius_predict.npz")
+    X, Q, y, t = g["out_X_train"], g["out_X_test"], g["out_y_class"], g["out_y_reg"]
+    tol = 10 * np.finfo(float).eps
+    cases = (("most frequent", 0, 0.0, False, False),
+             ("manual", -999, -123.0, True, True),
+             ("manual", 1, np.nan, False, True))
+    for i, (oh, lab_o, tgt_o, proba_warn, reg_warn) in enumerate(cases):
+        pr, w = orc.radius_predict_proba(X, y, Q, 4.0, weights="distance", outlier=oh,
+                                         outlier_label=lab_o)
+        np.testing.assert_allclose(pr, g[f"out_proba_{i}"].reshape(3, 3).T, rtol=tol, atol=tol)
+        assert w == proba_warn
+        lab = orc.radius_predict(X, y, Q, 4.0, weights="distance", outlier=oh,
+                                 outlier_label=lab_o)
+        np.testing.assert_array_equal(lab, g[f"out_labels_{i}"].astype(np.int32))
+        tg, w = orc.radius_predict_reg(X, t, Q, 4.0, weights="distance", outlier=oh,
+                                       outlier_target=tgt_o)
+        np.testing.assert_allclose(tg, g[f"out_targets_{i}"], rtol=tol, equal_nan=True)
+        assert w == reg_warn
+    with pytest.raises(LookupError):
+        orc.radius_predict_proba(X, y, Q, 4.0, weights="distance")
+
+
+def test_oracle_radius_predict_zero_rows(orc):
+    """AccuracyTestingZeroData_radius: every distance is 0, so every weight
+    of weights="distance" is 1."""
+    g = golden("nn_radius_predict.npz")
+    X, Q = np.zeros((4, 3)), np.zeros((3, 3))
+    pr, _ = orc.radius_predict_proba(X, g["zero_y_class"], Q, 0.5, weights="distance")
+    np.testing.assert_allclose(pr, g["zero_proba"].reshape(3, 3).T, rtol=1e-15)
+    lab = orc.radius_predict(X, g["zero_y_class"], Q, 0.5, weights="distance")
+    np.testing.assert_array_equal(lab, g["zero_labels"])
+    tg, _ = orc.radius_predict_reg(X, g["zero_y_reg"], Q, 0.5, weights="distance")
+    np.testing.assert_allclose(tg, np.full(3, g["zero_target"][0]), rtol=100 * np.finfo(float).eps)
+
+
+def ann_case(z, i):
+    """One IVF-flat functionality case of the reference: options, the
+    training rows and queries as n x d arrays, and the expected neighbours
+    as n_queries x k arrays (indices None where the reference checks only
+    their validity)."""
+    nl, npb, k, d, n, nq, ldx, ldq, it, row, frac, seed = z[f"c{i}_meta"]
+    nl, npb, k, d, n, nq, ldx, ldq, it, row, seed = map(int, (nl, npb, k, d, n, nq, ldx, ldq, it,
+                                                              row, seed))
+
+    def mat(flat, rows, ld):
+        flat = np.asarray(flat)
+        if row:
+            return flat.reshape(-1, ld)[:rows, :d].copy()
+        return flat[:ld * d].reshape(d, ld).T[:rows, :].copy()
+
+    X, Q = mat(z[f"c{i}_X_train"], n, ldx), mat(z[f"c{i}_X_test"], nq, ldq)
+    shape = (nq, k) if row else (k, nq)
+    wd = z[f"c{i}_kdist"].reshape(shape)
+    wi = z[f"c{i}_kind"].reshape(shape) if f"c{i}_kind" in z.files else None
+    if not row:
+        wd = wd.T
+        wi = None if wi is None else wi.T
+    opts = dict(n_list=nl, n_probe=npb, k=k, kmeans_iter=it, row=bool(row),
+                train_fraction=float(frac), seed=seed)
+    return opts, X, Q, wi, wd
+
+
+def test_oracle_ivf_functionality_cases(orc):
+    """The reference's IVF-flat functionality cases: their expected
+    neighbours are the exact ones, which the oracle's search reproduces with
+    every list probed."""
+    z = golden("ann_functionality.npz")
+    for i in range(len(z["names"])):
+        o, X, Q, wi, wd = ann_case(z, i)
+        C = X.mean(0, keepdims=True)
+        ind, dist, _ = orc.ivf_kneighbors(C, X, Q, o["k"], 1)
+        tol = 3000 * np.finfo(float).eps
+        np.testing.assert_allclose(dist, wd, rtol=tol, atol=tol, err_msg=str(z["names"][i]))
+        if wi is not None:
+            np.testing.assert_array_equal(ind, wi, err_msg=str(z["names"][i]))
