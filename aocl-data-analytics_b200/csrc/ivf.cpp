@@ -318,11 +318,12 @@ da_status IVF<T>::kneighbors(da_int nq, da_int d, const T *Xt, da_int ldt, da_in
     B200_TRY(cudaMemcpyAsync(dProbe.p, pr.data(), pr.size() * sizeof(int), cudaMemcpyHostToDevice,
                              st),
              "upload of the probes");
-    B200_TRY(launch_ivf_scan<T>(dQ.as<T>(), dQn.as<T>(), ld, (int)nq, dProbe.as<int>(),
-                                (int)n_probe, dOff.as<long long>(), dX.as<T>(), dXn.as<T>(),
-                                dGid.as<int>(), (int)k, metric == AM_EUC ? 1 : 0, dOutD.as<T>(),
-                                dOutI.as<int>(), st),
-             "list scan");
+    B200_TRY(cuda->timed("ivf_scan", [&] {
+        return launch_ivf_scan<T>(dQ.as<T>(), dQn.as<T>(), ld, (int)nq, dProbe.as<int>(),
+                                  (int)n_probe, dOff.as<long long>(), dX.as<T>(), dXn.as<T>(),
+                                  dGid.as<int>(), (int)k, metric == AM_EUC ? 1 : 0,
+                                  dOutD.as<T>(), dOutI.as<int>(), st);
+    }), "list scan");
     std::vector<int> oi(nk);
     std::vector<T> od(nk);
     B200_TRY(cudaMemcpyAsync(oi.data(), dOutI.p, nk * sizeof(int), cudaMemcpyDeviceToHost, st),

@@ -218,6 +218,8 @@ def main():
     ap.add_argument("--no-knn", action="store_true", help="skip the kNN (4.04M x 128) leg")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched k-means (512 data sets) leg")
+    ap.add_argument("--no-ivf", action="store_true",
+                    help="skip the IVF-flat approximate-neighbours leg")
     ap.add_argument("--no-serve", action="store_true",
                     help="skip the serving leg (8M x 96 index, 64 k-means models)")
     ap.add_argument("--serve-only", action="store_true",
@@ -407,6 +409,9 @@ def main():
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = run_batched(ab)
+    ivf = None
+    if rank == 0 and world == 1 and not args.no_ivf:
+        ivf = run_ivf(ab)
     serving = None
     if rank == 0 and world == 1 and not args.no_serve:
         serving = run_serving(ab)
@@ -430,6 +435,7 @@ def main():
         "knn": knn,
         "kmeans_batched": batched,
         "serving": serving,
+        "ivf_flat": ivf,
     }
     if rank == 0:
         print(json.dumps(out))
@@ -601,6 +607,88 @@ def run_knn(ab, nx=4_000_000, nq=10_000, d=128, k=100, comps=1024, seed=3, reps=
             "timing": "wall clock of one da_nn_kneighbors_s call with host arrays (best of 3)"}
     first = out[metrics[0]]
     return dict(first, **{m: out[m] for m in metrics[1:]})
+
+
+def run_ivf(ab, nx=1_000_000, nq=10_000, d=128, k=10, n_list=1024, n_probe=16, comps=1024,
+            seed=5, reps=3, cpu_queries=100):
+    """IVF-flat approximate neighbours, fp32 squared euclidean: 1,000,000 x 128
+    rows of a 1,024-component Gaussian mixture, n_list = 1,024 lists (GPU
+    k-means, 10 iterations), n_probe = 16, 10,000 queries from the mixture,
+    k = 10.  Each timed search is one da_approx_nn_kneighbors_s over all
+    queries with host arrays; recall@k against the exact GPU kNN of the same
+    rows.  Roofline of the list scan: the candidate rows it reads (each
+    query's probed lists: 4 * 128 + 8 bytes a row) over its CUDA-event time
+    -- reads that the 126 MB L2 serves count as well, so the figure can pass
+    the HBM copy bandwidth.  CPU: the oracle's search (numpy) on a sample of
+    queries, one thread of Python per query."""
+    rng = np.random.default_rng(seed)
+    means = rng.uniform(-10.0, 10.0, (comps, d)).astype(np.float32)
+    sig = rng.uniform(0.5, 2.0, comps).astype(np.float32)
+    lab = rng.integers(0, comps, nx)
+    X = means[lab] + rng.standard_normal((nx, d), dtype=np.float32) * sig[lab, None]
+    ql = rng.integers(0, comps, nq)
+    Q = means[ql] + rng.standard_normal((nq, d), dtype=np.float32) * sig[ql, None]
+    h = ab.ApproxNN("s", order=ab.ROW_MAJOR, n_list=n_list, n_probe=n_probe, seed=seed,
+                    kmeans_iter=10)
+    h.set_training_data(X)
+    t = time.perf_counter()
+    h.train()
+    train_s = time.perf_counter() - t
+    t = time.perf_counter()
+    h.add(X)
+    add_s = time.perf_counter() - t
+    h.kneighbors(Q[:256], k)
+    h.L.da_b200_set_kernel_timing(h.h, 1)
+    ts = []
+    for _ in range(reps):
+        t = time.perf_counter()
+        ind, dist = h.kneighbors(Q, k)
+        ts.append(time.perf_counter() - t)
+    ms_, n_ = h.kernel_time("ivf_scan")
+    scan_ms = ms_ / max(n_, 1)
+    sizes = h.list_sizes(n_list).astype(np.int64)
+    C = h.result(ab.APPROX_NN_CENTROIDS, n_list * d).reshape(n_list, d).astype(np.float64)
+    Qd = Q.astype(np.float64)
+    dc = (Qd * Qd).sum(1)[:, None] + (C * C).sum(1)[None] - 2.0 * Qd @ C.T
+    probes = np.argsort(dc, axis=1, kind="stable")[:, :n_probe]
+    cand = int(sizes[probes].sum())
+    bytes_ = cand * (4.0 * d + 8.0)
+    hbm, _, src = load_peaks()
+    h.close()
+    exact = ab.KNN("s", order=ab.ROW_MAJOR, metric="sqeuclidean").fit(X)
+    eind, _ = exact.kneighbors(Q, k)
+    exact.close()
+    recall = float(np.mean([len(set(a) & set(b)) / k for a, b in zip(ind, eind)]))
+    orc = _load("oracle_mod", os.path.join(ORACLE, "oracle.py"))
+    t = time.perf_counter()
+    member = np.zeros(nx, dtype=np.int32)
+    # the list of every row from the trained centroids (host, fp64), then
+    # the oracle's per-query search on a sample
+    for b in range(0, nx, 65536):
+        xb = X[b:b + 65536].astype(np.float64)
+        member[b:b + 65536] = np.argmin((xb * xb).sum(1)[:, None] + (C * C).sum(1)[None]
+                                        - 2.0 * xb @ C.T, axis=1)
+    assign_s = time.perf_counter() - t
+    t = time.perf_counter()
+    orc.ivf_kneighbors(C, X, Q[:cpu_queries], k, n_probe, "sqeuclidean", member)
+    cpu_s = time.perf_counter() - t
+    return {"workload": f"ivfflat_fp32_sqeuclidean_{nx}x{d}_nlist{n_list}_nprobe{n_probe}"
+                        f"_q{nq}_k{k}",
+            "unit": "queries/s", "qps": nq / min(ts), "train_s": train_s, "add_s": add_s,
+            "recall_at_k_vs_exact": recall, "scan_kernel_ms": scan_ms,
+            "candidates_per_query": cand / nq,
+            "roofline": {"bound": "hbm", "achieved": bytes_ / (scan_ms / 1e3) / 1e9,
+                         "peak": hbm, "unit": "GB/s",
+                         "frac": bytes_ / (scan_ms / 1e3) / 1e9 / hbm,
+                         "peak_source": src, "traffic": None,
+                         "note": "candidate-row bytes per launch; L2 hits included"},
+            "cpu_baseline": {"value": cpu_queries / cpu_s, "unit": "queries/s", "cores": 1,
+                             "kind": "port",
+                             "sample": f"{cpu_queries} queries, oracle numpy search "
+                                       f"(list assignment of the rows, {assign_s:.1f} s, "
+                                       "not included)"},
+            "timing": "wall clock of one da_approx_nn_kneighbors_s call with host arrays "
+                      "(best of 3)"}
 
 
 def run_serving(ab, nx=8_000_000, d=96, comps=2048, n_models=64, rates=(250.0, 1000.0, 2000.0),

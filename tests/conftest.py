@@ -56,3 +56,16 @@ def gpu():
 def golden(name):
     import numpy as np
     return np.load(os.path.join(GOLDEN, name))
+
+
+@pytest.fixture(scope="session")
+def da(ab):
+    """The ``aoclda`` drop-in Python package (aocl-data-analytics_b200/python)."""
+    path = os.path.join(PKG, "python")
+    if path not in sys.path:
+        sys.path.insert(0, path)
+    import aoclda
+    import aoclda.faiss
+    import aoclda.metrics
+    import aoclda.sklearn
+    return aoclda
