@@ -280,6 +280,10 @@ template <typename T> struct IVF : public AlgBase {
     da_status result_values(da_result q, da_int *dim, T *out);
     da_status make_coarse();
     da_status upload_lists();
+    // model persistence: the trained index (centroids, lists); the training
+    // array is the user's and is not saved
+    da_status save_state(ByteWriter &w) override;
+    da_status load_state(ByteReader &r) override;
 };
 
 } // namespace b200

@@ -355,7 +355,8 @@ da_status da_handle_load_model(da_handle *handle, const char *file_name) {
     r.pos = sizeof(kModelMagic);
     if (r.get<uint32_t>() != kModelVersion) return da_status_version_mismatch;
     const int32_t type = r.get<int32_t>(), prec = r.get<int32_t>();
-    if ((type != (int32_t)da_handle_nn && type != (int32_t)da_handle_kmeans) ||
+    if ((type != (int32_t)da_handle_nn && type != (int32_t)da_handle_kmeans &&
+         type != (int32_t)da_handle_approx_nn) ||
         (prec != (int32_t)da_single && prec != (int32_t)da_double))
         return da_status_invalid_file_data;
     da_handle h = nullptr;

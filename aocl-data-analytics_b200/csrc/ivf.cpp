@@ -409,6 +409,90 @@ template <typename T> da_status IVF<T>::get_result_int(da_result q, da_int *dim,
     return da_status_success;
 }
 
+// Model persistence (approximate_neighbors.cpp:1346-1432 keeps the same
+// state): the trained index -- centroids, run information and the lists in
+// insertion order.  A loaded handle searches and accepts adds like the saved
+// one; train() needs set_training_data again.
+template <typename T> da_status IVF<T>::save_state(ByteWriter &w) {
+    if (!model_trained)
+        return err->error(da_status_no_data,
+                          "No index has been trained. Please call da_approx_nn_train_s or "
+                          "da_approx_nn_train_d before saving the model.");
+    w.put<int64_t>(n_list);
+    w.put<int64_t>(n_features);
+    w.put<int64_t>(n_index);
+    w.put<int64_t>(kmeans_iter);
+    w.put<int32_t>((int32_t)algo);
+    w.put<int32_t>((int32_t)metric);
+    w.put<int32_t>((int32_t)data_order);
+    w.put<int32_t>(data_added ? 1 : 0);
+    w.put_vec(centroids.data(), centroids.size());
+    std::vector<T> rows, norms;
+    std::vector<int64_t> ids, sizes;
+    for (da_int c = 0; c < n_list; ++c) {
+        rows.insert(rows.end(), list_rows[c].begin(), list_rows[c].end());
+        norms.insert(norms.end(), list_norms[c].begin(), list_norms[c].end());
+        ids.insert(ids.end(), list_ids[c].begin(), list_ids[c].end());
+        sizes.push_back(list_sizes[c]);
+    }
+    w.put_vec(sizes.data(), sizes.size());
+    w.put_vec(ids.data(), ids.size());
+    w.put_vec(norms.data(), norms.size());
+    w.put_vec(rows.data(), rows.size());
+    return da_status_success;
+}
+
+template <typename T> da_status IVF<T>::load_state(ByteReader &r) {
+    const int64_t nl = r.get<int64_t>(), d = r.get<int64_t>(), ni = r.get<int64_t>(),
+                  it = r.get<int64_t>();
+    const int32_t al = r.get<int32_t>(), me = r.get<int32_t>(), ord = r.get<int32_t>(),
+                  added = r.get<int32_t>();
+    std::vector<T> cen = r.get_vec<T>();
+    std::vector<int64_t> sizes = r.get_vec<int64_t>(), ids = r.get_vec<int64_t>();
+    std::vector<T> norms = r.get_vec<T>(), rows = r.get_vec<T>();
+    const auto bad = [&] {
+        return err->error(da_status_invalid_file_data, "The model file is corrupted.");
+    };
+    if (!r.ok || nl < 1 || d < 1 || ni < 0 || cen.size() != (size_t)(nl * d) ||
+        sizes.size() != (size_t)nl || ids.size() != norms.size() ||
+        rows.size() != ids.size() * (size_t)d || (me != AM_EUC && me != AM_SQEUC))
+        return bad();
+    int64_t total = 0;
+    for (int64_t v : sizes) {
+        if (v < 0) return bad();
+        total += v;
+    }
+    if (total != (int64_t)ids.size() || total > ni) return bad();
+    for (int64_t v : ids)
+        if (v < 0 || v >= ni) return bad();
+    n_list = (da_int)nl;
+    n_features = (da_int)d;
+    n_index = (da_int)ni;
+    kmeans_iter = (da_int)it;
+    algo = al;
+    metric = me;
+    data_order = (da_order)ord;
+    data_added = added != 0;
+    centroids = std::move(cen);
+    list_sizes.assign((size_t)nl, 0);
+    list_rows.assign((size_t)nl, {});
+    list_norms.assign((size_t)nl, {});
+    list_ids.assign((size_t)nl, {});
+    size_t o = 0;
+    for (da_int c = 0; c < n_list; ++c) {
+        const size_t m = (size_t)sizes[c];
+        list_sizes[c] = (da_int)m;
+        list_rows[c].assign(rows.begin() + o * d, rows.begin() + (o + m) * d);
+        list_norms[c].assign(norms.begin() + o, norms.begin() + o + m);
+        for (size_t i = 0; i < m; ++i) list_ids[c].push_back((da_int)ids[o + i]);
+        o += m;
+    }
+    train_data_set = false;
+    lists_on_device = false;
+    model_trained = true;
+    return make_coarse();
+}
+
 template struct IVF<float>;
 template struct IVF<double>;
 

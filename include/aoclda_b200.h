@@ -158,10 +158,11 @@ da_status da_handle_get_error_message(da_handle handle, char **message);
 da_status da_handle_get_error_severity(da_handle handle, da_severity *severity);
 /* source/include/aoclda_handle.h:153 */
 void da_handle_refresh(da_handle handle);
-/* source/include/aoclda_handle.h:177 -- a trained kNN (training data set)
- * or k-means (computed) handle to a file: its options and its state (kNN:
- * the training rows and labels / targets; k-means: centres, labels, run
- * information).  The file format is this library's own (a magic string,
+/* source/include/aoclda_handle.h:177 -- a trained kNN (training data set),
+ * k-means (computed) or IVF-flat (trained) handle to a file: its options and
+ * its state (kNN: the training rows and labels / targets; k-means: centres,
+ * labels, run information; IVF-flat: centroids, run information and the
+ * inverted lists).  The file format is this library's own (a magic string,
  * format version 1, handle type, precision, options, state, FNV-1a
  * checksum), not the reference's. */
 da_status da_handle_save_model(da_handle handle, const char *file_name);

@@ -44,6 +44,10 @@ def test_model_file_errors(ab, tmp_path):
     km = ab.KMeans(3, "s")
     assert L.da_handle_save_model(km.h, str(tmp_path / "km.bin").encode()) == NO_DATA
     km.close()
+    # nor an untrained IVF-flat handle
+    ivf = ab.ApproxNN("d", n_list=2)
+    assert L.da_handle_save_model(ivf.h, str(tmp_path / "ivf.bin").encode()) == NO_DATA
+    ivf.close()
     assert L.da_handle_save_model(None, b"x") == INVALID_POINTER
     # a valid file, corrupted: the checksum rejects it; another format version
     rng = np.random.default_rng(1)
