@@ -581,10 +581,13 @@ da_status NN<T>::radius_compute(da_int nq, da_int d, const T *Xt, da_int ldt, T 
     const PairwiseArgs pa{acc, post, kc, (double)p, false, true};
     for (da_int q0 = 0; q0 < nq; q0 += B) {
         const int b = (int)std::min<da_int>(B, nq - q0);
-        B200_TRY(launch_pairwise<T>(dQ.as<T>() + (size_t)q0 * ld, ld, b, dX.as<T>(), ld,
-                                    (int)n, (int)d, qn ? qn + q0 : nullptr, xn, pa, dD.as<T>(), st),
-                 "distance kernel");
-        B200_TRY(launch_radius_count<T>(dD.as<T>(), b, (int)n, n, thr, dRc.as<int>(), st), "count");
+        B200_TRY(cuda->timed("radius_distances", [&] {
+            return launch_pairwise<T>(dQ.as<T>() + (size_t)q0 * ld, ld, b, dX.as<T>(), ld, (int)n,
+                                      (int)d, qn ? qn + q0 : nullptr, xn, pa, dD.as<T>(), st);
+        }), "distance kernel");
+        B200_TRY(cuda->timed("radius_count", [&] {
+            return launch_radius_count<T>(dD.as<T>(), b, (int)n, n, thr, dRc.as<int>(), st);
+        }), "count");
         B200_TRY(cudaMemcpyAsync(cnt.data(), dRc.p, (size_t)b * sizeof(int),
                                  cudaMemcpyDeviceToHost, st), "copy");
         B200_TRY(cudaStreamSynchronize(st), "radius search");
@@ -603,8 +606,10 @@ da_status NN<T>::radius_compute(da_int nq, da_int d, const T *Xt, da_int ldt, T 
             return err->error(da_status_memory_error, "Device memory allocation failed.");
         B200_TRY(cudaMemcpyAsync(dRs.p, start.data(), (size_t)b * sizeof(long long),
                                  cudaMemcpyHostToDevice, st), "copy");
-        B200_TRY(launch_radius_emit<T>(dD.as<T>(), b, (int)n, n, thr, dRs.as<long long>(),
-                                       dRi.as<int>(), dRv.as<T>(), st), "compaction");
+        B200_TRY(cuda->timed("radius_emit", [&] {
+            return launch_radius_emit<T>(dD.as<T>(), b, (int)n, n, thr, dRs.as<long long>(),
+                                         dRi.as<int>(), dRv.as<T>(), st);
+        }), "compaction");
         idx_out.resize(base + (size_t)tot);
         if (want_val) val_out.resize(base + (size_t)tot);
         std::vector<int> ii((size_t)tot);

@@ -218,6 +218,8 @@ def main():
     ap.add_argument("--no-knn", action="store_true", help="skip the kNN (4.04M x 128) leg")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched k-means (512 data sets) leg")
+    ap.add_argument("--no-radius", action="store_true",
+                    help="skip the radius-neighbours leg")
     ap.add_argument("--no-ivf", action="store_true",
                     help="skip the IVF-flat approximate-neighbours leg")
     ap.add_argument("--no-serve", action="store_true",
@@ -409,6 +411,9 @@ def main():
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = run_batched(ab)
+    radius = None
+    if rank == 0 and world == 1 and not args.no_radius:
+        radius = run_radius(ab)
     ivf = None
     if rank == 0 and world == 1 and not args.no_ivf:
         ivf = run_ivf(ab)
@@ -436,6 +441,7 @@ def main():
         "kmeans_batched": batched,
         "serving": serving,
         "ivf_flat": ivf,
+        "radius": radius,
     }
     if rank == 0:
         print(json.dumps(out))
@@ -607,6 +613,70 @@ def run_knn(ab, nx=4_000_000, nq=10_000, d=128, k=100, comps=1024, seed=3, reps=
             "timing": "wall clock of one da_nn_kneighbors_s call with host arrays (best of 3)"}
     first = out[metrics[0]]
     return dict(first, **{m: out[m] for m in metrics[1:]})
+
+
+def run_radius(ab, nx=1_000_000, nq=10_000, d=32, comps=256, target=100, seed=6, reps=3,
+               cpu_queries=20):
+    """Radius neighbours, fp32 euclidean: 1,000,000 x 32 rows of a 256-component
+    Gaussian mixture, 10,000 queries from the mixture, the radius at which the
+    median query has 100 neighbours.  Each timed call is one
+    da_nn_radius_neighbors_s over all queries with host arrays (queries up;
+    counts, indices and distances down; results in index order).  Roofline of
+    the distance-block pipeline: every block of queries writes its distance
+    rows once and the count and compaction kernels read them once each
+    (12 bytes per (query, row) pair) over the three kernels' CUDA-event time.
+    CPU: the oracle on a sample of queries."""
+    rng = np.random.default_rng(seed)
+    means = rng.uniform(-3.0, 3.0, (comps, d)).astype(np.float32)
+    lab = rng.integers(0, comps, nx)
+    X = means[lab] + rng.standard_normal((nx, d), dtype=np.float32)
+    ql = rng.integers(0, comps, nq)
+    Q = means[ql] + rng.standard_normal((nq, d), dtype=np.float32)
+    # the radius: median over 64 queries of the distance of their 100th neighbour
+    xs = (X.astype(np.float64) ** 2).sum(1)
+    kth = []
+    for q in Q[:64].astype(np.float64):
+        d2 = xs + (q * q).sum() - 2.0 * (X @ q.astype(np.float32)).astype(np.float64)
+        kth.append(np.sqrt(max(np.partition(d2, target)[target], 0.0)))
+    r = float(np.median(kth))
+    nn = ab.KNN("s", order=ab.ROW_MAJOR).fit(X)
+    nn.radius_neighbors(Q[:64], r, True, False)
+    nn.L.da_b200_set_kernel_timing(nn.h, 1)
+    ts = []
+    for _ in range(reps):
+        t = time.perf_counter()
+        cnt, off, ind, dist = nn.radius_neighbors(Q, r, True, False)
+        ts.append(time.perf_counter() - t)
+    kern = {}
+    for name in ("radius_distances", "radius_count", "radius_emit"):
+        ms_, n_ = nn.kernel_time(name)
+        kern[name] = (ms_, n_)
+    nn.close()
+    total_ms = sum(v[0] for v in kern.values()) / reps
+    bytes_ = 12.0 * nq * (nx)
+    hbm, _, src = load_peaks()
+    orc = _load("oracle_mod", os.path.join(ORACLE, "oracle.py"))
+    t = time.perf_counter()
+    ref = orc.radius(X, Q[:cpu_queries], r)
+    cpu_s = time.perf_counter() - t
+    same = all(np.array_equal(ind[off[q]:off[q] + cnt[q]], ref[q][0]) and
+               np.array_equal(dist[off[q]:off[q] + cnt[q]], ref[q][1])
+               for q in range(cpu_queries) if cnt[q])
+    return {"workload": f"radius_fp32_euclidean_{nx}x{d}_q{nq}_median{target}neighbours",
+            "unit": "queries/s", "qps": nq / min(ts), "radius": r,
+            "neighbours_mean": float(cnt[nq]) / nq,
+            "kernel_ms_per_call": {k: v[0] / reps for k, v in kern.items()},
+            "launches_per_call": {k: v[1] // reps for k, v in kern.items()},
+            "roofline": {"bound": "hbm", "achieved": bytes_ / (total_ms / 1e3) / 1e9,
+                         "peak": hbm, "unit": "GB/s",
+                         "frac": bytes_ / (total_ms / 1e3) / 1e9 / hbm, "peak_source": src,
+                         "traffic": None,
+                         "note": "12 bytes per (query, row): distance written, read twice"},
+            "identical_to_oracle_sample": bool(same),
+            "cpu_baseline": {"value": cpu_queries / cpu_s, "unit": "queries/s", "cores": 1,
+                             "kind": "port", "sample": f"{cpu_queries} queries, oracle"},
+            "timing": "wall clock of one da_nn_radius_neighbors_s call with host arrays "
+                      "(best of 3)"}
 
 
 def run_ivf(ab, nx=1_000_000, nq=10_000, d=128, k=10, n_list=1024, n_probe=16, comps=1024,
