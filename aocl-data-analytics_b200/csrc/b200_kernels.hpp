@@ -74,9 +74,13 @@ cudaError_t launch_pairwise(const T *X, int ldx, int m, const T *Y, int ldy, int
                             const T *xn, const T *yn, const PairwiseArgs &a, T *D,
                             cudaStream_t s);
 
-// Radius neighbours from a block of distances D (rows x n, row-major, ld):
-// per row the count of D <= thr, then the ordered compaction (index order)
-// of those (column, value) pairs at out offsets start[row].
+// Radius neighbours from a block of distances D (rows x n, row-major, ld),
+// each row cut into radius_chunks(n) chunks of RADIUS_CHUNK columns (one CTA
+// each): per (row, chunk) the count of D <= thr (cnt[row * chunks + chunk]),
+// then the ordered compaction (index order) of those (column, value) pairs
+// at out offsets start[row * chunks + chunk].
+constexpr int RADIUS_CHUNK = 16384;
+int radius_chunks(int n);
 template <typename T>
 cudaError_t launch_radius_count(const T *D, int rows, int n, size_t ld, T thr, int *cnt,
                                 cudaStream_t s);

@@ -519,10 +519,12 @@ B200_INST(double)
 // pass, then an ordered compaction (block-wide exclusive scans over tiles of
 // blockDim columns), so each row's hits come out in index order.
 template <typename T>
-__global__ void radius_count_kernel(const T *D, int n, size_t ld, T thr, int *cnt) {
-    const T *row = D + (size_t)blockIdx.x * ld;
+__global__ void radius_count_kernel(const T *D, int n, size_t ld, T thr, int chunk, int *cnt) {
+    const T *row = D + (size_t)blockIdx.y * ld;
+    const int j1 = min(n, (int)(blockIdx.x + 1) * chunk);
     int c = 0;
-    for (int j = threadIdx.x; j < n; j += blockDim.x) c += row[j] <= thr ? 1 : 0;
+    for (int j = (int)blockIdx.x * chunk + threadIdx.x; j < j1; j += blockDim.x)
+        c += row[j] <= thr ? 1 : 0;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
     __shared__ int ws[32];
@@ -531,20 +533,21 @@ __global__ void radius_count_kernel(const T *D, int n, size_t ld, T thr, int *cn
     if (threadIdx.x == 0) {
         int t = 0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
-        cnt[blockIdx.x] = t;
+        cnt[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
     }
 }
 template <typename T>
-__global__ void radius_emit_kernel(const T *D, int n, size_t ld, T thr, const long long *start,
-                                   int *idx, T *val) {
-    const T *row = D + (size_t)blockIdx.x * ld;
+__global__ void radius_emit_kernel(const T *D, int n, size_t ld, T thr, int chunk,
+                                   const long long *start, int *idx, T *val) {
+    const T *row = D + (size_t)blockIdx.y * ld;
     __shared__ int ws[33];
-    long long base = start[blockIdx.x];
+    long long base = start[(size_t)blockIdx.y * gridDim.x + blockIdx.x];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int j0 = 0; j0 < n; j0 += blockDim.x) {
+    const int j1 = min(n, (int)(blockIdx.x + 1) * chunk);
+    for (int j0 = (int)blockIdx.x * chunk; j0 < j1; j0 += blockDim.x) {
         const int j = j0 + threadIdx.x;
-        const T v = j < n ? row[j] : T(0);
-        const int f = (j < n && v <= thr) ? 1 : 0;
+        const T v = j < j1 ? row[j] : T(0);
+        const int f = (j < j1 && v <= thr) ? 1 : 0;
         const unsigned b = __ballot_sync(0xffffffffu, f);
         const int inw = __popc(b & ((1u << lane) - 1u));
         if (lane == 0) ws[w] = __popc(b);
@@ -568,18 +571,21 @@ __global__ void radius_emit_kernel(const T *D, int n, size_t ld, T thr, const lo
         __syncthreads();
     }
 }
+int radius_chunks(int n) { return (n + RADIUS_CHUNK - 1) / RADIUS_CHUNK; }
 template <typename T>
 cudaError_t launch_radius_count(const T *D, int rows, int n, size_t ld, T thr, int *cnt,
                                 cudaStream_t s) {
-    if (rows <= 0) return cudaSuccess;
-    radius_count_kernel<T><<<rows, 512, 0, s>>>(D, n, ld, thr, cnt);
+    if (rows <= 0 || n <= 0) return cudaSuccess;
+    const dim3 grid(radius_chunks(n), rows);
+    radius_count_kernel<T><<<grid, 256, 0, s>>>(D, n, ld, thr, RADIUS_CHUNK, cnt);
     return cudaGetLastError();
 }
 template <typename T>
 cudaError_t launch_radius_emit(const T *D, int rows, int n, size_t ld, T thr,
                                const long long *start, int *idx, T *val, cudaStream_t s) {
-    if (rows <= 0) return cudaSuccess;
-    radius_emit_kernel<T><<<rows, 512, 0, s>>>(D, n, ld, thr, start, idx, val);
+    if (rows <= 0 || n <= 0) return cudaSuccess;
+    const dim3 grid(radius_chunks(n), rows);
+    radius_emit_kernel<T><<<grid, 256, 0, s>>>(D, n, ld, thr, RADIUS_CHUNK, start, idx, val);
     return cudaGetLastError();
 }
 template cudaError_t launch_radius_count<float>(const float *, int, int, size_t, float, int *,

@@ -547,7 +547,7 @@ da_status NN<T>::radius_compute(da_int nq, da_int d, const T *Xt, da_int ldt, T 
         break;
     }
     squares = tf == 1;
-    const T thr = rnn_squares ? r * r : r;
+    const T thr = squares ? r * r : r;
     const bool fp64 = sizeof(T) == 8;
     const int kc = opts.key("reference isa") == 1 ? (fp64 ? 32 : 64) : (fp64 ? 512 : 256);
     if (!dQ.ensure((size_t)nq * ld * sizeof(T)))
@@ -572,12 +572,15 @@ da_status NN<T>::radius_compute(da_int nq, da_int d, const T *Xt, da_int ldt, T 
     }
     // query blocks whose distance rows fit in 256 MB
     const size_t n = (size_t)n_samples;
-    const da_int B = (da_int)std::max<size_t>(1, std::min<size_t>((size_t)nq, (256u << 20) / (n * sizeof(T))));
-    if (!dD.ensure((size_t)B * n * sizeof(T)) || !dRc.ensure((size_t)B * sizeof(int)) ||
-        !dRs.ensure((size_t)B * sizeof(long long)))
+    // (at most 65,535 rows: the count / compaction grids put the rows on y)
+    const da_int B = (da_int)std::max<size_t>(
+        1, std::min<size_t>({(size_t)nq, (256u << 20) / (n * sizeof(T)), (size_t)65535}));
+    const int nch = radius_chunks((int)n);
+    if (!dD.ensure((size_t)B * n * sizeof(T)) || !dRc.ensure((size_t)B * nch * sizeof(int)) ||
+        !dRs.ensure((size_t)B * nch * sizeof(long long)))
         return err->error(da_status_memory_error, "Device memory allocation failed.");
-    std::vector<int> cnt((size_t)B);
-    std::vector<long long> start((size_t)B);
+    std::vector<int> cnt((size_t)B * nch);
+    std::vector<long long> start((size_t)B * nch);
     const PairwiseArgs pa{acc, post, kc, (double)p, false, true};
     for (da_int q0 = 0; q0 < nq; q0 += B) {
         const int b = (int)std::min<da_int>(B, nq - q0);
@@ -588,23 +591,26 @@ da_status NN<T>::radius_compute(da_int nq, da_int d, const T *Xt, da_int ldt, T 
         B200_TRY(cuda->timed("radius_count", [&] {
             return launch_radius_count<T>(dD.as<T>(), b, (int)n, n, thr, dRc.as<int>(), st);
         }), "count");
-        B200_TRY(cudaMemcpyAsync(cnt.data(), dRc.p, (size_t)b * sizeof(int),
+        B200_TRY(cudaMemcpyAsync(cnt.data(), dRc.p, (size_t)b * nch * sizeof(int),
                                  cudaMemcpyDeviceToHost, st), "copy");
         B200_TRY(cudaStreamSynchronize(st), "radius search");
+        // chunk offsets in (row, chunk) order: every row's hits stay in index order
         long long tot = 0;
-        for (int i = 0; i < b; ++i) {
-            start[i] = tot;
-            tot += cnt[i];
-        }
         const size_t base = idx_out.size();
         for (int i = 0; i < b; ++i) {
-            cnt_out[(size_t)q0 + i] = (da_int)cnt[i];
-            start_out[(size_t)q0 + i] = (long long)base + start[i];
+            start_out[(size_t)q0 + i] = (long long)base + tot;
+            long long row = 0;
+            for (int c = 0; c < nch; ++c) {
+                start[(size_t)i * nch + c] = tot;
+                tot += cnt[(size_t)i * nch + c];
+                row += cnt[(size_t)i * nch + c];
+            }
+            cnt_out[(size_t)q0 + i] = (da_int)row;
         }
         if (tot == 0) continue;
         if (!dRi.ensure((size_t)tot * sizeof(int)) || !dRv.ensure((size_t)tot * sizeof(T)))
             return err->error(da_status_memory_error, "Device memory allocation failed.");
-        B200_TRY(cudaMemcpyAsync(dRs.p, start.data(), (size_t)b * sizeof(long long),
+        B200_TRY(cudaMemcpyAsync(dRs.p, start.data(), (size_t)b * nch * sizeof(long long),
                                  cudaMemcpyHostToDevice, st), "copy");
         B200_TRY(cuda->timed("radius_emit", [&] {
             return launch_radius_emit<T>(dD.as<T>(), b, (int)n, n, thr, dRs.as<long long>(),
