@@ -101,7 +101,7 @@ def data(rng, n, nq, d, dt):
 @pytest.mark.parametrize("metric,p,radius", [("euclidean", 2.0, 2.2), ("sqeuclidean", 2.0, 4.0),
                                               ("manhattan", 2.0, 4.5), ("cosine", 2.0, 0.08),
                                               ("minkowski", 3.0, 1.9),
-                                              ("inner product", 2.0, -5.0)])
+                                              ("inner product", 2.0, 0.0)])
 @pytest.mark.parametrize("weights", ["uniform", "distance"])
 @pytest.mark.parametrize("outlier", ["manual", "most frequent"])
 @pytest.mark.parametrize("prec,order", [("s", 1), ("d", 0)])
@@ -116,8 +116,12 @@ def test_radius_predict_matches_oracle(gpu, ab, orc, metric, p, radius, weights,
     if metric == "cosine":
         Q[1] = -X[:].sum(0) / 3000 * 50
         Q[2] = Q[1]
-    if metric == "inner product":   # a zero query: every dot is 0 > radius
-        Q[1] = 0
+    if metric == "inner product":
+        # positive rows: a mixed-sign query has the rows of dot <= 0 as
+        # neighbours, a positive query none (an outlier)
+        X = (np.abs(X) + 1).astype(dt)
+        Q = rng.standard_normal(Q.shape).astype(dt)
+        Q[1], Q[2] = 1, 2
     lab_o, tgt_o = 5, -2.5
     nn = ab.KNN(prec, order=order, metric=metric, minkowski_parameter=p, weights=weights,
                 radius=radius, outlier_handling=outlier, outlier_label=lab_o,
