@@ -18,7 +18,7 @@ namespace {
 
 constexpr int IVF_THREADS = 256;
 constexpr int IVF_GROUP = 4;          // lanes per candidate row
-constexpr int IVF_BATCH = 256;        // candidates per merge round (== threads)
+constexpr int IVF_BATCH = 256;        // candidates per merge step (== threads)
 constexpr int IVF_NOID = 0x7fffffff;  // empty top-k slot
 
 template <typename T> struct V16;
