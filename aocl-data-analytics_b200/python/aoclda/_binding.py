@@ -5,6 +5,7 @@ float32 stays single precision, everything else becomes double; a
 Fortran-ordered array stays column-major, anything else is row-major."""
 import importlib.util
 import os
+import tempfile
 
 import numpy as np
 
@@ -38,3 +39,21 @@ def convert(X, prec=None, order=None):
     X = np.asfortranarray(X, dtype=dt) if order == ab.COLUMN_MAJOR else \
         np.ascontiguousarray(X, dtype=dt)
     return X, prec, order
+
+
+def dump_model(h):
+    """The bytes of da_handle_save_model for handle object `h` (pickling)."""
+    with tempfile.TemporaryDirectory() as d:
+        f = os.path.join(d, "model.bin")
+        h.save_model(f)
+        with open(f, "rb") as fh:
+            return fh.read()
+
+
+def load_model(cls, data, prec):
+    """A new handle object of class `cls` from bytes written by dump_model."""
+    with tempfile.TemporaryDirectory() as d:
+        f = os.path.join(d, "model.bin")
+        with open(f, "wb") as fh:
+            fh.write(data)
+        return cls.load_model(f, prec)

@@ -3,7 +3,7 @@
 k-means handle."""
 import numpy as np
 
-from ._binding import ab, convert
+from ._binding import ab, convert, dump_model, load_model
 
 
 class kmeans():
@@ -86,3 +86,14 @@ class kmeans():
     def predict(self, Y):
         Y = convert(Y, self._h.prec, self._h.order)[0]
         return self._h.predict(Y)
+
+    # pickling (clustering.py:282-323): the parameters and the fitted model
+    def __getstate__(self):
+        st = {k: v for k, v in self.__dict__.items() if k != "_h"}
+        st["_model"] = None if self._h is None else (dump_model(self._h), self._h.prec)
+        return st
+
+    def __setstate__(self, st):
+        model = st.pop("_model")
+        self.__dict__.update(st)
+        self._h = None if model is None else load_model(ab.KMeans, model[0], model[1])

@@ -3,7 +3,7 @@ interface (python_interface/python_package/aoclda/neighbors.py:39-800) over
 the B200 kNN, radius and IVF-flat handles."""
 import numpy as np
 
-from ._binding import ab, convert
+from ._binding import ab, convert, dump_model, load_model
 
 _MODES = {"knn": ab.KNN_SEARCH, "radius_neighbors": ab.RADIUS_SEARCH,
           "radius": ab.RADIUS_SEARCH}
@@ -159,6 +159,18 @@ class nearest_neighbors():
         self._outliers(search_mode, True)
         return self._h.predict_reg(Q, _mode(search_mode))
 
+    # pickling (neighbors.py:537-572): the parameters, the labels / targets
+    # and the handle's model file (the training rows are in it)
+    def __getstate__(self):
+        st = {k: v for k, v in self.__dict__.items() if k != "_h"}
+        st["_model"] = None if self._h is None else (dump_model(self._h), self._h.prec)
+        return st
+
+    def __setstate__(self, st):
+        model = st.pop("_model")
+        self.__dict__.update(st)
+        self._h = None if model is None else load_model(ab.KNN, model[0], model[1])
+
 
 class approximate_neighbors():
     """IVF-flat approximate neighbours (neighbors.py:578-800)."""
@@ -244,3 +256,15 @@ class approximate_neighbors():
     @property
     def kmeans_iter(self):
         return int(self._rinfo()[3])
+
+    # pickling (neighbors.py:735-765): the parameters and the trained index
+    def __getstate__(self):
+        st = {k: v for k, v in self.__dict__.items() if k not in ("_h", "_X")}
+        st["_model"] = None if self._h is None else (dump_model(self._h), self._h.prec)
+        return st
+
+    def __setstate__(self, st):
+        model = st.pop("_model")
+        self.__dict__.update(st)
+        self._X = None
+        self._h = None if model is None else load_model(ab.ApproxNN, model[0], model[1])

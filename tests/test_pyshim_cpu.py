@@ -79,3 +79,25 @@ def test_faiss_shim_checks(da):
     except ImportError:
         with pytest.raises(ImportError):
             da.faiss.patch_faiss()
+
+
+def test_nearest_neighbors_pickle(da):
+    """Pickling keeps the parameters, the labels and the handle's model
+    (training rows included): the unpickled object pickles to the same
+    model bytes."""
+    import pickle
+
+    from aoclda.neighbors import nearest_neighbors
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal((40, 4))
+    y = rng.integers(0, 3, 40)
+    nn = nearest_neighbors(n_neighbors=3, metric="manhattan", weights="distance").fit(X, y)
+    nn2 = pickle.loads(pickle.dumps(nn))
+    assert (nn2.n_neighbors, nn2.metric, nn2.weights) == (3, "manhattan", "distance")
+    np.testing.assert_array_equal(nn2.y, y)
+    assert nn2._h.get_int("number of neighbors") == 3
+    assert nn2._h.get_string("metric") == "manhattan"
+    assert nn.__getstate__()["_model"] == nn2.__getstate__()["_model"]
+    # an unfitted object pickles too
+    nn3 = pickle.loads(pickle.dumps(nearest_neighbors(n_neighbors=2)))
+    assert nn3._h is None and nn3.n_neighbors == 2

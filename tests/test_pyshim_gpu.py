@@ -132,3 +132,23 @@ def test_pairwise_distances_shim(gpu, da, orc):
     for m in ("euclidean", "sqeuclidean", "manhattan", "cosine"):
         np.testing.assert_allclose(pairwise_distances(X, Y, metric=m), orc.pairwise(X, Y, m),
                                    rtol=1e-13, atol=1e-13)
+
+
+def test_pickle_kmeans_and_ann(gpu, da):
+    """Pickled k-means and IVF-flat objects answer as the originals."""
+    import pickle
+
+    from aoclda.clustering import kmeans
+    from aoclda.neighbors import approximate_neighbors
+    rng = np.random.default_rng(6)
+    X, Q = data(rng, 4000, 50, 8)
+    km = kmeans(n_clusters=5, n_init=1, seed=2).fit(X)
+    km2 = pickle.loads(pickle.dumps(km))
+    np.testing.assert_array_equal(km2.cluster_centres, km.cluster_centres)
+    np.testing.assert_array_equal(km2.labels, km.labels)
+    np.testing.assert_array_equal(km2.predict(Q), km.predict(Q))
+    ann = approximate_neighbors(n_neighbors=4, n_list=6, n_probe=2, seed=1).train_and_add(X)
+    ann2 = pickle.loads(pickle.dumps(ann))
+    assert ann2.n_index == 4000
+    for a, b in zip(ann2.kneighbors(Q), ann.kneighbors(Q)):
+        np.testing.assert_array_equal(a, b)
