@@ -107,7 +107,7 @@ template <typename T> da_status IVF<T>::train() {
     internal_seed = seed;
     if (internal_seed == -1) {
         std::random_device rd;
-        internal_seed = std::abs((da_int)rd());
+        internal_seed = (da_int)(rd() & 0x7fffffffu); // non-negative, no abs() overflow
     }
     std::mt19937 mt((unsigned)internal_seed);
     const bool cm = data_order == column_major;
