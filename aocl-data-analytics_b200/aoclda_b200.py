@@ -157,7 +157,8 @@ class DAError(RuntimeError):
 
 
 class Handle:
-    """A da_handle of one precision ('d' or 's') and one type (HANDLE_NN / HANDLE_KMEANS)."""
+    """A da_handle of one precision ('d' or 's') and one type (HANDLE_NN / HANDLE_KMEANS /
+    HANDLE_APPROX_NN)."""
 
     def __init__(self, htype, prec="d"):
         self.L = lib()
