@@ -2,8 +2,9 @@
 
 The training set of the kNN index and the centres of the k-means models stay
 in device memory for the life of the server (one library handle per worker).
-Requests -- a kNN search (queries, k) or a k-means predict (model, queries)
--- are queued as they arrive; a kNN request with more queries than one call
+Requests -- a kNN search (queries, k), an approximate (IVF-flat) search
+(queries, k) when the server holds an IVF-flat index, or a k-means predict
+(model, queries) -- are queued as they arrive; a kNN request with more queries than one call
 takes is split into parts of at most that many (each part is searched on its
 own; the request completes with its last part).  Each worker thread
 repeatedly takes pending requests of its kind that fit its share of the
@@ -39,8 +40,8 @@ class Request:
                  "_done", "parent", "offset", "parts_left")
 
     def __init__(self, kind, queries, k=None, model=None):
-        if kind not in ("knn", "predict"):
-            raise ValueError("kind must be 'knn' or 'predict'")
+        if kind not in ("knn", "ann", "predict"):
+            raise ValueError("kind must be 'knn', 'ann' or 'predict'")
         self.kind = kind
         self.queries = np.ascontiguousarray(queries, dtype=np.float32)
         self.k = k
@@ -65,11 +66,14 @@ class Request:
 class Server:
     """kNN index X (n x d, fp32, euclidean) and k-means models given as
     {name: (training rows, initial centres)}, fitted at start-up.  `workers`
-    kNN worker threads (one handle each) and one predict worker."""
+    kNN worker threads (one handle each) and one predict worker.  With
+    `ann` = {"n_list": .., "n_probe": ..} an IVF-flat index of X (squared
+    euclidean, trained and filled at start-up) serves "ann" requests on
+    one more worker."""
 
     def __init__(self, ab, X, models=None, workers=2, max_batch_queries=1024,
                  max_request_queries=4096, hbm_budget=16 << 30, precision_mode="bf16x3",
-                 small_queries=256, aging_ms=20.0):
+                 small_queries=256, aging_ms=20.0, ann=None):
         self.ab = ab
         self.small_queries = small_queries
         self.aging = aging_ms / 1e3
@@ -78,7 +82,8 @@ class Server:
         self.max_batch_queries = max_batch_queries
         self.hbm_budget = hbm_budget
         self.cv = threading.Condition()
-        self.pending = {"knn": collections.deque(), "predict": collections.deque()}
+        self.pending = {"knn": collections.deque(), "ann": collections.deque(),
+                        "predict": collections.deque()}
         self.stopping = False
         self.completed = []
         self.batches = []          # (kind, requests, queries, seconds) of every library call
@@ -107,10 +112,21 @@ class Server:
             # allocated now (an allocation later would stall every stream)
             km.predict(np.zeros((max_request_queries, Xm.shape[1]), dtype=np.float32))
             self.models[name] = km
+        self.ann = None
+        if ann is not None:
+            self.ann = ab.ApproxNN("s", order=ab.ROW_MAJOR, n_list=int(ann["n_list"]),
+                                   n_probe=int(ann.get("n_probe", 1)),
+                                   seed=int(ann.get("seed", 0)))
+            self.ann.set_training_data(self.X).train_and_add()
+            # every kernel and buffer of the request shapes, now
+            for nq in (1, min(max_request_queries, 512), max_batch_queries):
+                self.ann.kneighbors(self.X[np.arange(nq) % self.X.shape[0]], 256)
         self.bytes_per_query = self.d * 4 + KNN_LIST_BYTES + KNN_OUT_BYTES
         self.threads = [threading.Thread(target=self._knn_worker, args=(w,), daemon=True)
                         for w in range(workers)]
         self.threads.append(threading.Thread(target=self._predict_worker, daemon=True))
+        if self.ann is not None:
+            self.threads.append(threading.Thread(target=self._ann_worker, daemon=True))
         for t in self.threads:
             t.start()
 
@@ -118,17 +134,19 @@ class Server:
     def submit(self, req):
         if req.kind == "predict" and req.model not in self.models:
             raise KeyError(f"unknown model {req.model!r}")
-        if req.kind == "knn" and not (1 <= req.k <= 256):
+        if req.kind == "ann" and self.ann is None:
+            raise KeyError("the server holds no IVF-flat index")
+        if req.kind in ("knn", "ann") and not (1 <= req.k <= 256):
             raise ValueError("k must be in [1, 256]")
         req.t_submit = time.perf_counter()
         parts = [req]
         nq = req.queries.shape[0]
-        if req.kind == "knn" and nq > self.max_batch_queries:
+        if req.kind in ("knn", "ann") and nq > self.max_batch_queries:
             req.result = (np.empty((nq, req.k), dtype=np.int32),
                           np.empty((nq, req.k), dtype=np.float32))
             parts = []
             for o in range(0, nq, self.max_batch_queries):
-                part = Request("knn", req.queries[o:o + self.max_batch_queries], k=req.k)
+                part = Request(req.kind, req.queries[o:o + self.max_batch_queries], k=req.k)
                 part.t_submit, part.parent, part.offset = req.t_submit, req, o
                 parts.append(part)
             req.parts_left = len(parts)
@@ -147,6 +165,8 @@ class Server:
             h.close()
         for km in self.models.values():
             km.close()
+        if self.ann is not None:
+            self.ann.close()
 
     # ------------------------------------------------------------ workers --
     def _take(self, kind, cap_queries, cap_bytes, per_query_bytes, same_model=False):
@@ -215,17 +235,37 @@ class Server:
             if nfb:
                 with self.cv:
                     self.fallback_queries += nfb
-            o = 0
-            for r in batch:
-                m = r.queries.shape[0]
-                if r.parent is None:
-                    r.result = (ind[o:o + m, :r.k].copy(), dist[o:o + m, :r.k].copy())
-                else:  # a part: its rows of the parent's result
-                    pi, pd = r.parent.result
-                    pi[r.offset:r.offset + m] = ind[o:o + m, :r.k]
-                    pd[r.offset:r.offset + m] = dist[o:o + m, :r.k]
-                o += m
-            self._finish("knn", batch, Q.shape[0], secs)
+            self._scatter("knn", batch, Q, ind, dist, secs)
+
+    def _ann_worker(self):
+        """IVF-flat requests: one search of the batch with the largest k; a
+        request's own results are the prefix (the top-k over the probed lists
+        in (distance, index) order does not depend on k)."""
+        while True:
+            batch = self._take("ann", self.max_batch_queries, self.hbm_budget,
+                               self.bytes_per_query)
+            if batch is None:
+                return
+            Q = batch[0].queries if len(batch) == 1 else np.concatenate([r.queries for r in batch])
+            kmax = max(r.k for r in batch)
+            t0 = time.perf_counter()
+            ind, dist = self.ann.kneighbors(Q, kmax)
+            secs = time.perf_counter() - t0
+            self._scatter("ann", batch, Q, ind, dist, secs)
+
+    def _scatter(self, kind, batch, Q, ind, dist, secs):
+        """Every request of a search batch gets its rows and k-prefix."""
+        o = 0
+        for r in batch:
+            m = r.queries.shape[0]
+            if r.parent is None:
+                r.result = (ind[o:o + m, :r.k].copy(), dist[o:o + m, :r.k].copy())
+            else:  # a part: its rows of the parent's result
+                pi, pd = r.parent.result
+                pi[r.offset:r.offset + m] = ind[o:o + m, :r.k]
+                pd[r.offset:r.offset + m] = dist[o:o + m, :r.k]
+            o += m
+        self._finish(kind, batch, Q.shape[0], secs)
 
     def _predict_worker(self):
         while True:

@@ -126,3 +126,57 @@ def test_serving_small_requests_first():
     finally:
         gate.set()
         server.close()
+
+
+class FakeApproxNN(FakeKNN):
+    """Stands in for the IVF-flat handle: an exact search (all lists probed)."""
+
+    def __init__(self, prec, order=None, **options):
+        super().__init__(prec)
+        self.options = options
+
+    def set_training_data(self, X):
+        return self.fit(X)
+
+    def train_and_add(self):
+        return self
+
+
+def test_serving_ann_requests():
+    """IVF-flat requests are batched on their own worker, split when larger
+    than one call, and each gets its k-prefix; kNN requests are unaffected."""
+    sv = _load("aoclda_serving_cpu3", os.path.join(PKG, "serving.py"))
+
+    class AB(FakeAB):
+        ApproxNN = FakeApproxNN
+
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal((300, 6)).astype(np.float32)
+    server = sv.Server(AB(), X, workers=1, max_batch_queries=16, max_request_queries=64,
+                       ann={"n_list": 8, "n_probe": 8})
+    try:
+        assert server.ann.options == {"n_list": 8, "n_probe": 8, "seed": 0}
+        reqs = [server.submit(sv.Request(kind, rng.standard_normal((size, 6)), k=k))
+                for kind, size, k in (("ann", 3, 5), ("ann", 40, 2), ("knn", 5, 3),
+                                      ("ann", 16, 9))]
+        for r in reqs:
+            assert r.wait(30)
+        ref = FakeKNN("s").fit(X)
+        for r in reqs:
+            ind, dist = ref.kneighbors(r.queries, r.k)
+            np.testing.assert_array_equal(r.result[0], ind)
+            np.testing.assert_array_equal(r.result[1], dist)
+        ann_batches = [b for b in server.batches if b[0] == "ann"]
+        assert ann_batches and max(b[2] for b in ann_batches) <= 16
+    finally:
+        server.close()
+    # without an index, "ann" requests are refused
+    plain = sv.Server(FakeAB(), X, workers=1, max_batch_queries=16, max_request_queries=64)
+    try:
+        try:
+            plain.submit(sv.Request("ann", X[:2], k=1))
+            raise AssertionError("an ann request without an index was accepted")
+        except KeyError:
+            pass
+    finally:
+        plain.close()
