@@ -268,6 +268,26 @@ cudaError_t launch_kpp_cost(const T *w, const T *D, int n, int t, double *block_
 // w_i = max(0, min(w_i, D_ci)) for the chosen candidate (in place).
 template <typename T>
 cudaError_t launch_kpp_update(T *w, const T *Dc, int n, int chosen, cudaStream_t s);
+// Device-side k-means++ draws (kmeans_kpp.cu): weights grouped in blocks
+// of 2,048 (kpp_num_blocks(n) block sums).
+int kpp_num_blocks(int n);
+// w_i = 0 where negative, not finite or i == first; block sums; flag[0] |= 1
+// when a weight is positive.
+template <typename T>
+cudaError_t launch_kpp_clamp(T *w, int n, int first, double *bs, int *flag, cudaStream_t s);
+// The rows std::discrete_distribution over w gives for the nt canonical draws
+// U[0..nt) (cand), uncertified draws redone sequentially (exact_count[0] +=
+// their number); force_exact redoes all of them.
+template <typename T>
+cudaError_t launch_kpp_draw(const T *w, int n, const double *bs, const double *U, int nt,
+                            int force_exact, int *cand, int *unc, int *exact_count,
+                            cudaStream_t s);
+// Choose among the nt candidates by cost (chosen[c]), w_i = max(0, min(w_i,
+// D_best,i)), w_best = 0, block sums of the new w.
+template <typename T>
+cudaError_t launch_kpp_select_update(T *w, const T *D, int n, const double *cost,
+                                     const int *cand, int nt, int *chosen, int c, double *bs,
+                                     cudaStream_t s);
 
 // ------------------------------------------------- tensor-core k-means ---
 // 1 when the tcgen05 assignment handles (k clusters, d features) with the

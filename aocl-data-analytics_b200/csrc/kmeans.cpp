@@ -3,6 +3,7 @@
 // over the data runs on the GPU (kmeans_simt.cu), the random draws of the
 // initialisation use the same std:: generators as the reference on the host.
 #include "alg.hpp"
+#include <cstdlib>
 
 namespace b200 {
 
@@ -197,69 +198,74 @@ template <typename T> static inline T host_at(const KMeans<T> &km, da_int i, da_
                                          : km.A_host[(size_t)i * km.lda_host + j];
 }
 
-// kmeans.cpp:1524-1664 (distances on the device, draws on the host).
+// kmeans.cpp:1524-1664.  The host draws from the reference's engine in the
+// reference's order (the first centre, then n_trials canonical doubles per
+// further centre, consumed by std::discrete_distribution one each); the
+// device maps the draws to rows (kmeans_kpp.cu), computes the candidates'
+// distances and costs, chooses and updates the weights, with no host round
+// trip per centre.
 template <typename T> da_status KMeans<T>::kmeans_plusplus(T *dC) {
     cudaStream_t st = cuda->stream;
     const da_int n = n_samples, k = n_clusters, d = n_features;
     const da_int n_trials = 2 + (da_int)std::log(k);
-    if (!dW.ensure((size_t)n * sizeof(T)) || !dKD.ensure((size_t)n * (n_trials + 1) * sizeof(T)) ||
-        !dCand.ensure((size_t)(n_trials + 1) * sizeof(int)))
+    const int nb = kpp_num_blocks((int)n);
+    if (!dW.ensure((size_t)n * sizeof(T)) || !dKD.ensure((size_t)n * n_trials * sizeof(T)) ||
+        !dCand.ensure((size_t)(2 * n_trials + k + 2) * sizeof(int)) ||
+        !dKppU.ensure((size_t)std::max<da_int>(1, (k - 1) * n_trials) * sizeof(double)) ||
+        !dKppBs.ensure((size_t)(nb + n_trials) * sizeof(double)) ||
+        !dPartials.ensure((size_t)148 * 4 * n_trials * sizeof(double)))
         return err->error(da_status_memory_error, "Device memory allocation failed.");
-    std::vector<int> chosen(k, 0);
+    int *dCandv = dCand.as<int>();
+    int *dUnc = dCandv + n_trials;
+    int *dChosen = dUnc + n_trials;
+    int *dFlag = dChosen + k;       // [0] a positive weight, [1] redone draws
+    double *dBs = dKppBs.as<double>();
+    double *dCost = dBs + nb;
     std::uniform_int_distribution<> dis_int(0, n - 1);
     const int first = dis_int(mt_gen);
-    chosen[0] = first;
-    // works3: distances to the first centre, clamped
-    B200_TRY(cudaMemcpyAsync(dCand.p, &first, sizeof(int), cudaMemcpyHostToDevice, st), "copy");
-    B200_TRY(launch_kpp_dist<T>(dX.as<T>(), ld, n, d, dXn.as<T>(), dCand.as<int>(), 1, dW.as<T>(), st),
+    int init_words[3] = {first, 0, 0};
+    // chosen[0] = first; flags cleared
+    B200_TRY(cudaMemcpyAsync(dChosen, &init_words[0], sizeof(int), cudaMemcpyHostToDevice, st),
+             "copy");
+    B200_TRY(cudaMemcpyAsync(dFlag, &init_words[1], 2 * sizeof(int), cudaMemcpyHostToDevice, st),
+             "copy");
+    // w: distances to the first centre, clamped (kmeans.cpp:1561-1590)
+    B200_TRY(launch_kpp_dist<T>(dX.as<T>(), ld, n, d, dXn.as<T>(), dChosen, 1, dW.as<T>(), st),
              "k-means++ distances");
-    std::vector<T> w(n);
-    B200_TRY(cudaMemcpyAsync(w.data(), dW.p, n * sizeof(T), cudaMemcpyDeviceToHost, st), "copy");
+    B200_TRY(launch_kpp_clamp<T>(dW.as<T>(), (int)n, first, dBs, dFlag, st), "k-means++ weights");
+    int flags[2] = {0, 0};
+    B200_TRY(cudaMemcpyAsync(flags, dFlag, sizeof(flags), cudaMemcpyDeviceToHost, st), "copy");
     B200_TRY(cudaStreamSynchronize(st), "k-means++");
-    w[first] = T(0);
-    bool coincident = true;
-    for (da_int i = 0; i < n; ++i) {
-        if (!std::isfinite(w[i]) || w[i] < T(0)) w[i] = T(0);
-        if (w[i] > T(0)) coincident = false;
-    }
-    if (coincident) {
+    std::vector<int> chosen(k, 0);
+    if (!flags[0]) {
+        // all rows coincide with the first centre: rows 0..k-1
         for (da_int i = 0; i < k; ++i) chosen[i] = i;
-    } else {
-        B200_TRY(cudaMemcpyAsync(dW.p, w.data(), n * sizeof(T), cudaMemcpyHostToDevice, st), "copy");
-        std::vector<int> cand(n_trials);
-        std::vector<double> cost(n_trials);
+    } else if (k > 1) {
+        // the draws of std::discrete_distribution, in the reference's order
+        std::vector<double> U((size_t)(k - 1) * n_trials);
+        for (double &u : U) u = std::generate_canonical<double, std::numeric_limits<double>::digits>(mt_gen);
+        B200_TRY(cudaMemcpyAsync(dKppU.p, U.data(), U.size() * sizeof(double),
+                                 cudaMemcpyHostToDevice, st), "copy");
+        const double *dU = dKppU.as<double>();
+        const char *fe = std::getenv("AOCLDA_B200_KPP_EXACT_DRAWS");
+        const int force_exact = (fe && fe[0] == '1') ? 1 : 0;
         for (da_int c = 1; c < k; ++c) {
-            std::discrete_distribution<> weighted_dis(w.begin(), w.end());
-            for (da_int t = 0; t < n_trials; ++t) cand[t] = weighted_dis(mt_gen);
-            B200_TRY(cudaMemcpyAsync(dCand.p, cand.data(), n_trials * sizeof(int),
-                                     cudaMemcpyHostToDevice, st), "copy");
-            B200_TRY(launch_kpp_dist<T>(dX.as<T>(), ld, n, d, dXn.as<T>(), dCand.as<int>(),
-                                        n_trials, dKD.as<T>(), st), "k-means++ distances");
+            B200_TRY(launch_kpp_draw<T>(dW.as<T>(), (int)n, dBs, dU + (size_t)(c - 1) * n_trials,
+                                        (int)n_trials, force_exact, dCandv, dUnc, dFlag + 1, st),
+                     "k-means++ draws");
+            B200_TRY(launch_kpp_dist<T>(dX.as<T>(), ld, n, d, dXn.as<T>(), dCandv, n_trials,
+                                        dKD.as<T>(), st), "k-means++ distances");
             B200_TRY(launch_kpp_cost<T>(dW.as<T>(), dKD.as<T>(), n, n_trials, dPartials.as<double>(),
-                                        dScalars.as<double>(), st), "k-means++ cost");
-            B200_TRY(cudaMemcpyAsync(cost.data(), dScalars.p, n_trials * sizeof(double),
-                                     cudaMemcpyDeviceToHost, st), "copy");
-            B200_TRY(cudaStreamSynchronize(st), "k-means++");
-            int best = 0, best_t = -1;
-            double best_cost = std::numeric_limits<double>::infinity();
-            for (da_int t = 0; t < n_trials; ++t) {
-                bool repeat = false;
-                for (da_int u = 0; u < t; ++u)
-                    if (cand[u] == cand[t]) repeat = true;
-                if (repeat) continue;
-                if (std::isfinite(cost[t]) && cost[t] < best_cost) {
-                    best_cost = cost[t];
-                    best = cand[t];
-                    best_t = t;
-                }
-            }
-            if (best_t < 0) best_t = 0, best = cand[0];
-            chosen[c] = best;
-            B200_TRY(launch_kpp_update<T>(dW.as<T>(), dKD.as<T>() + (size_t)best_t * n, n, best, st),
+                                        dCost, st), "k-means++ cost");
+            B200_TRY(launch_kpp_select_update<T>(dW.as<T>(), dKD.as<T>(), (int)n, dCost, dCandv,
+                                                 (int)n_trials, dChosen, (int)c, dBs, st),
                      "k-means++ update");
-            B200_TRY(cudaMemcpyAsync(w.data(), dW.p, n * sizeof(T), cudaMemcpyDeviceToHost, st), "copy");
-            B200_TRY(cudaStreamSynchronize(st), "k-means++");
         }
+        B200_TRY(cudaMemcpyAsync(chosen.data(), dChosen, k * sizeof(int), cudaMemcpyDeviceToHost, st),
+                 "copy");
+        B200_TRY(cudaMemcpyAsync(flags, dFlag, sizeof(flags), cudaMemcpyDeviceToHost, st), "copy");
+        B200_TRY(cudaStreamSynchronize(st), "k-means++");
+        cuda->stats["kmeans_pp_exact_draws"] += (double)flags[1];
     }
     std::vector<T> Cc((size_t)k * d);
     for (da_int c = 0; c < k; ++c)

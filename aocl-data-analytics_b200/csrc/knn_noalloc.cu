@@ -18,10 +18,15 @@
 // GPU (different streams, or different host threads without ordering) race
 // on it and give wrong results.  The first call on each device looks up the
 // array's device address (cudaGetSymbolAddress, with that device current);
-// make that first call before any stream capture on the device.
+// make that first call before any stream capture on the device.  The address
+// belongs to the device's current context: when that context is replaced
+// (cudaDeviceReset, or another primary context made current), the next call
+// looks the address up again instead of using the old one.
 #include "b200_kernels.hpp"
 #include "../../include/aoclda_b200_ext.h"
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <mutex>
 
 namespace {
@@ -30,19 +35,49 @@ __device__ __align__(256) unsigned char knn_noalloc_scratch[DA_B200_KNN_NOALLOC_
 
 constexpr int MAX_DEVICES = 64;
 std::mutex g_setup_mu;
-void *g_scratch_addr[MAX_DEVICES] = {};
+struct ScratchSlot {
+    unsigned long long ctx_id; // unique id of the context the address belongs to
+    void *addr;
+};
+ScratchSlot g_scratch[MAX_DEVICES] = {};
 
-// Device address of the scratch array on the current device (looked up once
-// per device).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+template <typename F> F driver_entry(const char *name) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+        return nullptr;
+    return reinterpret_cast<F>(p);
+}
+
+// Unique id of the calling thread's current context (0 when there is none).
+unsigned long long current_context_id() {
+    static CtxGetCurrentFn get_cur = driver_entry<CtxGetCurrentFn>("cuCtxGetCurrent");
+    static CtxGetIdFn get_id = driver_entry<CtxGetIdFn>("cuCtxGetId");
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (!get_cur || !get_id || get_cur(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
+// Device address of the scratch array on the current device, looked up
+// once per device and context.
 cudaError_t scratch_address(int dev, void **out) {
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
+    const unsigned long long id = current_context_id();
+    if (!g_scratch[dev].addr || id == 0 || g_scratch[dev].ctx_id != id) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, knn_noalloc_scratch);
         if (e != cudaSuccess) return e;
-        g_scratch_addr[dev] = p;
+        g_scratch[dev].addr = p;
+        // the lookup makes the device's primary context current if none was
+        g_scratch[dev].ctx_id = current_context_id();
     }
-    *out = g_scratch_addr[dev];
+    *out = g_scratch[dev].addr;
     return cudaSuccess;
 }
 
@@ -83,7 +118,10 @@ extern "C" da_status da_b200_knn_euclidean_noalloc_s(const float *X, da_int n, c
     const int BN = knn_tile_rows_train(false);
     const int q_tiles = (int)((nq + 63) / 64);
     const int max_chunks = (int)((n + BN - 1) / BN);
-    int n_chunks = std::max(1, std::min(max_chunks, (nsm * 8 + q_tiles - 1) / q_tiles));
+    // enough CTAs to fill the GPU, but at most ~16K partial entries per query
+    // (the merge ranks every entry against every chunk list)
+    int n_chunks = std::max(1, std::min({max_chunks, (nsm * 8 + q_tiles - 1) / q_tiles,
+                                         std::max(8, 16384 / (int)k)}));
     const int cap = (int)std::min<size_t>((size_t)DA_B200_KNN_NOALLOC_SCRATCH_BYTES / per_chunk,
                                           (size_t)max_chunks);
     n_chunks = std::max(1, std::min(n_chunks, cap));

@@ -138,60 +138,72 @@ def dist_env():
     return rank, world, local
 
 
-def cpu_baseline(X, C0, sample_rows, iters):
-    """The reference's CPU algorithm on a bounded sample of the workload:
-    the compiled reference (oracle/_ref) when present, else the oracle port.
-    Returns iterations/s scaled to the full row count (time per iteration is
-    linear in the rows)."""
-    ref = os.path.join(ORACLE, "_ref", "libaoclda_ref.so")
-    Xs = np.ascontiguousarray(X[:sample_rows])
-    if os.path.exists(ref):
-        refmod = _load("ref_oracle", os.path.join(ORACLE, "ref", "ref_oracle.py"))
-        t, nit, cores = refmod.time_kmeans(Xs, C0, iters)
-        kind = "reference"
-    else:
-        orc = _load("oracle_mod", os.path.join(ORACLE, "oracle.py"))
-        Cc = np.ascontiguousarray(C0.copy())
-        lab = np.zeros(sample_rows, dtype=np.int32)
-        orc.kmeans_iteration(Xs, Cc, lab)  # warm-up
-        t0 = time.perf_counter()
-        for _ in range(iters):
-            orc.kmeans_iteration(Xs, Cc, lab)
-        t = time.perf_counter() - t0
-        nit = iters
-        cores = orc.num_threads()
-        kind = "port"
-    ips_sample = nit / t
-    value = ips_sample * sample_rows / X.shape[0]
-    return {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"{nit} Lloyd iterations on the first {sample_rows} of {X.shape[0]} rows "
-                      f"(k={C0.shape[0]}, d={X.shape[1]}), scaled linearly to {X.shape[0]} rows"}
+def _oracle():
+    return _load("oracle_mod", os.path.join(ORACLE, "oracle.py"))
+
+
+def cpu_baseline(X, C0, iters=3):
+    """The reference's CPU Lloyd iteration (kmeans_lloyd.hpp:106-405: blocks
+    of 512 rows over OpenMP threads, one BLAS sgemm per block, strict-'<'
+    argmin, thread-local sums merged under a lock) restated in the oracle
+    (oracle_blas.c) with scipy's OpenBLAS, on ALL rows of the workload from
+    the same initial centres, every host thread.  Returns iterations/s."""
+    orc = _oracle()
+    blas = orc.openblas()
+    Cc = np.ascontiguousarray(C0.copy())
+    lab = np.full(X.shape[0], -1, dtype=np.int32)
+    orc.lloyd_blas(X, Cc, lab, 1, blas)  # warm-up (first touch, thread pools)
+    t0 = time.perf_counter()
+    orc.lloyd_blas(X, Cc, lab, iters, blas)
+    t = time.perf_counter() - t0
+    cores = orc.num_threads()
+    return {"value": iters / t, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{iters} Lloyd iterations over all {X.shape[0]} rows (k={C0.shape[0]}, "
+                      f"d={X.shape[1]}) from the workload's k-means++ centres: the reference's "
+                      f"blocked form (512-row blocks, one OpenBLAS sgemm each, {cores} OpenMP "
+                      f"threads; {blas.config()})"}
 
 
 def run_reference(args):
+    """The reference arm: the reference's CPU k-means (the oracle's
+    restatement, oracle_kpp.cpp + oracle_blas.c, with OpenBLAS) on the same
+    workload -- k-means++ from seed 1 (timed once, reported as init_s), then
+    Lloyd iterations from those centres, `ITERS_PER_REF_STEP` per step."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
+    orc = _oracle()
+    blas = orc.openblas()
     X = make_data()
-    # fixed initial centres shared with the GPU arm: k-means++ from the library
-    # is not available here, so the reference arm seeds from the same rows the
-    # CPU reference's own k-means++ would see; centres only fix the work done.
-    rng = np.random.default_rng(SEED)
-    C0 = np.ascontiguousarray(X[rng.choice(N, K, replace=False)])
-    sample = int(os.environ.get("BENCH_CPU_SAMPLE", "131072"))
-    vals = []
-    cb = None
+    t0 = time.perf_counter()
+    chosen = orc.kmeanspp(X, K, SEED, gemm=blas)  # distances by BLAS, as the reference
+    init_s = time.perf_counter() - t0
+    C0 = np.ascontiguousarray(X[chosen])
+    Cc = C0.copy()
+    lab = np.full(N, -1, dtype=np.int32)
+    per_step = 2
     for _ in range(max(1, args.warmup)):
-        cpu_baseline(X, C0, sample, 1)
+        orc.lloyd_blas(X, Cc, lab, per_step, blas)
+    t0 = time.perf_counter()
     for _ in range(args.steps):
-        cb = cpu_baseline(X, C0, sample, 2)
-        vals.append(cb["value"])
-    v = float(np.mean(vals))
-    cb["value"] = v
+        orc.lloyd_blas(X, Cc, lab, per_step, blas)
+    t = time.perf_counter() - t0
+    v = args.steps * per_step / t
+    cores = orc.num_threads()
+    cb = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+          "sample": f"{args.steps} steps of {per_step} Lloyd iterations over all {N} rows "
+                    f"(k={K}, d={D}) continuing from k-means++ (seed {SEED}); the reference's "
+                    f"blocked form (512-row blocks, one OpenBLAS sgemm each, {cores} OpenMP "
+                    f"threads; {blas.config()})"}
+    cfg = config_dict(args) | {"init": f"k-means++ seed {SEED} (oracle restatement, "
+                                       f"{init_s:.1f} s on the host, not timed)",
+                               "init_s": init_s, "iterations_per_step": per_step,
+                               "step": f"{per_step} Lloyd iterations (blocked BLAS form) "
+                                       "continuing the fit"}
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v * MAX_ITER,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-           "data": "synthetic", "config": config_dict(args), "cpu_baseline": cb,
+           "data": "synthetic", "config": cfg, "cpu_baseline": cb,
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
     return 0
@@ -216,6 +228,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain fp32 comparison")
     ap.add_argument("--no-knn", action="store_true", help="skip the kNN (4.04M x 128) leg")
+    ap.add_argument("--no-c1", action="store_true", help="skip the fp64 kNN (10,000 x 32) leg")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the error checks against the fp64 oracle")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched k-means (512 data sets) leg")
     ap.add_argument("--no-radius", action="store_true",
@@ -270,7 +285,8 @@ def main():
     if args.knn_only:
         if rank == 0:
             print(json.dumps(run_knn(ab, nx=args.knn_rows, nq=args.knn_queries,
-                                     plain=bool(args.knn_plain))))
+                                     plain=bool(args.knn_plain),
+                                     accuracy=not args.no_accuracy)))
         return 0
 
     X = make_data()
@@ -398,16 +414,22 @@ def main():
                  "hbm_frac": achieved_gbs / hbm,
                  "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in kt.items() if v[1]}})
 
+    accuracy = None
+    if rank == 0 and world == 1 and not args.no_accuracy:
+        accuracy = c2_accuracy(ab, X, C0, km.labels(N), km.centres(K, D), float(km.rinfo()[4]))
     # e2e: host (pinned) -> device every step, labels + centres back
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(ab, km, X, C0, stream, args, world)
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cb = cpu_baseline(X, C0, int(os.environ.get("BENCH_CPU_SAMPLE", "131072")), 2)
+        cb = cpu_baseline(X, C0)
     knn = None
     if rank == 0 and world == 1 and not args.no_knn:
-        knn = run_knn(ab)
+        knn = run_knn(ab, accuracy=not args.no_accuracy)
+    c1 = None
+    if rank == 0 and world == 1 and not args.no_c1:
+        c1 = run_c1(ab)
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = run_batched(ab)
@@ -420,7 +442,8 @@ def main():
     serving = None
     if rank == 0 and world == 1 and not args.no_serve:
         serving = run_serving(ab)
-    extra = {"iterations_per_step": n_iter, "init_ms": init_ms,
+    extra = {"iterations_per_step": n_iter, "init_ms": init_ms, "accuracy": accuracy,
+             "legs_summary": legs_summary(knn, c1, batched, serving, radius, ivf, plain, value),
              "relabelled_rows_last_iteration": relabelled,
              "full_scan_rows_last_iteration": full_scan,
              "precision_path": (f"{mode} tcgen05 candidate pass + exact fp32 re-score of "
@@ -438,6 +461,7 @@ def main():
         "plain_fp32": plain,
         "speedup_vs_plain_fp32": (value / plain["value"]) if plain else None,
         "knn": knn,
+        "knn_fp64_c1": c1,
         "kmeans_batched": batched,
         "serving": serving,
         "ivf_flat": ivf,
@@ -447,6 +471,173 @@ def main():
         print(json.dumps(out))
         sys.stdout.flush()
     return 0
+
+
+def c2_accuracy(ab, X, C0, labels, centres, inertia, tie_rel=1e-6):
+    """Errors of the k-means results against the fp64 oracle, over all rows:
+    * the centre update: one Lloyd step from C0 on the default path (its
+      centres are the means of the fp32 assignment to C0) against the fp64
+      means of the oracle's fp32 assignment to C0 -- max abs / max rel error
+      (elements above 1e-3 of the largest) and the Frobenius relative error;
+    * the fit's labels against the oracle's fp32 assignment to the fit's
+      centres (mismatches, expected 0), and the rows whose best and second
+      best fp64 squared distances differ by at most tie_rel relative (where a
+      label depends on rounding: counted, not excluded);
+    * the fit's inertia against the fp64 inertia of its labels and centres."""
+    orc = _oracle()
+    k, d = C0.shape
+    h = ab.KMeans(k, "s", order=ab.ROW_MAJOR, max_iter=1, n_init=1)
+    h.set("convergence tolerance", TOL)
+    h.fit(X, C0=C0)
+    C1 = h.centres(k, d).astype(np.float64)
+    h.close()
+    lab0, _ = orc.kmeans_assign(X, C0)
+    Cm, _ = orc.kmeans_update(X, lab0, k)
+    err = np.abs(C1 - Cm)
+    big = np.abs(Cm) > 1e-3 * np.abs(Cm).max()
+    lab_o, gap = orc.kmeans_assign(X, centres)
+    Xd = X.astype(np.float64)
+    cd = centres.astype(np.float64)
+    best = ((Xd[:4096, None, :] - cd[None, :, :]) ** 2).sum(-1).min(1)  # scale of the gaps
+    scale = float(np.median(best))
+    i64 = orc.kmeans_inertia(X, labels, cd)
+    return {"centre_update_max_abs_err": float(err.max()),
+            "centre_update_max_rel_err": float((err[big] / np.abs(Cm[big])).max()),
+            "centre_update_frobenius_rel_err": float(np.linalg.norm(C1 - Cm) / np.linalg.norm(Cm)),
+            "label_mismatches_vs_oracle": int((labels != lab_o).sum()),
+            "near_tie_rows": int((gap <= tie_rel * scale).sum()),
+            "tie_tolerance": f"fp64 gap between best and second-best squared distance <= "
+                             f"{tie_rel:g} x the median best squared distance ({scale:.4g})",
+            "inertia_rel_err_vs_fp64": float(abs(inertia - i64) / i64),
+            "oracle": "fp32 assignment in the reference's fma order; fp64 means, inertia and gaps"}
+
+
+def knn_accuracy(X, Q, ind, dist, k, metric, nsample=20, tie_rel=1e-6):
+    """kNN results against the oracle on the first nsample queries: indices
+    and distances identical to the oracle's fp32 search; the returned fp32
+    distances against fp64 distances of the same rows (max abs / rel error);
+    queries whose k-th and (k+1)-th fp64 distances differ by at most
+    tie_rel relative."""
+    orc = _oracle()
+    Qs = np.ascontiguousarray(Q[:nsample])
+    oi, od = orc.knn(X, Qs, k, metric=metric)
+    same = bool(np.array_equal(oi, ind[:nsample]) and np.array_equal(od, dist[:nsample]))
+    Qd = Qs.astype(np.float64)
+    qn = (Qd * Qd).sum(1)
+    ref = np.zeros((nsample, k))
+    cand = []
+    for b in range(0, X.shape[0], 262_144):
+        xb = X[b:b + 262_144].astype(np.float64)
+        xn = (xb * xb).sum(1)
+        dot = xb @ Qd.T
+        if metric == "cosine":
+            dd = 1.0 - dot / np.sqrt(np.outer(xn, qn))
+        else:
+            dd = np.maximum(xn[:, None] + qn[None, :] - 2.0 * dot, 0.0)
+        part = np.partition(dd, k, axis=0)[: k + 1]
+        cand.append(part)
+    allc = np.sort(np.concatenate(cand, axis=0), axis=0)[: k + 1].T
+    for q in range(nsample):
+        xr = X[ind[q]].astype(np.float64)
+        if metric == "cosine":
+            xn = (xr * xr).sum(1)
+            ref[q] = 1.0 - (xr @ Qd[q]) / np.sqrt(xn * qn[q])
+        else:
+            ref[q] = np.sqrt(((xr - Qd[q]) ** 2).sum(1))
+    kth = allc
+    if metric != "cosine":
+        kth = np.sqrt(kth)
+    e = np.abs(dist[:nsample].astype(np.float64) - ref)
+    ties = int((kth[:, k] - kth[:, k - 1] <= tie_rel * np.maximum(np.abs(kth[:, k]), 1e-30)).sum())
+    return {"identical_to_oracle": same, "sample_queries": nsample,
+            "max_abs_err_vs_fp64": float(e.max()),
+            "max_rel_err_vs_fp64": float((e / np.maximum(np.abs(ref), 1e-30)).max()),
+            "queries_with_kth_tie": ties,
+            "tie_tolerance": f"k-th and (k+1)-th fp64 distances within {tie_rel:g} relative"}
+
+
+def run_c1(ab, reps=5):
+    """Plain brute-force kNN, fp64: 10,000 x 32 training rows from a
+    16-component isotropic Gaussian mixture (means U[-5, 5]^32, sigma 1,
+    labels = component id), 2,000 queries from the mixture, seed 0, k = 10,
+    euclidean, uniform weights.  A timed call is da_nn_kneighbors_d plus
+    da_nn_classifier_predict_d over all queries with host arrays (best of
+    5); the neighbours, distances and labels must equal the oracle's.  CPU:
+    the oracle's search (all host threads) and the same vote."""
+    rng = np.random.default_rng(0)
+    n, nq, d, comps, k = 10_000, 2_000, 32, 16, 10
+    means = rng.uniform(-5.0, 5.0, (comps, d))
+    y = rng.integers(0, comps, n)
+    X = means[y] + rng.standard_normal((n, d))
+    ql = rng.integers(0, comps, nq)
+    Q = means[ql] + rng.standard_normal((nq, d))
+    nn = ab.KNN("d", order=ab.ROW_MAJOR, weights="uniform", number_of_neighbors=k).fit(X, y=y)
+    nn.kneighbors(Q[:64], k)
+    nn.predict(Q[:64])
+    ts = []
+    for _ in range(reps):
+        t = time.perf_counter()
+        ind, dist = nn.kneighbors(Q, k)
+        pred = nn.predict(Q)
+        ts.append(time.perf_counter() - t)
+    nn.close()
+    orc = _oracle()
+    t = time.perf_counter()
+    oi, od = orc.knn(X, Q, k)
+    classes = np.unique(y)
+    cnt = np.zeros((nq, classes.size))
+    for r in range(k):
+        np.add.at(cnt, (np.arange(nq), np.searchsorted(classes, y[oi[:, r]])), 1.0)
+    opred = classes[np.argmax(cnt, axis=1)]
+    cpu_s = time.perf_counter() - t
+    return {"workload": f"knn_fp64_euclidean_{n}x{d}_q{nq}_k{k}_gmm{comps}_predict",
+            "unit": "queries/s", "qps": nq / min(ts),
+            "identical_to_oracle": bool(np.array_equal(ind, oi) and np.array_equal(dist, od)
+                                        and np.array_equal(pred, opred)),
+            "flops_per_call": 2.0 * n * nq * d,
+            "cpu_baseline": {"value": nq / cpu_s, "unit": "queries/s",
+                             "cores": orc.num_threads(), "kind": "port",
+                             "sample": "all 2,000 queries: the oracle's fp64 search (one query "
+                                       "per OpenMP thread at a time) and the uniform vote"},
+            "timing": "wall clock of da_nn_kneighbors_d + da_nn_classifier_predict_d with host "
+                      "arrays (best of 5)"}
+
+
+def legs_summary(knn, c1, batched, serving, radius, ivf, plain, value):
+    """One compact line per workload, kept beside the headline numbers."""
+    out = {"kmeans_c2": {"iters_per_s": value,
+                         "plain_fp32_iters_per_s": plain["value"] if plain else None}}
+    if knn:
+        for m in ("euclidean", "cosine"):
+            r = knn if m == "euclidean" else knn.get("cosine")
+            if r:
+                acc = r.get("accuracy") or {}
+                out[f"knn_c3_{m}"] = {"qps": r["qps"], "plain_qps": r["plain_qps"],
+                                      "identical_to_plain": r["identical_to_plain"],
+                                      "identical_to_oracle_sample": acc.get("identical_to_oracle"),
+                                      "max_rel_err_vs_fp64": acc.get("max_rel_err_vs_fp64"),
+                                      "queries_with_kth_tie": acc.get("queries_with_kth_tie")}
+    if c1:
+        out["knn_fp64_c1"] = {"qps": c1["qps"], "identical_to_oracle": c1["identical_to_oracle"],
+                              "cpu_qps": c1["cpu_baseline"]["value"]}
+    if batched:
+        out["kmeans_batched_c4"] = {"iters_per_s": batched["value"],
+                                    "speedup_vs_per_instance": batched["speedup_vs_per_instance_calls"],
+                                    "identical": batched["identical_to_single"]}
+    if serving:
+        srv = {}
+        for key, v in serving.items():
+            if isinstance(v, dict) and "requests_1_256_queries" in v:
+                srv[key] = {"p50_ms": v["requests_1_256_queries"]["p50_ms"],
+                            "p99_ms": v["requests_1_256_queries"]["p99_ms"],
+                            "queries_per_s": v["queries_per_s"]}
+        out["serving_c5_1_256_query_requests"] = srv
+    if radius:
+        out["radius"] = {"qps": radius["qps"], "identical_to_oracle_sample":
+                         radius["identical_to_oracle_sample"]}
+    if ivf:
+        out["ivf_flat"] = {"qps": ivf["qps"], "recall": ivf["recall_at_k_vs_exact"]}
+    return out
 
 
 def run_sharded(ab, args, rank, world, local):
@@ -557,7 +748,7 @@ def run_sharded(ab, args, rank, world, local):
 
 
 def run_knn(ab, nx=4_000_000, nq=10_000, d=128, k=100, comps=1024, seed=3, reps=3, plain=True,
-            metrics=("euclidean", "cosine")):
+            metrics=("euclidean", "cosine"), accuracy=True):
     """Brute-force kNN, fp32 euclidean and cosine: 4,000,000 x 128 training
     rows from a 1,024-component Gaussian mixture (the k-means recipe) plus 1%
     exact duplicate rows (ties), 10,000 queries from the same mixture, k =
@@ -610,6 +801,7 @@ def run_knn(ab, nx=4_000_000, nq=10_000, d=128, k=100, comps=1024, seed=3, reps=
             "tensor_tflops_algorithmic":
                 flops / (tc["kernel_ms"].get("knn_tc", float("nan")) / 1e3) / 1e12,
             "candidate_list_mean": tc["list_mean"], "plain_fallback_queries": tc["fallback"],
+            "accuracy": knn_accuracy(X, Q, tc["ind"], tc["dist"], k, metric) if accuracy else None,
             "timing": "wall clock of one da_nn_kneighbors_s call with host arrays (best of 3)"}
     first = out[metrics[0]]
     return dict(first, **{m: out[m] for m in metrics[1:]})

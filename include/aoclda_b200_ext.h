@@ -127,8 +127,10 @@ da_status da_b200_kmeans_batched_s(da_int n_inst, const da_int *n_samples,
  * The work is enqueued on `stream` (a cudaStream_t; NULL = legacy default
  * stream) and the call returns without waiting for it.  The first call on a
  * device looks up the scratch array's address; make it before any stream
- * capture on that device.  Calls share the scratch array: calls whose work
- * overlaps on the GPU race on it. */
+ * capture on that device.  The address is kept per device and context: after
+ * cudaDeviceReset (or with another context current) the next call looks it
+ * up again.  Calls share the scratch array: calls whose work overlaps on the
+ * GPU race on it. */
 #define DA_B200_KNN_NOALLOC_SCRATCH_BYTES (32u << 20)
 da_status da_b200_knn_euclidean_noalloc_s(const float *X, da_int n, const float *Q, da_int nq,
                                           da_int d, da_int ld, da_int k, float *dist,

@@ -56,6 +56,12 @@ def lib():
         _lib.orc_knn_reference_ties_d.argtypes = [i, P, i, P]
         _lib.orc_knn_reference_ties_d.restype = None
         _lib.orc_num_threads.restype = i
+        for sfx in ("s", "d"):
+            f = getattr(_lib, f"orc_kmeanspp_{sfx}")
+            f.argtypes = [i, i, P, i, C.c_longlong, i, P, P]
+            f.restype = i
+        _lib.orc_lloyd_blas_s.argtypes = [i, i, P, i, P, P, i, P, i]
+        _lib.orc_lloyd_blas_s.restype = i
     return _lib
 
 
@@ -330,3 +336,69 @@ def knn_reference_ties(keys, k):
 
 def num_threads():
     return lib().orc_num_threads()
+
+
+def kmeanspp(X, k, seed, cost_fp64=False, gemm=None):
+    """Row indices of the k-means++ initial centres (oracle_kpp.cpp, after
+    kmeans.cpp:1491-1664 and :1814-1822): the reference's std::mt19937_64
+    draws, distances in GEMM form, candidate costs summed in the working
+    precision (fp64 with cost_fp64).  gemm: an OpenBLAS handle (openblas())
+    for BLAS dot products instead of the sequential fma chain."""
+    X = np.ascontiguousarray(X)
+    n, d = X.shape
+    chosen = np.zeros(k, dtype=np.int32)
+    fn = None
+    if gemm is not None:
+        fn = gemm.sgemm if X.dtype == np.float32 else gemm.dgemm
+    r = getattr(lib(), f"orc_kmeanspp_{_sfx(X.dtype)}")(n, d, _p(X), k, int(seed),
+                                                         1 if cost_fp64 else 0, fn, _p(chosen))
+    if r < 0:
+        raise ValueError("kmeanspp: bad arguments")
+    return chosen
+
+
+class openblas:
+    """The OpenBLAS that ships with scipy (cblas_sgemm / cblas_dgemm and its
+    thread-count setter), loaded for the CPU baseline."""
+
+    def __init__(self):
+        import glob
+        import scipy
+        libs = os.path.join(os.path.dirname(os.path.dirname(scipy.__file__)), "scipy.libs")
+        cand = sorted(glob.glob(os.path.join(libs, "libscipy_openblas-*.so")))
+        if not cand:
+            raise OSError("scipy's OpenBLAS not found")
+        self.path = cand[0]
+        self.lib = C.CDLL(self.path)
+        self.sgemm = C.cast(self.lib.scipy_cblas_sgemm, C.c_void_p).value
+        self.dgemm = C.cast(self.lib.scipy_cblas_dgemm, C.c_void_p).value
+        self.lib.scipy_openblas_set_num_threads.argtypes = [C.c_int]
+        self.lib.scipy_openblas_get_num_threads.restype = C.c_int
+        self.lib.scipy_openblas_get_config.restype = C.c_char_p
+
+    def set_threads(self, t):
+        self.lib.scipy_openblas_set_num_threads(int(t))
+
+    def threads(self):
+        return int(self.lib.scipy_openblas_get_num_threads())
+
+    def config(self):
+        return self.lib.scipy_openblas_get_config().decode()
+
+
+def lloyd_blas(X, C, labels, n_iter, blas, threads=0):
+    """n_iter Lloyd iterations of the reference's blocked BLAS form
+    (oracle_blas.c, after kmeans_lloyd.hpp:106-405) in place on C (k x d,
+    fp32) and labels; BLAS one thread per call inside the OpenMP region.
+    Returns the number of labels changed by the last iteration."""
+    n, d = X.shape
+    old = blas.threads()
+    blas.set_threads(1)
+    try:
+        r = lib().orc_lloyd_blas_s(n, d, _p(X), C.shape[0], _p(C), _p(labels), n_iter,
+                                   blas.sgemm, threads)
+    finally:
+        blas.set_threads(old)
+    if r < 0:
+        raise MemoryError("lloyd_blas")
+    return r

@@ -1,9 +1,9 @@
 """Generate the golden fixtures of tests/golden/ from the AOCL-DA test assets.
 
-Run in a container where the AOCL-DA source tree is mounted (default
-/root/reference, override with AOCLDA_REF):
+Run where the AOCL-DA source tree is available, with AOCLDA_REF naming its
+root directory:
 
-    python tests/golden/make_golden.py
+    AOCLDA_REF=<path to the AOCL-DA source tree> python tests/golden/make_golden.py
 
 It converts, without retyping any value:
   * the "large data" kNN known-answer sets of the reference's nearest-neighbour
@@ -33,7 +33,9 @@ import re
 
 import numpy as np
 
-REF = os.environ.get("AOCLDA_REF", "/root/reference")
+REF = os.environ.get("AOCLDA_REF")
+if not REF:
+    raise SystemExit("set AOCLDA_REF to the root of the AOCL-DA source tree")
 OUT = os.path.dirname(os.path.abspath(__file__))
 NN = os.path.join(REF, "tests", "data", "nn_data")
 UT = os.path.join(REF, "tests", "unit_tests")
