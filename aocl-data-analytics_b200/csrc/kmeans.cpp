@@ -202,8 +202,9 @@ template <typename T> static inline T host_at(const KMeans<T> &km, da_int i, da_
 // reference's order (the first centre, then n_trials canonical doubles per
 // further centre, consumed by std::discrete_distribution one each); the
 // device maps the draws to rows (kmeans_kpp.cu), computes the candidates'
-// distances and costs, chooses and updates the weights, with no host round
-// trip per centre.
+// distances and their costs -- the reference's serial sums in the working
+// precision, reproduced exactly -- chooses and updates the weights, with no
+// host round trip per centre.
 template <typename T> da_status KMeans<T>::kmeans_plusplus(T *dC) {
     cudaStream_t st = cuda->stream;
     const da_int n = n_samples, k = n_clusters, d = n_features;
@@ -212,8 +213,7 @@ template <typename T> da_status KMeans<T>::kmeans_plusplus(T *dC) {
     if (!dW.ensure((size_t)n * sizeof(T)) || !dKD.ensure((size_t)n * n_trials * sizeof(T)) ||
         !dCand.ensure((size_t)(2 * n_trials + k + 2) * sizeof(int)) ||
         !dKppU.ensure((size_t)std::max<da_int>(1, (k - 1) * n_trials) * sizeof(double)) ||
-        !dKppBs.ensure((size_t)(nb + n_trials) * sizeof(double)) ||
-        !dPartials.ensure((size_t)148 * 4 * n_trials * sizeof(double)))
+        !dKppBs.ensure((size_t)(nb + n_trials) * sizeof(double)))
         return err->error(da_status_memory_error, "Device memory allocation failed.");
     int *dCandv = dCand.as<int>();
     int *dUnc = dCandv + n_trials;
@@ -255,8 +255,8 @@ template <typename T> da_status KMeans<T>::kmeans_plusplus(T *dC) {
                      "k-means++ draws");
             B200_TRY(launch_kpp_dist<T>(dX.as<T>(), ld, n, d, dXn.as<T>(), dCandv, n_trials,
                                         dKD.as<T>(), st), "k-means++ distances");
-            B200_TRY(launch_kpp_cost<T>(dW.as<T>(), dKD.as<T>(), n, n_trials, dPartials.as<double>(),
-                                        dCost, st), "k-means++ cost");
+            B200_TRY(launch_kpp_serial_cost<T>(dW.as<T>(), dKD.as<T>(), (int)n, (int)n_trials,
+                                               dCost, st), "k-means++ cost");
             B200_TRY(launch_kpp_select_update<T>(dW.as<T>(), dKD.as<T>(), (int)n, dCost, dCandv,
                                                  (int)n_trials, dChosen, (int)c, dBs, st),
                      "k-means++ update");

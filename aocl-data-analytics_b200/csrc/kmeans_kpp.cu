@@ -19,9 +19,12 @@
 //   * kpp_exact_kernel: the draws that are not certified (about one per
 //     k-means++ run on a million rows) are redone with the sequential sums
 //     themselves, in the reference's order of operations.
-// The candidates' distances and costs are the existing kpp_dist / kpp_cost
-// kernels; kpp_select_update_kernel picks the candidate with the smallest
-// finite cost (repeats skipped, first strictly smaller wins), writes it to
+// The candidates' distances are the kpp_dist kernel; their costs are the
+// reference's serial sums in the working precision, reproduced exactly by
+// kpp_serial_cost_kernel (at a million fp32 rows the rounding of those sums
+// decides between candidates whose costs are that close, so an fp64 sum
+// would choose differently); kpp_select_update_kernel picks the candidate
+// with the smallest finite cost (repeats skipped, first strictly smaller wins), writes it to
 // `chosen`, lowers w to the minimum with its distances, zeroes its own
 // weight and writes the block sums of the new w.  No host round trip per
 // centre.
@@ -256,6 +259,200 @@ kpp_exact_kernel(const T *w, int n, const double *U, int nt, int *cand, const in
     }
 }
 
+// ------------------------------------------------ serial cost sums ------
+// The reference's candidate cost (kmeans.cpp:1624-1636) is the serial sum,
+// in the working precision T and index order from 0, of m_i = max(0,
+// min(w_i, d_i)).  It is reproduced exactly, not approximated: while the
+// running sum s stays inside one binade [2^E, 2^(E+1)) every addition
+// rounds to the grid g = 2^(E - MANT) (s itself lies on it), so
+// fl(s + m_i) = s + RN_g(m_i) and a whole run of additions is one integer
+// sum of the independently rounded terms q_i = RN_g(m_i).  A chunk of 4,096
+// terms is added that way when no term is a tie (m_i / g exactly half-way,
+// where ties-to-even depends on the running sum's last bit) and the sum stays
+// below 2^(E+1); otherwise the terms before the first such term are added
+// as integers, that term is added serially in T (fl(s + m_p)), and the walk
+// goes on after it with the new binade.  One block per candidate; the
+// result is the T value the reference computes, stored as a double.
+template <typename T> struct FpTraits;
+template <> struct FpTraits<float> {
+    static constexpr int MANT = 23, EMIN = -126;
+    static __device__ __forceinline__ int exponent(float s) {
+        return (int)((__float_as_uint(s) >> 23) & 0xFF) - 127;
+    }
+};
+template <> struct FpTraits<double> {
+    static constexpr int MANT = 52, EMIN = -1022;
+    static __device__ __forceinline__ int exponent(double s) {
+        return (int)((__double_as_longlong(s) >> 52) & 0x7FF) - 1023;
+    }
+};
+
+static constexpr int SC_THREADS = 512;
+static constexpr int SC_PER = 8;
+static constexpr int SC_CHUNK = SC_THREADS * SC_PER;
+static constexpr unsigned long long SC_SAT = 1ull << 62;
+
+__device__ __forceinline__ unsigned long long sat_add(unsigned long long a, unsigned long long b) {
+    const unsigned long long r = a + b; // a, b <= 2^62: no wrap
+    return r > SC_SAT ? SC_SAT : r;
+}
+
+// the reference's works5 element: std::max(0, std::min(w, d))
+template <typename T> __device__ __forceinline__ T kpp_term(T wv, T dv) {
+    const T mn = (dv < wv) ? dv : wv;
+    return (T(0) < mn) ? mn : T(0);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SC_THREADS)
+kpp_serial_cost_kernel(const T *w, const T *D, int n, double *cost) {
+    using F = FpTraits<T>;
+    __shared__ unsigned long long s_wsum[SC_THREADS / 32];
+    __shared__ int s_wflag[SC_THREADS / 32];
+    __shared__ int s_p;
+    __shared__ T s_sum;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const T *Dt = D + (size_t)blockIdx.x * n;
+    T s = T(0);
+    long long pos = 0;
+    T m[SC_PER], mn[SC_PER];
+    // terms [at + 8 tid, at + 8 tid + 8) of the walk (0 past the end)
+    auto load = [&](T (&dst)[SC_PER], long long at) {
+#pragma unroll
+        for (int e = 0; e < SC_PER; ++e) {
+            const long long i = at + (long long)threadIdx.x * SC_PER + e;
+            dst[e] = i < n ? kpp_term(w[i], Dt[i]) : T(0);
+        }
+    };
+    load(m, 0);
+    while (pos < n && isfinite(s)) {
+        load(mn, pos + SC_CHUNK); // the next chunk, in flight while this one is summed
+        if (s == T(0)) {
+            // 0 + m = m exactly: the first nonzero term starts the sum
+            int mine = 0x7fffffff;
+#pragma unroll
+            for (int e = SC_PER - 1; e >= 0; --e)
+                if (m[e] != T(0)) mine = (int)threadIdx.x * SC_PER + e;
+            __syncthreads();
+            if (threadIdx.x == 0) s_p = 0x7fffffff;
+            __syncthreads();
+            if (mine != 0x7fffffff) atomicMin(&s_p, mine);
+            __syncthreads();
+            const int p = s_p;
+            if (p == 0x7fffffff) {
+                pos += SC_CHUNK;
+#pragma unroll
+                for (int e = 0; e < SC_PER; ++e) m[e] = mn[e];
+                continue;
+            }
+            if ((int)threadIdx.x == p / SC_PER) {
+#pragma unroll
+                for (int e = 0; e < SC_PER; ++e)
+                    if (e == p % SC_PER) s_sum = m[e];
+            }
+            __syncthreads();
+            s = s_sum;
+            pos += p + 1;
+            load(m, pos);
+            continue;
+        }
+        // the grid of the current binade, in units of g = 2^-sh
+        const int ex = F::exponent(s);
+        const bool sub = ex < F::EMIN;
+        const int E = sub ? F::EMIN : ex;
+        const int sh = F::MANT - E;
+        const unsigned long long limit = sub ? (1ull << F::MANT) : (2ull << F::MANT);
+        const unsigned long long s_int = (unsigned long long)ldexp((double)s, sh);
+        unsigned long long q[SC_PER];
+        unsigned long long tsum = 0;
+        int tie = 0;
+#pragma unroll
+        for (int e = 0; e < SC_PER; ++e) {
+            const double x = ldexp((double)m[e], sh);
+            unsigned long long qe = SC_SAT; // leaves the binade by itself
+            if (x < (double)limit) {
+                const double fl = floor(x), fr = x - fl;
+                qe = (unsigned long long)fl + (fr > 0.5 ? 1ull : 0ull);
+                if (fr == 0.5) {
+                    tie = 1;
+                    qe = SC_SAT; // ties-to-even needs the running sum: serial
+                }
+            }
+            q[e] = qe;
+            tsum = sat_add(tsum, qe);
+        }
+        // block total (saturating) and tie flag
+        unsigned long long incl = tsum;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl = sat_add(incl, y);
+        }
+        unsigned long long exw = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) exw = 0;
+        const int wt = __any_sync(0xffffffffu, tie);
+        __syncthreads();
+        if (lane == 31) {
+            s_wsum[warp] = incl;
+            s_wflag[warp] = wt;
+        }
+        __syncthreads();
+        unsigned long long Q = 0, before = 0;
+        int anytie = 0;
+        for (int v = 0; v < SC_THREADS / 32; ++v) {
+            if (v == warp) before = Q;
+            Q = sat_add(Q, s_wsum[v]);
+            anytie |= s_wflag[v];
+        }
+        if (!anytie && s_int + Q < limit) {
+            s = (T)ldexp((double)(s_int + Q), -sh);
+            pos += SC_CHUNK;
+#pragma unroll
+            for (int e = 0; e < SC_PER; ++e) m[e] = mn[e];
+            continue;
+        }
+        // the first term that ties or leaves the binade
+        unsigned long long run = sat_add(before, exw);
+        int mine = 0x7fffffff;
+        unsigned long long run_at = 0;
+#pragma unroll
+        for (int e = 0; e < SC_PER; ++e) {
+            const unsigned long long nxt = sat_add(run, q[e]);
+            if (mine == 0x7fffffff && (q[e] == SC_SAT || s_int + nxt >= limit)) {
+                mine = (int)threadIdx.x * SC_PER + e;
+                run_at = run;
+            }
+            run = nxt;
+        }
+        if (threadIdx.x == 0) s_p = 0x7fffffff;
+        __syncthreads();
+        if (mine != 0x7fffffff) atomicMin(&s_p, mine);
+        __syncthreads();
+        const int p = s_p;
+        if (mine == p) {
+            // the terms before p on the grid, then term p serially in T
+            T mp = T(0);
+#pragma unroll
+            for (int e = 0; e < SC_PER; ++e)
+                if (e == p % SC_PER) mp = m[e];
+            const T sp = (T)ldexp((double)(s_int + run_at), -sh);
+            s_sum = add_rn(sp, mp);
+        }
+        __syncthreads();
+        s = s_sum;
+        pos += p + 1;
+        load(m, pos);
+    }
+    if (threadIdx.x == 0) cost[blockIdx.x] = (double)s;
+}
+
+template <typename T>
+cudaError_t launch_kpp_serial_cost(const T *w, const T *D, int n, int nt, double *cost,
+                                   cudaStream_t s) {
+    kpp_serial_cost_kernel<T><<<nt, SC_THREADS, 0, s>>>(w, D, n, cost);
+    return cudaGetLastError();
+}
+
 // Choose the candidate (kmeans.cpp:1614-1646): repeats skipped, the first
 // finite cost strictly below the best so far; none: index 0.  Every block
 // makes the same choice; block 0 records it.  Then w_i = max(0, min(w_i,
@@ -349,7 +546,9 @@ cudaError_t launch_kpp_select_update(T *w, const T *D, int n, const double *cost
                                             int, int, int *, int *, int *, cudaStream_t);       \
     template cudaError_t launch_kpp_select_update<T>(T *, const T *, int, const double *,       \
                                                      const int *, int, int *, int, double *,    \
-                                                     cudaStream_t);
+                                                     cudaStream_t);                             \
+    template cudaError_t launch_kpp_serial_cost<T>(const T *, const T *, int, int, double *,    \
+                                                   cudaStream_t);
 B200_KPP_INST(float)
 B200_KPP_INST(double)
 
