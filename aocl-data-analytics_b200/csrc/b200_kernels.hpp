@@ -282,12 +282,15 @@ template <typename T>
 cudaError_t launch_kpp_draw(const T *w, int n, const double *bs, const double *U, int nt,
                             int force_exact, int *cand, int *unc, int *exact_count,
                             cudaStream_t s);
-// cost[t] = the serial sum in T, index order from 0, of max(0, min(w_i,
-// D[t*n + i])) -- the reference's value, computed exactly (kmeans_kpp.cu) --
-// for t < nt, stored as double.
+// Distances of every row to the t candidate rows (D[c*n + i], as
+// launch_kpp_dist) and cost[c] = the serial sum in T, index order from 0, of
+// max(0, min(w_i, D[c*n + i])) -- the reference's value, computed exactly
+// (kmeans_kpp.cu) -- stored as double.  work: kpp_cost_work_bytes(n, t).
 template <typename T>
-cudaError_t launch_kpp_serial_cost(const T *w, const T *D, int n, int nt, double *cost,
-                                   cudaStream_t s);
+cudaError_t launch_kpp_dist_cost(const T *X, int ldx, int n, int d, const T *xnorm,
+                                 const int *cand, int t, const T *w, T *D, double *cost,
+                                 void *work, cudaStream_t s);
+size_t kpp_cost_work_bytes(int n, int t);
 // Choose among the nt candidates by cost (chosen[c]), w_i = max(0, min(w_i,
 // D_best,i)), w_best = 0, block sums of the new w.
 template <typename T>

@@ -213,7 +213,8 @@ template <typename T> da_status KMeans<T>::kmeans_plusplus(T *dC) {
     if (!dW.ensure((size_t)n * sizeof(T)) || !dKD.ensure((size_t)n * n_trials * sizeof(T)) ||
         !dCand.ensure((size_t)(2 * n_trials + k + 2) * sizeof(int)) ||
         !dKppU.ensure((size_t)std::max<da_int>(1, (k - 1) * n_trials) * sizeof(double)) ||
-        !dKppBs.ensure((size_t)(nb + n_trials) * sizeof(double)))
+        !dKppBs.ensure((size_t)(nb + n_trials) * sizeof(double)) ||
+        !dPartials.ensure(kpp_cost_work_bytes((int)n, (int)n_trials)))
         return err->error(da_status_memory_error, "Device memory allocation failed.");
     int *dCandv = dCand.as<int>();
     int *dUnc = dCandv + n_trials;
@@ -253,10 +254,9 @@ template <typename T> da_status KMeans<T>::kmeans_plusplus(T *dC) {
             B200_TRY(launch_kpp_draw<T>(dW.as<T>(), (int)n, dBs, dU + (size_t)(c - 1) * n_trials,
                                         (int)n_trials, force_exact, dCandv, dUnc, dFlag + 1, st),
                      "k-means++ draws");
-            B200_TRY(launch_kpp_dist<T>(dX.as<T>(), ld, n, d, dXn.as<T>(), dCandv, n_trials,
-                                        dKD.as<T>(), st), "k-means++ distances");
-            B200_TRY(launch_kpp_serial_cost<T>(dW.as<T>(), dKD.as<T>(), (int)n, (int)n_trials,
-                                               dCost, st), "k-means++ cost");
+            B200_TRY(launch_kpp_dist_cost<T>(dX.as<T>(), ld, n, d, dXn.as<T>(), dCandv, n_trials,
+                                             dW.as<T>(), dKD.as<T>(), dCost, dPartials.p, st),
+                     "k-means++ distances and costs");
             B200_TRY(launch_kpp_select_update<T>(dW.as<T>(), dKD.as<T>(), (int)n, dCost, dCandv,
                                                  (int)n_trials, dChosen, (int)c, dBs, st),
                      "k-means++ update");

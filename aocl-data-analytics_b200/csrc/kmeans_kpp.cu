@@ -262,17 +262,26 @@ kpp_exact_kernel(const T *w, int n, const double *U, int nt, int *cand, const in
 // ------------------------------------------------ serial cost sums ------
 // The reference's candidate cost (kmeans.cpp:1624-1636) is the serial sum,
 // in the working precision T and index order from 0, of m_i = max(0,
-// min(w_i, d_i)).  It is reproduced exactly, not approximated: while the
-// running sum s stays inside one binade [2^E, 2^(E+1)) every addition
-// rounds to the grid g = 2^(E - MANT) (s itself lies on it), so
-// fl(s + m_i) = s + RN_g(m_i) and a whole run of additions is one integer
-// sum of the independently rounded terms q_i = RN_g(m_i).  A chunk of 4,096
-// terms is added that way when no term is a tie (m_i / g exactly half-way,
-// where ties-to-even depends on the running sum's last bit) and the sum stays
-// below 2^(E+1); otherwise the terms before the first such term are added
-// as integers, that term is added serially in T (fl(s + m_p)), and the walk
-// goes on after it with the new binade.  One block per candidate; the
-// result is the T value the reference computes, stored as a double.
+// min(w_i, d_i)).  It is reproduced exactly, not approximated.  While the
+// running sum s stays inside one binade [2^E, 2^(E+1)) every addition rounds
+// to the grid g = 2^(E - MANT) (s itself lies on it), so fl(s + m_i) =
+// s + RN_g(m_i) and a run of additions is one integer sum of the
+// independently rounded terms q_i = RN_g(m_i) -- unless a term is a tie
+// (m_i / g exactly half-way: ties-to-even then depends on the running sum's
+// last bit) or the sum leaves the binade; such a term is added serially in T.
+// Three passes per candidate set:
+//   * kpp_dist_csum_kernel: the candidates' distances and, per 256-row
+//     chunk, the fp64 sum of its terms;
+//   * kpp_chunk_q_kernel: the fp64 prefix of the chunk sums predicts the
+//     binade E_j of the serial sum at each chunk; the chunk's integer total
+//     Q_j on that binade's grid (flagged when a term ties);
+//   * kpp_walk_kernel, one block per candidate: walks the chunk records; a
+//     chunk is added as s += Q_j g when the running sum is in binade E_j, the
+//     chunk has no tie and the sum stays in the binade -- else the chunk is
+//     summed exactly term by term (integer runs, serial steps at the first
+//     tie or binade crossing).  The prediction only chooses the fast path;
+//     every fast step is checked, so the result is the reference's T value
+//     whatever the fp64 prefix says.
 template <typename T> struct FpTraits;
 template <> struct FpTraits<float> {
     static constexpr int MANT = 23, EMIN = -126;
@@ -287,9 +296,10 @@ template <> struct FpTraits<double> {
     }
 };
 
-static constexpr int SC_THREADS = 512;
-static constexpr int SC_PER = 8;
-static constexpr int SC_CHUNK = SC_THREADS * SC_PER;
+static constexpr int CK = 256;           // terms per chunk
+static constexpr int WALK_THREADS = 256;
+static constexpr int WALK_PER = 4; // chunk records per thread per pass
+static constexpr int NO_BINADE = -100000; // chunk record: sum it exactly
 static constexpr unsigned long long SC_SAT = 1ull << 62;
 
 __device__ __forceinline__ unsigned long long sat_add(unsigned long long a, unsigned long long b) {
@@ -303,154 +313,422 @@ template <typename T> __device__ __forceinline__ T kpp_term(T wv, T dv) {
     return (T(0) < mn) ? mn : T(0);
 }
 
-template <typename T>
-__global__ void __launch_bounds__(SC_THREADS)
-kpp_serial_cost_kernel(const T *w, const T *D, int n, double *cost) {
-    using F = FpTraits<T>;
-    __shared__ unsigned long long s_wsum[SC_THREADS / 32];
-    __shared__ int s_wflag[SC_THREADS / 32];
-    __shared__ int s_p;
-    __shared__ T s_sum;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const T *Dt = D + (size_t)blockIdx.x * n;
-    T s = T(0);
-    long long pos = 0;
-    T m[SC_PER], mn[SC_PER];
-    // terms [at + 8 tid, at + 8 tid + 8) of the walk (0 past the end)
-    auto load = [&](T (&dst)[SC_PER], long long at) {
-#pragma unroll
-        for (int e = 0; e < SC_PER; ++e) {
-            const long long i = at + (long long)threadIdx.x * SC_PER + e;
-            dst[e] = i < n ? kpp_term(w[i], Dt[i]) : T(0);
-        }
-    };
-    load(m, 0);
-    while (pos < n && isfinite(s)) {
-        load(mn, pos + SC_CHUNK); // the next chunk, in flight while this one is summed
-        if (s == T(0)) {
-            // 0 + m = m exactly: the first nonzero term starts the sum
-            int mine = 0x7fffffff;
-#pragma unroll
-            for (int e = SC_PER - 1; e >= 0; --e)
-                if (m[e] != T(0)) mine = (int)threadIdx.x * SC_PER + e;
-            __syncthreads();
-            if (threadIdx.x == 0) s_p = 0x7fffffff;
-            __syncthreads();
-            if (mine != 0x7fffffff) atomicMin(&s_p, mine);
-            __syncthreads();
-            const int p = s_p;
-            if (p == 0x7fffffff) {
-                pos += SC_CHUNK;
-#pragma unroll
-                for (int e = 0; e < SC_PER; ++e) m[e] = mn[e];
-                continue;
-            }
-            if ((int)threadIdx.x == p / SC_PER) {
-#pragma unroll
-                for (int e = 0; e < SC_PER; ++e)
-                    if (e == p % SC_PER) s_sum = m[e];
-            }
-            __syncthreads();
-            s = s_sum;
-            pos += p + 1;
-            load(m, pos);
-            continue;
-        }
-        // the grid of the current binade, in units of g = 2^-sh
-        const int ex = F::exponent(s);
+// The grid of the binade of s > 0: raw exponent (subnormals: EMIN - 1),
+// sh = -log2(g), the binade's end in grid units, s in grid units.
+template <typename T> struct Binade {
+    int ex, sh;
+    unsigned long long limit, s_int;
+    __device__ __forceinline__ void set(T s) {
+        using F = FpTraits<T>;
+        ex = F::exponent(s);
         const bool sub = ex < F::EMIN;
-        const int E = sub ? F::EMIN : ex;
-        const int sh = F::MANT - E;
-        const unsigned long long limit = sub ? (1ull << F::MANT) : (2ull << F::MANT);
-        const unsigned long long s_int = (unsigned long long)ldexp((double)s, sh);
-        unsigned long long q[SC_PER];
-        unsigned long long tsum = 0;
-        int tie = 0;
+        sh = F::MANT - (sub ? F::EMIN : ex);
+        limit = sub ? (1ull << F::MANT) : (2ull << F::MANT);
+        s_int = (unsigned long long)ldexp((double)s, sh);
+    }
+    // q = RN_g(m) for a non-tie; SC_SAT for a tie or a term that leaves the
+    // binade by itself.  t = 2 m / g is exact (power-of-two scaling in
+    // double, in two factors so that neither overflows); RN(t / 2) of a
+    // non-tie = (floor(t) + 1) / 2; a tie is t an odd integer.
+    __device__ __forceinline__ unsigned long long q(T m) const {
+        const int e2 = sh + 1, ea = min(e2, 1000), eb = e2 - ea;
+        const double sa = __longlong_as_double((long long)(ea + 1023) << 52);
+        const double sb = __longlong_as_double((long long)(eb + 1023) << 52);
+        const double tt = ((double)m * sa) * sb;
+        if (!(tt < 2.0 * (double)limit)) return SC_SAT;
+        const unsigned long long ti = __double2ull_rz(tt);
+        if ((ti & 1ull) && tt == __ull2double_rn(ti)) return SC_SAT;
+        return (ti + 1ull) >> 1;
+    }
+    // m stays inside the binade by itself (so SC_SAT from q() means a tie)
+    __device__ __forceinline__ bool q_in_range(T m) const {
+        const int e2 = sh + 1, ea = min(e2, 1000), eb = e2 - ea;
+        const double sa = __longlong_as_double((long long)(ea + 1023) << 52);
+        const double sb = __longlong_as_double((long long)(eb + 1023) << 52);
+        return ((double)m * sa) * sb < 2.0 * (double)limit;
+    }
+    __device__ __forceinline__ T value(unsigned long long units) const {
+        return (T)ldexp((double)units, -sh);
+    }
+};
+
+// Saturating prefix sums of one value per thread over a block of NT
+// threads: returns the inclusive prefix, `excl` the exclusive one (exact
+// while below 2^62), `total` the block's sum.  shm: 2 * (NT / 32) + 1 words.
+template <int NT>
+__device__ unsigned long long block_scan_sat(unsigned long long v, unsigned long long *shm,
+                                             unsigned long long &excl,
+                                             unsigned long long &total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = NT / 32;
+    unsigned long long x = v;
 #pragma unroll
-        for (int e = 0; e < SC_PER; ++e) {
-            const double x = ldexp((double)m[e], sh);
-            unsigned long long qe = SC_SAT; // leaves the binade by itself
-            if (x < (double)limit) {
-                const double fl = floor(x), fr = x - fl;
-                qe = (unsigned long long)fl + (fr > 0.5 ? 1ull : 0ull);
-                if (fr == 0.5) {
-                    tie = 1;
-                    qe = SC_SAT; // ties-to-even needs the running sum: serial
-                }
-            }
-            q[e] = qe;
-            tsum = sat_add(tsum, qe);
-        }
-        // block total (saturating) and tie flag
-        unsigned long long incl = tsum;
+    for (int off = 1; off < 32; off <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x = sat_add(x, y);
+    }
+    unsigned long long xe = __shfl_up_sync(0xffffffffu, x, 1);
+    if (lane == 0) xe = 0;
+    __syncthreads();
+    if (lane == 31) shm[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned long long y = lane < NW ? shm[lane] : 0ull;
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
-            const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, off);
-            if (lane >= off) incl = sat_add(incl, y);
+            const unsigned long long z = __shfl_up_sync(0xffffffffu, y, off);
+            if (lane >= off) y = sat_add(y, z);
         }
-        unsigned long long exw = __shfl_up_sync(0xffffffffu, incl, 1);
-        if (lane == 0) exw = 0;
-        const int wt = __any_sync(0xffffffffu, tie);
+        unsigned long long ye = __shfl_up_sync(0xffffffffu, y, 1);
+        if (lane == 0) ye = 0;
+        if (lane < NW) shm[NW + lane] = ye;
+        if (lane == NW - 1) shm[2 * NW] = y;
+    }
+    __syncthreads();
+    total = shm[2 * NW];
+    excl = sat_add(shm[NW + warp], xe);
+    return sat_add(shm[NW + warp], x);
+}
+
+// Distances of a 256-row chunk to the candidates (one thread per row), with
+// the chunk's fp64 sum of the cost terms per candidate.  A thread holds 64
+// (fp32) or 32 (fp64) features of its row in registers at a time -- 16
+// independent 16-byte loads in flight -- and runs eight candidates' fma
+// chains over them (features in order), the candidates' values broadcast
+// from shared memory (SMEM) or read through L1.
+template <typename T> struct SegTraits;
+template <> struct SegTraits<float> {
+    static constexpr int SEG = 64; // features per register segment
+    using V = float4;
+    static constexpr int W = 4;
+    static __device__ __forceinline__ void split(const float4 &v, float (&o)[4]) {
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    }
+};
+template <> struct SegTraits<double> {
+    static constexpr int SEG = 32;
+    using V = double2;
+    static constexpr int W = 2;
+    static __device__ __forceinline__ void split(const double2 &v, double (&o)[2]) {
+        o[0] = v.x; o[1] = v.y;
+    }
+};
+
+template <typename T, bool SMEM>
+__global__ void __launch_bounds__(CK, 2)
+kpp_dist_csum_kernel(const T *X, int ld, int n, int d, const T *xnorm, const int *cand, int t,
+                     const T *w, T *D, double *csum, int nchunks) {
+    using S = SegTraits<T>;
+    constexpr int NV = S::SEG / S::W;
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ double red[CK / 32][8];
+    T *cs = reinterpret_cast<T *>(sm); // [t][dp] when SMEM
+    const int dp = (d + S::W - 1) / S::W * S::W;
+    if (SMEM) {
+        for (int e = threadIdx.x; e < t * dp; e += CK) {
+            const int c = e / dp, f = e % dp;
+            cs[e] = f < d ? X[(size_t)cand[c] * ld + f] : T(0);
+        }
         __syncthreads();
-        if (lane == 31) {
-            s_wsum[warp] = incl;
-            s_wflag[warp] = wt;
-        }
-        __syncthreads();
-        unsigned long long Q = 0, before = 0;
-        int anytie = 0;
-        for (int v = 0; v < SC_THREADS / 32; ++v) {
-            if (v == warp) before = Q;
-            Q = sat_add(Q, s_wsum[v]);
-            anytie |= s_wflag[v];
-        }
-        if (!anytie && s_int + Q < limit) {
-            s = (T)ldexp((double)(s_int + Q), -sh);
-            pos += SC_CHUNK;
+    }
+    const int i = blockIdx.x * CK + threadIdx.x;
+    const bool valid = i < n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const T *x = X + (size_t)(valid ? i : 0) * ld;
+    const T xn = valid ? xnorm[i] : T(0);
+    const T wi = valid ? w[i] : T(0);
+    for (int c0 = 0; c0 < t; c0 += 8) {
+        T s[8];
 #pragma unroll
-            for (int e = 0; e < SC_PER; ++e) m[e] = mn[e];
-            continue;
+        for (int g = 0; g < 8; ++g) s[g] = T(0);
+        int cg[8];
+#pragma unroll
+        for (int g = 0; g < 8; ++g) cg[g] = min(c0 + g, t - 1);
+        if (valid) {
+            for (int f0 = 0; f0 < d; f0 += S::SEG) {
+                typename S::V xv[NV];
+#pragma unroll
+                for (int v = 0; v < NV; ++v)
+                    if (f0 + v * S::W < d) // rows are padded to 16 bytes
+                        xv[v] = *reinterpret_cast<const typename S::V *>(x + f0 + v * S::W);
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    const int fb = f0 + v * S::W;
+                    if (fb >= d) break;
+                    T xe[S::W];
+                    S::split(xv[v], xe);
+#pragma unroll
+                    for (int g = 0; g < 8; ++g) {
+                        T ce[S::W];
+                        if (SMEM) {
+                            S::split(*reinterpret_cast<const typename S::V *>(cs + (size_t)cg[g] * dp + fb), ce);
+                        } else {
+                            const T *yr = X + (size_t)cand[cg[g]] * ld + fb;
+                            S::split(*reinterpret_cast<const typename S::V *>(yr), ce);
+                        }
+#pragma unroll
+                        for (int u = 0; u < S::W; ++u)
+                            if (fb + u < d) s[g] = fma_rn(xe[u], ce[u], s[g]);
+                    }
+                }
+            }
         }
-        // the first term that ties or leaves the binade
-        unsigned long long run = sat_add(before, exw);
+        double part[8];
+#pragma unroll
+        for (int g = 0; g < 8; ++g) {
+            part[g] = 0.0;
+            if (valid && c0 + g < t) {
+                const T dv = fma_rn(T(-2), s[g], add_rn(xn, xnorm[cand[c0 + g]]));
+                D[(size_t)(c0 + g) * n + i] = dv;
+                part[g] = (double)kpp_term(wi, dv);
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) part[g] += __shfl_xor_sync(0xffffffffu, part[g], off);
+        }
+        __syncthreads();
+        if (lane == 0)
+#pragma unroll
+            for (int g = 0; g < 8; ++g) red[warp][g] = part[g];
+        __syncthreads();
+        if (threadIdx.x < 8 && c0 + (int)threadIdx.x < t) {
+            double a = 0.0;
+            for (int v = 0; v < CK / 32; ++v) a += red[v][threadIdx.x];
+            csum[(size_t)(c0 + threadIdx.x) * nchunks + blockIdx.x] = a;
+        }
+    }
+}
+
+// Exclusive fp64 prefix of the chunk sums of candidate blockIdx.x.
+__global__ void __launch_bounds__(1024) kpp_chunk_prefix_kernel(const double *csum, int nchunks,
+                                                                double *P) {
+    __shared__ double shd[33];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double *cs = csum + (size_t)blockIdx.x * nchunks;
+    double *Pt = P + (size_t)blockIdx.x * nchunks;
+    double carry = 0.0;
+    for (int c0 = 0; c0 < nchunks; c0 += 1024) {
+        const int j = c0 + threadIdx.x;
+        const double v = j < nchunks ? cs[j] : 0.0;
+        double x = v;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const double y = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= off) x += y;
+        }
+        __syncthreads();
+        if (lane == 31) shd[warp] = x;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0.0;
+            for (int q = 0; q < 32; ++q) {
+                const double tq = shd[q];
+                shd[q] = a;
+                a += tq;
+            }
+            shd[32] = a;
+        }
+        __syncthreads();
+        if (j < nchunks) Pt[j] = carry + shd[warp] + (x - v);
+        carry += shd[32];
+    }
+}
+
+// Chunk records of candidate blockIdx.y, one warp per chunk: the binade the
+// fp64 prefix predicts for the serial sum at the chunk (raw exponent of
+// (T)P_j, or NO_BINADE when P_j is 0 or not finite, or when a term ties) and
+// the chunk's integer total on that binade's grid (saturating).
+template <typename T>
+__global__ void __launch_bounds__(256)
+kpp_chunk_q_kernel(const T *w, const T *D, int n, int nchunks, const double *P,
+                   unsigned long long *Qr, int *Er) {
+    const int t = blockIdx.y;
+    const int j = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (j >= nchunks) return;
+    const size_t r = (size_t)t * nchunks + j;
+    const double Pj = P[r];
+    const T Ts = (T)Pj;
+    if (!(Pj > 0.0) || !isfinite(Ts) || Ts == T(0)) {
+        if (lane == 0) {
+            Qr[r] = 0;
+            Er[r] = NO_BINADE;
+        }
+        return;
+    }
+    Binade<T> b;
+    b.set(Ts);
+    const T *Dt = D + (size_t)t * n;
+    unsigned long long a = 0;
+    int tie = 0;
+#pragma unroll
+    for (int u = 0; u < CK / 32; ++u) {
+        const int i = j * CK + u * 32 + lane;
+        if (i < n) {
+            const T m = kpp_term(w[i], Dt[i]);
+            const unsigned long long q = b.q(m);
+            // a tie, unlike a term that leaves the binade, needs the exact path
+            if (q == SC_SAT && b.q_in_range(m)) tie = 1;
+            a = sat_add(a, q);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) a = sat_add(a, __shfl_xor_sync(0xffffffffu, a, off));
+    tie = __any_sync(0xffffffffu, tie);
+    if (lane == 0) {
+        Qr[r] = a;
+        Er[r] = tie ? NO_BINADE : b.ex;
+    }
+}
+
+// The serial sum of candidate blockIdx.x over the chunk records (see above).
+template <typename T>
+__global__ void __launch_bounds__(WALK_THREADS)
+kpp_walk_kernel(const T *w, const T *D, int n, int nchunks, const unsigned long long *Qr,
+                const int *Er, double *cost) {
+    __shared__ unsigned long long shm[2 * (WALK_THREADS / 32) + 1];
+    __shared__ int s_f;
+    __shared__ T s_val;
+    const int t = blockIdx.x;
+    const T *Dt = D + (size_t)t * n;
+    const unsigned long long *Qt = Qr + (size_t)t * nchunks;
+    const int *Et = Er + (size_t)t * nchunks;
+    T s = T(0);
+    int j = 0;
+    while (j < nchunks && isfinite(s)) {
+        Binade<T> b;
+        b.ex = NO_BINADE - 1;
+        b.sh = 0;
+        b.limit = 0;
+        b.s_int = 0;
+        if (s != T(0)) b.set(s);
+        // WALK_PER consecutive records per thread
+        const int r0 = j + (int)threadIdx.x * WALK_PER;
+        unsigned long long qv[WALK_PER];
+        bool okv[WALK_PER];
+        unsigned long long tq = 0;
+#pragma unroll
+        for (int u = 0; u < WALK_PER; ++u) {
+            const int r = r0 + u;
+            const bool valid = r < nchunks;
+            qv[u] = valid ? Qt[r] : 0ull;
+            okv[u] = !valid || Et[r] == b.ex;
+            tq = sat_add(tq, qv[u]);
+        }
+        unsigned long long total, excl;
+        block_scan_sat<WALK_THREADS>(tq, shm, excl, total);
         int mine = 0x7fffffff;
-        unsigned long long run_at = 0;
+        unsigned long long ex_at = 0, run = excl;
 #pragma unroll
-        for (int e = 0; e < SC_PER; ++e) {
-            const unsigned long long nxt = sat_add(run, q[e]);
-            if (mine == 0x7fffffff && (q[e] == SC_SAT || s_int + nxt >= limit)) {
-                mine = (int)threadIdx.x * SC_PER + e;
-                run_at = run;
+        for (int u = 0; u < WALK_PER; ++u) {
+            const unsigned long long nxt = sat_add(run, qv[u]);
+            if (mine == 0x7fffffff && r0 + u < nchunks && (!okv[u] || b.s_int + nxt >= b.limit)) {
+                mine = (int)threadIdx.x * WALK_PER + u;
+                ex_at = run;
             }
             run = nxt;
         }
-        if (threadIdx.x == 0) s_p = 0x7fffffff;
+        if (threadIdx.x == 0) s_f = 0x7fffffff;
         __syncthreads();
-        if (mine != 0x7fffffff) atomicMin(&s_p, mine);
+        if (mine != 0x7fffffff) atomicMin(&s_f, mine);
         __syncthreads();
-        const int p = s_p;
-        if (mine == p) {
-            // the terms before p on the grid, then term p serially in T
-            T mp = T(0);
-#pragma unroll
-            for (int e = 0; e < SC_PER; ++e)
-                if (e == p % SC_PER) mp = m[e];
-            const T sp = (T)ldexp((double)(s_int + run_at), -sh);
-            s_sum = add_rn(sp, mp);
+        const int f = s_f;
+        if (f == 0x7fffffff) {
+            s = b.value(b.s_int + total);
+            j += WALK_THREADS * WALK_PER;
+            continue;
         }
+        // the records before f on the grid
+        if (mine == f) s_val = (f == 0) ? s : b.value(b.s_int + ex_at);
         __syncthreads();
-        s = s_sum;
-        pos += p + 1;
-        load(m, pos);
+        s = s_val;
+        __syncthreads();
+        // chunk j + f, term by term
+        const int c = j + f;
+        int pos = c * CK;
+        const int end = min(n, pos + CK);
+        while (pos < end && isfinite(s)) {
+            const int i = pos + (int)threadIdx.x;
+            const bool in = (int)threadIdx.x < CK && i < end;
+            const T m = in ? kpp_term(w[i], Dt[i]) : T(0);
+            if (s == T(0)) {
+                // 0 + m = m exactly: the first nonzero term starts the sum
+                if (threadIdx.x == 0) s_f = 0x7fffffff;
+                __syncthreads();
+                if (in && m != T(0)) atomicMin(&s_f, (int)threadIdx.x);
+                __syncthreads();
+                const int p = s_f;
+                if (p == 0x7fffffff) {
+                    pos = end;
+                    break;
+                }
+                if ((int)threadIdx.x == p) s_val = m;
+                __syncthreads();
+                s = s_val;
+                pos += p + 1;
+                __syncthreads();
+                continue;
+            }
+            Binade<T> bb;
+            bb.set(s);
+            const unsigned long long qe = in ? bb.q(m) : 0ull;
+            unsigned long long tot, exc;
+            const unsigned long long inc = block_scan_sat<WALK_THREADS>(qe, shm, exc, tot);
+            const bool bad = in && (qe == SC_SAT || bb.s_int + inc >= bb.limit);
+            if (threadIdx.x == 0) s_f = 0x7fffffff;
+            __syncthreads();
+            if (bad) atomicMin(&s_f, (int)threadIdx.x);
+            __syncthreads();
+            const int p = s_f;
+            if (p == 0x7fffffff) {
+                s = bb.value(bb.s_int + tot);
+                pos = end;
+                break;
+            }
+            // the terms before p on the grid, then term p serially in T
+            if ((int)threadIdx.x == p) s_val = add_rn(bb.value(bb.s_int + exc), m);
+            __syncthreads();
+            s = s_val;
+            pos += p + 1;
+            __syncthreads();
+        }
+        j = c + 1;
     }
-    if (threadIdx.x == 0) cost[blockIdx.x] = (double)s;
+    if (threadIdx.x == 0) cost[t] = (double)s;
 }
 
+int kpp_num_chunks(int n) { return (n + CK - 1) / CK; }
+
 template <typename T>
-cudaError_t launch_kpp_serial_cost(const T *w, const T *D, int n, int nt, double *cost,
-                                   cudaStream_t s) {
-    kpp_serial_cost_kernel<T><<<nt, SC_THREADS, 0, s>>>(w, D, n, cost);
+cudaError_t launch_kpp_dist_cost(const T *X, int ldx, int n, int d, const T *xnorm,
+                                 const int *cand, int t, const T *w, T *D, double *cost,
+                                 void *work, cudaStream_t s) {
+    if (ldx % 4 != 0 || (reinterpret_cast<uintptr_t>(X) & 15) != 0) return cudaErrorInvalidValue;
+    const int nch = kpp_num_chunks(n);
+    double *csum = static_cast<double *>(work);
+    double *P = csum + (size_t)t * nch;
+    unsigned long long *Qr = reinterpret_cast<unsigned long long *>(P + (size_t)t * nch);
+    int *Er = reinterpret_cast<int *>(Qr + (size_t)t * nch);
+    // candidates' rows padded to 16 bytes, in shared memory when they fit
+    const int W = 16 / (int)sizeof(T);
+    const size_t want = (size_t)t * ((d + W - 1) / W * W) * sizeof(T);
+    if (want <= 96 * 1024) {
+        cudaError_t e = ensure_smem_limit(
+            reinterpret_cast<const void *>(kpp_dist_csum_kernel<T, true>), want);
+        if (e != cudaSuccess) return e;
+        kpp_dist_csum_kernel<T, true><<<nch, CK, want, s>>>(X, ldx, n, d, xnorm, cand, t, w, D,
+                                                            csum, nch);
+    } else {
+        kpp_dist_csum_kernel<T, false><<<nch, CK, 0, s>>>(X, ldx, n, d, xnorm, cand, t, w, D, csum,
+                                                          nch);
+    }
+    kpp_chunk_prefix_kernel<<<t, 1024, 0, s>>>(csum, nch, P);
+    kpp_chunk_q_kernel<T><<<dim3((nch + 7) / 8, t), 256, 0, s>>>(w, D, n, nch, P, Qr, Er);
+    kpp_walk_kernel<T><<<t, WALK_THREADS, 0, s>>>(w, D, n, nch, Qr, Er, cost);
     return cudaGetLastError();
+}
+
+size_t kpp_cost_work_bytes(int n, int t) {
+    return (size_t)kpp_num_chunks(n) * t * (8 + 8 + 8 + 4) + 256;
 }
 
 // Choose the candidate (kmeans.cpp:1614-1646): repeats skipped, the first
@@ -547,8 +825,9 @@ cudaError_t launch_kpp_select_update(T *w, const T *D, int n, const double *cost
     template cudaError_t launch_kpp_select_update<T>(T *, const T *, int, const double *,       \
                                                      const int *, int, int *, int, double *,    \
                                                      cudaStream_t);                             \
-    template cudaError_t launch_kpp_serial_cost<T>(const T *, const T *, int, int, double *,    \
-                                                   cudaStream_t);
+    template cudaError_t launch_kpp_dist_cost<T>(const T *, int, int, int, const T *,           \
+                                                 const int *, int, const T *, T *, double *,     \
+                                                 void *, cudaStream_t);
 B200_KPP_INST(float)
 B200_KPP_INST(double)
 

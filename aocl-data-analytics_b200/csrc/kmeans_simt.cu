@@ -392,33 +392,85 @@ cudaError_t launch_kmeans_inertia(const T *X, int ldx, int n, int d, const T *C,
 
 // ------------------------------------------------------------ k-means++ --
 // D[c*n + i] = fl(-2 x_i.x_c + fl(|x_i|^2 + |x_c|^2)) -- the GEMM form of
-// euclidean_gemm_distance with precomputed norms (kmeans.cpp:1491-1521).
+// euclidean_gemm_distance with precomputed norms (kmeans.cpp:1491-1521); the
+// dot product is one fma chain over the features in order.  One thread per
+// row: the row is read once per group of KPP_G candidates with 16-byte loads
+// (rows start on 16-byte boundaries), the candidates' rows broadcast from
+// shared memory (or read through L1 when they do not fit).
+static constexpr int KPP_G = 8;
+template <typename T> struct Vec16;
+template <> struct Vec16<float> {
+    using V = float4;
+    static constexpr int W = 4;
+    static __device__ __forceinline__ void get(const float *p, float (&o)[4]) {
+        const float4 v = *reinterpret_cast<const float4 *>(p);
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    }
+};
+template <> struct Vec16<double> {
+    static constexpr int W = 2;
+    static __device__ __forceinline__ void get(const double *p, double (&o)[2]) {
+        const double2 v = *reinterpret_cast<const double2 *>(p);
+        o[0] = v.x; o[1] = v.y;
+    }
+};
 template <typename T>
-__global__ void kpp_dist_kernel(const T *X, int ld, int n, int d, const T *xnorm,
-                                const int *cand, int t, T *D) {
+__global__ void __launch_bounds__(256) kpp_dist_kernel(const T *X, int ld, int n, int d,
+                                                       const T *xnorm, const int *cand, int t,
+                                                       T *D, int use_smem) {
     extern __shared__ __align__(16) unsigned char sm[];
     T *cs = reinterpret_cast<T *>(sm);
-    for (int e = threadIdx.x; e < t * d; e += blockDim.x) {
-        const int c = e / d, f = e % d;
-        cs[e] = X[(size_t)cand[c] * ld + f];
+    if (use_smem) {
+        for (int e = threadIdx.x; e < t * d; e += blockDim.x) {
+            const int c = e / d, f = e % d;
+            cs[e] = X[(size_t)cand[c] * ld + f];
+        }
+        __syncthreads();
     }
-    __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    constexpr int W = Vec16<T>::W;
     const T *x = X + (size_t)i * ld;
-    for (int c = 0; c < t; ++c) {
-        T s = T(0);
-        const T *y = cs + c * d;
-        for (int f = 0; f < d; ++f) s = fma_rn(x[f], y[f], s);
-        const T nn = add_rn(xnorm[i], xnorm[cand[c]]);
-        D[(size_t)c * n + i] = fma_rn(T(-2), s, nn);
+    const T xn = xnorm[i];
+    for (int c0 = 0; c0 < t; c0 += KPP_G) {
+        T s[KPP_G];
+        const T *y[KPP_G];
+#pragma unroll
+        for (int g = 0; g < KPP_G; ++g) {
+            const int c = min(c0 + g, t - 1);
+            s[g] = T(0);
+            y[g] = use_smem ? cs + (size_t)c * d : X + (size_t)cand[c] * ld;
+        }
+        int f = 0;
+        for (; f + W <= d; f += W) {
+            T xv[W];
+            Vec16<T>::get(x + f, xv);
+#pragma unroll
+            for (int u = 0; u < W; ++u)
+#pragma unroll
+                for (int g = 0; g < KPP_G; ++g) s[g] = fma_rn(xv[u], y[g][f + u], s[g]);
+        }
+        for (; f < d; ++f) {
+            const T xf = x[f];
+#pragma unroll
+            for (int g = 0; g < KPP_G; ++g) s[g] = fma_rn(xf, y[g][f], s[g]);
+        }
+#pragma unroll
+        for (int g = 0; g < KPP_G; ++g)
+            if (c0 + g < t) {
+                const T nn = add_rn(xn, xnorm[cand[c0 + g]]);
+                D[(size_t)(c0 + g) * n + i] = fma_rn(T(-2), s[g], nn);
+            }
     }
 }
 template <typename T>
 cudaError_t launch_kpp_dist(const T *X, int ldx, int n, int d, const T *xnorm, const int *cand,
                             int t, T *D, cudaStream_t s) {
-    const size_t sm = (size_t)t * d * sizeof(T);
-    kpp_dist_kernel<T><<<(n + 255) / 256, 256, sm, s>>>(X, ldx, n, d, xnorm, cand, t, D);
+    if (ldx % 4 != 0 || (reinterpret_cast<uintptr_t>(X) & 15) != 0) return cudaErrorInvalidValue;
+    const size_t want = (size_t)t * d * sizeof(T);
+    const int use_smem = want <= 48 * 1024 ? 1 : 0;
+    kpp_dist_kernel<T><<<(n + 255) / 256, 256, use_smem ? want : 0, s>>>(X, ldx, n, d, xnorm,
+                                                                        cand, t, D, use_smem);
     return cudaGetLastError();
 }
 template <typename T>
