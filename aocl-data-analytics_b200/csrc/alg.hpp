@@ -165,7 +165,10 @@ template <typename T> struct KMeans : public AlgBase {
     DevBuf dX, dXn, dC0, dC1, dCn, dL0, dL1, dCounts, dBlockCounts, dOffsets, dSorted,
         dChunkSums, dSegStart, dScalars, dFlags, dPartials, dW, dKD, dCand, dStage, dY, dYL,
         dBestL, dXh, dXl, dXnrm, dBh, dBl, dBaug, dAaug, dCtmp, dTcScal, dAmb, dFxScale,
-        dFxAcc, dFxTicket, dKppU, dKppBs;
+        dFxAcc, dFxTicket, dKppU, dKppBs, dChg;
+    // changed-row list of the graph loop's assignments (incremental update)
+    int chg_cap = 0;
+    bool chg_capture = false;
     int tc_split = 0;     // bf16 terms of the resident X copies (0: none)
     bool use_tc = false; // bf16 tensor-core assignment active for this compute
     bool dXbf_stale = true;

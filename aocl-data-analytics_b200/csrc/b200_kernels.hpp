@@ -200,6 +200,14 @@ cudaError_t launch_kmeans_update_fx(const float *X, int ld, int n, int d, int k,
                                     const float *C_prev, float *C_new, int *counts,
                                     double *block_partials, double *scalars, int *flags,
                                     unsigned *ticket, cudaStream_t s);
+// The rows whose label changed in an assignment, appended by the assignment
+// kernels when `count` is set: count[0] counts them all, the first `cap` are
+// listed as (rows, olds, news).  count[0] must be 0 on entry.
+struct ChangeList {
+    int *count = nullptr;
+    int *rows = nullptr, *olds = nullptr, *news = nullptr;
+    int cap = 0;
+};
 // Device state of a Lloyd loop run as a CUDA graph (WHILE node): the next
 // iteration's index, the limits, and the outcome written by the finalize.
 struct LloydLoopState {
@@ -209,15 +217,22 @@ struct LloydLoopState {
     int n_iter;   // the host loop's iteration count at its end
     double tol;
 };
-// One Lloyd update inside the graph loop: sums into accumulator set 0
-// (cleared first), new centres in place in C, the convergence test of
-// iteration ls->it, and cudaGraphSetConditional(cond, 0) when the loop ends.
+// One Lloyd update inside the graph loop: new centres in place in C, the
+// convergence test of iteration ls->it, and cudaGraphSetConditional(cond, 0)
+// when the loop ends.  Accumulator set 0 holds the sums and counts of the
+// labels before this iteration's assignment; with at most chg.cap changed
+// rows they are brought up to date by adding each changed row's fixed-point
+// features to its new cluster and subtracting them from its old one (exact
+// integer arithmetic: the same sums as a recount), else recounted over all
+// rows.  The finalize re-arms the iteration's counters: flags[0..1],
+// rearm[0] and rearm[2] (the relabel list's counts), chg.count.
 cudaError_t launch_kmeans_update_fx_loop(const float *X, int ld, int n, int d, int k,
                                          const int *labels, const float *scale,
                                          const double *inv_scale, void *accum, float *C,
                                          int *counts, double *block_partials, double *scalars,
                                          int *flags, unsigned *ticket, LloydLoopState *ls,
-                                         unsigned long long cond, cudaStream_t s);
+                                         unsigned long long cond, const ChangeList &chg,
+                                         int *rearm, cudaStream_t s);
 // One shard's share of a data set split across processes, packed for one
 // integer all-reduce: acc[0, k*d) the fixed-point sums (two's complement,
 // from zero), acc[k*d, k*d+k) the counts, acc[k*d+k] = (*changed != 0).
@@ -315,21 +330,27 @@ cudaError_t launch_prep_centres(const float *C, int ld, int k, int d, int ldo,
 // out[i] = |x_i| (fp32); *maxv = max_i |x_i| when maxv != null.
 cudaError_t launch_row_norm_max(const float *X, int ld, int rows, int d, float *out, float *maxv,
                                 cudaStream_t s);
+// launch_centre_norms + launch_prep_centres in one launch (Aaug already set).
+cudaError_t launch_prep_centres_norms(const float *C, int ld, int k, int d, int ldo,
+                                      float *cnorm, void *Bh, void *Bl, void *Baug,
+                                      cudaStream_t s);
 // Tensor-core candidate assignment: rows with a single candidate within the
 // error bound get their exact fp32 label; the others are appended to amb_rows
 // with up to 4 candidate clusters each (amb_ncand = 0: scan all).  *amb_count
-// must be 0 on entry.
+// must be 0 on entry.  Certified rows whose label changed go to `chg`.
 cudaError_t launch_kmeans_assign_tc(int split, const void *Xh, const void *Xl, int n, int ldbf,
                                     const void *Bh, const void *Bl, const void *Baug,
                                     const void *Aaug, int k, const float *xnorm,
                                     const float *cnorm, int *labels, const int *labels_prev,
                                     int *flags, int *amb_rows, int *amb_cand, int *amb_ncand,
-                                    int *amb_count, int *err, cudaStream_t s);
-// Exact fp32 labels of the rows listed by the tensor-core pass.
+                                    int *amb_count, int *err, const ChangeList &chg,
+                                    cudaStream_t s);
+// Exact fp32 labels of the rows listed by the tensor-core pass (changed
+// ones to `chg`).
 cudaError_t launch_kmeans_rescore(const float *X, int ld, int d, const float *C, int k,
                                   const float *cnorm, const int *amb_rows, const int *amb_cand,
                                   const int *amb_ncand, const int *amb_count, int max_rows,
                                   int *labels, const int *labels_prev, int *flags,
-                                  cudaStream_t s);
+                                  const ChangeList &chg, cudaStream_t s);
 
 } // namespace b200

@@ -495,22 +495,38 @@ template <typename T> da_status KMeans<T>::assign(const T *dC, int *dL, const in
             int *amb_ncand = amb_rows + n;
             int *amb_cand = amb_rows + 2 * (size_t)n;
             const bool s3 = tc_split == 3;
-            B200_TRY(launch_prep_centres(dC, ld, k, d, ldbf, dCn.as<float>(), dBh.p,
-                                         s3 ? dBl.p : nullptr, dBaug.p,
-                                         aaug_ready ? nullptr : dAaug.p, st), "centre operands");
-            aaug_ready = true;
-            B200_TRY(cudaMemsetAsync(amb_cnt, 0, 3 * sizeof(int), st), "memset");
+            if (chg_capture && aaug_ready) {
+                // the graph loop's body: norms and operands in one launch; the
+                // counters were re-armed by the previous iteration's finalize
+                B200_TRY(launch_prep_centres_norms(dC, ld, k, d, ldbf, dCn.as<float>(), dBh.p,
+                                                   s3 ? dBl.p : nullptr, dBaug.p, st),
+                         "centre operands");
+            } else {
+                B200_TRY(launch_prep_centres(dC, ld, k, d, ldbf, dCn.as<float>(), dBh.p,
+                                             s3 ? dBl.p : nullptr, dBaug.p,
+                                             aaug_ready ? nullptr : dAaug.p, st), "centre operands");
+                aaug_ready = true;
+                B200_TRY(cudaMemsetAsync(amb_cnt, 0, 3 * sizeof(int), st), "memset");
+            }
+            ChangeList chg;
+            if (chg_capture) {
+                chg.count = dChg.as<int>();
+                chg.rows = chg.count + 1;
+                chg.olds = chg.rows + chg_cap;
+                chg.news = chg.olds + chg_cap;
+                chg.cap = chg_cap;
+            }
             B200_TRY(cuda->timed("kmeans_assign", [&] {
                 return launch_kmeans_assign_tc(tc_split, dXh.p, s3 ? dXl.p : nullptr, n, ldbf,
                                                dBh.p, s3 ? dBl.p : nullptr, dBaug.p, dAaug.p, k,
                                                dXnrm.as<float>(), dCn.as<float>(), dL, dLprev,
                                                dFlags.as<int>(), amb_rows, amb_cand, amb_ncand,
-                                               amb_cnt, errf, st);
+                                               amb_cnt, errf, chg, st);
             }), "tensor-core assign");
             B200_TRY(cuda->timed("kmeans_rescore", [&] {
                 return launch_kmeans_rescore(dX.as<float>(), ld, d, dC, k, dCn.as<float>(),
                                              amb_rows, amb_cand, amb_ncand, amb_cnt, n, dL,
-                                             dLprev, dFlags.as<int>(), st);
+                                             dLprev, dFlags.as<int>(), chg, st);
             }), "relabel");
             return da_status_success;
         }
@@ -685,18 +701,27 @@ template <typename T> bool KMeans<T>::build_loop_graph(T *dC, int *dL) {
             ok = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0,
                                                cudaStreamCaptureModeThreadLocal) == cudaSuccess;
         if (ok) {
-            bool launched = launch_centre_norms<float>(dC, ld, k, d, dCn.as<float>(), st) ==
-                                cudaSuccess &&
-                            cudaMemsetAsync(dFlags.p, 0, 8 * sizeof(int), st) == cudaSuccess;
-            launched = launched && assign(dC, dL, dL) == da_status_success;
+            // the assignment lists its changed rows for the incremental update;
+            // the centre norms come with the operands (aaug_ready: iteration 0
+            // set the constant operand), the counters are re-armed by the
+            // finalize of the previous iteration (and before the graph starts)
+            chg_capture = true;
+            bool launched = aaug_ready && assign(dC, dL, dL) == da_status_success;
+            chg_capture = false;
+            ChangeList chg;
+            chg.count = dChg.as<int>();
+            chg.rows = chg.count + 1;
+            chg.olds = chg.rows + chg_cap;
+            chg.news = chg.olds + chg_cap;
+            chg.cap = chg_cap;
             const double *scale = dFxScale.as<double>();
             launched = launched &&
                        launch_kmeans_update_fx_loop(
                            dX.as<float>(), ld, n, d, k, dL, reinterpret_cast<const float *>(scale),
                            scale + d, dFxAcc.p, dC, dCounts.as<int>(), dScalars.as<double>() + 8,
                            dScalars.as<double>(), dFlags.as<int>(), dFxTicket.as<unsigned>(),
-                           dLoop.as<LloydLoopState>(), (unsigned long long)cond,
-                           st) == cudaSuccess;
+                           dLoop.as<LloydLoopState>(), (unsigned long long)cond, chg,
+                           reinterpret_cast<int *>(dTcScal.as<char>() + 16), st) == cudaSuccess;
             cudaGraph_t captured = nullptr;
             const bool ended = cudaStreamEndCapture(st, &captured) == cudaSuccess;
             ok = launched && ended;
@@ -728,6 +753,9 @@ da_status KMeans<T>::lloyd_graph(T *dC, int *dL, da_int &n_iter_out, int &conver
             return da_status_success; // the caller captures: run the host loop
         }
         if (!dLoop.ensure(sizeof(LloydLoopState))) return da_status_success;
+        // changed-row list: up to n / 16 rows (more: the update recounts)
+        chg_cap = (int)std::min<da_int>(n_samples, std::max<da_int>(8192, n_samples / 16));
+        if (!dChg.ensure((size_t)(3 * (size_t)chg_cap + 1) * sizeof(int))) return da_status_success;
         const std::vector<uintptr_t> key = {
             (uintptr_t)st, (uintptr_t)dC, (uintptr_t)dL, (uintptr_t)dX.p, (uintptr_t)dCn.p,
             (uintptr_t)dFlags.p, (uintptr_t)dFxAcc.p, (uintptr_t)dFxScale.p,
@@ -736,7 +764,7 @@ da_status KMeans<T>::lloyd_graph(T *dC, int *dL, da_int &n_iter_out, int &conver
             (uintptr_t)dBh.p, (uintptr_t)dBl.p, (uintptr_t)dBaug.p, (uintptr_t)dAaug.p,
             (uintptr_t)dCtmp.p, (uintptr_t)dTcScal.p, (uintptr_t)dAmb.p, (uintptr_t)n_samples,
             (uintptr_t)n_clusters, (uintptr_t)n_features, (uintptr_t)ld, (uintptr_t)use_tc,
-            (uintptr_t)tc_split, (uintptr_t)ldbf};
+            (uintptr_t)tc_split, (uintptr_t)ldbf, (uintptr_t)dChg.p, (uintptr_t)chg_cap};
         if (!loop_exec || key != loop_key) {
             drop_loop_graph();
             if (!build_loop_graph(dC, dL)) return da_status_success;
@@ -750,6 +778,23 @@ da_status KMeans<T>::lloyd_graph(T *dC, int *dL, da_int &n_iter_out, int &conver
         tc_state[0] = tc_state[1] = tc_state[2] = 0;
         B200_TRY(cudaMemcpyAsync(dLoop.p, hs, sizeof(LloydLoopState), cudaMemcpyHostToDevice, st),
                  "copy");
+        // the graph keeps the sums and counts of the current labels in
+        // accumulator set 0; iteration 0 left them in set 1 - fx_parity
+        if (fx_parity == 0) {
+            const size_t kd = (size_t)n_clusters * n_features;
+            char *acc = dFxAcc.as<char>();
+            B200_TRY(cudaMemcpyAsync(acc, acc + kd * 8, kd * 8, cudaMemcpyDeviceToDevice, st), "copy");
+            B200_TRY(cudaMemcpyAsync(acc + 2 * kd * 8, acc + 2 * kd * 8 + (size_t)n_clusters * 4,
+                                     (size_t)n_clusters * 4, cudaMemcpyDeviceToDevice, st), "copy");
+        }
+        // the first graph iteration's counters (later ones: re-armed by the finalize)
+        B200_TRY(cudaMemsetAsync(dChg.p, 0, sizeof(int), st), "memset");
+        B200_TRY(cudaMemsetAsync(dFlags.p, 0, 8 * sizeof(int), st), "memset");
+        if (use_tc) {
+            int *amb_cnt = reinterpret_cast<int *>(dTcScal.as<char>() + 16);
+            B200_TRY(cudaMemsetAsync(amb_cnt, 0, sizeof(int), st), "memset");
+            B200_TRY(cudaMemsetAsync(amb_cnt + 2, 0, sizeof(int), st), "memset");
+        }
         B200_TRY(cudaGraphLaunch(loop_exec, st), "Lloyd loop graph");
         B200_TRY(cudaMemcpyAsync(ho, dLoop.p, sizeof(LloydLoopState), cudaMemcpyDeviceToHost, st),
                  "copy");

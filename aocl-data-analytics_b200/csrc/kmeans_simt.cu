@@ -12,6 +12,7 @@
 // Here sums, shift and inertia are accumulated in fp64 in a fixed order, so
 // every result is run-to-run deterministic and independent of scheduling.
 #include "b200_common.cuh"
+#include <algorithm>
 #include "b200_kernels.hpp"
 #include "simt_engine.cuh"
 #include "kmeans_fx.cuh"
@@ -607,7 +608,10 @@ cudaError_t launch_col_absmax(const float *X, int ld, int n, int d, unsigned *co
 template <int VW>
 __global__ void __launch_bounds__(FX_THREADS, 1)
 fx_update_kernel(const float *X, int ld, int n, int d, int k, const int *labels,
-                 const float *scale, unsigned long long *gsum, int *gcnt, int sub_w) {
+                 const float *scale, unsigned long long *gsum, int *gcnt, int sub_w,
+                 const int *gate, int gate_max) {
+    // the delta update handles short change lists (fx_delta_kernel)
+    if (gate && *gate <= gate_max) return;
     extern __shared__ __align__(16) unsigned char fx_smem[];
     unsigned long long *acc = reinterpret_cast<unsigned long long *>(fx_smem);
     int *list = reinterpret_cast<int *>(acc + (size_t)k * d); // FX_BATCH row ids
@@ -741,18 +745,54 @@ static void fx_shape(const float *X, int ld, int d, int &vw, int &sub_w) {
 
 static void fx_launch(const float *X, int ld, int n, int d, int k, const int *labels,
                       const float *scale, unsigned long long *sums, int *counts, int nsm,
-                      size_t smem, cudaStream_t s) {
+                      size_t smem, cudaStream_t s, const int *gate = nullptr, int gate_max = 0) {
     int vw = 1, sub_w = 32;
     fx_shape(X, ld, d, vw, sub_w);
     if (vw == 4)
         fx_update_kernel<4><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale, sums,
-                                                          counts, sub_w);
+                                                          counts, sub_w, gate, gate_max);
     else if (vw == 2)
         fx_update_kernel<2><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale, sums,
-                                                          counts, sub_w);
+                                                          counts, sub_w, gate, gate_max);
     else
         fx_update_kernel<1><<<nsm, FX_THREADS, smem, s>>>(X, ld, n, d, k, labels, scale, sums,
-                                                          counts, sub_w);
+                                                          counts, sub_w, gate, gate_max);
+}
+
+// Bring the running sums up to date from the change list (when it holds
+// every changed row, *count <= cap): one warp per changed row moves the
+// row's fixed-point features q = round-to-nearest-even(x * 2^s_f) -- the
+// value fx_acc adds -- from its old cluster to its new one, and one count.
+// Integer additions in any order: the sums equal a recount's.  With a longer
+// list the sums and counts are cleared instead, for the recount that follows.
+__global__ void __launch_bounds__(256)
+fx_delta_kernel(const float *X, int ld, int d, int k, const float *scale, const int *count,
+                int cap, const int *rows, const int *olds, const int *news,
+                unsigned long long *sum, int *cnt) {
+    const int c = *count;
+    if (c > cap) {
+        const int kd = k * d;
+        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < kd; e += gridDim.x * blockDim.x)
+            sum[e] = 0ull;
+        for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < k; j += gridDim.x * blockDim.x)
+            cnt[j] = 0;
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    const int nwarps = gridDim.x * (blockDim.x >> 5);
+    for (int e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < c; e += nwarps) {
+        const int r = rows[e], jo = olds[e], jn = news[e];
+        const float *x = X + (size_t)r * ld;
+        for (int f = lane; f < d; f += 32) {
+            const long long q = __double2ll_rn((double)x[f] * (double)scale[f]);
+            atomicAdd(&sum[(size_t)jn * d + f], (unsigned long long)q);
+            atomicAdd(&sum[(size_t)jo * d + f], (unsigned long long)(-q));
+        }
+        if (lane == 0) {
+            atomicAdd(&cnt[jn], 1);
+            atomicSub(&cnt[jo], 1);
+        }
+    }
 }
 
 // One thread per (cluster, feature): the mean from the global sums, and fp64
@@ -773,7 +813,7 @@ fx_finalize_kernel(int k, int d, int ld, const unsigned long long *gsum, const C
                    unsigned long long *nsum, int *ncnt, const double *inv_scale,
                    const float *C_prev, float *C_new, int *counts, double *block_partials,
                    double *scalars, int *flags, unsigned *ticket, LloydLoopState *ls,
-                   unsigned long long cond) {
+                   unsigned long long cond, int *rearm0 = nullptr, int *rearm1 = nullptr) {
     __shared__ double s0[256], s1[256];
     __shared__ bool last;
     const int kd = k * d;
@@ -840,6 +880,17 @@ fx_finalize_kernel(int k, int d, int ld, const unsigned long long *gsum, const C
             ls->n_iter = conv > 0 ? it : next;
             ls->it = next;
             if (stop) cudaGraphSetConditional(cond, 0);
+            // the next iteration's counters start at zero: the label-change and
+            // empty-cluster flags (read above), the relabel list count and its
+            // full-scan count (rearm0[0], rearm0[2]; rearm0[1] is the sticky
+            // error word), the changed-row count (rearm1[0])
+            flags[0] = 0;
+            flags[1] = 0;
+            if (rearm0) {
+                rearm0[0] = 0;
+                rearm0[2] = 0;
+            }
+            if (rearm1) rearm1[0] = 0;
         }
     }
 }
@@ -885,9 +936,10 @@ cudaError_t launch_kmeans_update_fx_loop(const float *X, int ld, int n, int d, i
                                          const double *inv_scale, void *accum, float *C,
                                          int *counts, double *block_partials, double *scalars,
                                          int *flags, unsigned *ticket, LloydLoopState *ls,
-                                         unsigned long long cond, cudaStream_t s) {
+                                         unsigned long long cond, const ChangeList &chg,
+                                         int *rearm, cudaStream_t s) {
     const size_t smem = fx_update_smem(k, d);
-    if (smem > (size_t)FX_SMEM_LIMIT) return cudaErrorInvalidValue;
+    if (smem > (size_t)FX_SMEM_LIMIT || !chg.count) return cudaErrorInvalidValue;
     cudaError_t e = fx_smem_limit(smem);
     if (e != cudaSuccess) return e;
     int dev = 0, nsm = 148;
@@ -896,15 +948,16 @@ cudaError_t launch_kmeans_update_fx_loop(const float *X, int ld, int n, int d, i
     const size_t kd = (size_t)k * d;
     unsigned long long *sum = static_cast<unsigned long long *>(accum);
     int *cnt = reinterpret_cast<int *>(sum + 2 * kd);
-    e = cudaMemsetAsync(sum, 0, kd * 8, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, (size_t)k * 4, s);
-    if (e != cudaSuccess) return e;
-    fx_launch(X, ld, n, d, k, labels, scale, sum, cnt, nsm, smem, s);
+    // a short change list: the delta update; a long one: clear, then recount
+    fx_delta_kernel<<<nsm * 4, 256, 0, s>>>(X, ld, d, k, scale, chg.count, chg.cap, chg.rows,
+                                            chg.olds, chg.news, sum, cnt);
+    fx_launch(X, ld, n, d, k, labels, scale, sum, cnt, nsm, smem, s, chg.count, chg.cap);
     const int nb = (int)((kd + 255) / 256);
-    // in place: each element's old value is read by the thread that writes it
+    // in place: each element's old value is read by the thread that writes it;
+    // the last block re-arms the iteration's counters
     fx_finalize_kernel<int><<<nb, 256, 0, s>>>(k, d, ld, sum, cnt, nullptr, nullptr, inv_scale,
                                                C, C, counts, block_partials, scalars, flags,
-                                               ticket, ls, cond);
+                                               ticket, ls, cond, rearm, chg.count);
     return cudaGetLastError();
 }
 

@@ -46,7 +46,27 @@ struct TcAssignArgs {
     int *amb_ncand;      // number of candidates (0: scan every cluster)
     int *amb_count;      // [0] listed rows, [2] of them without a candidate list
     int *err;            // set on a timed-out wait
+    ChangeList chg;      // certified rows whose label changed
 };
+
+// Warp-collective: append the lanes with `chg` set to the change list.
+__device__ __forceinline__ void emit_changes(const ChangeList &c, bool chg, int r, int old_l,
+                                             int new_l) {
+    const unsigned cm = __ballot_sync(0xffffffffu, chg);
+    if (!cm) return;
+    const int lane = threadIdx.x & 31;
+    int b0 = 0;
+    if (lane == __ffs(cm) - 1) b0 = atomicAdd(c.count, __popc(cm));
+    b0 = __shfl_sync(0xffffffffu, b0, __ffs(cm) - 1);
+    if (chg) {
+        const int pos = b0 + __popc(cm & ((1u << lane) - 1u));
+        if (pos < c.cap) {
+            c.rows[pos] = r;
+            c.olds[pos] = old_l;
+            c.news[pos] = new_l;
+        }
+    }
+}
 
 struct __align__(16) TcShared {
     uint64_t full[8], empty[8], tfull[2], tempty[2], bfull;
@@ -372,6 +392,7 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
                 a.labels[r] = lbl;
                 if (a.labels_prev && lprev != lbl) changed = 1;
             }
+            if (a.chg.count) emit_changes(a.chg, certain && lprev != lab, r, lprev, lab);
             // several candidates (or non-finite scores): one atomic per warp
             const bool amb = valid && !certain;
             const unsigned mask = __ballot_sync(0xffffffffu, amb);
@@ -421,7 +442,7 @@ __global__ void __launch_bounds__(256)
 kmeans_rescore_kernel(const float *X, int ld, int d, int dp, const float *C, int k,
                       const float *cnorm, const int *amb_rows, const int *amb_cand,
                       const int *amb_ncand, const int *amb_count, int *labels,
-                      const int *labels_prev, int *flags, int c_in_smem) {
+                      const int *labels_prev, int *flags, int c_in_smem, ChangeList chg) {
     extern __shared__ __align__(16) float rs_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwb = blockDim.x >> 5;
     float *cs = rs_smem;
@@ -497,6 +518,8 @@ kmeans_rescore_kernel(const float *X, int ld, int d, int dp, const float *C, int
             }
         }
         __syncwarp();
+        bool chg_c = false;
+        int chg_old = 0, chg_new = 0;
         if (nc > 0) {
             int cj[TC_MAXC];
             const float *cp[TC_MAXC];
@@ -541,9 +564,16 @@ kmeans_rescore_kernel(const float *X, int ld, int d, int dp, const float *C, int
             }
             const int lbl = (bi == 0x7fffffff) ? cj[0] : bi;
             // read before the write: labels may be labels_prev (in place)
-            if (labels_prev && labels_prev[r] != lbl) changed = 1;
+            const int old_l = labels_prev ? labels_prev[r] : lbl;
+            if (old_l != lbl) {
+                changed = 1;
+                chg_c = true;
+                chg_old = old_l;
+                chg_new = lbl;
+            }
             labels[r] = lbl;
         }
+        if (chg.count) emit_changes(chg, chg_c, r, chg_old, chg_new);
         unsigned full = __ballot_sync(0xffffffffu, nc == 0);
         while (full) {
             const int src = __ffs(full) - 1;
@@ -602,7 +632,18 @@ kmeans_rescore_kernel(const float *X, int ld, int d, int dp, const float *C, int
             }
             if (lane == src) {
                 const int lbl = (bi == 0x7fffffff) ? 0 : bi;
-                if (labels_prev && labels_prev[r] != lbl) changed = 1;
+                const int old_l = labels_prev ? labels_prev[r] : lbl;
+                if (old_l != lbl) {
+                    changed = 1;
+                    if (chg.count) {
+                        const int pos = atomicAdd(chg.count, 1);
+                        if (pos < chg.cap) {
+                            chg.rows[pos] = r;
+                            chg.olds[pos] = old_l;
+                            chg.news[pos] = lbl;
+                        }
+                    }
+                }
                 labels[r] = lbl;
             }
         }
@@ -645,6 +686,43 @@ __global__ void prep_centres_kernel(const float *C, int ld, int k, int d, int np
             v = __float2bfloat16_rn(__int_as_float(0x7f800000));
         }
         Baug[e] = v;
+    }
+}
+// The centre operands with the centre norms computed in the same launch (the
+// graph loop's body): one block per padded centre row; thread 0 forms |c_j|^2
+// as the sequential fma chain over the features (the plain path's value),
+// then the block writes row j of B = -2 C (hi / lo) and of Baug.
+__global__ void prep_centres_norms_kernel(const float *C, int ld, int k, int d, int ldo,
+                                          float *cnorm, __nv_bfloat16 *Bh, __nv_bfloat16 *Bl,
+                                          __nv_bfloat16 *Baug) {
+    __shared__ float s_cn;
+    const int j = blockIdx.x;
+    if (threadIdx.x == 0) {
+        float sq = 0.f;
+        if (j < k) {
+            const float *c = C + (size_t)j * ld;
+            for (int f = 0; f < d; ++f) sq = __fmaf_rn(c[f], c[f], sq);
+            cnorm[j] = sq;
+        }
+        s_cn = sq;
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < ldo; f += blockDim.x) {
+        const float x = (j < k && f < d) ? -2.f * C[(size_t)j * ld + f] : 0.f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        Bh[(size_t)j * ldo + f] = h;
+        if (Bl) Bl[(size_t)j * ldo + f] = __float2bfloat16_rn(x - __bfloat162float(h));
+    }
+    for (int f = threadIdx.x; f < TC_KB; f += blockDim.x) {
+        __nv_bfloat16 v = __float2bfloat16_rn(0.f);
+        if (j < k) {
+            const __nv_bfloat16 h = __float2bfloat16_rn(s_cn);
+            if (f == 0) v = h;
+            if (f == 1) v = __float2bfloat16_rn(s_cn - __bfloat162float(h));
+        } else if (f == 0) {
+            v = __float2bfloat16_rn(__int_as_float(0x7f800000));
+        }
+        Baug[(size_t)j * TC_KB + f] = v;
     }
 }
 // The constant "ones" operand: 128 rows x 64, columns 0 and 1 equal to 1.
@@ -750,6 +828,16 @@ cudaError_t launch_prep_centres(const float *C, int ld, int k, int d, int ldo,
     return cudaGetLastError();
 }
 
+cudaError_t launch_prep_centres_norms(const float *C, int ld, int k, int d, int ldo,
+                                      float *cnorm, void *Bh, void *Bl, void *Baug,
+                                      cudaStream_t s) {
+    const int npad = (k + 15) & ~15;
+    prep_centres_norms_kernel<<<npad, 128, 0, s>>>(
+        C, ld, k, d, ldo, cnorm, reinterpret_cast<__nv_bfloat16 *>(Bh),
+        reinterpret_cast<__nv_bfloat16 *>(Bl), reinterpret_cast<__nv_bfloat16 *>(Baug));
+    return cudaGetLastError();
+}
+
 cudaError_t launch_row_norm_max(const float *X, int ld, int rows, int d, float *out, float *maxv,
                                 cudaStream_t s) {
     if (maxv) {
@@ -765,7 +853,8 @@ cudaError_t launch_kmeans_assign_tc(int split, const void *Xh, const void *Xl, i
                                     const void *Aaug, int k, const float *xnorm,
                                     const float *cnorm, int *labels, const int *labels_prev,
                                     int *flags, int *amb_rows, int *amb_cand, int *amb_ncand,
-                                    int *amb_count, int *err, cudaStream_t s) {
+                                    int *amb_count, int *err, const ChangeList &chg,
+                                    cudaStream_t s) {
     const int nkb = ldbf / TC_KB;
     const int npad = (k + 15) & ~15;
     const bool s3 = split == 3;
@@ -843,6 +932,7 @@ cudaError_t launch_kmeans_assign_tc(int split, const void *Xh, const void *Xl, i
     a.amb_ncand = amb_ncand;
     a.amb_count = amb_count;
     a.err = err;
+    a.chg = labels_prev ? chg : ChangeList();
     auto kern = s3 ? kmeans_assign_tc_kernel<3> : kmeans_assign_tc_kernel<1>;
     {
         cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(kern), smem);
@@ -860,7 +950,8 @@ cudaError_t launch_kmeans_rescore(const float *X, int ld, int d, const float *C,
                                   const float *cnorm, const int *amb_rows, const int *amb_cand,
                                   const int *amb_ncand, const int *amb_count, int max_rows,
                                   int *labels, const int *labels_prev, int *flags,
-                                  cudaStream_t s) {
+                                  const ChangeList &chg_in, cudaStream_t s) {
+    const ChangeList chg = labels_prev ? chg_in : ChangeList();
     if (max_rows <= 0) return cudaSuccess;
     const bool vec = (d % 4 == 0) && (ld % 4 == 0) &&
                      ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(C)) & 15) == 0;
@@ -888,13 +979,13 @@ cudaError_t launch_kmeans_rescore(const float *X, int ld, int d, const float *C,
         if (e != cudaSuccess) return e;
         kmeans_rescore_kernel<true><<<blocks, 32 * warps, smem, s>>>(
             X, ld, d, dp, C, k, cnorm, amb_rows, amb_cand, amb_ncand, amb_count, labels,
-            labels_prev, flags, c_in_smem);
+            labels_prev, flags, c_in_smem, chg);
     } else {
         e = ensure_smem_limit(reinterpret_cast<const void *>(kmeans_rescore_kernel<false>), smem);
         if (e != cudaSuccess) return e;
         kmeans_rescore_kernel<false><<<blocks, 32 * warps, smem, s>>>(
             X, ld, d, dp, C, k, cnorm, amb_rows, amb_cand, amb_ncand, amb_count, labels,
-            labels_prev, flags, c_in_smem);
+            labels_prev, flags, c_in_smem, chg);
     }
     return cudaGetLastError();
 }
