@@ -532,6 +532,9 @@ kmeans_rescore_kernel(const float *X, int ld, int d, int dp, const float *C, int
             }
             const float *xr = xw + (size_t)lane * dp;
             if (VEC) {
+                // unrolled: the candidate centres' loads of several feature
+                // groups in flight at once
+#pragma unroll 4
                 for (int f = 0; f < d; f += 4) {
                     const float4 xv = *reinterpret_cast<const float4 *>(xr + f);
 #pragma unroll
@@ -962,7 +965,7 @@ cudaError_t launch_kmeans_rescore(const float *X, int ld, int d, const float *C,
     // of behind a block-wide staging of C (measured faster than staging)
     const size_t limit = 220 * 1024;
     const size_t cs_bytes = (size_t)k * dp * 4, xw_bytes = (size_t)32 * dp * 4;
-    int warps = 2;
+    int warps = 8;
     const int c_in_smem = 0;
     while (warps > 1 && warps * xw_bytes > limit) warps >>= 1;
     if (warps * xw_bytes > limit) return cudaErrorInvalidValue;
