@@ -87,6 +87,17 @@ cudaError_t launch_radius_count(const T *D, int rows, int n, size_t ld, T thr, i
 template <typename T>
 cudaError_t launch_radius_emit(const T *D, int rows, int n, size_t ld, T thr,
                                const long long *start, int *idx, T *val, cudaStream_t s);
+// The counts and the output offsets of all (row, chunk) pieces in one launch
+// (a chained scan in (row, chunk) order, dist_simt.cu): start[row * chunks +
+// chunk] = the hits of the pieces before it, total[0] = all hits.  Its waits
+// on other CTAs are bounded: err[0] = 1 when one ran out (test_wait: piece 0
+// never publishes and the waits run out at once).  work:
+// radius_scan_work_bytes(rows, n).
+template <typename T>
+cudaError_t launch_radius_count_scan(const T *D, int rows, int n, size_t ld, T thr, void *work,
+                                     long long *start, long long *total, int *err, int test_wait,
+                                     cudaStream_t s);
+size_t radius_scan_work_bytes(int rows, int n);
 
 // ------------------------------------------------------------ kNN fused --
 struct KnnArgs {

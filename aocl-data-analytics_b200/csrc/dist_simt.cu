@@ -16,6 +16,7 @@
 // TM x TN register micro-tile; operands staged through double-buffered shared
 // memory in BK-dim slabs with 16-byte vector loads.
 #include "b200_common.cuh"
+#include <cuda/atomic>
 #include "b200_kernels.hpp"
 #include "simt_engine.cuh"
 #include <map>
@@ -572,6 +573,107 @@ __global__ void radius_emit_kernel(const T *D, int n, size_t ld, T thr, int chun
     }
 }
 int radius_chunks(int n) { return (n + RADIUS_CHUNK - 1) / RADIUS_CHUNK; }
+// Counts and output offsets of the (row, chunk) pieces in one pass: a chained
+// scan in (row, chunk) order.  Each CTA takes the next logical piece from a
+// ticket (so every piece before it has a CTA running or done), counts its
+// hits and publishes the count; thread 0 then looks back over the pieces
+// before it -- a piece's word holds 2 flag bits (1: its count, 2: its
+// inclusive prefix) and a 62-bit value -- adding counts until it meets a
+// prefix, and publishes its own inclusive prefix.  The look-back waits on
+// global memory for a predecessor that has not published yet; every wait is
+// bounded (`limit` polls), after which the CTA sets err[0] = 1 and leaves
+// its own prefix unpublished (its successors then time out as well: the
+// call fails with a status, the device stays usable).  start[piece] = the
+// exclusive prefix, total[0] = the inclusive prefix of the last piece.
+// skip_first (testing): piece 0 publishes nothing.
+template <typename T>
+__global__ void radius_count_scan_kernel(const T *D, int n, size_t ld, T thr, int chunk, int nch,
+                                         int pieces, unsigned *ticket,
+                                         unsigned long long *state, long long *start,
+                                         long long *total, int *err, unsigned limit,
+                                         int skip_first) {
+    __shared__ int s_id;
+    __shared__ int ws[32];
+    if (threadIdx.x == 0) s_id = (int)atomicAdd(ticket, 1u);
+    __syncthreads();
+    const int id = s_id;
+    if (id >= pieces) return;
+    const int rr = id / nch, cc = id - rr * nch;
+    const T *row = D + (size_t)rr * ld;
+    const int j1 = min(n, (cc + 1) * chunk);
+    int c = 0;
+    for (int j = cc * chunk + threadIdx.x; j < j1; j += blockDim.x) c += row[j] <= thr ? 1 : 0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    long long cnt = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) cnt += ws[w];
+    constexpr unsigned long long AGG = 1ull << 62, PRE = 2ull << 62, VAL = (1ull << 62) - 1;
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> me(state[id]);
+    if (id == 0) {
+        if (!skip_first) me.store(PRE | (unsigned long long)cnt, cuda::memory_order_release);
+        start[0] = 0;
+        if (pieces == 1) *total = cnt;
+        return;
+    }
+    me.store(AGG | (unsigned long long)cnt, cuda::memory_order_release);
+    long long excl = 0;
+    unsigned polls = 0;
+    bool failed = false;
+    for (int j = id - 1; j >= 0;) {
+        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> pj(state[j]);
+        const unsigned long long v = pj.load(cuda::memory_order_acquire);
+        const unsigned long long flag = v & ~VAL;
+        if (flag == 0) {
+            if (++polls > limit) {
+                failed = true;
+                break;
+            }
+            __nanosleep(64);
+            continue;
+        }
+        excl += (long long)(v & VAL);
+        if (flag == PRE) break;
+        --j;
+    }
+    if (failed) {
+        atomicExch(err, 1);
+        return;
+    }
+    me.store(PRE | (unsigned long long)(excl + cnt), cuda::memory_order_release);
+    start[id] = excl;
+    if (id == pieces - 1) *total = excl + cnt;
+}
+
+template <typename T>
+cudaError_t launch_radius_count_scan(const T *D, int rows, int n, size_t ld, T thr, void *work,
+                                     long long *start, long long *total, int *err, int test_wait,
+                                     cudaStream_t s) {
+    if (rows <= 0 || n <= 0) return cudaSuccess;
+    const int nch = radius_chunks(n);
+    const int pieces = rows * nch;
+    unsigned *ticket = static_cast<unsigned *>(work);
+    unsigned long long *state = reinterpret_cast<unsigned long long *>(static_cast<char *>(work) + 256);
+    cudaError_t e = cudaMemsetAsync(work, 0, 256 + (size_t)pieces * 8, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    // about a second of polling; the test mode's wait runs out in microseconds
+    const unsigned limit = test_wait ? 2000u : (1u << 24);
+    radius_count_scan_kernel<T><<<pieces, 256, 0, s>>>(D, n, ld, thr, RADIUS_CHUNK, nch, pieces,
+                                                      ticket, state, start, total, err, limit,
+                                                      test_wait);
+    return cudaGetLastError();
+}
+size_t radius_scan_work_bytes(int rows, int n) { return 256 + (size_t)rows * radius_chunks(n) * 8; }
+template cudaError_t launch_radius_count_scan<float>(const float *, int, int, size_t, float,
+                                                     void *, long long *, long long *, int *, int,
+                                                     cudaStream_t);
+template cudaError_t launch_radius_count_scan<double>(const double *, int, int, size_t, double,
+                                                      void *, long long *, long long *, int *,
+                                                      int, cudaStream_t);
+
 template <typename T>
 cudaError_t launch_radius_count(const T *D, int rows, int n, size_t ld, T thr, int *cnt,
                                 cudaStream_t s) {

@@ -1,6 +1,9 @@
 // Host-side infrastructure of the B200 library: error recording, the option
 // registry, device buffers and the per-handle CUDA context.
 #pragma once
+#include "device_alloc.hpp"
+#include <cstdlib>
+#include <mutex>
 #include "../../include/aoclda_b200.h"
 #include <cuda_runtime.h>
 #include <algorithm>
@@ -356,7 +359,7 @@ struct DevBuf {
         if (b <= bytes && p) return true;
         release();
         if (b == 0) b = 16;
-        if (cudaMalloc(&p, b) != cudaSuccess) {
+        if (device_alloc(&p, b) != cudaSuccess) {
             cudaGetLastError();
             p = nullptr;
             return false;

@@ -14,6 +14,7 @@
 // labels, centres and iteration count equal that path's.
 #include "b200_common.cuh"
 #include "b200_kernels.hpp"
+#include "device_alloc.hpp"
 #include "kmeans_fx.cuh"
 #include "simt_engine.cuh"
 #include "../../include/aoclda_b200_ext.h"
@@ -381,7 +382,9 @@ template <typename V> struct DBuf {
     ~DBuf() {
         if (p) cudaFree(p);
     }
-    cudaError_t alloc(size_t n) { return cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(V)); }
+    cudaError_t alloc(size_t n) {
+        return device_alloc(reinterpret_cast<void **>(&p), std::max<size_t>(n, 1) * sizeof(V));
+    }
 };
 
 } // namespace

@@ -3,6 +3,7 @@
 // source/core/nearest_neighbors/nearest_neighbors.cpp; the distance tile and
 // the top-k selection run on the GPU (dist_simt.cu).
 #include "alg.hpp"
+#include <cstdlib>
 #include <map>
 
 namespace b200 {
@@ -576,42 +577,52 @@ da_status NN<T>::radius_compute(da_int nq, da_int d, const T *Xt, da_int ldt, T 
     const da_int B = (da_int)std::max<size_t>(
         1, std::min<size_t>({(size_t)nq, (256u << 20) / (n * sizeof(T)), (size_t)65535}));
     const int nch = radius_chunks((int)n);
-    if (!dD.ensure((size_t)B * n * sizeof(T)) || !dRc.ensure((size_t)B * nch * sizeof(int)) ||
+    if (!dD.ensure((size_t)B * n * sizeof(T)) ||
+        !dRc.ensure(radius_scan_work_bytes((int)B, (int)n) + 64) ||
         !dRs.ensure((size_t)B * nch * sizeof(long long)))
         return err->error(da_status_memory_error, "Device memory allocation failed.");
-    std::vector<int> cnt((size_t)B * nch);
-    std::vector<long long> start((size_t)B * nch);
+    // testing hook: the offsets' waits run out (AOCLDA_B200_TEST_RADIUS_WAIT=1)
+    const char *tw = std::getenv("AOCLDA_B200_TEST_RADIUS_WAIT");
+    const int test_wait = (tw && tw[0] == '1') ? 1 : 0;
+    std::vector<long long> start((size_t)B * nch + 2);
     const PairwiseArgs pa{acc, post, kc, (double)p, false, true};
+    long long *d_total = reinterpret_cast<long long *>(dRc.as<char>() +
+                                                       radius_scan_work_bytes((int)B, (int)n));
+    int *d_err = reinterpret_cast<int *>(d_total + 1);
     for (da_int q0 = 0; q0 < nq; q0 += B) {
         const int b = (int)std::min<da_int>(B, nq - q0);
         B200_TRY(cuda->timed("radius_distances", [&] {
             return launch_pairwise<T>(dQ.as<T>() + (size_t)q0 * ld, ld, b, dX.as<T>(), ld, (int)n,
                                       (int)d, qn ? qn + q0 : nullptr, xn, pa, dD.as<T>(), st);
         }), "distance kernel");
+        // counts and offsets in (row, chunk) order on the device: every row's
+        // hits stay in index order
         B200_TRY(cuda->timed("radius_count", [&] {
-            return launch_radius_count<T>(dD.as<T>(), b, (int)n, n, thr, dRc.as<int>(), st);
+            return launch_radius_count_scan<T>(dD.as<T>(), b, (int)n, n, thr, dRc.p,
+                                               dRs.as<long long>(), d_total, d_err, test_wait, st);
         }), "count");
-        B200_TRY(cudaMemcpyAsync(cnt.data(), dRc.p, (size_t)b * nch * sizeof(int),
+        B200_TRY(cudaMemcpyAsync(start.data(), dRs.p, (size_t)b * nch * sizeof(long long),
+                                 cudaMemcpyDeviceToHost, st), "copy");
+        B200_TRY(cudaMemcpyAsync(start.data() + (size_t)b * nch, d_total, 2 * sizeof(long long),
                                  cudaMemcpyDeviceToHost, st), "copy");
         B200_TRY(cudaStreamSynchronize(st), "radius search");
-        // chunk offsets in (row, chunk) order: every row's hits stay in index order
-        long long tot = 0;
+        int scan_err = 0;
+        std::memcpy(&scan_err, start.data() + (size_t)b * nch + 1, sizeof(int));
+        if (scan_err != 0)
+            return err->error(da_status_internal_error,
+                              "The radius search's offset scan timed out waiting for another "
+                              "block of the GPU.");
+        const long long tot = start[(size_t)b * nch];
         const size_t base = idx_out.size();
         for (int i = 0; i < b; ++i) {
-            start_out[(size_t)q0 + i] = (long long)base + tot;
-            long long row = 0;
-            for (int c = 0; c < nch; ++c) {
-                start[(size_t)i * nch + c] = tot;
-                tot += cnt[(size_t)i * nch + c];
-                row += cnt[(size_t)i * nch + c];
-            }
-            cnt_out[(size_t)q0 + i] = (da_int)row;
+            const long long s0 = start[(size_t)i * nch];
+            const long long s1 = i + 1 < b ? start[(size_t)(i + 1) * nch] : tot;
+            start_out[(size_t)q0 + i] = (long long)base + s0;
+            cnt_out[(size_t)q0 + i] = (da_int)(s1 - s0);
         }
         if (tot == 0) continue;
         if (!dRi.ensure((size_t)tot * sizeof(int)) || !dRv.ensure((size_t)tot * sizeof(T)))
             return err->error(da_status_memory_error, "Device memory allocation failed.");
-        B200_TRY(cudaMemcpyAsync(dRs.p, start.data(), (size_t)b * nch * sizeof(long long),
-                                 cudaMemcpyHostToDevice, st), "copy");
         B200_TRY(cuda->timed("radius_emit", [&] {
             return launch_radius_emit<T>(dD.as<T>(), b, (int)n, n, thr, dRs.as<long long>(),
                                          dRi.as<int>(), dRv.as<T>(), st);
