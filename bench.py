@@ -811,7 +811,73 @@ def run_knn(ab, nx=4_000_000, nq=10_000, d=128, k=100, comps=1024, seed=3, reps=
             "accuracy": knn_accuracy(X, Q, tc["ind"], tc["dist"], k, metric) if accuracy else None,
             "timing": "wall clock of one da_nn_kneighbors_s call with host arrays (best of 3)"}
     first = out[metrics[0]]
-    return dict(first, **{m: out[m] for m in metrics[1:]})
+    res = dict(first, **{m: out[m] for m in metrics[1:]})
+    if accuracy:
+        res["fp8_candidate_measurement"] = fp8_candidate_measurement(X, Q, k)
+    return res
+
+
+def fp8_candidate_measurement(X, Q, k, nsample=64):
+    """Certified candidate sets of a one-pass tensor-core candidate search,
+    measured on the kNN workload's data (the first nsample queries, on the GPU
+    with torch): operands rounded as the pass would round them -- bf16 hi + lo
+    (the library's bf16x3 pass) or e4m3 hi + lo with a per-row power-of-two
+    scale (fp8) -- and, per (query, row), the ranking value
+    v' = |x|^2 - 2 x~.q~ with the rigorous operand-rounding bound
+    e = 2 (|x - x~| |q| + |x~| |q - q~|).  A row can belong to the true top k
+    only if v' - e <= T_q, with T_q the k-th smallest v' + e; those rows are
+    the candidates the exact re-score must read.  (The tensor core's fp32
+    accumulation adds to both bounds; it is left out, so the sets are lower
+    bounds.)  Reported per query: mean and max candidates, and the re-score
+    bytes they imply against one read of the bf16 operands."""
+    import torch
+    dev = torch.device("cuda")
+    Xg = torch.from_numpy(X).to(dev)
+    Qg = torch.from_numpy(np.ascontiguousarray(Q[:nsample])).to(dev)
+
+    def split_bf16(A):
+        h = A.to(torch.bfloat16).float()
+        lo = (A - h).to(torch.bfloat16).float()
+        return h + lo
+
+    def split_e4m3(A):
+        # per-row scale: a power of two that maps the row's max to <= 448
+        amax = A.abs().amax(dim=1, keepdim=True).clamp_min(1e-30)
+        sc = torch.exp2(torch.floor(torch.log2(448.0 / amax)))
+        As = A * sc
+        h = As.to(torch.float8_e4m3fn).float()
+        lo = (As - h).to(torch.float8_e4m3fn).float()
+        return (h + lo) / sc
+
+    xn2 = (Xg.double() ** 2).sum(1)
+    qn = Qg.double().norm(dim=1)
+    out = {}
+    for name, fn in (("bf16x3", split_bf16), ("fp8_e4m3_hi_lo", split_e4m3)):
+        Xt, Qt = fn(Xg), fn(Qg)
+        ex = (Xg - Xt).double().norm(dim=1)
+        xtn = Xt.double().norm(dim=1)
+        eq = (Qg - Qt).double().norm(dim=1)
+        cand = []
+        G = Xt.double() @ Qt.double().T  # rows x sample queries
+        for q in range(Qg.shape[0]):
+            v = xn2 - 2.0 * G[:, q]
+            e = 2.0 * (ex * qn[q] + xtn * eq[q])
+            T = torch.kthvalue((v + e).cpu(), k).values.item()
+            cand.append(int(((v - e) <= T).sum().item()))
+        del G
+        c = np.array(cand, dtype=np.float64)
+        out[name] = {"mean_candidates": float(c.mean()), "max_candidates": int(c.max()),
+                     "rescore_bytes_per_query": float(c.mean() * X.shape[1] * 4)}
+        del Xt, Qt
+    bf16_pass = X.shape[0] * X.shape[1] * 4  # bf16 hi + lo of every training row, once
+    for v in out.values():
+        v["rescore_bytes_vs_one_bf16x3_read_per_query"] = v["rescore_bytes_per_query"] / bf16_pass
+    out["sample_queries"] = int(Qg.shape[0])
+    out["note"] = ("operand-rounding part of the certificate only (lower bounds on the sets); "
+                   "re-score bytes = candidates x d x 4 per query")
+    del Xg, Qg
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_radius(ab, nx=1_000_000, nq=10_000, d=32, comps=256, target=100, seed=6, reps=3,
