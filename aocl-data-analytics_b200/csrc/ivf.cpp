@@ -4,6 +4,7 @@
 // k-means, the coarse probe, the assignment of added rows and the list scan
 // run on the GPU.
 #include "alg.hpp"
+#include <limits>
 
 namespace b200 {
 
@@ -453,13 +454,19 @@ template <typename T> da_status IVF<T>::load_state(ByteReader &r) {
     const auto bad = [&] {
         return err->error(da_status_invalid_file_data, "The model file is corrupted.");
     };
-    if (!r.ok || nl < 1 || d < 1 || ni < 0 || cen.size() != (size_t)(nl * d) ||
-        sizes.size() != (size_t)nl || ids.size() != norms.size() ||
-        rows.size() != ids.size() * (size_t)d || (me != AM_EUC && me != AM_SQEUC))
+    // every size must fit da_int before the narrowing casts below, and the
+    // products are formed only once both factors are in range
+    const int64_t imax = (int64_t)std::numeric_limits<da_int>::max();
+    if (!r.ok || nl < 1 || d < 1 || ni < 0 || nl > imax || d > imax || ni > imax ||
+        sizes.size() != (size_t)nl || cen.size() / (size_t)nl != (size_t)d ||
+        cen.size() != (size_t)nl * (size_t)d || ids.size() != norms.size() ||
+        rows.size() / (size_t)d != ids.size() || rows.size() != ids.size() * (size_t)d ||
+        (me != AM_EUC && me != AM_SQEUC))
         return bad();
+    // list sizes: each within the listed rows before it is added (no overflow)
     int64_t total = 0;
     for (int64_t v : sizes) {
-        if (v < 0) return bad();
+        if (v < 0 || v > (int64_t)ids.size() - total) return bad();
         total += v;
     }
     if (total != (int64_t)ids.size() || total > ni) return bad();

@@ -22,6 +22,13 @@ overlaps.  Every request records when it was submitted and completed;
 
 The library calls release the Python interpreter lock (ctypes), so the worker
 threads' device work proceeds concurrently.
+
+Admission: a batch's device bytes (its queries, their candidate lists and
+outputs) stay within the worker's share of `hbm_budget` and of the device
+memory free when the batch is formed (less `hbm_reserve`); the oldest
+request is always admitted, so no request waits for ever.  A library call
+that fails completes every request of its batch with `error` set (the
+workers keep serving).
 """
 import collections
 import threading
@@ -37,7 +44,7 @@ KNN_OUT_BYTES = 256 * 8
 
 class Request:
     __slots__ = ("kind", "queries", "k", "model", "t_submit", "t_start", "t_done", "result",
-                 "_done", "parent", "offset", "parts_left")
+                 "error", "_done", "parent", "offset", "parts_left")
 
     def __init__(self, kind, queries, k=None, model=None):
         if kind not in ("knn", "ann", "predict"):
@@ -50,6 +57,7 @@ class Request:
         self.t_start = None  # when a worker took it into a batch
         self.t_done = None
         self.result = None
+        self.error = None       # the library's error when its call failed
         self._done = threading.Event()
         self.parent = None      # for a part: the request it belongs to
         self.offset = 0         # for a part: its first query in the parent
@@ -73,8 +81,25 @@ class Server:
 
     def __init__(self, ab, X, models=None, workers=2, max_batch_queries=1024,
                  max_request_queries=4096, hbm_budget=16 << 30, precision_mode="bf16x3",
-                 small_queries=256, aging_ms=20.0, ann=None):
+                 small_queries=256, aging_ms=20.0, ann=None, free_memory="auto",
+                 hbm_reserve=1 << 30):
         self.ab = ab
+        # admission: a batch's device bytes stay within the worker's share of
+        # hbm_budget AND of the device memory free at the moment it is formed
+        # (less hbm_reserve); free_memory() -> bytes, None to use the budget only
+        if free_memory == "auto":
+            free_memory = None
+            try:
+                import torch
+                if torch.cuda.is_available():
+                    free_memory = lambda: torch.cuda.mem_get_info()[0]  # noqa: E731
+            except Exception:
+                free_memory = None
+        self.free_memory = free_memory
+        self.hbm_reserve = hbm_reserve
+        self.free_every = 0.05  # seconds between free-memory readings (a driver call)
+        self._free_at = -1.0
+        self._free_val = None
         self.small_queries = small_queries
         self.aging = aging_ms / 1e3
         self.X = np.ascontiguousarray(X, dtype=np.float32)
@@ -114,9 +139,10 @@ class Server:
             self.models[name] = km
         self.ann = None
         if ann is not None:
+            # euclidean, as the kNN requests (distances, not their squares)
             self.ann = ab.ApproxNN("s", order=ab.ROW_MAJOR, n_list=int(ann["n_list"]),
                                    n_probe=int(ann.get("n_probe", 1)),
-                                   seed=int(ann.get("seed", 0)))
+                                   seed=int(ann.get("seed", 0)), metric="euclidean")
             self.ann.set_training_data(self.X).train_and_add()
             # every kernel and buffer of the request shapes, now
             for nq in (1, min(max_request_queries, 512), max_batch_queries):
@@ -199,6 +225,28 @@ class Server:
             self.pending[kind] = collections.deque(r for r in q if id(r) not in taken)
             return batch
 
+    def _cap_bytes(self, share):
+        """The device bytes a batch may use now: the worker's share of the
+        budget, and of the free device memory less the reserve."""
+        if self.free_memory is None:
+            return share
+        now = time.perf_counter()
+        if self._free_val is None or now - self._free_at >= self.free_every:
+            try:
+                self._free_val = int(self.free_memory())
+            except Exception:
+                return share
+            self._free_at = now
+        free = self._free_val - self.hbm_reserve
+        return max(0, min(share, free // max(1, len(self.knn_handles))))
+
+    def _fail(self, kind, batch, exc):
+        """A library call failed: every request of the batch completes with
+        the error (its parent request too), and the worker goes on."""
+        for r in batch:
+            (r.parent or r).error = f"{type(exc).__name__}: {exc}"
+        self._finish(kind, batch, sum(r.queries.shape[0] for r in batch), 0.0)
+
     def _finish(self, kind, batch, nq, secs):
         t = time.perf_counter()
         done = []
@@ -223,15 +271,21 @@ class Server:
         h = self.knn_handles[w]
         share = self.hbm_budget // len(self.knn_handles)
         while True:
-            batch = self._take("knn", self.max_batch_queries, share, self.bytes_per_query)
+            batch = self._take("knn", self.max_batch_queries, self._cap_bytes(share),
+                               self.bytes_per_query)
             if batch is None:
                 return
-            Q = batch[0].queries if len(batch) == 1 else np.concatenate([r.queries for r in batch])
-            kmax = max(r.k for r in batch)
-            t0 = time.perf_counter()
-            ind, dist = h.kneighbors(Q, kmax)
-            secs = time.perf_counter() - t0
-            nfb = int(h.stat("knn_tc_fallback_queries"))
+            try:
+                Q = batch[0].queries if len(batch) == 1 else np.concatenate(
+                    [r.queries for r in batch])
+                kmax = max(r.k for r in batch)
+                t0 = time.perf_counter()
+                ind, dist = h.kneighbors(Q, kmax)
+                secs = time.perf_counter() - t0
+                nfb = int(h.stat("knn_tc_fallback_queries"))
+            except Exception as exc:  # the request fails, the worker stays
+                self._fail("knn", batch, exc)
+                continue
             if nfb:
                 with self.cv:
                     self.fallback_queries += nfb
@@ -242,15 +296,20 @@ class Server:
         request's own results are the prefix (the top-k over the probed lists
         in (distance, index) order does not depend on k)."""
         while True:
-            batch = self._take("ann", self.max_batch_queries, self.hbm_budget,
+            batch = self._take("ann", self.max_batch_queries, self._cap_bytes(self.hbm_budget),
                                self.bytes_per_query)
             if batch is None:
                 return
-            Q = batch[0].queries if len(batch) == 1 else np.concatenate([r.queries for r in batch])
-            kmax = max(r.k for r in batch)
-            t0 = time.perf_counter()
-            ind, dist = self.ann.kneighbors(Q, kmax)
-            secs = time.perf_counter() - t0
+            try:
+                Q = batch[0].queries if len(batch) == 1 else np.concatenate(
+                    [r.queries for r in batch])
+                kmax = max(r.k for r in batch)
+                t0 = time.perf_counter()
+                ind, dist = self.ann.kneighbors(Q, kmax)
+                secs = time.perf_counter() - t0
+            except Exception as exc:
+                self._fail("ann", batch, exc)
+                continue
             self._scatter("ann", batch, Q, ind, dist, secs)
 
     def _scatter(self, kind, batch, Q, ind, dist, secs):
@@ -272,11 +331,16 @@ class Server:
             batch = self._take("predict", 1 << 30, 1 << 62, 1, same_model=True)
             if batch is None:
                 return
-            km = self.models[batch[0].model]
-            Q = batch[0].queries if len(batch) == 1 else np.concatenate([r.queries for r in batch])
-            t0 = time.perf_counter()
-            lab = km.predict(Q)
-            secs = time.perf_counter() - t0
+            try:
+                km = self.models[batch[0].model]
+                Q = batch[0].queries if len(batch) == 1 else np.concatenate(
+                    [r.queries for r in batch])
+                t0 = time.perf_counter()
+                lab = km.predict(Q)
+                secs = time.perf_counter() - t0
+            except Exception as exc:
+                self._fail("predict", batch, exc)
+                continue
             o = 0
             for r in batch:
                 m = r.queries.shape[0]
@@ -315,7 +379,7 @@ def replay(server, trace, rng_queries):
         if wait > 0:
             time.sleep(wait)
         Q = rng_queries(size)
-        r = Request(kind, Q, k=arg if kind == "knn" else None,
+        r = Request(kind, Q, k=arg if kind in ("knn", "ann") else None,
                     model=arg if kind == "predict" else None)
         reqs.append(server.submit(r))
     for r in reqs:

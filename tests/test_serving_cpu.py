@@ -155,7 +155,8 @@ def test_serving_ann_requests():
     server = sv.Server(AB(), X, workers=1, max_batch_queries=16, max_request_queries=64,
                        ann={"n_list": 8, "n_probe": 8})
     try:
-        assert server.ann.options == {"n_list": 8, "n_probe": 8, "seed": 0}
+        assert server.ann.options == {"n_list": 8, "n_probe": 8, "seed": 0,
+                                      "metric": "euclidean"}
         reqs = [server.submit(sv.Request(kind, rng.standard_normal((size, 6)), k=k))
                 for kind, size, k in (("ann", 3, 5), ("ann", 40, 2), ("knn", 5, 3),
                                       ("ann", 16, 9))]
@@ -180,3 +181,73 @@ def test_serving_ann_requests():
             pass
     finally:
         plain.close()
+
+
+def test_serving_library_error_completes_the_batch():
+    """A library call that raises completes its requests with the error (and a
+    split request's parent), and the worker keeps serving the next ones."""
+    sv = _load("aoclda_serving_err", os.path.join(PKG, "serving.py"))
+
+    class FailingKNN(FakeKNN):
+        def kneighbors(self, Q, k):
+            if k == 13:
+                raise RuntimeError("da_nn_kneighbors_s: status 2 (memory_error)")
+            return super().kneighbors(Q, k)
+
+    class AB(FakeAB):
+        KNN = FailingKNN
+
+    rng = np.random.default_rng(9)
+    X = rng.standard_normal((300, 4)).astype(np.float32)
+    server = sv.Server(AB(), X, workers=1, max_batch_queries=8, max_request_queries=32,
+                       free_memory=None)
+    try:
+        bad = server.submit(sv.Request("knn", rng.standard_normal((20, 4)), k=13))
+        assert bad.wait(30)
+        assert bad.error and "memory_error" in bad.error
+        good = server.submit(sv.Request("knn", rng.standard_normal((5, 4)), k=3))
+        assert good.wait(30) and good.error is None
+        ind, dist = FakeKNN("s").fit(X).kneighbors(good.queries, 3)
+        np.testing.assert_array_equal(good.result[0], ind)
+    finally:
+        server.close()
+
+
+def test_serving_admission_follows_free_memory():
+    """With little device memory free, batches shrink to what fits (but the
+    oldest request is always taken)."""
+    sv = _load("aoclda_serving_adm", os.path.join(PKG, "serving.py"))
+    rng = np.random.default_rng(10)
+    X = rng.standard_normal((200, 4)).astype(np.float32)
+    free = {"bytes": 1 << 40}
+    gate = threading.Event()
+    armed = {"on": False}  # the start-up warm-up calls do not wait
+
+    class SlowKNN(FakeKNN):
+        def kneighbors(self, Q, k):
+            if armed["on"]:
+                gate.wait(10)
+            return super().kneighbors(Q, k)
+
+    class AB(FakeAB):
+        KNN = SlowKNN
+
+    server = sv.Server(AB(), X, workers=1, max_batch_queries=64, max_request_queries=64,
+                       free_memory=lambda: free["bytes"], hbm_reserve=0)
+    armed["on"] = True
+    server.free_every = 0.0  # read the free memory for every batch
+    try:
+        per_query = server.bytes_per_query
+        first = server.submit(sv.Request("knn", rng.standard_normal((1, 4)), k=1))
+        time.sleep(0.2)  # the worker holds the first batch
+        free["bytes"] = 3 * per_query  # room for three queries per batch
+        later = [server.submit(sv.Request("knn", rng.standard_normal((1, 4)), k=1))
+                 for _ in range(7)]
+        gate.set()
+        for r in [first] + later:
+            assert r.wait(30)
+        sizes = [b[2] for b in server.batches if b[0] == "knn"][1:]
+        assert max(sizes) <= 3 and sum(sizes) == 7
+    finally:
+        gate.set()
+        server.close()

@@ -76,3 +76,37 @@ def test_serving_results_alone_and_in_the_mix(gpu, ab):
     alone_knn.close()
     for km in alone_km.values():
         km.close()
+
+
+def test_serving_ann_alone_and_in_the_mix(gpu, ab):
+    """IVF-flat ("ann") requests served in a mix with kNN requests give, each,
+    what one search of the same index gives alone: the top-k over the probed
+    lists in (distance, index) order does not depend on the batch or on k."""
+    import os
+    sv = _load("aoclda_serving_ann", os.path.join(PKG, "serving.py"))
+    rng = np.random.default_rng(12)
+    nx, d = 100_000, 32
+    X = mixture(rng, nx, d, 64)
+    opts = {"n_list": 64, "n_probe": 8, "seed": 3}
+    server = sv.Server(ab, X, workers=1, max_batch_queries=128, max_request_queries=512, ann=opts)
+    try:
+        trace = []
+        for i in range(30):
+            size = int(np.clip(rng.lognormal(np.log(20), 1.0), 1, 300))
+            kind = "ann" if i % 3 else "knn"
+            trace.append((0.0 if i < 10 else i * 5e-4, kind, size, int(rng.choice([1, 10, 50]))))
+        reqs = sv.replay(server, trace, lambda size: mixture(rng, size, d, 64))
+        assert all(r.error is None and r.result is not None for r in reqs)
+        assert any(b[0] == "ann" and b[1] > 1 for b in server.batches)
+    finally:
+        server.close()
+    lone = ab.ApproxNN("s", order=ab.ROW_MAJOR, metric="euclidean", **opts)
+    lone.set_training_data(X).train_and_add()
+    knn = ab.KNN("s", order=ab.ROW_MAJOR, metric="euclidean").fit(X)
+    for r in reqs:
+        h = lone if r.kind == "ann" else knn
+        ind, dist = h.kneighbors(r.queries, r.k)
+        np.testing.assert_array_equal(r.result[0], ind)
+        np.testing.assert_array_equal(r.result[1], dist)
+    lone.close()
+    knn.close()
