@@ -124,6 +124,7 @@ def load(path=LIB_PATH):
         "da_b200_kmeans_shard_finalize_s": (_P, _P, _P, _P),
         "da_b200_kmeans_shard_inertia_s": (_P, da_int, C.POINTER(C.c_double)),
         "da_b200_kmeans_shard_result_s": (_P, _P, _P),
+        "da_b200_nn_share_data": (_P, _P),
     })
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -280,6 +281,16 @@ class KNN(Handle):
         if targets is not None:
             self.t = np.ascontiguousarray(targets, dtype=self.dtype)
             self.call(f"da_nn_set_targets_{self.prec}", n, ptr(self.t))
+        return self
+
+    def share(self, source):
+        """da_b200_nn_share_data: the training data of the fitted handle
+        `source`, held on the device once for both handles."""
+        self.call("da_b200_nn_share_data", source.h)
+        # the host arrays the handles point at live as long as either
+        for a in ("X", "y", "t"):
+            if hasattr(source, a):
+                setattr(self, a, getattr(source, a))
         return self
 
     def kneighbors(self, Q, k, return_distance=True):

@@ -87,6 +87,8 @@ template <typename T> struct NN : public AlgBase {
     da_status set_data(da_int n, da_int d, const T *X, da_int ldx);
     da_status set_labels(da_int n, const da_int *y);
     da_status set_targets(da_int n, const T *y);
+    // training data of another handle, with its device copies shared
+    da_status share_data(NN<T> &src);
     da_status kneighbors(da_int nq, da_int d, const T *Xt, da_int ldt, da_int *n_ind, T *n_dist,
                          da_int k, da_int return_distance);
     da_status classes_api(da_int *n_classes, da_int *cls);

@@ -684,6 +684,27 @@ da_status da_b200_reset_kernel_time(da_handle h) {
     h->cuda.ktime.clear();
     return da_status_success;
 }
+da_status da_b200_nn_share_data(da_handle h, da_handle source) {
+    if (!h || !source) return da_status_handle_not_initialized;
+    h->err.clear();
+    if (h == source)
+        return h->err.error(da_status_invalid_input, "A handle cannot share its own data.");
+    if (h->precision != source->precision)
+        return h->err.error(da_status_wrong_type,
+                            "The two handles were initialized with different precisions.");
+    if (h->precision == da_single) {
+        auto *a = as_nn<float>(h), *b = as_nn<float>(source);
+        if (!a || !b)
+            return h->err.error(da_status_invalid_handle_type,
+                                "Both handles must be initialized with handle_type=da_handle_nn.");
+        return a->share_data(*b);
+    }
+    auto *a = as_nn<double>(h), *b = as_nn<double>(source);
+    if (!a || !b)
+        return h->err.error(da_status_invalid_handle_type,
+                            "Both handles must be initialized with handle_type=da_handle_nn.");
+    return a->share_data(*b);
+}
 da_status da_b200_kmeans_shard_colmax_s(da_handle h, float *colmax) {
     KM_CALL(float, h, shard_colmax(colmax));
 }

@@ -345,27 +345,40 @@ inline void register_common_options(Registry &r) {
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
+    // owner of the allocation; handles that share a buffer (share()) hold it
+    // together and the last one frees it
+    std::shared_ptr<void> mem;
     DevBuf() = default;
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        mem.reset();
         p = nullptr;
         bytes = 0;
     }
-    // grow-only allocation; returns false on failure
+    // grow-only allocation of memory this buffer alone holds (a shared
+    // buffer is let go first: whoever calls ensure() writes into it);
+    // returns false on failure
     bool ensure(size_t b) {
-        if (b <= bytes && p) return true;
+        if (b <= bytes && p && mem.use_count() == 1) return true;
         release();
         if (b == 0) b = 16;
-        if (device_alloc(&p, b) != cudaSuccess) {
+        void *q = nullptr;
+        if (device_alloc(&q, b) != cudaSuccess) {
             cudaGetLastError();
-            p = nullptr;
             return false;
         }
+        mem = std::shared_ptr<void>(q, [](void *x) { cudaFree(x); });
+        p = q;
         bytes = b;
         return true;
+    }
+    // hold the same allocation as o (read-only by convention)
+    void share(const DevBuf &o) {
+        mem = o.mem;
+        p = o.p;
+        bytes = o.bytes;
     }
     template <typename T> T *as() const { return static_cast<T *>(p); }
 };

@@ -16,9 +16,9 @@
 // at every window boundary of the list, a warp merges a complete window into
 // the query's smallest listed values and lowers theta_q to their k-th
 // + 2 eps_q -- k distinct listed rows, so never below the global k-th:
-// theta_q stays a valid bound while it tightens.  theta_q starts from an exact pre-pass over the first
-// TK_PRE_ROWS training rows (the k-th smallest plain distance there bounds
-// the global one).  The finalize kernel re-scores the listed rows
+// theta_q stays a valid bound while it tightens.  theta_q starts from an
+// exact pre-pass over slices of the first training rows (the k-th smallest
+// plain distance within any slice bounds the global one).  The finalize kernel re-scores the listed rows
 // with v'_tc < theta_q exactly (the plain kernel's formula and order) and
 // keeps the k best by (distance, index): the plain path's neighbours.
 #include "b200_common.cuh"
@@ -37,13 +37,15 @@ constexpr int TK_BM = 128;         // train rows per tile (UMMA M, TMEM lanes)
 constexpr int TK_BN = 256;         // queries per tile (UMMA N, TMEM columns), at most
 constexpr int TK_KB = 64;          // bf16 elements per 128-byte K block
 constexpr int TK_THREADS = 320;    // TMA warp, MMA warp, 8 epilogue warps
-constexpr int TK_PRE_ROWS = 16384; // training rows of the threshold pre-pass (small batches;
-                                   // 4,096 from 2,048 queries up)
+constexpr int TK_PRE_SLICE = 2048; // unit of the threshold pre-pass's row count
 constexpr int TK_BEST = 256;       // smallest listed values kept per query (>= k)
 constexpr int TK_WIN = 128;        // list entries merged into them per refresh
 constexpr int TK_CHUNK_TILES = 64; // train tiles per work item
 constexpr int TK_FIN_MAX = 8192;   // candidates re-scored per query (more: fallback)
-constexpr int TK_STASH = 4;        // values below threshold held per lane before reserving
+// values below threshold held per lane before reserving list slots (the
+// 256-query tile keeps 4: its shared memory is needed for the stages)
+__host__ __device__ constexpr int tk_stash(int bn) { return bn >= 256 ? 4 : 8; }
+static_assert(TK_CHUNK_TILES <= 64 && TK_BN <= 256, "stash entry bit fields");
 
 struct KnnTcArgs {
     int nx, nq, k, nkb, stages, n_qtiles, n_xtiles, n_items, cap;
@@ -145,8 +147,9 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
     unsigned char *As = Bl + (size_t)nkb * kB; // S stages of (Ah, Al) for one K block
     float *th_w = reinterpret_cast<float *>(As + (size_t)S * 2 * kA); // 8 warps x BN
     int *col_w = reinterpret_cast<int *>(th_w + 8 * BN);                // 8 warps x BN
-    int2 *stash_w = reinterpret_cast<int2 *>(col_w + 8 * BN); // 8 warps x 32 lanes x TK_STASH
-    TkShared *sh = reinterpret_cast<TkShared *>(stash_w + 8 * 32 * TK_STASH);
+    constexpr int STASH = tk_stash(BN);
+    int2 *stash_w = reinterpret_cast<int2 *>(col_w + 8 * BN); // 8 warps x 32 lanes x STASH
+    TkShared *sh = reinterpret_cast<TkShared *>(stash_w + 8 * 32 * STASH);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -284,19 +287,23 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
         const int q = warp & 3;   // TMEM lane quarter
         float *thw = th_w + e * BN;
         int *colcnt = col_w + e * BN;                          // zero between flushes
-        int2 *stash = stash_w + (size_t)(e * 32 + lane) * TK_STASH; // (column, value bits)
+        // stash entry: (column | tile offset in the work item << 8 | rank << 14,
+        // value bits); the rank is assigned when list slots are reserved
+        int2 *stash = stash_w + (size_t)(e * 32 + lane) * STASH;
         int ns = 0;
         const float inf = __int_as_float(0x7f800000);
         // Reserve list slots for the stashed values (one global atomic per
         // query column, all columns at once), write them, and merge the list
         // windows they complete into the queries' best values (threshold
-        // refresh).  Warp-cooperative; `row` is this lane's train row.
-        auto flush = [&](int qt_, int row_) {
+        // refresh).  Warp-cooperative, once a lane's stash is full or the
+        // work item (query tile qt_, train tiles from x0_) ends: the global
+        // round trips are paid once per many tiles.
+        auto flush = [&](int qt_, int x0_) {
             if (!__any_sync(0xffffffffu, ns > 0)) return;
             for (int i = 0; i < ns; ++i) {
-                const int col = stash[i].x & 0xFFFF;
+                const int col = stash[i].x & 0xFF;
                 const int rank = atomicAdd(&colcnt[col], 1);
-                stash[i].x = col | (rank << 16);
+                stash[i].x = (stash[i].x & 0x3FFF) | (rank << 14);
             }
             __syncwarp();
             int nn[BN / 32], bb[BN / 32];
@@ -310,7 +317,9 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
             for (int j = 0; j < BN / 32; ++j) colcnt[j * 32 + lane] = bb[j];
             __syncwarp();
             for (int i = 0; i < ns; ++i) {
-                const int col = stash[i].x & 0xFFFF, rank = stash[i].x >> 16;
+                const int x = stash[i].x;
+                const int col = x & 0xFF, rank = x >> 14;
+                const int row_ = (x0_ + ((x >> 8) & 0x3F)) * TK_BM + q * 32 + lane;
                 const int pos = colcnt[col] + rank;
                 if (pos < a.cap)
                     a.list[(size_t)(qt_ * BN + col) * a.cap + pos] = make_int2(stash[i].y, row_);
@@ -408,8 +417,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                 tc_fence_after();
                 const uint32_t trow = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN);
                 // pass over the tile: values below their query's threshold
-                // go to this lane's stash (column, value); the list slots are
-                // reserved per tile, after the accumulator is released
+                // go to this lane's stash (column, tile, value)
                 for (int c = 0; c < BN / 32; ++c) {
                     float v[32];
                     tmem_ld32(trow + (uint32_t)(c * 32), v);
@@ -423,19 +431,21 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
                     for (int u = 0; u < 32; ++u)
                         bits |= (tk_val<COS>(v[u], xn) < thw[c * 32 + u] ? 1u : 0u) << u;
                     while (__any_sync(0xffffffffu, bits != 0)) {
-                        while (bits && ns < TK_STASH) {
+                        while (bits && ns < STASH) {
                             const int u = __ffs(bits) - 1;
                             bits &= bits - 1;
-                            stash[ns++] = make_int2(c * 32 + u, __float_as_int(tk_val<COS>(pick32(v, u), xn)));
+                            stash[ns++] = make_int2((c * 32 + u) | ((xt - x0) << 8),
+                                                    __float_as_int(tk_val<COS>(pick32(v, u), xn)));
                         }
                         // some lane's stash is full: reserve and write now
-                        if (__any_sync(0xffffffffu, bits != 0)) flush(qt, row);
+                        if (__any_sync(0xffffffffu, bits != 0)) flush(qt, x0);
                     }
                 }
                 tc_fence_before();
                 mbar_arrive(&sh->tempty[b]);
-                flush(qt, row);
             }
+            if (!ok) break;
+            flush(qt, x0);
         }
     }
     tc_fence_before();
@@ -478,21 +488,6 @@ __global__ void knn_tc_prep_queries(const float *Q, int ld, int nq, int d, int n
         cnt[qi] = 0;
         qsq[qi] = s;
     }
-}
-
-// theta_q from the pre-pass: p = k-th smallest plain squared distance over a
-// subset of the rows; theta_q = p - |q|^2 + 4 eps_q >= v'_tc(k) + 2 eps_q
-// (k rows with plain value <= p have v'_tc <= p - |q|^2 + eps_q; the fp32
-// |q|^2 is within eps_q of |q|^2).
-// Cosine: p is a plain cosine distance and theta_q = 2 (p - 1) + 4 eps.
-__global__ void knn_tc_init_theta(const float *pre_key, int k, int nq, const float *qsq,
-                                  const float *margin, unsigned *theta, int cosm) {
-    const int qi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (qi >= nq) return;
-    const float pk = pre_key[(size_t)qi * k + (k - 1)];
-    const float t = cosm ? nudge_up(2.f * (pk - 1.f) + 2.f * margin[qi])
-                         : nudge_up(pk - qsq[qi] + 2.f * margin[qi]);
-    if (t == t) theta[qi] = ord_bits(t);
 }
 
 __global__ void knn_tc_fill_best(float *best, size_t n) {
@@ -542,6 +537,183 @@ __device__ __forceinline__ float cos_ref(const float *x, const float *q, int d, 
     float g = 0.f;
     for (int f = 0; f < d; ++f) g = __fmaf_rn(x[f], q[f], g);
     return __fsub_rn(1.f, __fdiv_rn(g, __fmul_rn(xn, qn)));
+}
+
+// ---------------------------------------------------- threshold pre-pass --
+// theta_q starts from the k-th smallest plain key p over the first rows of
+// the training set: theta_q = p - |q|^2 + 4 eps_q >= v'_tc(k) + 2 eps_q (k
+// rows with plain value <= p have v'_tc <= p - |q|^2 + eps_q; the fp32 |q|^2
+// is within eps_q of |q|^2).  Cosine: p is a plain cosine distance and
+// theta_q = 2 (p - 1) + 4 eps.  The rows are cut into slices of TK_PRE_SLICE;
+// block (slice, query) computes the keys of its slice and keeps their k
+// smallest, and one block per query takes the k-th smallest of those.
+
+constexpr int TK_PRE_WARPS = 16;
+
+// The k-th smallest (1-based) of n keys in shared memory, by a radix select
+// on four 8-bit digits, most significant first.  Block-wide (every thread
+// gets the result); n >= k >= 1.
+__device__ unsigned block_kth(const unsigned *keys, int n, int k, int *hist, int *sel) {
+    unsigned prefix = 0, mask = 0;
+    int kk = k; // rank of the wanted key among those matching prefix
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const unsigned u = keys[i];
+            if ((u & mask) == prefix) atomicAdd(&hist[(u >> shift) & 255u], 1);
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            int c[8], sum = 0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                c[j] = hist[lane * 8 + j];
+                sum += c[j];
+            }
+            int inc = sum;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, inc, off);
+                if (lane >= off) inc += t;
+            }
+            const int exc = inc - sum;
+            if (exc < kk && kk <= inc) { // this lane's 8 digits hold the kk-th key
+                int run = exc, b = 7;
+                for (int j = 0; j < 8; ++j) {
+                    if (run + c[j] >= kk) {
+                        b = j;
+                        break;
+                    }
+                    run += c[j];
+                }
+                sel[0] = lane * 8 + b;
+                sel[1] = kk - run;
+            }
+        }
+        __syncthreads();
+        prefix |= (unsigned)sel[0] << shift;
+        mask |= 0xFFu << shift;
+        kk = sel[1];
+    }
+    return prefix;
+}
+
+// Keys (order-preserving bits) of rows r0 .. r0+n-1 against the query qv in
+// shared memory: each warp stages 32 rows x 32 columns at a time with
+// coalesced loads, and each lane accumulates one row in the plain path's
+// order (sqeuc_ref; cos_ref for cosine), carried across the column slabs.
+__device__ void block_keys(const float *X, int ld, int d, int kc, int r0, int n, const float *qv,
+                           unsigned *keys, float *stage, const float *xnp, float qn) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *t = stage + warp * 32 * 33;
+    const int d4 = d & ~3;
+    for (int rb = warp * 32; rb < n; rb += TK_PRE_WARPS * 32) {
+        const int nr = min(32, n - rb);
+        float g1 = 0.f, g2 = 0.f;
+        for (int c0 = 0; c0 < d; c0 += 32) {
+            const int cw = min(32, d - c0);
+            __syncwarp();
+            for (int r = 0; r < nr; ++r)
+                if (lane < cw) t[r * 33 + lane] = X[(size_t)(r0 + rb + r) * ld + c0 + lane];
+            __syncwarp();
+            if (lane < nr) {
+                const float *x = t + lane * 33 - c0; // x[f] for f in [c0, c0 + cw)
+                if (xnp) {
+                    for (int f = c0; f < c0 + cw; ++f) g1 = __fmaf_rn(x[f], qv[f], g1);
+                } else {
+                    int kg = c0;
+                    for (; kg < c0 + cw && kg < d4; kg += 4) {
+                        const float t0 = __fsub_rn(qv[kg], x[kg]), t1 = __fsub_rn(qv[kg + 1], x[kg + 1]);
+                        const float t2 = __fsub_rn(qv[kg + 2], x[kg + 2]);
+                        const float t3 = __fsub_rn(qv[kg + 3], x[kg + 3]);
+                        g1 = __fmaf_rn(t0, t0, g1);
+                        g1 = __fmaf_rn(t1, t1, g1);
+                        g2 = __fmaf_rn(t2, t2, g2);
+                        g2 = __fmaf_rn(t3, t3, g2);
+                        if (((kg + 4) % kc) == 0 || (kg + 4) == d4) {
+                            g1 = __fadd_rn(g1, g2);
+                            g2 = 0.f;
+                        }
+                    }
+                    for (int f = max(kg, d4); f < c0 + cw; ++f) {
+                        const float u = __fsub_rn(qv[f], x[f]);
+                        g1 = __fmaf_rn(u, u, g1);
+                    }
+                }
+            }
+        }
+        if (lane < nr) {
+            const int i = rb + lane;
+            const float v = xnp ? __fsub_rn(1.f, __fdiv_rn(g1, __fmul_rn(xnp[r0 + i], qn))) : g1;
+            keys[i] = ord_bits(v);
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned pre_theta_bits(unsigned kth, float qsq, float margin,
+                                                   bool cosm) {
+    const float pk = ord_float(kth);
+    const float t = cosm ? nudge_up(2.f * (pk - 1.f) + 2.f * margin)
+                         : nudge_up(pk - qsq + 2.f * margin);
+    return t == t ? ord_bits(t) : ord_bits(__int_as_float(0x7f800000));
+}
+
+// Block (slice, query).  slices == 1: theta_q directly from the slice's k-th
+// key.  Otherwise the slice's k smallest keys (padded with +inf when the
+// slice holds fewer than k rows) go to out[(q * slices + slice) * k ...].
+__global__ void __launch_bounds__(TK_PRE_WARPS * 32)
+knn_tc_pre_slice(const float *X, const float *Q, int ld, int d, int kc, int nx, int nq, int k,
+                 int slices, const float *qsq, const float *margin, unsigned *theta,
+                 unsigned *out, const float *xnp, const float *qnp) {
+    __shared__ int hist[256];
+    __shared__ int sel[2];
+    __shared__ int nlt;
+    extern __shared__ __align__(16) unsigned pre_sm[];
+    unsigned *keys = pre_sm;                                        // TK_PRE_SLICE
+    float *stage = reinterpret_cast<float *>(keys + TK_PRE_SLICE);  // warps x 32 x 33
+    float *qv = stage + TK_PRE_WARPS * 32 * 33;                     // d
+    const int sl = blockIdx.x, qi = blockIdx.y;
+    const int r0 = sl * TK_PRE_SLICE;
+    const int n = max(0, min(TK_PRE_SLICE, nx - r0));
+    for (int f = threadIdx.x; f < d; f += blockDim.x) qv[f] = Q[(size_t)qi * ld + f];
+    if (threadIdx.x == 0) nlt = 0;
+    __syncthreads();
+    block_keys(X, ld, d, kc, r0, n, qv, keys, stage, xnp, xnp ? qnp[qi] : 1.f);
+    __syncthreads();
+    if (slices == 1) {
+        if (n < k) return;
+        const unsigned kth = block_kth(keys, n, k, hist, sel);
+        if (threadIdx.x == 0) theta[qi] = pre_theta_bits(kth, qsq[qi], margin[qi], xnp != nullptr);
+        return;
+    }
+    unsigned *o = out + ((size_t)qi * slices + sl) * k;
+    if (n <= k) {
+        for (int i = threadIdx.x; i < k; i += blockDim.x)
+            o[i] = i < n ? keys[i] : ord_bits(__int_as_float(0x7f800000));
+        return;
+    }
+    const unsigned kth = block_kth(keys, n, k, hist, sel);
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (keys[i] < kth) o[atomicAdd(&nlt, 1)] = keys[i];
+    __syncthreads();
+    for (int i = nlt + threadIdx.x; i < k; i += blockDim.x) o[i] = kth; // ties at the k-th
+}
+
+// One block per query: theta_q from the k-th smallest of the slices' keys.
+__global__ void __launch_bounds__(256)
+knn_tc_pre_merge(const unsigned *in, int slices, int k, int nq, const float *qsq,
+                 const float *margin, unsigned *theta, int cosm) {
+    __shared__ int hist[256];
+    __shared__ int sel[2];
+    extern __shared__ __align__(16) unsigned merge_sm[]; // slices * k
+    const int qi = blockIdx.x;
+    const int n = slices * k;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) merge_sm[i] = in[(size_t)qi * n + i];
+    __syncthreads();
+    const unsigned kth = block_kth(merge_sm, n, k, hist, sel);
+    if (threadIdx.x == 0) theta[qi] = pre_theta_bits(kth, qsq[qi], margin[qi], cosm != 0);
 }
 
 __global__ void __launch_bounds__(256)
@@ -639,7 +811,7 @@ __global__ void sqrt_inplace_kernel(float *v) { *v = sqrtf(*v) * 1.0001f; }
 
 size_t tk_smem_bytes(int nkb, int stages, int bn = TK_BN) {
     return 1024 + (size_t)nkb * 2 * bn * 128 + (size_t)stages * 2 * TK_BM * 128 +
-           (size_t)8 * bn * 4 * 2 + (size_t)8 * 32 * TK_STASH * 8 + sizeof(TkShared) + 64;
+           (size_t)8 * bn * 4 * 2 + (size_t)8 * 32 * tk_stash(bn) * 8 + sizeof(TkShared) + 64;
 }
 
 } // namespace
@@ -730,30 +902,35 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
         knn_tc_prep_queries<<<(nq_pad + wpb - 1) / wpb, wpb * 32, 0, s>>>(
             Q, ld, nq, d, nq_pad, ldbf, Qh, Ql, (float)(cosm ? ec : e1), (float)e2, xmax, margin,
             theta, cnt, qsq, cosm ? cosine->qnorm : nullptr);
-        // exact pre-pass over the first training rows (plain kernels; its
-        // partial lists live in the candidate list buffer, its merged keys in
-        // the output arrays, both overwritten below)
-        // exact pre-pass rows: its cost grows with the batch, while large
-        // batches tighten their thresholds quickly on their own
-        const int pre = std::min(nx, nq >= 2048 ? 4096 : TK_PRE_ROWS);
-        if (pre >= k) {
-            const int BN = knn_tile_rows_train(false);
-            int n_chunks = std::max(1, std::min((pre + BN - 1) / BN, 16));
-            int chunk_rows = ((pre + n_chunks - 1) / n_chunks + BN - 1) / BN * BN;
-            n_chunks = (pre + chunk_rows - 1) / chunk_rows;
-            KnnArgs pa{cosm ? ACC_DOT : ACC_SQEUC, cosm ? POST_COSINE : POST_NONE, kc, 2.0, k,
-                       chunk_rows, n_chunks};
-            float *pk = static_cast<float *>(list);
-            int *pi = reinterpret_cast<int *>(pk + (size_t)nq * n_chunks * k);
-            cudaError_t e = launch_knn_chunks<float>(Q, ld, nq, X, ld, pre, d,
-                                                     cosm ? cosine->qnorm : nullptr,
-                                                     cosm ? cosine->xnorm : nullptr, pa, pk, pi,
-                                                     nullptr, s);
-            if (e == cudaSuccess)
-                e = launch_knn_merge<float>(pk, pi, nq, n_chunks, k, 0, out_key, out_idx, s);
+        // exact pre-pass over the first rows (slices of TK_PRE_SLICE): at
+        // least two blocks per SM in all, enough rows that the starting
+        // threshold alone would keep about 4,096 candidates per query over
+        // the whole set, at most 64 slices and about eight blocks per SM
+        {
+            const long long want_rows = (long long)nx * k / 4096;
+            int slices = std::max(296 / std::max(1, nq),
+                                  (int)std::min<long long>(64, (want_rows + TK_PRE_SLICE - 1) /
+                                                                   TK_PRE_SLICE));
+            slices = std::min(slices, std::max(1, 1184 / std::max(1, nq)));
+            slices = std::max(1, std::min(std::min(slices, 64), (nx + TK_PRE_SLICE - 1) / TK_PRE_SLICE));
+            const size_t psm = (size_t)TK_PRE_SLICE * 4 + (size_t)TK_PRE_WARPS * 32 * 33 * 4 +
+                               (size_t)d * sizeof(float);
+            cudaError_t e = ensure_smem_limit(reinterpret_cast<const void *>(knn_tc_pre_slice), psm);
             if (e != cudaSuccess) return e;
-            knn_tc_init_theta<<<(nq + 255) / 256, 256, 0, s>>>(out_key, k, nq, qsq, margin, theta,
-                                                               cosm ? 1 : 0);
+            // the slices' keys sit in the candidate list buffer (nq * cap
+            // entries of 8 bytes; slices * k <= 16,384 keys of 4), which is
+            // refilled below
+            unsigned *keys = static_cast<unsigned *>(list);
+            knn_tc_pre_slice<<<dim3(slices, nq), TK_PRE_WARPS * 32, psm, s>>>(
+                X, Q, ld, d, kc, nx, nq, k, slices, qsq, margin, theta, keys,
+                cosm ? cosine->xnorm : nullptr, cosm ? cosine->qnorm : nullptr);
+            if (slices > 1) {
+                const size_t msm = (size_t)slices * k * sizeof(unsigned);
+                e = ensure_smem_limit(reinterpret_cast<const void *>(knn_tc_pre_merge), msm);
+                if (e != cudaSuccess) return e;
+                knn_tc_pre_merge<<<nq, 256, msm, s>>>(keys, slices, k, nq, qsq, margin, theta,
+                                                      cosm ? 1 : 0);
+            }
         }
         const size_t nl = (size_t)nq * cap;
         knn_tc_fill_list<<<(unsigned)((nl + 255) / 256), 256, 0, s>>>(static_cast<int2 *>(list), nl);

@@ -138,6 +138,89 @@ da_status NN<T>::set_data(da_int n, da_int d, const T *X, da_int ldx) {
     return da_status_success;
 }
 
+// The training data of `src` (same precision and storage order, same device):
+// this handle takes its host pointers (rows, labels, targets) as set_data /
+// set_labels / set_targets would, and holds the same device copies of the
+// rows -- fp32/fp64 rows, and the tensor-core bf16 pair and norms when src
+// has built them -- instead of uploading its own.  Neither handle writes into
+// a shared copy: a later set_data on either gives that handle new buffers.
+template <typename T> da_status NN<T>::share_data(NN<T> &src) {
+    if (!src.have_X)
+        return err->error(da_status_no_data, "The source handle holds no training data.");
+    if (src.order() != order())
+        return err->error(da_status_invalid_input,
+                          "The two handles have different storage orders.");
+    if (n_samples > 0 && src.n_samples != n_samples)
+        return err->error(da_status_invalid_array_dimension,
+                          "n_samples = " + std::to_string(src.n_samples) +
+                              " doesn't match the training data size " +
+                              std::to_string(n_samples) + ".");
+    da_status s = cuda->init(*err);
+    if (s != da_status_success) return s;
+    if (src.cuda->init(*src.err) != da_status_success || src.ensure_device_data() != da_status_success)
+        return err->error(da_status_memory_error,
+                          "The source handle's training data are not on the device: " +
+                              src.err->message);
+    if (src.cuda->device != cuda->device)
+        return err->error(da_status_invalid_input, "The two handles use different devices.");
+    // the source's uploads are complete before this handle's stream reads them
+    B200_TRY(cudaStreamSynchronize(src.cuda->stream), "synchronisation with the source handle");
+    n_samples = src.n_samples;
+    n_features = src.n_features;
+    X_host = src.X_host;
+    if (!src.X_own.empty()) { // a loaded source owns its rows: keep a copy
+        X_own = src.X_own;
+        X_host = X_own.data();
+    }
+    ldx_host = src.ldx_host;
+    data_order = src.data_order;
+    have_X = true;
+    s = set_params();
+    if (s != da_status_success) return s;
+    locked_algo = algo;
+    locked_leaf = opts.i("leaf size");
+    locked_metric = metric;
+    locked_p = p;
+    ld = src.ld;
+    dX.share(src.dX);
+    X_on_device = true;
+    xn_kind = -1;
+    tc_train_ready = false;
+    if (src.tc_train_ready) {
+        // max |x| is the first scalar of the tensor-core state; the rest of
+        // that buffer is per call
+        if (!dTkScal.ensure(64))
+            return err->error(da_status_memory_error, "Device memory allocation failed.");
+        B200_TRY(cudaMemcpyAsync(dTkScal.p, src.dTkScal.p, 16, cudaMemcpyDeviceToDevice,
+                                 cuda->stream),
+                 "copy");
+        dXh.share(src.dXh);
+        dXl.share(src.dXl);
+        dXsq.share(src.dXsq);
+        tc_ldbf = src.tc_ldbf;
+        tc_train_ready = true;
+    }
+    if (src.have_labels) {
+        const da_int *y = src.y_class;
+        if (!src.y_own.empty()) {
+            y_own = src.y_own;
+            y = y_own.data();
+        }
+        s = set_labels(src.n_samples, y);
+        if (s != da_status_success) return s;
+    }
+    if (src.have_targets) {
+        const T *y = src.y_reg;
+        if (!src.t_own.empty()) {
+            t_own = src.t_own;
+            y = t_own.data();
+        }
+        s = set_targets(src.n_samples, y);
+        if (s != da_status_success) return s;
+    }
+    return da_status_success;
+}
+
 // Model persistence: the training rows in their storage order (dense), then
 // the labels and targets when set.  Loading replays set_data / set_labels /
 // set_targets on the handle's own copies (the options were loaded first).

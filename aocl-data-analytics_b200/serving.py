@@ -1,7 +1,9 @@
 """Request loop over device-resident kNN indexes and k-means models.
 
 The training set of the kNN index and the centres of the k-means models stay
-in device memory for the life of the server (one library handle per worker).
+in device memory for the life of the server: one library handle per worker,
+the kNN handles holding one shared device copy of the index
+(da_b200_nn_share_data).
 Requests -- a kNN search (queries, k), an approximate (IVF-flat) search
 (queries, k) when the server holds an IVF-flat index, or a k-means predict
 (model, queries) -- are queued as they arrive; a kNN request with more queries than one call
@@ -114,10 +116,15 @@ class Server:
         self.batches = []          # (kind, requests, queries, seconds) of every library call
         self.fallback_queries = 0  # kNN queries the tensor-core pass handed to the plain path
         self.knn_handles = []
-        for _ in range(workers):
+        for w in range(workers):
             h = ab.KNN("s", order=ab.ROW_MAJOR, metric="euclidean",
                        precision_mode=precision_mode)
-            h.fit(self.X)
+            if w == 0:
+                h.fit(self.X)
+            else:
+                # one device copy of the index (rows and tensor-core copies,
+                # built by the first handle's warm-up below) for every worker
+                h.share(self.knn_handles[0])
             # one call of the largest batch: the device copies and every
             # per-call buffer reach their final size now, so that no request
             # waits for a device allocation (which also stalls other work);

@@ -29,6 +29,19 @@ da_status da_b200_get_kernel_time(da_handle handle, const char *kernel, double *
                                   da_int *launches);
 da_status da_b200_reset_kernel_time(da_handle handle);
 
+/* kNN: give `handle` the training data (and labels / targets) already set on
+ * `source` -- same precision, storage order and device -- without a second
+ * device copy: both handles hold the same device rows (and the tensor-core
+ * bf16 copies when `source` has built them, i.e. after its first tensor-core
+ * search), which stay allocated until the last of them lets go.  `handle`
+ * keeps its own options and per-call buffers, so the two handles can search
+ * at the same time on their own streams.  Host pointers are taken as
+ * da_nn_set_data would take them.  A later da_nn_set_data on either handle
+ * gives that handle fresh device buffers.  Replaces, for a server with one
+ * handle per worker, a da_nn_set_data_{s,d} (nearest_neighbors_public.cpp)
+ * per worker. */
+da_status da_b200_nn_share_data(da_handle handle, da_handle source);
+
 /* Named statistics of the last call: "relabelled_rows" (k-means rows of the
  * last tensor-core assignment whose label needed the exact fp32 re-score),
  * "tensor_core" (1 when the last k-means compute used the tensor cores). */

@@ -34,6 +34,8 @@ def run(ab, X, Q, k, metric, mode, order):
     (300_000, 40, 64, 10, "euclidean", 0),       # 64-query tiles
     (180_000, 100, 96, 100, "sqeuclidean", 0),   # 128-query tiles
     (300_000, 1, 64, 1, "euclidean", 1),
+    (1_000_000, 1, 96, 100, "euclidean", 0),     # one query, all blocks on its list
+    (600_000, 3, 64, 256, "sqeuclidean", 1),
     (200_000, 700, 128, 100, "cosine", 0),
     (300_000, 40, 64, 10, "cosine", 1),
 ])

@@ -20,6 +20,10 @@ class FakeKNN:
         self.X = np.asarray(X, dtype=np.float64)
         return self
 
+    def share(self, source):
+        self.X = source.X
+        return self
+
     def kneighbors(self, Q, k):
         self.calls.append(Q.shape[0])
         d2 = ((np.asarray(Q, dtype=np.float64)[:, None, :] - self.X[None]) ** 2).sum(-1)
