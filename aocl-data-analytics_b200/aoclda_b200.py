@@ -558,3 +558,14 @@ def kmeans_batched(Xs, C0s, max_iter=300, tol=1e-4):
     return [{"centres": outs[i], "labels": labs[i], "n_iter": int(nit[i]),
              "inertia": float(inert[i]), "converged": int(conv[i])} for i in range(m)]
 
+
+def kmeans_batched_timing():
+    """da_b200_kmeans_batched_timing: (upload, fit, download) device
+    milliseconds of this thread's last kmeans_batched call."""
+    L = lib()
+    v = [C.c_double() for _ in range(3)]
+    st = L.da_b200_kmeans_batched_timing(*[C.byref(x) for x in v])
+    if st != SUCCESS:
+        raise DAError(st, "da_b200_kmeans_batched_timing")
+    return tuple(x.value for x in v)
+

@@ -106,9 +106,13 @@ da_status da_b200_kmeans_shard_result_s(da_handle handle, float *centres, da_int
  * "empty clusters" = "ignore": centres (C_out[i], k x d row-major), labels
  * (labels_out[i]), iteration count, convergence code (0: max_iter reached,
  * 1: centre shift below tol, 2: labels unchanged) and inertia (fp64 sum, to
- * within rounding).  All instances advance together on the device, each
- * Lloyd iteration one pass over (instance, tile) work tables, the whole fit
- * one CUDA graph.  Limits: k <= n and k * d <= 8192 per instance; finite
+ * within rounding).  All instances advance together on the device: in each
+ * Lloyd iteration persistent blocks take (instance, tile) items off work
+ * queues (the assignment, then the update of the changed rows' centroid
+ * sums), and the whole fit is one CUDA graph.  The assignment's tile shape
+ * for each (row width, k range) is picked by timing the candidates the
+ * first time the process meets that shape (the choice is kept; results do
+ * not depend on it).  Limits: k <= n and k * d <= 8192 per instance; finite
  * data (else da_status_invalid_input).  `stream`: a cudaStream_t the inputs
  * are uploaded on (NULL: the legacy default stream); the call returns when
  * the results are on the host. */
@@ -119,6 +123,12 @@ da_status da_b200_kmeans_batched_s(da_int n_inst, const da_int *n_samples,
                                    float *const *C_out, da_int *const *labels_out,
                                    da_int *n_iter, double *inertia, da_int *converged,
                                    void *stream);
+
+/* Device times, in milliseconds, of the calling thread's last successful
+ * da_b200_kmeans_batched_s call: the upload of the data sets and initial
+ * centres, the fit (the CUDA graph of all Lloyd iterations, the final
+ * relabelling and the inertia) and the download of centres and labels. */
+da_status da_b200_kmeans_batched_timing(double *upload_ms, double *fit_ms, double *download_ms);
 
 /* No counterpart in the AOCL-DA API.  Brute-force euclidean k nearest
  * neighbours for callers that cannot allocate device memory (code running

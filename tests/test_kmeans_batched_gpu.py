@@ -58,3 +58,20 @@ def test_batched_argument_checks(ab):
     assert L.da_b200_kmeans_batched_s(1, None, None, None, None, None, None, 10,
                                       C.c_double(1e-4), None, None, None, None, None,
                                       None) == 3  # invalid_pointer
+
+
+@pytest.mark.gpu
+def test_batched_timing_and_one_at_a_time(gpu, ab):
+    """The device timings of the last call are reported, and a data set
+    fitted alone (other tile shapes' groups absent) gives the same result as
+    in the batch."""
+    Xs, C0s = make_batch(5, 8)
+    out = ab.kmeans_batched(Xs, C0s, max_iter=20, tol=1e-4)
+    up, fit, down = ab.kmeans_batched_timing()
+    assert up > 0.0 and fit > 0.0 and down > 0.0
+    for X, C0, r in zip(Xs, C0s, out):
+        r1 = ab.kmeans_batched([X], [C0], max_iter=20, tol=1e-4)[0]
+        assert r1["n_iter"] == r["n_iter"]
+        np.testing.assert_array_equal(r1["labels"], r["labels"])
+        np.testing.assert_array_equal(r1["centres"], r["centres"])
+        assert r1["inertia"] == r["inertia"]
