@@ -110,6 +110,7 @@ def load(path=LIB_PATH):
     }
     sig.update({
         "da_b200_set_stream": (_P, _P),
+        "da_b200_set_stream_priority": (_P, da_int),
         "da_b200_set_kernel_timing": (_P, da_int),
         "da_b200_get_kernel_time": (_P, C.c_char_p, C.POINTER(C.c_double), C.POINTER(da_int)),
         "da_b200_reset_kernel_time": (_P,),
@@ -198,6 +199,12 @@ class Handle:
             self.close()
         except Exception:
             pass
+
+    def set_stream_priority(self, priority):
+        """da_b200_set_stream_priority: the handle's own stream recreated with
+        this CUDA priority (negative: higher)."""
+        self.call("da_b200_set_stream_priority", int(priority))
+        return self
 
     def kernel_time(self, name):
         ms = C.c_double()
@@ -557,6 +564,16 @@ def kmeans_batched(Xs, C0s, max_iter=300, tol=1e-4):
         raise DAError(st, "da_b200_kmeans_batched_s")
     return [{"centres": outs[i], "labels": labs[i], "n_iter": int(nit[i]),
              "inertia": float(inert[i]), "converged": int(conv[i])} for i in range(m)]
+
+
+def device_memory():
+    """da_b200_device_memory: (free, total) bytes of the current device."""
+    L = lib()
+    f, t = C.c_ulonglong(), C.c_ulonglong()
+    st = L.da_b200_device_memory(C.byref(f), C.byref(t))
+    if st != SUCCESS:
+        raise DAError(st, "da_b200_device_memory")
+    return f.value, t.value
 
 
 def kmeans_batched_timing():

@@ -3,6 +3,7 @@
 // reference implementation whose behaviour it reproduces.
 #include "alg.hpp"
 #include "../../include/aoclda_b200_ext.h"
+#include <algorithm>
 
 using namespace b200;
 
@@ -650,6 +651,27 @@ da_status da_b200_set_stream(da_handle h, void *stream) {
     h->cuda.stream = stream ? static_cast<cudaStream_t>(stream) : h->cuda.own_stream;
     return da_status_success;
 }
+da_status da_b200_set_stream_priority(da_handle h, da_int priority) {
+    if (!h) return da_status_handle_not_initialized;
+    h->err.clear();
+    da_status s = h->cuda.init(h->err);
+    if (s != da_status_success) return s;
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    const int p = std::max(greatest, std::min(least, (int)priority));
+    cudaStream_t ns = nullptr;
+    if (cudaStreamCreateWithPriority(&ns, cudaStreamNonBlocking, p) != cudaSuccess) {
+        cudaGetLastError();
+        return h->err.error(da_status_internal_error, "cudaStreamCreateWithPriority failed.");
+    }
+    // the work in flight on the old stream completes first
+    cudaStreamSynchronize(h->cuda.own_stream);
+    const bool bound_own = h->cuda.stream == h->cuda.own_stream;
+    cudaStreamDestroy(h->cuda.own_stream);
+    h->cuda.own_stream = ns;
+    if (bound_own) h->cuda.stream = ns;
+    return da_status_success;
+}
 da_status da_b200_set_kernel_timing(da_handle h, da_int enable) {
     if (!h) return da_status_handle_not_initialized;
     if (!enable) h->cuda.flush_timing();
@@ -682,6 +704,17 @@ da_status da_b200_reset_kernel_time(da_handle h) {
     if (!h) return da_status_handle_not_initialized;
     h->cuda.flush_timing();
     h->cuda.ktime.clear();
+    return da_status_success;
+}
+da_status da_b200_device_memory(unsigned long long *free_bytes, unsigned long long *total_bytes) {
+    if (!free_bytes || !total_bytes) return da_status_invalid_pointer;
+    size_t f = 0, t = 0;
+    if (cudaMemGetInfo(&f, &t) != cudaSuccess) {
+        cudaGetLastError();
+        return da_status_arch_not_supported;
+    }
+    *free_bytes = f;
+    *total_bytes = t;
     return da_status_success;
 }
 da_status da_b200_nn_share_data(da_handle h, da_handle source) {

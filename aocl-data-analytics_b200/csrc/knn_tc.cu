@@ -980,7 +980,10 @@ cudaError_t launch_knn_tc(const float *X, const void *Xh, const void *Xl, const 
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = std::min(nsm, a.n_items);
+    // one block per work item (64 train tiles): blocks end often, so the
+    // kernels of a higher-priority stream get SMs within one item's time
+    (void)nsm;
+    const int grid = a.n_items;
     kern<<<grid, TK_THREADS, smem, s>>>(mah, mal, mbh, mbl, a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;

@@ -14,7 +14,11 @@ device-memory budget and its query cap -- requests waiting longer than
 `aging_ms` first, then small ones (at most `small_queries` queries), then
 the rest, oldest first within each class -- (continuous batching: requests
 that arrive while a batch runs join the next one) and serves them with ONE
-library call: for kNN the
+library call.  With `fast_lane` (two kNN workers or more) the first kNN
+worker takes only small requests, on a high-priority stream, so that a
+small request never waits behind a large batch; the others take large
+requests first and small ones when nothing else is pending or when a small
+one has waited `overflow_ms` (the fast lane is behind).  For kNN the for kNN the
 queries are concatenated and searched with the largest k asked for; every
 request gets the prefix it asked for, which is exactly its own search because
 results are ordered by (distance, index).  Several kNN workers run their
@@ -33,6 +37,7 @@ that fails completes every request of its batch with `error` set (the
 workers keep serving).
 """
 import collections
+import gc
 import threading
 import time
 
@@ -84,25 +89,23 @@ class Server:
     def __init__(self, ab, X, models=None, workers=2, max_batch_queries=1024,
                  max_request_queries=4096, hbm_budget=16 << 30, precision_mode="bf16x3",
                  small_queries=256, aging_ms=20.0, ann=None, free_memory="auto",
-                 hbm_reserve=1 << 30):
+                 hbm_reserve=1 << 30, fast_lane=True, overflow_ms=2.0):
         self.ab = ab
         # admission: a batch's device bytes stay within the worker's share of
-        # hbm_budget AND of the device memory free at the moment it is formed
-        # (less hbm_reserve); free_memory() -> bytes, None to use the budget only
+        # hbm_budget AND of the device memory free (less hbm_reserve), read
+        # every free_every seconds by a monitor thread (the reading is a
+        # driver call that can wait behind other device work: no worker ever
+        # makes it); free_memory() -> bytes, None to use the budget only
         if free_memory == "auto":
-            free_memory = None
-            try:
-                import torch
-                if torch.cuda.is_available():
-                    free_memory = lambda: torch.cuda.mem_get_info()[0]  # noqa: E731
-            except Exception:
-                free_memory = None
+            dm = getattr(ab, "device_memory", None)
+            free_memory = (lambda: dm()[0]) if dm is not None else None  # noqa: E731
         self.free_memory = free_memory
         self.hbm_reserve = hbm_reserve
-        self.free_every = 0.05  # seconds between free-memory readings (a driver call)
-        self._free_at = -1.0
+        self.free_every = 0.05
         self._free_val = None
         self.small_queries = small_queries
+        self.fast_lane = bool(fast_lane) and workers >= 2
+        self.overflow = overflow_ms / 1e3
         self.aging = aging_ms / 1e3
         self.X = np.ascontiguousarray(X, dtype=np.float32)
         self.d = self.X.shape[1]
@@ -113,12 +116,18 @@ class Server:
                         "predict": collections.deque()}
         self.stopping = False
         self.completed = []
-        self.batches = []          # (kind, requests, queries, seconds) of every library call
+        # every library call: (kind, requests, queries, seconds, largest
+        # request, worker thread id)
+        self.batches = []
         self.fallback_queries = 0  # kNN queries the tensor-core pass handed to the plain path
         self.knn_handles = []
         for w in range(workers):
             h = ab.KNN("s", order=ab.ROW_MAJOR, metric="euclidean",
                        precision_mode=precision_mode)
+            if self.fast_lane and w == 0:
+                # the fast lane's kernels overtake the other workers' as SMs
+                # free up
+                h.set_stream_priority(-100)
             if w == 0:
                 h.fit(self.X)
             else:
@@ -155,8 +164,15 @@ class Server:
             for nq in (1, min(max_request_queries, 512), max_batch_queries):
                 self.ann.kneighbors(self.X[np.arange(nq) % self.X.shape[0]], 256)
         self.bytes_per_query = self.d * 4 + KNN_LIST_BYTES + KNN_OUT_BYTES
+        # the start-up objects (index, models, handles) leave the collector's
+        # view: a full collection then never walks them while requests wait
+        gc.collect()
+        gc.freeze()
         self.threads = [threading.Thread(target=self._knn_worker, args=(w,), daemon=True)
                         for w in range(workers)]
+        if self.free_memory is not None:
+            self.refresh_free_memory()
+            self.threads.append(threading.Thread(target=self._monitor, daemon=True))
         self.threads.append(threading.Thread(target=self._predict_worker, daemon=True))
         if self.ann is not None:
             self.threads.append(threading.Thread(target=self._ann_worker, daemon=True))
@@ -202,21 +218,32 @@ class Server:
             self.ann.close()
 
     # ------------------------------------------------------------ workers --
-    def _take(self, kind, cap_queries, cap_bytes, per_query_bytes, same_model=False):
+    def _take(self, kind, cap_queries, cap_bytes, per_query_bytes, same_model=False,
+              small_only=False, large_first=False):
         """Oldest pending requests of `kind` within the caps (at least one);
-        blocks until one is pending, None once the server stops."""
+        blocks until one is pending, None once the server stops.  small_only:
+        requests of at most small_queries queries only.  large_first (the
+        other workers beside a fast lane): large requests before small ones,
+        unless a small one has waited overflow_ms (the fast lane is behind)."""
+        def fits(r):
+            return not small_only or r.queries.shape[0] <= self.small_queries
+
         with self.cv:
-            while not self.pending[kind] and not self.stopping:
+            while not any(map(fits, self.pending[kind])) and not self.stopping:
                 self.cv.wait()
             q = self.pending[kind]
-            if not q:
+            if not any(map(fits, q)):
                 return None
             now = time.perf_counter()
             # aged requests, then small ones, then the rest (oldest first in each)
             def rank(r):
-                aged = now - r.t_submit >= self.aging
-                return (not aged, r.queries.shape[0] > self.small_queries, r.t_submit)
-            order = sorted(q, key=rank)
+                wait = now - r.t_submit
+                small = r.queries.shape[0] <= self.small_queries
+                if large_first:
+                    return (not (wait >= self.aging or (small and wait >= self.overflow)),
+                            small, r.t_submit)
+                return (wait < self.aging, not small, r.t_submit)
+            order = sorted(filter(fits, q), key=rank)
             model = order[0].model
             batch, nq = [], 0
             for r in order:
@@ -232,19 +259,26 @@ class Server:
             self.pending[kind] = collections.deque(r for r in q if id(r) not in taken)
             return batch
 
+    def refresh_free_memory(self):
+        """Read the free device memory now (the monitor thread does this
+        every free_every seconds)."""
+        try:
+            self._free_val = int(self.free_memory())
+        except Exception:
+            self._free_val = None
+
+    def _monitor(self):
+        while not self.stopping:
+            time.sleep(max(self.free_every, 0.001))
+            self.refresh_free_memory()
+
     def _cap_bytes(self, share):
         """The device bytes a batch may use now: the worker's share of the
-        budget, and of the free device memory less the reserve."""
-        if self.free_memory is None:
+        budget, and of the free device memory last read, less the reserve."""
+        free = self._free_val
+        if self.free_memory is None or free is None:
             return share
-        now = time.perf_counter()
-        if self._free_val is None or now - self._free_at >= self.free_every:
-            try:
-                self._free_val = int(self.free_memory())
-            except Exception:
-                return share
-            self._free_at = now
-        free = self._free_val - self.hbm_reserve
+        free -= self.hbm_reserve
         return max(0, min(share, free // max(1, len(self.knn_handles))))
 
     def _fail(self, kind, batch, exc):
@@ -270,7 +304,8 @@ class Server:
                     p.t_done = t
                     done.append(p)
             self.completed.extend(done)
-            self.batches.append((kind, len(batch), nq, secs))
+            self.batches.append((kind, len(batch), nq, secs,
+                                 max(r.queries.shape[0] for r in batch), threading.get_ident()))
         for r in done:
             r._done.set()
 
@@ -279,7 +314,8 @@ class Server:
         share = self.hbm_budget // len(self.knn_handles)
         while True:
             batch = self._take("knn", self.max_batch_queries, self._cap_bytes(share),
-                               self.bytes_per_query)
+                               self.bytes_per_query, small_only=self.fast_lane and w == 0,
+                               large_first=self.fast_lane and w > 0)
             if batch is None:
                 return
             try:

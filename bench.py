@@ -1034,8 +1034,9 @@ def run_serving(ab, nx=8_000_000, d=96, comps=2048, n_models=64,
     mixture).  A seeded trace of Poisson arrivals at 2,000 requests/s for 2 s:
     per-request query count lognormal(ln 16, 1.5) clipped to [1, 4096],
     k uniform in {1, 10, 100}, one request in five a predict on a random
-    model.  Served by the continuous-batching loop (two kNN workers, at most
-    512 queries per library call, larger requests split into parts, small and
+    model.  Served by the continuous-batching loop (two kNN workers, the
+    first a fast lane for requests of at most 256 queries, at most 512 queries
+    per library call, larger requests split into parts, small and
     long-waiting requests first), after 0.5 s of unmeasured traffic at the
     same rate; p50 / p99 latency (submit to completion)
     and queries/s at 250, 1,000, 2,000, 10,000 and 50,000 requests/s for the
@@ -1105,6 +1106,8 @@ def run_serving(ab, nx=8_000_000, d=96, comps=2048, n_models=64,
                 "queries_per_s": nq / wall, "knn_calls": len(kb),
                 "mean_queries_per_knn_call": float(np.mean([b[2] for b in kb])) if kb else 0.0,
                 "mean_knn_call_ms": float(np.mean([b[3] for b in kb]) * 1e3) if kb else 0.0,
+                "p99_knn_call_ms": float(np.percentile([b[3] for b in kb], 99) * 1e3) if kb else 0.0,
+                "max_knn_call_ms": float(max(b[3] for b in kb) * 1e3) if kb else 0.0,
                 "plain_fallback_queries": server.fallback_queries}
         server.close()
     return out

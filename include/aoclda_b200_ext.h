@@ -19,6 +19,13 @@ extern "C" {
  * return only after their results are complete. */
 da_status da_b200_set_stream(da_handle handle, void *stream);
 
+/* Recreate the handle's own stream with a CUDA stream priority: 0 is the
+ * default, negative values are higher priorities (clamped to the device's
+ * range).  Blocks of a higher-priority stream's kernels are scheduled first
+ * as SMs free up, so that a latency-critical handle's work overtakes a busy
+ * one's.  Work in flight on the old stream completes first. */
+da_status da_b200_set_stream_priority(da_handle handle, da_int priority);
+
 /* Kernel timing: when enabled, every launch of the named hot kernels is
  * bracketed by CUDA events on the handle's stream and accumulated.  Intended
  * for measurement (it serialises launches); off by default. */
@@ -28,6 +35,11 @@ da_status da_b200_set_kernel_timing(da_handle handle, da_int enable);
 da_status da_b200_get_kernel_time(da_handle handle, const char *kernel, double *total_ms,
                                   da_int *launches);
 da_status da_b200_reset_kernel_time(da_handle handle);
+
+/* Free and total device memory, in bytes, of the current device
+ * (da_status_arch_not_supported without one).  For admission control by
+ * callers that keep several handles busy at once. */
+da_status da_b200_device_memory(unsigned long long *free_bytes, unsigned long long *total_bytes);
 
 /* kNN: give `handle` the training data (and labels / targets) already set on
  * `source` -- same precision, storage order and device -- without a second

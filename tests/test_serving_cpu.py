@@ -24,6 +24,9 @@ class FakeKNN:
         self.X = source.X
         return self
 
+    def set_stream_priority(self, priority):
+        return self
+
     def kneighbors(self, Q, k):
         self.calls.append(Q.shape[0])
         d2 = ((np.asarray(Q, dtype=np.float64)[:, None, :] - self.X[None]) ** 2).sum(-1)
@@ -239,12 +242,12 @@ def test_serving_admission_follows_free_memory():
     server = sv.Server(AB(), X, workers=1, max_batch_queries=64, max_request_queries=64,
                        free_memory=lambda: free["bytes"], hbm_reserve=0)
     armed["on"] = True
-    server.free_every = 0.0  # read the free memory for every batch
     try:
         per_query = server.bytes_per_query
         first = server.submit(sv.Request("knn", rng.standard_normal((1, 4)), k=1))
         time.sleep(0.2)  # the worker holds the first batch
         free["bytes"] = 3 * per_query  # room for three queries per batch
+        server.refresh_free_memory()
         later = [server.submit(sv.Request("knn", rng.standard_normal((1, 4)), k=1))
                  for _ in range(7)]
         gate.set()
@@ -254,4 +257,31 @@ def test_serving_admission_follows_free_memory():
         assert max(sizes) <= 3 and sum(sizes) == 7
     finally:
         gate.set()
+        server.close()
+
+
+def test_serving_fast_lane():
+    """With two kNN workers the first serves only small requests (its batches
+    never hold a request of more than small_queries queries); every result is
+    still the request's own search."""
+    sv = _load("aoclda_serving_fast", os.path.join(PKG, "serving.py"))
+    rng = np.random.default_rng(8)
+    X = rng.standard_normal((300, 4)).astype(np.float32)
+    server = sv.Server(FakeAB(), X, workers=2, max_batch_queries=16, max_request_queries=64,
+                       small_queries=4)
+    try:
+        reqs = [server.submit(sv.Request("knn", rng.standard_normal((int(m), 4)), k=3))
+                for m in rng.choice([1, 2, 4, 9, 16, 40], 120)]
+        for r in reqs:
+            assert r.wait(30)
+        ref = FakeKNN("s").fit(X)
+        for r in reqs:
+            ind, dist = ref.kneighbors(r.queries, 3)
+            np.testing.assert_array_equal(r.result[0], ind)
+        fast = server.threads[0].ident
+        mine = [b for b in server.batches if b[0] == "knn" and b[5] == fast]
+        assert mine, "the fast lane served nothing"
+        assert all(b[4] <= 4 for b in mine)
+        assert any(b[4] > 4 for b in server.batches if b[0] == "knn")
+    finally:
         server.close()
