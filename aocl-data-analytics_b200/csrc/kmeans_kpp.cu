@@ -340,6 +340,24 @@ template <typename T> struct Binade {
         if ((ti & 1ull) && tt == __ull2double_rn(ti)) return SC_SAT;
         return (ti + 1ull) >> 1;
     }
+    // q for a term staying inside the binade by itself: RN_g(m) for a
+    // non-tie; for a tie (m / g = k + 1/2) k, with *tie set (its rounding
+    // depends on the running sum's parity); SC_SAT for a term that leaves
+    // the binade by itself
+    __device__ __forceinline__ unsigned long long qt(T m, bool &tie) const {
+        const int e2 = sh + 1, ea = min(e2, 1000), eb = e2 - ea;
+        const double sa = __longlong_as_double((long long)(ea + 1023) << 52);
+        const double sb = __longlong_as_double((long long)(eb + 1023) << 52);
+        const double tt = ((double)m * sa) * sb;
+        tie = false;
+        if (!(tt < 2.0 * (double)limit)) return SC_SAT;
+        const unsigned long long ti = __double2ull_rz(tt);
+        if ((ti & 1ull) && tt == __ull2double_rn(ti)) {
+            tie = true;
+            return ti >> 1;
+        }
+        return (ti + 1ull) >> 1;
+    }
     // m stays inside the binade by itself (so SC_SAT from q() means a tie)
     __device__ __forceinline__ bool q_in_range(T m) const {
         const int e2 = sh + 1, ea = min(e2, 1000), eb = e2 - ea;
@@ -352,42 +370,71 @@ template <typename T> struct Binade {
     }
 };
 
-// Saturating prefix sums of one value per thread over a block of NT
-// threads: returns the inclusive prefix, `excl` the exclusive one (exact
-// while below 2^62), `total` the block's sum.  shm: 2 * (NT / 32) + 1 words.
+// A run of additions on one grid as a function of the running sum's parity
+// (its last bit in grid units) at the run's start: q0 / q1 the run's total
+// for start parity 0 / 1, o bit p the parity at its end for start parity p.
+// A non-tie term q: (q, q, parity flips with q's last bit).  A tie term
+// m / g = k + 1/2 rounds to the even neighbour: k + ((R + k) & 1) for a
+// running sum R, after which the sum is even.  Runs compose associatively,
+// so a scan over them gives the running sum before every term.
+struct Pf {
+    unsigned long long q0, q1;
+    int o;
+};
+__device__ __forceinline__ Pf pf_id() { return Pf{0ull, 0ull, 2}; }
+__device__ __forceinline__ Pf pf_term(unsigned long long q, bool tie) {
+    if (!tie) {
+        const int b = (int)(q & 1ull);
+        return Pf{q, q, b | ((1 ^ b) << 1)};
+    }
+    return Pf{q + (q & 1ull), q + ((q + 1ull) & 1ull), 0};
+}
+__device__ __forceinline__ unsigned long long pf_q(const Pf &f, int p) { return p ? f.q1 : f.q0; }
+__device__ __forceinline__ int pf_o(const Pf &f, int p) { return (f.o >> p) & 1; }
+// a, then b
+__device__ __forceinline__ Pf pf_cat(const Pf &a, const Pf &b) {
+    const int a0 = a.o & 1, a1 = (a.o >> 1) & 1;
+    return Pf{sat_add(a.q0, pf_q(b, a0)), sat_add(a.q1, pf_q(b, a1)),
+              pf_o(b, a0) | (pf_o(b, a1) << 1)};
+}
+__device__ __forceinline__ Pf pf_shfl_up(const Pf &v, int off) {
+    return Pf{__shfl_up_sync(0xffffffffu, v.q0, off), __shfl_up_sync(0xffffffffu, v.q1, off),
+              __shfl_up_sync(0xffffffffu, v.o, off)};
+}
+
+// Scan of one run per thread over a block of NT threads in thread order:
+// the composition of the runs before this thread's (`excl`) and of all
+// (`total`).  shm: 2 * (NT / 32) + 1 entries.
 template <int NT>
-__device__ unsigned long long block_scan_sat(unsigned long long v, unsigned long long *shm,
-                                             unsigned long long &excl,
-                                             unsigned long long &total) {
+__device__ void block_scan_pf(const Pf &v, Pf *shm, Pf &excl, Pf &total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = NT / 32;
-    unsigned long long x = v;
+    Pf x = v;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, off);
-        if (lane >= off) x = sat_add(x, y);
+        const Pf y = pf_shfl_up(x, off);
+        if (lane >= off) x = pf_cat(y, x);
     }
-    unsigned long long xe = __shfl_up_sync(0xffffffffu, x, 1);
-    if (lane == 0) xe = 0;
+    Pf xe = pf_shfl_up(x, 1);
+    if (lane == 0) xe = pf_id();
     __syncthreads();
     if (lane == 31) shm[warp] = x;
     __syncthreads();
     if (warp == 0) {
-        unsigned long long y = lane < NW ? shm[lane] : 0ull;
+        Pf y = lane < NW ? shm[lane] : pf_id();
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
-            const unsigned long long z = __shfl_up_sync(0xffffffffu, y, off);
-            if (lane >= off) y = sat_add(y, z);
+            const Pf z = pf_shfl_up(y, off);
+            if (lane >= off) y = pf_cat(z, y);
         }
-        unsigned long long ye = __shfl_up_sync(0xffffffffu, y, 1);
-        if (lane == 0) ye = 0;
+        Pf ye = pf_shfl_up(y, 1);
+        if (lane == 0) ye = pf_id();
         if (lane < NW) shm[NW + lane] = ye;
         if (lane == NW - 1) shm[2 * NW] = y;
     }
     __syncthreads();
     total = shm[2 * NW];
-    excl = sat_add(shm[NW + warp], xe);
-    return sat_add(shm[NW + warp], x);
+    excl = pf_cat(shm[NW + warp], xe);
 }
 
 // Distances of a 256-row chunk to the candidates (one thread per row), with
@@ -535,12 +582,12 @@ __global__ void __launch_bounds__(1024) kpp_chunk_prefix_kernel(const double *cs
 
 // Chunk records of candidate blockIdx.y, one warp per chunk: the binade the
 // fp64 prefix predicts for the serial sum at the chunk (raw exponent of
-// (T)P_j, or NO_BINADE when P_j is 0 or not finite, or when a term ties) and
-// the chunk's integer total on that binade's grid (saturating).
+// (T)P_j, or NO_BINADE when P_j is 0 or not finite) and the chunk's run on
+// that binade's grid as a parity function (saturating totals).
 template <typename T>
 __global__ void __launch_bounds__(256)
 kpp_chunk_q_kernel(const T *w, const T *D, int n, int nchunks, const double *P,
-                   unsigned long long *Qr, int *Er) {
+                   unsigned long long *Q0, unsigned long long *Q1, int *Or, int *Er) {
     const int t = blockIdx.y;
     const int j = blockIdx.x * 8 + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
@@ -550,7 +597,8 @@ kpp_chunk_q_kernel(const T *w, const T *D, int n, int nchunks, const double *P,
     const T Ts = (T)Pj;
     if (!(Pj > 0.0) || !isfinite(Ts) || Ts == T(0)) {
         if (lane == 0) {
-            Qr[r] = 0;
+            Q0[r] = Q1[r] = 0;
+            Or[r] = 2;
             Er[r] = NO_BINADE;
         }
         return;
@@ -558,40 +606,44 @@ kpp_chunk_q_kernel(const T *w, const T *D, int n, int nchunks, const double *P,
     Binade<T> b;
     b.set(Ts);
     const T *Dt = D + (size_t)t * n;
-    unsigned long long a = 0;
-    int tie = 0;
+    // each lane composes 8 consecutive terms, then the lanes' runs in lane
+    // order (a tree over neighbouring blocks of lanes)
+    Pf acc = pf_id();
 #pragma unroll
     for (int u = 0; u < CK / 32; ++u) {
-        const int i = j * CK + u * 32 + lane;
+        const int i = j * CK + lane * (CK / 32) + u;
         if (i < n) {
-            const T m = kpp_term(w[i], Dt[i]);
-            const unsigned long long q = b.q(m);
-            // a tie, unlike a term that leaves the binade, needs the exact path
-            if (q == SC_SAT && b.q_in_range(m)) tie = 1;
-            a = sat_add(a, q);
+            bool tie;
+            const unsigned long long q = b.qt(kpp_term(w[i], Dt[i]), tie);
+            acc = pf_cat(acc, pf_term(q, tie));
         }
     }
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) a = sat_add(a, __shfl_xor_sync(0xffffffffu, a, off));
-    tie = __any_sync(0xffffffffu, tie);
+    for (int off = 1; off < 32; off <<= 1) {
+        const Pf y = Pf{__shfl_down_sync(0xffffffffu, acc.q0, off),
+                        __shfl_down_sync(0xffffffffu, acc.q1, off),
+                        __shfl_down_sync(0xffffffffu, acc.o, off)};
+        if ((lane & (2 * off - 1)) == 0) acc = pf_cat(acc, y);
+    }
     if (lane == 0) {
-        Qr[r] = a;
-        Er[r] = tie ? NO_BINADE : b.ex;
+        Q0[r] = acc.q0;
+        Q1[r] = acc.q1;
+        Or[r] = acc.o;
+        Er[r] = b.ex;
     }
 }
 
 // The serial sum of candidate blockIdx.x over the chunk records (see above).
 template <typename T>
 __global__ void __launch_bounds__(WALK_THREADS)
-kpp_walk_kernel(const T *w, const T *D, int n, int nchunks, const unsigned long long *Qr,
-                const int *Er, double *cost) {
-    __shared__ unsigned long long shm[2 * (WALK_THREADS / 32) + 1];
+kpp_walk_kernel(const T *w, const T *D, int n, int nchunks, const unsigned long long *Q0,
+                const unsigned long long *Q1, const int *Or, const int *Er, double *cost) {
+    __shared__ Pf shm[2 * (WALK_THREADS / 32) + 1];
     __shared__ int s_f;
     __shared__ T s_val;
     const int t = blockIdx.x;
     const T *Dt = D + (size_t)t * n;
-    const unsigned long long *Qt = Qr + (size_t)t * nchunks;
-    const int *Et = Er + (size_t)t * nchunks;
+    const size_t ro = (size_t)t * nchunks;
     T s = T(0);
     int j = 0;
     while (j < nchunks && isfinite(s)) {
@@ -601,31 +653,34 @@ kpp_walk_kernel(const T *w, const T *D, int n, int nchunks, const unsigned long 
         b.limit = 0;
         b.s_int = 0;
         if (s != T(0)) b.set(s);
+        const int p0 = (int)(b.s_int & 1ull);
         // WALK_PER consecutive records per thread
         const int r0 = j + (int)threadIdx.x * WALK_PER;
-        unsigned long long qv[WALK_PER];
+        Pf rv[WALK_PER];
         bool okv[WALK_PER];
-        unsigned long long tq = 0;
+        Pf loc = pf_id();
 #pragma unroll
         for (int u = 0; u < WALK_PER; ++u) {
             const int r = r0 + u;
             const bool valid = r < nchunks;
-            qv[u] = valid ? Qt[r] : 0ull;
-            okv[u] = !valid || Et[r] == b.ex;
-            tq = sat_add(tq, qv[u]);
+            rv[u] = valid ? Pf{Q0[ro + r], Q1[ro + r], Or[ro + r]} : pf_id();
+            okv[u] = !valid || Er[ro + r] == b.ex;
+            loc = pf_cat(loc, rv[u]);
         }
-        unsigned long long total, excl;
-        block_scan_sat<WALK_THREADS>(tq, shm, excl, total);
+        Pf excl, total;
+        block_scan_pf<WALK_THREADS>(loc, shm, excl, total);
         int mine = 0x7fffffff;
-        unsigned long long ex_at = 0, run = excl;
+        unsigned long long R = b.s_int + pf_q(excl, p0), R_at = 0; // running sum, grid units
+        int par = pf_o(excl, p0);
 #pragma unroll
         for (int u = 0; u < WALK_PER; ++u) {
-            const unsigned long long nxt = sat_add(run, qv[u]);
-            if (mine == 0x7fffffff && r0 + u < nchunks && (!okv[u] || b.s_int + nxt >= b.limit)) {
+            const unsigned long long q = pf_q(rv[u], par);
+            if (mine == 0x7fffffff && r0 + u < nchunks && (!okv[u] || R + q >= b.limit)) {
                 mine = (int)threadIdx.x * WALK_PER + u;
-                ex_at = run;
+                R_at = R;
             }
-            run = nxt;
+            R = sat_add(R, q);
+            par = pf_o(rv[u], par);
         }
         if (threadIdx.x == 0) s_f = 0x7fffffff;
         __syncthreads();
@@ -633,62 +688,68 @@ kpp_walk_kernel(const T *w, const T *D, int n, int nchunks, const unsigned long 
         __syncthreads();
         const int f = s_f;
         if (f == 0x7fffffff) {
-            s = b.value(b.s_int + total);
+            s = b.value(b.s_int + pf_q(total, p0));
             j += WALK_THREADS * WALK_PER;
             continue;
         }
         // the records before f on the grid
-        if (mine == f) s_val = (f == 0) ? s : b.value(b.s_int + ex_at);
+        if (mine == f) s_val = (f == 0) ? s : b.value(R_at);
         __syncthreads();
         s = s_val;
         __syncthreads();
-        // chunk j + f, term by term
+        // chunk j + f, term by term: ties by their parity rule, a serial
+        // step only where the sum leaves the binade (or a term does by itself)
         const int c = j + f;
         int pos = c * CK;
         const int end = min(n, pos + CK);
+        const int i = pos + (int)threadIdx.x;
+        const T mi = ((int)threadIdx.x < CK && i < end) ? kpp_term(w[i], Dt[i]) : T(0);
         while (pos < end && isfinite(s)) {
-            const int i = pos + (int)threadIdx.x;
-            const bool in = (int)threadIdx.x < CK && i < end;
-            const T m = in ? kpp_term(w[i], Dt[i]) : T(0);
+            const bool in = (int)threadIdx.x < CK && i >= pos && i < end;
+            const T m = in ? mi : T(0);
             if (s == T(0)) {
                 // 0 + m = m exactly: the first nonzero term starts the sum
                 if (threadIdx.x == 0) s_f = 0x7fffffff;
                 __syncthreads();
-                if (in && m != T(0)) atomicMin(&s_f, (int)threadIdx.x);
+                if (in && m != T(0)) atomicMin(&s_f, i);
                 __syncthreads();
                 const int p = s_f;
                 if (p == 0x7fffffff) {
                     pos = end;
                     break;
                 }
-                if ((int)threadIdx.x == p) s_val = m;
+                if (i == p) s_val = m;
                 __syncthreads();
                 s = s_val;
-                pos += p + 1;
+                pos = p + 1;
                 __syncthreads();
                 continue;
             }
             Binade<T> bb;
             bb.set(s);
-            const unsigned long long qe = in ? bb.q(m) : 0ull;
-            unsigned long long tot, exc;
-            const unsigned long long inc = block_scan_sat<WALK_THREADS>(qe, shm, exc, tot);
-            const bool bad = in && (qe == SC_SAT || bb.s_int + inc >= bb.limit);
+            const int pp = (int)(bb.s_int & 1ull);
+            bool tie = false;
+            const unsigned long long qv = in ? bb.qt(m, tie) : 0ull;
+            const Pf e = in ? pf_term(qv, tie) : pf_id();
+            Pf ex, tot;
+            block_scan_pf<WALK_THREADS>(e, shm, ex, tot);
+            const unsigned long long Rb = bb.s_int + pf_q(ex, pp);
+            const bool bad = in && (qv == SC_SAT || Rb + pf_q(e, pf_o(ex, pp)) >= bb.limit);
             if (threadIdx.x == 0) s_f = 0x7fffffff;
             __syncthreads();
-            if (bad) atomicMin(&s_f, (int)threadIdx.x);
+            if (bad) atomicMin(&s_f, i);
             __syncthreads();
             const int p = s_f;
             if (p == 0x7fffffff) {
-                s = bb.value(bb.s_int + tot);
+                s = bb.value(bb.s_int + pf_q(tot, pp));
                 pos = end;
                 break;
             }
             // the terms before p on the grid, then term p serially in T
-            if ((int)threadIdx.x == p) s_val = add_rn(bb.value(bb.s_int + exc), m);
+            if (i == p) s_val = add_rn(bb.value(Rb), m);
             __syncthreads();
             s = s_val;
-            pos += p + 1;
+            pos = p + 1;
             __syncthreads();
         }
         j = c + 1;
@@ -706,8 +767,10 @@ cudaError_t launch_kpp_dist_cost(const T *X, int ldx, int n, int d, const T *xno
     const int nch = kpp_num_chunks(n);
     double *csum = static_cast<double *>(work);
     double *P = csum + (size_t)t * nch;
-    unsigned long long *Qr = reinterpret_cast<unsigned long long *>(P + (size_t)t * nch);
-    int *Er = reinterpret_cast<int *>(Qr + (size_t)t * nch);
+    unsigned long long *Q0 = reinterpret_cast<unsigned long long *>(P + (size_t)t * nch);
+    unsigned long long *Q1 = Q0 + (size_t)t * nch;
+    int *Or = reinterpret_cast<int *>(Q1 + (size_t)t * nch);
+    int *Er = Or + (size_t)t * nch;
     // candidates' rows padded to 16 bytes, in shared memory when they fit
     const int W = 16 / (int)sizeof(T);
     const size_t want = (size_t)t * ((d + W - 1) / W * W) * sizeof(T);
@@ -722,13 +785,14 @@ cudaError_t launch_kpp_dist_cost(const T *X, int ldx, int n, int d, const T *xno
                                                           nch);
     }
     kpp_chunk_prefix_kernel<<<t, 1024, 0, s>>>(csum, nch, P);
-    kpp_chunk_q_kernel<T><<<dim3((nch + 7) / 8, t), 256, 0, s>>>(w, D, n, nch, P, Qr, Er);
-    kpp_walk_kernel<T><<<t, WALK_THREADS, 0, s>>>(w, D, n, nch, Qr, Er, cost);
+    kpp_chunk_q_kernel<T><<<dim3((nch + 7) / 8, t), 256, 0, s>>>(w, D, n, nch, P, Q0, Q1, Or,
+                                                                  Er);
+    kpp_walk_kernel<T><<<t, WALK_THREADS, 0, s>>>(w, D, n, nch, Q0, Q1, Or, Er, cost);
     return cudaGetLastError();
 }
 
 size_t kpp_cost_work_bytes(int n, int t) {
-    return (size_t)kpp_num_chunks(n) * t * (8 + 8 + 8 + 4) + 256;
+    return (size_t)kpp_num_chunks(n) * t * (8 + 8 + 8 + 8 + 4 + 4) + 256;
 }
 
 // Choose the candidate (kmeans.cpp:1614-1646): repeats skipped, the first
