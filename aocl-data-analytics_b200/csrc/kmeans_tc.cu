@@ -175,9 +175,9 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
     const uint32_t a_bytes = (uint32_t)TC_BM * 128u;  // one K block of a tile
     unsigned char *Bh = base;
     unsigned char *Bl = Bh + (size_t)nkb * b_bytes;                    // SPLIT == 3
-    unsigned char *Baug = Bl + (SPLIT == 3 ? (size_t)nkb * b_bytes : 0);
-    unsigned char *Aaug = Baug + b_bytes;
-    unsigned char *As = Aaug + a_bytes;                                // S stages
+    unsigned char *Baug = Bl + (SPLIT == 3 ? (size_t)nkb * b_bytes : 0); // npad x 32 B
+    unsigned char *Aaug = Baug + ((size_t)a.npad * 32 + 1023) / 1024 * 1024; // 128 x 32 B
+    unsigned char *As = Aaug + ((size_t)TC_BM * 32 + 1023) / 1024 * 1024;  // S stages
     TcShared *sh = reinterpret_cast<TcShared *>(As + (size_t)S * NX * nkb * a_bytes);
     int *cand_s = reinterpret_cast<int *>(sh + 1); // [TC_THREADS][TC_MAXC]
     float *xb1 = reinterpret_cast<float *>(cand_s + TC_THREADS * TC_MAXC); // pair exchange
@@ -216,7 +216,8 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
         if (lane == 0) {
             prefetch_tmap(&tmXh);
             prefetch_tmap(&tmBh);
-            mbar_arrive_expect_tx(&sh->bfull, (uint32_t)(NX * nkb + 1) * b_bytes + a_bytes);
+            mbar_arrive_expect_tx(&sh->bfull, (uint32_t)(NX * nkb) * b_bytes +
+                                                  (uint32_t)a.npad * 32u + (uint32_t)TC_BM * 32u);
             for (int kb = 0; kb < nkb; ++kb) {
                 tma_load_2d(&tmBh, &sh->bfull, Bh + (size_t)kb * b_bytes, kb * TC_KB, 0);
                 if (SPLIT == 3)
@@ -288,7 +289,7 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
                     }
                 }
                 // + |c_j|^2 (hi + lo) through the constant ones operand
-                mma_f16_ss(tacc, desc_k_sw128(aaug), desc_k_sw128(baug), idesc, 1);
+                mma_f16_ss(tacc, desc_k_sw32(aaug), desc_k_sw32(baug), idesc, 1);
                 mma_commit(&sh->empty[s]);
                 mma_commit(&sh->tfull[b]);
             }
@@ -776,22 +777,31 @@ static EncodeTiledFn get_encode() {
 
 // 2-D bf16 tensor map over a row-major [rows x cols] matrix, box {64, box_rows},
 // 128-byte swizzle, zero fill out of bounds.
-static bool make_map_bf16(CUtensorMap *m, const void *ptr, int rows, int cols, int box_rows) {
+// narrow: only the first 16 columns (32 bytes per row, 32-byte swizzle) --
+// the |c|^2 operands of the K = 16 MMA
+static bool make_map_bf16(CUtensorMap *m, const void *ptr, int rows, int cols, int box_rows,
+                          bool narrow = false) {
     EncodeTiledFn enc = get_encode();
     if (!enc || !ptr) return false;
-    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t dims[2] = {(cuuint64_t)(narrow ? 16 : cols), (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-    cuuint32_t box[2] = {(cuuint32_t)TC_KB, (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)(narrow ? 16 : TC_KB), (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box,
-               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+               estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               narrow ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_128B,
                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
            CUDA_SUCCESS;
 }
 
+// shared memory: B (hi, lo) K blocks, the narrow |c|^2 operands (rounded up to
+// 1 KB each), the stages, the barriers and the epilogue's exchange arrays
+static size_t tc_aug_bytes(int npad) {
+    return ((size_t)npad * 32 + 1023) / 1024 * 1024 + ((size_t)TC_BM * 32 + 1023) / 1024 * 1024;
+}
 static size_t tc_smem_bytes(int split, int nkb, int npad, int stages) {
     const int nx = split == 3 ? 2 : 1;
-    return 1024 + (size_t)(nx * nkb + 1) * npad * 128 + (size_t)TC_BM * 128 +
+    return 1024 + (size_t)nx * nkb * npad * 128 + tc_aug_bytes(npad) +
            (size_t)stages * nx * nkb * TC_BM * 128 + sizeof(TcShared) +
            (size_t)TC_THREADS * (TC_MAXC + 4) * 4 + 64;
 }
@@ -880,8 +890,8 @@ cudaError_t launch_kmeans_assign_tc(int split, const void *Xh, const void *Xl, i
         mc.ok = false;
         if (!make_map_bf16(&mc.m[0], Xh, n, ldbf, TC_BM) ||
             !make_map_bf16(&mc.m[2], Bh, npad, ldbf, npad) ||
-            !make_map_bf16(&mc.m[4], Baug, npad, TC_KB, npad) ||
-            !make_map_bf16(&mc.m[5], Aaug, TC_BM, TC_KB, TC_BM))
+            !make_map_bf16(&mc.m[4], Baug, npad, TC_KB, npad, true) ||
+            !make_map_bf16(&mc.m[5], Aaug, TC_BM, TC_KB, TC_BM, true))
             return cudaErrorInvalidValue;
         if (s3) {
             if (!make_map_bf16(&mc.m[1], Xl, n, ldbf, TC_BM) ||

@@ -124,6 +124,17 @@ __device__ __forceinline__ uint64_t desc_k_sw128(uint32_t smem_addr) {
     d |= (uint64_t)2 << 61;           // SWIZZLE_128B
     return d;
 }
+// The same for rows of 32 bytes (16 bf16, one K step) with 32-byte swizzle:
+// 8-row atoms of 256 bytes (SBO = 256 B).
+__device__ __forceinline__ uint64_t desc_k_sw32(uint32_t smem_addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((smem_addr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;          // LBO (16 B units, unused for swizzled K-major)
+    d |= (uint64_t)(256 >> 4) << 32; // SBO
+    d |= (uint64_t)1 << 46;          // descriptor version (sm_100)
+    d |= (uint64_t)6 << 61;          // SWIZZLE_32B
+    return d;
+}
 // Instruction descriptor: kind::f16, A = B = bf16, D = f32, K-major A and B.
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
