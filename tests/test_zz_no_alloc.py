@@ -37,7 +37,10 @@ def test_knn_noalloc_matches_kneighbors(ab, gpu):
     f = _entry(ab)
     dev = torch.device("cuda:0")
     stream = torch.cuda.current_stream(dev).cuda_stream
-    cases = [(5000, 300, 37, 10, 11), (20000, 1000, 64, 200, 12), (5000, 300, 37, 10, 11)]
+    # the last: one query over a million rows with k = 256, where the merge
+    # fan-in cap bounds the number of partial lists
+    cases = [(5000, 300, 37, 10, 11), (20000, 1000, 64, 200, 12), (5000, 300, 37, 10, 11),
+             (1_000_000, 1, 32, 256, 13)]
     for n, nq, d, k, seed in cases:
         rng = np.random.default_rng(seed)
         X = rng.standard_normal((n, d)).astype(np.float32)
