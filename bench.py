@@ -243,6 +243,12 @@ def main():
                     help="run only the serving leg and print its JSON")
     ap.add_argument("--knn-only", action="store_true",
                     help="run only the kNN leg (profiling captures) and print its JSON")
+    ap.add_argument("--kpp-only", action="store_true",
+                    help="run only the k-means++ initialisation of the k-means data (profiling "
+                         "captures) and print its times")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="run only one batched k-means call over the 512 data sets (profiling "
+                         "captures) and print its times")
     ap.add_argument("--knn-rows", type=int, default=4_000_000)
     ap.add_argument("--knn-queries", type=int, default=10_000)
     ap.add_argument("--knn-plain", type=int, default=1,
@@ -287,6 +293,27 @@ def main():
             print(json.dumps(run_knn(ab, nx=args.knn_rows, nq=args.knn_queries,
                                      plain=bool(args.knn_plain),
                                      accuracy=not args.no_accuracy)))
+        return 0
+    if args.kpp_only:
+        if rank == 0:
+            km = ab.KMeans(K, "s", order=ab.ROW_MAJOR, n_init=1, seed=SEED)
+            km.set_data(make_data())
+            ms = []
+            for _ in range(max(1, args.steps)):
+                t0 = time.perf_counter()
+                km.init_centres(K)
+                ms.append((time.perf_counter() - t0) * 1e3)
+            km.close()
+            print(json.dumps({"workload": "kmeans_pp_fp32_1000000x64_k256_seed1",
+                              "init_ms": ms}))
+        return 0
+    if args.batched_only:
+        if rank == 0:
+            Xs, C0s = batched_workload()
+            ab.kmeans_batched(Xs, C0s, max_iter=30, tol=1e-4)
+            up, fit, down = ab.kmeans_batched_timing()
+            print(json.dumps({"workload": "kmeans_batched_fp32_512_instances",
+                              "device_ms": {"upload": up, "fit": fit, "download": down}}))
         return 0
 
     X = make_data()
@@ -1113,14 +1140,11 @@ def run_serving(ab, nx=8_000_000, d=96, comps=2048, n_models=64,
     return out
 
 
-def run_batched(ab, count=512, max_iter=30, tol=1e-4, seed=4):
-    """Batched k-means: 512 independent fp32 data sets, n lognormal(ln 20000,
-    1) clipped to [1000, 200000], d uniform in {16, 32, 64, 128}, k uniform in
-    [8, 64], each a Gaussian mixture with k components (the k-means recipe),
-    initial centres k distinct rows, 30 Lloyd iterations at most (tol 1e-4).
-    One da_b200_kmeans_batched_s call (host arrays in and out) against one
-    da_kmeans_compute_s call per data set (precision mode plain, the
-    semantics the batched path reproduces); results must be identical."""
+def batched_workload(count=512, seed=4):
+    """512 independent fp32 data sets: n lognormal(ln 20000, 1) clipped to
+    [1000, 200000], d uniform in {16, 32, 64, 128}, k uniform in [8, 64],
+    each a Gaussian mixture with k components (the k-means recipe); initial
+    centres k distinct rows."""
     rng = np.random.default_rng(seed)
     Xs, C0s = [], []
     for _ in range(count):
@@ -1134,6 +1158,18 @@ def run_batched(ab, count=512, max_iter=30, tol=1e-4, seed=4):
         X = means[lab] + rng.standard_normal((n, d), dtype=np.float32) * sig[lab, None]
         Xs.append(np.ascontiguousarray(X))
         C0s.append(X[rng.choice(n, k, replace=False)].copy())
+    return Xs, C0s
+
+
+def run_batched(ab, count=512, max_iter=30, tol=1e-4, seed=4):
+    """Batched k-means: 512 independent fp32 data sets, n lognormal(ln 20000,
+    1) clipped to [1000, 200000], d uniform in {16, 32, 64, 128}, k uniform in
+    [8, 64], each a Gaussian mixture with k components (the k-means recipe),
+    initial centres k distinct rows, 30 Lloyd iterations at most (tol 1e-4).
+    One da_b200_kmeans_batched_s call (host arrays in and out) against one
+    da_kmeans_compute_s call per data set (precision mode plain, the
+    semantics the batched path reproduces); results must be identical."""
+    Xs, C0s = batched_workload(count, seed)
     # warm-up: one iteration over every data set (the tile-shape tuner meets
     # every shape here, so the timed call below uses its cached picks)
     ab.kmeans_batched(Xs, C0s, max_iter=1, tol=tol)
