@@ -417,6 +417,9 @@ def main():
     # previous labels and |x|
     traffic_alg = N * ldbf * 2 * terms + N * 4 * 3
     achieved_tflops = flops / (a_avg / 1e3) / 1e12
+    k_pad = (K + 15) // 16 * 16
+    executed = ((N + 127) // 128) * ((3 if terms == 2 else 1) * (ldbf // 16) + 1) * \
+        2.0 * 128 * k_pad * 16
     achieved_gbs = traffic_alg / (a_avg / 1e3) / 1e9
     t_tensor = flops / (bf16 * 1e12)
     t_hbm = traffic_alg / (hbm * 1e9)
@@ -443,6 +446,11 @@ def main():
                  "avg_launch_ms": a_avg, "tensor_tflops": achieved_tflops,
                  "tensor_frac": achieved_tflops / bf16, "hbm_gbs": achieved_gbs,
                  "hbm_frac": achieved_gbs / hbm,
+                 # the MMAs the kernel executes: per 128-row tile, per 16-wide K
+                 # step one product (bf16) or three (bf16x3), plus one K = 16
+                 # MMA adding |c|^2, each 2 x 128 x k_pad x 16 flop
+                 "executed_tensor_tflops": executed / (a_avg / 1e3) / 1e12,
+                 "executed_tensor_frac": executed / (a_avg / 1e3) / 1e12 / bf16,
                  "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in kt.items() if v[1]}})
 
     accuracy = None
