@@ -36,6 +36,8 @@ def run(ab, X, Q, k, metric, mode, order):
     (300_000, 1, 64, 1, "euclidean", 1),
     (1_000_000, 1, 96, 100, "euclidean", 0),     # one query, all blocks on its list
     (600_000, 3, 64, 256, "sqeuclidean", 1),
+    (220_000, 70, 80, 10, "euclidean", 0),       # last K block of 16 columns
+    (200_000, 50, 96, 10, "cosine", 1),          # last K block of 32 columns
     (200_000, 700, 128, 100, "cosine", 0),
     (300_000, 40, 64, 10, "cosine", 1),
 ])
