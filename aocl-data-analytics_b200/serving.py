@@ -14,11 +14,12 @@ device-memory budget and its query cap -- requests waiting longer than
 `aging_ms` first, then small ones (at most `small_queries` queries), then
 the rest, oldest first within each class -- (continuous batching: requests
 that arrive while a batch runs join the next one) and serves them with ONE
-library call.  With `fast_lane` (two kNN workers or more) the first kNN
-worker takes only small requests, on a high-priority stream, so that a
+library call.  With `fast_lane` (two kNN workers or more) the first
+`fast_lanes` kNN workers take only small requests (at most
+`fast_lane_max_queries` per call), on high-priority streams, so that a
 small request never waits behind a large batch; the others take large
 requests first and small ones when nothing else is pending or when a small
-one has waited `overflow_ms` (the fast lane is behind).  For kNN the for kNN the
+one has waited `overflow_ms` (the fast lane is behind).  For kNN the
 queries are concatenated and searched with the largest k asked for; every
 request gets the prefix it asked for, which is exactly its own search because
 results are ordered by (distance, index).  Several kNN workers run their
@@ -89,7 +90,8 @@ class Server:
     def __init__(self, ab, X, models=None, workers=2, max_batch_queries=1024,
                  max_request_queries=4096, hbm_budget=16 << 30, precision_mode="bf16x3",
                  small_queries=256, aging_ms=20.0, ann=None, free_memory="auto",
-                 hbm_reserve=1 << 30, fast_lane=True, overflow_ms=2.0):
+                 hbm_reserve=1 << 30, fast_lane=True, overflow_ms=2.0, fast_lanes=1,
+                 fast_lane_max_queries=None):
         self.ab = ab
         # admission: a batch's device bytes stay within the worker's share of
         # hbm_budget AND of the device memory free (less hbm_reserve), read
@@ -105,6 +107,11 @@ class Server:
         self._free_val = None
         self.small_queries = small_queries
         self.fast_lane = bool(fast_lane) and workers >= 2
+        # the first fast_lanes kNN workers are fast lanes (at least one other
+        # worker takes the large requests); a fast lane's batch holds at most
+        # fast_lane_max_queries queries
+        self.fast_lanes = max(1, min(int(fast_lanes), workers - 1)) if self.fast_lane else 0
+        self.fast_cap = int(fast_lane_max_queries or max_batch_queries)
         self.overflow = overflow_ms / 1e3
         self.aging = aging_ms / 1e3
         self.X = np.ascontiguousarray(X, dtype=np.float32)
@@ -124,7 +131,7 @@ class Server:
         for w in range(workers):
             h = ab.KNN("s", order=ab.ROW_MAJOR, metric="euclidean",
                        precision_mode=precision_mode)
-            if self.fast_lane and w == 0:
+            if w < self.fast_lanes:
                 # the fast lane's kernels overtake the other workers' as SMs
                 # free up
                 h.set_stream_priority(-100)
@@ -313,9 +320,10 @@ class Server:
         h = self.knn_handles[w]
         share = self.hbm_budget // len(self.knn_handles)
         while True:
-            batch = self._take("knn", self.max_batch_queries, self._cap_bytes(share),
-                               self.bytes_per_query, small_only=self.fast_lane and w == 0,
-                               large_first=self.fast_lane and w > 0)
+            fast = w < self.fast_lanes
+            batch = self._take("knn", self.fast_cap if fast else self.max_batch_queries,
+                               self._cap_bytes(share), self.bytes_per_query, small_only=fast,
+                               large_first=self.fast_lane and not fast)
             if batch is None:
                 return
             try:

@@ -1062,7 +1062,8 @@ def run_ivf(ab, nx=1_000_000, nq=10_000, d=128, k=10, n_list=1024, n_probe=16, c
 
 
 def run_serving(ab, nx=8_000_000, d=96, comps=2048, n_models=64,
-                rates=(250.0, 1000.0, 2000.0, 10000.0, 50000.0), seconds=2.0, seed=5):
+                rates=(250.0, 1000.0, 2000.0, 10000.0, 50000.0), seconds=2.0, seed=5,
+                server_kw=None, plain=True):
     """Serving: a resident kNN index of 8,000,000 x 96 fp32 rows from a
     2,048-component Gaussian mixture (the k-means recipe) and 64 k-means
     models (d = 96, 256 centres, each fitted on 20,000 rows of its own
@@ -1113,9 +1114,10 @@ def run_serving(ab, nx=8_000_000, d=96, comps=2048, n_models=64,
         return means[li] + qrng.standard_normal((size, d), dtype=np.float32) * sig[li, None]
 
     out = {"workload": f"serve_fp32_index_{nx}x{d}_{n_models}_models_poisson_{seconds:g}s"}
-    for mode, mode_rates in (("bf16x3", rates), ("plain", rates[:1])):
-        server = sv.Server(ab, X, models=models, workers=2, max_batch_queries=512,
-                           precision_mode=mode)
+    kw = {"workers": 2, "max_batch_queries": 512} | dict(server_kw or {})
+    modes = (("bf16x3", rates), ("plain", rates[:1])) if plain else (("bf16x3", rates),)
+    for mode, mode_rates in modes:
+        server = sv.Server(ab, X, models=models, precision_mode=mode, **kw)
         for rate in mode_rates:
             # half a second of the same traffic first (not measured): the
             # measured trace starts from a serving steady state

@@ -285,3 +285,26 @@ def test_serving_fast_lane():
         assert any(b[4] > 4 for b in server.batches if b[0] == "knn")
     finally:
         server.close()
+
+
+def test_serving_two_fast_lanes_with_a_cap():
+    """Two fast lanes of three kNN workers, each fast-lane call at most
+    fast_lane_max_queries queries; results are every request's own search."""
+    sv = _load("aoclda_serving_fast2", os.path.join(PKG, "serving.py"))
+    rng = np.random.default_rng(9)
+    X = rng.standard_normal((300, 4)).astype(np.float32)
+    server = sv.Server(FakeAB(), X, workers=3, fast_lanes=2, fast_lane_max_queries=6,
+                       max_batch_queries=16, max_request_queries=64, small_queries=4)
+    try:
+        reqs = [server.submit(sv.Request("knn", rng.standard_normal((int(m), 4)), k=2))
+                for m in rng.choice([1, 2, 3, 4, 9, 30], 150)]
+        for r in reqs:
+            assert r.wait(30)
+        ref = FakeKNN("s").fit(X)
+        for r in reqs:
+            np.testing.assert_array_equal(r.result[0], ref.kneighbors(r.queries, 2)[0])
+        fast = {server.threads[0].ident, server.threads[1].ident}
+        mine = [b for b in server.batches if b[0] == "knn" and b[5] in fast]
+        assert mine and all(b[2] <= 6 and b[4] <= 4 for b in mine)
+    finally:
+        server.close()
