@@ -182,6 +182,13 @@ template <typename T> struct KMeans : public AlgBase {
     int fx_parity = 0;
     int ldbf = 0;
     da_int amb_last = 0;  // rows relabelled exactly in the last tensor-core pass
+    // spherical (cosine) k-means (kmeans.cpp:396-405): the options of the
+    // current compute, those the fitted model was computed with, the rows'
+    // inverse norms (dXinv) and normalised rows (dXs) of the data set
+    bool sph = false, sph_norm = true, model_sph = false, model_sph_norm = true;
+    DevBuf dXinv, dXs;
+    int sph_ready = 0; // bit 0: dXinv, bit 1: dXs hold the current data set
+    const void *fx_src = nullptr; // rows the fixed-point scales were computed from
     T *h_pin = nullptr;
     void *h_small = nullptr; // pinned: flags + scalars
     // Lloyd iterations 1.. as one CUDA graph (a WHILE node whose body is one
@@ -213,6 +220,11 @@ template <typename T> struct KMeans : public AlgBase {
     da_status ensure_device_data();
     da_status alloc_work();
     da_status init_centres(T *dC);
+    da_status init_centres_raw(T *dC);
+    da_status prepare_sph();
+    // rows the centroid update sums: the normalised copy for spherical
+    // k-means on normalised data, else the data set
+    T *update_rows() { return (sph && sph_norm) ? dXs.as<T>() : dX.as<T>(); }
     da_status kmeans_plusplus(T *dC);
     da_status afk_mcmc(std::vector<T> &Cc);
     da_status run_lloyd(T *&dCcur, T *&dCprev, int *&dLcur, int *&dLprev, da_int &n_iter,

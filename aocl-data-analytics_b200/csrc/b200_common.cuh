@@ -34,6 +34,15 @@ B200_DEV float sqrt_rn(float a) { return __fsqrt_rn(a); }
 B200_DEV double sqrt_rn(double a) { return __dsqrt_rn(a); }
 B200_DEV float abs_(float a) { return fabsf(a); }
 B200_DEV double abs_(double a) { return fabs(a); }
+
+// Spherical k-means++ distance of row i to data row c (kmeans.cpp:1491-1510):
+// max(0, 1 - cos) with cos = fl(fl(dot inv_i) inv_c) for normalised data
+// (inv: inverse row norms), else cos = dot.  A NaN gives 0, as std::max(0, v).
+template <typename T> B200_DEV T cos_dist_kpp(T dot, const T *inv, int i, int c) {
+    const T cs = inv ? mul_rn(mul_rn(dot, inv[i]), inv[c]) : dot;
+    const T v = sub_rn(T(1), cs);
+    return T(0) < v ? v : T(0);
+}
 B200_DEV float pow_(float a, float p) { return powf(a, p); }
 B200_DEV double pow_(double a, double p) { return pow(a, p); }
 

@@ -282,11 +282,38 @@ template <typename T>
 cudaError_t launch_kmeans_inertia(const T *X, int ldx, int n, int d, const T *C, int ldc,
                                   const int *labels, double *block_partials, double *out,
                                   cudaStream_t s);
+// ------------------------------------------- spherical (cosine) k-means ---
+// Inverse row norms inv_i = 1 / sqrt(sqnorm_i) (0 for a zero row) and, when
+// Xs is given, the normalised rows Xs = fl(x_i inv_i) (same layout as X,
+// padding columns zero).
+template <typename T>
+cudaError_t launch_sph_data(const T *X, int ld, int n, int d, const T *sqnorm, T *inv, T *Xs,
+                            cudaStream_t s);
+// Centre rows scaled to unit length in place: c = fl(c / sqrt(sum c^2)) in
+// fp64 (a zero row stays zero).  With C_prev, scalars[0] = |C_prev|_F^2 and
+// scalars[1] = |C_prev - C|_F^2 of the normalised C (fixed order).
+template <typename T>
+cudaError_t launch_sph_centres(const T *C_prev, T *C, int k, int d, int ld, double *block_partials,
+                               double *scalars, cudaStream_t s);
+// Inertia sum_i (1 - cos_i), cos_i = fl(dot(x_i, c_{l_i}) inv_i) (inv null:
+// the dot itself); the dot is one fma chain in T, the sum fp64.
+template <typename T>
+cudaError_t launch_sph_inertia(const T *X, int ld, int n, int d, const T *C, const int *labels,
+                               const T *inv, double *block_partials, double *out, cudaStream_t s);
+// In place on D (m x k, row- or column-major, holding -dot as the pairwise
+// POST_NEG output): D = 1 - clamp(dot inv_i, -1, 1), inv_i = 1 / sqrt(sqnorm_i)
+// (0 for a zero row; sqnorm null: inv_i = 1).
+template <typename T>
+cudaError_t launch_sph_transform(T *D, int m, int k, bool rowmajor, const T *sqnorm,
+                                 cudaStream_t s);
 // k-means++ distances of every row to `t` candidate rows:
-// D[c*n + i] = (|x_i|^2 + |x_cand|^2) - 2 x_i.x_cand (GEMM form, no clamp).
+// D[c*n + i] = (|x_i|^2 + |x_cand|^2) - 2 x_i.x_cand (GEMM form, no clamp);
+// with `cosine` the spherical distance max(0, 1 - cos) of cos_dist_kpp
+// (xinv: the rows' inverse norms, or null for data used as given).
 template <typename T>
 cudaError_t launch_kpp_dist(const T *X, int ldx, int n, int d, const T *xnorm,
-                            const int *cand, int t, T *D, cudaStream_t s);
+                            const int *cand, int t, T *D, cudaStream_t s,
+                            const T *xinv = nullptr, int cosine = 0);
 // For each candidate c: cost_c = sum_i max(0, min(w_i, D_ci)) (fp64, fixed order).
 template <typename T>
 cudaError_t launch_kpp_cost(const T *w, const T *D, int n, int t, double *block_partials,
@@ -315,7 +342,8 @@ cudaError_t launch_kpp_draw(const T *w, int n, const double *bs, const double *U
 template <typename T>
 cudaError_t launch_kpp_dist_cost(const T *X, int ldx, int n, int d, const T *xnorm,
                                  const int *cand, int t, const T *w, T *D, double *cost,
-                                 void *work, cudaStream_t s);
+                                 void *work, cudaStream_t s, const T *xinv = nullptr,
+                                 int cosine = 0);
 size_t kpp_cost_work_bytes(int n, int t);
 // Choose among the nt candidates by cost (chosen[c]), w_i = max(0, min(w_i,
 // D_best,i)), w_best = 0, block sums of the new w.
@@ -349,13 +377,16 @@ cudaError_t launch_prep_centres_norms(const float *C, int ld, int k, int d, int 
 // error bound get their exact fp32 label; the others are appended to amb_rows
 // with up to 4 candidate clusters each (amb_ncand = 0: scan all).  *amb_count
 // must be 0 on entry.  Certified rows whose label changed go to `chg`.
+// cmax_sq_floor: a lower bound on max_j |c_j|^2 for the error bound, for
+// centres whose cnorm entries are not their norms (spherical k-means: cnorm
+// zero, the score -2 x.c, unit-length centres).
 cudaError_t launch_kmeans_assign_tc(int split, const void *Xh, const void *Xl, int n, int ldbf,
                                     const void *Bh, const void *Bl, const void *Baug,
                                     const void *Aaug, int k, const float *xnorm,
                                     const float *cnorm, int *labels, const int *labels_prev,
                                     int *flags, int *amb_rows, int *amb_cand, int *amb_ncand,
                                     int *amb_count, int *err, const ChangeList &chg,
-                                    cudaStream_t s);
+                                    cudaStream_t s, float cmax_sq_floor = 0.f);
 // Exact fp32 labels of the rows listed by the tensor-core pass (changed
 // ones to `chg`).
 cudaError_t launch_kmeans_rescore(const float *X, int ld, int d, const float *C, int k,

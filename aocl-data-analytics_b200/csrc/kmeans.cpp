@@ -114,6 +114,7 @@ template <typename T> da_status KMeans<T>::ensure_device_data() {
              "row norms");
     dXbf_stale = true;
     fx_stale = true;
+    sph_ready = 0;
     dx_loaded = true;
     return da_status_success;
 }
@@ -231,7 +232,11 @@ template <typename T> da_status KMeans<T>::kmeans_plusplus(T *dC) {
     B200_TRY(cudaMemcpyAsync(dFlag, &init_words[1], 2 * sizeof(int), cudaMemcpyHostToDevice, st),
              "copy");
     // w: distances to the first centre, clamped (kmeans.cpp:1561-1590)
-    B200_TRY(launch_kpp_dist<T>(dX.as<T>(), ld, n, d, dXn.as<T>(), dChosen, 1, dW.as<T>(), st),
+    // spherical k-means: the cosine distance of compute_distances_to_point
+    const T *xinv = (sph && sph_norm) ? dXinv.as<T>() : nullptr;
+    const int cosine = sph ? 1 : 0;
+    B200_TRY(launch_kpp_dist<T>(dX.as<T>(), ld, n, d, dXn.as<T>(), dChosen, 1, dW.as<T>(), st,
+                                xinv, cosine),
              "k-means++ distances");
     B200_TRY(launch_kpp_clamp<T>(dW.as<T>(), (int)n, first, dBs, dFlag, st), "k-means++ weights");
     int flags[2] = {0, 0};
@@ -255,7 +260,8 @@ template <typename T> da_status KMeans<T>::kmeans_plusplus(T *dC) {
                                         (int)n_trials, force_exact, dCandv, dUnc, dFlag + 1, st),
                      "k-means++ draws");
             B200_TRY(launch_kpp_dist_cost<T>(dX.as<T>(), ld, n, d, dXn.as<T>(), dCandv, n_trials,
-                                             dW.as<T>(), dKD.as<T>(), dCost, dPartials.p, st),
+                                             dW.as<T>(), dKD.as<T>(), dCost, dPartials.p, st,
+                                             xinv, cosine),
                      "k-means++ distances and costs");
             B200_TRY(launch_kpp_select_update<T>(dW.as<T>(), dKD.as<T>(), (int)n, dCost, dCandv,
                                                  (int)n_trials, dChosen, (int)c, dBs, st),
@@ -280,11 +286,26 @@ template <typename T> da_status KMeans<T>::afk_mcmc(std::vector<T> &Cc) {
     std::vector<T> xn(n, T(0));
     for (da_int i = 0; i < n; ++i)
         for (da_int j = 0; j < d; ++j) xn[i] += host_at(*this, i, j) * host_at(*this, i, j);
+    // spherical k-means on normalised data: inverse row norms (kmeans.cpp:681-703)
+    std::vector<T> inv;
+    if (sph && sph_norm) {
+        inv.resize(n);
+        for (da_int i = 0; i < n; ++i) {
+            const T nr = std::sqrt(xn[i]);
+            inv[i] = nr > T(0) ? T(1) / nr : T(0);
+        }
+    }
     std::uniform_int_distribution<> dis_int(0, n - 1);
     const da_int c1 = dis_int(mt_gen);
     Cc.assign((size_t)k * d, T(0));
-    for (da_int j = 0; j < d; ++j) Cc[(size_t)j * k] = host_at(*this, c1, j);
-    // d(x, c1)^2 in GEMM form
+    // a chosen row as a centre: scaled by its inverse norm for normalised
+    // spherical data (kmeans.cpp:1692-1697, 1803-1807)
+    auto place = [&](da_int c, da_int row) {
+        const T r = inv.empty() ? T(1) : inv[row];
+        for (da_int j = 0; j < d; ++j) Cc[c + (size_t)j * k] = host_at(*this, row, j) * r;
+    };
+    place(0, c1);
+    // d(x, c1)^2 in GEMM form, or the cosine distance (kmeans.cpp:1489-1510)
     std::vector<T> w3(n), q(n);
     T dot_c = T(0);
     for (da_int j = 0; j < d; ++j) dot_c += host_at(*this, c1, j) * host_at(*this, c1, j);
@@ -292,7 +313,13 @@ template <typename T> da_status KMeans<T>::afk_mcmc(std::vector<T> &Cc) {
     for (da_int i = 0; i < n; ++i) {
         T s = T(0);
         for (da_int j = 0; j < d; ++j) s += host_at(*this, i, j) * host_at(*this, c1, j);
-        T v = T(-2) * s + (xn[i] + dot_c);
+        T v;
+        if (sph) {
+            const T cs = inv.empty() ? s : s * inv[i] * inv[c1];
+            v = std::max(T(0), T(1) - cs);
+        } else {
+            v = T(-2) * s + (xn[i] + dot_c);
+        }
         w3[i] = std::max(T(0), v);
         sum += w3[i];
     }
@@ -303,9 +330,14 @@ template <typename T> da_status KMeans<T>::afk_mcmc(std::vector<T> &Cc) {
         T best = std::numeric_limits<T>::infinity();
         for (da_int c = 0; c < nc; ++c) {
             T dist = T(0);
-            for (da_int j = 0; j < d; ++j) {
-                T t = host_at(*this, idx, j) - Cc[c + (size_t)j * k];
-                dist += t * t;
+            if (sph) {
+                for (da_int j = 0; j < d; ++j) dist += host_at(*this, idx, j) * Cc[c + (size_t)j * k];
+                dist = std::max(T(0), T(1) - (inv.empty() ? dist : dist * inv[idx]));
+            } else {
+                for (da_int j = 0; j < d; ++j) {
+                    T t = host_at(*this, idx, j) - Cc[c + (size_t)j * k];
+                    dist += t * t;
+                }
             }
             if (dist < best) best = dist;
         }
@@ -325,13 +357,41 @@ template <typename T> da_status KMeans<T>::afk_mcmc(std::vector<T> &Cc) {
                 dx = dy;
             }
         }
-        for (da_int j = 0; j < d; ++j) Cc[i + (size_t)j * k] = host_at(*this, x, j);
+        place(i, x);
     }
     return da_status_success;
 }
 
-// kmeans.cpp:1400-1486
+// kmeans.cpp:1400-1486: the method's centres, scaled to unit length for
+// spherical k-means (kmeans.cpp:1478-1485).
 template <typename T> da_status KMeans<T>::init_centres(T *dC) {
+    da_status s = init_centres_raw(dC);
+    if (s != da_status_success || !sph) return s;
+    B200_TRY(launch_sph_centres<T>(nullptr, dC, (int)n_clusters, (int)n_features, ld,
+                                   dPartials.as<double>(), nullptr, cuda->stream),
+             "centre normalisation");
+    B200_TRY(cudaStreamSynchronize(cuda->stream), "centre normalisation");
+    return da_status_success;
+}
+
+// Inverse row norms and, for normalised data, the normalised rows of the
+// data set (kmeans.cpp:681-703), once per data set.
+template <typename T> da_status KMeans<T>::prepare_sph() {
+    if (!sph) return da_status_success;
+    const int want = sph_norm ? 3 : 1;
+    if ((sph_ready & want) == want) return da_status_success;
+    if (!dXinv.ensure((size_t)n_samples * sizeof(T)) ||
+        (sph_norm && !dXs.ensure((size_t)n_samples * ld * sizeof(T))))
+        return err->error(da_status_memory_error, "Device memory allocation failed.");
+    B200_TRY(launch_sph_data<T>(dX.as<T>(), ld, (int)n_samples, (int)n_features, dXn.as<T>(),
+                                dXinv.as<T>(), sph_norm ? dXs.as<T>() : nullptr, cuda->stream),
+             "row normalisation");
+    B200_TRY(cudaStreamSynchronize(cuda->stream), "row normalisation");
+    sph_ready |= want;
+    return da_status_success;
+}
+
+template <typename T> da_status KMeans<T>::init_centres_raw(T *dC) {
     const da_int n = n_samples, k = n_clusters, d = n_features;
     std::vector<T> Cc;
     switch (init_method) {
@@ -392,6 +452,8 @@ template <typename T> da_status KMeans<T>::prepare_fx() {
         const int n = n_samples, k = n_clusters, d = n_features;
         if (!fx_update_supported(k, d)) return da_status_success;
         cudaStream_t st = cuda->stream;
+        const float *src = update_rows();
+        if (fx_src != static_cast<const void *>(src)) fx_stale = true;
         const size_t accb = fx_accum_bytes(k, d);
         if (!dFxScale.ensure((size_t)2 * d * sizeof(double) + (size_t)d * 4 + 16) ||
             !dFxAcc.ensure(accb))
@@ -408,8 +470,7 @@ template <typename T> da_status KMeans<T>::prepare_fx() {
             double *scale = dFxScale.as<double>();
             unsigned *colmax = reinterpret_cast<unsigned *>(scale + 2 * d);
             int *nonfinite = reinterpret_cast<int *>(colmax + d);
-            B200_TRY(launch_col_absmax(dX.as<float>(), ld, n, d, colmax, nonfinite, st),
-                     "column maxima");
+            B200_TRY(launch_col_absmax(src, ld, n, d, colmax, nonfinite, st), "column maxima");
             std::vector<unsigned> hmax(d + 1);
             B200_TRY(cudaMemcpyAsync(hmax.data(), colmax, (d + 1) * sizeof(unsigned),
                                      cudaMemcpyDeviceToHost, st), "copy");
@@ -441,6 +502,7 @@ template <typename T> da_status KMeans<T>::prepare_fx() {
                 B200_TRY(cudaStreamSynchronize(st), "scales");
             }
             fx_stale = false;
+            fx_src = src;
         }
         use_fx = fx_data_ok;
     }
@@ -482,6 +544,12 @@ template <typename T> da_status KMeans<T>::prepare_tc() {
     return da_status_success;
 }
 
+// Spherical k-means assigns with zero centre norms (the score -2 x.c of
+// unit-length centres): the tensor-core error bound takes max |c|^2 from
+// this bound instead -- a centre normalised in fp64 and rounded to fp32 has
+// |c|^2 <= (1 + 2^-24)^2 -- with margin.
+static constexpr float SPH_CMAX_SQ = 1.001f;
+
 // Assignment of every row to its nearest centre (labels of the plain fp32
 // formula), on the tensor cores when use_tc, else on the CUDA cores.
 template <typename T> da_status KMeans<T>::assign(const T *dC, int *dL, const int *dLprev) {
@@ -521,7 +589,7 @@ template <typename T> da_status KMeans<T>::assign(const T *dC, int *dL, const in
                                                dBh.p, s3 ? dBl.p : nullptr, dBaug.p, dAaug.p, k,
                                                dXnrm.as<float>(), dCn.as<float>(), dL, dLprev,
                                                dFlags.as<int>(), amb_rows, amb_cand, amb_ncand,
-                                               amb_cnt, errf, chg, st);
+                                               amb_cnt, errf, chg, st, sph ? SPH_CMAX_SQ : 0.f);
             }), "tensor-core assign");
             B200_TRY(cuda->timed("kmeans_rescore", [&] {
                 return launch_kmeans_rescore(dX.as<float>(), ld, d, dC, k, dCn.as<float>(),
@@ -545,7 +613,10 @@ da_status KMeans<T>::lloyd_step(const T *dCprev, T *dCnew, int *dL, const int *d
                                 double *h_scal, int *h_flags) {
     cudaStream_t st = cuda->stream;
     const int n = n_samples, k = n_clusters, d = n_features;
-    B200_TRY(launch_centre_norms<T>(dCprev, ld, k, d, dCn.as<T>(), st), "centre norms");
+    if (sph) // -C X^T of kmeans_lloyd.hpp:144-146: the norms term is zero
+        B200_TRY(cudaMemsetAsync(dCn.p, 0, k * sizeof(T), st), "memset");
+    else
+        B200_TRY(launch_centre_norms<T>(dCprev, ld, k, d, dCn.as<T>(), st), "centre norms");
     B200_TRY(cudaMemsetAsync(dFlags.p, 0, 8 * sizeof(int), st), "memset");
     {
         da_status sa = assign(dCprev, dL, dLprev);
@@ -556,7 +627,7 @@ da_status KMeans<T>::lloyd_step(const T *dCprev, T *dCnew, int *dL, const int *d
             const double *scale = dFxScale.as<double>();
             B200_TRY(cuda->timed("kmeans_update", [&] {
                 return launch_kmeans_update_fx(
-                    dX.as<float>(), ld, n, d, k, dL, reinterpret_cast<const float *>(scale),
+                    update_rows(), ld, n, d, k, dL, reinterpret_cast<const float *>(scale),
                     scale + d, dFxAcc.p, fx_parity,
                     dCprev, dCnew, dCounts.as<int>(), dScalars.as<double>() + 8,
                     dScalars.as<double>(), dFlags.as<int>(), dFxTicket.as<unsigned>(), st);
@@ -570,12 +641,16 @@ da_status KMeans<T>::lloyd_step(const T *dCprev, T *dCnew, int *dL, const int *d
                                       dSorted.as<int>(), dFlags.as<int>(), st);
         }), "sort");
         B200_TRY(cuda->timed("kmeans_update", [&] {
-            return launch_kmeans_update<T>(dX.as<T>(), ld, n, d, k, dSorted.as<int>(),
+            return launch_kmeans_update<T>(update_rows(), ld, n, d, k, dSorted.as<int>(),
                                            dOffsets.as<int>(), dSegStart.as<int>(), SEG_ROWS,
                                            dChunkSums.as<double>(), dCounts.as<int>(), dCprev,
                                            dCnew, ld, dScalars.as<double>(), dFlags.as<int>(), st);
         }), "update");
     }
+    if (update && sph) // unit-length centres and their shift (kmeans_lloyd.hpp:373-405)
+        B200_TRY(launch_sph_centres<T>(dCprev, dCnew, k, d, ld, dPartials.as<double>(),
+                                       dScalars.as<double>(), st),
+                 "centre normalisation");
     if (h_scal) {
         B200_TRY(cudaMemcpyAsync(h_scal, dScalars.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, st),
                  "copy");
@@ -617,13 +692,33 @@ template <typename T> da_status KMeans<T>::split_empty(T *dC, int *dL, bool &spl
     for (da_int c = 0; c < k; ++c) n_empty += cnt[c] == 0;
     if (n_empty == 0) return da_status_success;
     std::vector<T> w(n);
+    // spherical k-means: 1 - cos with the rows' inverse norms (kmeans.cpp:1171-1192)
+    std::vector<T> inv;
+    if (sph && sph_norm) {
+        inv.resize(n);
+        B200_TRY(cudaMemcpyAsync(inv.data(), dXinv.p, n * sizeof(T), cudaMemcpyDeviceToHost,
+                                 cuda->stream), "copy");
+        B200_TRY(cudaStreamSynchronize(cuda->stream), "copy");
+    }
     auto dist_to = [&](da_int i, da_int c) {
         T s = T(0);
+        if (sph) {
+            for (da_int j = 0; j < d; ++j) s += host_at(*this, i, j) * Cc[c + (size_t)j * k];
+            return T(1) - (inv.empty() ? s : s * inv[i]);
+        }
         for (da_int j = 0; j < d; ++j) {
             T t = host_at(*this, i, j) - Cc[c + (size_t)j * k];
             s += t * t;
         }
         return s;
+    };
+    // spherical: a centre row scaled to unit length in T (kmeans.cpp:1243-1269)
+    auto unit = [&](da_int c) {
+        T sq = T(0);
+        for (da_int j = 0; j < d; ++j) sq += Cc[c + (size_t)j * k] * Cc[c + (size_t)j * k];
+        if (!(sq > T(0))) return;
+        const T r = T(1) / std::sqrt(sq);
+        for (da_int j = 0; j < d; ++j) Cc[c + (size_t)j * k] *= r;
     };
     for (da_int i = 0; i < n; ++i) w[i] = dist_to(i, lab[i]);
     for (da_int c = 0; c < k; ++c) {
@@ -637,11 +732,16 @@ template <typename T> da_status KMeans<T>::split_empty(T *dC, int *dL, bool &spl
             }
         if (bi < 0) break;
         const da_int old = lab[bi], nold = cnt[old];
+        const T ib = inv.empty() ? T(1) : inv[bi]; // the donor row as the update sums it
         for (da_int j = 0; j < d; ++j) {
             T &cv = Cc[old + (size_t)j * k];
-            cv = (cv * T(nold) - host_at(*this, bi, j)) / T(nold - 1);
+            cv = (cv * T(nold) - host_at(*this, bi, j) * ib) / T(nold - 1);
         }
-        for (da_int j = 0; j < d; ++j) Cc[c + (size_t)j * k] = host_at(*this, bi, j);
+        for (da_int j = 0; j < d; ++j) Cc[c + (size_t)j * k] = host_at(*this, bi, j) * ib;
+        if (sph) {
+            unit(old);
+            unit(c);
+        }
         cnt[old] -= 1;
         cnt[c] = 1;
         lab[bi] = (int)c;
@@ -831,7 +931,7 @@ da_status KMeans<T>::run_lloyd(T *&dCcur, T *&dCprev, int *&dLcur, int *&dLprev,
     converged = 0;
     empty_found = false;
     // iterations 1.. as one graph launch where the loop allows it
-    const bool graph = use_fx && use_tc && empty_mode == EC_IGNORE && !cuda->timing;
+    const bool graph = use_fx && use_tc && empty_mode == EC_IGNORE && !cuda->timing && !sph;
     da_int it = 0;
     for (it = 0; it < max_iter; ++it) {
         if (graph && it == 1) {
@@ -874,9 +974,14 @@ da_status KMeans<T>::run_lloyd(T *&dCcur, T *&dCprev, int *&dLcur, int *&dLprev,
         da_status s = lloyd_step(dCcur, nullptr, dLcur, nullptr, false, nullptr, nullptr);
         if (s != da_status_success) return s;
     }
-    B200_TRY(launch_kmeans_inertia<T>(dX.as<T>(), ld, n_samples, n_features, dCcur, ld, dLcur,
-                                      dPartials.as<double>(), dScalars.as<double>() + 2,
-                                      cuda->stream), "inertia");
+    if (sph)
+        B200_TRY(launch_sph_inertia<T>(dX.as<T>(), ld, n_samples, n_features, dCcur, dLcur,
+                                       sph_norm ? dXinv.as<T>() : nullptr, dPartials.as<double>(),
+                                       dScalars.as<double>() + 2, cuda->stream), "inertia");
+    else
+        B200_TRY(launch_kmeans_inertia<T>(dX.as<T>(), ld, n_samples, n_features, dCcur, ld, dLcur,
+                                          dPartials.as<double>(), dScalars.as<double>() + 2,
+                                          cuda->stream), "inertia");
     B200_TRY(cudaMemcpyAsync(h_scal + 2, dScalars.as<double>() + 2, sizeof(double),
                              cudaMemcpyDeviceToHost, cuda->stream), "copy");
     B200_TRY(cudaStreamSynchronize(cuda->stream), "inertia");
@@ -896,6 +1001,8 @@ template <typename T> da_status KMeans<T>::read_options() {
     algorithm = opts.key("algorithm");
     empty_mode = opts.key("empty clusters");
     const bool spherical = opts.key("distance") == 1;
+    sph = spherical;
+    sph_norm = opts.key("normalize data") == 1;
     da_status warn_status = da_status_success;
     std::string warn_msg;
     if (n_init > 1 && init_method == INIT_SUPPLIED) {
@@ -916,9 +1023,6 @@ template <typename T> da_status KMeans<T>::read_options() {
         return err->error(da_status_not_implemented,
                           "The B200 library implements Lloyd's algorithm (and Elkan, whose "
                           "iterates are Lloyd's); Hartigan-Wong and MacQueen are not provided.");
-    if (spherical)
-        return err->error(da_status_not_implemented,
-                          "Spherical (cosine) k-means is not provided by the B200 library.");
     if (n_clusters > n_samples)
         return err->error(da_status_incompatible_options,
                           "n_clusters = " + std::to_string(n_clusters) + ", and n_samples = " +
@@ -957,6 +1061,8 @@ template <typename T> da_status KMeans<T>::compute() {
     da_status s = ensure_device_data();
     if (s != da_status_success) return s;
     s = alloc_work();
+    if (s != da_status_success) return s;
+    s = prepare_sph();
     if (s != da_status_success) return s;
     s = prepare_tc();
     if (s != da_status_success) return s;
@@ -1009,6 +1115,8 @@ template <typename T> da_status KMeans<T>::compute() {
                               "cluster during the k-means iterations. A better set of initial "
                               "cluster centers is needed.");
     model_trained = true;
+    model_sph = sph;
+    model_sph_norm = sph_norm;
     if (warn_maxit) return err->warn(da_status_maxit, "The maximum number of iterations was reached.");
     // kmeans.cpp:413-420 only records this warning; compute() still succeeds
     if (warn_status != da_status_success) err->warn(warn_status, warn_msg);
@@ -1031,6 +1139,8 @@ template <typename T> da_status KMeans<T>::initial_centres(T *C, da_int ldc) {
     s = ensure_device_data();
     if (s != da_status_success) return s;
     s = alloc_work();
+    if (s != da_status_success) return s;
+    s = prepare_sph();
     if (s != da_status_success) return s;
     if (init_method != INIT_SUPPLIED) {
         if (seed == -1) {
@@ -1074,7 +1184,11 @@ da_status KMeans<T>::predict(da_int m, da_int d, const T *Y, da_int ldy, da_int 
         return err->error(da_status_memory_error, "Device memory allocation failed.");
     B200_TRY(upload_matrix<T>(order(), m, d, Y, ldy, dY.as<T>(), ld, dStage, st), "upload");
     B200_TRY(upload_centres<T>(best_centres, n_clusters, n_features, ld, dC0.as<T>(), st), "upload");
-    B200_TRY(launch_centre_norms<T>(dC0.as<T>(), ld, n_clusters, n_features, dCn.as<T>(), st), "norms");
+    if (model_sph) // -C Y^T (kmeans.cpp:976-981)
+        B200_TRY(cudaMemsetAsync(dCn.p, 0, n_clusters * sizeof(T), st), "memset");
+    else
+        B200_TRY(launch_centre_norms<T>(dC0.as<T>(), ld, n_clusters, n_features, dCn.as<T>(), st),
+                 "norms");
     B200_TRY(launch_kmeans_assign<T>(dY.as<T>(), ld, m, n_features, dC0.as<T>(), ld, n_clusters,
                                      dCn.as<T>(), dYL.as<int>(), nullptr, nullptr, nullptr, st),
              "assign");
@@ -1115,9 +1229,19 @@ da_status KMeans<T>::transform(da_int m, da_int d, const T *X, da_int ldx, T *Xt
     B200_TRY(upload_centres<T>(best_centres, n_clusters, n_features, ld, dC0.as<T>(), st), "upload");
     B200_TRY(launch_centre_norms<T>(dC0.as<T>(), ld, n_clusters, n_features, dCn.as<T>(), st), "norms");
     B200_TRY(launch_row_sqnorms<T>(dY.as<T>(), ld, m, n_features, dYL.as<T>(), st), "norms");
-    PairwiseArgs a{ACC_DOT, POST_GEMM_SQRT, 256, 2.0, false, order() == row_major};
-    B200_TRY(launch_pairwise<T>(dY.as<T>(), ld, m, dC0.as<T>(), ld, n_clusters, n_features,
-                                dYL.as<T>(), dCn.as<T>(), a, dKD.as<T>(), st), "transform");
+    if (model_sph) {
+        // 1 - clamp(x.c / |x|) (kmeans.cpp:821-858): -dot, then the post-op
+        PairwiseArgs a{ACC_DOT, POST_NEG, 256, 2.0, false, order() == row_major};
+        B200_TRY(launch_pairwise<T>(dY.as<T>(), ld, m, dC0.as<T>(), ld, n_clusters, n_features,
+                                    dYL.as<T>(), dCn.as<T>(), a, dKD.as<T>(), st), "transform");
+        B200_TRY(launch_sph_transform<T>(dKD.as<T>(), m, n_clusters, order() == row_major,
+                                         model_sph_norm ? dYL.as<T>() : nullptr, st),
+                 "transform");
+    } else {
+        PairwiseArgs a{ACC_DOT, POST_GEMM_SQRT, 256, 2.0, false, order() == row_major};
+        B200_TRY(launch_pairwise<T>(dY.as<T>(), ld, m, dC0.as<T>(), ld, n_clusters, n_features,
+                                    dYL.as<T>(), dCn.as<T>(), a, dKD.as<T>(), st), "transform");
+    }
     std::vector<T> out(outn);
     B200_TRY(cudaMemcpyAsync(out.data(), dKD.p, outn * sizeof(T), cudaMemcpyDeviceToHost, st), "copy");
     B200_TRY(cudaStreamSynchronize(st), "transform");
@@ -1260,6 +1384,9 @@ da_status KMeans<T>::shard_begin(const float *colmax_global, da_int n_global, co
         da_status s = read_options();
         if (s != da_status_success && err->severity == DA_ERROR) return s;
         err->clear();
+        if (sph)
+            return err->error(da_status_not_implemented,
+                              "Sharded k-means steps use the euclidean distance only.");
         const int k = n_clusters, d = n_features;
         if (!fx_update_supported(k, d))
             return err->error(da_status_not_implemented,
@@ -1512,6 +1639,9 @@ template <typename T> da_status KMeans<T>::load_state(ByteReader &r) {
     ld = pad4(n_features);
     initdone = false;
     model_trained = true;
+    // the options were restored before the state: the model's distance
+    model_sph = opts.key("distance") == 1;
+    model_sph_norm = opts.key("normalize data") == 1;
     return da_status_success;
 }
 

@@ -194,7 +194,7 @@ kpp_draw_kernel(const T *w, int n, const double *bs, int nb, const double *U, do
 
 // The uncertified draws with the reference's sequential arithmetic: S =
 // sum w (double, index order, from 0), p_i = w_i / S, cp_i = cp_{i-1} + p_i,
-// cp_{n-1} = 1, the first i with cp_i >= u.  One block; thread 0 carries the
+// cp_{n-1} = 1, the first i with !(cp_i < u) (std::lower_bound).  One block; thread 0 carries the
 // sequential sums over tiles that all threads stage in shared memory.
 // count[0] accumulates the number of redone draws.
 template <typename T>
@@ -244,7 +244,9 @@ kpp_exact_kernel(const T *w, int n, const double *U, int nt, int *cand, const in
                 for (int j = 0; j < m; ++j) {
                     cp = __dadd_rn(cp, tile[j]);
                     if (t0 + j == n - 1) cp = 1.0;
-                    if (cp >= u) {
+                    // std::lower_bound's test !(cp < u): with all weights
+                    // zero (S = 0) every cp is NaN and the first index wins
+                    if (!(cp < u)) {
                         s_res = t0 + j;
                         s_done = 1;
                         break;
@@ -464,7 +466,7 @@ template <> struct SegTraits<double> {
 template <typename T, bool SMEM>
 __global__ void __launch_bounds__(CK, 2)
 kpp_dist_csum_kernel(const T *X, int ld, int n, int d, const T *xnorm, const int *cand, int t,
-                     const T *w, T *D, double *csum, int nchunks) {
+                     const T *w, T *D, double *csum, int nchunks, const T *xinv, int cosine) {
     using S = SegTraits<T>;
     constexpr int NV = S::SEG / S::W;
     extern __shared__ __align__(16) unsigned char sm[];
@@ -525,7 +527,9 @@ kpp_dist_csum_kernel(const T *X, int ld, int n, int d, const T *xnorm, const int
         for (int g = 0; g < 8; ++g) {
             part[g] = 0.0;
             if (valid && c0 + g < t) {
-                const T dv = fma_rn(T(-2), s[g], add_rn(xn, xnorm[cand[c0 + g]]));
+                const int cc = cand[c0 + g];
+                const T dv = cosine ? cos_dist_kpp(s[g], xinv, i, cc)
+                                    : fma_rn(T(-2), s[g], add_rn(xn, xnorm[cc]));
                 D[(size_t)(c0 + g) * n + i] = dv;
                 part[g] = (double)kpp_term(wi, dv);
             }
@@ -762,7 +766,7 @@ int kpp_num_chunks(int n) { return (n + CK - 1) / CK; }
 template <typename T>
 cudaError_t launch_kpp_dist_cost(const T *X, int ldx, int n, int d, const T *xnorm,
                                  const int *cand, int t, const T *w, T *D, double *cost,
-                                 void *work, cudaStream_t s) {
+                                 void *work, cudaStream_t s, const T *xinv, int cosine) {
     if (ldx % 4 != 0 || (reinterpret_cast<uintptr_t>(X) & 15) != 0) return cudaErrorInvalidValue;
     const int nch = kpp_num_chunks(n);
     double *csum = static_cast<double *>(work);
@@ -779,10 +783,10 @@ cudaError_t launch_kpp_dist_cost(const T *X, int ldx, int n, int d, const T *xno
             reinterpret_cast<const void *>(kpp_dist_csum_kernel<T, true>), want);
         if (e != cudaSuccess) return e;
         kpp_dist_csum_kernel<T, true><<<nch, CK, want, s>>>(X, ldx, n, d, xnorm, cand, t, w, D,
-                                                            csum, nch);
+                                                            csum, nch, xinv, cosine);
     } else {
         kpp_dist_csum_kernel<T, false><<<nch, CK, 0, s>>>(X, ldx, n, d, xnorm, cand, t, w, D, csum,
-                                                          nch);
+                                                          nch, xinv, cosine);
     }
     kpp_chunk_prefix_kernel<<<t, 1024, 0, s>>>(csum, nch, P);
     kpp_chunk_q_kernel<T><<<dim3((nch + 7) / 8, t), 256, 0, s>>>(w, D, n, nch, P, Q0, Q1, Or,
@@ -891,7 +895,7 @@ cudaError_t launch_kpp_select_update(T *w, const T *D, int n, const double *cost
                                                      cudaStream_t);                             \
     template cudaError_t launch_kpp_dist_cost<T>(const T *, int, int, int, const T *,           \
                                                  const int *, int, const T *, T *, double *,     \
-                                                 void *, cudaStream_t);
+                                                 void *, cudaStream_t, const T *, int);
 B200_KPP_INST(float)
 B200_KPP_INST(double)
 

@@ -418,7 +418,8 @@ template <> struct Vec16<double> {
 template <typename T>
 __global__ void __launch_bounds__(256) kpp_dist_kernel(const T *X, int ld, int n, int d,
                                                        const T *xnorm, const int *cand, int t,
-                                                       T *D, int use_smem) {
+                                                       T *D, int use_smem, const T *xinv,
+                                                       int cosine) {
     extern __shared__ __align__(16) unsigned char sm[];
     T *cs = reinterpret_cast<T *>(sm);
     if (use_smem) {
@@ -459,19 +460,22 @@ __global__ void __launch_bounds__(256) kpp_dist_kernel(const T *X, int ld, int n
 #pragma unroll
         for (int g = 0; g < KPP_G; ++g)
             if (c0 + g < t) {
-                const T nn = add_rn(xn, xnorm[cand[c0 + g]]);
-                D[(size_t)(c0 + g) * n + i] = fma_rn(T(-2), s[g], nn);
+                const int cg = cand[c0 + g];
+                D[(size_t)(c0 + g) * n + i] =
+                    cosine ? cos_dist_kpp(s[g], xinv, i, cg)
+                           : fma_rn(T(-2), s[g], add_rn(xn, xnorm[cg]));
             }
     }
 }
 template <typename T>
 cudaError_t launch_kpp_dist(const T *X, int ldx, int n, int d, const T *xnorm, const int *cand,
-                            int t, T *D, cudaStream_t s) {
+                            int t, T *D, cudaStream_t s, const T *xinv, int cosine) {
     if (ldx % 4 != 0 || (reinterpret_cast<uintptr_t>(X) & 15) != 0) return cudaErrorInvalidValue;
     const size_t want = (size_t)t * d * sizeof(T);
     const int use_smem = want <= 48 * 1024 ? 1 : 0;
     kpp_dist_kernel<T><<<(n + 255) / 256, 256, use_smem ? want : 0, s>>>(X, ldx, n, d, xnorm,
-                                                                        cand, t, D, use_smem);
+                                                                        cand, t, D, use_smem,
+                                                                        xinv, cosine);
     return cudaGetLastError();
 }
 template <typename T>
@@ -532,12 +536,173 @@ cudaError_t launch_kpp_update(T *w, const T *Dc, int n, int chosen, cudaStream_t
                                                   const int *, double *, double *,              \
                                                   cudaStream_t);                                \
     template cudaError_t launch_kpp_dist<T>(const T *, int, int, int, const T *, const int *,   \
-                                            int, T *, cudaStream_t);                            \
+                                            int, T *, cudaStream_t, const T *, int);            \
     template cudaError_t launch_kpp_cost<T>(const T *, const T *, int, int, double *, double *, \
                                             cudaStream_t);                                      \
     template cudaError_t launch_kpp_update<T>(T *, const T *, int, int, cudaStream_t);
 B200_KM_INST(float)
 B200_KM_INST(double)
+
+// ------------------------------------------- spherical (cosine) k-means ---
+// Inverse norms of the rows (kmeans.cpp:681-703: safe_inv of the row norm)
+// and the normalised rows Xs = x_i inv_i that the centroid update sums
+// (kmeans_lloyd.hpp:279-300), one element per thread.
+template <typename T>
+__global__ void sph_data_kernel(const T *X, int ld, int n, int d, const T *sqnorm, T *inv, T *Xs) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (size_t)n * ld) return;
+    const int i = (int)(e / ld), f = (int)(e - (size_t)i * ld);
+    const T sq = sqnorm[i];
+    const T r = sq > T(0) ? div_rn(T(1), sqrt_rn(sq)) : T(0);
+    if (f == 0) inv[i] = r;
+    if (Xs) Xs[e] = f < d ? mul_rn(X[e], r) : T(0);
+}
+template <typename T>
+cudaError_t launch_sph_data(const T *X, int ld, int n, int d, const T *sqnorm, T *inv, T *Xs,
+                            cudaStream_t s) {
+    const size_t tot = (size_t)n * ld;
+    if (tot == 0) return cudaSuccess;
+    sph_data_kernel<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(X, ld, n, d, sqnorm, inv, Xs);
+    return cudaGetLastError();
+}
+
+// Centres to unit length (kmeans_lloyd.hpp:373-405, normalize_rows_inplace of
+// da_utils.cpp:807-853; a zero row keeps the factor 1): one warp per centre;
+// lane 0 sums the squares in feature order in fp64, every lane scales its
+// features by 1 / sqrt of that sum.  With C_prev, per-block fp64 partials of
+// |c_prev|^2 and |c_prev - c|^2 (fixed reduction order).
+template <typename T>
+__global__ void __launch_bounds__(256)
+sph_centres_kernel(const T *C_prev, T *C, int k, int d, int ld, double *block_partials) {
+    __shared__ double sh[2][8];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int j = blockIdx.x * 8 + warp;
+    double pn = 0.0, ps = 0.0;
+    if (j < k) {
+        T *c = C + (size_t)j * ld;
+        double sq = 0.0;
+        if (lane == 0)
+            for (int f = 0; f < d; ++f) {
+                const double v = (double)c[f];
+                sq = __fma_rn(v, v, sq);
+            }
+        sq = __shfl_sync(0xffffffffu, sq, 0);
+        const double r = sq > 0.0 ? __ddiv_rn(1.0, __dsqrt_rn(sq)) : 1.0;
+        for (int f = lane; f < d; f += 32) {
+            const T v = (T)__dmul_rn((double)c[f], r);
+            c[f] = v;
+            if (C_prev) {
+                const double cp = (double)C_prev[(size_t)j * ld + f];
+                pn += cp * cp;
+                const double df = cp - (double)v;
+                ps += df * df;
+            }
+        }
+    }
+    if (!C_prev) return;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        pn += __shfl_down_sync(0xffffffffu, pn, off);
+        ps += __shfl_down_sync(0xffffffffu, ps, off);
+    }
+    if (lane == 0) {
+        sh[0][warp] = pn;
+        sh[1][warp] = ps;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            a += sh[0][w];
+            b += sh[1][w];
+        }
+        block_partials[2 * blockIdx.x] = a;
+        block_partials[2 * blockIdx.x + 1] = b;
+    }
+}
+template <typename T>
+cudaError_t launch_sph_centres(const T *C_prev, T *C, int k, int d, int ld, double *block_partials,
+                               double *scalars, cudaStream_t s) {
+    const int nb = (k + 7) / 8;
+    sph_centres_kernel<T><<<nb, 256, 0, s>>>(C_prev, C, k, d, ld, block_partials);
+    if (C_prev) sum_partials_kernel<<<1, 32, 0, s>>>(block_partials, nb, 2, 2, scalars);
+    return cudaGetLastError();
+}
+
+// Spherical inertia (kmeans.cpp:1065-1098): per row 1 - cos with the dot as
+// one fma chain over the features in T, one thread per row, fp64 sum in a
+// fixed order.
+template <typename T>
+__global__ void __launch_bounds__(256)
+sph_inertia_kernel(const T *X, int ld, int n, int d, const T *C, const int *labels, const T *inv,
+                   double *block_partials) {
+    __shared__ double sh[8];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const T *x = X + (size_t)i * ld;
+        const T *c = C + (size_t)labels[i] * ld;
+        T dot = T(0);
+        for (int f = 0; f < d; ++f) dot = fma_rn(x[f], c[f], dot);
+        const T cs = inv ? mul_rn(dot, inv[i]) : dot;
+        acc += (double)sub_rn(T(1), cs);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if (lane == 0) sh[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += sh[w];
+        block_partials[blockIdx.x] = t;
+    }
+}
+template <typename T>
+cudaError_t launch_sph_inertia(const T *X, int ld, int n, int d, const T *C, const int *labels,
+                               const T *inv, double *block_partials, double *out, cudaStream_t s) {
+    const int nb = 148 * 8;
+    sph_inertia_kernel<T><<<nb, 256, 0, s>>>(X, ld, n, d, C, labels, inv, block_partials);
+    sum_partials_kernel<<<1, 32, 0, s>>>(block_partials, nb, 1, 1, out);
+    return cudaGetLastError();
+}
+
+// Cosine transform (kmeans.cpp:821-858 with dot_to_cosine_distance_*):
+// D holds -dot; D = 1 - clamp(dot inv_i) with inv_i = safe_inv_sqrt(|x_i|^2).
+template <typename T>
+__global__ void sph_transform_kernel(T *D, int m, int k, int rowmajor, const T *sqnorm) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (size_t)m * k) return;
+    const int i = rowmajor ? (int)(e / k) : (int)(e % m);
+    T r = T(1);
+    if (sqnorm) {
+        const T sq = sqnorm[i];
+        r = sq > T(0) ? div_rn(T(1), sqrt_rn(sq)) : T(0);
+    }
+    T cs = mul_rn(-D[e], r);
+    cs = cs < T(1) ? cs : T(1);
+    cs = T(-1) < cs ? cs : T(-1);
+    D[e] = sub_rn(T(1), cs);
+}
+template <typename T>
+cudaError_t launch_sph_transform(T *D, int m, int k, bool rowmajor, const T *sqnorm,
+                                 cudaStream_t s) {
+    const size_t tot = (size_t)m * k;
+    if (tot == 0) return cudaSuccess;
+    sph_transform_kernel<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(D, m, k, rowmajor ? 1 : 0,
+                                                                         sqnorm);
+    return cudaGetLastError();
+}
+
+#define B200_SPH_INST(T)                                                                       \
+    template cudaError_t launch_sph_data<T>(const T *, int, int, int, const T *, T *, T *,      \
+                                            cudaStream_t);                                      \
+    template cudaError_t launch_sph_centres<T>(const T *, T *, int, int, int, double *, double *,\
+                                               cudaStream_t);                                   \
+    template cudaError_t launch_sph_inertia<T>(const T *, int, int, int, const T *, const int *,\
+                                               const T *, double *, double *, cudaStream_t);    \
+    template cudaError_t launch_sph_transform<T>(T *, int, int, bool, const T *, cudaStream_t);
+B200_SPH_INST(float)
+B200_SPH_INST(double)
 
 
 // ------------------------------------------- fixed-point update (fp32 X) ---

@@ -38,6 +38,7 @@ struct TcAssignArgs {
     const float *xnorm;  // n   (fp32 |x_i|)
     const float *cnorm;  // k   (fp32 |c_j|^2, the plain path's values)
     float e1, e2;        // eps_i = e1 |x_i| cmax + e2 cmax^2, cmax = max_j |c_j|
+    float cm_floor;      // lower bound on cmax^2 (cnorm not the norms: spherical)
     int *labels;
     const int *labels_prev;
     int *flags;          // [0] labels changed
@@ -315,7 +316,7 @@ kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
         const int tail = a.npad - (nchunks - 1) * 32; // valid columns of the last chunk
         const int c_lo = h == 0 ? 0 : (nchunks + 1) / 2;
         const int c_hi = h == 0 ? (nchunks + 1) / 2 : nchunks;
-        float cm = 0.f;
+        float cm = a.cm_floor;
         for (int j = lane; j < a.k; j += 32) cm = fmaxf(cm, a.cnorm[j]);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) cm = fmaxf(cm, __shfl_xor_sync(0xffffffffu, cm, off));
@@ -867,7 +868,7 @@ cudaError_t launch_kmeans_assign_tc(int split, const void *Xh, const void *Xl, i
                                     const float *cnorm, int *labels, const int *labels_prev,
                                     int *flags, int *amb_rows, int *amb_cand, int *amb_ncand,
                                     int *amb_count, int *err, const ChangeList &chg,
-                                    cudaStream_t s) {
+                                    cudaStream_t s, float cmax_sq_floor) {
     const int nkb = ldbf / TC_KB;
     const int npad = (k + 15) & ~15;
     const bool s3 = split == 3;
@@ -937,6 +938,7 @@ cudaError_t launch_kmeans_assign_tc(int split, const void *Xh, const void *Xl, i
     a.cnorm = cnorm;
     a.e1 = (float)e1;
     a.e2 = (float)e2;
+    a.cm_floor = cmax_sq_floor;
     a.labels = labels;
     a.labels_prev = labels_prev;
     a.flags = flags;

@@ -445,6 +445,128 @@ int orc_kmeans_iteration_s(int n, int d, const float *X, int k, float *C, int32_
     return changed;
 }
 
+/* ------------------------------------------------------------------ */
+/* Spherical (cosine) k-means                                          */
+/* ------------------------------------------------------------------ */
+/* The "distance" = "cosine" option of kmeans_options.hpp:111-121, Lloyd
+ * iterations (kmeans_lloyd.hpp:106-271, 373-405; kmeans.cpp:681-703,
+ * 1065-1098, 1478-1485):
+ *   inv_i  = 1 / sqrt(|x_i|^2) (0 for a zero row; |x|^2 one fma chain) --
+ *            safe_inv of the row norm;
+ *   assign = argmin_j fl(-dot(x_i, c_j)) on the rows as given (strict '<',
+ *            ties keep the lower j): the -C A^T GEMM with zero norms, here
+ *            the same comparison as fl(-2 dot + 0);
+ *   update = per cluster the fp64 sum of the rows, each scaled to
+ *            fl(x_i inv_i) when normalise (kmeans_lloyd.hpp:279-300), divided
+ *            by max(count, 1), rounded to T; then every centre (and the
+ *            initial ones) scaled to unit length: sq = sum c^2 in fp64 in
+ *            feature order, c = fl(c / sqrt(sq)) in fp64, a zero row kept
+ *            (normalize_rows_inplace of da_utils.cpp:807-853 uses the factor
+ *            1 for it).  The reference normalises in T; normalising the
+ *            rounded mean in fp64 changes no direction by more than an ulp;
+ *   shift / convergence as orc_kmeans_lloyd_s;
+ *   inertia = sum_i (1 - fl(dot(x_i, c_{l_i}) inv_i)) with each term in T
+ *            (normalise off: 1 - dot), summed in fp64. */
+#define ORC_SPH_DEFINE(T, SFX, DOT, SQN, SQRT)                                              \
+static void sph_unit_##SFX(T *C, int k, int d) {                                            \
+    for (int j = 0; j < k; ++j) {                                                           \
+        T *c = C + (size_t)j * d;                                                           \
+        double sq = 0;                                                                      \
+        for (int f = 0; f < d; ++f) sq = fma((double)c[f], (double)c[f], sq);               \
+        const double r = sq > 0 ? 1.0 / sqrt(sq) : 1.0;                                     \
+        for (int f = 0; f < d; ++f) c[f] = (T)((double)c[f] * r);                           \
+    }                                                                                       \
+}                                                                                           \
+static void sph_inv_##SFX(int n, int d, const T *X, T *inv) {                               \
+    for (int i = 0; i < n; ++i) {                                                           \
+        const T sq = SQN(X + (size_t)i * d, d);                                             \
+        inv[i] = sq > 0 ? (T)1 / SQRT(sq) : (T)0;                                           \
+    }                                                                                       \
+}                                                                                           \
+void orc_kmeans_assign_sph_##SFX(int n, int d, const T *X, int k, const T *C,               \
+                                 int32_t *labels, double *gap) {                            \
+    _Pragma("omp parallel for schedule(static)")                                            \
+    for (int i = 0; i < n; ++i) {                                                           \
+        const T *x = X + (size_t)i * d;                                                     \
+        T best = INFINITY; int bj = 0;                                                      \
+        double b1 = INFINITY, b2 = INFINITY;                                                \
+        for (int j = 0; j < k; ++j) {                                                       \
+            const T dt = DOT(x, C + (size_t)j * d, d);                                      \
+            const T v = -dt;                                                                \
+            if (v < best) { best = v; bj = j; }                                             \
+            if (!gap) continue;                                                             \
+            double e = 0;                                                                   \
+            for (int f = 0; f < d; ++f) e += (double)x[f] * (double)C[(size_t)j * d + f];   \
+            e = -e;                                                                         \
+            if (e < b1) { b2 = b1; b1 = e; } else if (e < b2) b2 = e;                       \
+        }                                                                                   \
+        labels[i] = bj;                                                                     \
+        if (gap) gap[i] = b2 - b1;                                                          \
+    }                                                                                       \
+}                                                                                           \
+double orc_kmeans_inertia_sph_##SFX(int n, int d, const T *X, const int32_t *labels,        \
+                                    const T *C, int normalise) {                            \
+    T *inv = malloc(sizeof(T) * (size_t)(n > 0 ? n : 1));                                   \
+    sph_inv_##SFX(n, d, X, inv);                                                            \
+    double acc = 0;                                                                         \
+    for (int i = 0; i < n; ++i) {                                                           \
+        const T dt = DOT(X + (size_t)i * d, C + (size_t)labels[i] * d, d);                  \
+        const T cs = normalise ? dt * inv[i] : dt;                                          \
+        acc += (double)((T)1 - cs);                                                         \
+    }                                                                                       \
+    free(inv);                                                                              \
+    return acc;                                                                             \
+}                                                                                           \
+void orc_kmeans_sph_lloyd_##SFX(int n, int d, const T *X, int k, const T *C0, int max_iter, \
+                                double tol, int normalise, T *C_out, int32_t *labels_out,   \
+                                int32_t *n_iter_out, double *inertia_out) {                 \
+    T *inv = malloc(sizeof(T) * (size_t)n);                                                 \
+    double *Xs = malloc(sizeof(double) * (size_t)n * d);                                    \
+    sph_inv_##SFX(n, d, X, inv);                                                            \
+    for (int i = 0; i < n; ++i)                                                             \
+        for (int f = 0; f < d; ++f) {                                                       \
+            const T v = X[(size_t)i * d + f];                                               \
+            Xs[(size_t)i * d + f] = (double)(normalise ? v * inv[i] : v);                   \
+        }                                                                                   \
+    T *Cp = malloc(sizeof(T) * (size_t)k * d), *Cc = malloc(sizeof(T) * (size_t)k * d);     \
+    double *Cn = malloc(sizeof(double) * (size_t)k * d);                                    \
+    int32_t *lp = calloc(n, sizeof(int32_t)), *lc = calloc(n, sizeof(int32_t));             \
+    int32_t *cnt = malloc(sizeof(int32_t) * k);                                             \
+    memcpy(Cc, C0, sizeof(T) * (size_t)k * d);                                              \
+    sph_unit_##SFX(Cc, k, d);                                                               \
+    int it, converged = 0;                                                                  \
+    for (it = 0; it < max_iter; ++it) {                                                     \
+        T *t = Cp; Cp = Cc; Cc = t;                                                         \
+        int32_t *tl = lp; lp = lc; lc = tl;                                                 \
+        orc_kmeans_assign_sph_##SFX(n, d, X, k, Cp, lc, NULL);                              \
+        orc_kmeans_update_d(n, d, Xs, lc, k, Cn, cnt);                                      \
+        for (size_t e = 0; e < (size_t)k * d; ++e) Cc[e] = (T)Cn[e];                        \
+        sph_unit_##SFX(Cc, k, d);                                                           \
+        double normc = 0, shift = 0;                                                        \
+        for (size_t e = 0; e < (size_t)k * d; ++e) {                                        \
+            normc += (double)Cp[e] * (double)Cp[e];                                         \
+            const double df = (double)Cp[e] - (double)Cc[e];                                \
+            shift += df * df;                                                               \
+        }                                                                                   \
+        int conv = 0;                                                                       \
+        if (it > 1) {                                                                       \
+            conv = 2;                                                                       \
+            for (int i = 0; i < n; ++i) if (lc[i] != lp[i]) { conv = 0; break; }            \
+        }                                                                                   \
+        if (conv == 0 && sqrt(shift) < tol * sqrt(normc)) conv = 1;                         \
+        converged = conv;                                                                   \
+        if (converged) break;                                                               \
+    }                                                                                       \
+    if (converged == 1 || it == max_iter) orc_kmeans_assign_sph_##SFX(n, d, X, k, Cc, lc, NULL); \
+    *inertia_out = orc_kmeans_inertia_sph_##SFX(n, d, X, lc, Cc, normalise);                \
+    *n_iter_out = it;                                                                       \
+    memcpy(C_out, Cc, sizeof(T) * (size_t)k * d);                                           \
+    memcpy(labels_out, lc, sizeof(int32_t) * n);                                            \
+    free(inv); free(Xs); free(Cp); free(Cc); free(Cn); free(lp); free(lc); free(cnt);       \
+}
+ORC_SPH_DEFINE(float, s, dot_s, sqnorm_s, sqrtf)
+ORC_SPH_DEFINE(double, d, dot_d, sqnorm_d, sqrt)
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -60,6 +60,18 @@ def lib():
             f = getattr(_lib, f"orc_kmeanspp_{sfx}")
             f.argtypes = [i, i, P, i, C.c_longlong, i, P, P]
             f.restype = i
+            f = getattr(_lib, f"orc_kmeanspp_cos_{sfx}")
+            f.argtypes = [i, i, P, i, C.c_longlong, i, P]
+            f.restype = i
+            f = getattr(_lib, f"orc_kmeans_assign_sph_{sfx}")
+            f.argtypes = [i, i, P, i, P, P, P]
+            f.restype = None
+            f = getattr(_lib, f"orc_kmeans_inertia_sph_{sfx}")
+            f.argtypes = [i, i, P, P, P, i]
+            f.restype = C.c_double
+            f = getattr(_lib, f"orc_kmeans_sph_lloyd_{sfx}")
+            f.argtypes = [i, i, P, i, P, i, C.c_double, i, P, P, P, P]
+            f.restype = None
         _lib.orc_lloyd_blas_s.argtypes = [i, i, P, i, P, P, i, P, i]
         _lib.orc_lloyd_blas_s.restype = i
     return _lib
@@ -355,6 +367,57 @@ def kmeanspp(X, k, seed, cost_fp64=False, gemm=None):
     if r < 0:
         raise ValueError("kmeanspp: bad arguments")
     return chosen
+
+
+def kmeanspp_cosine(X, k, seed, normalise=True):
+    """k-means++ rows of spherical k-means (oracle_kpp.cpp; the cosine
+    distance of kmeans.cpp:1495-1510)."""
+    X = np.ascontiguousarray(X)
+    n, d = X.shape
+    chosen = np.zeros(k, dtype=np.int32)
+    r = getattr(lib(), f"orc_kmeanspp_cos_{_sfx(X.dtype)}")(n, d, _p(X), k, int(seed),
+                                                             1 if normalise else 0, _p(chosen))
+    if r < 0:
+        raise ValueError("kmeanspp_cosine: bad arguments")
+    return chosen
+
+
+def kmeans_assign_sph(X, C):
+    """Spherical assignment argmin_j -x.c_j (oracle.c) and the fp64 gap
+    between the best two values (near-tie classification)."""
+    X = np.ascontiguousarray(X)
+    C = np.ascontiguousarray(C, dtype=X.dtype)
+    n, d = X.shape
+    lab = np.zeros(n, dtype=np.int32)
+    gap = np.zeros(n, dtype=np.float64)
+    getattr(lib(), f"orc_kmeans_assign_sph_{_sfx(X.dtype)}")(n, d, _p(X), C.shape[0], _p(C),
+                                                             _p(lab), _p(gap))
+    return lab, gap
+
+
+def kmeans_inertia_sph(X, labels, C, normalise=True):
+    X = np.ascontiguousarray(X)
+    C = np.ascontiguousarray(C, dtype=X.dtype)
+    n, d = X.shape
+    return getattr(lib(), f"orc_kmeans_inertia_sph_{_sfx(X.dtype)}")(
+        n, d, _p(X), _p(np.ascontiguousarray(labels, np.int32)), _p(C), 1 if normalise else 0)
+
+
+def kmeans_sph_lloyd(X, C0, max_iter=300, tol=1e-4, normalise=True):
+    """Spherical (cosine) Lloyd from the given centres (oracle.c)."""
+    X = np.ascontiguousarray(X)
+    dt = X.dtype
+    C0 = np.ascontiguousarray(C0, dtype=dt)
+    n, d = X.shape
+    k = C0.shape[0]
+    Cout = np.zeros_like(C0)
+    lab = np.zeros(n, dtype=np.int32)
+    nit = np.zeros(1, dtype=np.int32)
+    inertia = np.zeros(1, dtype=np.float64)
+    getattr(lib(), f"orc_kmeans_sph_lloyd_{_sfx(dt)}")(n, d, _p(X), k, _p(C0), max_iter, tol,
+                                                       1 if normalise else 0, _p(Cout), _p(lab),
+                                                       _p(nit), _p(inertia))
+    return Cout, lab, int(nit[0]), float(inertia[0])
 
 
 class openblas:

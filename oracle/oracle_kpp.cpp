@@ -53,9 +53,12 @@ template <> struct Gemm<double> {
     }
 };
 
+// cosine = 1: spherical k-means (kmeans.cpp:1495-1510), the distance
+// max(0, 1 - cos) with cos = fl(fl(dot inv_i) inv_c) (normalise) or dot;
+// inv = 1 / sqrt(|x|^2), 0 for a zero row (kmeans.cpp:681-703).
 template <typename T>
 int kmeanspp(int n, int d, const T *X, int k, long long seed, int cost_fp64, void *gemm,
-             int32_t *chosen) {
+             int32_t *chosen, int cosine = 0, int normalise = 0) {
     if (n < 1 || d < 1 || k < 1 || k > n) return -1;
     std::mt19937_64 gen;
     gen.seed((uint64_t)seed);
@@ -65,6 +68,11 @@ int kmeanspp(int n, int d, const T *X, int k, long long seed, int cost_fp64, voi
         T s = T(0);
         for (int f = 0; f < d; ++f) s = fma_t(X[(size_t)i * d + f], X[(size_t)i * d + f], s);
         xn[i] = s;
+    }
+    std::vector<T> inv;
+    if (cosine && normalise) {
+        inv.resize(n);
+        for (int i = 0; i < n; ++i) inv[i] = xn[i] > T(0) ? T(1) / std::sqrt(xn[i]) : T(0);
     }
     const int n_trials = 2 + (int)std::log((double)k);
     // squared distances of every row to the candidate rows cand[0..t)
@@ -87,6 +95,11 @@ int kmeanspp(int n, int d, const T *X, int k, long long seed, int cost_fp64, voi
                     s = T(0);
                     for (int f = 0; f < d; ++f)
                         s = fma_t(X[(size_t)i * d + f], X[(size_t)cand[c] * d + f], s);
+                }
+                if (cosine) {
+                    const T cs = inv.empty() ? s : (s * inv[i]) * inv[cand[c]];
+                    out[(size_t)c * n + i] = std::max(T(0), T(1) - cs);
+                    continue;
                 }
                 const T nn = xn[i] + xn[cand[c]];
                 out[(size_t)c * n + i] = fma_t(T(-2), s, nn);
@@ -169,5 +182,14 @@ int orc_kmeanspp_s(int n, int d, const float *X, int k, long long seed, int cost
 int orc_kmeanspp_d(int n, int d, const double *X, int k, long long seed, int cost_fp64,
                    void *dgemm, int32_t *chosen) {
     return kmeanspp<double>(n, d, X, k, seed, cost_fp64, dgemm, chosen);
+}
+// Spherical k-means++ (cosine distance; normalise: the "normalize data" option).
+int orc_kmeanspp_cos_s(int n, int d, const float *X, int k, long long seed, int normalise,
+                       int32_t *chosen) {
+    return kmeanspp<float>(n, d, X, k, seed, 0, nullptr, chosen, 1, normalise);
+}
+int orc_kmeanspp_cos_d(int n, int d, const double *X, int k, long long seed, int normalise,
+                       int32_t *chosen) {
+    return kmeanspp<double>(n, d, X, k, seed, 0, nullptr, chosen, 1, normalise);
 }
 }

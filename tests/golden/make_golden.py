@@ -25,7 +25,8 @@ It converts, without retyping any value:
     n_list / n_probe / k, storage order, leading dimensions, expected
     neighbour indices and squared distances), into ann_functionality.npz;
   * the Lloyd "larger data matrix" k-means case of
-    tests/unit_tests/kmeans/kmeans_test_data.hpp:444-526 into kmeans_lloyd80.npz.
+    tests/unit_tests/kmeans/kmeans_test_data.hpp:444-526 into kmeans_lloyd80.npz;
+  * the data of the spherical k-means tests into kmeans_spherical.npz.
 The d=130 set cannot be converted: its inputs are absent from the tree.
 """
 import os
@@ -237,6 +238,37 @@ def kmeans_lloyd80():
         max_iter=np.array([30]), tol=np.array([1.0e-4]))
 
 
+def kmeans_spherical():
+    """The data of the reference's spherical k-means tests: the 20 x 3 set,
+    the unnormalised supplied centres and the empty-cluster split case of
+    tests/unit_tests/kmeans/kmeans_public.cpp:722-1200 (column-major
+    initialisers), and the 6 x 3 array of
+    python_interface/tests/kmeans_test.py:313-337.  The tests assert
+    properties only (unit-length centres, invariance to scaling the data,
+    predict / transform of scaled centres, normalise on = off for
+    normalised data, split recovery), which the fixture's users repeat."""
+    text = open(os.path.join(UT, "kmeans", "kmeans_public.cpp")).read()
+    start = text.index("TYPED_TEST(KMeansTest, SphericalKMeans)")
+    end = text.index("TYPED_TEST(", start + 10)
+    block = text[start:end]
+    a = assigned_lists(block, "A_col")[0]
+    c = assigned_lists(block, "C")[0]
+    ec_a = assigned_lists(block, "ec_A_col")[0]
+    ec_c = assigned_lists(block, "ec_C_col")[0]
+    py = open(os.path.join(REF, "python_interface", "tests", "kmeans_test.py")).read()
+    ps = py.index("def test_kmeans_spherical")
+    m = re.search(r"np\.array\(\[(.*?)\],\s*dtype", py[ps:], re.S)
+    rows = re.findall(r"\[([^\[\]]+)\]", m.group(1))
+    pa = np.array([[float(v) for v in r.split(",")] for r in rows])
+    np.savez_compressed(
+        os.path.join(OUT, "kmeans_spherical.npz"),
+        A=a.reshape(3, 20).T.copy(),             # column-major 20 x 3
+        C=c.reshape(3, 3).T.copy(),              # column-major 3 x 3 supplied centres
+        ec_A=ec_a.reshape(2, 5).T.copy(),        # column-major 5 x 2
+        ec_C=ec_c.reshape(2, 2).T.copy(),        # column-major 2 x 2
+        py_a=pa)
+
+
 if __name__ == "__main__":
     nn_large(2092, 2071, 5)
     nn_large(2125, 2068, 20)
@@ -244,6 +276,7 @@ if __name__ == "__main__":
     nn_radius_predict()
     ann_functionality()
     kmeans_lloyd80()
+    kmeans_spherical()
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))

@@ -233,3 +233,59 @@ def test_oracle_ivf_functionality_cases(orc):
         np.testing.assert_allclose(dist, wd, rtol=tol, atol=tol, err_msg=str(z["names"][i]))
         if wi is not None:
             np.testing.assert_array_equal(ind, wi, err_msg=str(z["names"][i]))
+
+
+# ----------------------------------------------------- spherical k-means --
+# The reference's spherical tests (kmeans_public.cpp:722-1200,
+# kmeans_test.py:313-337) assert properties rather than values; the oracle
+# must satisfy each of them on the same data.
+SPH_TOL = {np.float32: 1e-6, np.float64: 1e-12}
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_oracle_spherical_properties(orc, dtype):
+    z = golden("kmeans_spherical.npz")
+    A = z["A"].astype(dtype)
+    tol = SPH_TOL[dtype]
+    for C0 in (A[orc.kmeanspp_cosine(A, 3, 42)], z["C"].astype(dtype)):
+        C, lab, nit, inertia = orc.kmeans_sph_lloyd(A, C0, 300, 1e-4)
+        np.testing.assert_allclose((C.astype(np.float64) ** 2).sum(1), 1.0, atol=tol)
+        # invariance to scaling the data: identical results (power-of-two scale)
+        C2, lab2, nit2, inertia2 = orc.kmeans_sph_lloyd(2 * A, C0, 300, 1e-4)
+        np.testing.assert_array_equal(C, C2)
+        np.testing.assert_array_equal(lab, lab2)
+        assert nit == nit2 and inertia == inertia2
+        # the returned labels are the assignment to the returned centres
+        np.testing.assert_array_equal(orc.kmeans_assign_sph(A, C)[0], lab)
+        assert inertia == orc.kmeans_inertia_sph(A, lab, C)
+        # predicting 2 x the centres gives each centre (kmeans_public.cpp:873-912)
+        np.testing.assert_array_equal(orc.kmeans_assign_sph(2 * C, C)[0], np.arange(3))
+    # k-means++ on the cosine distance chooses the same rows for 2 A
+    np.testing.assert_array_equal(orc.kmeanspp_cosine(A, 3, 42), orc.kmeanspp_cosine(2 * A, 3, 42))
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_oracle_spherical_normalise_on_off(orc, dtype):
+    """Normalised data: "normalize data" yes and no give the same labels and
+    centres within the reference's tolerance (kmeans_public.cpp:980-1106)."""
+    z = golden("kmeans_spherical.npz")
+    A = z["A"].astype(dtype)
+    nrm = np.sqrt((A * A).sum(1, dtype=dtype))
+    An = (A * (1 / nrm)[:, None]).astype(dtype)
+    tol = SPH_TOL[dtype]
+    C0 = An[orc.kmeanspp_cosine(An, 3, 42)]
+    Con, lon, _, _ = orc.kmeans_sph_lloyd(An, C0, 300, 1e-4, normalise=True)
+    Coff, loff, _, _ = orc.kmeans_sph_lloyd(An, C0, 300, 1e-4, normalise=False)
+    np.testing.assert_array_equal(lon, loff)
+    np.testing.assert_allclose(Con, Coff, atol=tol)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_oracle_spherical_python_case(orc, dtype):
+    """kmeans_test.py:313-337: 6 x 3, two clusters, data used as given."""
+    a = golden("kmeans_spherical.npz")["py_a"].astype(dtype)
+    C0 = a[orc.kmeanspp_cosine(a, 2, 42, normalise=False)]
+    C, lab, nit, _ = orc.kmeans_sph_lloyd(a, C0, 300, 1e-4, normalise=False)
+    np.testing.assert_allclose(np.linalg.norm(C.astype(np.float64), axis=1), 1.0,
+                               atol=SPH_TOL[dtype])
+    assert set(lab) <= {0, 1}
