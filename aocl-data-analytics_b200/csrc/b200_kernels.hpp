@@ -262,17 +262,21 @@ cudaError_t launch_kmeans_finalize_shards(int k, int d, int ld, const long long 
 cudaError_t ensure_smem_limit(const void *func, size_t smem);
 
 // ------------------------------------------------------------ IVF-flat ---
-// Scan of the probed inverted lists (squared GEMM-form distances, exact
-// top-k in (distance, global index) order).  X: list-ordered rows (ld a
-// multiple of 4), xn their squared norms, gid their global indices, loff the
-// n_list + 1 row offsets of the lists; probe: n_probe list ids per query.
-// Outputs q-major (q * k + r): index -1 / distance +inf for empty slots,
-// square root of non-negative values when take_sqrt.
+// Scan of the probed inverted lists (exact top-k in (key, global index)
+// order).  X: list-ordered rows (ld a multiple of 4), xn their squared norms,
+// gid their global indices, loff the n_list + 1 row offsets of the lists;
+// probe: n_probe list ids per query.  The key and the output distance by
+// `out`: IVF_OUT_SQ / IVF_OUT_SQRT the GEMM-form squared distance (its
+// square root where non-negative), IVF_OUT_IP key -q.x and distance q.x,
+// IVF_OUT_COS key -q.x and distance 1 - q.x (rows and queries normalised).
+// Outputs q-major (q * k + r): index -1 and the distance of an infinite key
+// (+inf; -inf for the inner product) for empty slots.
+enum { IVF_OUT_SQ = 0, IVF_OUT_SQRT = 1, IVF_OUT_IP = 2, IVF_OUT_COS = 3 };
 size_t ivf_scan_smem(int k, bool fp64);
 template <typename T>
 cudaError_t launch_ivf_scan(const T *Q, const T *qn, int ld, int nq, const int *probe,
                             int n_probe, const long long *loff, const T *X, const T *xn,
-                            const int *gid, int k, int take_sqrt, T *out_d, int *out_i,
+                            const int *gid, int k, int out, T *out_d, int *out_i,
                             cudaStream_t s);
 // Squared row norms of the centres (sequential fma chain over features).
 template <typename T>

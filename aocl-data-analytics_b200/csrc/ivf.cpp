@@ -65,14 +65,50 @@ da_status IVF<T>::set_training_data(da_int n, da_int d, const T *X, da_int ldx) 
     return da_status_success;
 }
 
+// Rows scaled to unit length in place (normalize_rows of da_utils.cpp:
+// 807-905): the sum of squares accumulated feature by feature in T, factor
+// 1 / sqrt (1 for a zero row).  X: rows x d with leading dimension ld in the
+// given storage order.
+template <typename T>
+static void normalise_rows(bool cm, da_int rows, da_int d, T *X, da_int ld) {
+    for (da_int i = 0; i < rows; ++i) {
+        T s = T(0);
+        for (da_int j = 0; j < d; ++j) {
+            const T v = X[cm ? i + (size_t)j * ld : (size_t)i * ld + j];
+            s += v * v;
+        }
+        const T nrm = std::sqrt(s);
+        const T r = nrm == T(0) ? T(1) : T(1) / nrm;
+        for (da_int j = 0; j < d; ++j) X[cm ? i + (size_t)j * ld : (size_t)i * ld + j] *= r;
+    }
+}
+
+// A normalised copy of rows x d (leading dimension ldx) in the same storage
+// order with leading dimension rows (column-major) or d (row-major).
+template <typename T>
+static std::vector<T> normalised_copy(bool cm, da_int rows, da_int d, const T *X, da_int ldx,
+                                      da_int &ld_out) {
+    ld_out = cm ? rows : d;
+    std::vector<T> out((size_t)rows * d);
+    for (da_int i = 0; i < rows; ++i)
+        for (da_int j = 0; j < d; ++j)
+            out[cm ? i + (size_t)j * ld_out : (size_t)i * ld_out + j] =
+                X[cm ? i + (size_t)j * ldx : (size_t)i * ldx + j];
+    normalise_rows(cm, rows, d, out.data(), ld_out);
+    return out;
+}
+
 // The coarse quantiser's kNN handle: the centroids as its training rows,
 // squared GEMM-form distances (the reference's euclidean_gemm_distance of the
-// coarse step, approximate_neighbors.cpp:660-680, 1098-1104), ties to the
-// lower centroid (its first-minimum / strict-< heap rules).
+// coarse step, approximate_neighbors.cpp:660-680, 1098-1104) or, for the
+// inner-product and cosine indexes, the key -q.c (the GEMMs with alpha = -1
+// of :712-727, 1094-1100), ties to the lower centroid (its first-minimum /
+// strict-< heap rules).
 template <typename T> da_status IVF<T>::make_coarse() {
     coarse.reset(new NN<T>(err, cuda, opts.single));
     auto &o = coarse->opts;
-    if (o.set_string("metric", "sqeuclidean_gemm") != da_status_success ||
+    const bool sph = metric == AM_IP || metric == AM_COS;
+    if (o.set_string("metric", sph ? "inner product" : "sqeuclidean_gemm") != da_status_success ||
         o.set_string("algorithm", "brute") != da_status_success ||
         o.set_string("precision mode", "plain") != da_status_success ||
         o.set_string("storage order", "row-major") != da_status_success)
@@ -100,11 +136,6 @@ template <typename T> da_status IVF<T>::train() {
         return err->error(da_status_invalid_array_dimension,
                           "n_samples = " + std::to_string(n_samples) +
                               " must be at least as large as n_list = " + std::to_string(n_list));
-    if (metric == AM_IP || metric == AM_COS)
-        return err->error(da_status_not_implemented,
-                          "The inner product and cosine metrics of the IVF-flat index (spherical "
-                          "k-means) are not provided by the B200 library; use euclidean or "
-                          "sqeuclidean.");
     internal_seed = seed;
     if (internal_seed == -1) {
         std::random_device rd;
@@ -135,6 +166,17 @@ template <typename T> da_status IVF<T>::train() {
                     X_train[cm ? perm[i] + (size_t)j * ldx_train : (size_t)perm[i] * ldx_train + j];
         tp = Xs.data();
     }
+    // the inner-product and cosine indexes quantise with spherical k-means on
+    // the rows as given, normalised first for cosine (:368-456)
+    const bool sph = metric == AM_IP || metric == AM_COS;
+    if (metric == AM_COS) {
+        if (Xs.empty()) {
+            Xs = normalised_copy(cm, n_train, n_features, tp, tld, tld);
+        } else {
+            normalise_rows(cm, n_train, n_features, Xs.data(), tld);
+        }
+        tp = Xs.data();
+    }
     KMeans<T> km(err, cuda, opts.single);
     auto &o = km.opts;
     if (o.set_int("n_clusters", n_list) != da_status_success ||
@@ -145,7 +187,9 @@ template <typename T> da_status IVF<T>::train() {
         o.set_string("algorithm", "lloyd") != da_status_success ||
         o.set_string("storage order", cm ? "column-major" : "row-major") != da_status_success ||
         o.set_real("convergence tolerance", std::sqrt(std::numeric_limits<T>::epsilon())) !=
-            da_status_success)
+            da_status_success ||
+        (sph && (o.set_string("distance", "cosine") != da_status_success ||
+                 o.set_string("normalize data", "no") != da_status_success)))
         return err->error(da_status_internal_error, "Could not configure the coarse k-means.");
     da_status s = km.set_data(n_train, n_features, tp, tld);
     if (s != da_status_success) return s;
@@ -189,10 +233,17 @@ template <typename T> da_status IVF<T>::add(da_int n, da_int d, const T *X, da_i
                           "The function was called with n_features = " + std::to_string(d) +
                               " but the index has been trained with " +
                               std::to_string(n_features) + " features.");
+    const bool cm = ord == column_major;
+    // cosine: the rows are normalised before they are assigned and stored
+    // (approximate_neighbors.cpp:577-598)
+    std::vector<T> Xn;
+    if (metric == AM_COS) {
+        Xn = normalised_copy(cm, n, d, X, ldx, ldx);
+        X = Xn.data();
+    }
     std::vector<da_int> near;
     s = coarse->kneighbors_compute(n, d, X, ldx, ord, 1, near, nullptr);
     if (s != da_status_success) return s;
-    const bool cm = ord == column_major;
     for (da_int i = 0; i < n; ++i) {
         const da_int c = near[i];
         auto &rows = list_rows[c];
@@ -300,6 +351,12 @@ da_status IVF<T>::kneighbors(da_int nq, da_int d, const T *Xt, da_int ldt, da_in
         return err->error(da_status_not_implemented,
                           "k = " + std::to_string(k) +
                               " exceeds the on-chip top-k of the B200 IVF-flat search.");
+    // cosine: the queries are normalised first (approximate_neighbors.cpp:1066-1080)
+    std::vector<T> Qn;
+    if (metric == AM_COS) {
+        Qn = normalised_copy(ord == column_major, nq, d, Xt, ldt, ldt);
+        Xt = Qn.data();
+    }
     std::vector<da_int> probe;
     s = coarse->kneighbors_compute(nq, d, Xt, ldt, ord, n_probe, probe, nullptr);
     if (s != da_status_success) return s;
@@ -322,7 +379,11 @@ da_status IVF<T>::kneighbors(da_int nq, da_int d, const T *Xt, da_int ldt, da_in
     B200_TRY(cuda->timed("ivf_scan", [&] {
         return launch_ivf_scan<T>(dQ.as<T>(), dQn.as<T>(), ld, (int)nq, dProbe.as<int>(),
                                   (int)n_probe, dOff.as<long long>(), dX.as<T>(), dXn.as<T>(),
-                                  dGid.as<int>(), (int)k, metric == AM_EUC ? 1 : 0,
+                                  dGid.as<int>(), (int)k,
+                                  metric == AM_EUC   ? IVF_OUT_SQRT
+                                  : metric == AM_IP  ? IVF_OUT_IP
+                                  : metric == AM_COS ? IVF_OUT_COS
+                                                     : IVF_OUT_SQ,
                                   dOutD.as<T>(), dOutI.as<int>(), st);
     }), "list scan");
     std::vector<int> oi(nk);
@@ -461,7 +522,7 @@ template <typename T> da_status IVF<T>::load_state(ByteReader &r) {
         sizes.size() != (size_t)nl || cen.size() / (size_t)nl != (size_t)d ||
         cen.size() != (size_t)nl * (size_t)d || ids.size() != norms.size() ||
         rows.size() / (size_t)d != ids.size() || rows.size() != ids.size() * (size_t)d ||
-        (me != AM_EUC && me != AM_SQEUC))
+        me < AM_EUC || me > AM_COS)
         return bad();
     // list sizes: each within the listed rows before it is added (no overflow)
     int64_t total = 0;

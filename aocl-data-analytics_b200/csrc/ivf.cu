@@ -1,6 +1,7 @@
 // IVF-flat inverted-list scan (approximate_neighbors.cpp:971-1191): for every
-// query, the GEMM-form squared distances |q|^2 + |v|^2 - 2 q.v to the vectors
-// of its n_probe probed lists, and the k smallest of them.
+// query, the GEMM-form squared distances |q|^2 + |v|^2 - 2 q.v (or, for the
+// inner-product and cosine indexes, -q.v) to the vectors of its n_probe
+// probed lists, and the k smallest of them.
 //
 // One CTA per query.  The probed lists are contiguous row ranges of the
 // list-ordered index (rows padded to a multiple of 4 elements, so every row
@@ -11,6 +12,7 @@
 // lexicographically, so the result is exact and deterministic: the k smallest
 // distances over the probed lists, equal distances in index order.
 #include "b200_common.cuh"
+#include "b200_kernels.hpp"
 
 namespace b200 {
 
@@ -46,7 +48,7 @@ __global__ void __launch_bounds__(IVF_THREADS)
 ivf_scan_kernel(const T *__restrict__ Q, const T *__restrict__ qn, int ld, int nq,
                 const int *__restrict__ probe, int n_probe, const long long *__restrict__ loff,
                 const T *__restrict__ X, const T *__restrict__ xn, const int *__restrict__ gid,
-                int k, int take_sqrt, T *__restrict__ out_d, int *__restrict__ out_i) {
+                int k, int out, T *__restrict__ out_d, int *__restrict__ out_i) {
     using V = typename V16<T>::V;
     extern __shared__ __align__(16) unsigned char ivf_smem[];
     T *Ld = reinterpret_cast<T *>(ivf_smem); // current top-k, ascending
@@ -90,7 +92,8 @@ ivf_scan_kernel(const T *__restrict__ Q, const T *__restrict__ qn, int ld, int n
                     acc += __shfl_xor_sync(0xffffffffu, acc, 2);
                     if (lane == 0) {
                         if (valid) {
-                            Bd[c] = add_rn(add_rn(qq, xn[b0 + c]), T(-2) * acc);
+                            Bd[c] = out >= IVF_OUT_IP ? -acc
+                                                      : add_rn(add_rn(qq, xn[b0 + c]), T(-2) * acc);
                             Bi[c] = gid[b0 + c];
                         } else {
                             Bd[c] = inf;
@@ -152,12 +155,15 @@ ivf_scan_kernel(const T *__restrict__ Q, const T *__restrict__ qn, int ld, int n
                 __syncthreads();
             }
         }
-        // empty slots: index -1, distance +inf; euclidean: the square root of
-        // non-negative values (approximate_neighbors.cpp:1292-1299)
+        // empty slots: index -1, key +inf; euclidean: the square root of
+        // non-negative values; inner product: -key; cosine: 1 + key
+        // (approximate_neighbors.cpp:1287-1312)
         for (int r = tid; r < k; r += IVF_THREADS) {
             const int i = Li[r];
             T d = i == IVF_NOID ? inf : Ld[r];
-            if (take_sqrt && d >= T(0)) d = sqrt_rn(d);
+            if (out == IVF_OUT_SQRT && d >= T(0)) d = sqrt_rn(d);
+            else if (out == IVF_OUT_IP) d = -d;
+            else if (out == IVF_OUT_COS) d = add_rn(T(1), d);
             out_d[(size_t)q * k + r] = d;
             out_i[(size_t)q * k + r] = i == IVF_NOID ? -1 : i;
         }
@@ -175,7 +181,7 @@ size_t ivf_scan_smem(int k, bool fp64) {
 template <typename T>
 cudaError_t launch_ivf_scan(const T *Q, const T *qn, int ld, int nq, const int *probe,
                             int n_probe, const long long *loff, const T *X, const T *xn,
-                            const int *gid, int k, int take_sqrt, T *out_d, int *out_i,
+                            const int *gid, int k, int out, T *out_d, int *out_i,
                             cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
     if (ld % 4 != 0 || k < 1) return cudaErrorInvalidValue;
@@ -184,7 +190,7 @@ cudaError_t launch_ivf_scan(const T *Q, const T *qn, int ld, int nq, const int *
     if (e != cudaSuccess) return e;
     const int grid = nq < 148 * 64 ? nq : 148 * 64;
     ivf_scan_kernel<T><<<grid, IVF_THREADS, smem, s>>>(Q, qn, ld, nq, probe, n_probe, loff, X,
-                                                        xn, gid, k, take_sqrt, out_d, out_i);
+                                                        xn, gid, k, out, out_d, out_i);
     return cudaGetLastError();
 }
 

@@ -56,6 +56,8 @@ def lib():
         _lib.orc_knn_reference_ties_d.argtypes = [i, P, i, P]
         _lib.orc_knn_reference_ties_d.restype = None
         _lib.orc_num_threads.restype = i
+        _lib.orc_random_rows.argtypes = [i, i, C.c_longlong, P]
+        _lib.orc_random_rows.restype = i
         for sfx in ("s", "d"):
             f = getattr(_lib, f"orc_kmeanspp_{sfx}")
             f.argtypes = [i, i, P, i, C.c_longlong, i, P, P]
@@ -253,22 +255,73 @@ def _gemm_sq(A, B):
     return (A * A).sum(1)[:, None] + (B * B).sum(1)[None, :] - 2.0 * A @ B.T
 
 
-def ivf_lists(C, X):
+SPHERICAL_METRICS = ("inner product", "cosine")
+
+
+def _ivf_key(A, B, metric):
+    """The IVF-flat ranking key: the GEMM-form squared distance, or -a.b for
+    the inner-product and cosine metrics (the GEMMs with alpha = -1 of
+    approximate_neighbors.cpp:712-727, 1094-1100, 1148-1154).  fp64."""
+    if metric in SPHERICAL_METRICS:
+        return -(np.asarray(A, dtype=np.float64) @ np.asarray(B, dtype=np.float64).T)
+    return _gemm_sq(A, B)
+
+
+def normalise_rows(X):
+    """normalize_rows of utilities/da_utils.cpp:858-905 in the working
+    precision: the row's sum of squares accumulated feature by feature
+    (v * v rounded, then added), norm = sqrt, factor 1 / norm (1 for a zero
+    row), every element times the factor."""
+    X = np.asarray(X)
+    dt = X.dtype.type
+    s = np.zeros(X.shape[0], dtype=X.dtype)
+    for f in range(X.shape[1]):
+        s = s + X[:, f] * X[:, f]
+    nrm = np.sqrt(s)
+    inv = np.where(nrm == 0, dt(1), dt(1) / np.where(nrm == 0, dt(1), nrm)).astype(X.dtype)
+    return (X * inv[:, None]).astype(X.dtype)
+
+
+def random_rows(n, k, seed):
+    """The random-samples initial rows of k-means (oracle_kpp.cpp)."""
+    out = np.zeros(min(k, n), dtype=np.int32)
+    lib().orc_random_rows(n, k, int(seed), _p(out))
+    return out
+
+
+def ivf_train_spherical(X, n_list, seed, max_iter, metric):
+    """The coarse quantiser of the inner-product / cosine index
+    (approximate_neighbors.cpp:368-478): the training rows (normalised for
+    cosine), random-samples initial centres, spherical Lloyd on the rows as
+    given ("normalize data" off), tolerance sqrt(eps).  Returns the
+    centroids (n_list x d)."""
+    X = np.ascontiguousarray(X)
+    Xt = normalise_rows(X) if metric == "cosine" else X
+    C0 = Xt[random_rows(len(X), n_list, seed)]
+    tol = float(np.sqrt(np.finfo(X.dtype).eps))
+    C, _, _, _ = kmeans_sph_lloyd(Xt, C0, max_iter, tol, normalise=False)
+    return C
+
+
+def ivf_lists(C, X, metric="sqeuclidean"):
     """add_ivfflat (approximate_neighbors.cpp:565-842): every row joins the
     list of its nearest centroid (first minimum), after the rows already
-    there.  Returns the list of every row."""
-    return np.argmin(_gemm_sq(X, C), axis=1).astype(np.int32)
+    there.  Returns the list of every row (X normalised by the caller for
+    cosine)."""
+    return np.argmin(_ivf_key(X, C, metric), axis=1).astype(np.int32)
 
 
 def ivf_kneighbors(C, X, Q, k, n_probe, metric="sqeuclidean", lists=None):
     """IVF-flat search (approximate_neighbors.cpp:971-1344): per query the
     n_probe nearest centroids (lower index on ties), then the k nearest index
-    rows of those lists in (distance, index) order; index -1 / distance +inf
-    where the lists hold fewer than k rows; euclidean returns the square root
-    of non-negative values.  Distances in fp64.  Returns (ind, dist, probes),
-    q-major."""
-    lists = ivf_lists(C, X) if lists is None else lists
-    dc = _gemm_sq(Q, C)
+    rows of those lists in (key, index) order; index -1 / distance +inf
+    (-inf for the inner product) where the lists hold fewer than k rows;
+    euclidean returns the square root of non-negative values, inner product
+    the dot (-key), cosine 1 + key (X and Q normalised by the caller for
+    cosine).  Distances in fp64.
+    Returns (ind, dist, probes), q-major."""
+    lists = ivf_lists(C, X, metric) if lists is None else lists
+    dc = _ivf_key(Q, C, metric)
     nq = len(Q)
     ind = np.full((nq, k), -1, dtype=np.int32)
     dist = np.full((nq, k), np.inf)
@@ -279,13 +332,17 @@ def ivf_kneighbors(C, X, Q, k, n_probe, metric="sqeuclidean", lists=None):
         rows = np.nonzero(np.isin(lists, pr))[0]
         if len(rows) == 0:
             continue
-        dq = _gemm_sq(Q[q:q + 1], X[rows])[0]
+        dq = _ivf_key(Q[q:q + 1], X[rows], metric)[0]
         o = np.lexsort((rows, dq))[:k]
         ind[q, :len(o)] = rows[o]
         dist[q, :len(o)] = dq[o]
     if metric == "euclidean":
         pos = dist >= 0
         dist[pos] = np.sqrt(dist[pos])
+    if metric == "inner product":   # empty slots: -inf, as the reference's scaling by -1
+        dist = -dist
+    elif metric == "cosine":
+        dist = 1.0 + dist
     return ind, dist, probes
 
 

@@ -24,6 +24,7 @@
 // as GCC contracts it (one fma per feature).  The candidate cost accumulates
 // in the working precision T, serially, as the reference does; cost_fp64 = 1
 // accumulates in fp64 instead (to classify a disagreement).
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <limits>
@@ -191,5 +192,27 @@ int orc_kmeanspp_cos_s(int n, int d, const float *X, int k, long long seed, int 
 int orc_kmeanspp_cos_d(int n, int d, const double *X, int k, long long seed, int normalise,
                        int32_t *chosen) {
     return kmeanspp<double>(n, d, X, k, seed, 0, nullptr, chosen, 1, normalise);
+}
+}
+
+extern "C" {
+// Random-samples initialisation (kmeans.cpp:1403-1424 with da_std::sample,
+// utilities/da_std.hpp:102-118): selection sampling over the rows 0..n-1,
+// std::mt19937_64 seeded with `seed`, one std::uniform_int_distribution over
+// [0, remaining - 1] per row visited (da_int = 32-bit).  Writes min(k, n)
+// row indices in increasing order.
+int orc_random_rows(int n, int k, long long seed, int32_t *out) {
+    if (n < 1 || k < 1) return -1;
+    std::mt19937_64 gen;
+    gen.seed((uint64_t)seed);
+    int32_t need = std::min(k, n), pop = n, m = 0;
+    for (int32_t i = 0; need > 0; ++i, --pop) {
+        std::uniform_int_distribution<int32_t> d(0, pop - 1);
+        if (d(gen) < need) {
+            out[m++] = i;
+            --need;
+        }
+    }
+    return m;
 }
 }

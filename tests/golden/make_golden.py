@@ -23,7 +23,9 @@ It converts, without retyping any value:
   * the squared-euclidean functionality cases of the IVF-flat tests
     (tests/unit_tests/approximate_neighbors/ann_tests.hpp:395-1260: data,
     n_list / n_probe / k, storage order, leading dimensions, expected
-    neighbour indices and squared distances), into ann_functionality.npz;
+    neighbour indices and squared distances), into ann_functionality.npz,
+    and its inner-product and cosine cases (with their metric) into
+    ann_functionality_spherical.npz;
   * the Lloyd "larger data matrix" k-means case of
     tests/unit_tests/kmeans/kmeans_test_data.hpp:444-526 into kmeans_lloyd80.npz;
   * the data of the spherical k-means tests into kmeans_spherical.npz.
@@ -178,9 +180,9 @@ def nn_radius_predict():
     np.savez_compressed(os.path.join(OUT, "nn_radius_predict.npz"), **out)
 
 
-def ann_functionality():
+def ann_functionality(metrics=("sqeuclidean",), fname="ann_functionality.npz"):
     text = open(os.path.join(UT, "approximate_neighbors", "ann_tests.hpp")).read()
-    out, names = {}, []
+    out, names, mets = {}, [], []
     for m in re.finditer(r"template <typename T> void (\w+)\(std::vector<ANNParamType<T>> &params\) \{",
                          text):
         body = text[m.end():]
@@ -189,7 +191,7 @@ def ann_functionality():
         body = body[:body.index("params.push_back(test);")]
         ctor = re.search(r'ANNParamType<T> test\((\d+), (\d+), (\d+), "([^"]+)", "([^"]+)", "([^"]+)"\)',
                          body)
-        if ctor is None or ctor.group(4) != "sqeuclidean":
+        if ctor is None or ctor.group(4) not in metrics:
             continue
         nlist, nprobe, k = (int(ctor.group(i)) for i in (1, 2, 3))
         vals = {"n_features": None, "n_samples": None, "n_queries": None, "ldx_train": None,
@@ -206,6 +208,7 @@ def ann_functionality():
             continue
         i = len(names)
         names.append(m.group(1))
+        mets.append(ctor.group(4))
         row = ctor.group(6) == "row-major"
         out[f"c{i}_meta"] = np.array([nlist, nprobe, k, vals["n_features"], vals["n_samples"],
                                       vals["n_queries"], vals["ldx_train"], vals["ldx_test"],
@@ -217,7 +220,9 @@ def ann_functionality():
         if lists["expected_kind"]:
             out[f"c{i}_kind"] = lists["expected_kind"][0].astype(np.int32)
     out["names"] = np.array(names)
-    np.savez_compressed(os.path.join(OUT, "ann_functionality.npz"), **out)
+    if metrics != ("sqeuclidean",):
+        out["metrics"] = np.array(mets)
+    np.savez_compressed(os.path.join(OUT, fname), **out)
 
 
 def kmeans_lloyd80():
@@ -275,6 +280,7 @@ if __name__ == "__main__":
     nn_small()
     nn_radius_predict()
     ann_functionality()
+    ann_functionality(("inner product", "cosine"), "ann_functionality_spherical.npz")
     kmeans_lloyd80()
     kmeans_spherical()
     for f in sorted(os.listdir(OUT)):

@@ -4,7 +4,7 @@ any device work, with the reference's statuses (approximate_neighbors.cpp:
 import numpy as np
 import pytest
 
-NOT_IMPLEMENTED, INVALID_HANDLE_TYPE, WRONG_TYPE, INVALID_DIM, NO_DATA = 5, 9, 7, 17, 20
+INVALID_HANDLE_TYPE, WRONG_TYPE, INVALID_DIM, NO_DATA = 9, 7, 17, 20
 
 
 def test_ivf_argument_checks(ab):
@@ -27,14 +27,6 @@ def test_ivf_argument_checks(ab):
         b.train()
     assert e.value.status == INVALID_DIM
     b.close()
-    # spherical k-means metrics are not provided
-    for m in ("cosine", "inner product"):
-        c = ab.ApproxNN("d", metric=m, n_list=2)
-        c.set_training_data(X)
-        with pytest.raises(ab.DAError) as e:
-            c.train()
-        assert e.value.status == NOT_IMPLEMENTED
-        c.close()
     # a kNN handle is not an IVF handle
     nn = ab.KNN("d")
     assert L.da_approx_nn_train_d(nn.h) == INVALID_HANDLE_TYPE

@@ -289,3 +289,26 @@ def test_oracle_spherical_python_case(orc, dtype):
     np.testing.assert_allclose(np.linalg.norm(C.astype(np.float64), axis=1), 1.0,
                                atol=SPH_TOL[dtype])
     assert set(lab) <= {0, 1}
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_oracle_ivf_spherical_cases(orc, dtype):
+    """The reference's inner-product and cosine IVF-flat functionality cases
+    (ann_tests.hpp): spherical k-means coarse quantiser from the seeded
+    random rows, lists by -x.c, the probed lists' k best rows.  The outlier
+    cases' expectations depend on the trained lists (the unprobed list holds
+    the rows with the largest inner products)."""
+    z = golden("ann_functionality_spherical.npz")
+    for i, name in enumerate(z["names"]):
+        metric = str(z["metrics"][i])
+        o, X, Q, wi, wd = ann_case(z, i)
+        X, Q = X.astype(dtype), Q.astype(dtype)
+        C = orc.ivf_train_spherical(X, o["n_list"], o["seed"], o["kmeans_iter"], metric)
+        if metric == "cosine":
+            X, Q = orc.normalise_rows(X), orc.normalise_rows(Q)
+        ind, dist, _ = orc.ivf_kneighbors(C.astype(np.float64), X, Q, o["k"], o["n_probe"],
+                                          metric)
+        tol = 3000 * np.finfo(dtype).eps
+        np.testing.assert_allclose(dist, wd, rtol=tol, atol=tol, err_msg=str(name))
+        if wi is not None:
+            np.testing.assert_array_equal(ind, wi, err_msg=str(name))
