@@ -305,6 +305,16 @@ template <typename T> struct IVF : public AlgBase {
 
 } // namespace b200
 
+namespace b200 {
+// Model files of AOCL-DA's own da_handle_save_model (ref_model.cpp): the
+// test for its keyword, and a new handle of the file's type and precision
+// (created by handle_init) holding its options and trained state.
+bool is_reference_model(const char *p, size_t n);
+da_status load_reference_model(const char *p, size_t n, da_handle *out,
+                               da_status (*handle_init)(da_handle *, da_handle_type,
+                                                        da_precision));
+} // namespace b200
+
 // The opaque handle of the C ABI (source/include/aoclda_handle.h:98).
 struct _da_handle {
     da_precision precision = da_unknown;

@@ -344,6 +344,9 @@ da_status da_handle_load_model(da_handle *handle, const char *file_name) {
         std::fclose(f);
         if (bad) return da_status_io_error;
     }
+    // a file of AOCL-DA's own da_handle_save_model (ref_model.cpp)
+    if (is_reference_model(buf.data(), buf.size()))
+        return load_reference_model(buf.data(), buf.size(), handle, handle_init);
     const size_t head = sizeof(kModelMagic) + 4 + 4 + 4;
     if (buf.size() < head + 8 || std::memcmp(buf.data(), kModelMagic, sizeof(kModelMagic)) != 0)
         return da_status_invalid_file_data;

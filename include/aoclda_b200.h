@@ -167,9 +167,12 @@ void da_handle_refresh(da_handle handle);
  * checksum), not the reference's. */
 da_status da_handle_save_model(da_handle handle, const char *file_name);
 /* source/include/aoclda_handle.h:201 -- a new handle (*handle must be null)
- * from a file written by da_handle_save_model: da_status_io_error when it
- * cannot be read, da_status_invalid_file_data when it is not a model file or
- * is corrupted, da_status_version_mismatch for another format version. */
+ * from a file written by da_handle_save_model -- this library's, or
+ * AOCL-DA's own format (utilities/model_persistence.cpp) for k-means, kNN and
+ * IVF-flat models: da_status_io_error when it cannot be read,
+ * da_status_invalid_file_data when it is not a model file or is corrupted,
+ * da_status_version_mismatch for another format version,
+ * da_status_not_implemented for an AOCL-DA model of another handle type. */
 da_status da_handle_load_model(da_handle *handle, const char *file_name);
 
 /* ======================================================================== */
