@@ -237,13 +237,25 @@ struct LloydLoopState {
 // integer arithmetic: the same sums as a recount), else recounted over all
 // rows.  The finalize re-arms the iteration's counters: flags[0..1],
 // rearm[0] and rearm[2] (the relabel list's counts), chg.count.
+//
+// amb: the rows the tensor-core pass left uncertified (at most KM_AMB_MAXC
+// candidate clusters each, or none: scan every cluster); they get their exact
+// fp32 labels here (the plain path's fma order against the centres C and
+// their norms cnorm), in the same launch as the delta update.  recount: one
+// int the launch sets to 1 when the sums are recounted instead (the changed
+// certified rows plus the listed rows exceed chg.cap).
+struct AmbList {
+    const int *rows = nullptr, *cand = nullptr, *ncand = nullptr, *count = nullptr;
+};
+constexpr int KM_AMB_MAXC = 4; // candidate clusters kept per uncertified row
 cudaError_t launch_kmeans_update_fx_loop(const float *X, int ld, int n, int d, int k,
-                                         const int *labels, const float *scale,
+                                         int *labels, const float *scale,
                                          const double *inv_scale, void *accum, float *C,
                                          int *counts, double *block_partials, double *scalars,
                                          int *flags, unsigned *ticket, LloydLoopState *ls,
                                          unsigned long long cond, const ChangeList &chg,
-                                         int *rearm, cudaStream_t s);
+                                         int *rearm, const float *cnorm, const AmbList &amb,
+                                         int *recount, cudaStream_t s);
 // One shard's share of a data set split across processes, packed for one
 // integer all-reduce: acc[0, k*d) the fixed-point sums (two's complement,
 // from zero), acc[k*d, k*d+k) the counts, acc[k*d+k] = (*changed != 0).

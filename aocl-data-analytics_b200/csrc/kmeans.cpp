@@ -591,6 +591,9 @@ template <typename T> da_status KMeans<T>::assign(const T *dC, int *dL, const in
                                                dFlags.as<int>(), amb_rows, amb_cand, amb_ncand,
                                                amb_cnt, errf, chg, st, sph ? SPH_CMAX_SQ : 0.f);
             }), "tensor-core assign");
+            // the graph loop re-scores the listed rows in its update launch
+            // (fx_rescore_delta_kernel)
+            if (chg_capture) return da_status_success;
             B200_TRY(cuda->timed("kmeans_rescore", [&] {
                 return launch_kmeans_rescore(dX.as<float>(), ld, d, dC, k, dCn.as<float>(),
                                              amb_rows, amb_cand, amb_ncand, amb_cnt, n, dL,
@@ -815,13 +818,19 @@ template <typename T> bool KMeans<T>::build_loop_graph(T *dC, int *dL) {
             chg.news = chg.olds + chg_cap;
             chg.cap = chg_cap;
             const double *scale = dFxScale.as<double>();
+            AmbList amb;
+            amb.rows = dAmb.as<int>();
+            amb.ncand = amb.rows + n;
+            amb.cand = amb.rows + 2 * (size_t)n;
+            amb.count = reinterpret_cast<const int *>(dTcScal.as<char>() + 16);
             launched = launched &&
                        launch_kmeans_update_fx_loop(
                            dX.as<float>(), ld, n, d, k, dL, reinterpret_cast<const float *>(scale),
                            scale + d, dFxAcc.p, dC, dCounts.as<int>(), dScalars.as<double>() + 8,
                            dScalars.as<double>(), dFlags.as<int>(), dFxTicket.as<unsigned>(),
                            dLoop.as<LloydLoopState>(), (unsigned long long)cond, chg,
-                           reinterpret_cast<int *>(dTcScal.as<char>() + 16), st) == cudaSuccess;
+                           reinterpret_cast<int *>(dTcScal.as<char>() + 16), dCn.as<float>(), amb,
+                           chg.news + chg_cap, st) == cudaSuccess;
             cudaGraph_t captured = nullptr;
             const bool ended = cudaStreamEndCapture(st, &captured) == cudaSuccess;
             ok = launched && ended;
@@ -855,7 +864,8 @@ da_status KMeans<T>::lloyd_graph(T *dC, int *dL, da_int &n_iter_out, int &conver
         if (!dLoop.ensure(sizeof(LloydLoopState))) return da_status_success;
         // changed-row list: up to n / 16 rows (more: the update recounts)
         chg_cap = (int)std::min<da_int>(n_samples, std::max<da_int>(8192, n_samples / 16));
-        if (!dChg.ensure((size_t)(3 * (size_t)chg_cap + 1) * sizeof(int))) return da_status_success;
+        // [count][rows][olds][news][recount word]
+        if (!dChg.ensure((size_t)(3 * (size_t)chg_cap + 2) * sizeof(int))) return da_status_success;
         const std::vector<uintptr_t> key = {
             (uintptr_t)st, (uintptr_t)dC, (uintptr_t)dL, (uintptr_t)dX.p, (uintptr_t)dCn.p,
             (uintptr_t)dFlags.p, (uintptr_t)dFxAcc.p, (uintptr_t)dFxScale.p,

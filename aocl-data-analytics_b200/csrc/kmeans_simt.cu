@@ -775,7 +775,8 @@ __global__ void __launch_bounds__(FX_THREADS, 1)
 fx_update_kernel(const float *X, int ld, int n, int d, int k, const int *labels,
                  const float *scale, unsigned long long *gsum, int *gcnt, int sub_w,
                  const int *gate, int gate_max) {
-    // the delta update handles short change lists (fx_delta_kernel)
+    // skipped when the gate word is at most gate_max (the graph loop's
+    // delta update kept the sums up to date: fx_rescore_delta_kernel)
     if (gate && *gate <= gate_max) return;
     extern __shared__ __align__(16) unsigned char fx_smem[];
     unsigned long long *acc = reinterpret_cast<unsigned long long *>(fx_smem);
@@ -924,30 +925,168 @@ static void fx_launch(const float *X, int ld, int n, int d, int k, const int *la
                                                           counts, sub_w, gate, gate_max);
 }
 
-// Bring the running sums up to date from the change list (when it holds
-// every changed row, *count <= cap): one warp per changed row moves the
-// row's fixed-point features q = round-to-nearest-even(x * 2^s_f) -- the
-// value fx_acc adds -- from its old cluster to its new one, and one count.
-// Integer additions in any order: the sums equal a recount's.  With a longer
-// list the sums and counts are cleared instead, for the recount that follows.
+
+// The graph loop's exact re-score and delta update in one launch.  Every
+// block reads the final counts of the tensor-core pass first: with the
+// changed certified rows plus the listed (uncertified) rows within `cap` the
+// sums are brought up to date here -- a listed row whose exact label differs
+// from its previous one moves its fixed-point features at once, the changed
+// certified rows from the change list -- else the sums and counts are
+// cleared and *recount = 1 asks the recount that follows.  Listed rows: one
+// lane per row over warp tasks of 32 rows dealt to the blocks first, the
+// candidates' dot products as the plain path's fma chains (features in
+// order), v = fl(-2 s + |c|^2), ties to the lower cluster; a row with no
+// candidate list scans every cluster with the whole warp.  Xr: the rows the
+// labels are computed from; Xu: the rows the sums hold (the same here).
+template <bool VEC>
 __global__ void __launch_bounds__(256)
-fx_delta_kernel(const float *X, int ld, int d, int k, const float *scale, const int *count,
-                int cap, const int *rows, const int *olds, const int *news,
-                unsigned long long *sum, int *cnt) {
+fx_rescore_delta_kernel(const float *Xr, const float *Xu, int ld, int d, const float *C, int k,
+                        const float *cnorm, AmbList amb, int *labels, int *flags,
+                        const float *scale, const int *count, int cap, const int *rows,
+                        const int *olds, const int *news, unsigned long long *sum, int *cnt,
+                        int *recount) {
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;
+    const int na = *amb.count;
     const int c = *count;
-    if (c > cap) {
+    const bool delta = (long long)c + na <= (long long)cap;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *recount = delta ? 0 : 1;
+    if (!delta) {
         const int kd = k * d;
         for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < kd; e += gridDim.x * blockDim.x)
             sum[e] = 0ull;
         for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < k; j += gridDim.x * blockDim.x)
             cnt[j] = 0;
-        return;
     }
-    const int lane = threadIdx.x & 31;
-    const int nwarps = gridDim.x * (blockDim.x >> 5);
-    for (int e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < c; e += nwarps) {
+    const int nwarps = gridDim.x * nwb;
+    const int gw = wib * gridDim.x + blockIdx.x;
+    const float inf = __int_as_float(0x7f800000);
+    int changed = 0;
+    for (int e0 = gw * 32; e0 < na; e0 += nwarps * 32) {
+        const int e = e0 + lane;
+        const bool in = e < na;
+        const int nc = in ? amb.ncand[e] : -1;
+        const int r = in ? amb.rows[e] : 0;
+        int cand_raw[KM_AMB_MAXC];
+#pragma unroll
+        for (int q = 0; q < KM_AMB_MAXC; ++q)
+            cand_raw[q] = in ? amb.cand[(size_t)e * KM_AMB_MAXC + q] : 0;
+        const int old_l = in ? labels[r] : -1;
+        int lbl = old_l;
+        if (nc > 0) {
+            int cj[KM_AMB_MAXC];
+            const float *cp[KM_AMB_MAXC];
+            float sd[KM_AMB_MAXC];
+#pragma unroll
+            for (int q = 0; q < KM_AMB_MAXC; ++q) {
+                cj[q] = q < nc ? cand_raw[q] : cand_raw[0];
+                cp[q] = C + (size_t)cj[q] * ld;
+                sd[q] = 0.f;
+            }
+            const float *xr = Xr + (size_t)r * ld;
+            if (VEC) {
+#pragma unroll 4
+                for (int f = 0; f < d; f += 4) {
+                    const float4 xv = *reinterpret_cast<const float4 *>(xr + f);
+#pragma unroll
+                    for (int q = 0; q < KM_AMB_MAXC; ++q) {
+                        const float4 cv = *reinterpret_cast<const float4 *>(cp[q] + f);
+                        sd[q] = __fmaf_rn(xv.x, cv.x, sd[q]);
+                        sd[q] = __fmaf_rn(xv.y, cv.y, sd[q]);
+                        sd[q] = __fmaf_rn(xv.z, cv.z, sd[q]);
+                        sd[q] = __fmaf_rn(xv.w, cv.w, sd[q]);
+                    }
+                }
+            } else {
+                for (int f = 0; f < d; ++f) {
+                    const float xf = xr[f];
+#pragma unroll
+                    for (int q = 0; q < KM_AMB_MAXC; ++q) sd[q] = __fmaf_rn(xf, cp[q][f], sd[q]);
+                }
+            }
+            float best = inf;
+            int bi = 0x7fffffff;
+#pragma unroll
+            for (int q = 0; q < KM_AMB_MAXC; ++q) {
+                if (q < nc) {
+                    const float v = __fmaf_rn(-2.f, sd[q], cnorm[cj[q]]);
+                    if (key_less(v, cj[q], best, bi)) {
+                        best = v;
+                        bi = cj[q];
+                    }
+                }
+            }
+            lbl = (bi == 0x7fffffff) ? cj[0] : bi;
+        }
+        unsigned full = __ballot_sync(0xffffffffu, nc == 0);
+        while (full) {
+            const int src = __ffs(full) - 1;
+            full &= full - 1;
+            const float *xr = Xr + (size_t)__shfl_sync(0xffffffffu, r, src) * ld;
+            float best = inf;
+            int bi = 0x7fffffff;
+            for (int j0 = lane; j0 < k; j0 += 128) {
+                const float *cc[4];
+                float sd[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int t = 0; t < 4; ++t) cc[t] = C + (size_t)min(j0 + 32 * t, k - 1) * ld;
+                for (int f = 0; f < d; ++f) {
+                    const float xf = xr[f];
+#pragma unroll
+                    for (int t = 0; t < 4; ++t) sd[t] = __fmaf_rn(xf, cc[t][f], sd[t]);
+                }
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const int j = j0 + 32 * t;
+                    if (j < k) {
+                        const float v = __fmaf_rn(-2.f, sd[t], cnorm[j]);
+                        if (key_less(v, j, best, bi)) {
+                            best = v;
+                            bi = j;
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const float ov = __shfl_xor_sync(0xffffffffu, best, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                if (key_less(ov, oi, best, bi)) {
+                    best = ov;
+                    bi = oi;
+                }
+            }
+            if (lane == src) lbl = (bi == 0x7fffffff) ? 0 : bi;
+        }
+        if (in) labels[r] = lbl;
+        const bool ch = in && lbl != old_l;
+        if (ch) changed = 1;
+        // the changed rows' features move from the old cluster to the new
+        unsigned mv = __ballot_sync(0xffffffffu, ch && delta);
+        while (mv) {
+            const int src = __ffs(mv) - 1;
+            mv &= mv - 1;
+            const int rs = __shfl_sync(0xffffffffu, r, src);
+            const int jo = __shfl_sync(0xffffffffu, old_l, src);
+            const int jn = __shfl_sync(0xffffffffu, lbl, src);
+            const float *x = Xu + (size_t)rs * ld;
+            for (int f = lane; f < d; f += 32) {
+                const long long q = __double2ll_rn((double)x[f] * (double)scale[f]);
+                atomicAdd(&sum[(size_t)jn * d + f], (unsigned long long)q);
+                atomicAdd(&sum[(size_t)jo * d + f], (unsigned long long)(-q));
+            }
+            if (lane == 0) {
+                atomicAdd(&cnt[jn], 1);
+                atomicSub(&cnt[jo], 1);
+            }
+        }
+    }
+    if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(&flags[0], 1);
+    if (!delta) return;
+    // the changed certified rows: one warp per row moves its fixed-point
+    // features q = round-to-nearest-even(x * 2^s_f), the values fx_acc adds
+    for (int e = gw; e < c; e += nwarps) {
         const int r = rows[e], jo = olds[e], jn = news[e];
-        const float *x = X + (size_t)r * ld;
+        const float *x = Xu + (size_t)r * ld;
         for (int f = lane; f < d; f += 32) {
             const long long q = __double2ll_rn((double)x[f] * (double)scale[f]);
             atomicAdd(&sum[(size_t)jn * d + f], (unsigned long long)q);
@@ -1097,14 +1236,16 @@ cudaError_t launch_kmeans_update_fx(const float *X, int ld, int n, int d, int k,
 }
 
 cudaError_t launch_kmeans_update_fx_loop(const float *X, int ld, int n, int d, int k,
-                                         const int *labels, const float *scale,
+                                         int *labels, const float *scale,
                                          const double *inv_scale, void *accum, float *C,
                                          int *counts, double *block_partials, double *scalars,
                                          int *flags, unsigned *ticket, LloydLoopState *ls,
                                          unsigned long long cond, const ChangeList &chg,
-                                         int *rearm, cudaStream_t s) {
+                                         int *rearm, const float *cnorm, const AmbList &amb,
+                                         int *recount, cudaStream_t s) {
     const size_t smem = fx_update_smem(k, d);
-    if (smem > (size_t)FX_SMEM_LIMIT || !chg.count) return cudaErrorInvalidValue;
+    if (smem > (size_t)FX_SMEM_LIMIT || !chg.count || !amb.count || !recount)
+        return cudaErrorInvalidValue;
     cudaError_t e = fx_smem_limit(smem);
     if (e != cudaSuccess) return e;
     int dev = 0, nsm = 148;
@@ -1113,10 +1254,19 @@ cudaError_t launch_kmeans_update_fx_loop(const float *X, int ld, int n, int d, i
     const size_t kd = (size_t)k * d;
     unsigned long long *sum = static_cast<unsigned long long *>(accum);
     int *cnt = reinterpret_cast<int *>(sum + 2 * kd);
-    // a short change list: the delta update; a long one: clear, then recount
-    fx_delta_kernel<<<nsm * 4, 256, 0, s>>>(X, ld, d, k, scale, chg.count, chg.cap, chg.rows,
-                                            chg.olds, chg.news, sum, cnt);
-    fx_launch(X, ld, n, d, k, labels, scale, sum, cnt, nsm, smem, s, chg.count, chg.cap);
+    // the listed rows' exact labels with a short change list's delta update,
+    // or with the clearing of the sums for the recount that follows
+    const bool vec = (d % 4 == 0) && (ld % 4 == 0) &&
+                     ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(C)) & 15) == 0;
+    if (vec)
+        fx_rescore_delta_kernel<true><<<nsm * 4, 256, 0, s>>>(
+            X, X, ld, d, C, k, cnorm, amb, labels, flags, scale, chg.count, chg.cap, chg.rows,
+            chg.olds, chg.news, sum, cnt, recount);
+    else
+        fx_rescore_delta_kernel<false><<<nsm * 4, 256, 0, s>>>(
+            X, X, ld, d, C, k, cnorm, amb, labels, flags, scale, chg.count, chg.cap, chg.rows,
+            chg.olds, chg.news, sum, cnt, recount);
+    fx_launch(X, ld, n, d, k, labels, scale, sum, cnt, nsm, smem, s, recount, 0);
     const int nb = (int)((kd + 255) / 256);
     // in place: each element's old value is read by the thread that writes it;
     // the last block re-arms the iteration's counters

@@ -31,7 +31,7 @@ static constexpr int TC_BM = 128;       // rows per tile (UMMA M)
 static constexpr int TC_KB = 64;        // bf16 elements per 128-byte K block
 static constexpr int TC_EPI_WARPS = 16; // 2 accumulators x 2 column halves x 4 lane quarters
 static constexpr int TC_THREADS = 64 + 32 * TC_EPI_WARPS; // + producer and MMA warps
-static constexpr int TC_MAXC = 4;       // candidates kept per uncertified row
+static constexpr int TC_MAXC = KM_AMB_MAXC; // candidates kept per uncertified row
 
 struct TcAssignArgs {
     int n, k, npad, nkb, stages, bufcols;
@@ -483,11 +483,21 @@ kmeans_rescore_kernel(const float *X, int ld, int d, int dp, const float *C, int
     const float inf = __int_as_float(0x7f800000);
     int changed = 0;
     const int nw = gridDim.x * nwb;
-    for (int e0 = (blockIdx.x * nwb + warp) * 32; e0 < cnt; e0 += nw * 32) {
+    // warp tasks of 32 listed rows, dealt to the blocks first (warp-major):
+    // a short list spreads over every SM instead of filling a few blocks
+    for (int e0 = (warp * gridDim.x + blockIdx.x) * 32; e0 < cnt; e0 += nw * 32) {
         const int e = e0 + lane;
-        const int nc = e < cnt ? amb_ncand[e] : -1;
-        const int r = e < cnt ? amb_rows[e] : 0;
+        const bool in = e < cnt;
+        const int nc = in ? amb_ncand[e] : -1;
+        const int r = in ? amb_rows[e] : 0;
         const int nrows = min(32, cnt - e0);
+        // loads that need only e and r go out before the row staging: the
+        // candidate list (every slot is in bounds; those past nc are unused)
+        // and the previous label (read before this thread writes it)
+        int cand_raw[TC_MAXC];
+#pragma unroll
+        for (int q = 0; q < TC_MAXC; ++q) cand_raw[q] = in ? amb_cand[(size_t)e * TC_MAXC + q] : 0;
+        const int old_label = (in && labels_prev) ? labels_prev[r] : -1;
         __syncwarp();
         // stage the warp's rows: row ids come from the lanes (shuffles), and
         // eight loads per lane are issued before their stores, so the loads
@@ -528,7 +538,7 @@ kmeans_rescore_kernel(const float *X, int ld, int d, int dp, const float *C, int
             float sd[TC_MAXC];
 #pragma unroll
             for (int q = 0; q < TC_MAXC; ++q) {
-                cj[q] = amb_cand[(size_t)e * TC_MAXC + (q < nc ? q : 0)];
+                cj[q] = q < nc ? cand_raw[q] : cand_raw[0];
                 cp[q] = cbase + (size_t)cj[q] * cst;
                 sd[q] = 0.f;
             }
@@ -568,8 +578,7 @@ kmeans_rescore_kernel(const float *X, int ld, int d, int dp, const float *C, int
                 }
             }
             const int lbl = (bi == 0x7fffffff) ? cj[0] : bi;
-            // read before the write: labels may be labels_prev (in place)
-            const int old_l = labels_prev ? labels_prev[r] : lbl;
+            const int old_l = labels_prev ? old_label : lbl;
             if (old_l != lbl) {
                 changed = 1;
                 chg_c = true;
@@ -637,7 +646,7 @@ kmeans_rescore_kernel(const float *X, int ld, int d, int dp, const float *C, int
             }
             if (lane == src) {
                 const int lbl = (bi == 0x7fffffff) ? 0 : bi;
-                const int old_l = labels_prev ? labels_prev[r] : lbl;
+                const int old_l = labels_prev ? old_label : lbl;
                 if (old_l != lbl) {
                     changed = 1;
                     if (chg.count) {
