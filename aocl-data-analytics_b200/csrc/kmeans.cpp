@@ -950,6 +950,7 @@ da_status KMeans<T>::run_lloyd(T *&dCcur, T *&dCprev, int *&dLcur, int *&dLprev,
             int conv = 0;
             da_status s = lloyd_graph(dCcur, dLcur, nit, conv, ran);
             if (s != da_status_success) return s;
+            cuda->stats["graph_loop"] = ran ? 1.0 : 0.0;
             if (ran) {
                 converged = conv;
                 it = nit;

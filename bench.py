@@ -390,6 +390,7 @@ def main():
     n_iter = iters // args.steps
     relabelled = km.stat("relabelled_rows")
     full_scan = km.stat("full_scan_rows")
+    graph_loop = km.stat("graph_loop")
     tensor_core = km.stat("tensor_core") == 1.0
     kt = kernel_times(km)
 
@@ -487,6 +488,7 @@ def main():
              "accuracy": accuracy,
              "legs_summary": legs_summary(knn, c1, batched, serving, radius, ivf, plain, value),
              "relabelled_rows_last_iteration": relabelled,
+             "lloyd_loop_as_cuda_graph": bool(graph_loop == 1.0),
              "full_scan_rows_last_iteration": full_scan,
              "precision_path": (f"{mode} tcgen05 candidate pass + exact fp32 re-score of "
                                 "uncertified rows") if tensor_core else "plain fp32 (SIMT)"}
