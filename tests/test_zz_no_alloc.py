@@ -1,7 +1,8 @@
 """da_b200_knn_euclidean_noalloc_s: the k-nearest-neighbour search for callers
 that cannot allocate device memory.  Its working memory is a fixed array in
 the library, so its results are checked against da_nn_kneighbors_s (the
-handle path, which allocates its own buffers) on two calls in a row -- the
+handle path, which allocates its own buffers) and, where the oracle's search
+is quick, against the oracle, on two calls in a row -- the
 second call runs over what the first left in the shared array -- plus a
 repeat of the first.  kNN results are compared bit for bit, as in the other
 kNN tests.  This file is collected last so that it also runs after every
@@ -31,7 +32,7 @@ def _reference(ab, X, Q, k):
 
 
 @pytest.mark.gpu
-def test_knn_noalloc_matches_kneighbors(ab, gpu):
+def test_knn_noalloc_matches_kneighbors(ab, orc, gpu):
     import torch
 
     f = _entry(ab)
@@ -62,6 +63,12 @@ def test_knn_noalloc_matches_kneighbors(ab, gpu):
         torch.cuda.synchronize(dev)
         np.testing.assert_array_equal(ind.cpu().numpy(), ind_ref)
         np.testing.assert_array_equal(dist.cpu().numpy(), dist_ref)
+        if n * nq <= 20_000_000:
+            # and the oracle's search (the reference's arithmetic, ties to
+            # the lower index)
+            oind, odist = orc.knn(X, Q, k, "euclidean")
+            np.testing.assert_array_equal(ind.cpu().numpy(), oind)
+            np.testing.assert_array_equal(dist.cpu().numpy(), odist)
 
 
 @pytest.mark.gpu
