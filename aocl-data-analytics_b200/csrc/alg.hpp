@@ -110,7 +110,7 @@ template <typename T> struct NN : public AlgBase {
     std::vector<long long> rnn_start;
     std::vector<T> rnn_val;
     bool rnn_dist = false, rnn_squares = false;
-    DevBuf dD, dRc, dRs, dRi, dRv;
+    DevBuf dD, dRc, dRs, dRi, dRv, dRh;
     da_status radius_neighbors(da_int nq, da_int d, const T *Xt, da_int ldt, T radius,
                                da_int return_distance, da_int sort_results);
     da_status get_result(da_result q, da_int *dim, double *out) override;

@@ -67,6 +67,11 @@ struct PairwiseArgs {
     double p;      // Minkowski exponent
     bool x_is_y;   // cosine / gemm: diagonal forced to 0
     bool out_rowmajor; // D row-major (m x n, ld = n) or column-major (ld = m)
+    // radius search (row-major D only): with `hits`, every stored value
+    // D(i, j) <= thr also counts into hits[i * radius_chunks(n) + j / RADIUS_CHUNK]
+    // (integer atomics; hits zeroed by the caller)
+    double thr = 0.0;
+    int *hits = nullptr;
 };
 // D(i,j) = dist(x_i, y_j), i < m (rows of X), j < n (rows of Y).
 template <typename T>
@@ -92,11 +97,12 @@ cudaError_t launch_radius_emit(const T *D, int rows, int n, size_t ld, T thr,
 // chunk] = the hits of the pieces before it, total[0] = all hits.  Its waits
 // on other CTAs are bounded: err[0] = 1 when one ran out (test_wait: piece 0
 // never publishes and the waits run out at once).  work:
-// radius_scan_work_bytes(rows, n).
+// radius_scan_work_bytes(rows, n).  hits: the pieces' counts made by the
+// distance kernel (PairwiseArgs::hits); then D is not read.
 template <typename T>
 cudaError_t launch_radius_count_scan(const T *D, int rows, int n, size_t ld, T thr, void *work,
                                      long long *start, long long *total, int *err, int test_wait,
-                                     cudaStream_t s);
+                                     cudaStream_t s, const int *hits = nullptr);
 size_t radius_scan_work_bytes(int rows, int n);
 
 // ------------------------------------------------------------ kNN fused --

@@ -69,7 +69,8 @@ B200_DEV T post_value(int post, T g, T xn, T yn, T invp) {
 template <typename T, int ACC>
 __global__ void __launch_bounds__(256)
 pairwise_kernel(const T *X, int m, const T *Y, int n, int ld, int d, const T *xn, const T *yn,
-                int post, int kc, T p, T invp, int x_is_y, int out_rowmajor, T *D) {
+                int post, int kc, T p, T invp, int x_is_y, int out_rowmajor, T *D, T thr,
+                int *hits, int nch) {
     using C = SimtCfg<T>;
     constexpr int TM = C::TM, TN = C::TN, BK = C::BK, BM = 16 * TM, BN = 16 * TN;
     __shared__ __align__(16) Stage<T, BM, BN, BK> st[2];
@@ -78,8 +79,10 @@ pairwise_kernel(const T *X, int m, const T *Y, int n, int ld, int d, const T *xn
     Acc<T, TM, TN> acc;
     compute_tile<T, ACC, TM, TN, BM, BN, BK>(st, X, ld, m, i0, Y, ld, n, j0, d, kc, p, acc, tid);
     const int tm = tid / 16, tn = tid % 16;
+    int hit[TM];
 #pragma unroll
     for (int i = 0; i < TM; ++i) {
+        hit[i] = 0;
         const int gi = i0 + tm * 4 + i;
         if (gi >= m) continue;
         const T xv = xn ? xn[gi] : T(0);
@@ -96,7 +99,21 @@ pairwise_kernel(const T *X, int m, const T *Y, int n, int ld, int d, const T *xn
                 D[(size_t)gi * n + gj] = v;
             else
                 D[(size_t)gj * m + gi] = v;
+            hit[i] += v <= thr ? 1 : 0;
         }
+    }
+    if (!hits) return;
+    // the tile's hits per row: the 16 lanes of a row group (one half-warp)
+    // sum theirs, lane tn = 0 adds them to the row's chunk (a tile lies in
+    // one chunk: RADIUS_CHUNK is a multiple of BN)
+    static_assert(RADIUS_CHUNK % BN == 0, "tiles within one radius chunk");
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+        int c = hit[i];
+#pragma unroll
+        for (int off = 8; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+        const int gi = i0 + tm * 4 + i;
+        if (tn == 0 && gi < m && c > 0) atomicAdd(&hits[(size_t)gi * nch + j0 / RADIUS_CHUNK], c);
     }
 }
 
@@ -110,25 +127,31 @@ cudaError_t launch_pairwise(const T *X, int ldx, int m, const T *Y, int ldy, int
     dim3 grid((n + BN - 1) / BN, (m + BM - 1) / BM);
     const T p = T(a.p);
     const T invp = T(1.0 / (double)p);
+    if (a.hits && !a.out_rowmajor) return cudaErrorInvalidValue;
+    const T thr = T(a.thr);
+    const int nch = radius_chunks(n);
     switch (a.acc) {
     case ACC_SQEUC:
         pairwise_kernel<T, ACC_SQEUC><<<grid, 256, 0, s>>>(X, m, Y, n, ldx, d, xn, yn, a.post,
                                                            a.kc, p, invp, a.x_is_y,
-                                                           a.out_rowmajor, D);
+                                                           a.out_rowmajor, D, thr, a.hits, nch);
         break;
     case ACC_DOT:
         pairwise_kernel<T, ACC_DOT><<<grid, 256, 0, s>>>(X, m, Y, n, ldx, d, xn, yn, a.post, a.kc,
-                                                         p, invp, a.x_is_y, a.out_rowmajor, D);
+                                                         p, invp, a.x_is_y, a.out_rowmajor, D,
+                                                         thr, a.hits, nch);
         break;
     case ACC_MANHATTAN:
         pairwise_kernel<T, ACC_MANHATTAN><<<grid, 256, 0, s>>>(X, m, Y, n, ldx, d, xn, yn,
                                                                a.post, a.kc, p, invp, a.x_is_y,
-                                                               a.out_rowmajor, D);
+                                                               a.out_rowmajor, D, thr, a.hits,
+                                                               nch);
         break;
     default:
         pairwise_kernel<T, ACC_MINKOWSKI><<<grid, 256, 0, s>>>(X, m, Y, n, ldx, d, xn, yn,
                                                                a.post, a.kc, p, invp, a.x_is_y,
-                                                               a.out_rowmajor, D);
+                                                               a.out_rowmajor, D, thr, a.hits,
+                                                               nch);
         break;
     }
     return cudaGetLastError();
@@ -572,6 +595,69 @@ __global__ void radius_emit_kernel(const T *D, int n, size_t ld, T thr, int chun
         __syncthreads();
     }
 }
+// radius_emit_kernel with W consecutive elements per thread (one 16-byte
+// load; rows and chunk bounds multiples of W): the thread's hits in index
+// order, a warp scan of the per-thread counts, then the warps in order.
+template <typename T> struct Vec16Of;
+template <> struct Vec16Of<float> { using V = float4; };
+template <> struct Vec16Of<double> { using V = double2; };
+template <typename T>
+__global__ void radius_emit_vec_kernel(const T *D, int n, size_t ld, T thr, int chunk,
+                                       const long long *start, int *idx, T *val) {
+    constexpr int W = 16 / (int)sizeof(T);
+    using V = typename Vec16Of<T>::V;
+    const T *row = D + (size_t)blockIdx.y * ld;
+    __shared__ int ws[33];
+    long long base = start[(size_t)blockIdx.y * gridDim.x + blockIdx.x];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int j1 = min(n, (int)(blockIdx.x + 1) * chunk);
+    for (int j0 = (int)blockIdx.x * chunk; j0 < j1; j0 += (int)blockDim.x * W) {
+        const int j = j0 + (int)threadIdx.x * W;
+        T v[W];
+        if (j < j1) {
+            const V t = *reinterpret_cast<const V *>(row + j);
+            const T *tp = reinterpret_cast<const T *>(&t);
+#pragma unroll
+            for (int u = 0; u < W; ++u) v[u] = tp[u];
+        }
+        int c = 0;
+        unsigned fm = 0;
+#pragma unroll
+        for (int u = 0; u < W; ++u)
+            if (j < j1 && v[u] <= thr) {
+                fm |= 1u << u;
+                ++c;
+            }
+        int x = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) ws[w] = x;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int q = 0; q < nw; ++q) {
+                const int cq = ws[q];
+                ws[q] = t;
+                t += cq;
+            }
+            ws[32] = t;
+        }
+        __syncthreads();
+        long long pos = base + ws[w] + (x - c);
+#pragma unroll
+        for (int u = 0; u < W; ++u)
+            if (fm & (1u << u)) {
+                idx[pos] = j + u;
+                val[pos] = v[u];
+                ++pos;
+            }
+        base += ws[32];
+        __syncthreads();
+    }
+}
 int radius_chunks(int n) { return (n + RADIUS_CHUNK - 1) / RADIUS_CHUNK; }
 // Counts and output offsets of the (row, chunk) pieces in one pass: a chained
 // scan in (row, chunk) order.  Each CTA takes the next logical piece from a
@@ -591,7 +677,7 @@ __global__ void radius_count_scan_kernel(const T *D, int n, size_t ld, T thr, in
                                          int pieces, unsigned *ticket,
                                          unsigned long long *state, long long *start,
                                          long long *total, int *err, unsigned limit,
-                                         int skip_first) {
+                                         int skip_first, const int *hits) {
     __shared__ int s_id;
     __shared__ int ws[32];
     if (threadIdx.x == 0) s_id = (int)atomicAdd(ticket, 1u);
@@ -602,7 +688,11 @@ __global__ void radius_count_scan_kernel(const T *D, int n, size_t ld, T thr, in
     const T *row = D + (size_t)rr * ld;
     const int j1 = min(n, (cc + 1) * chunk);
     int c = 0;
-    for (int j = cc * chunk + threadIdx.x; j < j1; j += blockDim.x) c += row[j] <= thr ? 1 : 0;
+    if (hits) { // counted by the distance kernel
+        if (threadIdx.x == 0) c = hits[id];
+    } else {
+        for (int j = cc * chunk + threadIdx.x; j < j1; j += blockDim.x) c += row[j] <= thr ? 1 : 0;
+    }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
     if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
@@ -650,7 +740,7 @@ __global__ void radius_count_scan_kernel(const T *D, int n, size_t ld, T thr, in
 template <typename T>
 cudaError_t launch_radius_count_scan(const T *D, int rows, int n, size_t ld, T thr, void *work,
                                      long long *start, long long *total, int *err, int test_wait,
-                                     cudaStream_t s) {
+                                     cudaStream_t s, const int *hits) {
     if (rows <= 0 || n <= 0) return cudaSuccess;
     const int nch = radius_chunks(n);
     const int pieces = rows * nch;
@@ -663,16 +753,16 @@ cudaError_t launch_radius_count_scan(const T *D, int rows, int n, size_t ld, T t
     const unsigned limit = test_wait ? 2000u : (1u << 24);
     radius_count_scan_kernel<T><<<pieces, 256, 0, s>>>(D, n, ld, thr, RADIUS_CHUNK, nch, pieces,
                                                       ticket, state, start, total, err, limit,
-                                                      test_wait);
+                                                      test_wait, hits);
     return cudaGetLastError();
 }
 size_t radius_scan_work_bytes(int rows, int n) { return 256 + (size_t)rows * radius_chunks(n) * 8; }
 template cudaError_t launch_radius_count_scan<float>(const float *, int, int, size_t, float,
                                                      void *, long long *, long long *, int *, int,
-                                                     cudaStream_t);
+                                                     cudaStream_t, const int *);
 template cudaError_t launch_radius_count_scan<double>(const double *, int, int, size_t, double,
                                                       void *, long long *, long long *, int *,
-                                                      int, cudaStream_t);
+                                                      int, cudaStream_t, const int *);
 
 template <typename T>
 cudaError_t launch_radius_count(const T *D, int rows, int n, size_t ld, T thr, int *cnt,
@@ -687,7 +777,12 @@ cudaError_t launch_radius_emit(const T *D, int rows, int n, size_t ld, T thr,
                                const long long *start, int *idx, T *val, cudaStream_t s) {
     if (rows <= 0 || n <= 0) return cudaSuccess;
     const dim3 grid(radius_chunks(n), rows);
-    radius_emit_kernel<T><<<grid, 256, 0, s>>>(D, n, ld, thr, RADIUS_CHUNK, start, idx, val);
+    constexpr int W = 16 / (int)sizeof(T);
+    if (n % W == 0 && ld % W == 0 && (reinterpret_cast<uintptr_t>(D) & 15) == 0)
+        radius_emit_vec_kernel<T><<<grid, 256, 0, s>>>(D, n, ld, thr, RADIUS_CHUNK, start, idx,
+                                                       val);
+    else
+        radius_emit_kernel<T><<<grid, 256, 0, s>>>(D, n, ld, thr, RADIUS_CHUNK, start, idx, val);
     return cudaGetLastError();
 }
 template cudaError_t launch_radius_count<float>(const float *, int, int, size_t, float, int *,

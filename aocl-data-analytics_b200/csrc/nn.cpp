@@ -662,18 +662,23 @@ da_status NN<T>::radius_compute(da_int nq, da_int d, const T *Xt, da_int ldt, T 
     const int nch = radius_chunks((int)n);
     if (!dD.ensure((size_t)B * n * sizeof(T)) ||
         !dRc.ensure(radius_scan_work_bytes((int)B, (int)n) + 64) ||
-        !dRs.ensure((size_t)B * nch * sizeof(long long)))
+        !dRs.ensure((size_t)B * nch * sizeof(long long)) ||
+        !dRh.ensure((size_t)B * nch * sizeof(int)))
         return err->error(da_status_memory_error, "Device memory allocation failed.");
     // testing hook: the offsets' waits run out (AOCLDA_B200_TEST_RADIUS_WAIT=1)
     const char *tw = std::getenv("AOCLDA_B200_TEST_RADIUS_WAIT");
     const int test_wait = (tw && tw[0] == '1') ? 1 : 0;
     std::vector<long long> start((size_t)B * nch + 2);
-    const PairwiseArgs pa{acc, post, kc, (double)p, false, true};
+    // the distance kernel also counts each (row, chunk) piece's hits
+    PairwiseArgs pa{acc, post, kc, (double)p, false, true};
+    pa.thr = (double)thr;
+    pa.hits = dRh.as<int>();
     long long *d_total = reinterpret_cast<long long *>(dRc.as<char>() +
                                                        radius_scan_work_bytes((int)B, (int)n));
     int *d_err = reinterpret_cast<int *>(d_total + 1);
     for (da_int q0 = 0; q0 < nq; q0 += B) {
         const int b = (int)std::min<da_int>(B, nq - q0);
+        B200_TRY(cudaMemsetAsync(dRh.p, 0, (size_t)b * nch * sizeof(int), st), "memset");
         B200_TRY(cuda->timed("radius_distances", [&] {
             return launch_pairwise<T>(dQ.as<T>() + (size_t)q0 * ld, ld, b, dX.as<T>(), ld, (int)n,
                                       (int)d, qn ? qn + q0 : nullptr, xn, pa, dD.as<T>(), st);
@@ -682,7 +687,8 @@ da_status NN<T>::radius_compute(da_int nq, da_int d, const T *Xt, da_int ldt, T 
         // hits stay in index order
         B200_TRY(cuda->timed("radius_count", [&] {
             return launch_radius_count_scan<T>(dD.as<T>(), b, (int)n, n, thr, dRc.p,
-                                               dRs.as<long long>(), d_total, d_err, test_wait, st);
+                                               dRs.as<long long>(), d_total, d_err, test_wait, st,
+                                               dRh.as<int>());
         }), "count");
         B200_TRY(cudaMemcpyAsync(start.data(), dRs.p, (size_t)b * nch * sizeof(long long),
                                  cudaMemcpyDeviceToHost, st), "copy");

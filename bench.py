@@ -925,8 +925,9 @@ def run_radius(ab, nx=1_000_000, nq=10_000, d=32, comps=256, target=100, seed=6,
     da_nn_radius_neighbors_s over all queries with host arrays (queries up;
     counts, indices and distances down; results in index order).  Roofline of
     the distance-block pipeline: every block of queries writes its distance
-    rows once and the count and compaction kernels read them once each
-    (12 bytes per (query, row) pair) over the three kernels' CUDA-event time.
+    rows once (the distance kernel also counts the hits) and the compaction
+    reads them once (8 bytes per (query, row) pair) over the three kernels'
+    CUDA-event time.
     CPU: the oracle on a sample of queries."""
     rng = np.random.default_rng(seed)
     means = rng.uniform(-3.0, 3.0, (comps, d)).astype(np.float32)
@@ -955,7 +956,7 @@ def run_radius(ab, nx=1_000_000, nq=10_000, d=32, comps=256, target=100, seed=6,
         kern[name] = (ms_, n_)
     nn.close()
     total_ms = sum(v[0] for v in kern.values()) / reps
-    bytes_ = 12.0 * nq * (nx)
+    bytes_ = 8.0 * nq * (nx)
     hbm, _, src = load_peaks()
     orc = _load("oracle_mod", os.path.join(ORACLE, "oracle.py"))
     t = time.perf_counter()
@@ -973,7 +974,7 @@ def run_radius(ab, nx=1_000_000, nq=10_000, d=32, comps=256, target=100, seed=6,
                          "peak": hbm, "unit": "GB/s",
                          "frac": bytes_ / (total_ms / 1e3) / 1e9 / hbm, "peak_source": src,
                          "traffic": None,
-                         "note": "12 bytes per (query, row): distance written, read twice"},
+                         "note": "8 bytes per (query, row): distance written once, read once"},
             "identical_to_oracle_sample": bool(same),
             "cpu_baseline": {"value": cpu_queries / cpu_s, "unit": "queries/s", "cores": 1,
                              "kind": "port", "sample": f"{cpu_queries} queries, oracle"},
