@@ -751,7 +751,9 @@ cudaError_t launch_radius_count_scan(const T *D, int rows, int n, size_t ld, T t
     if (e != cudaSuccess) return e;
     // about a second of polling; the test mode's wait runs out in microseconds
     const unsigned limit = test_wait ? 2000u : (1u << 24);
-    radius_count_scan_kernel<T><<<pieces, 256, 0, s>>>(D, n, ld, thr, RADIUS_CHUNK, nch, pieces,
+    // with the counts given, one warp per piece (thread 0 does the look-back)
+    radius_count_scan_kernel<T><<<pieces, hits ? 32 : 256, 0, s>>>(D, n, ld, thr, RADIUS_CHUNK,
+                                                                    nch, pieces,
                                                       ticket, state, start, total, err, limit,
                                                       test_wait, hits);
     return cudaGetLastError();
