@@ -23,6 +23,11 @@
 #include <mutex>
 
 namespace b200 {
+
+// 16-byte vector of T
+template <typename T> struct Vec16Of;
+template <> struct Vec16Of<float> { using V = float4; };
+template <> struct Vec16Of<double> { using V = double2; };
 // Raises (never lowers) a kernel's dynamic shared-memory limit on the current
 // device.  The limit belongs to the function and device for the whole
 // process, so callers on several threads that need different sizes must not
@@ -79,6 +84,10 @@ pairwise_kernel(const T *X, int m, const T *Y, int n, int ld, int d, const T *xn
     Acc<T, TM, TN> acc;
     compute_tile<T, ACC, TM, TN, BM, BN, BK>(st, X, ld, m, i0, Y, ld, n, j0, d, kc, p, acc, tid);
     const int tm = tid / 16, tn = tid % 16;
+    // row-major D with n a multiple of 4: a thread's four consecutive columns
+    // go out as 16-byte stores (D from cudaMalloc, rows of n elements)
+    const bool vec_out = out_rowmajor && (n & 3) == 0 &&
+                         (reinterpret_cast<uintptr_t>(D) & 15) == 0;
     int hit[TM];
 #pragma unroll
     for (int i = 0; i < TM; ++i) {
@@ -87,19 +96,37 @@ pairwise_kernel(const T *X, int m, const T *Y, int n, int ld, int d, const T *xn
         if (gi >= m) continue;
         const T xv = xn ? xn[gi] : T(0);
 #pragma unroll
-        for (int j = 0; j < TN; ++j) {
-            const int gj = j0 + (j / 4) * 64 + tn * 4 + (j % 4);
-            if (gj >= n) continue;
-            const T yv = yn ? yn[gj] : T(0);
-            T v = post_value<T>(post, acc.g1[i][j], xv, yv, invp);
-            if (x_is_y && gi == gj && (post == POST_COSINE || post == POST_GEMM_SQ ||
-                                       post == POST_GEMM_SQRT))
-                v = T(0);
-            if (out_rowmajor)
-                D[(size_t)gi * n + gj] = v;
-            else
-                D[(size_t)gj * m + gi] = v;
-            hit[i] += v <= thr ? 1 : 0;
+        for (int g = 0; g < TN / 4; ++g) {
+            const int gj0 = j0 + g * 64 + tn * 4;
+            T v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int gj = gj0 + u;
+                const T yv = (yn && gj < n) ? yn[gj] : T(0);
+                v[u] = post_value<T>(post, acc.g1[i][g * 4 + u], xv, yv, invp);
+                if (x_is_y && gi == gj && (post == POST_COSINE || post == POST_GEMM_SQ ||
+                                           post == POST_GEMM_SQRT))
+                    v[u] = T(0);
+                if (gj < n) hit[i] += v[u] <= thr ? 1 : 0;
+            }
+            if (vec_out && gj0 + 3 < n) {
+                using V = typename Vec16Of<T>::V;
+                constexpr int W = 16 / (int)sizeof(T);
+#pragma unroll
+                for (int u = 0; u < 4; u += W)
+                    *reinterpret_cast<V *>(D + (size_t)gi * n + gj0 + u) =
+                        *reinterpret_cast<const V *>(&v[u]);
+            } else {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int gj = gj0 + u;
+                    if (gj >= n) continue;
+                    if (out_rowmajor)
+                        D[(size_t)gi * n + gj] = v[u];
+                    else
+                        D[(size_t)gj * m + gi] = v[u];
+                }
+            }
         }
     }
     if (!hits) return;
@@ -598,9 +625,6 @@ __global__ void radius_emit_kernel(const T *D, int n, size_t ld, T thr, int chun
 // radius_emit_kernel with W consecutive elements per thread (one 16-byte
 // load; rows and chunk bounds multiples of W): the thread's hits in index
 // order, a warp scan of the per-thread counts, then the warps in order.
-template <typename T> struct Vec16Of;
-template <> struct Vec16Of<float> { using V = float4; };
-template <> struct Vec16Of<double> { using V = double2; };
 template <typename T>
 __global__ void radius_emit_vec_kernel(const T *D, int n, size_t ld, T thr, int chunk,
                                        const long long *start, int *idx, T *val) {
