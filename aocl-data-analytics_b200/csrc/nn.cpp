@@ -657,8 +657,11 @@ da_status NN<T>::radius_compute(da_int nq, da_int d, const T *Xt, da_int ldt, T 
     // query blocks whose distance rows fit in 256 MB
     const size_t n = (size_t)n_samples;
     // (at most 65,535 rows: the count / compaction grids put the rows on y)
-    const da_int B = (da_int)std::max<size_t>(
+    // (and a whole number of the distance kernel's 64-row tiles when there
+    // are more queries: a partial last tile row costs a full one)
+    da_int B = (da_int)std::max<size_t>(
         1, std::min<size_t>({(size_t)nq, (256u << 20) / (n * sizeof(T)), (size_t)65535}));
+    if (B < nq && B > 64) B -= B % 64;
     const int nch = radius_chunks((int)n);
     if (!dD.ensure((size_t)B * n * sizeof(T)) ||
         !dRc.ensure(radius_scan_work_bytes((int)B, (int)n) + 64) ||
