@@ -152,3 +152,28 @@ def test_pickle_kmeans_and_ann(gpu, da):
     assert ann2.n_index == 4000
     for a, b in zip(ann2.kneighbors(Q), ann.kneighbors(Q)):
         np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+@pytest.mark.parametrize("algorithm", ["lloyd", "elkan"])
+def test_kmeans_spherical_shim(gpu, da, orc, dt, algorithm):
+    """kmeans_test.py:313-337 of the reference (distance="cosine",
+    normalize_data=False on its 6 x 3 array): unit-length centres; and
+    the oracle's spherical Lloyd from the same initial centres."""
+    from aoclda.clustering import kmeans
+    a = golden("kmeans_spherical.npz")["py_a"].astype(dt)
+    km = kmeans(n_clusters=2, algorithm=algorithm, distance="cosine", normalize_data=False,
+                seed=42, n_init=1)
+    km.fit(a)
+    tol = 1e-6 if dt == np.float32 else 1e-12
+    np.testing.assert_allclose(np.linalg.norm(km.cluster_centres.astype(np.float64), axis=1),
+                               1.0, atol=tol)
+    # supplied initial centres: the oracle's trajectory
+    C0 = a[[0, 3]].copy()
+    km = kmeans(n_clusters=2, C=C0, initialization_method="supplied", n_init=1,
+                algorithm=algorithm, distance="cosine", normalize_data=True)
+    km.fit(a)
+    C, lab, _, _ = orc.kmeans_sph_lloyd(a, C0, 300, 1e-4, normalise=True)
+    np.testing.assert_array_equal(km.labels, lab)
+    np.testing.assert_allclose(km.cluster_centres, C, rtol=1e-5 if dt == np.float32 else 1e-12,
+                               atol=1e-6 if dt == np.float32 else 1e-12)
