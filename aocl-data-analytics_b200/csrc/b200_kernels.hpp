@@ -80,25 +80,22 @@ cudaError_t launch_pairwise(const T *X, int ldx, int m, const T *Y, int ldy, int
                             cudaStream_t s);
 
 // Radius neighbours from a block of distances D (rows x n, row-major, ld),
-// each row cut into radius_chunks(n) chunks of RADIUS_CHUNK columns (one CTA
-// each): per (row, chunk) the count of D <= thr (cnt[row * chunks + chunk]),
-// then the ordered compaction (index order) of those (column, value) pairs
-// at out offsets start[row * chunks + chunk].
+// each row cut into radius_chunks(n) chunks of RADIUS_CHUNK columns: the
+// ordered compaction (index order) of each (row, chunk) piece's (column,
+// value) pairs with D <= thr at out offsets start[row * chunks + chunk] (one
+// CTA per piece).
 constexpr int RADIUS_CHUNK = 16384;
 int radius_chunks(int n);
 template <typename T>
-cudaError_t launch_radius_count(const T *D, int rows, int n, size_t ld, T thr, int *cnt,
-                                cudaStream_t s);
-template <typename T>
 cudaError_t launch_radius_emit(const T *D, int rows, int n, size_t ld, T thr,
                                const long long *start, int *idx, T *val, cudaStream_t s);
-// The counts and the output offsets of all (row, chunk) pieces in one launch
-// (a chained scan in (row, chunk) order, dist_simt.cu): start[row * chunks +
-// chunk] = the hits of the pieces before it, total[0] = all hits.  Its waits
-// on other CTAs are bounded: err[0] = 1 when one ran out (test_wait: piece 0
-// never publishes and the waits run out at once).  work:
-// radius_scan_work_bytes(rows, n).  hits: the pieces' counts made by the
-// distance kernel (PairwiseArgs::hits); then D is not read.
+// The output offsets of all (row, chunk) pieces from their hit counts (hits,
+// made by the distance kernel: PairwiseArgs::hits) in one launch (a chained
+// scan in (row, chunk) order over groups of 32 pieces, dist_simt.cu):
+// start[row * chunks + chunk] = the hits of the pieces before it, total[0] =
+// all hits.  Its waits on other warps are bounded: err[0] = 1 when one ran
+// out (test_wait: the first group never publishes and the waits run out at
+// once).  work: radius_scan_work_bytes(rows, n).  D, ld and thr are unused.
 template <typename T>
 cudaError_t launch_radius_count_scan(const T *D, int rows, int n, size_t ld, T thr, void *work,
                                      long long *start, long long *total, int *err, int test_wait,

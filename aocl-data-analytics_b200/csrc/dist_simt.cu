@@ -566,27 +566,10 @@ B200_INST(double)
 
 // ------------------------------------------------------ radius search ---
 // nearest_neighbors.cpp:2070-2247 keeps, per query, the training rows with
-// D <= (squared) radius.  One block per row of a distance block: a count
-// pass, then an ordered compaction (block-wide exclusive scans over tiles of
-// blockDim columns), so each row's hits come out in index order.
-template <typename T>
-__global__ void radius_count_kernel(const T *D, int n, size_t ld, T thr, int chunk, int *cnt) {
-    const T *row = D + (size_t)blockIdx.y * ld;
-    const int j1 = min(n, (int)(blockIdx.x + 1) * chunk);
-    int c = 0;
-    for (int j = (int)blockIdx.x * chunk + threadIdx.x; j < j1; j += blockDim.x)
-        c += row[j] <= thr ? 1 : 0;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
-    __shared__ int ws[32];
-    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int t = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
-        cnt[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
-    }
-}
+// D <= (squared) radius.  The distance kernel counts the hits of every (row,
+// 16,384-column chunk) piece; the pieces' output offsets come from a chained
+// scan; one block per piece compacts it in index order (exclusive scans
+// over tiles of columns), so each row's hits come out in index order.
 template <typename T>
 __global__ void radius_emit_kernel(const T *D, int n, size_t ld, T thr, int chunk,
                                    const long long *start, int *idx, T *val) {
@@ -683,103 +666,94 @@ __global__ void radius_emit_vec_kernel(const T *D, int n, size_t ld, T thr, int 
     }
 }
 int radius_chunks(int n) { return (n + RADIUS_CHUNK - 1) / RADIUS_CHUNK; }
-// Counts and output offsets of the (row, chunk) pieces in one pass: a chained
-// scan in (row, chunk) order.  Each CTA takes the next logical piece from a
-// ticket (so every piece before it has a CTA running or done), counts its
-// hits and publishes the count; thread 0 then looks back over the pieces
-// before it -- a piece's word holds 2 flag bits (1: its count, 2: its
-// inclusive prefix) and a 62-bit value -- adding counts until it meets a
-// prefix, and publishes its own inclusive prefix.  The look-back waits on
-// global memory for a predecessor that has not published yet; every wait is
-// bounded (`limit` polls), after which the CTA sets err[0] = 1 and leaves
-// its own prefix unpublished (its successors then time out as well: the
-// call fails with a status, the device stays usable).  start[piece] = the
-// exclusive prefix, total[0] = the inclusive prefix of the last piece.
-// skip_first (testing): piece 0 publishes nothing.
-template <typename T>
-__global__ void radius_count_scan_kernel(const T *D, int n, size_t ld, T thr, int chunk, int nch,
-                                         int pieces, unsigned *ticket,
-                                         unsigned long long *state, long long *start,
-                                         long long *total, int *err, unsigned limit,
-                                         int skip_first, const int *hits) {
-    __shared__ int s_id;
-    __shared__ int ws[32];
-    if (threadIdx.x == 0) s_id = (int)atomicAdd(ticket, 1u);
-    __syncthreads();
-    const int id = s_id;
-    if (id >= pieces) return;
-    const int rr = id / nch, cc = id - rr * nch;
-    const T *row = D + (size_t)rr * ld;
-    const int j1 = min(n, (cc + 1) * chunk);
-    int c = 0;
-    if (hits) { // counted by the distance kernel
-        if (threadIdx.x == 0) c = hits[id];
-    } else {
-        for (int j = cc * chunk + threadIdx.x; j < j1; j += blockDim.x) c += row[j] <= thr ? 1 : 0;
-    }
+// Output offsets of the (row, chunk) pieces from their hit counts (made by
+// the distance kernel): a chained scan in (row, chunk) order over groups of
+// 32 pieces, one warp per group.  Each warp takes the next logical group from
+// a ticket (so every group before it has a warp running or done), scans its
+// 32 counts with shuffles and publishes the group's count; lane 0 then looks
+// back over the groups before it -- a group's word holds 2 flag bits (1: its
+// count, 2: its inclusive prefix) and a 62-bit value -- adding counts until
+// it meets a prefix, and publishes the group's inclusive prefix.  The
+// look-back waits on global memory for a predecessor that has not published
+// yet; every wait is bounded (`limit` polls), after which the warp sets
+// err[0] = 1 and leaves its own prefix unpublished (its successors then time
+// out as well: the call fails with a status, the device stays usable).
+// start[piece] = the exclusive prefix, total[0] = all hits.  skip_first
+// (testing): group 0 publishes nothing.
+__global__ void __launch_bounds__(32)
+radius_scan_groups_kernel(const int *hits, int pieces, int groups, unsigned *ticket,
+                          unsigned long long *state, long long *start, long long *total,
+                          int *err, unsigned limit, int skip_first) {
+    const int lane = threadIdx.x;
+    int id = 0;
+    if (lane == 0) id = (int)atomicAdd(ticket, 1u);
+    id = __shfl_sync(0xffffffffu, id, 0);
+    if (id >= groups) return;
+    const int p = id * 32 + lane;
+    const int c = p < pieces ? hits[p] : 0;
+    int x = c; // inclusive scan of the group's counts
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
-    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
-    __syncthreads();
-    if (threadIdx.x != 0) return;
-    long long cnt = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) cnt += ws[w];
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    const long long gsum = (long long)__shfl_sync(0xffffffffu, x, 31);
     constexpr unsigned long long AGG = 1ull << 62, PRE = 2ull << 62, VAL = (1ull << 62) - 1;
-    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> me(state[id]);
-    if (id == 0) {
-        if (!skip_first) me.store(PRE | (unsigned long long)cnt, cuda::memory_order_release);
-        start[0] = 0;
-        if (pieces == 1) *total = cnt;
-        return;
-    }
-    me.store(AGG | (unsigned long long)cnt, cuda::memory_order_release);
     long long excl = 0;
-    unsigned polls = 0;
-    bool failed = false;
-    for (int j = id - 1; j >= 0;) {
-        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> pj(state[j]);
-        const unsigned long long v = pj.load(cuda::memory_order_acquire);
-        const unsigned long long flag = v & ~VAL;
-        if (flag == 0) {
-            if (++polls > limit) {
-                failed = true;
-                break;
+    int failed = 0;
+    if (lane == 0) {
+        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> me(state[id]);
+        if (id == 0) {
+            if (!skip_first) me.store(PRE | (unsigned long long)gsum, cuda::memory_order_release);
+        } else {
+            me.store(AGG | (unsigned long long)gsum, cuda::memory_order_release);
+            unsigned polls = 0;
+            for (int j = id - 1; j >= 0;) {
+                cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> pj(state[j]);
+                const unsigned long long v = pj.load(cuda::memory_order_acquire);
+                const unsigned long long flag = v & ~VAL;
+                if (flag == 0) {
+                    if (++polls > limit) {
+                        failed = 1;
+                        break;
+                    }
+                    __nanosleep(64);
+                    continue;
+                }
+                excl += (long long)(v & VAL);
+                if (flag == PRE) break;
+                --j;
             }
-            __nanosleep(64);
-            continue;
+            if (failed) atomicExch(err, 1);
+            else me.store(PRE | (unsigned long long)(excl + gsum), cuda::memory_order_release);
         }
-        excl += (long long)(v & VAL);
-        if (flag == PRE) break;
-        --j;
     }
-    if (failed) {
-        atomicExch(err, 1);
-        return;
-    }
-    me.store(PRE | (unsigned long long)(excl + cnt), cuda::memory_order_release);
-    start[id] = excl;
-    if (id == pieces - 1) *total = excl + cnt;
+    failed = __shfl_sync(0xffffffffu, failed, 0);
+    excl = __shfl_sync(0xffffffffu, excl, 0);
+    if (failed) return;
+    if (p < pieces) start[p] = excl + x - c;
+    if (p == pieces - 1) *total = excl + x;
 }
 
 template <typename T>
 cudaError_t launch_radius_count_scan(const T *D, int rows, int n, size_t ld, T thr, void *work,
                                      long long *start, long long *total, int *err, int test_wait,
                                      cudaStream_t s, const int *hits) {
+    (void)D, (void)ld, (void)thr;
     if (rows <= 0 || n <= 0) return cudaSuccess;
+    if (!hits) return cudaErrorInvalidValue;
     const int nch = radius_chunks(n);
     const int pieces = rows * nch;
+    const int groups = (pieces + 31) / 32;
     unsigned *ticket = static_cast<unsigned *>(work);
     unsigned long long *state = reinterpret_cast<unsigned long long *>(static_cast<char *>(work) + 256);
-    cudaError_t e = cudaMemsetAsync(work, 0, 256 + (size_t)pieces * 8, s);
+    cudaError_t e = cudaMemsetAsync(work, 0, 256 + (size_t)groups * 8, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), s);
     if (e != cudaSuccess) return e;
     // about a second of polling; the test mode's wait runs out in microseconds
     const unsigned limit = test_wait ? 2000u : (1u << 24);
-    // with the counts given, one warp per piece (thread 0 does the look-back)
-    radius_count_scan_kernel<T><<<pieces, hits ? 32 : 256, 0, s>>>(D, n, ld, thr, RADIUS_CHUNK,
-                                                                    nch, pieces,
-                                                      ticket, state, start, total, err, limit,
-                                                      test_wait, hits);
+    radius_scan_groups_kernel<<<groups, 32, 0, s>>>(hits, pieces, groups, ticket, state, start,
+                                                    total, err, limit, test_wait);
     return cudaGetLastError();
 }
 size_t radius_scan_work_bytes(int rows, int n) { return 256 + (size_t)rows * radius_chunks(n) * 8; }
@@ -790,14 +764,6 @@ template cudaError_t launch_radius_count_scan<double>(const double *, int, int, 
                                                       void *, long long *, long long *, int *,
                                                       int, cudaStream_t, const int *);
 
-template <typename T>
-cudaError_t launch_radius_count(const T *D, int rows, int n, size_t ld, T thr, int *cnt,
-                                cudaStream_t s) {
-    if (rows <= 0 || n <= 0) return cudaSuccess;
-    const dim3 grid(radius_chunks(n), rows);
-    radius_count_kernel<T><<<grid, 256, 0, s>>>(D, n, ld, thr, RADIUS_CHUNK, cnt);
-    return cudaGetLastError();
-}
 template <typename T>
 cudaError_t launch_radius_emit(const T *D, int rows, int n, size_t ld, T thr,
                                const long long *start, int *idx, T *val, cudaStream_t s) {
@@ -811,10 +777,6 @@ cudaError_t launch_radius_emit(const T *D, int rows, int n, size_t ld, T thr,
         radius_emit_kernel<T><<<grid, 256, 0, s>>>(D, n, ld, thr, RADIUS_CHUNK, start, idx, val);
     return cudaGetLastError();
 }
-template cudaError_t launch_radius_count<float>(const float *, int, int, size_t, float, int *,
-                                                cudaStream_t);
-template cudaError_t launch_radius_count<double>(const double *, int, int, size_t, double, int *,
-                                                 cudaStream_t);
 template cudaError_t launch_radius_emit<float>(const float *, int, int, size_t, float,
                                                const long long *, int *, float *, cudaStream_t);
 template cudaError_t launch_radius_emit<double>(const double *, int, int, size_t, double,

@@ -1,8 +1,8 @@
 """A bounded wait on global memory that runs out: the radius search computes
-its output offsets with a chained scan in which every block waits for the
-blocks before it.  AOCLDA_B200_TEST_RADIUS_WAIT=1 keeps the first block from
-publishing its count -- a flag that nothing sets -- and shortens the waits;
-every waiting block gives up at its limit and the call returns
+its output offsets with a chained scan in which every group of 32 pieces
+waits for the groups before it.  AOCLDA_B200_TEST_RADIUS_WAIT=1 keeps the
+first group from publishing its count -- a flag that nothing sets -- and
+shortens the waits; every waiting group gives up at its limit and the call returns
 da_status_internal_error instead of hanging.  The same handle, and a fresh
 one, then search normally: the device stays usable."""
 import os
